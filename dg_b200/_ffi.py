@@ -1,0 +1,115 @@
+"""ctypes binding of the C ABI declared in include/dgb.h (loads the in-tree libdgb.so)."""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from pathlib import Path
+
+import numpy as np
+
+LIB_PATH = Path(__file__).resolve().parent / "lib" / "libdgb.so"
+
+# enum values (include/dgb.h)
+OK, ERR_ARG, ERR_IO, ERR_MESH, ERR_UNSUPPORTED, ERR_CUDA, ERR_NONFINITE, ERR_DT_SMALL, ERR_TIMEOUT, ERR_NO_DEVICE = range(10)
+FLUX = {"rusanov": 0, "rus": 0, "llf": 0, "hll": 1, "roe": 2}
+LIMITER = {"none": 0, "hrl": 1, "m2l": 2, "hri": 3, "m2i": 4, "prl": 5, "pri": 6, "p0i": 7}
+SSPRK3, RK4 = 3, 4
+BC = {"periodic": 1, "transmissive": 2, "reflective": 3, "frozen": 4}
+
+# every exported entry point of include/dgb.h
+EXPORTS = [
+    "dgb_last_error", "dgb_abi_version", "dgb_problem_from_deck", "dgb_problem_structured",
+    "dgb_mesh_write_msh", "dgb_problem_destroy", "dgb_problem_info", "dgb_problem_array_size",
+    "dgb_problem_get_array", "dgb_problem_init_state", "dgb_write_pos", "dgb_read_pos", "dgb_create",
+    "dgb_destroy", "dgb_set_state", "dgb_get_state", "dgb_set_state_device", "dgb_get_state_device",
+    "dgb_residual", "dgb_solve", "dgb_limit", "dgb_dt_from_cfl", "dgb_advance", "dgb_last_dt",
+    "dgb_conservation", "dgb_last_timing", "dgb_set_profiling", "dgb_kernel_timing",
+]
+
+
+class MeshSpec(C.Structure):
+    _fields_ = [("dim", C.c_int), ("order", C.c_int), ("nx", C.c_int), ("ny", C.c_int),
+                ("x0", C.c_double), ("x1", C.c_double), ("y0", C.c_double), ("y1", C.c_double),
+                ("bc", C.c_int * 4)]
+
+
+class Options(C.Structure):
+    _fields_ = [("flux", C.c_int), ("limiter", C.c_int), ("cfl", C.c_double),
+                ("thresholds", C.c_double * 3), ("n_thresholds", C.c_int)]
+
+
+class Info(C.Structure):
+    _fields_ = [(n, C.c_int) for n in
+                "dim order n_fields n_elem n_s n_g n_ifaces m_s m_g n_n n_reflective cartesian "
+                "gpu_supported flux limiter nx ny".split()] + \
+               [(n, C.c_double) for n in "cfl dx_min cfl_scaled final_time".split()] + \
+               [("n_output_times", C.c_int)]
+
+
+class DGBError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"dgb error {code}: {msg}")
+        self.code = code
+
+
+_lib = None
+
+
+def lib() -> C.CDLL:
+    """Loads libdgb.so; raises if it is missing (no fallback path exists)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    path = Path(os.environ.get("DGB_LIB", LIB_PATH))
+    if not path.exists():
+        raise ImportError(f"{path} is not built; run `python -m dg_b200.build`")
+    L = C.CDLL(str(path))
+    vp, ip, dp, cp = C.c_void_p, C.c_int, C.POINTER(C.c_double), C.c_char_p
+    L.dgb_last_error.restype = cp
+    L.dgb_abi_version.restype = ip
+    sig = {
+        "dgb_problem_from_deck": [cp, C.POINTER(vp)],
+        "dgb_problem_structured": [C.POINTER(MeshSpec), C.POINTER(Options), C.POINTER(vp)],
+        "dgb_mesh_write_msh": [C.POINTER(MeshSpec), cp],
+        "dgb_problem_info": [vp, C.POINTER(Info)],
+        "dgb_problem_array_size": [vp, cp, C.POINTER(C.c_size_t)],
+        "dgb_problem_get_array": [vp, cp, vp, C.c_size_t],
+        "dgb_problem_init_state": [vp, cp, dp, ip, C.c_uint64, dp],
+        "dgb_write_pos": [vp, dp, ip, C.c_double, cp],
+        "dgb_read_pos": [vp, ip, cp, dp, dp],
+        "dgb_create": [vp, ip, C.POINTER(vp)],
+        "dgb_set_state": [vp, dp],
+        "dgb_get_state": [vp, dp],
+        "dgb_set_state_device": [vp, vp],
+        "dgb_get_state_device": [vp, vp],
+        "dgb_residual": [vp, dp, dp],
+        "dgb_solve": [vp, C.c_double, dp, dp],
+        "dgb_limit": [vp, dp],
+        "dgb_dt_from_cfl": [vp, dp, dp],
+        "dgb_advance": [vp, ip, ip, C.c_double, dp],
+        "dgb_last_dt": [vp, dp],
+        "dgb_conservation": [vp, dp],
+        "dgb_last_timing": [vp, dp, C.POINTER(C.c_longlong)],
+        "dgb_set_profiling": [vp, ip],
+        "dgb_kernel_timing": [vp, cp, dp, C.POINTER(C.c_longlong)],
+    }
+    for name, args in sig.items():
+        f = getattr(L, name)
+        f.argtypes = args
+        f.restype = ip
+    L.dgb_problem_destroy.argtypes = [vp]
+    L.dgb_problem_destroy.restype = None
+    L.dgb_destroy.argtypes = [vp]
+    L.dgb_destroy.restype = None
+    _lib = L
+    return L
+
+
+def check(rc: int) -> None:
+    if rc != OK:
+        raise DGBError(rc, lib().dgb_last_error().decode())
+
+
+def dptr(a: np.ndarray):
+    assert a.dtype == np.float64 and a.flags["C_CONTIGUOUS"]
+    return a.ctypes.data_as(C.POINTER(C.c_double))

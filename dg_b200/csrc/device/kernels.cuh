@@ -1,0 +1,714 @@
+// sm_100a kernels of the DG residual / time-step path (FP64 plain form).
+//
+//   residual2d_kernel  fused  collocation -> volume flux/source -> lift  +  face traces ->
+//                      Riemann flux -> face lift  +  inverse mass  +  RK stage update.
+//                      Replaces the 13 launches of DG_SOLVER::dg_solver
+//                      (code/src/dg/dg_solver.h:292-364) plus Lsolver and the BLAS axpy/copy
+//                      of RK::RK_integration (code/src/time_integration/rk.cc:164-198).
+//   residual1d_kernel  the same for 1D, one thread per element.
+//   lim*_kernel        hierarchical-reconstruction limiters HR / m2 (code/src/limiting/limiting.cc:11-594)
+//   wavespeed_kernel   max |u|+a for the CFL step (code/src/time_integration/rk.cc:250-272)
+//
+// Work decomposition of residual2d_kernel: one CTA owns TE consecutive elements and stages their
+// nodal state (and the neighbours' face traces) in shared memory; threads then sweep
+// (element, quadrature point), (element, field, node) and (element, face, face point) work items.
+// Every face flux is computed by both owners with the same canonical orientation (left/bottom
+// element as the "L" state, +x/+y normal), so the two copies are bit-identical and the scheme
+// stays exactly conservative without atomics.
+#pragma once
+#include "common.cuh"
+#include "physics.cuh"
+
+namespace dgb {
+
+// Modes of the residual kernels.
+enum { MODE_RESIDUAL = 0,  // out = S + F + Q                         (dg_solver)
+       MODE_SSP = 1,       // out = a*Ubase + b*(U + dt*Minv*(S+F+Q))  (SSP-RK stage)
+       MODE_RK4 = 2 };     // out = dt*Minv*(S+F+Q); Uacc += b*out     (Lsolver + axpy)
+
+struct StageArgs {
+  const double* __restrict__ U;      // stage input (internal layout)
+  const double* __restrict__ Ubase;  // SSP: U^n
+  double* __restrict__ out;
+  double* __restrict__ Uacc;         // RK4 accumulator (may be null)
+  const int* __restrict__ nbr;       // [face][ld] neighbours, boundary codes < 0
+  const DevScalars* __restrict__ scal;
+  double a, b;
+  double dt_override;                // > 0: use this step instead of scal->dt
+};
+
+__device__ __forceinline__ void copy_consts(Consts& dst, const Consts& src) {
+  const unsigned long long* s = reinterpret_cast<const unsigned long long*>(&src);
+  unsigned long long* d = reinterpret_cast<unsigned long long*>(&dst);
+  for (int k = threadIdx.x; k < (int)(sizeof(Consts) / 8); k += blockDim.x) d[k] = s[k];
+}
+
+template <int P>
+struct Dims2 {
+  static constexpr int N1 = P + 1;
+  static constexpr int NG1 = (P == 1) ? 2 : P + 2;
+  static constexpr int NS = N1 * N1;
+  static constexpr int NG = NG1 * NG1;
+  static constexpr int NF = 5;
+};
+
+template <int P, int TE>
+constexpr size_t residual2d_smem_doubles() {
+  using Dm = Dims2<P>;
+  constexpr size_t g1 = (size_t)9 * Dm::NG * TE;
+  constexpr size_t g2 = (size_t)Dm::NF * 4 * Dm::N1 * TE;
+  return (size_t)Dm::NF * Dm::NS * TE * 2 + (size_t)4 * Dm::NF * Dm::N1 * TE + (g1 > g2 ? g1 : g2) +
+         (size_t)3 * Dm::NG * Dm::NS;
+}
+
+// node of face k (0 L, 1 R, 2 D, 3 U) at face position j, and the matching node of the
+// neighbour across that face
+template <int P>
+__device__ __forceinline__ int face_node(int k, int j) {
+  constexpr int N1 = P + 1;
+  return k == 0 ? N1 * j : k == 1 ? P + N1 * j : k == 2 ? j : j + N1 * P;
+}
+template <int P>
+__device__ __forceinline__ int across_node(int k, int j) {
+  constexpr int N1 = P + 1;
+  return k == 0 ? P + N1 * j : k == 1 ? N1 * j : k == 2 ? j + N1 * P : j;
+}
+
+template <int P, int FLUX, int MODE, int TE, int NT>
+__global__ void __launch_bounds__(NT) residual2d_kernel(const Consts cin, const StageArgs a) {
+  using Dm = Dims2<P>;
+  constexpr int N1 = Dm::N1, NG1 = Dm::NG1, NS = Dm::NS, NG = Dm::NG, NF = Dm::NF;
+  constexpr int GSZ = (9 * NG * TE > NF * 4 * N1 * TE) ? 9 * NG * TE : NF * 4 * N1 * TE;
+  __shared__ Consts c;
+  extern __shared__ double sm[];
+  double* Us = sm;                        // [NF][NS][TE]
+  double* Uh = Us + NF * NS * TE;         // [4][NF][N1][TE]  neighbour traces
+  double* Rs = Uh + 4 * NF * N1 * TE;     // [NF][NS][TE]     residual
+  double* G = Rs + NF * NS * TE;          // volume: [9][NG][TE]; faces: [NF][4][N1][TE]
+  double* Phi = G + GSZ;                  // [NG][NS]
+  double* dPx = Phi + NG * NS;
+  double* dPy = dPx + NG * NS;
+
+  const int tid = threadIdx.x;
+  copy_consts(c, cin);
+  if (a.scal && a.scal->flags) return;  // a failed CFL step stops the integration here
+  __syncthreads();
+  const int ld = c.ld, NE = c.n_elem;
+  const int e0 = blockIdx.x * TE;
+  for (int i = tid; i < NG * NS; i += NT) {
+    const int g = i / NS, t = i % NS, gx = g / NG1, gy = g % NG1, ix = t % N1, iy = t / N1;
+    Phi[i] = c.Bq[gx][ix] * c.Bq[gy][iy];
+    dPx[i] = c.Dq[gx][ix] * c.Bq[gy][iy];
+    dPy[i] = c.Bq[gx][ix] * c.Dq[gy][iy];
+  }
+  // ---- stage the tile's state and the neighbours' face traces ----
+  for (int i = tid; i < NF * NS * TE; i += NT) {
+    const int el = i % TE, ft = i / TE, e = e0 + el;
+    Us[i] = e < NE ? __ldg(a.U + (size_t)ft * ld + e) : 0.0;
+  }
+  for (int i = tid; i < 4 * NF * N1 * TE; i += NT) {
+    const int el = i % TE;
+    int r = i / TE;
+    const int j = r % N1;
+    r /= N1;
+    const int f = r % NF, k = r / NF, e = e0 + el;
+    double v = 0.0;
+    if (e < NE) {
+      const int nb = __ldg(a.nbr + (size_t)k * ld + e);
+      if (nb >= 0) v = __ldg(a.U + (size_t)(f * NS + across_node<P>(k, j)) * ld + nb);
+      else {
+        v = __ldg(a.U + (size_t)(f * NS + face_node<P>(k, j)) * ld + e);
+        // reflective wall: mirror the wall-normal momentum (rflctive, code/src/bc/boundaries.cu:20-67)
+        if (nb == -3 && ((k < 2 && f == 1) || (k >= 2 && f == 2))) v = -v;
+      }
+    }
+    Uh[i] = v;
+  }
+  __syncthreads();
+
+  // ---- volume: states, fluxes and the alpha source at the quadrature points ----
+  for (int i = tid; i < NG * TE; i += NT) {
+    const int el = i % TE, g = i / TE;
+    if (e0 + el >= NE) continue;
+    double ug[NF] = {0, 0, 0, 0, 0}, dax = 0, day = 0;
+#pragma unroll
+    for (int t = 0; t < NS; ++t) {
+      const double ph = Phi[g * NS + t];
+#pragma unroll
+      for (int f = 0; f < NF; ++f) ug[f] += ph * Us[(f * NS + t) * TE + el];
+      const double al = Us[(4 * NS + t) * TE + el];
+      dax += dPx[g * NS + t] * al;
+      day += dPy[g * NS + t] * al;
+    }
+    const double rho = ug[0], u = ug[1] / rho, v = ug[2] / rho, Et = ug[3];
+    const double gamma = 1 + 1.0 / ug[4];
+    const double p = (gamma - 1) * (Et - 0.5 * rho * (u * u + v * v));
+    const double W = c.wq[g / NG1] * c.wq[g % NG1];
+    const double cx = W * (c.ixx * c.J), cy = W * (c.iyy * c.J);
+    G[(0 * NG + g) * TE + el] = cx * (rho * u);
+    G[(1 * NG + g) * TE + el] = cx * (rho * u * u + p);
+    G[(2 * NG + g) * TE + el] = cx * (rho * u * v);
+    G[(3 * NG + g) * TE + el] = cx * ((Et + p) * u);
+    G[(4 * NG + g) * TE + el] = cy * (rho * v);
+    G[(5 * NG + g) * TE + el] = cy * (rho * u * v);
+    G[(6 * NG + g) * TE + el] = cy * (rho * v * v + p);
+    G[(7 * NG + g) * TE + el] = cy * ((Et + p) * v);
+    // GAMNCON source -u.grad(alpha) (physics.cu:282-291)
+    const double s = -u * dax * c.ixx - v * day * c.iyy;
+    G[(8 * NG + g) * TE + el] = (W * c.J) * s;
+  }
+  __syncthreads();
+  // ---- volume lift: F = dphi_w^T fJ, S = phi_w^T sJ ----
+  for (int i = tid; i < NF * NS * TE; i += NT) {
+    const int el = i % TE, ft = i / TE, f = ft / NS, t = ft % NS;
+    double r = 0.0;
+    if (f < 4) {
+#pragma unroll 4
+      for (int g = 0; g < NG; ++g)
+        r += dPx[g * NS + t] * G[(f * NG + g) * TE + el] + dPy[g * NS + t] * G[((4 + f) * NG + g) * TE + el];
+    } else {
+#pragma unroll 4
+      for (int g = 0; g < NG; ++g) r += Phi[g * NS + t] * G[(8 * NG + g) * TE + el];
+    }
+    Rs[i] = r;
+  }
+  __syncthreads();
+  // ---- faces: Riemann flux at the face quadrature points ----
+  for (int i = tid; i < 4 * N1 * TE; i += NT) {
+    const int el = i % TE, r = i / TE, g = r % N1, k = r / N1, e = e0 + el;
+    if (e >= NE) continue;
+    double uo[NF], un[NF];
+#pragma unroll
+    for (int f = 0; f < NF; ++f) {
+      double so = 0, sn = 0;
+#pragma unroll
+      for (int j = 0; j < N1; ++j) {
+        so += c.Bf[g][j] * Us[(f * NS + face_node<P>(k, j)) * TE + el];
+        sn += c.Bf[g][j] * Uh[((k * NF + f) * N1 + j) * TE + el];
+      }
+      uo[f] = so;
+      un[f] = sn;
+    }
+    const int nb = __ldg(a.nbr + (size_t)k * ld + e);
+    const bool xface = k < 2;
+    // interior faces use the canonical orientation (left/bottom element is L, normal +x/+y);
+    // boundary faces take the element as L with its outward normal
+    const bool swapLR = nb >= 0 && (k == 0 || k == 2);
+    const double sgn = swapLR ? 1.0 : -1.0;
+    double nx = xface ? 1.0 : 0.0, ny = xface ? 0.0 : 1.0;
+    if (nb < 0 && k == 0) nx = -1.0;
+    if (nb < 0 && k == 2) ny = -1.0;
+    double L[NF], R[NF];
+#pragma unroll
+    for (int f = 0; f < NF; ++f) { L[f] = swapLR ? un[f] : uo[f]; R[f] = swapLR ? uo[f] : un[f]; }
+    double F[NF], nc;
+    phys::riemann2d<FLUX>(L[0], R[0], L[1] / L[0], R[1] / R[0], L[2] / L[0], R[2] / R[0], L[3], R[3], L[4], R[4], nx,
+                          ny, F, nc);
+    const double jw = (xface ? c.JFx : c.JFy) * c.wf[g];
+#pragma unroll
+    for (int f = 0; f < NF; ++f) {
+      const double q = sgn * F[f] + (f == 4 ? nc : 0.0);
+      G[((f * 4 + k) * N1 + g) * TE + el] = q * jw;
+    }
+  }
+  __syncthreads();
+  // ---- face lift and total ----
+  for (int i = tid; i < NF * NS * TE; i += NT) {
+    const int el = i % TE, ft = i / TE, f = ft / NS, t = ft % NS, e = e0 + el;
+    const int ix = t % N1, iy = t / N1;
+    double r = Rs[i];
+#pragma unroll
+    for (int g = 0; g < N1; ++g) {
+      if (ix == 0) r += c.Bf[g][iy] * G[((f * 4 + 0) * N1 + g) * TE + el];
+      if (ix == P) r += c.Bf[g][iy] * G[((f * 4 + 1) * N1 + g) * TE + el];
+      if (iy == 0) r += c.Bf[g][ix] * G[((f * 4 + 2) * N1 + g) * TE + el];
+      if (iy == P) r += c.Bf[g][ix] * G[((f * 4 + 3) * N1 + g) * TE + el];
+    }
+    if (MODE == MODE_RESIDUAL) {
+      if (e < NE) a.out[(size_t)ft * ld + e] = r;
+    } else {
+      Rs[i] = r;
+    }
+  }
+  if (MODE == MODE_RESIDUAL) return;
+  __syncthreads();
+  // ---- epilogue: DU = dt Minv R and the stage update ----
+  const double dt = a.dt_override > 0 ? a.dt_override : a.scal->dt;
+  for (int i = tid; i < NF * NS * TE; i += NT) {
+    const int el = i % TE, ft = i / TE, f = ft / NS, t = ft % NS, e = e0 + el;
+    if (e >= NE) continue;
+    double s = 0.0;
+#pragma unroll
+    for (int tt = 0; tt < NS; ++tt) s += c.Minv[t][tt] * Rs[(f * NS + tt) * TE + el];
+    const double du = dt * s;
+    const size_t gi = (size_t)ft * ld + e;
+    if (MODE == MODE_SSP) {
+      const double base = a.a != 0.0 ? a.a * __ldg(a.Ubase + gi) : 0.0;
+      a.out[gi] = base + a.b * (Us[i] + du);
+    } else {
+      a.out[gi] = du;
+      if (a.Uacc) a.Uacc[gi] += a.b * du;
+    }
+  }
+}
+
+// ------------------------------------------------------------------------------------------
+// 1D: one thread per element, everything in registers
+// ------------------------------------------------------------------------------------------
+template <int P, int FLUX, int MODE>
+__global__ void __launch_bounds__(128) residual1d_kernel(const Consts cin, const StageArgs a) {
+  constexpr int N1 = P + 1, NG = P + 1, NF = 4;
+  __shared__ Consts c;
+  copy_consts(c, cin);
+  if (a.scal && a.scal->flags) return;
+  __syncthreads();
+  const int ld = c.ld, e = blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= c.n_elem) return;
+  double u[NF][N1], r[NF][N1];
+#pragma unroll
+  for (int f = 0; f < NF; ++f)
+#pragma unroll
+    for (int t = 0; t < N1; ++t) { u[f][t] = __ldg(a.U + (size_t)(f * N1 + t) * ld + e); r[f][t] = 0.0; }
+  // volume
+#pragma unroll
+  for (int g = 0; g < NG; ++g) {
+    double ug[NF] = {0, 0, 0, 0}, da = 0;
+#pragma unroll
+    for (int t = 0; t < N1; ++t) {
+#pragma unroll
+      for (int f = 0; f < NF; ++f) ug[f] += c.Bq[g][t] * u[f][t];
+      da += c.Dq[g][t] * u[3][t];
+    }
+    const double rho = ug[0], vx = ug[1] / rho, Et = ug[2];
+    const double gamma = 1 + 1.0 / ug[3];
+    const double p = (gamma - 1) * (Et - 0.5 * rho * vx * vx);
+    const double cx = c.wq[g] * (c.ixx * c.J);
+    const double fx[3] = {rho * vx, rho * vx * vx + p, (Et + p) * vx};
+    const double s = (c.wq[g] * c.J) * (-vx * da * c.ixx);  // physics.cu:126-127
+#pragma unroll
+    for (int t = 0; t < N1; ++t) {
+#pragma unroll
+      for (int f = 0; f < 3; ++f) r[f][t] += c.Dq[g][t] * (cx * fx[f]);
+      r[3][t] += c.Bq[g][t] * s;
+    }
+  }
+  // faces: left (node 0, x = -1) and right (node P, x = +1)
+#pragma unroll
+  for (int side = 0; side < 2; ++side) {
+    const int nb = __ldg(a.nbr + (size_t)side * ld + e);
+    const int to = side == 0 ? 0 : P;
+    double uo[NF], un[NF];
+#pragma unroll
+    for (int f = 0; f < NF; ++f) {
+      uo[f] = u[f][to];
+      if (nb >= 0) un[f] = __ldg(a.U + (size_t)(f * N1 + (side == 0 ? P : 0)) * ld + nb);
+      else un[f] = (nb == -3 && f == 1) ? -uo[f] : uo[f];
+    }
+    const bool swapLR = side == 0 && nb >= 0;
+    const double sgn = swapLR ? 1.0 : -1.0;
+    const double nx = (side == 0 && nb < 0) ? -1.0 : 1.0;
+    double L[NF], R[NF];
+#pragma unroll
+    for (int f = 0; f < NF; ++f) { L[f] = swapLR ? un[f] : uo[f]; R[f] = swapLR ? uo[f] : un[f]; }
+    double F[NF], nc;
+    phys::riemann1d<FLUX>(L[0], R[0], L[1] / L[0], R[1] / R[0], L[2], R[2], L[3], R[3], nx, F, nc);
+#pragma unroll
+    for (int f = 0; f < NF; ++f) r[f][to] += sgn * F[f] + (f == 3 ? nc : 0.0);
+  }
+  if (MODE == MODE_RESIDUAL) {
+#pragma unroll
+    for (int f = 0; f < NF; ++f)
+#pragma unroll
+      for (int t = 0; t < N1; ++t) a.out[(size_t)(f * N1 + t) * ld + e] = r[f][t];
+    return;
+  }
+  const double dt = a.dt_override > 0 ? a.dt_override : a.scal->dt;
+#pragma unroll
+  for (int f = 0; f < NF; ++f)
+#pragma unroll
+    for (int t = 0; t < N1; ++t) {
+      double s = 0.0;
+#pragma unroll
+      for (int tt = 0; tt < N1; ++tt) s += c.Minv[t][tt] * r[f][tt];
+      const double du = dt * s;
+      const size_t gi = (size_t)(f * N1 + t) * ld + e;
+      if (MODE == MODE_SSP) {
+        const double base = a.a != 0.0 ? a.a * __ldg(a.Ubase + gi) : 0.0;
+        a.out[gi] = base + a.b * (u[f][t] + du);
+      } else {
+        a.out[gi] = du;
+        if (a.Uacc) a.Uacc[gi] += a.b * du;
+      }
+    }
+}
+
+// ------------------------------------------------------------------------------------------
+// Limiters.  Fields are limited slice by slice in the scaled Taylor basis (T, Tinv).
+// ------------------------------------------------------------------------------------------
+template <int N1>
+__device__ __forceinline__ void to_mono(const Consts& c, const double* v, double* a) {
+#pragma unroll
+  for (int m = 0; m < N1; ++m) {
+    double s = 0;
+#pragma unroll
+    for (int i = 0; i < N1; ++i) s += c.T[m][i] * v[i];
+    a[m] = s;
+  }
+}
+template <int N1>
+__device__ __forceinline__ void to_lag(const Consts& c, const double* a, double* v) {
+#pragma unroll
+  for (int i = 0; i < N1; ++i) {
+    double s = 0;
+#pragma unroll
+    for (int m = 0; m < N1; ++m) s += c.Tinv[i][m] * a[m];
+    v[i] = s;
+  }
+}
+
+// Limit one slice given the nodal values of the centre and (when interior) both neighbours.
+// phys: 0 interior, 2/3 flatten (zero-gradient / reflective), 4 leave unchanged, 5 copy
+// (reflective wall-normal momentum under HR limiting, hrl1D limiting_kernels.cu:291-302).
+template <int P>
+__device__ __forceinline__ void limit_slice(const Consts& c, int phys, const double* vL, const double* vC,
+                                            const double* vR, double* lim) {
+  constexpr int N1 = P + 1;
+  double aC[N1];
+  to_mono<N1>(c, vC, aC);
+  if (phys == 0) {
+    double aL[N1], aR[N1];
+    to_mono<N1>(c, vL, aL);
+    to_mono<N1>(c, vR, aR);
+    limit_monomial<P>(c, aL, aC, aR, lim);
+  } else if (phys == 2 || phys == 3) {
+    average_monomial<P>(c, aC, lim);
+  } else {
+#pragma unroll
+    for (int m = 0; m < N1; ++m) lim[m] = aC[m];
+  }
+}
+
+// rho e = Leibniz product of the monomial p and alpha (internal_energy_multifluid,
+// limiting_kernels.cu:160-199), then E (reconstruct_energy, limiting_kernels.cu:111-156)
+template <int P>
+__device__ __forceinline__ void reconstruct_energy(const Consts& c, const double* plim, const double* alim,
+                                                   const double* Kmono, const double* Emono, double* Elim) {
+  constexpr int N1 = P + 1;
+  constexpr double binom[4][4] = {{1, 0, 0, 0}, {1, 1, 0, 0}, {1, 2, 1, 0}, {1, 3, 3, 1}};
+  double rhoe[N1];
+#pragma unroll
+  for (int m = 0; m < N1; ++m) {
+    double I = 0;
+#pragma unroll
+    for (int k = 0; k <= m; ++k) I += binom[m][k] * plim[m - k] * alim[k];
+    rhoe[m] = I;
+  }
+#pragma unroll
+  for (int m = 1; m < N1; ++m) Elim[m] = rhoe[m] + Kmono[m];
+  double E0 = Emono[0];
+#pragma unroll
+  for (int k = 2; k < N1; k += 2) E0 -= c.ifact[k + 1] * (Elim[k] - Emono[k]);
+  Elim[0] = E0;
+}
+
+__device__ __forceinline__ int boundary_code(int left, int right) {
+  int phys = 0;
+  if (left < 0) phys = -left;
+  if (right < 0) phys = -right;
+  return phys;
+}
+
+// 2D x pass, one thread per (element, y-slice).  METHOD 2 (m2): rho, rho u, rho v, alpha and
+// p are limited and E rebuilt; output X = [rho, rhou, rhov, alpha, p, E] (Lagrange).
+// METHOD 1 (HR): all conserved fields limited; output X = the five conserved fields.
+template <int P, int METHOD>
+__global__ void __launch_bounds__(128) lim2d_xpass_kernel(const Consts cin, const double* __restrict__ U,
+                                                          const int* __restrict__ nbr, double* __restrict__ X,
+                                                          const DevScalars* __restrict__ scal) {
+  constexpr int N1 = P + 1, NS = N1 * N1;
+  __shared__ Consts c;
+  copy_consts(c, cin);
+  if (scal && scal->flags) return;
+  __syncthreads();
+  const int ld = c.ld, e = blockIdx.x * blockDim.x + threadIdx.x, iy = blockIdx.y;
+  if (e >= c.n_elem) return;
+  const int nL = __ldg(nbr + e), nR = __ldg(nbr + (size_t)ld + e);
+  const int phys = boundary_code(nL, nR);
+  double v[3][5][N1];  // [L,C,R][field][ix]
+#pragma unroll
+  for (int s = 0; s < 3; ++s) {
+    const int el = s == 0 ? nL : s == 1 ? e : nR;
+    if (s != 1 && phys != 0) continue;
+#pragma unroll
+    for (int f = 0; f < 5; ++f)
+#pragma unroll
+      for (int ix = 0; ix < N1; ++ix) v[s][f][ix] = __ldg(U + (size_t)(f * NS + ix + N1 * iy) * ld + el);
+  }
+  if (METHOD == 1) {
+#pragma unroll
+    for (int f = 0; f < 5; ++f) {
+      double lim[N1], out[N1];
+      const int ph = (phys == 3 && f == 1) ? 5 : phys;
+      limit_slice<P>(c, ph, v[0][f], v[1][f], v[2][f], lim);
+      to_lag<N1>(c, lim, out);
+#pragma unroll
+      for (int ix = 0; ix < N1; ++ix) X[(size_t)(f * NS + ix + N1 * iy) * ld + e] = out[ix];
+    }
+    return;
+  }
+  // pressure from the unlimited state (pressure kernel, physics.cu:891-958)
+  double pr[3][N1];
+#pragma unroll
+  for (int s = 0; s < 3; ++s) {
+    if (s != 1 && phys != 0) continue;
+#pragma unroll
+    for (int ix = 0; ix < N1; ++ix) {
+      const double rho = v[s][0][ix], ru = v[s][1][ix], rv = v[s][2][ix], E = v[s][3][ix];
+      const double gamma = 1.0 + 1.0 / v[s][4][ix];
+      pr[s][ix] = (gamma - 1) * (E - 0.5 * (ru * ru + rv * rv) / rho);
+    }
+  }
+  double lr[N1], lu[N1], lv[N1], la[N1], lp[N1];
+  limit_slice<P>(c, phys, v[0][0], v[1][0], v[2][0], lr);
+  limit_slice<P>(c, phys, v[0][1], v[1][1], v[2][1], lu);
+  limit_slice<P>(c, phys, v[0][2], v[1][2], v[2][2], lv);
+  limit_slice<P>(c, phys, v[0][4], v[1][4], v[2][4], la);
+  limit_slice<P>(c, phys, pr[0], pr[1], pr[2], lp);
+  double r_[N1], u_[N1], v_[N1], a_[N1], p_[N1], K[N1], Km[N1], Em[N1], El[N1], E_[N1];
+  to_lag<N1>(c, lr, r_);
+  to_lag<N1>(c, lu, u_);
+  to_lag<N1>(c, lv, v_);
+  to_lag<N1>(c, la, a_);
+  to_lag<N1>(c, lp, p_);
+#pragma unroll
+  for (int ix = 0; ix < N1; ++ix) K[ix] = 0.5 * (u_[ix] * u_[ix] + v_[ix] * v_[ix]) / r_[ix];
+  to_mono<N1>(c, K, Km);
+  to_mono<N1>(c, v[1][3], Em);
+  reconstruct_energy<P>(c, lp, la, Km, Em, El);
+  to_lag<N1>(c, El, E_);
+  const double* outs[6] = {r_, u_, v_, a_, p_, E_};
+#pragma unroll
+  for (int q = 0; q < 6; ++q)
+#pragma unroll
+    for (int ix = 0; ix < N1; ++ix) X[(size_t)(q * NS + ix + N1 * iy) * ld + e] = outs[q][ix];
+}
+
+// 2D y pass, one thread per (element, x-column): reads the x-pass output X of the element and
+// its bottom/top neighbours and writes the limited conserved state.
+template <int P, int METHOD>
+__global__ void __launch_bounds__(128) lim2d_ypass_kernel(const Consts cin, const double* __restrict__ X,
+                                                          const int* __restrict__ nbr, double* __restrict__ Uout,
+                                                          const DevScalars* __restrict__ scal) {
+  constexpr int N1 = P + 1, NS = N1 * N1;
+  constexpr int NQ = METHOD == 1 ? 5 : 6;
+  __shared__ Consts c;
+  copy_consts(c, cin);
+  if (scal && scal->flags) return;
+  __syncthreads();
+  const int ld = c.ld, e = blockIdx.x * blockDim.x + threadIdx.x, ix = blockIdx.y;
+  if (e >= c.n_elem) return;
+  const int nD = __ldg(nbr + (size_t)2 * ld + e), nU = __ldg(nbr + (size_t)3 * ld + e);
+  const int phys = boundary_code(nD, nU);
+  double v[3][NQ][N1];  // [D,C,U][field][iy]
+#pragma unroll
+  for (int s = 0; s < 3; ++s) {
+    const int el = s == 0 ? nD : s == 1 ? e : nU;
+    if (s != 1 && phys != 0) continue;
+#pragma unroll
+    for (int q = 0; q < NQ; ++q)
+#pragma unroll
+      for (int iy = 0; iy < N1; ++iy) v[s][q][iy] = __ldg(X + (size_t)(q * NS + ix + N1 * iy) * ld + el);
+  }
+  if (METHOD == 1) {
+#pragma unroll
+    for (int f = 0; f < 5; ++f) {
+      double lim[N1], out[N1];
+      const int ph = (phys == 3 && f == 2) ? 5 : phys;
+      limit_slice<P>(c, ph, v[0][f], v[1][f], v[2][f], lim);
+      to_lag<N1>(c, lim, out);
+#pragma unroll
+      for (int iy = 0; iy < N1; ++iy) Uout[(size_t)(f * NS + ix + N1 * iy) * ld + e] = out[iy];
+    }
+    return;
+  }
+  double lr[N1], lu[N1], lv[N1], la[N1], lp[N1];
+  limit_slice<P>(c, phys, v[0][0], v[1][0], v[2][0], lr);
+  limit_slice<P>(c, phys, v[0][1], v[1][1], v[2][1], lu);
+  limit_slice<P>(c, phys, v[0][2], v[1][2], v[2][2], lv);
+  limit_slice<P>(c, phys, v[0][3], v[1][3], v[2][3], la);
+  limit_slice<P>(c, phys, v[0][4], v[1][4], v[2][4], lp);
+  double r_[N1], u_[N1], v_[N1], a_[N1], K[N1], Km[N1], Em[N1], El[N1], E_[N1];
+  to_lag<N1>(c, lr, r_);
+  to_lag<N1>(c, lu, u_);
+  to_lag<N1>(c, lv, v_);
+  to_lag<N1>(c, la, a_);
+#pragma unroll
+  for (int iy = 0; iy < N1; ++iy) K[iy] = 0.5 * (u_[iy] * u_[iy] + v_[iy] * v_[iy]) / r_[iy];
+  to_mono<N1>(c, K, Km);
+  to_mono<N1>(c, v[1][5], Em);
+  reconstruct_energy<P>(c, lp, la, Km, Em, El);
+  to_lag<N1>(c, El, E_);
+  const double* outs[5] = {r_, u_, v_, E_, a_};
+#pragma unroll
+  for (int f = 0; f < 5; ++f)
+#pragma unroll
+    for (int iy = 0; iy < N1; ++iy) Uout[(size_t)(f * NS + ix + N1 * iy) * ld + e] = outs[f][iy];
+}
+
+// 1D HR / m2 limiter, one thread per element, in place through Uout (reads U).
+template <int P, int METHOD>
+__global__ void __launch_bounds__(128) lim1d_kernel(const Consts cin, const double* __restrict__ U,
+                                                    const int* __restrict__ nbr, double* __restrict__ Uout,
+                                                    const DevScalars* __restrict__ scal) {
+  constexpr int N1 = P + 1;
+  __shared__ Consts c;
+  copy_consts(c, cin);
+  if (scal && scal->flags) return;
+  __syncthreads();
+  const int ld = c.ld, e = blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= c.n_elem) return;
+  const int nL = __ldg(nbr + e), nR = __ldg(nbr + (size_t)ld + e);
+  const int phys = boundary_code(nL, nR);
+  double v[3][4][N1];
+#pragma unroll
+  for (int s = 0; s < 3; ++s) {
+    const int el = s == 0 ? nL : s == 1 ? e : nR;
+    if (s != 1 && phys != 0) continue;
+#pragma unroll
+    for (int f = 0; f < 4; ++f)
+#pragma unroll
+      for (int i = 0; i < N1; ++i) v[s][f][i] = __ldg(U + (size_t)(f * N1 + i) * ld + el);
+  }
+  if (METHOD == 1) {
+#pragma unroll
+    for (int f = 0; f < 4; ++f) {
+      double lim[N1], out[N1];
+      const int ph = (phys == 3 && f == 1) ? 5 : phys;
+      limit_slice<P>(c, ph, v[0][f], v[1][f], v[2][f], lim);
+      to_lag<N1>(c, lim, out);
+#pragma unroll
+      for (int i = 0; i < N1; ++i) Uout[(size_t)(f * N1 + i) * ld + e] = out[i];
+    }
+    return;
+  }
+  double pr[3][N1];
+#pragma unroll
+  for (int s = 0; s < 3; ++s) {
+    if (s != 1 && phys != 0) continue;
+#pragma unroll
+    for (int i = 0; i < N1; ++i) {
+      const double rho = v[s][0][i], ru = v[s][1][i], E = v[s][2][i];
+      const double gamma = 1.0 + 1.0 / v[s][3][i];
+      pr[s][i] = (gamma - 1) * (E - 0.5 * ru * ru / rho);
+    }
+  }
+  double lr[N1], lu[N1], la[N1], lp[N1];
+  limit_slice<P>(c, phys, v[0][0], v[1][0], v[2][0], lr);
+  limit_slice<P>(c, phys, v[0][1], v[1][1], v[2][1], lu);
+  limit_slice<P>(c, phys, v[0][3], v[1][3], v[2][3], la);
+  limit_slice<P>(c, phys, pr[0], pr[1], pr[2], lp);
+  double r_[N1], u_[N1], a_[N1], K[N1], Km[N1], Em[N1], El[N1], E_[N1];
+  to_lag<N1>(c, lr, r_);
+  to_lag<N1>(c, lu, u_);
+  to_lag<N1>(c, la, a_);
+#pragma unroll
+  for (int i = 0; i < N1; ++i) K[i] = 0.5 * u_[i] * u_[i] / r_[i];  // kinetic_energy1D
+  to_mono<N1>(c, K, Km);
+  to_mono<N1>(c, v[1][2], Em);
+  reconstruct_energy<P>(c, lp, la, Km, Em, El);
+  to_lag<N1>(c, El, E_);
+  const double* outs[4] = {r_, u_, E_, a_};
+#pragma unroll
+  for (int f = 0; f < 4; ++f)
+#pragma unroll
+    for (int i = 0; i < N1; ++i) Uout[(size_t)(f * N1 + i) * ld + e] = outs[f][i];
+}
+
+// ------------------------------------------------------------------------------------------
+// CFL step: max over nodes of the wave speed, then dt = CFL_scaled / max (on the device)
+// ------------------------------------------------------------------------------------------
+template <int DIM, int NS>
+__global__ void __launch_bounds__(256) wavespeed_kernel(const double* __restrict__ U, int n_elem, int ld,
+                                                        DevScalars* __restrict__ scal) {
+  if (scal->flags) return;
+  double m = 0.0;
+  bool bad = false;
+  for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < n_elem; e += gridDim.x * blockDim.x) {
+#pragma unroll
+    for (int t = 0; t < NS; ++t) {
+      double w;
+      if (DIM == 1)
+        w = phys::wave_speed1d(__ldg(U + (size_t)(0 * NS + t) * ld + e), __ldg(U + (size_t)(1 * NS + t) * ld + e),
+                               __ldg(U + (size_t)(2 * NS + t) * ld + e), __ldg(U + (size_t)(3 * NS + t) * ld + e));
+      else
+        w = phys::wave_speed2d(__ldg(U + (size_t)(0 * NS + t) * ld + e), __ldg(U + (size_t)(1 * NS + t) * ld + e),
+                               __ldg(U + (size_t)(2 * NS + t) * ld + e), __ldg(U + (size_t)(3 * NS + t) * ld + e),
+                               __ldg(U + (size_t)(4 * NS + t) * ld + e));
+      if (!(w == w)) bad = true;
+      else m = fmax(m, fabs(w));
+    }
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
+  __shared__ double wm[8];
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  if (lane == 0) wm[w] = m;
+  if (__any_sync(0xffffffffu, bad) && lane == 0) atomicOr(&scal->flags, (unsigned)FLAG_NONFINITE);
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double mm = 0.0;
+    for (int k = 0; k < (int)(blockDim.x >> 5); ++k) mm = fmax(mm, wm[k]);
+    atomicMax(&scal->umax, (unsigned long long)__double_as_longlong(mm));
+  }
+}
+
+__global__ void finish_dt_kernel(DevScalars* scal, double cfl_scaled) {
+  if (scal->flags) return;
+  double dt;
+  if (scal->dt_fixed > 0) dt = scal->dt_fixed;
+  else {
+    const double umax = __longlong_as_double((long long)scal->umax);
+    dt = cfl_scaled / umax;
+    if (!(dt == dt)) atomicOr(&scal->flags, (unsigned)FLAG_NONFINITE);
+    else if (dt < 1e-14) atomicOr(&scal->flags, (unsigned)FLAG_DT_SMALL);
+  }
+  scal->umax = 0ull;
+  if (scal->flags) return;
+  scal->dt = dt;
+  scal->time += dt;
+}
+
+// ------------------------------------------------------------------------------------------
+// Layout conversion (API boundary only), RK4 helpers
+// ------------------------------------------------------------------------------------------
+__global__ void ref_to_internal_kernel(const double* __restrict__ Uref, double* __restrict__ Uint,
+                                       const int* __restrict__ perm, int n_elem, int nf, int ns, int ld) {
+  const size_t n = (size_t)n_elem * nf * ns;
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+    const int t = (int)(i % ns);
+    const size_t r = i / ns;
+    const int f = (int)(r % nf);
+    const int e = (int)(r / nf);
+    Uint[(size_t)(f * ns + t) * ld + e] = Uref[((size_t)e * nf + f) * ns + perm[t]];
+  }
+}
+__global__ void internal_to_ref_kernel(const double* __restrict__ Uint, double* __restrict__ Uref,
+                                       const int* __restrict__ perm, int n_elem, int nf, int ns, int ld) {
+  const size_t n = (size_t)n_elem * nf * ns;
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+    const int t = (int)(i % ns);
+    const size_t r = i / ns;
+    const int f = (int)(r % nf);
+    const int e = (int)(r / nf);
+    Uref[((size_t)e * nf + f) * ns + perm[t]] = Uint[(size_t)(f * ns + t) * ld + e];
+  }
+}
+// y = x + beta*d over n values (Ustar = Us + beta DU, rk.cc:167-168)
+__global__ void axpy_kernel(const double* __restrict__ x, const double* __restrict__ d, double beta,
+                            double* __restrict__ y, size_t n, const DevScalars* __restrict__ scal) {
+  if (scal && scal->flags) return;
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
+    y[i] = x[i] + beta * d[i];
+}
+
+}  // namespace dgb

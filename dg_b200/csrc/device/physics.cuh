@@ -1,0 +1,183 @@
+// Gamma-model (GAMNCON) multifluid physics at one point, FP64.
+//
+// State per point: 1D (rho, rho u, E, alpha), 2D (rho, rho u, rho v, E, alpha) with
+// alpha = 1/(gamma-1) carried non-conservatively (no flux; volume source -u.grad(alpha);
+// interface term ncterm).  Formulas restate the reference's:
+//   volume flux/source   evaluate_sf   code/src/physics/physics.cu:96-143 (1D), 248-301 (2D)
+//   Rusanov              oned_multifluid_rusanov  code/src/face_fluxes/oned_multifluid_fluxes.h:30-94
+//                        twod_multifluid_rusanov  code/src/face_fluxes/twod_multifluid_fluxes.h:30-97
+//   HLL (1D)             oned_multifluid_hll      oned_multifluid_fluxes.h:117-226
+//   Roe                  oned_multifluid_roe      oned_multifluid_fluxes.h:237-382
+//                        twod_multifluid_roe      twod_multifluid_fluxes.h:151-342
+//   wave speed           oned/twod_multifluid_upa code/src/physics/upa.h:61-85
+// The operation order is kept where it is natural so the FP64 results agree with the
+// reference CPU build to rounding (the GPU contracts a*b+c into FMA).
+#pragma once
+
+namespace dgb {
+namespace phys {
+
+enum { FLUX_RUS = 0, FLUX_HLL = 1, FLUX_ROE = 2 };
+
+// ---------------------------------------------------------------- 1D -------------------------
+// Interface flux F[4] and ncterm for the alpha equation (F[3] holds the alpha dissipation).
+// Caller forms q_L = -F + nc (element on side L) and q_R = F + nc (physics.cu:800-804).
+template <int FLUX>
+__device__ __forceinline__ void riemann1d(double rhoL, double rhoR, double vxL, double vxR, double EtL, double EtR,
+                                          double alphaL, double alphaR, double nx, double F[4], double& nc) {
+  const double gammaL = 1.0 + 1.0 / alphaL;
+  const double gammaR = 1.0 + 1.0 / alphaR;
+  const double pL = (gammaL - 1) * (EtL - 0.5 * rhoL * vxL * vxL);
+  const double pR = (gammaR - 1) * (EtR - 0.5 * rhoR * vxR * vxR);
+  const double aL = sqrt((gammaL * pL) / rhoL);
+  const double aR = sqrt((gammaR * pR) / rhoR);
+  if (FLUX == FLUX_RUS) {
+    const double maxvap = fmax(fabs(vxL) + aL, fabs(vxR) + aR);
+    F[0] = 0.5 * ((rhoL * vxL + rhoR * vxR) * nx - maxvap * (rhoR - rhoL));
+    F[1] = 0.5 * ((rhoL * vxL * vxL + pL + rhoR * vxR * vxR + pR) * nx - maxvap * (rhoR * vxR - rhoL * vxL));
+    F[2] = 0.5 * (((EtL + pL) * vxL + (EtR + pR) * vxR) * nx - maxvap * (EtR - EtL));
+    F[3] = 0.5 * (-maxvap * (alphaR - alphaL));
+    nc = -0.5 * 0.5 * (vxL + vxR) * (alphaR - alphaL) * nx;
+  } else if (FLUX == FLUX_HLL) {
+    // Davis wave-speed estimates (Toro 10.48); fhll of basic_fluxes.h:22-27.  The momentum
+    // component passes the velocities as its state jump, and no branch is taken when SL == 0,
+    // both exactly as oned_multifluid_hll does.
+    const double SL = fmin(vxL * nx - aL, vxR * nx - aR);
+    const double SR = fmax(vxL * nx + aL, vxR * nx + aR);
+    const double vnc = -0.5 * (vxL * nx + vxR * nx) * (alphaL - alphaR);
+    const double vncabs = -0.5 * fabs(vxL * nx + vxR * nx) * (alphaL - alphaR);
+    auto fhll = [](double UL, double SLv, double FL, double UR, double SRv, double FR) {
+      return (SRv * FL - SLv * FR + SLv * SRv * (UR - UL)) / fabs(SRv - SLv);
+    };
+    F[0] = F[1] = F[2] = F[3] = 0.0;
+    if (SL > 0) {
+      F[0] = rhoL * vxL * nx;
+      F[1] = (rhoL * vxL * vxL + pL) * nx;
+      F[2] = (EtL + pL) * vxL * nx;
+      F[3] = -0.5 * vncabs;
+    } else if ((SL < 0) && (SR > 0)) {
+      F[0] = fhll(rhoL, SL, rhoL * vxL * nx, rhoR, SR, rhoR * vxR * nx);
+      F[1] = fhll(vxL, SL, (rhoL * vxL * vxL + pL) * nx, vxR, SR, (rhoR * vxR * vxR + pR) * nx);
+      F[2] = fhll(EtL, SL, (EtL + pL) * vxL * nx, EtR, SR, (EtR + pR) * vxR * nx);
+      F[3] = fhll(alphaL, SL, 0, alphaR, SR, 0) - 0.5 * fabs(SR + SL) / fabs(SR - SL) * vncabs;
+    } else if (SR < 0) {
+      F[0] = rhoR * vxR * nx;
+      F[1] = (rhoR * vxR * vxR + pR) * nx;
+      F[2] = (EtR + pR) * vxR * nx;
+      F[3] = 0.5 * vncabs;
+    }
+    nc = -0.5 * vnc;
+  } else {
+    const double RT = sqrt(rhoR / rhoL);
+    const double rho = RT * rhoL;
+    const double v = (vxL + RT * vxR) / (1 + RT);
+    const double HL = (EtL + pL) / rhoL;
+    const double HR = (EtR + pR) / rhoR;
+    const double H = (HL + RT * HR) / (1 + RT);
+    const double alpha = (alphaL + RT * alphaR) / (1 + RT);
+    const double gamma = 1 + 1.0 / alpha;
+    const double a = sqrt((gamma - 1) * (H - 0.5 * v * v));
+    const double iL = pL * alphaL;
+    const double iR = pR * alphaR;
+    const double i = (sqrt(rhoL) * iL + sqrt(rhoR) * iR) / (sqrt(rhoL) + sqrt(rhoR));
+    const double Dp = (gamma - 1) * (gamma - 1) * (alpha * (iR - iL) - i * (alphaR - alphaL));
+    const double p = (gamma - 1) * i;
+    const double dV0 = (Dp - rho * a * (vxR - vxL)) / (2 * a * a);
+    const double dV1 = (rhoR - rhoL) - Dp / (a * a);
+    const double dV2 = (Dp + rho * a * (vxR - vxL)) / (2 * a * a);
+    const double dV3 = alphaR - alphaL;
+    const double ws0 = fabs(v - a), ws1 = fabs(v), ws2 = fabs(v + a), ws3 = fabs(v);
+    // right eigenvectors R0=(1, v-a, H-va, 0), R1=(1, v, v^2/2, 0), R2=(1, v+a, H+va, 0), R3=(0,0,p,1)
+    F[0] = 0.5 * (rhoL * vxL + rhoR * vxR) * nx - 0.5 * (ws0 * dV0 * 1 + ws1 * dV1 * 1 + ws2 * dV2 * 1 + ws3 * dV3 * 0);
+    F[1] = 0.5 * (rhoL * vxL * vxL + pL + rhoR * vxR * vxR + pR) * nx -
+           0.5 * (ws0 * dV0 * (v - a) + ws1 * dV1 * v + ws2 * dV2 * (v + a) + ws3 * dV3 * 0);
+    F[2] = 0.5 * ((EtL + pL) * vxL + (EtR + pR) * vxR) * nx -
+           0.5 * (ws0 * dV0 * (H - v * a) + ws1 * dV1 * (0.5 * v * v) + ws2 * dV2 * (H + v * a) + ws3 * dV3 * p);
+    F[3] = 0 + -0.5 * (ws0 * dV0 * 0 + ws1 * dV1 * 0 + ws2 * dV2 * 0 + ws3 * dV3 * 1);
+    nc = -0.5 * v * (alphaR - alphaL) * nx;
+  }
+}
+
+// ---------------------------------------------------------------- 2D -------------------------
+template <int FLUX>
+__device__ __forceinline__ void riemann2d(double rhoL, double rhoR, double vxL, double vxR, double vyL, double vyR,
+                                          double EtL, double EtR, double alphaL, double alphaR, double nx, double ny,
+                                          double F[5], double& nc) {
+  const double vnL = vxL * nx + vyL * ny;
+  const double vnR = vxR * nx + vyR * ny;
+  const double gammaL = 1.0 + 1.0 / alphaL;
+  const double gammaR = 1.0 + 1.0 / alphaR;
+  const double pL = (gammaL - 1) * (EtL - 0.5 * rhoL * (vxL * vxL + vyL * vyL));
+  const double pR = (gammaR - 1) * (EtR - 0.5 * rhoR * (vxR * vxR + vyR * vyR));
+  const double aL = sqrt((gammaL * pL) / rhoL);
+  const double aR = sqrt((gammaR * pR) / rhoR);
+  const double HL = (EtL + pL) / rhoL;
+  const double HR = (EtR + pR) / rhoR;
+  if (FLUX == FLUX_ROE) {
+    const double tx = -ny, ty = nx;
+    const double vtL = vxL * tx + vyL * ty;
+    const double vtR = vxR * tx + vyR * ty;
+    const double iL = pL * alphaL;
+    const double iR = pR * alphaR;
+    const double RT = sqrt(rhoR / rhoL);
+    const double rho = RT * rhoL;
+    const double vx = (vxL + RT * vxR) / (1 + RT);
+    const double vy = (vyL + RT * vyR) / (1 + RT);
+    const double vn = vx * nx + vy * ny;
+    const double vt = vx * tx + vy * ty;
+    const double H = (HL + RT * HR) / (1 + RT);
+    const double alpha = (alphaL + RT * alphaR) / (1 + RT);
+    const double gamma = 1 + 1.0 / alpha;
+    const double a = sqrt((gamma - 1) * (H - 0.5 * (vx * vx + vy * vy)));
+    const double i = (iL + RT * iR) / (1 + RT);
+    const double p = (gamma - 1) * i;
+    const double drho = rhoR - rhoL;
+    const double dp = (gamma - 1) * (gamma - 1) * (alpha * (iR - iL) - i * (alphaR - alphaL));
+    const double dvn = vnR - vnL;
+    const double dvt = vtR - vtL;
+    const double dV0 = (dp - rho * a * dvn) / (2 * a * a);
+    const double dV1 = rho * dvt / a;
+    const double dV2 = drho - dp / (a * a);
+    const double dV3 = (dp + rho * a * dvn) / (2 * a * a);
+    const double dV4 = alphaR - alphaL;
+    const double ws0 = fabs(vn - a), ws1 = fabs(vn), ws2 = fabs(vn), ws3 = fabs(vn + a), ws4 = fabs(vn);
+    F[0] = 0.5 * (rhoL * vnL + rhoR * vnR) - 0.5 * (ws0 * dV0 * 1 + ws1 * dV1 * 0 + ws2 * dV2 * 1 + ws3 * dV3 * 1 + ws4 * dV4 * 0);
+    F[1] = 0.5 * ((rhoL * vnL * vxL + pL * nx) + (rhoR * vnR * vxR + pR * nx)) -
+           0.5 * (ws0 * dV0 * (vx - a * nx) + ws1 * dV1 * (a * tx) + ws2 * dV2 * vx + ws3 * dV3 * (vx + a * nx) + ws4 * dV4 * 0);
+    F[2] = 0.5 * ((rhoL * vnL * vyL + pL * ny) + (rhoR * vnR * vyR + pR * ny)) -
+           0.5 * (ws0 * dV0 * (vy - a * ny) + ws1 * dV1 * (a * ty) + ws2 * dV2 * vy + ws3 * dV3 * (vy + a * ny) + ws4 * dV4 * 0);
+    F[3] = 0.5 * (rhoL * vnL * HL + rhoR * vnR * HR) -
+           0.5 * (ws0 * dV0 * (H - vn * a) + ws1 * dV1 * (vt * a) + ws2 * dV2 * (0.5 * (vx * vx + vy * vy)) +
+                  ws3 * dV3 * (H + vn * a) + ws4 * dV4 * p);
+    F[4] = 0 + -0.5 * (ws0 * dV0 * 0 + ws1 * dV1 * 0 + ws2 * dV2 * 0 + ws3 * dV3 * 0 + ws4 * dV4 * 1);
+    nc = -0.5 * vn * (alphaR - alphaL);
+  } else {
+    // Rusanov (2D HLL is a stub in the reference, twod_multifluid_fluxes.h:119-141; the host
+    // rejects it before any launch)
+    const double maxvap = fmax(fabs(vnL) + aL, fabs(vnR) + aR);
+    F[0] = 0.5 * (rhoL * vnL + rhoR * vnR - maxvap * (rhoR - rhoL));
+    F[1] = 0.5 * ((rhoL * vnL * vxL + pL * nx) + (rhoR * vnR * vxR + pR * nx) - maxvap * (rhoR * vxR - rhoL * vxL));
+    F[2] = 0.5 * ((rhoL * vnL * vyL + pL * ny) + (rhoR * vnR * vyR + pR * ny) - maxvap * (rhoR * vyR - rhoL * vyL));
+    F[3] = 0.5 * (rhoL * vnL * HL + rhoR * vnR * HR - maxvap * (EtR - EtL));
+    F[4] = 0.5 * (-maxvap * (alphaR - alphaL));
+    nc = -0.5 * 0.5 * (vnL + vnR) * (alphaR - alphaL);
+  }
+}
+
+// max(|u|+a, |v|+a) at a node (upa.h:61-85)
+__device__ __forceinline__ double wave_speed1d(double rho, double rhou, double E, double alpha) {
+  const double u = rhou / rho;
+  const double gamma = 1.0 + 1.0 / alpha;
+  const double p = (gamma - 1) * (E - 0.5 * rho * u * u);
+  return fabs(u) + sqrt(gamma * p / rho);
+}
+__device__ __forceinline__ double wave_speed2d(double rho, double rhou, double rhov, double E, double alpha) {
+  const double u = rhou / rho, v = rhov / rho;
+  const double gamma = 1.0 + 1.0 / alpha;
+  const double p = (gamma - 1) * (E - 0.5 * rho * (u * u + v * v));
+  const double a = sqrt(gamma * p / rho);
+  return fmax(fabs(u) + a, fabs(v) + a);
+}
+
+}  // namespace phys
+}  // namespace dgb

@@ -1,0 +1,622 @@
+// Device context and the device half of the C ABI (include/dgb.h).
+//
+// One context = one problem on one GPU: uploaded basis constants and neighbour table, the
+// resident state and the stage buffers of the chosen integrator, and one CUDA stream on which
+// every kernel of the context runs.  Steps of dgb_advance are captured once into a CUDA graph
+// per (scheme, step mode) and replayed.
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/dgb.h"
+#include "device/kernels.cuh"
+#include "host/host.h"
+
+namespace dgb {
+int set_error(int code, const std::string& msg);
+}
+const dgb::Problem& dgb_problem_ref(const dgb_problem* p);
+
+using namespace dgb;
+
+#define DGB_CUDA(call)                                                                          \
+  do {                                                                                          \
+    cudaError_t err_ = (call);                                                                  \
+    if (err_ != cudaSuccess)                                                                    \
+      return set_error(DGB_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(err_));     \
+  } while (0)
+
+namespace {
+
+constexpr int RES2D_TE = 16;
+constexpr int RES2D_NT = 256;
+
+enum { KC_RESIDUAL = 0, KC_LIMITER = 1, KC_DT = 2, KC_OTHER = 3, KC_N = 4 };
+
+double fact(int n) { double f = 1; for (int i = 2; i <= n; ++i) f *= i; return f; }
+
+Consts make_consts(const Problem& P, int ld) {
+  Consts c;
+  std::memset(&c, 0, sizeof(c));
+  c.p = P.p;
+  c.n1 = P.p + 1;
+  c.dim = P.D;
+  c.ng1 = P.D == 1 ? P.p + 1 : (P.p == 1 ? 2 : P.p + 2);
+  c.ns = P.N_s;
+  c.ng = P.N_G;
+  c.nf = P.N_F;
+  c.ld = ld;
+  c.n_elem = P.N_E;
+  const int n1 = c.n1;
+  // ascending 1D nodes (tensor order)
+  std::vector<double> xs(n1);
+  for (int i = 0; i < n1; ++i) xs[i] = -1.0 + 2.0 * i / P.p;
+  std::vector<double> xq, wq, xf, wf;
+  gauss_legendre(c.ng1, xq, wq);
+  gauss_legendre(n1, xf, wf);
+  for (int g = 0; g < c.ng1; ++g) {
+    c.wq[g] = wq[g];
+    for (int i = 0; i < n1; ++i) { c.Bq[g][i] = lagrange1d(xs, i, xq[g]); c.Dq[g][i] = dlagrange1d(xs, i, xq[g]); }
+  }
+  for (int g = 0; g < n1; ++g) {
+    c.wf[g] = wf[g];
+    for (int i = 0; i < n1; ++i) c.Bf[g][i] = lagrange1d(xs, i, xf[g]);
+  }
+  // element inverse mass matrix (element 0; uniform mesh) permuted to tensor order
+  for (int t = 0; t < P.N_s; ++t)
+    for (int u = 0; u < P.N_s; ++u) c.Minv[t][u] = P.Minv[(size_t)P.tensor_perm[u] * P.N_s + P.tensor_perm[t]];
+  // Lagrange -> scaled Taylor monomials: T = V^-1 phi on the (p+1) Gauss points
+  // (monovandermonde1d and Lag2Mono of main.cc:558-567, 1146-1157)
+  std::vector<double> V((size_t)n1 * n1), phi1((size_t)n1 * n1);
+  for (int g = 0; g < n1; ++g)
+    for (int j = 0; j < n1; ++j) {
+      V[g + (size_t)j * n1] = std::pow(xf[g], j) / fact(j);
+      phi1[g + (size_t)j * n1] = lagrange1d(xs, j, xf[g]);
+    }
+  invert(V, n1);
+  std::vector<double> T((size_t)n1 * n1, 0.0);
+  for (int m = 0; m < n1; ++m)
+    for (int i = 0; i < n1; ++i) {
+      double s = 0;
+      for (int g = 0; g < n1; ++g) s += V[m + (size_t)g * n1] * phi1[g + (size_t)i * n1];
+      T[m + (size_t)i * n1] = s;
+    }
+  std::vector<double> Ti = T;
+  invert(Ti, n1);
+  for (int m = 0; m < n1; ++m)
+    for (int i = 0; i < n1; ++i) { c.T[m][i] = T[m + (size_t)i * n1]; c.Tinv[i][m] = Ti[i + (size_t)m * n1]; }
+  // limiter integrals (integrate_monomial_derivative(_bounds), limiting_kernels.cu:1748-1775)
+  for (int k = 0; k < MAXN; ++k)
+    for (int n = 0; n < MAXN; ++n) {
+      const int num = n - k + 1;
+      if (num < 1) continue;
+      c.imd[k][n] = (num % 2) ? 2.0 / fact(num) : 0.0;
+      c.imdL[k][n] = (std::pow(-1.0, num) - std::pow(-3.0, num)) / fact(num);
+      c.imdR[k][n] = (std::pow(3.0, num) - std::pow(1.0, num)) / fact(num);
+    }
+  for (int k = 0; k < 8; ++k) c.ifact[k] = 1.0 / fact(k);
+  const int D = P.D, NG = P.N_G;
+  c.J = P.J[0];
+  c.ixx = P.invJac[((size_t)0 * NG + 0) * D * D + 0];
+  c.iyy = D == 2 ? P.invJac[((size_t)0 * NG + 0) * D * D + 3] : 0.0;
+  c.JFx = D == 2 ? 0.5 * P.hy : 1.0;
+  c.JFy = D == 2 ? 0.5 * P.hx : 1.0;
+  c.cfl_scaled = P.cfl_scaled;
+  return c;
+}
+
+}  // namespace
+
+struct dgb_ctx {
+  int device = 0;
+  cudaStream_t st = nullptr;
+  int D = 1, p = 1, nf = 4, ns = 2, ne = 0, ld = 0, flux = 2, limiter = 0;
+  size_t nstate = 0;
+  Consts cs;
+  double *A = nullptr, *B = nullptr, *C = nullptr, *DU = nullptr, *X = nullptr, *ref = nullptr;
+  int *nbr = nullptr, *perm = nullptr;
+  DevScalars* scal = nullptr;
+  DevScalars* h_scal = nullptr;  // pinned
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  double last_ms = 0.0;
+  long long last_launches = 0;
+  long long launches_per_step = 0;
+  cudaGraphExec_t graphs[2][2] = {{nullptr, nullptr}, {nullptr, nullptr}};
+  long long graph_launches[2][2] = {{0, 0}, {0, 0}};
+  // profiling (per kernel class)
+  bool prof = false;
+  std::vector<std::pair<int, std::pair<cudaEvent_t, cudaEvent_t>>> pev;
+  std::vector<cudaEvent_t> ev_pool;
+  size_t ev_used = 0;
+  double kc_ms[KC_N] = {0, 0, 0, 0};
+  long long kc_n[KC_N] = {0, 0, 0, 0};
+  long long counter = 0;  // launches issued since the last reset
+};
+
+namespace {
+
+cudaEvent_t pool_event(dgb_ctx* c) {
+  if (c->ev_used == c->ev_pool.size()) {
+    cudaEvent_t e;
+    cudaEventCreate(&e);
+    c->ev_pool.push_back(e);
+  }
+  return c->ev_pool[c->ev_used++];
+}
+
+struct ProfScope {
+  dgb_ctx* c;
+  int kc;
+  cudaEvent_t a = nullptr, b = nullptr;
+  ProfScope(dgb_ctx* ctx, int k) : c(ctx), kc(k) {
+    c->counter++;
+    if (c->prof) { a = pool_event(c); b = pool_event(c); cudaEventRecord(a, c->st); }
+  }
+  ~ProfScope() {
+    if (c->prof) { cudaEventRecord(b, c->st); c->pev.push_back({kc, {a, b}}); }
+  }
+};
+
+template <int P, int FLUX, int MODE>
+void launch_res2d(dgb_ctx* c, const StageArgs& a) {
+  constexpr size_t smem = residual2d_smem_doubles<P, RES2D_TE>() * sizeof(double);
+  auto k = residual2d_kernel<P, FLUX, MODE, RES2D_TE, RES2D_NT>;
+  static bool attr = false;
+  if (!attr) { cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem); attr = true; }
+  const int grid = (c->ne + RES2D_TE - 1) / RES2D_TE;
+  ProfScope ps(c, KC_RESIDUAL);
+  k<<<grid, RES2D_NT, smem, c->st>>>(c->cs, a);
+}
+
+template <int P, int FLUX, int MODE>
+void launch_res1d(dgb_ctx* c, const StageArgs& a) {
+  const int grid = (c->ne + 127) / 128;
+  ProfScope ps(c, KC_RESIDUAL);
+  residual1d_kernel<P, FLUX, MODE><<<grid, 128, 0, c->st>>>(c->cs, a);
+}
+
+template <int MODE>
+int residual_dispatch(dgb_ctx* c, const StageArgs& a) {
+#define R2(P, F) case P * 10 + F: launch_res2d<P, F, MODE>(c, a); return 0;
+#define R1(P, F) case P * 10 + F: launch_res1d<P, F, MODE>(c, a); return 0;
+  const int key = c->p * 10 + c->flux;
+  if (c->D == 2) {
+    switch (key) {
+      R2(1, 0) R2(1, 2) R2(2, 0) R2(2, 2) R2(3, 0) R2(3, 2)
+      default: break;
+    }
+  } else {
+    switch (key) {
+      R1(1, 0) R1(1, 1) R1(1, 2) R1(2, 0) R1(2, 1) R1(2, 2) R1(3, 0) R1(3, 1) R1(3, 2)
+      default: break;
+    }
+  }
+#undef R2
+#undef R1
+  return set_error(DGB_ERR_UNSUPPORTED, "no residual kernel for this (dim, p, flux)");
+}
+
+template <int P, int METHOD>
+void launch_lim2d(dgb_ctx* c, double* U) {
+  dim3 grid((c->ne + 127) / 128, P + 1);
+  ProfScope ps(c, KC_LIMITER);
+  lim2d_xpass_kernel<P, METHOD><<<grid, 128, 0, c->st>>>(c->cs, U, c->nbr, c->X, c->scal);
+  lim2d_ypass_kernel<P, METHOD><<<grid, 128, 0, c->st>>>(c->cs, c->X, c->nbr, U, c->scal);
+  c->counter++;
+}
+
+template <int P, int METHOD>
+void launch_lim1d(dgb_ctx* c, double* U) {
+  const int grid = (c->ne + 127) / 128;
+  {
+    ProfScope ps(c, KC_LIMITER);
+    lim1d_kernel<P, METHOD><<<grid, 128, 0, c->st>>>(c->cs, U, c->nbr, c->X, c->scal);
+  }
+  cudaMemcpyAsync(U, c->X, c->nstate * sizeof(double), cudaMemcpyDeviceToDevice, c->st);
+}
+
+// in-place limiting of a state buffer with the context's limiter
+int limit_dispatch(dgb_ctx* c, double* U) {
+  if (c->limiter == 0) return 0;
+  const int key = c->p * 10 + c->limiter;
+#define L2(P, M) case P * 10 + M: launch_lim2d<P, M>(c, U); return 0;
+#define L1(P, M) case P * 10 + M: launch_lim1d<P, M>(c, U); return 0;
+  if (c->D == 2) {
+    switch (key) { L2(1, 1) L2(1, 2) L2(2, 1) L2(2, 2) L2(3, 1) L2(3, 2) default: break; }
+  } else {
+    switch (key) { L1(1, 1) L1(1, 2) L1(2, 1) L1(2, 2) L1(3, 1) L1(3, 2) default: break; }
+  }
+#undef L2
+#undef L1
+  return set_error(DGB_ERR_UNSUPPORTED, "limiter not available on the device path");
+}
+
+void launch_dt(dgb_ctx* c, const double* U, bool cfl) {
+  ProfScope ps(c, KC_DT);
+  if (cfl) {
+    const int grid = std::max(1, std::min(4 * 148, (c->ne + 255) / 256));
+    switch (c->D * 100 + c->ns) {
+      case 102: wavespeed_kernel<1, 2><<<grid, 256, 0, c->st>>>(U, c->ne, c->ld, c->scal); break;
+      case 103: wavespeed_kernel<1, 3><<<grid, 256, 0, c->st>>>(U, c->ne, c->ld, c->scal); break;
+      case 104: wavespeed_kernel<1, 4><<<grid, 256, 0, c->st>>>(U, c->ne, c->ld, c->scal); break;
+      case 204: wavespeed_kernel<2, 4><<<grid, 256, 0, c->st>>>(U, c->ne, c->ld, c->scal); break;
+      case 209: wavespeed_kernel<2, 9><<<grid, 256, 0, c->st>>>(U, c->ne, c->ld, c->scal); break;
+      case 216: wavespeed_kernel<2, 16><<<grid, 256, 0, c->st>>>(U, c->ne, c->ld, c->scal); break;
+      default: break;
+    }
+    c->counter++;
+  }
+  finish_dt_kernel<<<1, 1, 0, c->st>>>(c->scal, c->cs.cfl_scaled);
+}
+
+StageArgs stage_args(dgb_ctx* c) {
+  StageArgs a;
+  std::memset(&a, 0, sizeof(a));
+  a.nbr = c->nbr;
+  a.scal = c->scal;
+  return a;
+}
+
+// One SSP-RK3 step on c->A (Shu-Osher form); limiter after every stage.
+int step_ssprk3(dgb_ctx* c, bool cfl) {
+  launch_dt(c, c->A, cfl);
+  StageArgs a = stage_args(c);
+  const double coef[3][2] = {{0.0, 1.0}, {0.75, 0.25}, {1.0 / 3.0, 2.0 / 3.0}};
+  double* in[3] = {c->A, c->B, c->C};
+  double* out[3] = {c->B, c->C, c->A};
+  for (int s = 0; s < 3; ++s) {
+    a.U = in[s];
+    a.Ubase = c->A;
+    a.out = out[s];
+    a.a = coef[s][0];
+    a.b = coef[s][1];
+    if (int rc = residual_dispatch<MODE_SSP>(c, a)) return rc;
+    if (int rc = limit_dispatch(c, out[s])) return rc;
+  }
+  return 0;
+}
+
+// One classical RK4 step in the reference's form (rk.cc:155-209): A = U, B = Us, C = Ustar.
+int step_rk4(dgb_ctx* c, bool cfl) {
+  launch_dt(c, c->A, cfl);
+  const double beta[4] = {0.0, 0.5, 0.5, 1.0};
+  const double gam[4] = {1.0 / 6.0, 2.0 / 6.0, 2.0 / 6.0, 1.0 / 6.0};
+  cudaMemcpyAsync(c->B, c->A, c->nstate * sizeof(double), cudaMemcpyDeviceToDevice, c->st);
+  StageArgs a = stage_args(c);
+  for (int k = 0; k < 4; ++k) {
+    const double* in = c->B;
+    if (k > 0) {
+      const int grid = (int)std::min<size_t>((c->nstate + 255) / 256, 148 * 16);
+      {
+        ProfScope ps(c, KC_OTHER);
+        axpy_kernel<<<grid, 256, 0, c->st>>>(c->B, c->DU, beta[k], c->C, c->nstate, c->scal);
+      }
+      if (int rc = limit_dispatch(c, c->C)) return rc;
+      in = c->C;
+    }
+    a.U = in;
+    a.out = c->DU;
+    a.Uacc = c->A;
+    a.b = gam[k];
+    if (int rc = residual_dispatch<MODE_RK4>(c, a)) return rc;
+  }
+  return limit_dispatch(c, c->A);
+}
+
+int to_internal(dgb_ctx* c, const double* Uref_dev, double* Uint) {
+  const int grid = (int)std::min<size_t>(((size_t)c->ne * c->nf * c->ns + 255) / 256, 148 * 32);
+  ref_to_internal_kernel<<<grid, 256, 0, c->st>>>(Uref_dev, Uint, c->perm, c->ne, c->nf, c->ns, c->ld);
+  DGB_CUDA(cudaGetLastError());
+  return 0;
+}
+int to_ref(dgb_ctx* c, const double* Uint, double* Uref_dev) {
+  const int grid = (int)std::min<size_t>(((size_t)c->ne * c->nf * c->ns + 255) / 256, 148 * 32);
+  internal_to_ref_kernel<<<grid, 256, 0, c->st>>>(Uint, Uref_dev, c->perm, c->ne, c->nf, c->ns, c->ld);
+  DGB_CUDA(cudaGetLastError());
+  return 0;
+}
+size_t ref_bytes(dgb_ctx* c) { return (size_t)c->ne * c->nf * c->ns * sizeof(double); }
+
+int upload(dgb_ctx* c, const double* host, double* Uint) {
+  DGB_CUDA(cudaMemcpyAsync(c->ref, host, ref_bytes(c), cudaMemcpyHostToDevice, c->st));
+  return to_internal(c, c->ref, Uint);
+}
+int download(dgb_ctx* c, const double* Uint, double* host) {
+  if (int rc = to_ref(c, Uint, c->ref)) return rc;
+  DGB_CUDA(cudaMemcpyAsync(host, c->ref, ref_bytes(c), cudaMemcpyDeviceToHost, c->st));
+  DGB_CUDA(cudaStreamSynchronize(c->st));
+  return 0;
+}
+
+int reset_scalars(dgb_ctx* c, double dt_fixed) {
+  std::memset(c->h_scal, 0, sizeof(DevScalars));
+  c->h_scal->dt_fixed = dt_fixed;
+  DGB_CUDA(cudaMemcpyAsync(c->scal, c->h_scal, sizeof(DevScalars), cudaMemcpyHostToDevice, c->st));
+  return 0;
+}
+int read_scalars(dgb_ctx* c) {
+  DGB_CUDA(cudaMemcpyAsync(c->h_scal, c->scal, sizeof(DevScalars), cudaMemcpyDeviceToHost, c->st));
+  DGB_CUDA(cudaStreamSynchronize(c->st));
+  return 0;
+}
+
+int prof_collect(dgb_ctx* c) {
+  if (!c->prof) return 0;
+  DGB_CUDA(cudaStreamSynchronize(c->st));
+  for (auto& pe : c->pev) {
+    float ms = 0;
+    cudaEventElapsedTime(&ms, pe.second.first, pe.second.second);
+    c->kc_ms[pe.first] += ms;
+    c->kc_n[pe.first] += 1;
+  }
+  c->pev.clear();
+  c->ev_used = 0;
+  return 0;
+}
+
+}  // namespace
+
+extern "C" int dgb_create(const dgb_problem* prob, int device, dgb_ctx** out) {
+  if (!prob || !out) return set_error(DGB_ERR_ARG, "null argument");
+  *out = nullptr;
+  const Problem& P = dgb_problem_ref(prob);
+  if (!P.gpu_ok) return set_error(DGB_ERR_UNSUPPORTED, P.gpu_reason);
+  if (P.D == 2 && P.flux == DGB_FLUX_HLL)
+    return set_error(DGB_ERR_UNSUPPORTED, "2D HLL is a stub in the reference (twod_multifluid_fluxes.h:119-141)");
+  if (P.limiter != 0 && P.limiter != 1 && P.limiter != 2)
+    return set_error(DGB_ERR_UNSUPPORTED, "device limiters: none, hrl, m2l");
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return set_error(DGB_ERR_NO_DEVICE, "no CUDA device");
+  if (device < 0 || device >= ndev) return set_error(DGB_ERR_ARG, "bad device index");
+  cudaDeviceProp prop;
+  DGB_CUDA(cudaGetDeviceProperties(&prop, device));
+  if (prop.major != 10) return set_error(DGB_ERR_NO_DEVICE, "kernels are built for sm_100a");
+  DGB_CUDA(cudaSetDevice(device));
+  auto* c = new dgb_ctx();
+  c->device = device;
+  c->D = P.D; c->p = P.p; c->nf = P.N_F; c->ns = P.N_s; c->ne = P.N_E;
+  c->ld = (P.N_E + 63) / 64 * 64;
+  c->flux = P.flux; c->limiter = P.limiter;
+  c->nstate = (size_t)c->nf * c->ns * c->ld;
+  c->cs = make_consts(P, c->ld);
+  auto fail = [&](cudaError_t e, const char* what) {
+    dgb_destroy(c);
+    return set_error(DGB_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
+  };
+  cudaError_t e;
+  if ((e = cudaStreamCreateWithFlags(&c->st, cudaStreamNonBlocking)) != cudaSuccess) return fail(e, "stream");
+  const size_t sb = c->nstate * sizeof(double);
+  double** bufs[4] = {&c->A, &c->B, &c->C, &c->DU};
+  for (auto b : bufs) {
+    if ((e = cudaMalloc(b, sb)) != cudaSuccess) return fail(e, "state allocation");
+    cudaMemset(*b, 0, sb);
+  }
+  const size_t xb = (size_t)6 * c->ns * c->ld * sizeof(double);
+  if ((e = cudaMalloc(&c->X, std::max(xb, sb))) != cudaSuccess) return fail(e, "limiter scratch");
+  cudaMemset(c->X, 0, std::max(xb, sb));
+  if ((e = cudaMalloc(&c->ref, (size_t)c->ne * c->nf * c->ns * sizeof(double))) != cudaSuccess) return fail(e, "staging");
+  if ((e = cudaMalloc(&c->nbr, (size_t)P.N_N * c->ld * sizeof(int))) != cudaSuccess) return fail(e, "neighbours");
+  std::vector<int> nb((size_t)P.N_N * c->ld, -4);
+  for (int k = 0; k < P.N_N; ++k)
+    for (int el = 0; el < P.N_E; ++el) nb[(size_t)k * c->ld + el] = P.nbr[(size_t)k * P.N_E + el];
+  cudaMemcpy(c->nbr, nb.data(), nb.size() * sizeof(int), cudaMemcpyHostToDevice);
+  if ((e = cudaMalloc(&c->perm, c->ns * sizeof(int))) != cudaSuccess) return fail(e, "perm");
+  cudaMemcpy(c->perm, P.tensor_perm.data(), c->ns * sizeof(int), cudaMemcpyHostToDevice);
+  if ((e = cudaMalloc(&c->scal, sizeof(DevScalars))) != cudaSuccess) return fail(e, "scalars");
+  cudaMemset(c->scal, 0, sizeof(DevScalars));
+  if ((e = cudaMallocHost(&c->h_scal, sizeof(DevScalars))) != cudaSuccess) return fail(e, "pinned scalars");
+  cudaEventCreate(&c->e0);
+  cudaEventCreate(&c->e1);
+  if ((e = cudaDeviceSynchronize()) != cudaSuccess) return fail(e, "create");
+  *out = c;
+  return DGB_OK;
+}
+
+extern "C" void dgb_destroy(dgb_ctx* c) {
+  if (!c) return;
+  cudaSetDevice(c->device);
+  if (c->st) cudaStreamSynchronize(c->st);
+  for (auto& row : c->graphs)
+    for (auto& g : row)
+      if (g) cudaGraphExecDestroy(g);
+  for (double* b : {c->A, c->B, c->C, c->DU, c->X, c->ref}) if (b) cudaFree(b);
+  if (c->nbr) cudaFree(c->nbr);
+  if (c->perm) cudaFree(c->perm);
+  if (c->scal) cudaFree(c->scal);
+  if (c->h_scal) cudaFreeHost(c->h_scal);
+  for (auto ev : c->ev_pool) cudaEventDestroy(ev);
+  if (c->e0) cudaEventDestroy(c->e0);
+  if (c->e1) cudaEventDestroy(c->e1);
+  if (c->st) cudaStreamDestroy(c->st);
+  delete c;
+}
+
+extern "C" int dgb_set_state(dgb_ctx* c, const double* U) {
+  if (!c || !U) return set_error(DGB_ERR_ARG, "null argument");
+  DGB_CUDA(cudaSetDevice(c->device));
+  if (int rc = upload(c, U, c->A)) return rc;
+  DGB_CUDA(cudaStreamSynchronize(c->st));
+  return DGB_OK;
+}
+
+extern "C" int dgb_get_state(dgb_ctx* c, double* U) {
+  if (!c || !U) return set_error(DGB_ERR_ARG, "null argument");
+  DGB_CUDA(cudaSetDevice(c->device));
+  return download(c, c->A, U);
+}
+
+extern "C" int dgb_set_state_device(dgb_ctx* c, const double* U_dev) {
+  if (!c || !U_dev) return set_error(DGB_ERR_ARG, "null argument");
+  DGB_CUDA(cudaSetDevice(c->device));
+  if (int rc = to_internal(c, U_dev, c->A)) return rc;
+  DGB_CUDA(cudaStreamSynchronize(c->st));
+  return DGB_OK;
+}
+
+extern "C" int dgb_get_state_device(dgb_ctx* c, double* U_dev) {
+  if (!c || !U_dev) return set_error(DGB_ERR_ARG, "null argument");
+  DGB_CUDA(cudaSetDevice(c->device));
+  if (int rc = to_ref(c, c->A, U_dev)) return rc;
+  DGB_CUDA(cudaStreamSynchronize(c->st));
+  return DGB_OK;
+}
+
+extern "C" int dgb_residual(dgb_ctx* c, const double* U, double* f) {
+  if (!c || !U || !f) return set_error(DGB_ERR_ARG, "null argument");
+  DGB_CUDA(cudaSetDevice(c->device));
+  if (int rc = upload(c, U, c->B)) return rc;
+  StageArgs a = stage_args(c);
+  a.scal = nullptr;
+  a.U = c->B;
+  a.out = c->C;
+  if (int rc = residual_dispatch<MODE_RESIDUAL>(c, a)) return rc;
+  DGB_CUDA(cudaGetLastError());
+  return download(c, c->C, f);
+}
+
+extern "C" int dgb_solve(dgb_ctx* c, double dt, const double* U, double* DU) {
+  if (!c || !U || !DU) return set_error(DGB_ERR_ARG, "null argument");
+  if (!(dt > 0)) return set_error(DGB_ERR_ARG, "dt must be > 0");
+  DGB_CUDA(cudaSetDevice(c->device));
+  if (int rc = upload(c, U, c->B)) return rc;
+  StageArgs a = stage_args(c);
+  a.scal = nullptr;
+  a.U = c->B;
+  a.out = c->C;
+  a.Uacc = nullptr;
+  a.dt_override = dt;
+  if (int rc = residual_dispatch<MODE_RK4>(c, a)) return rc;
+  DGB_CUDA(cudaGetLastError());
+  return download(c, c->C, DU);
+}
+
+extern "C" int dgb_limit(dgb_ctx* c, double* U) {
+  if (!c || !U) return set_error(DGB_ERR_ARG, "null argument");
+  DGB_CUDA(cudaSetDevice(c->device));
+  if (int rc = upload(c, U, c->B)) return rc;
+  if (int rc = reset_scalars(c, 0.0)) return rc;
+  if (int rc = limit_dispatch(c, c->B)) return rc;
+  DGB_CUDA(cudaGetLastError());
+  return download(c, c->B, U);
+}
+
+extern "C" int dgb_dt_from_cfl(dgb_ctx* c, const double* U, double* dt) {
+  if (!c || !U || !dt) return set_error(DGB_ERR_ARG, "null argument");
+  DGB_CUDA(cudaSetDevice(c->device));
+  if (int rc = upload(c, U, c->B)) return rc;
+  if (int rc = reset_scalars(c, 0.0)) return rc;
+  launch_dt(c, c->B, true);
+  DGB_CUDA(cudaGetLastError());
+  if (int rc = read_scalars(c)) return rc;
+  if (c->h_scal->flags & FLAG_NONFINITE) return set_error(DGB_ERR_NONFINITE, "time step is NaN");
+  if (c->h_scal->flags & FLAG_DT_SMALL) return set_error(DGB_ERR_DT_SMALL, "next time step is too small (< 1e-14)");
+  *dt = c->h_scal->dt;
+  return DGB_OK;
+}
+
+extern "C" int dgb_advance(dgb_ctx* c, int scheme, int nsteps, double dt, double* time) {
+  if (!c) return set_error(DGB_ERR_ARG, "null context");
+  if (scheme != DGB_SSPRK3 && scheme != DGB_RK4) return set_error(DGB_ERR_ARG, "scheme must be 3 or 4");
+  if (nsteps < 0) return set_error(DGB_ERR_ARG, "nsteps < 0");
+  if (!(dt > 0) && !(c->cs.cfl_scaled > 0)) return set_error(DGB_ERR_ARG, "no fixed dt and no positive CFL");
+  DGB_CUDA(cudaSetDevice(c->device));
+  const bool cfl = !(dt > 0);
+  if (int rc = reset_scalars(c, cfl ? 0.0 : dt)) return rc;
+  const int si = scheme == DGB_RK4 ? 1 : 0, mi = cfl ? 1 : 0;
+  c->counter = 0;
+  if (c->prof) {
+    // eager launches with per-kernel-class events
+    DGB_CUDA(cudaEventRecord(c->e0, c->st));
+    for (int s = 0; s < nsteps; ++s) {
+      int rc = scheme == DGB_RK4 ? step_rk4(c, cfl) : step_ssprk3(c, cfl);
+      if (rc) return rc;
+    }
+    DGB_CUDA(cudaEventRecord(c->e1, c->st));
+    DGB_CUDA(cudaGetLastError());
+    c->last_launches = c->counter;
+    if (int rc = prof_collect(c)) return rc;
+  } else {
+    if (!c->graphs[si][mi] && nsteps > 0) {
+      cudaGraph_t g;
+      DGB_CUDA(cudaStreamBeginCapture(c->st, cudaStreamCaptureModeThreadLocal));
+      c->counter = 0;
+      int rc = scheme == DGB_RK4 ? step_rk4(c, cfl) : step_ssprk3(c, cfl);
+      cudaError_t ec = cudaStreamEndCapture(c->st, &g);
+      if (rc) { if (ec == cudaSuccess) cudaGraphDestroy(g); return rc; }
+      DGB_CUDA(ec);
+      DGB_CUDA(cudaGraphInstantiate(&c->graphs[si][mi], g, 0));
+      cudaGraphDestroy(g);
+      c->graph_launches[si][mi] = c->counter;
+    }
+    DGB_CUDA(cudaEventRecord(c->e0, c->st));
+    for (int s = 0; s < nsteps; ++s) DGB_CUDA(cudaGraphLaunch(c->graphs[si][mi], c->st));
+    DGB_CUDA(cudaEventRecord(c->e1, c->st));
+    c->last_launches = c->graph_launches[si][mi] * nsteps;
+  }
+  if (int rc = read_scalars(c)) return rc;
+  float ms = 0;
+  cudaEventElapsedTime(&ms, c->e0, c->e1);
+  c->last_ms = ms;
+  if (time) *time += c->h_scal->time;
+  if (c->h_scal->flags & FLAG_NONFINITE) return set_error(DGB_ERR_NONFINITE, "time step is NaN");
+  if (c->h_scal->flags & FLAG_DT_SMALL) return set_error(DGB_ERR_DT_SMALL, "next time step is too small (< 1e-14)");
+  return DGB_OK;
+}
+
+extern "C" int dgb_last_dt(dgb_ctx* c, double* dt) {
+  if (!c || !dt) return set_error(DGB_ERR_ARG, "null argument");
+  *dt = c->h_scal->dt;
+  return DGB_OK;
+}
+
+extern "C" int dgb_last_timing(dgb_ctx* c, double* ms, long long* launches) {
+  if (!c) return set_error(DGB_ERR_ARG, "null context");
+  if (ms) *ms = c->last_ms;
+  if (launches) *launches = c->last_launches;
+  return DGB_OK;
+}
+
+extern "C" int dgb_set_profiling(dgb_ctx* c, int on) {
+  if (!c) return set_error(DGB_ERR_ARG, "null context");
+  c->prof = on != 0;
+  for (int k = 0; k < KC_N; ++k) { c->kc_ms[k] = 0; c->kc_n[k] = 0; }
+  return DGB_OK;
+}
+
+extern "C" int dgb_kernel_timing(dgb_ctx* c, const char* name, double* ms, long long* launches) {
+  if (!c || !name) return set_error(DGB_ERR_ARG, "null argument");
+  const std::string n = name;
+  int k = n == "residual" ? KC_RESIDUAL : n == "limiter" ? KC_LIMITER : n == "dt" ? KC_DT : n == "other" ? KC_OTHER : -1;
+  if (k < 0) return set_error(DGB_ERR_ARG, "unknown kernel class " + n);
+  if (ms) *ms = c->kc_ms[k];
+  if (launches) *launches = c->kc_n[k];
+  return DGB_OK;
+}
+
+extern "C" int dgb_conservation(dgb_ctx* c, double* totals) {
+  if (!c || !totals) return set_error(DGB_ERR_ARG, "null argument");
+  // integral of each field: sum_e sum_i U_i * (J * int phi_i) ; computed on the host from a
+  // state download (diagnostic only, as DG_SOLVER::conservation is)
+  std::vector<double> U((size_t)c->ne * c->nf * c->ns);
+  if (int rc = dgb_get_state(c, U.data())) return rc;
+  // int phi_i over the reference element, tensor factors from the volume quadrature
+  const Consts& cs = c->cs;
+  std::vector<double> w1(cs.n1, 0.0);
+  for (int i = 0; i < cs.n1; ++i)
+    for (int g = 0; g < cs.ng1; ++g) w1[i] += cs.wq[g] * cs.Bq[g][i];
+  std::vector<int> perm(c->ns);
+  cudaMemcpy(perm.data(), c->perm, c->ns * sizeof(int), cudaMemcpyDeviceToHost);
+  for (int f = 0; f < c->nf; ++f) totals[f] = 0.0;
+  for (int e = 0; e < c->ne; ++e)
+    for (int f = 0; f < c->nf; ++f)
+      for (int t = 0; t < c->ns; ++t) {
+        const int ix = t % cs.n1, iy = t / cs.n1;
+        const double w = c->D == 2 ? w1[ix] * w1[iy] : w1[ix];
+        totals[f] += U[((size_t)e * c->nf + f) * c->ns + perm[t]] * w * cs.J;
+      }
+  return DGB_OK;
+}

@@ -1,0 +1,186 @@
+"""Host-side mirror of the reference's solver objects over the C ABI.
+
+The reference drives its hot path through C++ objects built in code/src/main.cc:
+``DG_SOLVER`` (code/src/dg/dg_solver.h:104, ``dg_solver()`` at :292), ``Limiting``
+(code/src/limiting/limiting.h:123/249), ``RK`` (code/src/time_integration/rk.h:27,
+``RK_integration`` rk.cc:11, ``DtFromCFL`` rk.cc:250).  ``Problem`` and ``DGSolver`` below expose
+the same operations on the B200 path with the same argument meaning; states are float64 arrays in
+the reference layout ``U[(e*N_F+f)*N_s+i]`` (main.cc:814-820).  Failures the reference turns into
+``exit(1)`` raise :class:`DGBError` with the C status code.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from pathlib import Path
+from typing import Iterable, Sequence
+
+import numpy as np
+
+from . import _ffi as F
+
+
+class Problem:
+    """Deck + mesh + basis/quadrature/geometry setup (main.cc:273-860), host only."""
+
+    def __init__(self, handle: C.c_void_p):
+        self._h = handle
+        info = F.Info()
+        F.check(F.lib().dgb_problem_info(self._h, C.byref(info)))
+        self.info = info
+
+    @classmethod
+    def from_deck(cls, deck: str | Path) -> "Problem":
+        h = C.c_void_p()
+        F.check(F.lib().dgb_problem_from_deck(str(deck).encode(), C.byref(h)))
+        return cls(h)
+
+    @classmethod
+    def structured(cls, dim: int, order: int, nx: int, ny: int = 1, x0: float = 0.0, x1: float = 1.0,
+                   y0: float = 0.0, y1: float = 1.0, bc: Sequence[str | int] = ("transmissive",) * 4,
+                   flux: str = "roe", limiter: str = "m2l", cfl: float = -1.0,
+                   thresholds: Iterable[float] = ()) -> "Problem":
+        spec = mesh_spec(dim, order, nx, ny, x0, x1, y0, y1, bc)
+        opt = F.Options()
+        opt.flux = F.FLUX[flux.lower()]
+        opt.limiter = F.LIMITER[limiter.lower()]
+        opt.cfl = cfl
+        th = list(thresholds)[:3]
+        for k, t in enumerate(th):
+            opt.thresholds[k] = t
+        opt.n_thresholds = len(th)
+        h = C.c_void_p()
+        F.check(F.lib().dgb_problem_structured(C.byref(spec), C.byref(opt), C.byref(h)))
+        return cls(h)
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h:
+            F.lib().dgb_problem_destroy(h)
+            self._h = None
+
+    @property
+    def state_size(self) -> int:
+        i = self.info
+        return i.n_elem * i.n_fields * i.n_s
+
+    def array(self, name: str) -> np.ndarray:
+        n = C.c_size_t()
+        F.check(F.lib().dgb_problem_array_size(self._h, name.encode(), C.byref(n)))
+        ints = name in ("map", "invmap", "neighbors", "tensor_perm")
+        a = np.zeros(n.value // (4 if ints else 8), np.int32 if ints else np.float64)
+        F.check(F.lib().dgb_problem_get_array(self._h, name.encode(), a.ctypes.data_as(C.c_void_p), n.value))
+        return a
+
+    def init_state(self, ic: str, params: Sequence[float] = (), seed: int = 0) -> np.ndarray:
+        U = np.zeros(self.state_size)
+        prm = np.asarray(list(params), np.float64)
+        F.check(F.lib().dgb_problem_init_state(self._h, ic.encode(), F.dptr(prm) if prm.size else None,
+                                               int(prm.size), int(seed), F.dptr(U)))
+        return U
+
+    def write_pos(self, U: np.ndarray, step: int, time: float, directory: str | Path) -> None:
+        U = np.ascontiguousarray(U, np.float64)
+        F.check(F.lib().dgb_write_pos(self._h, F.dptr(U), int(step), float(time), str(directory).encode()))
+
+    def read_pos(self, step: int, directory: str | Path) -> tuple[np.ndarray, float]:
+        U = np.zeros(self.state_size)
+        t = C.c_double()
+        F.check(F.lib().dgb_read_pos(self._h, int(step), str(directory).encode(), C.byref(t), F.dptr(U)))
+        return U, t.value
+
+
+def mesh_spec(dim, order, nx, ny=1, x0=0.0, x1=1.0, y0=0.0, y1=1.0, bc=("transmissive",) * 4) -> F.MeshSpec:
+    s = F.MeshSpec()
+    s.dim, s.order, s.nx, s.ny = dim, order, nx, ny
+    s.x0, s.x1, s.y0, s.y1 = x0, x1, y0, y1
+    for k, b in enumerate(list(bc)[:4]):
+        s.bc[k] = b if isinstance(b, int) else F.BC[b]
+    return s
+
+
+def write_msh(path: str | Path, dim, order, nx, ny=1, x0=0.0, x1=1.0, y0=0.0, y1=1.0,
+              bc=("transmissive",) * 4) -> None:
+    """Gmsh 2.2 file of a structured mesh (element order row-major, boundary tags bc)."""
+    spec = mesh_spec(dim, order, nx, ny, x0, x1, y0, y1, bc)
+    F.check(F.lib().dgb_mesh_write_msh(C.byref(spec), str(path).encode()))
+
+
+class DGSolver:
+    """Device context: DG_SOLVER + Limiting + RK of the reference, on one GPU."""
+
+    def __init__(self, problem: Problem, device: int = 0):
+        self.problem = problem
+        self._h = C.c_void_p()
+        F.check(F.lib().dgb_create(problem._h, int(device), C.byref(self._h)))
+        self.n = problem.state_size
+
+    def close(self):
+        if getattr(self, "_h", None):
+            F.lib().dgb_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        self.close()
+
+    def _arr(self, U) -> np.ndarray:
+        U = np.ascontiguousarray(U, np.float64)
+        if U.size != self.n:
+            raise ValueError(f"state has {U.size} values, expected {self.n}")
+        return U
+
+    def set_state(self, U) -> None:
+        F.check(F.lib().dgb_set_state(self._h, F.dptr(self._arr(U))))
+
+    def get_state(self) -> np.ndarray:
+        U = np.zeros(self.n)
+        F.check(F.lib().dgb_get_state(self._h, F.dptr(U)))
+        return U
+
+    def dg_solver(self, U) -> np.ndarray:
+        """f = S + F + Q (DG_SOLVER::dg_solver)."""
+        f = np.zeros(self.n)
+        F.check(F.lib().dgb_residual(self._h, F.dptr(self._arr(U)), F.dptr(f)))
+        return f
+
+    def solve(self, dt: float, U) -> np.ndarray:
+        """DU = dt Minv f(U) (Lsolver applied to dg_solver's output)."""
+        DU = np.zeros(self.n)
+        F.check(F.lib().dgb_solve(self._h, float(dt), F.dptr(self._arr(U)), F.dptr(DU)))
+        return DU
+
+    def limit(self, U) -> np.ndarray:
+        """Limited copy of U with the problem's limiter (Limiting::*limiting)."""
+        V = self._arr(U).copy()
+        F.check(F.lib().dgb_limit(self._h, F.dptr(V)))
+        return V
+
+    def dt_from_cfl(self, U) -> float:
+        dt = C.c_double()
+        F.check(F.lib().dgb_dt_from_cfl(self._h, F.dptr(self._arr(U)), C.byref(dt)))
+        return dt.value
+
+    def advance(self, nsteps: int, dt: float = 0.0, scheme: int = F.SSPRK3) -> float:
+        """Advances the resident state; returns the time advanced (RK::RK_integration loop)."""
+        t = C.c_double(0.0)
+        F.check(F.lib().dgb_advance(self._h, int(scheme), int(nsteps), float(dt), C.byref(t)))
+        return t.value
+
+    def last_timing(self) -> tuple[float, int]:
+        ms = C.c_double()
+        n = C.c_longlong()
+        F.check(F.lib().dgb_last_timing(self._h, C.byref(ms), C.byref(n)))
+        return ms.value, n.value
+
+    def set_profiling(self, on: bool) -> None:
+        F.check(F.lib().dgb_set_profiling(self._h, 1 if on else 0))
+
+    def kernel_timing(self, name: str) -> tuple[float, int]:
+        ms = C.c_double()
+        n = C.c_longlong()
+        F.check(F.lib().dgb_kernel_timing(self._h, name.encode(), C.byref(ms), C.byref(n)))
+        return ms.value, n.value
+
+    def conservation(self) -> np.ndarray:
+        tot = np.zeros(self.problem.info.n_fields)
+        F.check(F.lib().dgb_conservation(self._h, F.dptr(tot)))
+        return tot

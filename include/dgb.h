@@ -1,0 +1,197 @@
+/*
+ * dgb.h -- C ABI of the B200-native DG residual / time-step path for the 1D/2D
+ * gamma-model multifluid Euler solver (drop-in for the reference's DG_SOLVER / RK /
+ * Limiting path).
+ *
+ * Two layers:
+ *   1. Host setup (C++; needs no GPU).  Replaces the setup sequence of the reference
+ *      driver code/src/main.cc:75-906: deck parsing (code/src/deck/deck.cc:11), Gmsh 2.2
+ *      mesh reading (code/src/mesh/simpleMesh.cc:141), interfaces/normals/neighbours
+ *      (simpleMesh.cc:206, 664, 770), nodal Lagrange basis and Gauss quadrature
+ *      (code/src/polynomials/polynomialBasis.cc:938, code/src/quadratures/Gauss*.cc),
+ *      Jacobians and inverse mass matrices (code/src/dg/dg_functions.cc:33-174) and the
+ *      limiter's Lagrange<->monomial transforms (main.cc:558-583, 1348-1524).
+ *   2. Device context (CUDA, sm_100a).  Replaces the reference's device-side path:
+ *      DG_SOLVER::dg_solver (code/src/dg/dg_solver.h:292), Lsolver
+ *      (code/src/time_integration/rk_kernels.cu:182), Limiting::HRlimiting/M2limiting
+ *      (code/src/limiting/limiting.cc:11, 123), RK::DtFromCFL (code/src/time_integration/rk.cc:250)
+ *      and RK::RK_integration (rk.cc:11).
+ *
+ * Conventions (all entry points):
+ *   - every call returns an int status (DGB_OK == 0); dgb_last_error() gives a message.
+ *     The reference exits the process on these conditions (rk.cc:147-148, deck.cc:58-61,
+ *     simpleMesh.cc:412-415); here they are returned.
+ *   - state arrays in the reference layout: U[(e*N_F + f)*N_s + i], float64, element-major,
+ *     field-major within the element, Gmsh node order fastest (main.cc:814-820).
+ *   - the library owns all device memory of a context; calls on one context are not reentrant.
+ *   - no CPU fallback: device entry points fail with DGB_ERR_NO_DEVICE / DGB_ERR_CUDA when the
+ *     GPU path cannot run.
+ */
+#ifndef DGB_H
+#define DGB_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define DGB_ABI_VERSION 1
+
+enum dgb_status {
+  DGB_OK = 0,
+  DGB_ERR_ARG = 1,         /* bad argument, size or name */
+  DGB_ERR_IO = 2,          /* deck / mesh / .pos file missing or malformed */
+  DGB_ERR_MESH = 3,        /* interface without two sides, bad neighbour normal */
+  DGB_ERR_UNSUPPORTED = 4, /* configuration outside the GPU path (see dgb_last_error) */
+  DGB_ERR_CUDA = 5,        /* CUDA runtime error */
+  DGB_ERR_NONFINITE = 6,   /* time step is NaN (reference rk.cc:148 exits) */
+  DGB_ERR_DT_SMALL = 7,    /* time step < 1e-14 (reference rk.cc:147 exits) */
+  DGB_ERR_TIMEOUT = 8,     /* a bounded device wait expired */
+  DGB_ERR_NO_DEVICE = 9    /* no CUDA device / wrong architecture */
+};
+
+/* Riemann solver (compile-time FLUX=RUS|HLL|ROE in the reference Makefile:30-51). */
+enum dgb_flux { DGB_FLUX_RUSANOV = 0, DGB_FLUX_HLL = 1, DGB_FLUX_ROE = 2 };
+
+/* Limiter codes, same numbering as the reference deck strings (main.cc:167-175). */
+enum dgb_limiter {
+  DGB_LIM_NONE = 0, DGB_LIM_HRL = 1, DGB_LIM_M2L = 2, DGB_LIM_HRI = 3,
+  DGB_LIM_M2I = 4, DGB_LIM_PRL = 5, DGB_LIM_PRI = 6, DGB_LIM_P0I = 7
+};
+
+/* Time integrators: classical RK4 (reference rk.h:44-57) and Shu-Osher SSP-RK3 (new). */
+enum dgb_scheme { DGB_SSPRK3 = 3, DGB_RK4 = 4 };
+
+/* Gmsh physical tags used for boundaries (simpleMesh.cc:842-845, 702; boundaries.cu:20). */
+enum dgb_bc { DGB_BC_PERIODIC = 1, DGB_BC_TRANSMISSIVE = 2, DGB_BC_REFLECTIVE = 3, DGB_BC_FROZEN = 4 };
+
+const char* dgb_last_error(void);
+int dgb_abi_version(void);
+
+/* ------------------------------------------------------------------------------------
+ * Host setup
+ * ------------------------------------------------------------------------------------ */
+typedef struct dgb_problem dgb_problem;
+
+/* Structured Cartesian mesh of the kind a Gmsh .geo "Transfinite ... Recombine" produces:
+ * nx (x ny) elements of order `order`, elements numbered row-major (x fastest), boundary
+ * elements carrying physical tags bc[] (1D: left,right; 2D: bottom,right,top,left). */
+typedef struct {
+  int dim;        /* 1 or 2 */
+  int order;      /* polynomial order p >= 1 */
+  int nx, ny;     /* elements per direction (ny ignored in 1D) */
+  double x0, x1, y0, y1;
+  int bc[4];
+} dgb_mesh_spec;
+
+/* Solver options that the reference takes from the deck and its compile-time flags. */
+typedef struct {
+  int flux;            /* enum dgb_flux */
+  int limiter;         /* enum dgb_limiter */
+  double cfl;          /* deck CFL; < 0 selects a fixed step (rk.cc:136-139) */
+  double thresholds[3];/* sensor thresholds (sensor.h:35-45); n_thresholds of them are set */
+  int n_thresholds;
+} dgb_options;
+
+/* Reads a reference input deck (format of code/src/deck/deck.cc:11-64) and the Gmsh 2.2 mesh
+ * it names (path relative to the deck's directory).  The flux comes from the deck's optional
+ * "#Make options" block (FLUX=ROE|RUS|HLL, the block tests/runtests.py:80-87 reads), else ROE. */
+int dgb_problem_from_deck(const char* deck_path, dgb_problem** out);
+/* Builds the same problem from an in-memory structured mesh (identical to reading the file
+ * that dgb_mesh_write_msh writes for the same spec). */
+int dgb_problem_structured(const dgb_mesh_spec* mesh, const dgb_options* opt, dgb_problem** out);
+/* Writes a Gmsh 2.2 ASCII mesh for the spec (replaces running gmsh on a .geo file). */
+int dgb_mesh_write_msh(const dgb_mesh_spec* mesh, const char* path);
+void dgb_problem_destroy(dgb_problem* p);
+
+typedef struct {
+  int dim, order, n_fields;      /* D, p, N_F */
+  int n_elem, n_s, n_g;          /* N_E, N_s, N_G */
+  int n_ifaces, m_s, m_g, n_n;   /* M_T, M_s, M_G, N_N */
+  int n_reflective;              /* reflective interfaces (M_B of buildBoundary) */
+  int cartesian;                 /* iscartesian() (simpleMesh.cc:1102) */
+  int gpu_supported;             /* 1 when the device path supports this problem */
+  int flux, limiter;
+  int nx, ny;                    /* structured extents when detected, else 0 */
+  double cfl, dx_min, cfl_scaled;/* cfl_scaled = CFL*Dx/(2p+1) (main.cc:896-897) */
+  double final_time;
+  int n_output_times;
+} dgb_info;
+
+int dgb_problem_info(const dgb_problem* p, dgb_info* out);
+
+/* Copies a named host array, in the reference's own layout, into dst (nbytes must match).
+ * Names: "phi","dphi","phi_w","dphi_w","psi","psi_w","weight","J","invJac","JF","normals",
+ * "Minv","map","invmap","neighbors","Lag2Mono","Mono2Lag","Lag2MonoX","MonoX2MonoY",
+ * "MonoY2Lag","MonoX2Lag","Lag2MonoY","xyz_nodes","output_times". */
+int dgb_problem_array_size(const dgb_problem* p, const char* name, size_t* nbytes);
+int dgb_problem_get_array(const dgb_problem* p, const char* name, void* dst, size_t nbytes);
+
+/* Seeded initial states (reference layout).  Names: "sodtube" (reference init_cond.cc:400),
+ * "tube_noise" (two-fluid tube split at params[0] with +-params[1] uniform noise on rho),
+ * "shock_bubble" (Mach-1.5 shock hitting a gamma=1.67 bubble, 1% seeded Fourier
+ * perturbation of the radius), "quadrants" (four-quadrant Riemann problem, seeded states). */
+int dgb_problem_init_state(const dgb_problem* p, const char* ic, const double* params, int nparams,
+                           uint64_t seed, double* U);
+
+/* Output in the reference .pos format (code/src/mesh/simpleMesh.cc:322-376 via
+ * code/src/printer/printer.cc:77): one file per primitive field, <dir>/<name><step>.pos. */
+int dgb_write_pos(const dgb_problem* p, const double* U, int step, double time, const char* dir);
+/* Restart read of the same files (printer.cc:108, simpleMesh.cc:378). */
+int dgb_read_pos(const dgb_problem* p, int step, const char* dir, double* time, double* U);
+
+/* ------------------------------------------------------------------------------------
+ * Device context
+ * ------------------------------------------------------------------------------------ */
+typedef struct dgb_ctx dgb_ctx;
+
+/* Uploads geometry, basis and limiter data and allocates the resident state
+ * (replaces the DG_SOLVER, Limiting and RK constructors: dg_solver.h:104, limiting.h:123/249). */
+int dgb_create(const dgb_problem* p, int device, dgb_ctx** out);
+void dgb_destroy(dgb_ctx* c);
+
+/* Resident state from / to host memory (reference layout). */
+int dgb_set_state(dgb_ctx* c, const double* U_host);
+int dgb_get_state(dgb_ctx* c, double* U_host);
+/* Same with device pointers in the reference layout (no host staging). */
+int dgb_set_state_device(dgb_ctx* c, const double* U_dev);
+int dgb_get_state_device(dgb_ctx* c, double* U_dev);
+
+/* f = S + F + Q for the state U (DG_SOLVER::dg_solver, dg_solver.h:292-364).
+ * Host arrays in the reference layout; the resident state is not touched. */
+int dgb_residual(dgb_ctx* c, const double* U_host, double* f_host);
+/* DU = dt * Minv * f(U) (Lsolver, rk_kernels.cu:182, applied to dg_solver's output). */
+int dgb_solve(dgb_ctx* c, double dt, const double* U_host, double* DU_host);
+/* In-place limiting with the problem's limiter (Limiting::*limiting, limiting.cc). */
+int dgb_limit(dgb_ctx* c, double* U_host);
+/* Dt = CFL_scaled / max_nodes(|u|+a) (RK::DtFromCFL, rk.cc:250-272). */
+int dgb_dt_from_cfl(dgb_ctx* c, const double* U_host, double* dt);
+
+/* Advances the resident state by nsteps steps of `scheme`.
+ * dt > 0: fixed step (the reference's CFL<0 mode, rk.cc:136-139);
+ * dt <= 0: step from the CFL condition, computed on the device each step.
+ * Limiter placement follows rk.cc:176-209 (stage inputs after the first, end of step).
+ * *time is advanced by the steps taken.  Status DGB_ERR_NONFINITE / DGB_ERR_DT_SMALL when the
+ * CFL step is NaN / < 1e-14 (checked after the run; the state then holds the failing step). */
+int dgb_advance(dgb_ctx* c, int scheme, int nsteps, double dt, double* time);
+
+/* Last step size used by dgb_advance (host copy). */
+int dgb_last_dt(dgb_ctx* c, double* dt);
+
+/* Conserved totals sum_e sum_g U_g J w_g per field (DG_SOLVER::conservation, dg_solver.h:367). */
+int dgb_conservation(dgb_ctx* c, double* totals /* N_F */);
+
+/* Device time (ms) of the last dgb_advance measured with CUDA events on the library stream,
+ * and the number of kernel launches it issued. */
+int dgb_last_timing(dgb_ctx* c, double* ms, long long* launches);
+/* Per-kernel device time of the last dgb_advance when profiling is on:
+ * names "residual", "limiter", "dt"; ms and launches of that kernel class. */
+int dgb_set_profiling(dgb_ctx* c, int on);
+int dgb_kernel_timing(dgb_ctx* c, const char* name, double* ms, long long* launches);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* DGB_H */

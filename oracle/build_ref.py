@@ -1,0 +1,125 @@
+"""Build recipe for the reference CPU oracle binaries (test infrastructure only).
+
+Compiles the reference's own sources, where they lie under the read-only checkout
+(code/src/**/*.cc and *.cu, the latter as C++ exactly as the reference Makefile does for
+ARCH=USE_CPU, code/Makefile:187-189), once per compile-time configuration, and links each
+set with oracle/ref_harness.cc into ``oracle/_ref/dgref_<variant>``.  Outputs go only to
+``oracle/_ref/`` (git-ignored; it travels with the working tree to GPU hosts).
+
+Compile-time configuration follows code/Makefile:147-156 (DEFINES) for the gamma-model
+multifluid build: USE_CPU, USE_DOUBLE, MULTIFLUID, GAMNCON, NO_MPI, N_Y=0, and
+N_F=4 (1D) / 5 (2D), D=1/2, DF=1, with the flux flag ROE, RUS or HLL.
+
+Out-of-tree additions (none of them touch reference arithmetic):
+  * an empty ``gsl/gsl_integration.h`` (code/src/ic/init_cond.cc:10 includes it, never calls it);
+  * LP64 OpenBLAS/LAPACK from the image (plain F77 symbol names);
+  * ``--wrap`` of blasIdamax, which lacks a return statement (code/src/utils/misc.cc:38-41);
+  * ``--wrap`` of RK::RK_integration so the harness can drive single operators;
+  * main() renamed to dgref_main.
+
+Usage: python oracle/build_ref.py [--ref /root/reference/code/src] [--jobs 8] [variant ...]
+"""
+from __future__ import annotations
+
+import argparse
+import concurrent.futures as cf
+import hashlib
+import os
+import subprocess
+import sys
+from pathlib import Path
+
+HERE = Path(__file__).resolve().parent
+OUT = HERE / "_ref"
+DEFAULT_REF = Path("/root/reference/code/src")
+BLAS_DIR = Path("/opt/prime-rl/.venv/lib/python3.12/site-packages/opencv_python_headless.libs")
+BLAS_LIB = "libopenblasp-r0-59ffcd50.3.15.so"
+
+VARIANTS = {
+    "1d_roe": dict(dims="ONED", nf=4, d=1, flux="ROE"),
+    "1d_rus": dict(dims="ONED", nf=4, d=1, flux="RUS"),
+    "1d_hll": dict(dims="ONED", nf=4, d=1, flux="HLL"),
+    "2d_roe": dict(dims="TWOD", nf=5, d=2, flux="ROE"),
+    "2d_rus": dict(dims="TWOD", nf=5, d=2, flux="RUS"),
+}
+
+RK_SYM = ("_ZN2RK14RK_integrationEdiiiiiiiPdS0_R8LimitingbR9DG_SOLVERR12COMMUNICATORR7PRINTER"
+          "R6SENSORR6TIMERSR11MEM_COUNTERR18LAGRANGE_PARTICLES")
+
+
+def defines(v: dict) -> list[str]:
+    return ["-DHAVE_BLAS", "-DHAVE_LAPACK", "-DUSE_CPU", "-DHOME", "-DUSE_DOUBLE", "-DMULTIFLUID",
+            "-DGAMNCON", f"-D{v['flux']}", f"-D{v['dims']}", "-DNO_MPI", "-DN_Y=0", f"-DN_F={v['nf']}",
+            "-DNOERROR", "-DNOCONS", f"-DD={v['d']}", "-DDF=1"]
+
+
+def sources(ref: Path) -> list[Path]:
+    return sorted([p for p in ref.rglob("*") if p.suffix in (".cc", ".cu")])
+
+
+def includes(ref: Path) -> list[str]:
+    dirs = sorted({p.parent for p in ref.rglob("*.h")} | {ref})
+    return [f"-I{HERE / 'stub'}"] + [f"-I{d}" for d in dirs]
+
+
+def compile_one(src: Path, obj: Path, flags: list[str]) -> tuple[Path, int, str]:
+    obj.parent.mkdir(parents=True, exist_ok=True)
+    cmd = ["g++", "-std=gnu++98", "-O3", "-w", "-x", "c++"] + flags + ["-c", str(src), "-o", str(obj)]
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    return obj, r.returncode, r.stderr[-2000:]
+
+
+def build_variant(name: str, ref: Path, pool: cf.Executor) -> Path:
+    v = VARIANTS[name]
+    flags = defines(v) + includes(ref)
+    key = hashlib.sha1((" ".join(flags) + str(ref)).encode()).hexdigest()[:8]
+    objdir = OUT / f"obj_{name}_{key}"
+    jobs = []
+    for src in sources(ref):
+        rel = src.relative_to(ref)
+        obj = objdir / (str(rel).replace("/", "__") + ".o")
+        extra = ["-Dmain=dgref_main"] if rel.name == "main.cc" else []
+        if obj.exists() and obj.stat().st_mtime >= src.stat().st_mtime:
+            continue
+        jobs.append(pool.submit(compile_one, src, obj, flags + extra))
+    for j in jobs:
+        obj, rc, err = j.result()
+        if rc != 0:
+            raise RuntimeError(f"compile failed for {obj.name}:\n{err}")
+    harness_obj = objdir / "ref_harness.o"
+    hsrc = HERE / "ref_harness.cc"
+    if not harness_obj.exists() or harness_obj.stat().st_mtime < hsrc.stat().st_mtime:
+        cmd = ["g++", "-std=gnu++11", "-O3", "-w"] + flags + ["-c", str(hsrc), "-o", str(harness_obj)]
+        r = subprocess.run(cmd, capture_output=True, text=True)
+        if r.returncode != 0:
+            raise RuntimeError(f"harness compile failed:\n{r.stderr[-3000:]}")
+    exe = OUT / f"dgref_{name}"
+    objs = sorted(str(p) for p in objdir.glob("*.o"))
+    link = (["g++", "-o", str(exe)] + objs +
+            [f"-Wl,--wrap=_Z10blasIdamaxiPdi", f"-Wl,--wrap={RK_SYM}",
+             f"-L{BLAS_DIR}", f"-l:{BLAS_LIB}", "-Wl,--disable-new-dtags", f"-Wl,-rpath,{BLAS_DIR}", "-lm"])
+    r = subprocess.run(link, capture_output=True, text=True)
+    if r.returncode != 0:
+        raise RuntimeError(f"link failed for {name}:\n{r.stderr[-3000:]}")
+    return exe
+
+
+def main(argv=None) -> int:
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--ref", type=Path, default=DEFAULT_REF)
+    ap.add_argument("--jobs", type=int, default=os.cpu_count() or 4)
+    ap.add_argument("variants", nargs="*", default=list(VARIANTS))
+    a = ap.parse_args(argv)
+    if not a.ref.is_dir():
+        print(f"reference sources not found at {a.ref}; nothing built", file=sys.stderr)
+        return 1
+    OUT.mkdir(parents=True, exist_ok=True)
+    with cf.ThreadPoolExecutor(a.jobs) as pool:
+        for name in a.variants:
+            exe = build_variant(name, a.ref, pool)
+            print(f"built {exe}")
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,266 @@
+// Oracle harness around the UNMODIFIED reference CPU build (test infrastructure only).
+//
+// The reference sources under code/src are compiled as-is (CPU mode, g++ -x c++) by
+// oracle/build_ref.py; code/src/main.cc is compiled with -Dmain=dgref_main so that this
+// file owns the process entry point.  The reference main() builds every host array
+// (mesh, basis, quadrature, Jacobians, inverse mass matrices, maps, limiter transforms)
+// exactly as it does in production and then calls RK::RK_integration
+// (code/src/time_integration/rk.cc:11).  That call is intercepted with the linker's
+// --wrap so that, instead of (or in addition to) the reference time loop, this harness
+// can run one command on a state read from a file:
+//
+//   dump      write the solver's host arrays (phi, dphi, ..., Minv, maps, neighbors,
+//             limiter transforms) and the reference initial condition
+//   residual  f = DG_SOLVER::dg_solver(U)            (code/src/dg/dg_solver.h:292)
+//   solve     DU = Dt Minv f                          (code/src/time_integration/rk_kernels.cu:182)
+//   limit     U <- Limiting::<deck method>(U)         (code/src/limiting/limiting.cc)
+//   dt        Dt = RK::DtFromCFL(U)                   (code/src/time_integration/rk.cc:250)
+//   rk4       the reference time loop itself on U     (code/src/time_integration/rk.cc:11)
+//   rk4n      n steps of the reference RK4 step body (rk.cc:155-209), fixed or CFL step
+//   rk3       SSP-RK3 (Shu-Osher) built from the reference residual, Lsolver and limiter,
+//             with the limiter placed as rk.cc:176-209 places it for RK4
+//
+// Nothing here changes reference arithmetic.  Two link-level workarounds are needed to run
+// the reference at all with a modern g++: blasIdamax (code/src/utils/misc.cc:38) has no
+// return statement, so it is wrapped to return idamax_'s value.
+//
+// Usage: dgref -d deck.inp --cmd <name> [--in U.bin] [--out out.bin] [--dir dumpdir]
+//              [--dt value] [--nsteps n] [--repeat n]
+// U files are raw little-endian float64 in the reference layout U[(e*N_F+f)*N_s+i].
+
+#include <string>
+#include <vector>
+#include <map>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <cmath>
+#include <iostream>
+#include <fstream>
+#include <sstream>
+#include <algorithm>
+#include <stdexcept>
+#include <chrono>
+
+// The harness reads private members of the reference classes (host copies of the arrays
+// they were constructed with).  Access specifiers do not change layout here.
+#define private public
+#include "scalar_def.h"
+#include "rk.h"
+#include "dg_solver.h"
+#include "limiting.h"
+#include "sensor.h"
+#include "printer.h"
+#undef private
+
+extern "C" int idamax_(int* n, double* x, int* incx);
+
+extern "C" int __wrap__Z10blasIdamaxiPdi(int N, double* x, int incx) { return idamax_(&N, x, &incx); }
+
+int dgref_main(int argc, char** argv);
+
+namespace {
+
+struct Args {
+  std::string deck = "deck.inp";
+  std::string cmd = "none";
+  std::string in, out, dir = ".";
+  double dt = 0.0;
+  int nsteps = 1;
+  int repeat = 1;
+};
+Args g_args;
+
+std::vector<double> read_doubles(const std::string& path, size_t n) {
+  std::vector<double> v(n);
+  FILE* f = fopen(path.c_str(), "rb");
+  if (!f) { fprintf(stderr, "dgref: cannot open %s\n", path.c_str()); exit(3); }
+  size_t got = fread(v.data(), sizeof(double), n, f);
+  fclose(f);
+  if (got != n) { fprintf(stderr, "dgref: %s holds %zu doubles, expected %zu\n", path.c_str(), got, n); exit(3); }
+  return v;
+}
+
+template <typename T>
+void write_raw(const std::string& path, const T* p, size_t n) {
+  FILE* f = fopen(path.c_str(), "wb");
+  if (!f) { fprintf(stderr, "dgref: cannot write %s\n", path.c_str()); exit(3); }
+  fwrite(p, sizeof(T), n, f);
+  fclose(f);
+}
+
+void limit_in_place(Limiting& L, COMMUNICATOR& comm, SENSOR& sensor, DG_SOLVER& dg, scalar* U) {
+  switch (L.getLimitingMethod()) {
+    case 1: L.HRlimiting(comm, U); break;
+    case 2: L.M2limiting(comm, U); break;
+    case 3: L.HRIlimiting(comm, sensor, U); break;
+    case 4: L.M2Ilimiting(comm, sensor, U); break;
+    case 5: L.PRlimiting(comm, U); break;
+    case 6: L.PRIlimiting(comm, sensor, U); break;
+    case 7: L.P0Ilimiting(comm, sensor, dg, U); break;
+    default: break;
+  }
+}
+
+}  // namespace
+
+typedef void (*rk_fn)(RK*, scalar, int, int, int, int, int, int, int, scalar*, scalar*, Limiting*, bool,
+                      DG_SOLVER*, COMMUNICATOR*, PRINTER*, SENSOR*, TIMERS*, MEM_COUNTER*, LAGRANGE_PARTICLES*);
+
+extern "C" void
+__real__ZN2RK14RK_integrationEdiiiiiiiPdS0_R8LimitingbR9DG_SOLVERR12COMMUNICATORR7PRINTERR6SENSORR6TIMERSR11MEM_COUNTERR18LAGRANGE_PARTICLES(
+    RK*, scalar, int, int, int, int, int, int, int, scalar*, scalar*, Limiting*, bool, DG_SOLVER*, COMMUNICATOR*,
+    PRINTER*, SENSOR*, TIMERS*, MEM_COUNTER*, LAGRANGE_PARTICLES*);
+
+extern "C" void
+__wrap__ZN2RK14RK_integrationEdiiiiiiiPdS0_R8LimitingbR9DG_SOLVERR12COMMUNICATORR7PRINTERR6SENSORR6TIMERSR11MEM_COUNTERR18LAGRANGE_PARTICLES(
+    RK* rk, scalar CFL, int restart_step, int N_E, int N_s, int N_G, int M_T, int M_s, int N_ghosts, scalar* h_Minv,
+    scalar* h_U, Limiting* Lim, bool order0, DG_SOLVER* dg, COMMUNICATOR* comm, PRINTER* printer, SENSOR* sensor,
+    TIMERS* timers, MEM_COUNTER* mem, LAGRANGE_PARTICLES* particles) {
+  const Args& a = g_args;
+  const size_t n = (size_t)N_s * N_E * N_F;
+  if (a.cmd == "dump") {
+    const std::string d = a.dir + "/";
+    write_raw(d + "U0.bin", h_U, n);
+    write_raw(d + "phi.bin", dg->_phi, (size_t)N_G * N_s);
+    write_raw(d + "dphi.bin", dg->_dphi, (size_t)D * N_G * N_s);
+    write_raw(d + "phi_w.bin", dg->_phi_w, (size_t)N_G * N_s);
+    write_raw(d + "dphi_w.bin", dg->_dphi_w, (size_t)D * N_G * N_s);
+    write_raw(d + "psi.bin", dg->_psi, (size_t)dg->_M_G * M_s);
+    write_raw(d + "psi_w.bin", dg->_psi_w, (size_t)dg->_M_G * M_s);
+    write_raw(d + "J.bin", dg->_J, (size_t)N_E);
+    write_raw(d + "invJac.bin", dg->_invJac, (size_t)N_G * D * N_E * D);
+    write_raw(d + "JF.bin", dg->_JF, (size_t)2 * M_T);
+    write_raw(d + "normals.bin", dg->_normals, (size_t)D * M_T);
+    write_raw(d + "map.bin", dg->_map, (size_t)M_s * M_T * N_F * 2);
+    write_raw(d + "invmap.bin", dg->_invmap, (size_t)M_s * dg->_N_N * N_E * N_F * 2);
+    write_raw(d + "weight.bin", dg->_weight, (size_t)N_G);
+    write_raw(d + "Minv.bin", h_Minv, (size_t)N_s * N_s * N_E);
+    if (Lim->_neighbors) write_raw(d + "neighbors.bin", Lim->_neighbors, (size_t)Lim->_N_N * N_E);
+    const size_t m2 = (size_t)N_s * N_s;
+    if (Lim->_Lag2Mono) write_raw(d + "Lag2Mono.bin", Lim->_Lag2Mono, m2);
+    if (Lim->_Mono2Lag) write_raw(d + "Mono2Lag.bin", Lim->_Mono2Lag, m2);
+    if (Lim->_Lag2MonoX) write_raw(d + "Lag2MonoX.bin", Lim->_Lag2MonoX, m2);
+    if (Lim->_MonoX2MonoY) write_raw(d + "MonoX2MonoY.bin", Lim->_MonoX2MonoY, m2);
+    if (Lim->_MonoY2Lag) write_raw(d + "MonoY2Lag.bin", Lim->_MonoY2Lag, m2);
+    if (Lim->_MonoX2Lag) write_raw(d + "MonoX2Lag.bin", Lim->_MonoX2Lag, m2);
+    if (Lim->_Lag2MonoY) write_raw(d + "Lag2MonoY.bin", Lim->_Lag2MonoY, m2);
+    FILE* f = fopen((d + "meta.txt").c_str(), "w");
+    fprintf(f, "D %d\nN_F %d\nN_E %d\nN_s %d\nN_G %d\nM_T %d\nM_s %d\nM_G %d\nN_N %d\nM_B %d\n", D, N_F, N_E, N_s,
+            N_G, M_T, M_s, dg->_M_G, dg->_N_N, dg->_M_B);
+    fprintf(f, "cfl_scaled %.17g\nlimiter %d\ncartesian %d\n", (double)CFL, Lim->getLimitingMethod(),
+            (int)Lim->_cartesian);
+    fclose(f);
+    return;
+  }
+  if (a.cmd == "none") {
+    __real__ZN2RK14RK_integrationEdiiiiiiiPdS0_R8LimitingbR9DG_SOLVERR12COMMUNICATORR7PRINTERR6SENSORR6TIMERSR11MEM_COUNTERR18LAGRANGE_PARTICLES(
+        rk, CFL, restart_step, N_E, N_s, N_G, M_T, M_s, N_ghosts, h_Minv, h_U, Lim, order0, dg, comm, printer, sensor,
+        timers, mem, particles);
+    return;
+  }
+  std::vector<double> U = read_doubles(a.in, n);
+  if (a.cmd == "residual") {
+    std::vector<double> f(n, 0.0);
+    for (int r = 0; r < a.repeat; ++r) dg->dg_solver(U.data(), f.data());
+    write_raw(a.out, f.data(), n);
+  } else if (a.cmd == "solve") {
+    std::vector<double> f(n, 0.0), DU(n, 0.0);
+    dg->dg_solver(U.data(), f.data());
+    Lsolver(N_s, N_E, a.dt, h_Minv, f.data(), DU.data());
+    write_raw(a.out, DU.data(), n);
+  } else if (a.cmd == "limit") {
+    for (int r = 0; r < a.repeat; ++r) limit_in_place(*Lim, *comm, *sensor, *dg, U.data());
+    write_raw(a.out, U.data(), n);
+  } else if (a.cmd == "dt") {
+    std::vector<double> upa((size_t)N_s * N_E, 0.0);
+    double dt = rk->DtFromCFL(N_s, N_E, CFL, U.data(), upa.data());
+    write_raw(a.out, &dt, 1);
+  } else if (a.cmd == "rk4") {
+    memcpy(h_U, U.data(), n * sizeof(double));
+    auto t0 = std::chrono::steady_clock::now();
+    __real__ZN2RK14RK_integrationEdiiiiiiiPdS0_R8LimitingbR9DG_SOLVERR12COMMUNICATORR7PRINTERR6SENSORR6TIMERSR11MEM_COUNTERR18LAGRANGE_PARTICLES(
+        rk, CFL, 0, N_E, N_s, N_G, M_T, M_s, N_ghosts, h_Minv, h_U, Lim, order0, dg, comm, printer, sensor, timers,
+        mem, particles);
+    auto t1 = std::chrono::steady_clock::now();
+    fprintf(stdout, "DGREF_WALL_S %.9f\n", std::chrono::duration<double>(t1 - t0).count());
+    write_raw(a.out, h_U, n);
+  } else if (a.cmd == "rk4n") {
+    // a.nsteps steps of the reference step body (rk.cc:155-209) with step a.dt, or the CFL step
+    // (DtFromCFL) when a.dt <= 0; no output-time clipping.
+    std::vector<double> Us(n), Ustar(n), f(n), DU(n), upa((size_t)N_s * N_E);
+    auto t0 = std::chrono::steady_clock::now();
+    for (int s = 0; s < a.nsteps; ++s) {
+      const double Dt = a.dt > 0 ? a.dt : rk->DtFromCFL(N_s, N_E, CFL, U.data(), upa.data());
+      blasCopy(N_F * N_s * N_E, U.data(), 1, Us.data(), 1);
+      for (int k = 0; k < 4; ++k) {
+        blasCopy(N_F * N_s * N_E, Us.data(), 1, Ustar.data(), 1);
+        if (k > 0) blasAxpy(N_s * N_F * N_E, rk->_beta[k], DU.data(), 1, Ustar.data(), 1);
+        if (k > 0) limit_in_place(*Lim, *comm, *sensor, *dg, Ustar.data());
+        dg->dg_solver(Ustar.data(), f.data());
+        Lsolver(N_s, N_E, Dt, h_Minv, f.data(), DU.data());
+        blasAxpy(N_s * N_F * N_E, rk->_gamma[k], DU.data(), 1, U.data(), 1);
+      }
+      limit_in_place(*Lim, *comm, *sensor, *dg, U.data());
+    }
+    auto t1 = std::chrono::steady_clock::now();
+    fprintf(stdout, "DGREF_WALL_S %.9f\n", std::chrono::duration<double>(t1 - t0).count());
+    write_raw(a.out, U.data(), n);
+  } else if (a.cmd == "rk3") {
+    // Shu-Osher SSP-RK3 with a fixed step a.dt, a.nsteps steps; limiter on every stage input
+    // after the first and on the end-of-step solution (placement of rk.cc:176-209).
+    std::vector<double> Un(n), U1(n), f(n), DU(n);
+    auto t0 = std::chrono::steady_clock::now();
+    std::vector<double> upa((size_t)N_s * N_E);
+    for (int s = 0; s < a.nsteps; ++s) {
+      const double Dt = a.dt > 0 ? a.dt : rk->DtFromCFL(N_s, N_E, CFL, U.data(), upa.data());
+      Un = U;
+      // stage 1: U1 = Un + dt L(Un)
+      dg->dg_solver(U.data(), f.data());
+      Lsolver(N_s, N_E, Dt, h_Minv, f.data(), DU.data());
+      for (size_t k = 0; k < n; ++k) U1[k] = Un[k] + DU[k];
+      limit_in_place(*Lim, *comm, *sensor, *dg, U1.data());
+      // stage 2: U2 = 3/4 Un + 1/4 (U1 + dt L(U1))
+      dg->dg_solver(U1.data(), f.data());
+      Lsolver(N_s, N_E, Dt, h_Minv, f.data(), DU.data());
+      for (size_t k = 0; k < n; ++k) U1[k] = 0.75 * Un[k] + 0.25 * (U1[k] + DU[k]);
+      limit_in_place(*Lim, *comm, *sensor, *dg, U1.data());
+      // stage 3: U = 1/3 Un + 2/3 (U2 + dt L(U2))
+      dg->dg_solver(U1.data(), f.data());
+      Lsolver(N_s, N_E, Dt, h_Minv, f.data(), DU.data());
+      for (size_t k = 0; k < n; ++k) U[k] = (1.0 / 3.0) * Un[k] + (2.0 / 3.0) * (U1[k] + DU[k]);
+      limit_in_place(*Lim, *comm, *sensor, *dg, U.data());
+    }
+    auto t1 = std::chrono::steady_clock::now();
+    fprintf(stdout, "DGREF_WALL_S %.9f\n", std::chrono::duration<double>(t1 - t0).count());
+    write_raw(a.out, U.data(), n);
+  } else {
+    fprintf(stderr, "dgref: unknown command %s\n", a.cmd.c_str());
+    exit(2);
+  }
+}
+
+int main(int argc, char** argv) {
+  for (int i = 1; i < argc; ++i) {
+    std::string k = argv[i];
+    auto next = [&](void) -> std::string {
+      if (i + 1 >= argc) { fprintf(stderr, "dgref: %s needs a value\n", k.c_str()); exit(2); }
+      return std::string(argv[++i]);
+    };
+    if (k == "-d") g_args.deck = next();
+    else if (k == "--cmd") g_args.cmd = next();
+    else if (k == "--in") g_args.in = next();
+    else if (k == "--out") g_args.out = next();
+    else if (k == "--dir") g_args.dir = next();
+    else if (k == "--dt") g_args.dt = atof(next().c_str());
+    else if (k == "--nsteps") g_args.nsteps = atoi(next().c_str());
+    else if (k == "--repeat") g_args.repeat = atoi(next().c_str());
+    else { fprintf(stderr, "dgref: unknown argument %s\n", k.c_str()); return 2; }
+  }
+  std::string deck = g_args.deck;
+  char a0[] = "dgref", a1[] = "-d";
+  std::vector<char> a2(deck.begin(), deck.end());
+  a2.push_back('\0');
+  char* av[] = {a0, a1, a2.data(), nullptr};
+  return dgref_main(3, av);
+}

@@ -1,0 +1,153 @@
+"""Driver for the reference CPU oracle binaries built by oracle/build_ref.py (test infrastructure).
+
+Writes a Gmsh mesh and a reference input deck into a work directory, runs
+``oracle/_ref/dgref_<dim>d_<flux> -d deck.inp --cmd <cmd>`` (see oracle/ref_harness.cc) on a
+state file and reads the result back.  Only tests, fixture generation and the CPU-baseline leg
+of bench.py use this module.
+"""
+from __future__ import annotations
+
+import os
+import subprocess
+import tempfile
+from dataclasses import dataclass, field
+from pathlib import Path
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+REF_DIR = HERE / "_ref"
+
+FLUX_TAG = {"rusanov": "rus", "rus": "rus", "roe": "roe", "hll": "hll"}
+BC_TAG = {"periodic": 1, "transmissive": 2, "reflective": 3, "frozen": 4}
+
+
+def binary(dim: int, flux: str) -> Path:
+    return REF_DIR / f"dgref_{dim}d_{FLUX_TAG[flux.lower()]}"
+
+
+def available(dim: int = 2, flux: str = "rusanov") -> bool:
+    return binary(dim, flux).exists()
+
+
+@dataclass
+class RefCase:
+    dim: int
+    order: int
+    nx: int
+    ny: int = 1
+    x0: float = 0.0
+    x1: float = 1.0
+    y0: float = 0.0
+    y1: float = 1.0
+    bc: tuple = ("transmissive",) * 4
+    flux: str = "rusanov"
+    limiter: str = "m2l"
+    cfl: float = -1.0
+    output_times: tuple = (0.0, 1e-3)
+    workdir: Path | None = None
+    _tmp: object = field(default=None, repr=False)
+
+    def __post_init__(self):
+        if self.workdir is None:
+            self._tmp = tempfile.TemporaryDirectory(prefix="dgref_")
+            self.workdir = Path(self._tmp.name)
+        self.workdir = Path(self.workdir)
+        self.workdir.mkdir(parents=True, exist_ok=True)
+        from dg_b200.solver import write_msh  # the mesh file is an input to both codes
+        write_msh(self.workdir / "mesh.msh", self.dim, self.order, self.nx, self.ny, self.x0, self.x1,
+                  self.y0, self.y1, self.bc)
+        self.write_deck()
+
+    def write_deck(self, cfl: float | None = None, output_times=None) -> Path:
+        cfl = self.cfl if cfl is None else cfl
+        out = self.output_times if output_times is None else output_times
+        lines = ["#Code options", "#time integration", "rk4", "#output time array",
+                 " ".join(repr(float(t)) for t in out), "#final time", repr(float(out[-1])),
+                 "#Courant-Friedrichs-Lewy condition", repr(float(cfl)), "#order", str(self.order),
+                 "#mesh file", "mesh.msh", "lin" if self.dim == 1 else "qua", "#limiter", self.limiter,
+                 "#initial condition", "sodtube" if self.dim == 1 else "sodcirc"]
+        p = self.workdir / "deck.inp"
+        p.write_text("\n".join(lines) + "\n")
+        return p
+
+    def run(self, cmd: str, U: np.ndarray | None = None, dt: float = 0.0, nsteps: int = 1,
+            repeat: int = 1, timeout: float = 600.0, extra_env: dict | None = None) -> tuple[np.ndarray, str]:
+        exe = binary(self.dim, self.flux)
+        if not exe.exists():
+            raise FileNotFoundError(f"{exe} missing: run python oracle/build_ref.py")
+        args = [str(exe), "-d", "deck.inp", "--cmd", cmd, "--dt", repr(float(dt)), "--nsteps", str(nsteps),
+                "--repeat", str(repeat)]
+        if U is not None:
+            np.ascontiguousarray(U, np.float64).tofile(self.workdir / "in.bin")
+            args += ["--in", "in.bin"]
+        args += ["--out", "out.bin", "--dir", "."]
+        env = dict(os.environ, OPENBLAS_NUM_THREADS="1", OMP_NUM_THREADS="1")
+        if extra_env:
+            env.update(extra_env)
+        r = subprocess.run(args, cwd=self.workdir, capture_output=True, text=True, timeout=timeout, env=env)
+        if r.returncode != 0:
+            raise RuntimeError(f"{' '.join(args)} failed ({r.returncode}):\n{r.stdout[-2000:]}\n{r.stderr[-2000:]}")
+        out = self.workdir / "out.bin"
+        res = np.fromfile(out) if out.exists() else np.zeros(0)
+        return res, r.stdout
+
+    def dump(self) -> dict:
+        self.run("dump")
+        d = {}
+        for f in self.workdir.glob("*.bin"):
+            if f.stem in ("in", "out"):
+                continue
+            ints = f.stem in ("map", "invmap", "neighbors")
+            d[f.stem] = np.fromfile(f, np.int32 if ints else np.float64)
+        meta = {}
+        for line in (self.workdir / "meta.txt").read_text().splitlines():
+            k, v = line.split()
+            meta[k] = float(v) if "." in v or "e" in v else int(v)
+        d["meta"] = meta
+        return d
+
+    def residual(self, U):
+        return self.run("residual", U)[0]
+
+    def solve(self, U, dt):
+        return self.run("solve", U, dt=dt)[0]
+
+    def limit(self, U):
+        return self.run("limit", U)[0]
+
+    def dt_cfl(self, U, cfl):
+        self.write_deck(cfl=cfl)
+        try:
+            return float(self.run("dt", U)[0][0])
+        finally:
+            self.write_deck()
+
+    def rk4(self, U, dt, nsteps, cfl: float | None = None):
+        """nsteps reference RK4 steps; dt <= 0 takes the CFL step from a deck with CFL `cfl`."""
+        if cfl is not None:
+            self.write_deck(cfl=cfl)
+        try:
+            return self.run("rk4n", U, dt=dt, nsteps=nsteps)[0]
+        finally:
+            self.write_deck()
+
+    def rk3(self, U, dt, nsteps, cfl: float | None = None):
+        if cfl is not None:
+            self.write_deck(cfl=cfl)
+        try:
+            return self.run("rk3", U, dt=dt, nsteps=nsteps)[0]
+        finally:
+            self.write_deck()
+
+    def rk4_loop(self, U, dt, nsteps) -> tuple[np.ndarray, float]:
+        """The reference time loop itself (RK::RK_integration) over output times k*dt; returns the
+        state and the loop's wall time (s)."""
+        times = [k * dt for k in range(nsteps + 1)]
+        self.write_deck(cfl=-1.0, output_times=times)
+        try:
+            out, log = self.run("rk4", U)
+        finally:
+            self.write_deck()
+        wall = float(log.split("DGREF_WALL_S")[1].split()[0])
+        return out, wall

@@ -1,0 +1,47 @@
+import json
+import sys
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+ROOT = Path(__file__).resolve().parents[1]
+if str(ROOT) not in sys.path:
+    sys.path.insert(0, str(ROOT))
+
+GOLDEN = Path(__file__).resolve().parent / "golden"
+
+
+def pytest_configure(config):
+    config.addinivalue_line("markers", "gpu: needs a B200 (sm_100a) GPU")
+
+
+def golden_cases():
+    return sorted(p.stem for p in GOLDEN.glob("*.npz"))
+
+
+def load_golden(name: str):
+    d = dict(np.load(GOLDEN / f"{name}.npz"))
+    meta = json.loads(str(d.pop("meta")))
+    return meta, d
+
+
+def problem_for(meta, **over):
+    import dg_b200 as dgb
+    x0, x1, y0, y1 = meta["dom"]
+    kw = dict(flux=meta["flux"], limiter=meta["limiter"], cfl=meta["cfl"])
+    kw.update(over)
+    return dgb.Problem.structured(meta["dim"], meta["order"], meta["nx"], meta["ny"], x0, x1, y0, y1,
+                                  tuple(meta["bc"]), **kw)
+
+
+def rel_err(a, b):
+    a = np.asarray(a)
+    b = np.asarray(b)
+    return float(np.abs(a - b).max() / max(np.abs(b).max(), 1e-300))
+
+
+@pytest.fixture(scope="session")
+def have_gpu():
+    import torch
+    return torch.cuda.is_available()

@@ -1,0 +1,117 @@
+"""Generates the golden fixtures in tests/golden/*.npz from the reference CPU build.
+
+Each case is a small structured mesh (written with the package's Gmsh writer, read by the
+reference's own reader) and a seeded state Uraw; U0 is Uraw after the reference limiter (or Uraw
+when the case has no limiter).  The reference binaries of oracle/build_ref.py
+(compiled from the reference sources) compute, on that state:
+    f      DG_SOLVER::dg_solver                 (code/src/dg/dg_solver.h:292)
+    DU     dt * Minv * f                        (Lsolver, code/src/time_integration/rk_kernels.cu:182)
+    Ulim   the deck's limiter on the raw state Uraw (Limiting::M2limiting / HRlimiting, limiting.cc)
+    dt     RK::DtFromCFL at CFL `cfl`           (code/src/time_integration/rk.cc:250)
+    rk4    `nsteps` reference RK4 steps, step `dt_fixed`      (rk.cc:155-209)
+    rk3    `nsteps` SSP-RK3 steps of reference operators, step `dt_fixed`
+    rk3c   `nsteps` SSP-RK3 steps with the CFL step
+plus the reference's setup arrays (phi, ..., Minv, neighbours) for the host-setup pins.
+
+Run from the repository root after `python oracle/build_ref.py` and `python -m dg_b200.build`:
+    python tests/golden/make_golden.py
+"""
+from __future__ import annotations
+
+import json
+import sys
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parents[2]
+sys.path.insert(0, str(ROOT))
+
+from oracle.ref_run import RefCase  # noqa: E402
+import dg_b200 as dgb  # noqa: E402
+
+OUT = Path(__file__).resolve().parent
+
+CASES = [
+    # name, dim, order, nx, ny, domain, bc, flux, limiter, ic, cfl, dt_fixed, nsteps
+    dict(name="d1_p2_roe_m2l", dim=1, order=2, nx=24, ny=1, dom=(0, 1, 0, 1), bc=("transmissive",) * 2,
+         flux="roe", limiter="m2l", ic="tube_noise", cfl=0.4, dt=4e-4, nsteps=5),
+    dict(name="d1_p1_rus_hrl_wall", dim=1, order=1, nx=20, ny=1, dom=(0, 1, 0, 1), bc=("reflective",) * 2,
+         flux="rusanov", limiter="hrl", ic="tube_noise", cfl=0.4, dt=5e-4, nsteps=5),
+    dict(name="d1_p3_hll_m2l_periodic", dim=1, order=3, nx=16, ny=1, dom=(0, 1, 0, 1), bc=("periodic",) * 2,
+         flux="hll", limiter="m2l", ic="tube_noise", cfl=0.3, dt=2e-4, nsteps=5),
+    dict(name="d1_p2_rus_none", dim=1, order=2, nx=18, ny=1, dom=(0, 1, 0, 1), bc=("transmissive",) * 2,
+         flux="rusanov", limiter="none", ic="tube_noise", cfl=0.4, dt=4e-4, nsteps=5),
+    dict(name="d2_p2_rus_m2l", dim=2, order=2, nx=8, ny=4, dom=(0, 2, 0, 1), bc=("transmissive",) * 4,
+         flux="rusanov", limiter="m2l", ic="shock_bubble", cfl=0.3, dt=1e-3, nsteps=4),
+    dict(name="d2_p2_roe_m2l_walls", dim=2, order=2, nx=8, ny=4, dom=(0, 2, 0, 1),
+         bc=("reflective", "transmissive", "reflective", "transmissive"),
+         flux="roe", limiter="m2l", ic="shock_bubble", cfl=0.3, dt=1e-3, nsteps=4),
+    dict(name="d2_p1_rus_hrl_periodic", dim=2, order=1, nx=6, ny=6, dom=(0, 1, 0, 1), bc=("periodic",) * 4,
+         flux="rusanov", limiter="hrl", ic="quadrants", cfl=0.3, dt=1e-3, nsteps=4),
+    dict(name="d2_p3_roe_m2l", dim=2, order=3, nx=6, ny=4, dom=(0, 2, 0, 1), bc=("transmissive",) * 4,
+         flux="roe", limiter="m2l", ic="shock_bubble", cfl=0.3, dt=5e-4, nsteps=4),
+    dict(name="d2_p2_rus_hrl_box", dim=2, order=2, nx=6, ny=6, dom=(0, 1, 0, 1), bc=("reflective",) * 4,
+         flux="rusanov", limiter="hrl", ic="quadrants", cfl=0.3, dt=1e-3, nsteps=4),
+    dict(name="d2_p2_roe_none", dim=2, order=2, nx=5, ny=3, dom=(0, 2, 0, 1), bc=("transmissive",) * 4,
+         flux="roe", limiter="none", ic="quadrants", cfl=0.3, dt=1e-3, nsteps=3),
+]
+
+
+def perturbed_state(prob: "dgb.Problem", ic: str, seed: int) -> np.ndarray:
+    """Seeded IC plus a 1% nodal perturbation of density, momentum and energy (positivity kept)."""
+    U = prob.init_state(ic, seed=seed)
+    i = prob.info
+    V = U.reshape(i.n_elem, i.n_fields, i.n_s)
+    rng = np.random.default_rng(seed + 1000)
+    nmom = i.dim
+    rho = V[:, 0, :] * (1 + 0.01 * rng.uniform(-1, 1, V[:, 0, :].shape))
+    V[:, 1:1 + nmom, :] += 0.01 * rng.uniform(-1, 1, V[:, 1:1 + nmom, :].shape) * rho[:, None, :]
+    V[:, 0, :] = rho
+    V[:, 1 + nmom, :] *= 1 + 0.01 * rng.uniform(-1, 1, V[:, 1 + nmom, :].shape)
+    return V.reshape(-1).copy()
+
+
+def make_case(c: dict, seed: int) -> dict:
+    x0, x1, y0, y1 = c["dom"]
+    bc = tuple(c["bc"]) + ("transmissive",) * (4 - len(c["bc"]))
+    ref = RefCase(c["dim"], c["order"], c["nx"], c["ny"], x0, x1, y0, y1, bc, c["flux"], c["limiter"])
+    prob = dgb.Problem.structured(c["dim"], c["order"], c["nx"], c["ny"], x0, x1, y0, y1, bc, flux=c["flux"],
+                                  limiter=c["limiter"], cfl=c["cfl"])
+    Uraw = perturbed_state(prob, c["ic"], seed)
+    out = dict(Uraw=Uraw)
+    out["Ulim"] = ref.limit(Uraw)
+    # operators and steps start from the limited state when a limiter is on (the reference limits
+    # the initial condition before integrating, rk.cc:108-114): a raw high-order interpolation of
+    # a discontinuous state can have negative pressure at quadrature points
+    U0 = out["Ulim"] if c["limiter"] != "none" else Uraw
+    out["U0"] = U0
+    out["f"] = ref.residual(U0)
+    out["DU"] = ref.solve(U0, c["dt"])
+    out["dt_cfl"] = np.array([ref.dt_cfl(U0, c["cfl"])])
+    out["rk4"] = ref.rk4(U0, c["dt"], c["nsteps"])
+    out["rk3"] = ref.rk3(U0, c["dt"], c["nsteps"])
+    out["rk3c"] = ref.rk3(U0, 0.0, c["nsteps"], cfl=c["cfl"])
+    dump = ref.dump()
+    for k in ("phi", "dphi", "phi_w", "dphi_w", "psi", "psi_w", "weight", "J", "invJac", "JF", "normals",
+              "Minv", "map", "invmap", "neighbors", "Lag2Mono", "Mono2Lag", "Lag2MonoX", "MonoX2MonoY",
+              "MonoY2Lag", "MonoX2Lag", "Lag2MonoY"):
+        if k in dump:
+            out["ref_" + k] = dump[k]
+    for k, v in out.items():
+        if not np.all(np.isfinite(v)):
+            raise RuntimeError(f"{c['name']}: reference output {k} is not finite")
+    out["meta"] = np.array(json.dumps({**c, "bc": list(bc), "seed": seed, "ref_meta": dump["meta"]}))
+    return out
+
+
+def main() -> int:
+    for k, c in enumerate(CASES):
+        data = make_case(c, seed=100 + k)
+        np.savez_compressed(OUT / f"{c['name']}.npz", **data)
+        print(f"wrote {c['name']}.npz")
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,82 @@
+"""Host setup (C++, no GPU) against the reference's own arrays dumped by the oracle harness.
+
+The reference builds these in code/src/main.cc:273-860 (basis, quadrature, Jacobians, inverse
+mass matrices, maps, neighbours, limiter transforms).  Integer arrays must match exactly;
+floating-point arrays to 1e-13 relative (the reference inverts with LAPACK, this code with its
+own LU).
+"""
+import numpy as np
+import pytest
+
+from conftest import golden_cases, load_golden, problem_for
+
+INT_ARRAYS = ("map", "invmap", "neighbors")
+FLOAT_ARRAYS = ("phi", "dphi", "phi_w", "dphi_w", "psi", "psi_w", "weight", "J", "invJac", "JF", "normals",
+                "Minv", "Lag2Mono", "Mono2Lag", "Lag2MonoX", "MonoX2MonoY", "MonoY2Lag", "MonoX2Lag", "Lag2MonoY")
+
+
+@pytest.mark.parametrize("name", golden_cases())
+def test_setup_arrays_match_reference(name):
+    meta, d = load_golden(name)
+    prob = problem_for(meta)
+    checked = 0
+    for k in INT_ARRAYS + FLOAT_ARRAYS:
+        if "ref_" + k not in d:
+            continue
+        ref = d["ref_" + k]
+        if k not in INT_ARRAYS and not np.any(ref):
+            continue  # allocated but never filled by the reference for this limiter
+        if k in ("MonoX2Lag", "Lag2MonoY") and meta["limiter"] not in ("m2l", "hri", "m2i", "pri"):
+            continue  # the 2D Limiting constructor forms these only for those methods (limiting.h:318-319)
+        mine = prob.array(k)
+        assert mine.shape == ref.shape, k
+        if k in INT_ARRAYS:
+            assert np.array_equal(mine, ref), k
+        else:
+            scale = max(np.abs(ref).max(), 1e-300)
+            assert np.abs(mine - ref).max() <= 1e-13 * scale, (k, np.abs(mine - ref).max() / scale)
+        checked += 1
+    assert checked >= 12
+
+
+@pytest.mark.parametrize("name", golden_cases())
+def test_sizes_match_reference(name):
+    meta, _ = load_golden(name)
+    rm = meta["ref_meta"]
+    i = problem_for(meta).info
+    assert (i.n_elem, i.n_s, i.n_g, i.n_ifaces, i.m_s, i.m_g, i.n_n) == \
+        (rm["N_E"], rm["N_s"], rm["N_G"], rm["M_T"], rm["M_s"], rm["M_G"], rm["N_N"])
+    assert i.limiter == rm["limiter"]
+    if meta["dim"] == 2:  # the 1D Limiting constructor leaves its cartesian flag unset
+        assert i.cartesian == rm["cartesian"]
+    # the fixtures' decks carry CFL = -1: cfl_scaled = CFL * Dx / (2p+1) (main.cc:896-897)
+    assert abs(i.cfl_scaled / meta["cfl"] - rm["cfl_scaled"] / -1.0) <= 1e-15 * abs(rm["cfl_scaled"])
+
+
+def test_msh_roundtrip_equals_in_memory_mesh(tmp_path):
+    import dg_b200 as dgb
+    dgb.write_msh(tmp_path / "mesh.msh", 2, 2, 6, 3, 0.0, 2.0, 0.0, 1.0,
+                  ("reflective", "transmissive", "reflective", "transmissive"))
+    (tmp_path / "deck.inp").write_text(
+        "#Make options\nFLUX=RUS\n#Code options\n#time integration\nrk4\n#output time array\n0 0.1\n"
+        "#final time\n0.1\n#Courant-Friedrichs-Lewy condition\n0.3\n#order\n2\n#mesh file\nmesh.msh\nqua\n"
+        "#limiter\nm2l\n#initial condition\nsodcirc\n")
+    a = dgb.Problem.from_deck(tmp_path / "deck.inp")
+    b = dgb.Problem.structured(2, 2, 6, 3, 0.0, 2.0, 0.0, 1.0,
+                               ("reflective", "transmissive", "reflective", "transmissive"),
+                               flux="rusanov", limiter="m2l", cfl=0.3)
+    assert a.info.flux == 0 and a.info.limiter == 2 and a.info.n_output_times == 2
+    for k in ("map", "invmap", "neighbors", "normals", "Minv", "J", "JF", "xyz_nodes"):
+        assert np.array_equal(a.array(k), b.array(k)), k
+
+
+def test_pos_roundtrip(tmp_path):
+    import dg_b200 as dgb
+    p = dgb.Problem.structured(2, 2, 4, 3, flux="rusanov", limiter="m2l")
+    U = p.init_state("quadrants", seed=5)
+    p.write_pos(U, 3, 0.125, tmp_path)
+    assert sorted(f.name for f in tmp_path.iterdir()) == \
+        ["g0000000003.pos", "p0000000003.pos", "rho0000000003.pos", "ux0000000003.pos", "uy0000000003.pos"]
+    V, t = p.read_pos(3, tmp_path)
+    assert t == 0.125
+    assert np.abs(U - V).max() <= 1e-14 * np.abs(U).max()
