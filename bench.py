@@ -1,0 +1,332 @@
+"""Benchmark of the DG residual / time-step path: DOF*RK-stages per second.
+
+Workload (one GPU): 2D shock-bubble on [0,2]x[0,1], 512x256 structured quads, p = 2 (9 nodal DOF per
+field, 5 fields), Rusanov flux, m2 limiter, SSP-RK3 with the CFL step (CFL 0.3), plain FP64.
+Synthetic seeded initial state (Mach-1.5 shock hitting a gamma=1.67 bubble; no dataset involved).
+A "step" is one SSP-RK3 step = 3 stages (residual + stage update + limiter each) plus the
+device-side CFL step.  DOF = N_E * N_s * N_F = 5,898,240.
+
+  value      whole-job DOF*stages/s with the state resident in HBM, device time (CUDA events on the
+             library stream) summed over exactly K steps; L2 is flushed before every timed step
+  e2e        the same metric through the C ABI with host buffers: every step copies the state from
+             pinned host memory (dgb_set_state), advances one step (dgb_advance) and reads the state
+             back (dgb_get_state); wall clock
+  roofline   the fused residual kernel: algorithmic HBM bytes per launch (21.33 B per DOF and stage
+             on average for SSP-RK3) / its average device time from a profiled pass of the same steps
+  cpu_baseline  the reference CPU build (oracle/_ref, compiled from the reference sources) on a
+             bounded sample of the same workload, one process on one core
+
+--impl reference runs the reference CPU implementation (oracle/_ref) on the host cores: one process
+per core, each advancing its own copy of the workload; a bench step there is one SSP-RK3 stage
+(a bounded sample: a full step of this workload takes seconds on one core).
+
+Multi-GPU (torchrun): every rank advances its own replica of the workload (weak scaling, no data-path
+collective); the timed region is bracketed by barriers and the max over ranks is taken.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "DOF·RK-stages/sec: plain FP64 vs mixed+learned-limiter form at equal L1 error"
+UNIT = "DOF*stages/s"
+NX, NY, ORDER = 512, 256, 2
+DOMAIN = (0.0, 2.0, 0.0, 1.0)
+BC = ("reflective", "transmissive", "reflective", "transmissive")  # bottom, right, top, left
+CFL = 0.3
+SEED = 7
+STAGES_PER_STEP = 3
+BYTES_PER_DOF_STAGE = (16.0 + 24.0 + 24.0) / 3.0  # SSP-RK3 Shu-Osher, fully fused stages
+
+
+def config(extra=None):
+    c = {"workload": "2D shock-bubble 512x256 quads, p=2, Rusanov, m2l limiter, SSP-RK3, CFL 0.3",
+         "form": "plain FP64", "n_elem": NX * NY, "order": ORDER, "dof": NX * NY * (ORDER + 1) ** 2 * 5,
+         "scheme": "SSP-RK3 (3 stages/step)", "l2": "flushed (256 MiB write) before every timed step",
+         "parallelism": "replicas"}
+    if extra:
+        c.update(extra)
+    return c
+
+
+def dist_env():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return ws, rank, local
+
+
+class Clocks:
+    """nvidia-smi samples of SM clock and throttle reasons during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.proc = None
+        self.tmp = None
+
+    def __enter__(self):
+        try:
+            self.tmp = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=self.tmp, stderr=subprocess.DEVNULL)
+        except (FileNotFoundError, OSError):
+            self.proc = None
+        return self
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            time.sleep(0.25)
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        if self.proc is None or self.tmp is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.tmp.flush()
+        rows = []
+        for line in Path(self.tmp.name).read_text().splitlines():
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) >= 9:
+                rows.append(parts)
+        os.unlink(self.tmp.name)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        smax = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[k] for r in rows for k in range(4) if r[5 + k].lower() == "active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(smax) if smax else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+def build_problem(nx=NX, ny=NY):
+    import dg_b200 as dgb
+    x0, x1, y0, y1 = DOMAIN
+    prob = dgb.Problem.structured(2, ORDER, nx, ny, x0, x1, y0, y1, BC, flux="rusanov", limiter="m2l", cfl=CFL)
+    U0 = prob.init_state("shock_bubble", seed=SEED)
+    return prob, U0
+
+
+def cpu_baseline(U0_limited: np.ndarray, steps: int = 2):
+    """Reference CPU build, one process on one core, `steps` SSP-RK3 steps of the workload."""
+    from oracle.ref_run import RefCase, available
+    if not available(2, "rusanov"):
+        return {"value": None, "unit": UNIT, "cores": 0, "kind": "reference",
+                "sample": "oracle/_ref binaries not built on this host"}
+    x0, x1, y0, y1 = DOMAIN
+    case = RefCase(2, ORDER, NX, NY, x0, x1, y0, y1, BC, "rusanov", "m2l")
+    case.write_deck(cfl=CFL)
+    out, log = case.run("rk3", U0_limited, dt=0.0, nsteps=steps, timeout=1800)
+    wall = float(log.split("DGREF_WALL_S")[1].split()[0])
+    dof = NX * NY * (ORDER + 1) ** 2 * 5
+    return {"value": dof * STAGES_PER_STEP * steps / wall, "unit": UNIT, "cores": 1, "kind": "reference",
+            "sample": f"{steps} SSP-RK3 steps ({steps * STAGES_PER_STEP} stages) of the full 512x256 workload, "
+                      f"reference residual/Lsolver/m2l limiter/DtFromCFL, 1 process, {wall:.2f} s"}
+
+
+def run_reference(args):
+    """--impl reference: the reference CPU implementation on all host cores (one process per core)."""
+    ws, rank, _ = dist_env()
+    if rank != 0:
+        return 0
+    from oracle.ref_run import RefCase, available
+    if not available(2, "rusanov"):
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref reference binaries are not built"}))
+        return 0
+    import dg_b200 as dgb  # host-only use: mesh file writer and the seeded initial state
+    prob, U0 = build_problem()
+    ncores = len(os.sched_getaffinity(0)) if hasattr(os, "sched_getaffinity") else os.cpu_count()
+    x0, x1, y0, y1 = DOMAIN
+    total = args.warmup + args.steps  # bench steps; one reference bench step = one SSP-RK3 stage
+    rk_steps = (total + STAGES_PER_STEP - 1) // STAGES_PER_STEP
+    procs, cases = [], []
+    for k in range(ncores):
+        case = RefCase(2, ORDER, NX, NY, x0, x1, y0, y1, BC, "rusanov", "m2l")
+        case.write_deck(cfl=CFL)
+        np.ascontiguousarray(U0).tofile(case.workdir / "in.bin")
+        exe = str(ROOT / "oracle" / "_ref" / "dgref_2d_rus")
+        cmd = [exe, "-d", "deck.inp", "--cmd", "rk3", "--dt", "0", "--nsteps", str(rk_steps), "--in", "in.bin",
+               "--out", "out.bin"]
+        if hasattr(os, "sched_setaffinity"):
+            cpus = sorted(os.sched_getaffinity(0))
+            cmd = ["taskset", "-c", str(cpus[k % len(cpus)])] + cmd
+        env = dict(os.environ, OPENBLAS_NUM_THREADS="1", OMP_NUM_THREADS="1")
+        procs.append(subprocess.Popen(cmd, cwd=case.workdir, stdout=subprocess.PIPE, stderr=subprocess.PIPE,
+                                      text=True, env=env))
+        cases.append(case)
+    per_proc = []
+    for p in procs:
+        out, err = p.communicate(timeout=3600)
+        if p.returncode != 0:
+            print(json.dumps({"impl": "reference", "unavailable": f"reference run failed: {err[-200:]}"}))
+            return 0
+        marks = [float(l.split()[3]) for l in out.splitlines() if l.startswith("DGREF_STAGE_S")]
+        stages = [marks[0]] + [marks[i] - marks[i - 1] for i in range(1, len(marks))]
+        per_proc.append(stages)
+    timed = [max(pp[args.warmup + k] for pp in per_proc) for k in range(args.steps)]
+    t = sum(timed)
+    dof = NX * NY * (ORDER + 1) ** 2 * 5
+    value = ncores * dof * args.steps / t
+    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": 1e3 * t / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "impl": "reference", "config": config({"parallelism": f"{ncores} independent CPU processes",
+                                                   "step": "one SSP-RK3 stage per bench step"}),
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": ncores, "kind": "reference",
+                             "sample": f"each of {ncores} processes (one per core) advances its own copy of the "
+                                       f"workload; one bench step = one SSP-RK3 stage (reference residual, "
+                                       f"Lsolver, update, m2l limiter; the CFL step in stage 1); stage time = "
+                                       f"max over processes"},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line))
+    return 0
+
+
+def main(argv=None) -> int:
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=40)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--e2e-steps", type=int, default=10)
+    ap.add_argument("--nx", type=int, default=NX, help="elements in x (profiling cases; default the workload)")
+    ap.add_argument("--ny", type=int, default=NY)
+    args = ap.parse_args(argv)
+    if args.impl == "reference":
+        return run_reference(args)
+    args.warmup = max(args.warmup, 3)
+
+    import torch
+    import torch.distributed as dist
+    import dg_b200 as dgb
+
+    ws, rank, local = dist_env()
+    if ws > 1:
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=120))
+    torch.cuda.set_device(local)
+    dev = local
+
+    prob, U0 = build_problem(args.nx, args.ny)
+    solver = dgb.DGSolver(prob, device=dev)
+    U0 = solver.limit(U0)  # the reference limits the initial condition when CFL > 0 (rk.cc:108-114)
+    solver.set_state(U0)
+    dof = prob.info.n_elem * prob.info.n_s * prob.info.n_fields
+
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=f"cuda:{dev}")
+    ev_a = torch.cuda.Event(enable_timing=True)
+    ev_b = torch.cuda.Event(enable_timing=True)
+
+    for _ in range(args.warmup):
+        solver.advance(1, 0.0, scheme=dgb.SSPRK3)
+    torch.cuda.synchronize()
+    if ws > 1:
+        dist.barrier()
+    launches = 0
+    dev_ms = 0.0
+    with Clocks(dev) as clk:
+        torch.cuda.synchronize()
+        for _ in range(args.steps):
+            flush.fill_(1.0)  # evict L2 (126 MB) before the step
+            torch.cuda.synchronize()
+            solver.advance(1, 0.0, scheme=dgb.SSPRK3)
+            ms, n = solver.last_timing()  # CUDA events on the library stream around the step
+            dev_ms += ms
+            launches += n
+        torch.cuda.synchronize()
+    if ws > 1:
+        dist.barrier()
+    clocks = clk.summary()
+    t_s = dev_ms / 1e3
+    if ws > 1:
+        tt = torch.tensor([t_s], device=f"cuda:{dev}")
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        t_s = float(tt.item())
+    value = ws * dof * STAGES_PER_STEP * args.steps / t_s
+
+    # per-kernel device time (profiled pass over the same number of steps, same state evolution)
+    solver.set_profiling(True)
+    solver.advance(args.steps, 0.0, scheme=dgb.SSPRK3)
+    res_ms, res_n = solver.kernel_timing("residual")
+    lim_ms, lim_n = solver.kernel_timing("limiter")
+    dt_ms, dt_n = solver.kernel_timing("dt")
+    solver.set_profiling(False)
+    res_avg_s = res_ms / 1e3 / max(res_n, 1)
+    achieved_gbs = BYTES_PER_DOF_STAGE * dof / res_avg_s / 1e9
+    peaks = json.loads((ROOT / "MEASURED_PEAKS.json").read_text()) if (ROOT / "MEASURED_PEAKS.json").exists() else {}
+    peak = peaks.get("hbm_gbs", 6650.0)
+    traffic = None
+    tf = ROOT / "profiles" / "residual2d_p2_traffic.json"
+    if tf.exists():
+        traffic = json.loads(tf.read_text()).get("bytes_per_launch_full_size")
+
+    # end to end through the C ABI with pinned host buffers
+    n_state = prob.state_size
+    host = torch.empty(n_state, dtype=torch.float64, pin_memory=True)
+    hostv = host.numpy()
+    hostv[:] = solver.get_state()
+    t0 = time.perf_counter()
+    args.e2e_steps = max(args.e2e_steps, 1)
+    for _ in range(args.e2e_steps):
+        solver.set_state(hostv)
+        solver.advance(1, 0.0, scheme=dgb.SSPRK3)
+        hostv[:] = solver.get_state()
+    e2e_s = time.perf_counter() - t0
+    if ws > 1:
+        tt = torch.tensor([e2e_s], device=f"cuda:{dev}")
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        e2e_s = float(tt.item())
+    e2e = {"value": ws * dof * STAGES_PER_STEP * args.e2e_steps / e2e_s, "unit": UNIT,
+           "h2d_bytes_per_step": n_state * 8, "d2h_bytes_per_step": n_state * 8,
+           "steps": args.e2e_steps}
+
+    cpu = None
+    if rank == 0 and ws == 1 and not args.no_cpu_baseline and (args.nx, args.ny) == (NX, NY):
+        cpu = cpu_baseline(U0)
+
+    if rank == 0:
+        line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": dev_ms / args.steps, "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+                "config": config() if (args.nx, args.ny) == (NX, NY) else config(
+                    {"workload": f"profiling case {args.nx}x{args.ny} (not the benchmark workload)",
+                     "n_elem": args.nx * args.ny, "dof": dof}),
+                "e2e": e2e,
+                "roofline": {"bound": "hbm", "achieved": achieved_gbs, "peak": peak, "unit": "GB/s",
+                             "frac": achieved_gbs / peak, "traffic": traffic,
+                             "kernel": "residual2d_kernel<p=2,Rusanov,SSP> (fused residual + stage update)",
+                             "algorithmic_bytes_per_launch": BYTES_PER_DOF_STAGE * dof,
+                             "avg_launch_ms": res_avg_s * 1e3, "peak_source": "MEASURED_PEAKS.json hbm_gbs (measured copy)"},
+                "kernel_ms_per_step": {"residual": res_ms / args.steps, "limiter": lim_ms / args.steps,
+                                       "dt": dt_ms / args.steps},
+                "cpu_baseline": cpu, "clocks": clocks, "gpu_launches": launches}
+        print(json.dumps(line))
+    solver.close()
+    if ws > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -73,6 +73,9 @@ def build(force: bool = False, verbose: bool = False) -> Path:
         with cf.ThreadPoolExecutor(min(8, len(jobs))) as ex:
             for f in [ex.submit(_run, j, verbose) for j in jobs]:
                 f.result()
+    for stale in BUILD.glob("*.o"):
+        if stale not in objs:
+            stale.unlink()
     stamp = hashlib.sha1("".join(str(o) for o in objs).encode()).hexdigest()
     stamp_file = BUILD / "libdgb.stamp"
     if force or not LIB.exists() or not stamp_file.exists() or stamp_file.read_text() != stamp:

@@ -61,26 +61,42 @@ __device__ __forceinline__ double minmod2(double a, double b) {
   return fa < fb ? sa * fa : sa * fb;
 }
 
+// 1D tables of the limiter for order P (reference element, identical for every problem):
+//   T, Tinv   Lagrange (ascending nodes) <-> scaled Taylor monomial x^n/n! transforms
+//   imd[k][n] = int_{-1}^{1} d^k/dx^k x^n/n! dx, imdL over [-3,-1], imdR over [1,3]
+//             (integrate_monomial_derivative(_bounds), limiting_kernels.cu:1748-1775)
+//   ifact[k]  = 1/k!
+template <int P>
+struct LimTab {
+  double T[P + 1][P + 1], Tinv[P + 1][P + 1];
+  double imd[P + 1][P + 1], imdL[P + 1][P + 1], imdR[P + 1][P + 1];
+  double ifact[P + 3];
+};
+__constant__ LimTab<1> c_lim_p1;
+__constant__ LimTab<2> c_lim_p2;
+__constant__ LimTab<3> c_lim_p3;
+// by-name access (a reference to a __constant__ object can be materialised as a local copy)
+#define DGB_LIM(P, member) ((P) == 1 ? c_lim_p1.member : (P) == 2 ? c_lim_p2.member : c_lim_p3.member)
+
 // Hierarchical-reconstruction limiting of one 1D slice of scaled Taylor coefficients
 // (limit_monomial, limiting_kernels.cu:1534-1583).  N = polynomial order.
 template <int N>
-__device__ __forceinline__ void limit_monomial(const Consts& c, const double* AL, const double* AC, const double* AR,
-                                               double* Alim) {
+__device__ __forceinline__ void limit_monomial(const double* AL, const double* AC, const double* AR, double* Alim) {
   double avgLC = 0.0;
 #pragma unroll
   for (int m = N; m > 0; --m) {
     double dUL = 0, dUC = 0, dUR = 0, RL = 0, RC = 0, RR = 0;
 #pragma unroll
     for (int n = m - 1; n <= N; ++n) {
-      const double integral = c.imd[m - 1][n];
+      const double integral = DGB_LIM(N, imd[m - 1][n]);
       dUL += AL[n] * integral;
       dUC += AC[n] * integral;
       dUR += AR[n] * integral;
       if (n >= m + 1) {
         const double al = Alim[n];
-        RL += al * c.imdL[m - 1][n];
+        RL += al * DGB_LIM(N, imdL[m - 1][n]);
         RC += al * integral;
-        RR += al * c.imdR[m - 1][n];
+        RR += al * DGB_LIM(N, imdR[m - 1][n]);
       }
     }
     const double avgLL = 0.5 * (dUL - RL);
@@ -95,11 +111,16 @@ __device__ __forceinline__ void limit_monomial(const Consts& c, const double* AL
 
 // average_monomial (limiting_kernels.cu:1777-1790): keep the cell average, zero the slopes
 template <int N>
-__device__ __forceinline__ void average_monomial(const Consts& c, const double* A, double* Alim) {
+__device__ __forceinline__ void average_monomial(const double* A, double* Alim) {
   double avg = 0;
 #pragma unroll
-  for (int n = 0; n <= N; ++n) { avg += A[n] * c.imd[0][n]; Alim[n] = 0; }
+  for (int n = 0; n <= N; ++n) { avg += A[n] * DGB_LIM(N, imd[0][n]); Alim[n] = 0; }
   Alim[0] = 0.5 * avg;
 }
+
+template <int P>
+__device__ __forceinline__ double lim_T(int m, int i) { return DGB_LIM(P, T[m][i]); }
+template <int P>
+__device__ __forceinline__ double lim_Tinv(int i, int m) { return DGB_LIM(P, Tinv[i][m]); }
 
 }  // namespace dgb

@@ -345,23 +345,23 @@ __global__ void __launch_bounds__(128) residual1d_kernel(const Consts cin, const
 // ------------------------------------------------------------------------------------------
 // Limiters.  Fields are limited slice by slice in the scaled Taylor basis (T, Tinv).
 // ------------------------------------------------------------------------------------------
-template <int N1>
-__device__ __forceinline__ void to_mono(const Consts& c, const double* v, double* a) {
+template <int P>
+__device__ __forceinline__ void to_mono(const double* v, double* a) {
 #pragma unroll
-  for (int m = 0; m < N1; ++m) {
+  for (int m = 0; m <= P; ++m) {
     double s = 0;
 #pragma unroll
-    for (int i = 0; i < N1; ++i) s += c.T[m][i] * v[i];
+    for (int i = 0; i <= P; ++i) s += lim_T<P>(m, i) * v[i];
     a[m] = s;
   }
 }
-template <int N1>
-__device__ __forceinline__ void to_lag(const Consts& c, const double* a, double* v) {
+template <int P>
+__device__ __forceinline__ void to_lag(const double* a, double* v) {
 #pragma unroll
-  for (int i = 0; i < N1; ++i) {
+  for (int i = 0; i <= P; ++i) {
     double s = 0;
 #pragma unroll
-    for (int m = 0; m < N1; ++m) s += c.Tinv[i][m] * a[m];
+    for (int m = 0; m <= P; ++m) s += lim_Tinv<P>(i, m) * a[m];
     v[i] = s;
   }
 }
@@ -370,18 +370,18 @@ __device__ __forceinline__ void to_lag(const Consts& c, const double* a, double*
 // phys: 0 interior, 2/3 flatten (zero-gradient / reflective), 4 leave unchanged, 5 copy
 // (reflective wall-normal momentum under HR limiting, hrl1D limiting_kernels.cu:291-302).
 template <int P>
-__device__ __forceinline__ void limit_slice(const Consts& c, int phys, const double* vL, const double* vC,
-                                            const double* vR, double* lim) {
+__device__ __forceinline__ void limit_slice(int phys, const double* vL, const double* vC, const double* vR,
+                                            double* lim) {
   constexpr int N1 = P + 1;
   double aC[N1];
-  to_mono<N1>(c, vC, aC);
+  to_mono<P>(vC, aC);
   if (phys == 0) {
     double aL[N1], aR[N1];
-    to_mono<N1>(c, vL, aL);
-    to_mono<N1>(c, vR, aR);
-    limit_monomial<P>(c, aL, aC, aR, lim);
+    to_mono<P>(vL, aL);
+    to_mono<P>(vR, aR);
+    limit_monomial<P>(aL, aC, aR, lim);
   } else if (phys == 2 || phys == 3) {
-    average_monomial<P>(c, aC, lim);
+    average_monomial<P>(aC, lim);
   } else {
 #pragma unroll
     for (int m = 0; m < N1; ++m) lim[m] = aC[m];
@@ -391,8 +391,8 @@ __device__ __forceinline__ void limit_slice(const Consts& c, int phys, const dou
 // rho e = Leibniz product of the monomial p and alpha (internal_energy_multifluid,
 // limiting_kernels.cu:160-199), then E (reconstruct_energy, limiting_kernels.cu:111-156)
 template <int P>
-__device__ __forceinline__ void reconstruct_energy(const Consts& c, const double* plim, const double* alim,
-                                                   const double* Kmono, const double* Emono, double* Elim) {
+__device__ __forceinline__ void reconstruct_energy(const double* plim, const double* alim, const double* Kmono,
+                                                   const double* Emono, double* Elim) {
   constexpr int N1 = P + 1;
   constexpr double binom[4][4] = {{1, 0, 0, 0}, {1, 1, 0, 0}, {1, 2, 1, 0}, {1, 3, 3, 1}};
   double rhoe[N1];
@@ -407,7 +407,7 @@ __device__ __forceinline__ void reconstruct_energy(const Consts& c, const double
   for (int m = 1; m < N1; ++m) Elim[m] = rhoe[m] + Kmono[m];
   double E0 = Emono[0];
 #pragma unroll
-  for (int k = 2; k < N1; k += 2) E0 -= c.ifact[k + 1] * (Elim[k] - Emono[k]);
+  for (int k = 2; k < N1; k += 2) E0 -= DGB_LIM(P, ifact[k + 1]) * (Elim[k] - Emono[k]);
   Elim[0] = E0;
 }
 
@@ -418,20 +418,21 @@ __device__ __forceinline__ int boundary_code(int left, int right) {
   return phys;
 }
 
+struct LimArgs {
+  int ld, n_elem;
+};
+
 // 2D x pass, one thread per (element, y-slice).  METHOD 2 (m2): rho, rho u, rho v, alpha and
 // p are limited and E rebuilt; output X = [rho, rhou, rhov, alpha, p, E] (Lagrange).
 // METHOD 1 (HR): all conserved fields limited; output X = the five conserved fields.
 template <int P, int METHOD>
-__global__ void __launch_bounds__(128) lim2d_xpass_kernel(const Consts cin, const double* __restrict__ U,
+__global__ void __launch_bounds__(128) lim2d_xpass_kernel(const LimArgs la, const double* __restrict__ U,
                                                           const int* __restrict__ nbr, double* __restrict__ X,
                                                           const DevScalars* __restrict__ scal) {
   constexpr int N1 = P + 1, NS = N1 * N1;
-  __shared__ Consts c;
-  copy_consts(c, cin);
   if (scal && scal->flags) return;
-  __syncthreads();
-  const int ld = c.ld, e = blockIdx.x * blockDim.x + threadIdx.x, iy = blockIdx.y;
-  if (e >= c.n_elem) return;
+  const int ld = la.ld, e = blockIdx.x * blockDim.x + threadIdx.x, iy = blockIdx.y;
+  if (e >= la.n_elem) return;
   const int nL = __ldg(nbr + e), nR = __ldg(nbr + (size_t)ld + e);
   const int phys = boundary_code(nL, nR);
   double v[3][5][N1];  // [L,C,R][field][ix]
@@ -444,69 +445,71 @@ __global__ void __launch_bounds__(128) lim2d_xpass_kernel(const Consts cin, cons
 #pragma unroll
       for (int ix = 0; ix < N1; ++ix) v[s][f][ix] = __ldg(U + (size_t)(f * NS + ix + N1 * iy) * ld + el);
   }
-  if (METHOD == 1) {
+  if constexpr (METHOD == 1) {
 #pragma unroll
     for (int f = 0; f < 5; ++f) {
       double lim[N1], out[N1];
       const int ph = (phys == 3 && f == 1) ? 5 : phys;
-      limit_slice<P>(c, ph, v[0][f], v[1][f], v[2][f], lim);
-      to_lag<N1>(c, lim, out);
+      limit_slice<P>(ph, v[0][f], v[1][f], v[2][f], lim);
+      to_lag<P>(lim, out);
 #pragma unroll
       for (int ix = 0; ix < N1; ++ix) X[(size_t)(f * NS + ix + N1 * iy) * ld + e] = out[ix];
     }
-    return;
-  }
-  // pressure from the unlimited state (pressure kernel, physics.cu:891-958)
-  double pr[3][N1];
+  } else {
+    // pressure from the unlimited state (pressure kernel, physics.cu:891-958)
+    double pr[3][N1];
 #pragma unroll
-  for (int s = 0; s < 3; ++s) {
-    if (s != 1 && phys != 0) continue;
+    for (int s = 0; s < 3; ++s) {
+      if (s != 1 && phys != 0) continue;
+#pragma unroll
+      for (int ix = 0; ix < N1; ++ix) {
+        const double ru = v[s][1][ix], rv = v[s][2][ix], E = v[s][3][ix];
+        const double gm1 = __drcp_rn(v[s][4][ix]);
+        pr[s][ix] = gm1 * (E - 0.5 * (ru * ru + rv * rv) * __drcp_rn(v[s][0][ix]));
+      }
+    }
+    double lr[N1], lu[N1], lv[N1], la_[N1], lp[N1];
+    limit_slice<P>(phys, v[0][0], v[1][0], v[2][0], lr);
+    limit_slice<P>(phys, v[0][1], v[1][1], v[2][1], lu);
+    limit_slice<P>(phys, v[0][2], v[1][2], v[2][2], lv);
+    limit_slice<P>(phys, v[0][4], v[1][4], v[2][4], la_);
+    limit_slice<P>(phys, pr[0], pr[1], pr[2], lp);
+    double r_[N1], u_[N1], v_[N1], a_[N1], p_[N1], K[N1], Km[N1], Em[N1], El[N1], E_[N1];
+    to_lag<P>(lr, r_);
+    to_lag<P>(lu, u_);
+    to_lag<P>(lv, v_);
+    to_lag<P>(la_, a_);
+    to_lag<P>(lp, p_);
+#pragma unroll
+    for (int ix = 0; ix < N1; ++ix) K[ix] = 0.5 * (u_[ix] * u_[ix] + v_[ix] * v_[ix]) * __drcp_rn(r_[ix]);
+    to_mono<P>(K, Km);
+    to_mono<P>(v[1][3], Em);
+    reconstruct_energy<P>(lp, la_, Km, Em, El);
+    to_lag<P>(El, E_);
 #pragma unroll
     for (int ix = 0; ix < N1; ++ix) {
-      const double rho = v[s][0][ix], ru = v[s][1][ix], rv = v[s][2][ix], E = v[s][3][ix];
-      const double gamma = 1.0 + 1.0 / v[s][4][ix];
-      pr[s][ix] = (gamma - 1) * (E - 0.5 * (ru * ru + rv * rv) / rho);
+      const size_t o = (size_t)(ix + N1 * iy) * ld + e;
+      X[o + (size_t)0 * NS * ld] = r_[ix];
+      X[o + (size_t)1 * NS * ld] = u_[ix];
+      X[o + (size_t)2 * NS * ld] = v_[ix];
+      X[o + (size_t)3 * NS * ld] = a_[ix];
+      X[o + (size_t)4 * NS * ld] = p_[ix];
+      X[o + (size_t)5 * NS * ld] = E_[ix];
     }
   }
-  double lr[N1], lu[N1], lv[N1], la[N1], lp[N1];
-  limit_slice<P>(c, phys, v[0][0], v[1][0], v[2][0], lr);
-  limit_slice<P>(c, phys, v[0][1], v[1][1], v[2][1], lu);
-  limit_slice<P>(c, phys, v[0][2], v[1][2], v[2][2], lv);
-  limit_slice<P>(c, phys, v[0][4], v[1][4], v[2][4], la);
-  limit_slice<P>(c, phys, pr[0], pr[1], pr[2], lp);
-  double r_[N1], u_[N1], v_[N1], a_[N1], p_[N1], K[N1], Km[N1], Em[N1], El[N1], E_[N1];
-  to_lag<N1>(c, lr, r_);
-  to_lag<N1>(c, lu, u_);
-  to_lag<N1>(c, lv, v_);
-  to_lag<N1>(c, la, a_);
-  to_lag<N1>(c, lp, p_);
-#pragma unroll
-  for (int ix = 0; ix < N1; ++ix) K[ix] = 0.5 * (u_[ix] * u_[ix] + v_[ix] * v_[ix]) / r_[ix];
-  to_mono<N1>(c, K, Km);
-  to_mono<N1>(c, v[1][3], Em);
-  reconstruct_energy<P>(c, lp, la, Km, Em, El);
-  to_lag<N1>(c, El, E_);
-  const double* outs[6] = {r_, u_, v_, a_, p_, E_};
-#pragma unroll
-  for (int q = 0; q < 6; ++q)
-#pragma unroll
-    for (int ix = 0; ix < N1; ++ix) X[(size_t)(q * NS + ix + N1 * iy) * ld + e] = outs[q][ix];
 }
 
 // 2D y pass, one thread per (element, x-column): reads the x-pass output X of the element and
 // its bottom/top neighbours and writes the limited conserved state.
 template <int P, int METHOD>
-__global__ void __launch_bounds__(128) lim2d_ypass_kernel(const Consts cin, const double* __restrict__ X,
+__global__ void __launch_bounds__(128) lim2d_ypass_kernel(const LimArgs la, const double* __restrict__ X,
                                                           const int* __restrict__ nbr, double* __restrict__ Uout,
                                                           const DevScalars* __restrict__ scal) {
   constexpr int N1 = P + 1, NS = N1 * N1;
   constexpr int NQ = METHOD == 1 ? 5 : 6;
-  __shared__ Consts c;
-  copy_consts(c, cin);
   if (scal && scal->flags) return;
-  __syncthreads();
-  const int ld = c.ld, e = blockIdx.x * blockDim.x + threadIdx.x, ix = blockIdx.y;
-  if (e >= c.n_elem) return;
+  const int ld = la.ld, e = blockIdx.x * blockDim.x + threadIdx.x, ix = blockIdx.y;
+  if (e >= la.n_elem) return;
   const int nD = __ldg(nbr + (size_t)2 * ld + e), nU = __ldg(nbr + (size_t)3 * ld + e);
   const int phys = boundary_code(nD, nU);
   double v[3][NQ][N1];  // [D,C,U][field][iy]
@@ -519,54 +522,55 @@ __global__ void __launch_bounds__(128) lim2d_ypass_kernel(const Consts cin, cons
 #pragma unroll
       for (int iy = 0; iy < N1; ++iy) v[s][q][iy] = __ldg(X + (size_t)(q * NS + ix + N1 * iy) * ld + el);
   }
-  if (METHOD == 1) {
+  if constexpr (METHOD == 1) {
 #pragma unroll
     for (int f = 0; f < 5; ++f) {
       double lim[N1], out[N1];
       const int ph = (phys == 3 && f == 2) ? 5 : phys;
-      limit_slice<P>(c, ph, v[0][f], v[1][f], v[2][f], lim);
-      to_lag<N1>(c, lim, out);
+      limit_slice<P>(ph, v[0][f], v[1][f], v[2][f], lim);
+      to_lag<P>(lim, out);
 #pragma unroll
       for (int iy = 0; iy < N1; ++iy) Uout[(size_t)(f * NS + ix + N1 * iy) * ld + e] = out[iy];
     }
-    return;
+  } else {
+    double lr[N1], lu[N1], lv[N1], la_[N1], lp[N1];
+    limit_slice<P>(phys, v[0][0], v[1][0], v[2][0], lr);
+    limit_slice<P>(phys, v[0][1], v[1][1], v[2][1], lu);
+    limit_slice<P>(phys, v[0][2], v[1][2], v[2][2], lv);
+    limit_slice<P>(phys, v[0][3], v[1][3], v[2][3], la_);
+    limit_slice<P>(phys, v[0][4], v[1][4], v[2][4], lp);
+    double r_[N1], u_[N1], v_[N1], a_[N1], K[N1], Km[N1], Em[N1], El[N1], E_[N1];
+    to_lag<P>(lr, r_);
+    to_lag<P>(lu, u_);
+    to_lag<P>(lv, v_);
+    to_lag<P>(la_, a_);
+#pragma unroll
+    for (int iy = 0; iy < N1; ++iy) K[iy] = 0.5 * (u_[iy] * u_[iy] + v_[iy] * v_[iy]) * __drcp_rn(r_[iy]);
+    to_mono<P>(K, Km);
+    to_mono<P>(v[1][5], Em);
+    reconstruct_energy<P>(lp, la_, Km, Em, El);
+    to_lag<P>(El, E_);
+#pragma unroll
+    for (int iy = 0; iy < N1; ++iy) {
+      const size_t o = (size_t)(ix + N1 * iy) * ld + e;
+      Uout[o + (size_t)0 * NS * ld] = r_[iy];
+      Uout[o + (size_t)1 * NS * ld] = u_[iy];
+      Uout[o + (size_t)2 * NS * ld] = v_[iy];
+      Uout[o + (size_t)3 * NS * ld] = E_[iy];
+      Uout[o + (size_t)4 * NS * ld] = a_[iy];
+    }
   }
-  double lr[N1], lu[N1], lv[N1], la[N1], lp[N1];
-  limit_slice<P>(c, phys, v[0][0], v[1][0], v[2][0], lr);
-  limit_slice<P>(c, phys, v[0][1], v[1][1], v[2][1], lu);
-  limit_slice<P>(c, phys, v[0][2], v[1][2], v[2][2], lv);
-  limit_slice<P>(c, phys, v[0][3], v[1][3], v[2][3], la);
-  limit_slice<P>(c, phys, v[0][4], v[1][4], v[2][4], lp);
-  double r_[N1], u_[N1], v_[N1], a_[N1], K[N1], Km[N1], Em[N1], El[N1], E_[N1];
-  to_lag<N1>(c, lr, r_);
-  to_lag<N1>(c, lu, u_);
-  to_lag<N1>(c, lv, v_);
-  to_lag<N1>(c, la, a_);
-#pragma unroll
-  for (int iy = 0; iy < N1; ++iy) K[iy] = 0.5 * (u_[iy] * u_[iy] + v_[iy] * v_[iy]) / r_[iy];
-  to_mono<N1>(c, K, Km);
-  to_mono<N1>(c, v[1][5], Em);
-  reconstruct_energy<P>(c, lp, la, Km, Em, El);
-  to_lag<N1>(c, El, E_);
-  const double* outs[5] = {r_, u_, v_, E_, a_};
-#pragma unroll
-  for (int f = 0; f < 5; ++f)
-#pragma unroll
-    for (int iy = 0; iy < N1; ++iy) Uout[(size_t)(f * NS + ix + N1 * iy) * ld + e] = outs[f][iy];
 }
 
-// 1D HR / m2 limiter, one thread per element, in place through Uout (reads U).
+// 1D HR / m2 limiter, one thread per element (reads U, writes Uout).
 template <int P, int METHOD>
-__global__ void __launch_bounds__(128) lim1d_kernel(const Consts cin, const double* __restrict__ U,
+__global__ void __launch_bounds__(128) lim1d_kernel(const LimArgs la, const double* __restrict__ U,
                                                     const int* __restrict__ nbr, double* __restrict__ Uout,
                                                     const DevScalars* __restrict__ scal) {
   constexpr int N1 = P + 1;
-  __shared__ Consts c;
-  copy_consts(c, cin);
   if (scal && scal->flags) return;
-  __syncthreads();
-  const int ld = c.ld, e = blockIdx.x * blockDim.x + threadIdx.x;
-  if (e >= c.n_elem) return;
+  const int ld = la.ld, e = blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= la.n_elem) return;
   const int nL = __ldg(nbr + e), nR = __ldg(nbr + (size_t)ld + e);
   const int phys = boundary_code(nL, nR);
   double v[3][4][N1];
@@ -579,49 +583,51 @@ __global__ void __launch_bounds__(128) lim1d_kernel(const Consts cin, const doub
 #pragma unroll
       for (int i = 0; i < N1; ++i) v[s][f][i] = __ldg(U + (size_t)(f * N1 + i) * ld + el);
   }
-  if (METHOD == 1) {
+  if constexpr (METHOD == 1) {
 #pragma unroll
     for (int f = 0; f < 4; ++f) {
       double lim[N1], out[N1];
       const int ph = (phys == 3 && f == 1) ? 5 : phys;
-      limit_slice<P>(c, ph, v[0][f], v[1][f], v[2][f], lim);
-      to_lag<N1>(c, lim, out);
+      limit_slice<P>(ph, v[0][f], v[1][f], v[2][f], lim);
+      to_lag<P>(lim, out);
 #pragma unroll
       for (int i = 0; i < N1; ++i) Uout[(size_t)(f * N1 + i) * ld + e] = out[i];
     }
-    return;
-  }
-  double pr[3][N1];
+  } else {
+    double pr[3][N1];
 #pragma unroll
-  for (int s = 0; s < 3; ++s) {
-    if (s != 1 && phys != 0) continue;
+    for (int s = 0; s < 3; ++s) {
+      if (s != 1 && phys != 0) continue;
+#pragma unroll
+      for (int i = 0; i < N1; ++i) {
+        const double ru = v[s][1][i], E = v[s][2][i];
+        const double gm1 = __drcp_rn(v[s][3][i]);
+        pr[s][i] = gm1 * (E - 0.5 * ru * ru * __drcp_rn(v[s][0][i]));
+      }
+    }
+    double lr[N1], lu[N1], la_[N1], lp[N1];
+    limit_slice<P>(phys, v[0][0], v[1][0], v[2][0], lr);
+    limit_slice<P>(phys, v[0][1], v[1][1], v[2][1], lu);
+    limit_slice<P>(phys, v[0][3], v[1][3], v[2][3], la_);
+    limit_slice<P>(phys, pr[0], pr[1], pr[2], lp);
+    double r_[N1], u_[N1], a_[N1], K[N1], Km[N1], Em[N1], El[N1], E_[N1];
+    to_lag<P>(lr, r_);
+    to_lag<P>(lu, u_);
+    to_lag<P>(la_, a_);
+#pragma unroll
+    for (int i = 0; i < N1; ++i) K[i] = 0.5 * u_[i] * u_[i] * __drcp_rn(r_[i]);  // kinetic_energy1D
+    to_mono<P>(K, Km);
+    to_mono<P>(v[1][2], Em);
+    reconstruct_energy<P>(lp, la_, Km, Em, El);
+    to_lag<P>(El, E_);
 #pragma unroll
     for (int i = 0; i < N1; ++i) {
-      const double rho = v[s][0][i], ru = v[s][1][i], E = v[s][2][i];
-      const double gamma = 1.0 + 1.0 / v[s][3][i];
-      pr[s][i] = (gamma - 1) * (E - 0.5 * ru * ru / rho);
+      Uout[(size_t)(0 * N1 + i) * ld + e] = r_[i];
+      Uout[(size_t)(1 * N1 + i) * ld + e] = u_[i];
+      Uout[(size_t)(2 * N1 + i) * ld + e] = E_[i];
+      Uout[(size_t)(3 * N1 + i) * ld + e] = a_[i];
     }
   }
-  double lr[N1], lu[N1], la[N1], lp[N1];
-  limit_slice<P>(c, phys, v[0][0], v[1][0], v[2][0], lr);
-  limit_slice<P>(c, phys, v[0][1], v[1][1], v[2][1], lu);
-  limit_slice<P>(c, phys, v[0][3], v[1][3], v[2][3], la);
-  limit_slice<P>(c, phys, pr[0], pr[1], pr[2], lp);
-  double r_[N1], u_[N1], a_[N1], K[N1], Km[N1], Em[N1], El[N1], E_[N1];
-  to_lag<N1>(c, lr, r_);
-  to_lag<N1>(c, lu, u_);
-  to_lag<N1>(c, la, a_);
-#pragma unroll
-  for (int i = 0; i < N1; ++i) K[i] = 0.5 * u_[i] * u_[i] / r_[i];  // kinetic_energy1D
-  to_mono<N1>(c, K, Km);
-  to_mono<N1>(c, v[1][2], Em);
-  reconstruct_energy<P>(c, lp, la, Km, Em, El);
-  to_lag<N1>(c, El, E_);
-  const double* outs[4] = {r_, u_, E_, a_};
-#pragma unroll
-  for (int f = 0; f < 4; ++f)
-#pragma unroll
-    for (int i = 0; i < N1; ++i) Uout[(size_t)(f * N1 + i) * ld + e] = outs[f][i];
 }
 
 // ------------------------------------------------------------------------------------------

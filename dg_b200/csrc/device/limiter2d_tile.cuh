@@ -1,0 +1,214 @@
+// Tiled 2D limiter passes for structured row-major grids (HR and m2 methods).
+//
+// Same arithmetic as lim2d_xpass_kernel / lim2d_ypass_kernel, but every element's monomial
+// coefficients (and, for m2, its nodal pressure) are computed once per slice and shared through
+// shared memory with the neighbours that need them, instead of being recomputed by the three
+// threads that read them.
+//   x pass: CTA = 30 consecutive elements of one element row (+ left/right neighbour slots),
+//           threads (element slot, y-slice)
+//   y pass: CTA = 32 x 4 elements (+ bottom/top neighbour rows), threads (x slot, row slot),
+//           one x-column of nodes per CTA (grid z)
+// Output of the x pass (global scratch X): m2 -> [rho, rhou, rhov, alpha, p, E],
+// HR -> the five conserved fields, all x-limited and in Lagrange form (limiting.cc:271-409).
+#pragma once
+#include "kernels.cuh"
+
+namespace dgb {
+
+template <int P, int METHOD>
+__global__ void __launch_bounds__(32 * (P + 1)) lim2d_xpass_tile_kernel(const LimArgs la, int nx,
+                                                                      const double* __restrict__ U,
+                                                                      const int* __restrict__ nbr,
+                                                                      double* __restrict__ X,
+                                                                      const DevScalars* __restrict__ scal) {
+  constexpr int N1 = P + 1, NS = N1 * N1, NQ = 5, TWI = 30;
+  __shared__ double A[NQ][N1][N1][32];  // [quantity][slice][coefficient][slot]
+  if (scal && scal->flags) return;
+  const int ld = la.ld;
+  const int tx = threadIdx.x, sl = threadIdx.y;
+  const int ey = blockIdx.y, x0 = blockIdx.x * TWI;
+  const int ex = x0 - 1 + tx;
+  // element held by this slot: interior element, or the neighbour of the adjacent interior one
+  const bool interior = tx >= 1 && tx <= TWI && ex < nx;
+  int e = -1;
+  if (interior) e = ey * nx + ex;
+  else if (tx == 0) e = __ldg(nbr + (size_t)0 * ld + ey * nx + x0);
+  else if (ex - 1 < nx && ex - 1 >= 0) e = __ldg(nbr + (size_t)1 * ld + ey * nx + ex - 1);
+  double v[5][N1];
+  double Em[N1];
+  if (e >= 0) {
+#pragma unroll
+    for (int f = 0; f < 5; ++f)
+#pragma unroll
+      for (int ix = 0; ix < N1; ++ix) v[f][ix] = __ldg(U + (size_t)(f * NS + ix + N1 * sl) * ld + e);
+    double q[NQ][N1];
+#pragma unroll
+    for (int ix = 0; ix < N1; ++ix) {
+      if constexpr (METHOD == 1) {
+#pragma unroll
+        for (int f = 0; f < 5; ++f) q[f][ix] = v[f][ix];
+      } else {
+        q[0][ix] = v[0][ix];
+        q[1][ix] = v[1][ix];
+        q[2][ix] = v[2][ix];
+        q[3][ix] = v[4][ix];
+        // pressure from the unlimited state (pressure kernel, physics.cu:891-958)
+        const double ru = v[1][ix], rv = v[2][ix];
+        q[4][ix] = (1.0 / v[4][ix]) * (v[3][ix] - 0.5 * (ru * ru + rv * rv) / v[0][ix]);
+      }
+    }
+#pragma unroll
+    for (int k = 0; k < NQ; ++k) {
+      double a[N1];
+      to_mono<P>(q[k], a);
+#pragma unroll
+      for (int m = 0; m < N1; ++m) A[k][sl][m][tx] = a[m];
+    }
+    if constexpr (METHOD == 2) to_mono<P>(v[3], Em);
+  }
+  __syncthreads();
+  if (!interior) return;
+  const int phys = boundary_code(__ldg(nbr + (size_t)0 * ld + e), __ldg(nbr + (size_t)1 * ld + e));
+  double lim[NQ][N1];
+#pragma unroll
+  for (int k = 0; k < NQ; ++k) {
+    double aL[N1], aC[N1], aR[N1];
+#pragma unroll
+    for (int m = 0; m < N1; ++m) aC[m] = A[k][sl][m][tx];
+    const int ph = (METHOD == 1 && phys == 3 && k == 1) ? 5 : phys;
+    if (ph == 0) {
+#pragma unroll
+      for (int m = 0; m < N1; ++m) { aL[m] = A[k][sl][m][tx - 1]; aR[m] = A[k][sl][m][tx + 1]; }
+      limit_monomial<P>(aL, aC, aR, lim[k]);
+    } else if (ph == 2 || ph == 3) {
+      average_monomial<P>(aC, lim[k]);
+    } else {
+#pragma unroll
+      for (int m = 0; m < N1; ++m) lim[k][m] = aC[m];
+    }
+  }
+  if constexpr (METHOD == 1) {
+#pragma unroll
+    for (int k = 0; k < NQ; ++k) {
+      double out[N1];
+      to_lag<P>(lim[k], out);
+#pragma unroll
+      for (int ix = 0; ix < N1; ++ix) X[(size_t)(k * NS + ix + N1 * sl) * ld + e] = out[ix];
+    }
+  } else {
+    double r_[N1], u_[N1], v_[N1], a_[N1], p_[N1], K[N1], Km[N1], El[N1], E_[N1];
+    to_lag<P>(lim[0], r_);
+    to_lag<P>(lim[1], u_);
+    to_lag<P>(lim[2], v_);
+    to_lag<P>(lim[3], a_);
+    to_lag<P>(lim[4], p_);
+#pragma unroll
+    for (int ix = 0; ix < N1; ++ix) K[ix] = 0.5 * (u_[ix] * u_[ix] + v_[ix] * v_[ix]) / r_[ix];
+    to_mono<P>(K, Km);
+    reconstruct_energy<P>(lim[4], lim[3], Km, Em, El);
+    to_lag<P>(El, E_);
+#pragma unroll
+    for (int ix = 0; ix < N1; ++ix) {
+      const size_t o = (size_t)(ix + N1 * sl) * ld + e;
+      X[o + (size_t)0 * NS * ld] = r_[ix];
+      X[o + (size_t)1 * NS * ld] = u_[ix];
+      X[o + (size_t)2 * NS * ld] = v_[ix];
+      X[o + (size_t)3 * NS * ld] = a_[ix];
+      X[o + (size_t)4 * NS * ld] = p_[ix];
+      X[o + (size_t)5 * NS * ld] = E_[ix];
+    }
+  }
+}
+
+template <int P, int METHOD>
+__global__ void __launch_bounds__(32 * 6) lim2d_ypass_tile_kernel(const LimArgs la, int nx, int ny,
+                                                                  const double* __restrict__ X,
+                                                                  const int* __restrict__ nbr,
+                                                                  double* __restrict__ Uout,
+                                                                  const DevScalars* __restrict__ scal) {
+  constexpr int N1 = P + 1, NS = N1 * N1, NQ = 5, THI = 4;
+  __shared__ double B[NQ][N1][THI + 2][32];  // [quantity][coefficient][row slot][x slot]
+  if (scal && scal->flags) return;
+  const int ld = la.ld;
+  const int tx = threadIdx.x, ty = threadIdx.y, ix = blockIdx.z;
+  const int x = blockIdx.x * 32 + tx;
+  const int y0 = blockIdx.y * THI;
+  const int yy = y0 - 1 + ty;
+  const bool interior = ty >= 1 && ty <= THI && yy < ny && x < nx;
+  int e = -1;
+  if (x < nx) {
+    if (interior) e = yy * nx + x;
+    else if (ty == 0) e = __ldg(nbr + (size_t)2 * ld + y0 * nx + x);
+    else if (yy - 1 < ny && yy - 1 >= 0) e = __ldg(nbr + (size_t)3 * ld + (yy - 1) * nx + x);
+  }
+  double Em[N1];
+  if (e >= 0) {
+#pragma unroll
+    for (int k = 0; k < NQ; ++k) {
+      double col[N1], a[N1];
+#pragma unroll
+      for (int iy = 0; iy < N1; ++iy) col[iy] = __ldg(X + (size_t)(k * NS + ix + N1 * iy) * ld + e);
+      to_mono<P>(col, a);
+#pragma unroll
+      for (int m = 0; m < N1; ++m) B[k][m][ty][tx] = a[m];
+    }
+    if constexpr (METHOD == 2) {
+      double col[N1];
+#pragma unroll
+      for (int iy = 0; iy < N1; ++iy) col[iy] = __ldg(X + (size_t)(5 * NS + ix + N1 * iy) * ld + e);
+      to_mono<P>(col, Em);
+    }
+  }
+  __syncthreads();
+  if (!interior) return;
+  const int phys = boundary_code(__ldg(nbr + (size_t)2 * ld + e), __ldg(nbr + (size_t)3 * ld + e));
+  double lim[NQ][N1];
+#pragma unroll
+  for (int k = 0; k < NQ; ++k) {
+    double aD[N1], aC[N1], aU[N1];
+#pragma unroll
+    for (int m = 0; m < N1; ++m) aC[m] = B[k][m][ty][tx];
+    const int ph = (METHOD == 1 && phys == 3 && k == 2) ? 5 : phys;
+    if (ph == 0) {
+#pragma unroll
+      for (int m = 0; m < N1; ++m) { aD[m] = B[k][m][ty - 1][tx]; aU[m] = B[k][m][ty + 1][tx]; }
+      limit_monomial<P>(aD, aC, aU, lim[k]);
+    } else if (ph == 2 || ph == 3) {
+      average_monomial<P>(aC, lim[k]);
+    } else {
+#pragma unroll
+      for (int m = 0; m < N1; ++m) lim[k][m] = aC[m];
+    }
+  }
+  if constexpr (METHOD == 1) {
+#pragma unroll
+    for (int k = 0; k < NQ; ++k) {
+      double out[N1];
+      to_lag<P>(lim[k], out);
+#pragma unroll
+      for (int iy = 0; iy < N1; ++iy) Uout[(size_t)(k * NS + ix + N1 * iy) * ld + e] = out[iy];
+    }
+  } else {
+    double r_[N1], u_[N1], v_[N1], a_[N1], K[N1], Km[N1], El[N1], E_[N1];
+    to_lag<P>(lim[0], r_);
+    to_lag<P>(lim[1], u_);
+    to_lag<P>(lim[2], v_);
+    to_lag<P>(lim[3], a_);
+#pragma unroll
+    for (int iy = 0; iy < N1; ++iy) K[iy] = 0.5 * (u_[iy] * u_[iy] + v_[iy] * v_[iy]) / r_[iy];
+    to_mono<P>(K, Km);
+    reconstruct_energy<P>(lim[4], lim[3], Km, Em, El);
+    to_lag<P>(El, E_);
+#pragma unroll
+    for (int iy = 0; iy < N1; ++iy) {
+      const size_t o = (size_t)(ix + N1 * iy) * ld + e;
+      Uout[o + (size_t)0 * NS * ld] = r_[iy];
+      Uout[o + (size_t)1 * NS * ld] = u_[iy];
+      Uout[o + (size_t)2 * NS * ld] = v_[iy];
+      Uout[o + (size_t)3 * NS * ld] = E_[iy];
+      Uout[o + (size_t)4 * NS * ld] = a_[iy];
+    }
+  }
+}
+
+}  // namespace dgb

@@ -181,3 +181,78 @@ __device__ __forceinline__ double wave_speed2d(double rho, double rhou, double r
 
 }  // namespace phys
 }  // namespace dgb
+
+namespace dgb {
+namespace phys {
+
+// The same 2D interface fluxes evaluated with one reciprocal per state instead of repeated
+// divisions (x/rho -> x * (1/rho), gamma-1 = 1/alpha).  Agrees with riemann2d to a few ulp,
+// far inside the 1e-12 parity bound; used by the tiled kernel.
+template <int FLUX>
+__device__ __forceinline__ void riemann2d_rcp(const double* L, const double* R, double nx, double ny, double F[5],
+                                              double& nc) {
+  const double rhoL = L[0], rhoR = R[0];
+  const double irL = __drcp_rn(rhoL), irR = __drcp_rn(rhoR);
+  const double vxL = L[1] * irL, vyL = L[2] * irL, vxR = R[1] * irR, vyR = R[2] * irR;
+  const double EtL = L[3], EtR = R[3], alphaL = L[4], alphaR = R[4];
+  const double gm1L = __drcp_rn(alphaL), gm1R = __drcp_rn(alphaR);
+  const double vnL = vxL * nx + vyL * ny;
+  const double vnR = vxR * nx + vyR * ny;
+  const double pL = gm1L * (EtL - 0.5 * rhoL * (vxL * vxL + vyL * vyL));
+  const double pR = gm1R * (EtR - 0.5 * rhoR * (vxR * vxR + vyR * vyR));
+  const double aL = sqrt((1.0 + gm1L) * pL * irL);
+  const double aR = sqrt((1.0 + gm1R) * pR * irR);
+  const double HL = (EtL + pL) * irL;
+  const double HR = (EtR + pR) * irR;
+  if (FLUX == FLUX_ROE) {
+    const double tx = -ny, ty = nx;
+    const double vtL = vxL * tx + vyL * ty;
+    const double vtR = vxR * tx + vyR * ty;
+    const double iL = pL * alphaL, iR = pR * alphaR;
+    const double RT = sqrt(rhoR * irL);
+    const double rho = RT * rhoL;
+    const double i1 = __drcp_rn(1 + RT);
+    const double vx = (vxL + RT * vxR) * i1;
+    const double vy = (vyL + RT * vyR) * i1;
+    const double vn = vx * nx + vy * ny;
+    const double vt = vx * tx + vy * ty;
+    const double H = (HL + RT * HR) * i1;
+    const double alpha = (alphaL + RT * alphaR) * i1;
+    const double gm1 = __drcp_rn(alpha);
+    const double a = sqrt(gm1 * (H - 0.5 * (vx * vx + vy * vy)));
+    const double ia = __drcp_rn(a);
+    const double i = (iL + RT * iR) * i1;
+    const double p = gm1 * i;
+    const double drho = rhoR - rhoL;
+    const double dp = gm1 * gm1 * (alpha * (iR - iL) - i * (alphaR - alphaL));
+    const double dvn = vnR - vnL, dvt = vtR - vtL;
+    const double h2a = 0.5 * ia * ia;
+    const double dV0 = (dp - rho * a * dvn) * h2a;
+    const double dV1 = rho * dvt * ia;
+    const double dV2 = drho - dp * (ia * ia);
+    const double dV3 = (dp + rho * a * dvn) * h2a;
+    const double dV4 = alphaR - alphaL;
+    const double ws0 = fabs(vn - a), ws1 = fabs(vn), ws3 = fabs(vn + a);
+    const double w0 = ws0 * dV0, w1 = ws1 * dV1, w2 = ws1 * dV2, w3 = ws3 * dV3, w4 = ws1 * dV4;
+    F[0] = 0.5 * (rhoL * vnL + rhoR * vnR) - 0.5 * (w0 + w2 + w3);
+    F[1] = 0.5 * ((rhoL * vnL * vxL + pL * nx) + (rhoR * vnR * vxR + pR * nx)) -
+           0.5 * (w0 * (vx - a * nx) + w1 * (a * tx) + w2 * vx + w3 * (vx + a * nx));
+    F[2] = 0.5 * ((rhoL * vnL * vyL + pL * ny) + (rhoR * vnR * vyR + pR * ny)) -
+           0.5 * (w0 * (vy - a * ny) + w1 * (a * ty) + w2 * vy + w3 * (vy + a * ny));
+    F[3] = 0.5 * (rhoL * vnL * HL + rhoR * vnR * HR) -
+           0.5 * (w0 * (H - vn * a) + w1 * (vt * a) + w2 * (0.5 * (vx * vx + vy * vy)) + w3 * (H + vn * a) + w4 * p);
+    F[4] = -0.5 * w4;
+    nc = -0.5 * vn * (alphaR - alphaL);
+  } else {
+    const double maxvap = fmax(fabs(vnL) + aL, fabs(vnR) + aR);
+    F[0] = 0.5 * (rhoL * vnL + rhoR * vnR - maxvap * (rhoR - rhoL));
+    F[1] = 0.5 * ((rhoL * vnL * vxL + pL * nx) + (rhoR * vnR * vxR + pR * nx) - maxvap * (R[1] - L[1]));
+    F[2] = 0.5 * ((rhoL * vnL * vyL + pL * ny) + (rhoR * vnR * vyR + pR * ny) - maxvap * (R[2] - L[2]));
+    F[3] = 0.5 * (rhoL * vnL * HL + rhoR * vnR * HR - maxvap * (EtR - EtL));
+    F[4] = 0.5 * (-maxvap * (alphaR - alphaL));
+    nc = -0.5 * 0.5 * (vnL + vnR) * (alphaR - alphaL);
+  }
+}
+
+}  // namespace phys
+}  // namespace dgb

@@ -1,0 +1,392 @@
+// Tiled 2D residual + stage update for structured (row-major nx x ny) Cartesian meshes.
+//
+// One CTA owns a TW x TH tile of elements, one thread per element.
+//   phase 0  the tile's nodal state and the four neighbour face-trace strips -> shared memory
+//            (coalesced: a warp reads 32 consecutive elements of one (field, node) row)
+//   phase 1  every face of the tile exactly once: (TW+1)*TH x-faces and TW*(TH+1) y-faces,
+//            spread evenly over the threads (work item = face quadrature point); Riemann flux in
+//            the canonical orientation (left/bottom state first, +x/+y normal)
+//   phase 2  per element (thread): state from shared memory into registers, volume terms at the
+//            (p+2)^2 quadrature points with the reference-element tables read as warp-uniform
+//            __constant__ operands, face contributions from phase 1, tensor-factored inverse mass
+//            M^-1 = (1/J) M1^-1 (x) M1^-1, stage update, coalesced stores.
+// Equivalent to DG_SOLVER::dg_solver (code/src/dg/dg_solver.h:292-364) + Lsolver + the RK
+// register update, up to FP64 rounding.
+#pragma once
+#include "common.cuh"
+#include "physics.cuh"
+#include "tma.cuh"
+
+namespace dgb {
+
+// Reference-element tables of the tiled kernel (tensor node order t = ix + (p+1)*iy,
+// quadrature point g = gx*(p+2) + gy).
+template <int P>
+struct Tab2 {
+  static constexpr int N1 = P + 1, NG1 = (P == 1) ? 2 : P + 2, NS = N1 * N1, NG = NG1 * NG1;
+  double Phi[NG][NS];   // l_ix(x_gx) l_iy(x_gy)
+  double dPx[NG][NS];   // l_ix'(x_gx) l_iy(x_gy)
+  double dPy[NG][NS];   // l_ix(x_gx) l_iy'(x_gy)
+  double W[NG];         // w_gx w_gy
+  double Bf[N1][N1];    // l_j(xf_g) on the p+1 face Gauss points
+  double wf[N1];
+  double M1i[N1][N1];   // inverse of the 1D reference mass matrix (exact with p+2 Gauss points)
+  double B1[NG1][N1];   // l_i(x_g) on the p+2 volume Gauss points (1D factor)
+  double D1[NG1][N1];   // l_i'(x_g)
+  double W1[NG1];       // 1D volume weights
+};
+
+__constant__ Tab2<1> c_tab2_p1;
+__constant__ Tab2<2> c_tab2_p2;
+__constant__ Tab2<3> c_tab2_p3;
+
+// by-name access to the table of order P (a reference to a __constant__ object could be
+// materialised as a local-memory copy)
+#define DGB_TAB2(P, member) ((P) == 1 ? c_tab2_p1.member : (P) == 2 ? c_tab2_p2.member : c_tab2_p3.member)
+
+struct TileArgs {
+  const double* __restrict__ U;
+  const double* __restrict__ Ubase;
+  double* __restrict__ out;
+  double* __restrict__ Uacc;
+  const int* __restrict__ nbr;
+  const DevScalars* __restrict__ scal;
+  unsigned int* errflag;  // receives FLAG_TIMEOUT when a bounded wait runs out
+  double a, b, dt_override;
+  double invJ;           // 1 / J
+  double cx, cy;         // J * 2/hx, J * 2/hy  (volume flux metric)
+  double sx, sy;         // 2/hx, 2/hy          (gradient metric of the alpha source)
+  double J;
+  double JFx, JFy;       // face Jacobians of x-faces and y-faces
+  int nx, ny, ld;
+};
+
+template <int P, int TW, int TH>
+struct TileDims {
+  static constexpr int N1 = P + 1, NS = N1 * N1, NF = 5, NT = TW * TH;
+  static constexpr int NXF = (TW + 1) * TH * N1;  // x-face points
+  static constexpr int NYF = TW * (TH + 1) * N1;  // y-face points
+  static constexpr int NCODE = 2 * TH + 2 * TW;   // boundary codes / neighbours of the tile edges
+  static constexpr size_t head_bytes = 128;        // mbarrier + ok flag
+  static constexpr size_t code_bytes = (NCODE * 4 + 127) / 128 * 128;
+  static constexpr size_t tile_doubles = (size_t)NF * NS * NT;
+  static constexpr uint32_t tile_bytes = (uint32_t)(tile_doubles * 8);
+  static constexpr size_t halo_doubles = (size_t)2 * TH * NF * N1 + (size_t)2 * TW * NF * N1;
+  static constexpr size_t face_doubles = (size_t)6 * (NXF + NYF);
+  // the face buffer is reused for the prefetched stage base, so it is at least one tile
+  static constexpr size_t fbuf_doubles = face_doubles > tile_doubles ? face_doubles : tile_doubles;
+  // byte offsets; every region a TMA copy lands in starts on a 128-byte boundary
+  static constexpr size_t off_tile = head_bytes + code_bytes;
+  static constexpr size_t off_halo = off_tile + (tile_doubles * 8 + 127) / 128 * 128;
+  static constexpr size_t off_face = off_halo + (halo_doubles * 8 + 127) / 128 * 128;
+  static constexpr size_t smem_bytes = off_face + fbuf_doubles * 8;
+  static_assert(off_tile % 128 == 0 && off_face % 128 == 0, "TMA destinations must be 128-byte aligned");
+};
+
+enum { FLAG_TIMEOUT = 4u };
+
+template <int P, int FLUX, int MODE, int TW, int TH>
+__global__ void __launch_bounds__(TW * TH, 2)
+    residual2d_tile_kernel(const TileArgs a, const __grid_constant__ CUtensorMap mapU,
+                           const __grid_constant__ CUtensorMap mapB) {
+  using Dm = TileDims<P, TW, TH>;
+  constexpr int N1 = Dm::N1, NS = Dm::NS, NF = 5, NT = Dm::NT, NXF = Dm::NXF, NYF = Dm::NYF;
+  constexpr int NG = Tab2<P>::NG;
+  extern __shared__ __align__(128) unsigned char smraw[];
+  uint64_t* bar = reinterpret_cast<uint64_t*>(smraw);
+  int* s_ok = reinterpret_cast<int*>(smraw + 8);
+  int* codes = reinterpret_cast<int*>(smraw + Dm::head_bytes);  // [L: TH][R: TH][D: TW][U: TW]
+  double* Us = reinterpret_cast<double*>(smraw + Dm::off_tile);  // [NF*NS][NT]
+  double* HL = reinterpret_cast<double*>(smraw + Dm::off_halo);  // [TH][NF][N1] left neighbours' right-face nodes
+  double* HR = HL + TH * NF * N1;          // [TH][NF][N1]
+  double* HD = HR + TH * NF * N1;          // [TW][NF][N1]  bottom neighbours' top-face nodes
+  double* HU = HD + TW * NF * N1;          // [TW][NF][N1]
+  double* Fs = reinterpret_cast<double*>(smraw + Dm::off_face);  // [NXF + NYF][6] F[5], nc
+
+  if (a.scal && a.scal->flags) return;
+  const int tid = threadIdx.x;
+  const int tx0 = blockIdx.x * TW, ty0 = blockIdx.y * TH;
+  const int ld = a.ld, nx = a.nx;
+  constexpr bool kPrefetch = MODE != MODE_RESIDUAL;
+
+  // ---------------- phase 0: stage the tile (TMA) and the neighbour strips ----------------
+  if (tid == 0) {
+    mbar_init(bar, 1);
+    fence_mbar_init();
+  }
+  for (int k = tid; k < Dm::NCODE; k += NT) {
+    int face, eo;
+    if (k < TH) { face = 0; eo = (ty0 + k) * nx + tx0; }
+    else if (k < 2 * TH) { face = 1; eo = (ty0 + k - TH) * nx + tx0 + TW - 1; }
+    else if (k < 2 * TH + TW) { face = 2; eo = ty0 * nx + tx0 + (k - 2 * TH); }
+    else { face = 3; eo = (ty0 + TH - 1) * nx + tx0 + (k - 2 * TH - TW); }
+    codes[k] = __ldg(a.nbr + (size_t)face * ld + eo);
+  }
+  __syncthreads();
+  // a TMA copy must land on a 128-byte shared boundary and start on a 16-byte global column;
+  // otherwise record the fault and skip the copy (the wait below then reports it)
+  const bool tma_ok = (smem_u32(Us) & 127u) == 0 && (smem_u32(Fs) & 127u) == 0 && ((tx0 * 8) & 15) == 0;
+  if (tid == 0) {
+    if (tma_ok) {
+      mbar_arrive_expect_tx(bar, Dm::tile_bytes);
+      tma_load_3d(Us, &mapU, tx0, ty0, 0, bar);
+    } else {
+      atomicOr(a.errflag, (unsigned)FLAG_TIMEOUT);
+    }
+  }
+  for (int k = tid; k < 2 * TH * NF * N1; k += NT) {
+    const int side = k / (TH * NF * N1);
+    const int r = k % (TH * NF * N1);
+    const int ty = r / (NF * N1), f = (r / N1) % NF, j = r % N1;
+    const int nb = codes[side * TH + ty];
+    double v = 0.0;
+    if (nb >= 0) v = __ldg(a.U + (size_t)(f * NS + (side == 0 ? P + N1 * j : N1 * j)) * ld + nb);
+    (side == 0 ? HL : HR)[r] = v;
+  }
+  for (int k = tid; k < 2 * TW * NF * N1; k += NT) {
+    const int side = k / (TW * NF * N1);
+    const int r = k % (TW * NF * N1);
+    const int tx = r / (NF * N1), f = (r / N1) % NF, j = r % N1;
+    const int nb = codes[2 * TH + side * TW + tx];
+    double v = 0.0;
+    if (nb >= 0) v = __ldg(a.U + (size_t)(f * NS + (side == 0 ? j + N1 * P : j)) * ld + nb);
+    (side == 0 ? HD : HU)[r] = v;
+  }
+  if (tid == 0) {
+    bool ok = tma_ok && mbar_wait(bar, 0);
+    if (tma_ok && !ok) {
+      atomicOr(a.errflag, (unsigned)FLAG_TIMEOUT);
+      mbar_wait(bar, 0);
+    }
+    *s_ok = ok ? 1 : 0;
+  }
+  __syncthreads();
+  if (!*s_ok) return;
+
+  // ---------------- phase 1: face fluxes, each face of the tile once ----------------
+  for (int k = tid; k < NXF + NYF; k += NT) {
+    double L[NF], R[NF];
+    double nxv, nyv, sgn = 1.0;
+    double vl[NF][N1], vr[NF][N1];
+    int code = 0;
+    bool first_edge;
+    int mom;
+    int g;
+    if (k < NXF) {
+      // x-face fx (0..TW) of row fy; left element (fx-1, fy), right element (fx, fy)
+      g = k % N1;
+      const int fy = (k / N1) % TH, fx = k / (N1 * TH);
+      if (fx == 0) code = codes[fy];
+      if (fx == TW) code = codes[TH + fy];
+#pragma unroll
+      for (int f = 0; f < NF; ++f)
+#pragma unroll
+        for (int j = 0; j < N1; ++j) {
+          vl[f][j] = fx > 0 ? Us[(f * NS + P + N1 * j) * NT + fy * TW + fx - 1] : HL[(fy * NF + f) * N1 + j];
+          vr[f][j] = fx < TW ? Us[(f * NS + N1 * j) * NT + fy * TW + fx] : HR[(fy * NF + f) * N1 + j];
+        }
+      nxv = 1.0;
+      nyv = 0.0;
+      first_edge = fx == 0;
+      mom = 1;
+    } else {
+      const int kk = k - NXF;
+      g = kk % N1;
+      const int fx = (kk / N1) % TW, fy = kk / (N1 * TW);
+      if (fy == 0) code = codes[2 * TH + fx];
+      if (fy == TH) code = codes[2 * TH + TW + fx];
+#pragma unroll
+      for (int f = 0; f < NF; ++f)
+#pragma unroll
+        for (int j = 0; j < N1; ++j) {
+          vl[f][j] = fy > 0 ? Us[(f * NS + j + N1 * P) * NT + (fy - 1) * TW + fx] : HD[(fx * NF + f) * N1 + j];
+          vr[f][j] = fy < TH ? Us[(f * NS + j) * NT + fy * TW + fx] : HU[(fx * NF + f) * N1 + j];
+        }
+      nxv = 0.0;
+      nyv = 1.0;
+      first_edge = fy == 0;
+      mom = 2;
+    }
+    if (code < 0) {
+      // domain boundary: the inside element is L with its outward normal, the mirror state is R
+      // (reflective walls mirror the wall-normal momentum, code/src/bc/boundaries.cu:20-67)
+#pragma unroll
+      for (int f = 0; f < NF; ++f)
+#pragma unroll
+        for (int j = 0; j < N1; ++j) {
+          const double own = first_edge ? vr[f][j] : vl[f][j];
+          vl[f][j] = own;
+          vr[f][j] = (code == -3 && f == mom) ? -own : own;
+        }
+      if (first_edge) { nxv = -nxv; nyv = -nyv; sgn = -1.0; }
+    }
+#pragma unroll
+    for (int f = 0; f < NF; ++f) {
+      double sl = 0, sr = 0;
+#pragma unroll
+      for (int j = 0; j < N1; ++j) { sl += DGB_TAB2(P, Bf[g][j]) * vl[f][j]; sr += DGB_TAB2(P, Bf[g][j]) * vr[f][j]; }
+      L[f] = sl;
+      R[f] = sr;
+    }
+    double F[NF], nc;
+    phys::riemann2d_rcp<FLUX>(L, R, nxv, nyv, F, nc);
+    // boundary faces seen from the right/top element store -F so that every consumer forms
+    // (+F + nc) on its left/bottom face and (-F + nc) on its right/top face
+#pragma unroll
+    for (int f = 0; f < NF; ++f) Fs[k * 6 + f] = sgn * F[f];
+    Fs[k * 6 + 5] = nc;
+  }
+  __syncthreads();
+
+  // ---------------- phase 2: volume terms and assembly, one thread per element ----------------
+  const int tx = tid % TW, ty = tid / TW;
+  const int e = (ty0 + ty) * nx + tx0 + tx;
+  constexpr int NG1 = Tab2<P>::NG1;
+  double r[NF][NS];
+#pragma unroll
+  for (int f = 0; f < NF; ++f)
+#pragma unroll
+    for (int t = 0; t < NS; ++t) r[f][t] = 0.0;
+  // face contributions of the four faces (L: +F+nc, R: -F+nc, D: +F+nc, U: -F+nc)
+#pragma unroll
+  for (int kf = 0; kf < 4; ++kf) {
+    int base;
+    double s, jw;
+    if (kf == 0) { base = (tx * TH + ty) * N1; s = 1.0; jw = a.JFx; }
+    else if (kf == 1) { base = ((tx + 1) * TH + ty) * N1; s = -1.0; jw = a.JFx; }
+    else if (kf == 2) { base = NXF + (ty * TW + tx) * N1; s = 1.0; jw = a.JFy; }
+    else { base = NXF + ((ty + 1) * TW + tx) * N1; s = -1.0; jw = a.JFy; }
+#pragma unroll
+    for (int g = 0; g < N1; ++g) {
+      const double* fp = Fs + (base + g) * 6;
+      const double w = jw * DGB_TAB2(P, wf[g]);
+      double c[NF];
+#pragma unroll
+      for (int f = 0; f < NF; ++f) c[f] = (s * fp[f] + (f == 4 ? fp[5] : 0.0)) * w;
+#pragma unroll
+      for (int j = 0; j < N1; ++j) {
+        const int t = kf == 0 ? N1 * j : kf == 1 ? P + N1 * j : kf == 2 ? j : j + N1 * P;
+        const double b = DGB_TAB2(P, Bf[g][j]);
+#pragma unroll
+        for (int f = 0; f < NF; ++f) r[f][t] += b * c[f];
+      }
+    }
+  }
+  double* Ub = Fs;  // prefetched stage base (SSP) / accumulator (RK4), [NF*NS][NT]
+  const bool need = (MODE == MODE_SSP && a.a != 0.0) || (MODE == MODE_RK4 && a.Uacc != nullptr);
+  if (kPrefetch) {
+    // the face buffer is free once every thread has read its face fluxes
+    fence_proxy_async_smem();
+    __syncthreads();
+    if (tid == 0 && need) {
+      mbar_arrive_expect_tx(bar, Dm::tile_bytes);
+      tma_load_3d(Ub, &mapB, tx0, ty0, 0, bar);
+    }
+  }
+
+  // volume terms: collocation sum-factorised (x-contraction per quadrature column gx, then y per
+  // point), lift accumulated per point with the tensor-product derivative tables
+  const double* us = Us + tid;  // thread-private column of the tile: us[(f*NS + t)*NT]
+#pragma unroll
+  for (int gx = 0; gx < NG1; ++gx) {
+    double Tc[NF][N1], dT[N1];  // column values: sum_ix l_ix(x_gx) u(ix, iy), and of l' for alpha
+#pragma unroll
+    for (int iy = 0; iy < N1; ++iy) {
+#pragma unroll
+      for (int f = 0; f < NF; ++f) {
+        double sacc = 0;
+#pragma unroll
+        for (int ix = 0; ix < N1; ++ix) sacc += DGB_TAB2(P, B1[gx][ix]) * us[(f * NS + ix + N1 * iy) * NT];
+        Tc[f][iy] = sacc;
+      }
+      double sd = 0;
+#pragma unroll
+      for (int ix = 0; ix < N1; ++ix) sd += DGB_TAB2(P, D1[gx][ix]) * us[(4 * NS + ix + N1 * iy) * NT];
+      dT[iy] = sd;
+    }
+#pragma unroll
+    for (int gy = 0; gy < NG1; ++gy) {
+      const int g = gx * NG1 + gy;
+      double ug[NF], dax = 0, day = 0;
+#pragma unroll
+      for (int f = 0; f < NF; ++f) {
+        double sacc = 0;
+#pragma unroll
+        for (int iy = 0; iy < N1; ++iy) sacc += DGB_TAB2(P, B1[gy][iy]) * Tc[f][iy];
+        ug[f] = sacc;
+      }
+#pragma unroll
+      for (int iy = 0; iy < N1; ++iy) { dax += DGB_TAB2(P, B1[gy][iy]) * dT[iy]; day += DGB_TAB2(P, D1[gy][iy]) * Tc[4][iy]; }
+      const double rho = ug[0], irho = __drcp_rn(rho);
+      const double uu = ug[1] * irho, vv = ug[2] * irho, Et = ug[3];
+      const double gm1 = __drcp_rn(ug[4]);
+      const double p = gm1 * (Et - 0.5 * rho * (uu * uu + vv * vv));
+      const double wx = DGB_TAB2(P, W[g]) * a.cx, wy = DGB_TAB2(P, W[g]) * a.cy;
+      const double mx = ug[1] * wx, my = ug[2] * wy;
+      const double gxv[4] = {mx, mx * uu + wx * p, mx * vv, wx * ((Et + p) * uu)};
+      const double gyv[4] = {my, my * uu, my * vv + wy * p, wy * ((Et + p) * vv)};
+      const double gs = (DGB_TAB2(P, W[g]) * a.J) * (-uu * dax * a.sx - vv * day * a.sy);
+#pragma unroll
+      for (int t = 0; t < NS; ++t) {
+#pragma unroll
+        for (int f = 0; f < 4; ++f) r[f][t] += DGB_TAB2(P, dPx[g][t]) * gxv[f] + DGB_TAB2(P, dPy[g][t]) * gyv[f];
+        r[4][t] += DGB_TAB2(P, Phi[g][t]) * gs;
+      }
+    }
+  }
+  if (MODE == MODE_RESIDUAL) {
+#pragma unroll
+    for (int f = 0; f < NF; ++f)
+#pragma unroll
+      for (int t = 0; t < NS; ++t) a.out[(size_t)(f * NS + t) * ld + e] = r[f][t];
+    return;
+  }
+  if (need) {
+    if (tid == 0) {
+      bool ok = mbar_wait(bar, 1);
+      if (!ok) {
+        atomicOr(a.errflag, (unsigned)FLAG_TIMEOUT);
+        mbar_wait(bar, 1);
+      }
+      *s_ok = ok ? 1 : 0;
+    }
+    __syncthreads();
+    if (!*s_ok) return;
+  }
+  const double dt = a.dt_override > 0 ? a.dt_override : a.scal->dt;
+  const double sc = dt * a.invJ;
+#pragma unroll
+  for (int f = 0; f < NF; ++f) {
+    // DU = dt/J (M1^-1 (x) M1^-1) R : first along x then along y
+    double tmp[NS];
+#pragma unroll
+    for (int iy = 0; iy < N1; ++iy)
+#pragma unroll
+      for (int ix = 0; ix < N1; ++ix) {
+        double s = 0;
+#pragma unroll
+        for (int q = 0; q < N1; ++q) s += DGB_TAB2(P, M1i[ix][q]) * r[f][q + N1 * iy];
+        tmp[ix + N1 * iy] = s;
+      }
+#pragma unroll
+    for (int iy = 0; iy < N1; ++iy)
+#pragma unroll
+      for (int ix = 0; ix < N1; ++ix) {
+        double s = 0;
+#pragma unroll
+        for (int q = 0; q < N1; ++q) s += DGB_TAB2(P, M1i[iy][q]) * tmp[ix + N1 * q];
+        const double du = sc * s;
+        const int t = ix + N1 * iy;
+        const size_t gi = (size_t)(f * NS + t) * ld + e;
+        if (MODE == MODE_SSP) {
+          const double base = a.a != 0.0 ? a.a * Ub[(f * NS + t) * NT + tid] : 0.0;
+          a.out[gi] = base + a.b * (us[(f * NS + t) * NT] + du);
+        } else {
+          a.out[gi] = du;
+          if (a.Uacc) a.Uacc[gi] = Ub[(f * NS + t) * NT + tid] + a.b * du;
+        }
+      }
+  }
+}
+
+}  // namespace dgb

@@ -4,16 +4,21 @@
 // resident state and the stage buffers of the chosen integrator, and one CUDA stream on which
 // every kernel of the context runs.  Steps of dgb_advance are captured once into a CUDA graph
 // per (scheme, step mode) and replayed.
+#include <cuda.h>
+#include <cudaTypedefs.h>
 #include <cuda_runtime.h>
 
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <string>
 #include <vector>
 
 #include "../../include/dgb.h"
 #include "device/kernels.cuh"
+#include "device/tile2d.cuh"
+#include "device/limiter2d_tile.cuh"
 #include "host/host.h"
 
 namespace dgb {
@@ -109,12 +114,68 @@ Consts make_consts(const Problem& P, int ld) {
   return c;
 }
 
+template <int P>
+Tab2<P> make_tab2(const Consts& c) {
+  Tab2<P> T;
+  std::memset(&T, 0, sizeof(T));
+  constexpr int N1 = Tab2<P>::N1, NG1 = Tab2<P>::NG1;
+  for (int gx = 0; gx < NG1; ++gx)
+    for (int gy = 0; gy < NG1; ++gy) {
+      const int g = gx * NG1 + gy;
+      T.W[g] = c.wq[gx] * c.wq[gy];
+      for (int iy = 0; iy < N1; ++iy)
+        for (int ix = 0; ix < N1; ++ix) {
+          const int t = ix + N1 * iy;
+          T.Phi[g][t] = c.Bq[gx][ix] * c.Bq[gy][iy];
+          T.dPx[g][t] = c.Dq[gx][ix] * c.Bq[gy][iy];
+          T.dPy[g][t] = c.Bq[gx][ix] * c.Dq[gy][iy];
+        }
+    }
+  for (int g = 0; g < N1; ++g) {
+    T.wf[g] = c.wf[g];
+    for (int j = 0; j < N1; ++j) T.Bf[g][j] = c.Bf[g][j];
+  }
+  for (int g = 0; g < NG1; ++g) {
+    T.W1[g] = c.wq[g];
+    for (int i = 0; i < N1; ++i) { T.B1[g][i] = c.Bq[g][i]; T.D1[g][i] = c.Dq[g][i]; }
+  }
+  std::vector<double> M((size_t)N1 * N1, 0.0);
+  for (int i = 0; i < N1; ++i)
+    for (int j = 0; j < N1; ++j)
+      for (int g = 0; g < NG1; ++g) M[i + (size_t)j * N1] += c.wq[g] * c.Bq[g][i] * c.Bq[g][j];
+  invert(M, N1);
+  for (int i = 0; i < N1; ++i)
+    for (int j = 0; j < N1; ++j) T.M1i[i][j] = M[i + (size_t)j * N1];
+  return T;
+}
+
+// structured row-major grid test: interior neighbours are e-1, e+1, e-nx, e+nx
+bool is_row_major_grid(const Problem& P) {
+  if (P.D != 2 || P.nx <= 0 || P.ny <= 0 || (long)P.nx * P.ny != P.N_E) return false;
+  const int nx = P.nx, ne = P.N_E;
+  for (int e = 0; e < ne; ++e) {
+    const int ix = e % nx, iy = e / nx;
+    const int L = P.nbr[(size_t)0 * ne + e], R = P.nbr[(size_t)1 * ne + e];
+    const int Dn = P.nbr[(size_t)2 * ne + e], Up = P.nbr[(size_t)3 * ne + e];
+    if (ix > 0 && L != e - 1) return false;
+    if (ix < nx - 1 && R != e + 1) return false;
+    if (iy > 0 && Dn != e - nx) return false;
+    if (iy < P.ny - 1 && Up != e + nx) return false;
+  }
+  return true;
+}
+
 }  // namespace
 
 struct dgb_ctx {
   int device = 0;
   cudaStream_t st = nullptr;
   int D = 1, p = 1, nf = 4, ns = 2, ne = 0, ld = 0, flux = 2, limiter = 0;
+  int nx = 0, ny = 0;
+  bool tiled = false;     // structured row-major grid with tile-multiple extents: tiled residual kernel
+  bool rowmajor = false;  // structured row-major grid: tiled limiter passes
+  CUtensorMap mapA, mapB, mapC;  // TMA descriptors of the state buffers (tiled kernel)
+  double hx = 0, hy = 0;
   size_t nstate = 0;
   Consts cs;
   double *A = nullptr, *B = nullptr, *C = nullptr, *DU = nullptr, *X = nullptr, *ref = nullptr;
@@ -179,8 +240,74 @@ void launch_res1d(dgb_ctx* c, const StageArgs& a) {
   residual1d_kernel<P, FLUX, MODE><<<grid, 128, 0, c->st>>>(c->cs, a);
 }
 
+constexpr int TILE_W = 32, TILE_H = 4;
+
+const CUtensorMap& map_of(dgb_ctx* c, const double* p) {
+  if (p == c->B) return c->mapB;
+  if (p == c->C) return c->mapC;
+  return c->mapA;
+}
+
+template <int P, int FLUX, int MODE>
+void launch_tile2d(dgb_ctx* c, const StageArgs& s) {
+  using Dm = TileDims<P, TILE_W, TILE_H>;
+  constexpr size_t smem = Dm::smem_bytes;
+  auto k = residual2d_tile_kernel<P, FLUX, MODE, TILE_W, TILE_H>;
+  static bool attr = false;
+  if (!attr) { cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem); attr = true; }
+  TileArgs a;
+  a.U = s.U; a.Ubase = s.Ubase; a.out = s.out; a.Uacc = s.Uacc; a.nbr = s.nbr; a.scal = s.scal;
+  a.errflag = &c->scal->flags;
+  a.a = s.a; a.b = s.b; a.dt_override = s.dt_override;
+  a.J = c->cs.J;
+  a.invJ = 1.0 / c->cs.J;
+  a.cx = c->cs.J * c->cs.ixx;
+  a.cy = c->cs.J * c->cs.iyy;
+  a.sx = c->cs.ixx;
+  a.sy = c->cs.iyy;
+  a.JFx = c->cs.JFx;
+  a.JFy = c->cs.JFy;
+  a.nx = c->nx; a.ny = c->ny; a.ld = c->ld;
+  const CUtensorMap& mu = map_of(c, s.U);
+  const CUtensorMap& mb = MODE == MODE_SSP ? map_of(c, s.Ubase) : MODE == MODE_RK4 && s.Uacc ? map_of(c, s.Uacc) : mu;
+  dim3 grid(c->nx / TILE_W, c->ny / TILE_H);
+  ProfScope ps(c, KC_RESIDUAL);
+  k<<<grid, TILE_W * TILE_H, smem, c->st>>>(a, mu, mb);
+}
+
+// TMA descriptor of a state buffer viewed as (x: nx, y: ny, z: N_F*N_s rows of stride ld)
+bool encode_state_map(dgb_ctx* c, double* ptr, CUtensorMap* map) {
+  static PFN_cuTensorMapEncodeTiled_v12000 encode = nullptr;
+  if (!encode) {
+    cudaDriverEntryPointQueryResult q;
+    void* fn = nullptr;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q) != cudaSuccess ||
+        q != cudaDriverEntryPointSuccess || !fn)
+      return false;
+    encode = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(fn);
+  }
+  const cuuint64_t dims[3] = {(cuuint64_t)c->nx, (cuuint64_t)c->ny, (cuuint64_t)(c->nf * c->ns)};
+  const cuuint64_t strides[2] = {(cuuint64_t)c->nx * sizeof(double), (cuuint64_t)c->ld * sizeof(double)};
+  const cuuint32_t box[3] = {(cuuint32_t)TILE_W, (cuuint32_t)TILE_H, (cuuint32_t)(c->nf * c->ns)};
+  const cuuint32_t estr[3] = {1, 1, 1};
+  CUresult r = encode(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 3, ptr, dims, strides, box, estr,
+                      CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                      CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  return r == CUDA_SUCCESS;
+}
+
 template <int MODE>
 int residual_dispatch(dgb_ctx* c, const StageArgs& a) {
+  if (c->tiled) {
+    const int key = c->p * 10 + c->flux;
+    switch (key) {
+      case 10: launch_tile2d<1, 0, MODE>(c, a); return 0;
+      case 12: launch_tile2d<1, 2, MODE>(c, a); return 0;
+      case 20: launch_tile2d<2, 0, MODE>(c, a); return 0;
+      case 22: launch_tile2d<2, 2, MODE>(c, a); return 0;
+      default: break;
+    }
+  }
 #define R2(P, F) case P * 10 + F: launch_res2d<P, F, MODE>(c, a); return 0;
 #define R1(P, F) case P * 10 + F: launch_res1d<P, F, MODE>(c, a); return 0;
   const int key = c->p * 10 + c->flux;
@@ -202,10 +329,18 @@ int residual_dispatch(dgb_ctx* c, const StageArgs& a) {
 
 template <int P, int METHOD>
 void launch_lim2d(dgb_ctx* c, double* U) {
-  dim3 grid((c->ne + 127) / 128, P + 1);
   ProfScope ps(c, KC_LIMITER);
-  lim2d_xpass_kernel<P, METHOD><<<grid, 128, 0, c->st>>>(c->cs, U, c->nbr, c->X, c->scal);
-  lim2d_ypass_kernel<P, METHOD><<<grid, 128, 0, c->st>>>(c->cs, c->X, c->nbr, U, c->scal);
+  const LimArgs la{c->ld, c->ne};
+  if (c->rowmajor) {
+    dim3 gx((c->nx + 29) / 30, c->ny), bx(32, P + 1);
+    lim2d_xpass_tile_kernel<P, METHOD><<<gx, bx, 0, c->st>>>(la, c->nx, U, c->nbr, c->X, c->scal);
+    dim3 gy((c->nx + 31) / 32, (c->ny + 3) / 4, P + 1), by(32, 6);
+    lim2d_ypass_tile_kernel<P, METHOD><<<gy, by, 0, c->st>>>(la, c->nx, c->ny, c->X, c->nbr, U, c->scal);
+  } else {
+    dim3 grid((c->ne + 127) / 128, P + 1);
+    lim2d_xpass_kernel<P, METHOD><<<grid, 128, 0, c->st>>>(la, U, c->nbr, c->X, c->scal);
+    lim2d_ypass_kernel<P, METHOD><<<grid, 128, 0, c->st>>>(la, c->X, c->nbr, U, c->scal);
+  }
   c->counter++;
 }
 
@@ -214,7 +349,8 @@ void launch_lim1d(dgb_ctx* c, double* U) {
   const int grid = (c->ne + 127) / 128;
   {
     ProfScope ps(c, KC_LIMITER);
-    lim1d_kernel<P, METHOD><<<grid, 128, 0, c->st>>>(c->cs, U, c->nbr, c->X, c->scal);
+    const LimArgs la{c->ld, c->ne};
+    lim1d_kernel<P, METHOD><<<grid, 128, 0, c->st>>>(la, U, c->nbr, c->X, c->scal);
   }
   cudaMemcpyAsync(U, c->X, c->nstate * sizeof(double), cudaMemcpyDeviceToDevice, c->st);
 }
@@ -383,6 +519,38 @@ extern "C" int dgb_create(const dgb_problem* prob, int device, dgb_ctx** out) {
   c->flux = P.flux; c->limiter = P.limiter;
   c->nstate = (size_t)c->nf * c->ns * c->ld;
   c->cs = make_consts(P, c->ld);
+  c->nx = P.nx;
+  c->ny = P.ny;
+  c->hx = P.hx;
+  c->hy = P.hy;
+  c->rowmajor = P.D == 2 && is_row_major_grid(P) && std::getenv("DGB_NO_TILE") == nullptr;
+  c->tiled = c->rowmajor && P.p <= 2 && P.nx % TILE_W == 0 && P.ny % TILE_H == 0;
+  {
+    cudaError_t el = cudaSuccess;
+    auto fill = [&](auto& t, int n1) {
+      std::memset(&t, 0, sizeof(t));
+      for (int m = 0; m < n1; ++m)
+        for (int i = 0; i < n1; ++i) {
+          t.T[m][i] = c->cs.T[m][i];
+          t.Tinv[m][i] = c->cs.Tinv[m][i];
+          t.imd[m][i] = c->cs.imd[m][i];
+          t.imdL[m][i] = c->cs.imdL[m][i];
+          t.imdR[m][i] = c->cs.imdR[m][i];
+        }
+      for (int k = 0; k < n1 + 2; ++k) t.ifact[k] = c->cs.ifact[k];
+    };
+    if (P.p == 1) { LimTab<1> t; fill(t, 2); el = cudaMemcpyToSymbol(c_lim_p1, &t, sizeof(t)); }
+    if (P.p == 2) { LimTab<2> t; fill(t, 3); el = cudaMemcpyToSymbol(c_lim_p2, &t, sizeof(t)); }
+    if (P.p == 3) { LimTab<3> t; fill(t, 4); el = cudaMemcpyToSymbol(c_lim_p3, &t, sizeof(t)); }
+    if (el != cudaSuccess) { delete c; return set_error(DGB_ERR_CUDA, std::string("limiter tables: ") + cudaGetErrorString(el)); }
+  }
+  if (P.D == 2) {
+    cudaError_t et = cudaSuccess;
+    if (P.p == 1) { auto t = make_tab2<1>(c->cs); et = cudaMemcpyToSymbol(c_tab2_p1, &t, sizeof(t)); }
+    if (P.p == 2) { auto t = make_tab2<2>(c->cs); et = cudaMemcpyToSymbol(c_tab2_p2, &t, sizeof(t)); }
+    if (P.p == 3) { auto t = make_tab2<3>(c->cs); et = cudaMemcpyToSymbol(c_tab2_p3, &t, sizeof(t)); }
+    if (et != cudaSuccess) { delete c; return set_error(DGB_ERR_CUDA, std::string("constant tables: ") + cudaGetErrorString(et)); }
+  }
   auto fail = [&](cudaError_t e, const char* what) {
     dgb_destroy(c);
     return set_error(DGB_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
@@ -409,6 +577,12 @@ extern "C" int dgb_create(const dgb_problem* prob, int device, dgb_ctx** out) {
   if ((e = cudaMalloc(&c->scal, sizeof(DevScalars))) != cudaSuccess) return fail(e, "scalars");
   cudaMemset(c->scal, 0, sizeof(DevScalars));
   if ((e = cudaMallocHost(&c->h_scal, sizeof(DevScalars))) != cudaSuccess) return fail(e, "pinned scalars");
+  if (c->tiled) {
+    // row starts must be 16-byte aligned for TMA: nx is a multiple of TILE_W (32) and ld of 64
+    if (!(encode_state_map(c, c->A, &c->mapA) && encode_state_map(c, c->B, &c->mapB) &&
+          encode_state_map(c, c->C, &c->mapC)))
+      c->tiled = false;
+  }
   cudaEventCreate(&c->e0);
   cudaEventCreate(&c->e1);
   if ((e = cudaDeviceSynchronize()) != cudaSuccess) return fail(e, "create");
@@ -469,13 +643,16 @@ extern "C" int dgb_residual(dgb_ctx* c, const double* U, double* f) {
   if (!c || !U || !f) return set_error(DGB_ERR_ARG, "null argument");
   DGB_CUDA(cudaSetDevice(c->device));
   if (int rc = upload(c, U, c->B)) return rc;
+  if (int rc = reset_scalars(c, 0.0)) return rc;
   StageArgs a = stage_args(c);
-  a.scal = nullptr;
   a.U = c->B;
   a.out = c->C;
   if (int rc = residual_dispatch<MODE_RESIDUAL>(c, a)) return rc;
   DGB_CUDA(cudaGetLastError());
-  return download(c, c->C, f);
+  if (int rc = download(c, c->C, f)) return rc;
+  if (int rc = read_scalars(c)) return rc;
+  if (c->h_scal->flags & FLAG_TIMEOUT) return set_error(DGB_ERR_TIMEOUT, "a bounded device wait expired");
+  return DGB_OK;
 }
 
 extern "C" int dgb_solve(dgb_ctx* c, double dt, const double* U, double* DU) {
@@ -483,15 +660,18 @@ extern "C" int dgb_solve(dgb_ctx* c, double dt, const double* U, double* DU) {
   if (!(dt > 0)) return set_error(DGB_ERR_ARG, "dt must be > 0");
   DGB_CUDA(cudaSetDevice(c->device));
   if (int rc = upload(c, U, c->B)) return rc;
+  if (int rc = reset_scalars(c, 0.0)) return rc;
   StageArgs a = stage_args(c);
-  a.scal = nullptr;
   a.U = c->B;
   a.out = c->C;
   a.Uacc = nullptr;
   a.dt_override = dt;
   if (int rc = residual_dispatch<MODE_RK4>(c, a)) return rc;
   DGB_CUDA(cudaGetLastError());
-  return download(c, c->C, DU);
+  if (int rc = download(c, c->C, DU)) return rc;
+  if (int rc = read_scalars(c)) return rc;
+  if (c->h_scal->flags & FLAG_TIMEOUT) return set_error(DGB_ERR_TIMEOUT, "a bounded device wait expired");
+  return DGB_OK;
 }
 
 extern "C" int dgb_limit(dgb_ctx* c, double* U) {
@@ -562,6 +742,7 @@ extern "C" int dgb_advance(dgb_ctx* c, int scheme, int nsteps, double dt, double
   cudaEventElapsedTime(&ms, c->e0, c->e1);
   c->last_ms = ms;
   if (time) *time += c->h_scal->time;
+  if (c->h_scal->flags & FLAG_TIMEOUT) return set_error(DGB_ERR_TIMEOUT, "a bounded device wait expired");
   if (c->h_scal->flags & FLAG_NONFINITE) return set_error(DGB_ERR_NONFINITE, "time step is NaN");
   if (c->h_scal->flags & FLAG_DT_SMALL) return set_error(DGB_ERR_DT_SMALL, "next time step is too small (< 1e-14)");
   return DGB_OK;

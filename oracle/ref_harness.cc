@@ -202,6 +202,8 @@ __wrap__ZN2RK14RK_integrationEdiiiiiiiPdS0_R8LimitingbR9DG_SOLVERR12COMMUNICATOR
         blasAxpy(N_s * N_F * N_E, rk->_gamma[k], DU.data(), 1, U.data(), 1);
       }
       limit_in_place(*Lim, *comm, *sensor, *dg, U.data());
+      fprintf(stdout, "DGREF_STEP_S %d %.9f\n", s,
+              std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count());
     }
     auto t1 = std::chrono::steady_clock::now();
     fprintf(stdout, "DGREF_WALL_S %.9f\n", std::chrono::duration<double>(t1 - t0).count());
@@ -220,16 +222,25 @@ __wrap__ZN2RK14RK_integrationEdiiiiiiiPdS0_R8LimitingbR9DG_SOLVERR12COMMUNICATOR
       Lsolver(N_s, N_E, Dt, h_Minv, f.data(), DU.data());
       for (size_t k = 0; k < n; ++k) U1[k] = Un[k] + DU[k];
       limit_in_place(*Lim, *comm, *sensor, *dg, U1.data());
+      fprintf(stdout, "DGREF_STAGE_S %d 0 %.9f\n", s,
+              std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count());
       // stage 2: U2 = 3/4 Un + 1/4 (U1 + dt L(U1))
       dg->dg_solver(U1.data(), f.data());
       Lsolver(N_s, N_E, Dt, h_Minv, f.data(), DU.data());
       for (size_t k = 0; k < n; ++k) U1[k] = 0.75 * Un[k] + 0.25 * (U1[k] + DU[k]);
       limit_in_place(*Lim, *comm, *sensor, *dg, U1.data());
+      fprintf(stdout, "DGREF_STAGE_S %d 1 %.9f\n", s,
+              std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count());
       // stage 3: U = 1/3 Un + 2/3 (U2 + dt L(U2))
       dg->dg_solver(U1.data(), f.data());
       Lsolver(N_s, N_E, Dt, h_Minv, f.data(), DU.data());
       for (size_t k = 0; k < n; ++k) U[k] = (1.0 / 3.0) * Un[k] + (2.0 / 3.0) * (U1[k] + DU[k]);
       limit_in_place(*Lim, *comm, *sensor, *dg, U.data());
+      fprintf(stdout, "DGREF_STAGE_S %d 2 %.9f\n", s,
+              std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count());
+      fprintf(stdout, "DGREF_STEP_S %d %.9f\n", s,
+              std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count());
+      fflush(stdout);
     }
     auto t1 = std::chrono::steady_clock::now();
     fprintf(stdout, "DGREF_WALL_S %.9f\n", std::chrono::duration<double>(t1 - t0).count());

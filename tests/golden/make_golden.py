@@ -55,6 +55,14 @@ CASES = [
          flux="rusanov", limiter="hrl", ic="quadrants", cfl=0.3, dt=1e-3, nsteps=4),
     dict(name="d2_p2_roe_none", dim=2, order=2, nx=5, ny=3, dom=(0, 2, 0, 1), bc=("transmissive",) * 4,
          flux="roe", limiter="none", ic="quadrants", cfl=0.3, dt=1e-3, nsteps=3),
+    # grids whose extents are multiples of the 32 x 4 element tile (tiled residual kernel)
+    dict(name="t2_p2_rus_m2l_walls", dim=2, order=2, nx=32, ny=8, dom=(0, 2, 0, 1),
+         bc=("reflective", "transmissive", "reflective", "transmissive"),
+         flux="rusanov", limiter="m2l", ic="shock_bubble", cfl=0.3, dt=5e-4, nsteps=4),
+    dict(name="t2_p1_roe_hrl_periodic", dim=2, order=1, nx=64, ny=8, dom=(0, 1, 0, 1), bc=("periodic",) * 4,
+         flux="roe", limiter="hrl", ic="quadrants", cfl=0.3, dt=5e-4, nsteps=4),
+    dict(name="t2_p2_roe_m2l_box", dim=2, order=2, nx=32, ny=12, dom=(0, 1, 0, 1), bc=("reflective",) * 4,
+         flux="roe", limiter="m2l", ic="quadrants", cfl=0.3, dt=5e-4, nsteps=4),
 ]
 
 
