@@ -23,7 +23,7 @@ EXPORTS = [
     "dgb_problem_get_array", "dgb_problem_init_state", "dgb_write_pos", "dgb_read_pos", "dgb_create",
     "dgb_destroy", "dgb_set_state", "dgb_get_state", "dgb_set_state_device", "dgb_get_state_device",
     "dgb_residual", "dgb_solve", "dgb_limit", "dgb_dt_from_cfl", "dgb_advance", "dgb_last_dt",
-    "dgb_conservation", "dgb_last_timing", "dgb_set_profiling", "dgb_kernel_timing",
+    "dgb_conservation", "dgb_last_timing", "dgb_set_profiling", "dgb_kernel_timing", "dgb_limit_noalloc",
 ]
 
 
@@ -92,6 +92,7 @@ def lib() -> C.CDLL:
         "dgb_last_timing": [vp, dp, C.POINTER(C.c_longlong)],
         "dgb_set_profiling": [vp, ip],
         "dgb_kernel_timing": [vp, cp, dp, C.POINTER(C.c_longlong)],
+        "dgb_limit_noalloc": [vp, vp, vp, vp],
     }
     for name, args in sig.items():
         f = getattr(L, name)

@@ -72,9 +72,10 @@ struct LimTab {
   double imd[P + 1][P + 1], imdL[P + 1][P + 1], imdR[P + 1][P + 1];
   double ifact[P + 3];
 };
-__constant__ LimTab<1> c_lim_p1;
-__constant__ LimTab<2> c_lim_p2;
-__constant__ LimTab<3> c_lim_p3;
+// one copy per translation unit (each .cu file is its own device module)
+static __constant__ LimTab<1> c_lim_p1;
+static __constant__ LimTab<2> c_lim_p2;
+static __constant__ LimTab<3> c_lim_p3;
 // by-name access (a reference to a __constant__ object can be materialised as a local copy)
 #define DGB_LIM(P, member) ((P) == 1 ? c_lim_p1.member : (P) == 2 ? c_lim_p2.member : c_lim_p3.member)
 

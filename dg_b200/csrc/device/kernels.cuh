@@ -668,7 +668,7 @@ __global__ void __launch_bounds__(256) wavespeed_kernel(const double* __restrict
   }
 }
 
-__global__ void finish_dt_kernel(DevScalars* scal, double cfl_scaled) {
+static __global__ void finish_dt_kernel(DevScalars* scal, double cfl_scaled) {
   if (scal->flags) return;
   double dt;
   if (scal->dt_fixed > 0) dt = scal->dt_fixed;
@@ -687,7 +687,7 @@ __global__ void finish_dt_kernel(DevScalars* scal, double cfl_scaled) {
 // ------------------------------------------------------------------------------------------
 // Layout conversion (API boundary only), RK4 helpers
 // ------------------------------------------------------------------------------------------
-__global__ void ref_to_internal_kernel(const double* __restrict__ Uref, double* __restrict__ Uint,
+static __global__ void ref_to_internal_kernel(const double* __restrict__ Uref, double* __restrict__ Uint,
                                        const int* __restrict__ perm, int n_elem, int nf, int ns, int ld) {
   const size_t n = (size_t)n_elem * nf * ns;
   for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
@@ -698,7 +698,7 @@ __global__ void ref_to_internal_kernel(const double* __restrict__ Uref, double* 
     Uint[(size_t)(f * ns + t) * ld + e] = Uref[((size_t)e * nf + f) * ns + perm[t]];
   }
 }
-__global__ void internal_to_ref_kernel(const double* __restrict__ Uint, double* __restrict__ Uref,
+static __global__ void internal_to_ref_kernel(const double* __restrict__ Uint, double* __restrict__ Uref,
                                        const int* __restrict__ perm, int n_elem, int nf, int ns, int ld) {
   const size_t n = (size_t)n_elem * nf * ns;
   for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
@@ -710,7 +710,7 @@ __global__ void internal_to_ref_kernel(const double* __restrict__ Uint, double* 
   }
 }
 // y = x + beta*d over n values (Ustar = Us + beta DU, rk.cc:167-168)
-__global__ void axpy_kernel(const double* __restrict__ x, const double* __restrict__ d, double beta,
+static __global__ void axpy_kernel(const double* __restrict__ x, const double* __restrict__ d, double beta,
                             double* __restrict__ y, size_t n, const DevScalars* __restrict__ scal) {
   if (scal && scal->flags) return;
   for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)

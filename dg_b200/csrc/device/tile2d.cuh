@@ -36,9 +36,9 @@ struct Tab2 {
   double W1[NG1];       // 1D volume weights
 };
 
-__constant__ Tab2<1> c_tab2_p1;
-__constant__ Tab2<2> c_tab2_p2;
-__constant__ Tab2<3> c_tab2_p3;
+static __constant__ Tab2<1> c_tab2_p1;
+static __constant__ Tab2<2> c_tab2_p2;
+static __constant__ Tab2<3> c_tab2_p3;
 
 // by-name access to the table of order P (a reference to a __constant__ object could be
 // materialised as a local-memory copy)

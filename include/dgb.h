@@ -191,6 +191,24 @@ int dgb_last_timing(dgb_ctx* c, double* ms, long long* launches);
 int dgb_set_profiling(dgb_ctx* c, int on);
 int dgb_kernel_timing(dgb_ctx* c, const char* name, double* ms, long long* launches);
 
+/* ------------------------------------------------------------------------------------
+ * Allocation-free limiter (no counterpart in the reference)
+ * ------------------------------------------------------------------------------------
+ * For callers that cannot allocate device memory themselves -- an application that manages a
+ * fixed device-memory budget claimed at start-up, or a time loop that must not trigger
+ * cudaMalloc (and the device synchronisation it implies) -- and therefore cannot call
+ * dgb_create.  Applies the problem's limiter (hrl or m2l) to the state U_in_dev and writes the
+ * result to U_out_dev (both in the caller's device memory, reference layout, may alias), on the
+ * CUDA stream `stream` (0 = default stream) of the current device, and returns once it is done.
+ * Temporaries live in one library-owned device array of 128 MiB, which every GPU that loads
+ * this library holds until the process exits; a problem that needs more (2D: above about 166k
+ * elements at p=2, 94k at p=3) is rejected with DGB_ERR_ARG.  The first call on a device looks
+ * up that array's device address and uploads the limiter tables; make it before any stream
+ * capture.  All calls share the array and it keeps the last call's contents: two calls that
+ * overlap on the GPU (different streams or host threads) race.  Nothing in it needs to start at
+ * zero; every call writes what it reads. */
+int dgb_limit_noalloc(const dgb_problem* p, const double* U_in_dev, double* U_out_dev, void* stream);
+
 #ifdef __cplusplus
 }
 #endif
