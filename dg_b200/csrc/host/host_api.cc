@@ -178,6 +178,7 @@ static int array_op(const dgb_problem* p, const char* name, void* dst, size_t nb
   if (n == "map") return export_vec(P.map, dst, nbytes, size_out);
   if (n == "invmap") return export_vec(P.invmap, dst, nbytes, size_out);
   if (n == "neighbors") return export_vec(P.neighbors, dst, nbytes, size_out);
+  if (n == "boundaryMap") return export_vec(P.boundary_map, dst, nbytes, size_out);
   if (n == "Lag2Mono") return export_vec(P.Lag2Mono, dst, nbytes, size_out);
   if (n == "Mono2Lag") return export_vec(P.Mono2Lag, dst, nbytes, size_out);
   if (n == "Lag2MonoX") return export_vec(P.Lag2MonoX, dst, nbytes, size_out);

@@ -66,7 +66,7 @@ class Problem:
     def array(self, name: str) -> np.ndarray:
         n = C.c_size_t()
         F.check(F.lib().dgb_problem_array_size(self._h, name.encode(), C.byref(n)))
-        ints = name in ("map", "invmap", "neighbors", "tensor_perm")
+        ints = name in ("map", "invmap", "boundaryMap", "neighbors", "tensor_perm")
         a = np.zeros(n.value // (4 if ints else 8), np.int32 if ints else np.float64)
         F.check(F.lib().dgb_problem_get_array(self._h, name.encode(), a.ctypes.data_as(C.c_void_p), n.value))
         return a

@@ -124,7 +124,7 @@ int dgb_problem_info(const dgb_problem* p, dgb_info* out);
 
 /* Copies a named host array, in the reference's own layout, into dst (nbytes must match).
  * Names: "phi","dphi","phi_w","dphi_w","psi","psi_w","weight","J","invJac","JF","normals",
- * "Minv","map","invmap","neighbors","Lag2Mono","Mono2Lag","Lag2MonoX","MonoX2MonoY",
+ * "Minv","map","invmap","boundaryMap","neighbors","Lag2Mono","Mono2Lag","Lag2MonoX","MonoX2MonoY",
  * "MonoY2Lag","MonoX2Lag","Lag2MonoY","xyz_nodes","output_times". */
 int dgb_problem_array_size(const dgb_problem* p, const char* name, size_t* nbytes);
 int dgb_problem_get_array(const dgb_problem* p, const char* name, void* dst, size_t nbytes);

@@ -9,7 +9,7 @@
 // --wrap so that, instead of (or in addition to) the reference time loop, this harness
 // can run one command on a state read from a file:
 //
-//   dump      write the solver's host arrays (phi, dphi, ..., Minv, maps, neighbors,
+//   dump      write the solver's host arrays (phi, dphi, ..., Minv, maps, boundaryMap, neighbors,
 //             limiter transforms) and the reference initial condition
 //   residual  f = DG_SOLVER::dg_solver(U)            (code/src/dg/dg_solver.h:292)
 //   solve     DU = Dt Minv f                          (code/src/time_integration/rk_kernels.cu:182)
@@ -135,6 +135,7 @@ __wrap__ZN2RK14RK_integrationEdiiiiiiiPdS0_R8LimitingbR9DG_SOLVERR12COMMUNICATOR
     write_raw(d + "map.bin", dg->_map, (size_t)M_s * M_T * N_F * 2);
     write_raw(d + "invmap.bin", dg->_invmap, (size_t)M_s * dg->_N_N * N_E * N_F * 2);
     write_raw(d + "weight.bin", dg->_weight, (size_t)N_G);
+    if (dg->_M_B > 0) write_raw(d + "boundaryMap.bin", dg->_boundaryMap, (size_t)dg->_M_B);
     write_raw(d + "Minv.bin", h_Minv, (size_t)N_s * N_s * N_E);
     if (Lim->_neighbors) write_raw(d + "neighbors.bin", Lim->_neighbors, (size_t)Lim->_N_N * N_E);
     const size_t m2 = (size_t)N_s * N_s;
@@ -148,8 +149,8 @@ __wrap__ZN2RK14RK_integrationEdiiiiiiiPdS0_R8LimitingbR9DG_SOLVERR12COMMUNICATOR
     FILE* f = fopen((d + "meta.txt").c_str(), "w");
     fprintf(f, "D %d\nN_F %d\nN_E %d\nN_s %d\nN_G %d\nM_T %d\nM_s %d\nM_G %d\nN_N %d\nM_B %d\n", D, N_F, N_E, N_s,
             N_G, M_T, M_s, dg->_M_G, dg->_N_N, dg->_M_B);
-    fprintf(f, "cfl_scaled %.17g\nlimiter %d\ncartesian %d\n", (double)CFL, Lim->getLimitingMethod(),
-            (int)Lim->_cartesian);
+    fprintf(f, "cfl_scaled %.17g\nlimiter %d\ncartesian %d\nrflctive %d\n", (double)CFL, Lim->getLimitingMethod(),
+            (int)Lim->_cartesian, dg->_rflctiveIdx);
     fclose(f);
     return;
   }

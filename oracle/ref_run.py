@@ -98,7 +98,7 @@ class RefCase:
         for f in self.workdir.glob("*.bin"):
             if f.stem in ("in", "out"):
                 continue
-            ints = f.stem in ("map", "invmap", "neighbors")
+            ints = f.stem in ("map", "invmap", "neighbors", "boundaryMap")
             d[f.stem] = np.fromfile(f, np.int32 if ints else np.float64)
         meta = {}
         for line in (self.workdir / "meta.txt").read_text().splitlines():

@@ -45,3 +45,25 @@ def rel_err(a, b):
 def have_gpu():
     import torch
     return torch.cuda.is_available()
+
+
+def perturbed_state(prob, ic: str, seed: int) -> np.ndarray:
+    """Seeded initial condition with a 1% seeded nodal perturbation of density, momentum and
+    energy (same recipe as the golden fixtures)."""
+    U = prob.init_state(ic, seed=seed)
+    i = prob.info
+    V = U.reshape(i.n_elem, i.n_fields, i.n_s)
+    rng = np.random.default_rng(seed + 1000)
+    nmom = i.dim
+    rho = V[:, 0, :] * (1 + 0.01 * rng.uniform(-1, 1, V[:, 0, :].shape))
+    V[:, 1:1 + nmom, :] += 0.01 * rng.uniform(-1, 1, V[:, 1:1 + nmom, :].shape) * rho[:, None, :]
+    V[:, 0, :] = rho
+    V[:, 1 + nmom, :] *= 1 + 0.01 * rng.uniform(-1, 1, V[:, 1 + nmom, :].shape)
+    return V.reshape(-1).copy()
+
+
+def l1_density_error(U, Uref, n_elem, n_fields, n_s) -> float:
+    """sum |rho - rho_ref| / sum |rho_ref| over all density nodes."""
+    a = np.asarray(U).reshape(n_elem, n_fields, n_s)[:, 0]
+    b = np.asarray(Uref).reshape(n_elem, n_fields, n_s)[:, 0]
+    return float(np.abs(a - b).sum() / np.abs(b).sum())

@@ -101,10 +101,13 @@ def make_case(c: dict, seed: int) -> dict:
     out["rk3"] = ref.rk3(U0, c["dt"], c["nsteps"])
     out["rk3c"] = ref.rk3(U0, 0.0, c["nsteps"], cfl=c["cfl"])
     dump = ref.dump()
+    # MonoX2Lag / Lag2MonoY are formed only for the limiters that use them (main.cc:558-583); for
+    # the others the reference leaves those buffers uninitialised, so they are not stored.
+    partial = ("MonoX2Lag", "Lag2MonoY") if c["limiter"] not in ("m2l", "m2i", "hri", "pri") else ()
     for k in ("phi", "dphi", "phi_w", "dphi_w", "psi", "psi_w", "weight", "J", "invJac", "JF", "normals",
-              "Minv", "map", "invmap", "neighbors", "Lag2Mono", "Mono2Lag", "Lag2MonoX", "MonoX2MonoY",
-              "MonoY2Lag", "MonoX2Lag", "Lag2MonoY"):
-        if k in dump:
+              "Minv", "map", "invmap", "boundaryMap", "neighbors", "Lag2Mono", "Mono2Lag", "Lag2MonoX",
+              "MonoX2MonoY", "MonoY2Lag", "MonoX2Lag", "Lag2MonoY"):
+        if k in dump and k not in partial:
             out["ref_" + k] = dump[k]
     for k, v in out.items():
         if not np.all(np.isfinite(v)):

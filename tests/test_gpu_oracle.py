@@ -1,0 +1,131 @@
+"""CUDA path (through the C ABI) against the numpy oracle at sizes and seeds the golden fixtures
+do not cover: ragged grids (extents not multiples of the 32 x 4 element tile), tile-aligned grids
+(tiled kernels), p = 1..3, all fluxes, both limiters, walls / periodic / transmissive
+boundaries, the 1D shock-tube workload (1000 elements, p=2, Roe, m2l, RK4) and the 2D
+shock-bubble workload at its full size (512 x 256 elements, p=2, Rusanov, m2l, SSP-RK3).
+
+Tolerances: 1e-12 relative per operator (residual, limiter, Minv solve, CFL step), 1e-10
+relative after a few RK steps, and 1e-10 in relative L1 density after 100 steps.
+"""
+import numpy as np
+import pytest
+
+from conftest import l1_density_error, perturbed_state, rel_err
+from oracle import dg_oracle as O
+
+pytestmark = pytest.mark.gpu
+
+WALLS = ("reflective", "transmissive", "reflective", "transmissive")
+
+CASES = [
+    # id, dim, order, nx, ny, bc, flux, limiter, ic
+    ("2d_p2_rus_m2l_ragged_walls", 2, 2, 40, 18, WALLS, "rusanov", "m2l", "shock_bubble"),
+    ("2d_p1_roe_hrl_ragged_periodic", 2, 1, 26, 14, ("periodic",) * 4, "roe", "hrl", "quadrants"),
+    ("2d_p3_roe_m2l_ragged", 2, 3, 18, 10, ("transmissive",) * 4, "roe", "m2l", "shock_bubble"),
+    ("2d_p2_roe_hrl_tiled_box", 2, 2, 64, 32, ("reflective",) * 4, "roe", "hrl", "quadrants"),
+    ("2d_p2_rus_m2l_tiled_walls", 2, 2, 96, 20, WALLS, "rusanov", "m2l", "shock_bubble"),
+    ("2d_p1_rus_m2l_tiled", 2, 1, 64, 8, ("transmissive",) * 4, "rusanov", "m2l", "quadrants"),
+    ("1d_p3_hll_hrl_walls", 1, 3, 301, 1, ("reflective",) * 2, "hll", "hrl", "tube_noise"),
+    ("1d_p1_rus_m2l_periodic", 1, 1, 257, 1, ("periodic",) * 2, "rusanov", "m2l", "tube_noise"),
+    ("1d_p2_roe_none", 1, 2, 123, 1, ("transmissive",) * 2, "roe", "none", "tube_noise"),
+]
+
+
+def make(case, seed):
+    import dg_b200 as dgb
+    _, dim, order, nx, ny, bc, flux, limiter, ic = case
+    x1 = 2.0 if dim == 2 and ic == "shock_bubble" else 1.0
+    prob = dgb.Problem.structured(dim, order, nx, ny, 0.0, x1, 0.0, 1.0, bc, flux=flux, limiter=limiter, cfl=0.3)
+    S = O.Setup.from_problem(prob)
+    U0 = O.limit(S, perturbed_state(prob, ic, seed))
+    return prob, S, U0
+
+
+@pytest.mark.parametrize("case", CASES, ids=[c[0] for c in CASES])
+def test_operators_match_oracle(case):
+    import dg_b200 as dgb
+    prob, S, U0 = make(case, seed=17)
+    s = dgb.DGSolver(prob)
+    try:
+        assert rel_err(s.dg_solver(U0), O.residual(S, U0)) < 1e-12
+        assert rel_err(s.solve(1e-3, U0), O.solve(S, 1e-3, O.residual(S, U0))) < 1e-12
+        Uraw = perturbed_state(prob, case[-1], 23)
+        assert rel_err(s.limit(Uraw), O.limit(S, Uraw)) < 1e-12
+        dt = s.dt_from_cfl(U0)
+        assert abs(dt - O.dt_from_cfl(S, U0)) <= 1e-13 * dt
+    finally:
+        s.close()
+
+
+@pytest.mark.parametrize("case", CASES, ids=[c[0] for c in CASES])
+def test_time_steps_match_oracle(case):
+    import dg_b200 as dgb
+    prob, S, U0 = make(case, seed=29)
+    s = dgb.DGSolver(prob)
+    try:
+        s.set_state(U0)
+        s.advance(3, 0.0, scheme=dgb.SSPRK3)
+        assert rel_err(s.get_state(), O.ssprk3_steps(S, U0, 0.0, 3)) < 1e-10
+        s.set_state(U0)
+        s.advance(2, 5e-4, scheme=dgb.RK4)
+        assert rel_err(s.get_state(), O.rk4_steps(S, U0, 5e-4, 2)) < 1e-10
+    finally:
+        s.close()
+
+
+def test_shock_tube_workload_100_steps_l1_density():
+    """1D two-fluid shock tube: [0,1], 1000 elements, p=2, Roe, m2l, RK4, transmissive ends,
+    seeded +-1e-3 density noise; 100 fixed steps of the CFL-0.4 size."""
+    import dg_b200 as dgb
+    prob = dgb.Problem.structured(1, 2, 1000, 1, 0.0, 1.0, 0.0, 1.0, ("transmissive",) * 2, flux="roe",
+                                  limiter="m2l", cfl=0.4)
+    S = O.Setup.from_problem(prob)
+    U0 = prob.init_state("tube_noise", seed=5)
+    dt = O.dt_from_cfl(S, U0)
+    s = dgb.DGSolver(prob)
+    try:
+        s.set_state(U0)
+        s.advance(100, dt, scheme=dgb.RK4)
+        Ug = s.get_state()
+    finally:
+        s.close()
+    Uo = O.rk4_steps(S, U0, dt, 100)
+    i = prob.info
+    assert l1_density_error(Ug, Uo, i.n_elem, i.n_fields, i.n_s) < 1e-10
+
+
+def test_shock_bubble_small_100_steps_l1_density():
+    """2D shock-bubble on a 32 x 16 grid (p=2, Rusanov, m2l, SSP-RK3, CFL step), 100 steps."""
+    import dg_b200 as dgb
+    prob = dgb.Problem.structured(2, 2, 32, 16, 0.0, 2.0, 0.0, 1.0, WALLS, flux="rusanov", limiter="m2l", cfl=0.3)
+    S = O.Setup.from_problem(prob)
+    U0 = O.limit(S, prob.init_state("shock_bubble", seed=7))
+    s = dgb.DGSolver(prob)
+    try:
+        s.set_state(U0)
+        s.advance(100, 0.0, scheme=dgb.SSPRK3)
+        Ug = s.get_state()
+    finally:
+        s.close()
+    Uo = O.ssprk3_steps(S, U0, 0.0, 100)
+    i = prob.info
+    assert l1_density_error(Ug, Uo, i.n_elem, i.n_fields, i.n_s) < 1e-10
+
+
+def test_shock_bubble_full_size_one_step():
+    """The 2D workload at full size (512 x 256, p=2, Rusanov, m2l): residual, limiter and one
+    SSP-RK3 step (CFL 0.3) against the oracle."""
+    import dg_b200 as dgb
+    prob = dgb.Problem.structured(2, 2, 512, 256, 0.0, 2.0, 0.0, 1.0, WALLS, flux="rusanov", limiter="m2l", cfl=0.3)
+    S = O.Setup.from_problem(prob)
+    Uraw = prob.init_state("shock_bubble", seed=7)
+    s = dgb.DGSolver(prob)
+    try:
+        U0 = s.limit(Uraw)
+        assert rel_err(U0, O.limit(S, Uraw)) < 1e-12
+        assert rel_err(s.dg_solver(U0), O.residual(S, U0)) < 1e-12
+        s.set_state(U0)
+        s.advance(1, 0.0, scheme=dgb.SSPRK3)
+        assert rel_err(s.get_state(), O.ssprk3_steps(S, U0, 0.0, 1)) < 1e-11
+    finally:
+        s.close()

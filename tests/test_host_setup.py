@@ -10,7 +10,7 @@ import pytest
 
 from conftest import golden_cases, load_golden, problem_for
 
-INT_ARRAYS = ("map", "invmap", "neighbors")
+INT_ARRAYS = ("map", "invmap", "boundaryMap", "neighbors")
 FLOAT_ARRAYS = ("phi", "dphi", "phi_w", "dphi_w", "psi", "psi_w", "weight", "J", "invJac", "JF", "normals",
                 "Minv", "Lag2Mono", "Mono2Lag", "Lag2MonoX", "MonoX2MonoY", "MonoY2Lag", "MonoX2Lag", "Lag2MonoY")
 
