@@ -314,7 +314,7 @@ def main(argv=None) -> int:
                 "e2e": e2e,
                 "roofline": {"bound": "hbm", "achieved": achieved_gbs, "peak": peak, "unit": "GB/s",
                              "frac": achieved_gbs / peak, "traffic": traffic,
-                             "kernel": "residual2d_kernel<p=2,Rusanov,SSP> (fused residual + stage update)",
+                             "kernel": "residual2d_tile_kernel<p=2,Rusanov,SSP> (fused residual + stage update)",
                              "algorithmic_bytes_per_launch": BYTES_PER_DOF_STAGE * dof,
                              "avg_launch_ms": res_avg_s * 1e3, "peak_source": "MEASURED_PEAKS.json hbm_gbs (measured copy)"},
                 "kernel_ms_per_step": {"residual": res_ms / args.steps, "limiter": lim_ms / args.steps,

@@ -25,7 +25,8 @@ CASES = [
     ("2d_p2_roe_hrl_tiled_box", 2, 2, 64, 32, ("reflective",) * 4, "roe", "hrl", "quadrants"),
     ("2d_p2_rus_m2l_tiled_walls", 2, 2, 96, 20, WALLS, "rusanov", "m2l", "shock_bubble"),
     ("2d_p1_rus_m2l_tiled", 2, 1, 64, 8, ("transmissive",) * 4, "rusanov", "m2l", "quadrants"),
-    ("1d_p3_hll_hrl_walls", 1, 3, 301, 1, ("reflective",) * 2, "hll", "hrl", "tube_noise"),
+    # p=3 with hrl between walls goes unstable at CFL 0.3 in the oracle as well; run it at 0.15
+    ("1d_p3_hll_hrl_walls", 1, 3, 301, 1, ("reflective",) * 2, "hll", "hrl", "tube_noise", 0.15),
     ("1d_p1_rus_m2l_periodic", 1, 1, 257, 1, ("periodic",) * 2, "rusanov", "m2l", "tube_noise"),
     ("1d_p2_roe_none", 1, 2, 123, 1, ("transmissive",) * 2, "roe", "none", "tube_noise"),
 ]
@@ -33,9 +34,10 @@ CASES = [
 
 def make(case, seed):
     import dg_b200 as dgb
-    _, dim, order, nx, ny, bc, flux, limiter, ic = case
+    _, dim, order, nx, ny, bc, flux, limiter, ic = case[:9]
+    cfl = case[9] if len(case) > 9 else 0.3
     x1 = 2.0 if dim == 2 and ic == "shock_bubble" else 1.0
-    prob = dgb.Problem.structured(dim, order, nx, ny, 0.0, x1, 0.0, 1.0, bc, flux=flux, limiter=limiter, cfl=0.3)
+    prob = dgb.Problem.structured(dim, order, nx, ny, 0.0, x1, 0.0, 1.0, bc, flux=flux, limiter=limiter, cfl=cfl)
     S = O.Setup.from_problem(prob)
     U0 = O.limit(S, perturbed_state(prob, ic, seed))
     return prob, S, U0
@@ -49,7 +51,7 @@ def test_operators_match_oracle(case):
     try:
         assert rel_err(s.dg_solver(U0), O.residual(S, U0)) < 1e-12
         assert rel_err(s.solve(1e-3, U0), O.solve(S, 1e-3, O.residual(S, U0))) < 1e-12
-        Uraw = perturbed_state(prob, case[-1], 23)
+        Uraw = perturbed_state(prob, case[8], 23)
         assert rel_err(s.limit(Uraw), O.limit(S, Uraw)) < 1e-12
         dt = s.dt_from_cfl(U0)
         assert abs(dt - O.dt_from_cfl(S, U0)) <= 1e-13 * dt
@@ -66,9 +68,10 @@ def test_time_steps_match_oracle(case):
         s.set_state(U0)
         s.advance(3, 0.0, scheme=dgb.SSPRK3)
         assert rel_err(s.get_state(), O.ssprk3_steps(S, U0, 0.0, 3)) < 1e-10
+        dt = 0.5 * O.dt_from_cfl(S, U0)  # a fixed step inside the case's CFL limit
         s.set_state(U0)
-        s.advance(2, 5e-4, scheme=dgb.RK4)
-        assert rel_err(s.get_state(), O.rk4_steps(S, U0, 5e-4, 2)) < 1e-10
+        s.advance(2, dt, scheme=dgb.RK4)
+        assert rel_err(s.get_state(), O.rk4_steps(S, U0, dt, 2)) < 1e-10
     finally:
         s.close()
 
