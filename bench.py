@@ -276,7 +276,7 @@ def main(argv=None) -> int:
     peaks = json.loads((ROOT / "MEASURED_PEAKS.json").read_text()) if (ROOT / "MEASURED_PEAKS.json").exists() else {}
     peak = peaks.get("hbm_gbs", 6650.0)
     traffic = None
-    tf = ROOT / "profiles" / "residual2d_p2_traffic.json"
+    tf = ROOT / "profiles" / "residual2d_tile_p2_512x256_traffic.json"
     if tf.exists():
         traffic = json.loads(tf.read_text()).get("bytes_per_launch_full_size")
 
