@@ -59,6 +59,7 @@ class Setup:
     a: dict = field(default_factory=dict)
     gx: float = 0.0          # constants::GLOBAL_GX / GLOBAL_GY (zero unless an IC sets gravity)
     gy: float = 0.0
+    thresholds: tuple = ()   # "#sensor thresholds" of the deck (sensor.h:35-45)
 
     @property
     def order(self) -> int:
@@ -71,10 +72,11 @@ class Setup:
         arrays = {k[4:]: v for k, v in d.items() if k.startswith("ref_")}
         return cls(D=rm["D"], N_F=rm["N_F"], N_E=rm["N_E"], N_s=rm["N_s"], N_G=rm["N_G"], M_T=rm["M_T"],
                    M_s=rm["M_s"], M_G=rm["M_G"], N_N=rm["N_N"], flux=meta["flux"], limiter=meta["limiter"],
-                   cfl_scaled=rm["cfl_scaled"], n_reflective=rm.get("rflctive", 0), a=arrays)
+                   cfl_scaled=rm["cfl_scaled"], n_reflective=rm.get("rflctive", 0), a=arrays,
+                   thresholds=tuple(meta.get("thresholds", ())))
 
     @classmethod
-    def from_problem(cls, prob) -> "Setup":
+    def from_problem(cls, prob, thresholds=()) -> "Setup":
         """From a dg_b200.Problem (host setup pinned to the reference arrays by tests)."""
         i = prob.info
         names = {0: "rusanov", 1: "hll", 2: "roe"}
@@ -87,7 +89,7 @@ class Setup:
                 pass
         return cls(D=i.dim, N_F=i.n_fields, N_E=i.n_elem, N_s=i.n_s, N_G=i.n_g, M_T=i.n_ifaces, M_s=i.m_s,
                    M_G=i.m_g, N_N=i.n_n, flux=names[i.flux], limiter=lims[i.limiter], cfl_scaled=i.cfl_scaled,
-                   n_reflective=i.n_reflective, a=arrays)
+                   n_reflective=i.n_reflective, a=arrays, thresholds=tuple(thresholds))
 
 
 # ---------------------------------------------------------------------------------------------
@@ -566,6 +568,10 @@ def limit(S: Setup, U: np.ndarray) -> np.ndarray:
         return _hr(S, U)
     if S.limiter == "m2l":
         return _m2(S, U)
+    if S.limiter == "prl":
+        return prim2cons(S, _hr(S, cons2prim(S, U)))
+    if S.limiter in ("hri", "m2i", "pri", "p0i"):
+        return _sensor_gated(S, U)
     raise NotImplementedError(f"limiter {S.limiter}")
 
 
@@ -683,3 +689,239 @@ def ssprk3_steps(S: Setup, U: np.ndarray, dt: float, nsteps: int) -> np.ndarray:
         U2 = limit(S, 0.75 * Un + 0.25 * (U1 + solve(S, Dt, residual(S, U1))))
         U = limit(S, (1.0 / 3.0) * Un + (2.0 / 3.0) * (U2 + solve(S, Dt, residual(S, U2))))
     return U
+
+
+# ---------------------------------------------------------------------------------------------
+# sensors and the sensor-gated (per-element) limiters
+# ---------------------------------------------------------------------------------------------
+
+def cons2prim(S: Setup, U: np.ndarray) -> np.ndarray:
+    """Cons2Prim, limiting_kernels.cu:1009-1059 (gamma model): (rho, u, [v,] p, alpha)."""
+    V = np.array(U, np.float64, copy=True).reshape(S.N_E, S.N_F, S.N_s)
+    rho, ru = V[:, 0].copy(), V[:, 1].copy()
+    rv = V[:, 2].copy() if S.D == 2 else np.zeros_like(rho)
+    E, al = V[:, S.D + 1].copy(), V[:, S.D + 2].copy()
+    V[:, 1] = ru / rho
+    if S.D == 2:
+        V[:, 2] = rv / rho
+    V[:, S.D + 1] = (E - 0.0 - 0.5 * (ru * ru + rv * rv) / rho) / al
+    return V.reshape(-1)
+
+
+def prim2cons(S: Setup, W: np.ndarray) -> np.ndarray:
+    """Prim2Cons, limiting_kernels.cu:957-1007: rho u -> momentum, p alpha + kinetic -> E."""
+    V = np.array(W, np.float64, copy=True).reshape(S.N_E, S.N_F, S.N_s)
+    rho, u = V[:, 0].copy(), V[:, 1].copy()
+    v = V[:, 2].copy() if S.D == 2 else np.zeros_like(rho)
+    p, al = V[:, S.D + 1].copy(), V[:, S.D + 2].copy()
+    V[:, 1] = rho * u
+    if S.D == 2:
+        V[:, 2] = rho * v
+    V[:, S.D + 1] = p * al + 0.0 + 0.5 * rho * (u * u + v * v)
+    return V.reshape(-1)
+
+
+def _cell_means(S: Setup, U: np.ndarray) -> np.ndarray:
+    """SENSOR::sensing's "average solution" (sensor.cc:26): nodal mean per element and field."""
+    V = np.asarray(U).reshape(S.N_E, S.N_F, S.N_s)
+    acc = V[:, :, 0].copy()
+    for i in range(1, S.N_s):
+        acc = acc + V[:, :, i]
+    return acc * (1.0 / S.N_s)
+
+
+def sensors(S: Setup, U: np.ndarray) -> np.ndarray:
+    """SENSOR::sensing (sensor.cc:11-35) with calc_sensors (sensor_kernels.cu:19-165), CPU order.
+
+    Each element not yet flagged tests its neighbours in order (left, right[, bottom, top]) with
+    Roe-averaged cell means: sensor 1 (contact, density wave strength), sensor 2 (shock: converging
+    acoustic characteristics and a pressure jump), sensor 3 (contact, gamma jump), each against its
+    deck threshold; the first hit flags the element and that neighbour with the sensor number and
+    stops its loop; a boundary neighbour (negative index) flags the element with 1 and stops.
+    Elements are visited in index order and an element flagged by an earlier one skips its own
+    tests -- this sequential order is part of the result."""
+    th = list(S.thresholds)
+    on1, on2, on3 = len(th) > 0, len(th) > 1, len(th) > 2
+    t1 = th[0] if on1 else 0.0
+    t2 = th[1] if on2 else 0.0
+    t3 = th[2] if on3 else 0.0
+    A = _cell_means(S, U)
+    rho = A[:, 0]
+    vx = A[:, 1] / rho
+    vy = A[:, 2] / rho if S.D == 2 else np.zeros_like(rho)
+    Et = A[:, S.D + 1]
+    al = A[:, S.D + 2]
+    gam = 1.0 + 1.0 / al
+    pinf = (1 - 1.0 / gam) * 0.0
+    p = (gam - 1) * (Et - 0.0 - 0.5 * rho * (vx * vx + vy * vy))
+    ie = p * al
+    with np.errstate(invalid="ignore", divide="ignore"):
+        a = np.sqrt((gam * (p + pinf)) / rho)
+    H = (Et + p) / rho
+    nb = S.a["neighbors"].reshape(S.N_E, S.N_N)
+    hit = np.zeros((S.N_E, S.N_N), dtype=np.int64)  # 0 none, 1..3 sensor, -1 boundary
+    with np.errstate(invalid="ignore", divide="ignore"):
+        for nn in range(S.N_N):
+            r = nb[:, nn]
+            ok = r >= 0
+            R = np.where(ok, r, 0)
+            RT = np.sqrt(rho[R] / rho)
+            ux = (vx + RT * vx[R]) / (1 + RT)
+            uy = (vy + RT * vy[R]) / (1 + RT)
+            alr = (al + RT * al[R]) / (1 + RT)
+            gr = 1 + 1.0 / alr
+            Hr = (H + RT * H[R]) / (1 + RT)
+            ar = np.sqrt((gr - 1) * (Hr - 0.5 * (ux * ux + uy * uy)))
+            ir = (ie + RT * ie[R]) / (1 + RT)
+            drho = rho[R] - rho
+            dp = (gr - 1) * (gr - 1) * (alr * (ie[R] - ie) - ir * (al[R] - al))
+            dV2 = drho - dp / (ar * ar)
+            G = np.abs(dV2) / (rho + rho[R])
+            d1 = on1 & (2 * G / ((1 + G) * (1 + G)) > t1)
+            shock = ((vx - a > ux - ar) & (ux - ar > vx[R] - a[R])) | ((vy - a > uy - ar) & (uy - ar > vy[R] - a[R]))
+            psi = np.abs(p[R] - p) / (p + p[R])
+            d2 = on2 & shock & (2 * psi / ((1 + psi) * (1 + psi)) > t2)
+            G3 = np.abs(gam[R] - gam) / (gam + gam[R])
+            d3 = on3 & (2 * G3 / ((1 + G3) * (1 + G3)) > t3)
+            typ = np.where(d1, 1, np.where(d2, 2, np.where(d3, 3, 0)))
+            hit[:, nn] = np.where(ok, typ, -1)
+    sens = np.zeros(S.N_E, dtype=np.int64)
+    for e in range(S.N_E):
+        if sens[e] != 0:
+            continue
+        for nn in range(S.N_N):
+            h = hit[e, nn]
+            if h == -1:
+                sens[e] = 1
+                break
+            if h > 0:
+                sens[e] = h
+                sens[nb[e, nn]] = h
+                break
+    return sens
+
+
+def _set2average(L2M, M2L, X, n1, Ns):
+    """set2average, limiting_kernels.cu:1792-1827: every slice to its average; returns the nodal
+    result and the limited monomial coefficients."""
+    A = _apply(L2M, X, Ns).reshape(X.shape[:-1] + (Ns // n1, n1))
+    Al = average_monomial(A).reshape(X.shape)
+    return _apply(M2L, Al, Ns).reshape(X.shape), Al
+
+
+def _HR(L2M, M2L, XL, XC, XR, n1, Ns):
+    """HR, limiting_kernels.cu:1829-1868: per slice limit_monomial of the three cells."""
+    sh = XC.shape[:-1] + (Ns // n1, n1)
+    Al = limit_monomial(_apply(L2M, XL, Ns).reshape(sh), _apply(L2M, XC, Ns).reshape(sh),
+                        _apply(L2M, XR, Ns).reshape(sh)).reshape(XC.shape)
+    return _apply(M2L, Al, Ns).reshape(XC.shape), Al
+
+
+def _phys_codes(S: Setup, offxy: int):
+    nb = S.a["neighbors"].reshape(S.N_E, S.N_N)
+    left, right = nb[:, offxy], nb[:, offxy + 1]
+    phys = np.zeros(S.N_E, dtype=np.int64)
+    phys = np.where(left < 0, -left, phys)
+    phys = np.where(right < 0, -right, phys)
+    return phys, np.where(left >= 0, left, 0), np.where(right >= 0, right, 0)
+
+
+def _hri_pass(S: Setup, U: np.ndarray, offxy: int, L2M, M2L, n1: int) -> np.ndarray:
+    """hri1D, limiting_kernels.cu:322-429, evaluated for every element (callers keep the flagged
+    ones): per field, HR with the neighbours' nodal values, averages at transmissive boundaries,
+    averages except the wall-normal momentum at walls, unchanged for code 4."""
+    Ns = S.N_s
+    V = np.asarray(U).reshape(S.N_E, S.N_F, Ns)
+    phys, L, R = _phys_codes(S, offxy)
+    full, _ = _HR(L2M, M2L, V[L], V, V[R], n1, Ns)
+    avg, _ = _set2average(L2M, M2L, V, n1, Ns)
+    out = V.copy()
+    m = ~np.isin(phys, (2, 3, 4))
+    out[m] = full[m]
+    out[phys == 2] = avg[phys == 2]
+    w = phys == 3
+    un = 1 if offxy == 0 else 2
+    for fc in range(S.N_F):
+        if fc != un:
+            out[w, fc] = avg[w, fc]
+    return out.reshape(-1)
+
+
+def _m2i_pass(S: Setup, U: np.ndarray, offxy: int, L2M, M2L, n1: int) -> np.ndarray:
+    """m2i1D, limiting_kernels.cu:431-722 (gamma model), for every element: HR (or averaging at
+    boundaries) of rho, momenta, 1/(gamma-1) and the nodal pressure, then the total energy rebuilt
+    from the limited pressure, 1/(gamma-1) and kinetic energy (limiting_kernels.cu:1870-1990)."""
+    Ns, D = S.N_s, S.D
+    V = np.asarray(U).reshape(S.N_E, S.N_F, Ns)
+    phys, L, R = _phys_codes(S, offxy)
+    iE, iG = D + 1, D + 2
+    mom = [1, 2] if D == 2 else [1]
+
+    def press(X):
+        kin = X[:, 1] * X[:, 1] + (X[:, 2] * X[:, 2] if D == 2 else 0.0)
+        return (X[:, iE] - 0.5 * kin / X[:, 0]) / X[:, iG]
+
+    pC, pL, pR = press(V), press(V[L]), press(V[R])
+    out = V.copy()
+    # limited / averaged primitive-like quantities, per element case
+    hr = {k: _HR(L2M, M2L, V[L][:, k], V[:, k], V[R][:, k], n1, Ns) for k in [0] + mom + [iG]}
+    av = {k: _set2average(L2M, M2L, V[:, k], n1, Ns) for k in [0] + mom + [iG]}
+    hrp = _HR(L2M, M2L, pL, pC, pR, n1, Ns)
+    avp = _set2average(L2M, M2L, pC, n1, Ns)
+    full = ~np.isin(phys, (2, 3, 4))
+    walls = phys == 3
+    trans = phys == 2
+    glim = np.where(full[:, None], hr[iG][1], av[iG][1])
+    plim = np.where(full[:, None], hrp[1], avp[1])
+    for k in [0] + mom + [iG]:
+        out[full, k] = hr[k][0][full]
+        out[trans, k] = av[k][0][trans]
+    out[walls, 0] = av[0][0][walls]
+    out[walls, iG] = av[iG][0][walls]
+    if D == 2:
+        tang = 2 if offxy == 0 else 1   # the momentum along the wall is averaged, the normal one kept
+        out[walls, tang] = av[tang][0][walls]
+    kin = out[:, 1] * out[:, 1] + (out[:, 2] * out[:, 2] if D == 2 else 0.0)
+    K = _apply(L2M, 0.5 * kin / out[:, 0], Ns)
+    sl = (S.N_E, Ns // n1, n1)
+    rhoe = _internal_energy(plim.reshape(sl), glim.reshape(sl))
+    EM = _apply(L2M, V[:, iE], Ns).reshape(sl)
+    E = _apply(M2L, _reconstruct_energy(rhoe, K.reshape(sl), EM).reshape(S.N_E, Ns), Ns)
+    act = full | walls | trans
+    out[act, iE] = E[act]
+    return out.reshape(-1)
+
+
+def p0i_average(S: Setup, U: np.ndarray) -> np.ndarray:
+    """p0i, limiting_kernels.cu:723-770: every node set to the cell average
+    sum_g sum_i phi_w[i*N_G+g] U_i / |reference element| (4 for quads; 2 for lines, where the
+    reference leaves the area unset, main.cc:284)."""
+    ref_area = 4.0 if S.D == 2 else 2.0
+    V = np.asarray(U).reshape(S.N_E, S.N_F, S.N_s)
+    pw = S.a["phi_w"].reshape(S.N_s, S.N_G)
+    avg = np.einsum("efi,ig->ef", V, pw) / ref_area
+    return np.broadcast_to(avg[:, :, None], V.shape).reshape(-1).copy()
+
+
+def _sensor_gated(S: Setup, U: np.ndarray) -> np.ndarray:
+    """Limiting::HRIlimiting / PRIlimiting / M2Ilimiting / P0Ilimiting (limiting.cc:596-742): the
+    sensor on the conserved state, then the per-element limiter on the flagged elements only, x
+    slices then y slices (each pass reading the previous pass's state); pri works on primitive
+    variables (all elements converted there and back)."""
+    U = np.asarray(U, np.float64)
+    flag = (sensors(S, U) != 0)
+    NE, NF, Ns = S.N_E, S.N_F, S.N_s
+    fl = np.repeat(flag, NF * Ns)
+    if S.limiter == "p0i":
+        return np.where(fl, p0i_average(S, U), U)
+    W = cons2prim(S, U) if S.limiter == "pri" else U.copy()
+    a = S.a
+    if S.D == 1:
+        passes = [(0, a["Lag2Mono"], a["Mono2Lag"], Ns)]
+    else:
+        n1 = S.order + 1
+        passes = [(0, a["Lag2MonoX"], a["MonoX2Lag"], n1), (2, a["Lag2MonoY"], a["MonoY2Lag"], n1)]
+    fn = _m2i_pass if S.limiter == "m2i" else _hri_pass
+    for off, L2M, M2L, n1 in passes:
+        W = np.where(fl, fn(S, W, off, L2M, M2L, n1), W)
+    return prim2cons(S, W) if S.limiter == "pri" else W

@@ -14,6 +14,7 @@
 //   residual  f = DG_SOLVER::dg_solver(U)            (code/src/dg/dg_solver.h:292)
 //   solve     DU = Dt Minv f                          (code/src/time_integration/rk_kernels.cu:182)
 //   limit     U <- Limiting::<deck method>(U)         (code/src/limiting/limiting.cc)
+//   sensors   SENSOR::sensing(neighbors, U) flags     (code/src/sensors/sensor.cc:11)
 //   dt        Dt = RK::DtFromCFL(U)                   (code/src/time_integration/rk.cc:250)
 //   rk4       the reference time loop itself on U     (code/src/time_integration/rk.cc:11)
 //   rk4n      n steps of the reference RK4 step body (rk.cc:155-209), fixed or CFL step
@@ -173,6 +174,12 @@ __wrap__ZN2RK14RK_integrationEdiiiiiiiPdS0_R8LimitingbR9DG_SOLVERR12COMMUNICATOR
   } else if (a.cmd == "limit") {
     for (int r = 0; r < a.repeat; ++r) limit_in_place(*Lim, *comm, *sensor, *dg, U.data());
     write_raw(a.out, U.data(), n);
+  } else if (a.cmd == "sensors") {
+    // SENSOR::sensing on U (sensor.cc:11); the flags are written as doubles
+    sensor->sensing(Lim->_neighbors, U.data());
+    std::vector<double> flags(N_E);
+    for (int e = 0; e < N_E; ++e) flags[e] = sensor->getSensors()[e];
+    write_raw(a.out, flags.data(), (size_t)N_E);
   } else if (a.cmd == "dt") {
     std::vector<double> upa((size_t)N_s * N_E, 0.0);
     double dt = rk->DtFromCFL(N_s, N_E, CFL, U.data(), upa.data());

@@ -45,6 +45,7 @@ class RefCase:
     limiter: str = "m2l"
     cfl: float = -1.0
     output_times: tuple = (0.0, 1e-3)
+    thresholds: tuple = ()
     workdir: Path | None = None
     _tmp: object = field(default=None, repr=False)
 
@@ -67,6 +68,8 @@ class RefCase:
                  "#Courant-Friedrichs-Lewy condition", repr(float(cfl)), "#order", str(self.order),
                  "#mesh file", "mesh.msh", "lin" if self.dim == 1 else "qua", "#limiter", self.limiter,
                  "#initial condition", "sodtube" if self.dim == 1 else "sodcirc"]
+        if self.thresholds:
+            lines += ["#sensor thresholds", " ".join(repr(float(t)) for t in self.thresholds)]
         p = self.workdir / "deck.inp"
         p.write_text("\n".join(lines) + "\n")
         return p
@@ -115,6 +118,9 @@ class RefCase:
 
     def limit(self, U):
         return self.run("limit", U)[0]
+
+    def sensors(self, U):
+        return self.run("sensors", U)[0].astype(np.int64)
 
     def dt_cfl(self, U, cfl):
         self.write_deck(cfl=cfl)

@@ -63,6 +63,27 @@ CASES = [
          flux="roe", limiter="hrl", ic="quadrants", cfl=0.3, dt=5e-4, nsteps=4),
     dict(name="t2_p2_roe_m2l_box", dim=2, order=2, nx=32, ny=12, dom=(0, 1, 0, 1), bc=("reflective",) * 4,
          flux="roe", limiter="m2l", ic="quadrants", cfl=0.3, dt=5e-4, nsteps=4),
+    # sensor-gated limiters (per-element HR / m2 / primitive HR / p=0 on flagged elements) and the
+    # primitive-variable HR limiter; thresholds are the deck's "#sensor thresholds"
+    dict(name="s2_p2_rus_hri_walls", dim=2, order=2, nx=12, ny=8, dom=(0, 2, 0, 1),
+         bc=("reflective", "transmissive", "reflective", "transmissive"), flux="rusanov", limiter="hri",
+         ic="shock_bubble", cfl=0.3, dt=5e-4, nsteps=3, thresholds=(0.01, 0.05, 0.01)),
+    dict(name="s2_p2_roe_m2i_periodic", dim=2, order=2, nx=12, ny=8, dom=(0, 1, 0, 1), bc=("periodic",) * 4,
+         flux="roe", limiter="m2i", ic="quadrants", cfl=0.3, dt=5e-4, nsteps=3, thresholds=(0.02, 0.02, 0.02)),
+    dict(name="s2_p2_rus_m2i_box", dim=2, order=2, nx=10, ny=10, dom=(0, 1, 0, 1), bc=("reflective",) * 4,
+         flux="rusanov", limiter="m2i", ic="quadrants", cfl=0.3, dt=5e-4, nsteps=3, thresholds=(0.02, 0.05)),
+    dict(name="s2_p1_roe_pri", dim=2, order=1, nx=10, ny=6, dom=(0, 1, 0, 1), bc=("transmissive",) * 4,
+         flux="roe", limiter="pri", ic="quadrants", cfl=0.3, dt=5e-4, nsteps=3, thresholds=(0.02, 0.02)),
+    dict(name="s2_p2_rus_p0i", dim=2, order=2, nx=12, ny=8, dom=(0, 2, 0, 1), bc=("transmissive",) * 4,
+         flux="rusanov", limiter="p0i", ic="shock_bubble", cfl=0.3, dt=5e-4, nsteps=3, thresholds=(0.05,)),
+    dict(name="s1_p2_roe_m2i", dim=1, order=2, nx=30, ny=1, dom=(0, 1, 0, 1), bc=("transmissive",) * 2,
+         flux="roe", limiter="m2i", ic="tube_noise", cfl=0.3, dt=2e-4, nsteps=4, thresholds=(0.01, 0.01, 0.01)),
+    dict(name="s1_p3_hll_hri_wall", dim=1, order=3, nx=30, ny=1, dom=(0, 1, 0, 1), bc=("reflective",) * 2,
+         flux="hll", limiter="hri", ic="tube_noise", cfl=0.15, dt=1e-4, nsteps=4, thresholds=(0.01, 0.05)),
+    dict(name="s1_p2_rus_pri_periodic", dim=1, order=2, nx=30, ny=1, dom=(0, 1, 0, 1), bc=("periodic",) * 2,
+         flux="rusanov", limiter="pri", ic="tube_noise", cfl=0.3, dt=2e-4, nsteps=4, thresholds=(0.001,)),
+    dict(name="s1_p2_rus_prl", dim=1, order=2, nx=30, ny=1, dom=(0, 1, 0, 1), bc=("transmissive",) * 2,
+         flux="rusanov", limiter="prl", ic="tube_noise", cfl=0.3, dt=2e-4, nsteps=4),
 ]
 
 
@@ -83,11 +104,15 @@ def perturbed_state(prob: "dgb.Problem", ic: str, seed: int) -> np.ndarray:
 def make_case(c: dict, seed: int) -> dict:
     x0, x1, y0, y1 = c["dom"]
     bc = tuple(c["bc"]) + ("transmissive",) * (4 - len(c["bc"]))
-    ref = RefCase(c["dim"], c["order"], c["nx"], c["ny"], x0, x1, y0, y1, bc, c["flux"], c["limiter"])
+    th = tuple(c.get("thresholds", ()))
+    ref = RefCase(c["dim"], c["order"], c["nx"], c["ny"], x0, x1, y0, y1, bc, c["flux"], c["limiter"],
+                  thresholds=th)
     prob = dgb.Problem.structured(c["dim"], c["order"], c["nx"], c["ny"], x0, x1, y0, y1, bc, flux=c["flux"],
-                                  limiter=c["limiter"], cfl=c["cfl"])
+                                  limiter=c["limiter"], cfl=c["cfl"], thresholds=th)
     Uraw = perturbed_state(prob, c["ic"], seed)
     out = dict(Uraw=Uraw)
+    if th:
+        out["sens"] = ref.sensors(Uraw)   # SENSOR::sensing flags of the raw state
     out["Ulim"] = ref.limit(Uraw)
     # operators and steps start from the limited state when a limiter is on (the reference limits
     # the initial condition before integrating, rk.cc:108-114): a raw high-order interpolation of
@@ -112,7 +137,10 @@ def make_case(c: dict, seed: int) -> dict:
     for k, v in out.items():
         if not np.all(np.isfinite(v)):
             raise RuntimeError(f"{c['name']}: reference output {k} is not finite")
-    out["meta"] = np.array(json.dumps({**c, "bc": list(bc), "seed": seed, "ref_meta": dump["meta"]}))
+    meta = dict(dump["meta"])
+    if c["dim"] == 1:
+        meta.pop("cartesian", None)  # never set by the reference's 1D Limiting constructor
+    out["meta"] = np.array(json.dumps({**c, "bc": list(bc), "seed": seed, "ref_meta": meta}))
     return out
 
 

@@ -70,3 +70,10 @@ def test_oracle_on_package_setup_arrays(name):
     S = O.Setup.from_problem(problem_for(meta))
     assert rel_err(O.residual(S, d["U0"]), d["f"]) < 1e-12
     assert rel_err(O.limit(S, d["Uraw"]), d["Ulim"]) < 1e-12
+
+
+@pytest.mark.parametrize("name", [c for c in CASES if "thresholds" in load_golden(c)[0]])
+def test_oracle_sensors(name):
+    """SENSOR::sensing flags (sequential CPU semantics) on the raw state, exactly."""
+    meta, d, S = setup_for(name)
+    assert np.array_equal(O.sensors(S, d["Uraw"]), d["sens"])
