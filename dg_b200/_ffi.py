@@ -24,6 +24,7 @@ EXPORTS = [
     "dgb_destroy", "dgb_set_state", "dgb_get_state", "dgb_set_state_device", "dgb_get_state_device",
     "dgb_residual", "dgb_solve", "dgb_limit", "dgb_dt_from_cfl", "dgb_advance", "dgb_last_dt",
     "dgb_conservation", "dgb_last_timing", "dgb_set_profiling", "dgb_kernel_timing", "dgb_limit_noalloc",
+    "dgb_sensors",
 ]
 
 
@@ -85,6 +86,7 @@ def lib() -> C.CDLL:
         "dgb_residual": [vp, dp, dp],
         "dgb_solve": [vp, C.c_double, dp, dp],
         "dgb_limit": [vp, dp],
+        "dgb_sensors": [vp, dp, C.POINTER(C.c_int)],
         "dgb_dt_from_cfl": [vp, dp, dp],
         "dgb_advance": [vp, ip, ip, C.c_double, dp],
         "dgb_last_dt": [vp, dp],

@@ -29,6 +29,9 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 CXXFLAGS = ["-std=c++17", "-O2", "-fPIC", "-Wall", "-Wno-sign-compare"]
 NVFLAGS = ["-std=c++17", "-O3", "-lineinfo", "-Xcompiler", "-fPIC", "--expt-relaxed-constexpr",
            "-Xptxas", "-warn-spills"] + ARCH
+# per-file additions: the sensors take threshold decisions that must see the same separately
+# rounded products and sums as the reference's CPU arithmetic, so no multiply-add contraction there
+FILE_NVFLAGS = {"dgb_sensor.cu": ["-fmad=false"]}
 
 
 def _deps_digest(paths: list[Path]) -> str:
@@ -64,7 +67,8 @@ def build(force: bool = False, verbose: bool = False) -> Path:
         if obj.exists() and not force:
             continue
         if src.suffix == ".cu":
-            cmd = [NVCC] + NVFLAGS + [f"-I{INC}", f"-I{SRC}", "-c", str(src), "-o", str(obj)]
+            cmd = [NVCC] + NVFLAGS + FILE_NVFLAGS.get(src.name, []) + [f"-I{INC}", f"-I{SRC}", "-c", str(src), "-o",
+                                                                       str(obj)]
         else:
             cmd = ["g++"] + CXXFLAGS + [f"-I{INC}", f"-I{SRC}", "-c", str(src), "-o", str(obj)]
         jobs.append(cmd)

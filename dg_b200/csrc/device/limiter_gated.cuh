@@ -1,0 +1,194 @@
+// Sensor-gated (per-element) limiters and the primitive-variable HR limiter.
+//
+//   hri  HR on every field of the flagged elements, x slices then y slices, each pass reading the
+//        state the previous pass left (Limiting::HRIlimiting, code/src/limiting/limiting.cc:596-625,
+//        hri1D limiting_kernels.cu:322-429)
+//   m2i  the m2 limiter on the flagged elements, pressure recomputed from each pass's input state
+//        (Limiting::M2Ilimiting, limiting.cc:661-690, m2i1D limiting_kernels.cu:431-722)
+//   pri  hri on primitive variables (rho, u, [v,] p, alpha); every element goes to primitive
+//        variables and back (Limiting::PRIlimiting, limiting.cc:627-659)
+//   p0i  flagged elements set to their cell average (Limiting::P0Ilimiting, limiting.cc:692-710,
+//        p0i limiting_kernels.cu:723-770)
+//   prl  HR limiting of the primitive variables on all elements (Limiting::PRlimiting,
+//        limiting.cc:102-121)
+// Flags come from the sensor kernels (dgb_sensor.cu).  Unflagged elements are copied unchanged
+// (converted, for pri).  One thread per (element, slice); the slice arithmetic is the same scaled
+// Taylor-monomial machinery as the global limiters.
+#pragma once
+#include "kernels.cuh"
+
+namespace dgb {
+
+// gamma-model conserved <-> primitive at one node, in place (Cons2Prim / Prim2Cons,
+// limiting_kernels.cu:957-1059): (rho, rho u, [rho v,] E, alpha) <-> (rho, u, [v,] p, alpha)
+template <int D>
+__device__ __forceinline__ void cons_to_prim(double* q) {
+  const double rho = q[0], ru = q[1], rv = D == 2 ? q[2] : 0.0, E = q[D + 1], al = q[D + 2];
+  q[1] = ru / rho;
+  if (D == 2) q[2] = rv / rho;
+  q[D + 1] = (E - 0.5 * (ru * ru + rv * rv) / rho) / al;
+}
+template <int D>
+__device__ __forceinline__ void prim_to_cons(double* q) {
+  const double rho = q[0], u = q[1], v = D == 2 ? q[2] : 0.0, p = q[D + 1], al = q[D + 2];
+  q[1] = rho * u;
+  if (D == 2) q[2] = rho * v;
+  q[D + 1] = p * al + 0.5 * rho * (u * u + v * v);
+}
+
+// One pass of hri / pri (METHOD 1) or m2i (METHOD 2).  PASS 0: x slices (row iy = blockIdx.y,
+// neighbours left/right); PASS 1: y slices (column ix = blockIdx.y, neighbours bottom/top); 1D: the
+// element is the slice.  IN_PRIM converts loaded values to primitive variables, OUT_CONS converts
+// stored values back.  out must not alias U.
+template <int D, int P, int METHOD, int PASS, bool IN_PRIM, bool OUT_CONS>
+__global__ void __launch_bounds__(128) lim_gated_kernel(const LimArgs la, const int* __restrict__ sens,
+                                                        const double* __restrict__ U, const int* __restrict__ nbr,
+                                                        double* __restrict__ out, const DevScalars* __restrict__ scal) {
+  constexpr int N1 = P + 1, NS = D == 2 ? N1 * N1 : N1, NF = D + 3, IE = D + 1, IA = D + 2;
+  constexpr int UN = (D == 2 && PASS == 1) ? 2 : 1;  // wall-normal momentum of this pass
+  if (scal && scal->flags) return;
+  const int ld = la.ld, e = blockIdx.x * blockDim.x + threadIdx.x, sl = blockIdx.y;
+  if (e >= la.n_elem) return;
+  auto node = [&](int k) { return D == 1 ? k : (PASS == 0 ? k + N1 * sl : sl + N1 * k); };
+  auto load = [&](int el, double (*v)[N1]) {
+#pragma unroll
+    for (int k = 0; k < N1; ++k) {
+      double q[NF];
+#pragma unroll
+      for (int f = 0; f < NF; ++f) q[f] = __ldg(U + (size_t)(f * NS + node(k)) * ld + el);
+      if (IN_PRIM) cons_to_prim<D>(q);
+#pragma unroll
+      for (int f = 0; f < NF; ++f) v[f][k] = q[f];
+    }
+  };
+  auto store = [&](double (*v)[N1]) {
+#pragma unroll
+    for (int k = 0; k < N1; ++k) {
+      double q[NF];
+#pragma unroll
+      for (int f = 0; f < NF; ++f) q[f] = v[f][k];
+      if (OUT_CONS) prim_to_cons<D>(q);
+#pragma unroll
+      for (int f = 0; f < NF; ++f) out[(size_t)(f * NS + node(k)) * ld + e] = q[f];
+    }
+  };
+  double c[NF][N1];
+  load(e, c);
+  if (!__ldg(sens + e)) {
+    store(c);
+    return;
+  }
+  const int o = PASS == 0 ? 0 : 2;
+  const int nA = __ldg(nbr + (size_t)o * ld + e), nB = __ldg(nbr + (size_t)(o + 1) * ld + e);
+  const int phys = boundary_code(nA, nB);
+  if (phys == 4) {  // "leave data unchanged"
+    store(c);
+    return;
+  }
+  double l[NF][N1], r[NF][N1];
+  if (phys == 0) {
+    load(nA, l);
+    load(nB, r);
+  }
+  double res[NF][N1];
+  if constexpr (METHOD == 1) {
+#pragma unroll
+    for (int f = 0; f < NF; ++f) {
+      if (phys == 3 && f == UN) {  // the wall-normal momentum is not limited at a wall
+#pragma unroll
+        for (int k = 0; k < N1; ++k) res[f][k] = c[f][k];
+        continue;
+      }
+      double lim[N1];
+      limit_slice<P>(phys, l[f], c[f], r[f], lim);
+      to_lag<P>(lim, res[f]);
+    }
+  } else {
+    // nodal pressure of the three cells (pressure, limiting_kernels.cu:1870-1897)
+    double pc[N1], pl[N1], pr[N1];
+    auto press = [&](double (*v)[N1], double* p) {
+#pragma unroll
+      for (int k = 0; k < N1; ++k) {
+        const double kin = v[1][k] * v[1][k] + (D == 2 ? v[2][k] * v[2][k] : 0.0);
+        p[k] = (v[IE][k] - 0.5 * kin / v[0][k]) / v[IA][k];
+      }
+    };
+    press(c, pc);
+    if (phys == 0) {
+      press(l, pl);
+      press(r, pr);
+    }
+    double mr[N1], ma[N1], mp[N1];
+    limit_slice<P>(phys, l[0], c[0], r[0], mr);
+    limit_slice<P>(phys, l[IA], c[IA], r[IA], ma);
+    limit_slice<P>(phys, pl, pc, pr, mp);
+    to_lag<P>(mr, res[0]);
+    to_lag<P>(ma, res[IA]);
+#pragma unroll
+    for (int f = 1; f <= D; ++f) {
+      if (phys == 3 && f == UN) {
+#pragma unroll
+        for (int k = 0; k < N1; ++k) res[f][k] = c[f][k];
+      } else {
+        double mm[N1];
+        limit_slice<P>(phys, l[f], c[f], r[f], mm);
+        to_lag<P>(mm, res[f]);
+      }
+    }
+    // total energy from the limited pressure, 1/(gamma-1) and kinetic energy
+    double K[N1], Km[N1], Em[N1], El[N1];
+#pragma unroll
+    for (int k = 0; k < N1; ++k) {
+      const double kin = res[1][k] * res[1][k] + (D == 2 ? res[2][k] * res[2][k] : 0.0);
+      K[k] = 0.5 * kin / res[0][k];
+    }
+    to_mono<P>(K, Km);
+    to_mono<P>(c[IE], Em);
+    reconstruct_energy<P>(mp, ma, Km, Em, El);
+    to_lag<P>(El, res[IE]);
+  }
+  store(res);
+}
+
+// p0i: flagged elements to their cell average sum_t w_t U_t (w from phi_w / |reference element|)
+struct CellAverageWeights {
+  double w[16];
+};
+template <int NS, int NF>
+__global__ void __launch_bounds__(128) p0i_kernel(const LimArgs la, const int* __restrict__ sens,
+                                                  const CellAverageWeights wt, double* __restrict__ U,
+                                                  const DevScalars* __restrict__ scal) {
+  if (scal && scal->flags) return;
+  const int ld = la.ld, e = blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= la.n_elem || !__ldg(sens + e)) return;
+#pragma unroll
+  for (int f = 0; f < NF; ++f) {
+    double s = 0.0;
+#pragma unroll
+    for (int t = 0; t < NS; ++t) s += wt.w[t] * U[(size_t)(f * NS + t) * ld + e];
+#pragma unroll
+    for (int t = 0; t < NS; ++t) U[(size_t)(f * NS + t) * ld + e] = s;
+  }
+}
+
+// prl: all elements to primitive variables (TO_PRIM) or back, in place
+template <int D, int NS, bool TO_PRIM>
+__global__ void __launch_bounds__(256) convert_state_kernel(const LimArgs la, double* __restrict__ U,
+                                                            const DevScalars* __restrict__ scal) {
+  constexpr int NF = D + 3;
+  if (scal && scal->flags) return;
+  const int ld = la.ld, e = blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= la.n_elem) return;
+#pragma unroll
+  for (int t = 0; t < NS; ++t) {
+    double q[NF];
+#pragma unroll
+    for (int f = 0; f < NF; ++f) q[f] = U[(size_t)(f * NS + t) * ld + e];
+    if (TO_PRIM) cons_to_prim<D>(q);
+    else prim_to_cons<D>(q);
+#pragma unroll
+    for (int f = 0; f < NF; ++f) U[(size_t)(f * NS + t) * ld + e] = q[f];
+  }
+}
+
+}  // namespace dgb

@@ -19,6 +19,8 @@
 #include "device/kernels.cuh"
 #include "device/tile2d.cuh"
 #include "device/limiter2d_tile.cuh"
+#include "device/limiter_gated.cuh"
+#include "device/sensor.h"
 #include "host/host.h"
 
 namespace dgb {
@@ -180,6 +182,13 @@ struct dgb_ctx {
   Consts cs;
   double *A = nullptr, *B = nullptr, *C = nullptr, *DU = nullptr, *X = nullptr, *ref = nullptr;
   int *nbr = nullptr, *perm = nullptr;
+  // sensor-gated limiters (hri, m2i, pri, p0i): sensor work arrays and flags
+  bool gated = false, has_sensors = false;
+  SensorLaunch sl;
+  int* iperm = nullptr;
+  double* smean = nullptr;
+  int* sint = nullptr;          // target, type, processed, mask, list (ld each), count, flags (ld)
+  CellAverageWeights p0w;       // p0i: cell-average weights in internal node order
   DevScalars* scal = nullptr;
   DevScalars* h_scal = nullptr;  // pinned
   cudaEvent_t e0 = nullptr, e1 = nullptr;
@@ -355,9 +364,92 @@ void launch_lim1d(dgb_ctx* c, double* U) {
   cudaMemcpyAsync(U, c->X, c->nstate * sizeof(double), cudaMemcpyDeviceToDevice, c->st);
 }
 
+// sensor-gated limiters: sensors on U, then the per-element passes (U -> X -> U in 2D)
+template <int D, int P>
+int launch_gated(dgb_ctx* c, double* U) {
+  ProfScope ps(c, KC_LIMITER);
+  SensorLaunch s = c->sl;
+  s.U = U;
+  if (int rc = launch_sensors(s, c->st)) return set_error(DGB_ERR_CUDA, std::string("sensors: ") + cudaGetErrorString((cudaError_t)rc));
+  c->counter += 5;
+  const LimArgs la{c->ld, c->ne};
+  const int* sens = s.sens;
+  const int g = (c->ne + 127) / 128;
+  if (c->limiter == DGB_LIM_P0I) {
+    p0i_kernel<(D == 2 ? (P + 1) * (P + 1) : P + 1), D + 3><<<g, 128, 0, c->st>>>(la, sens, c->p0w, U, c->scal);
+    return 0;
+  }
+  const bool pri = c->limiter == DGB_LIM_PRI;
+  if (D == 2) {
+    dim3 grid(g, P + 1);
+    if (c->limiter == DGB_LIM_M2I) {
+      lim_gated_kernel<2, P, 2, 0, false, false><<<grid, 128, 0, c->st>>>(la, sens, U, c->nbr, c->X, c->scal);
+      lim_gated_kernel<2, P, 2, 1, false, false><<<grid, 128, 0, c->st>>>(la, sens, c->X, c->nbr, U, c->scal);
+    } else if (pri) {
+      lim_gated_kernel<2, P, 1, 0, true, false><<<grid, 128, 0, c->st>>>(la, sens, U, c->nbr, c->X, c->scal);
+      lim_gated_kernel<2, P, 1, 1, false, true><<<grid, 128, 0, c->st>>>(la, sens, c->X, c->nbr, U, c->scal);
+    } else {
+      lim_gated_kernel<2, P, 1, 0, false, false><<<grid, 128, 0, c->st>>>(la, sens, U, c->nbr, c->X, c->scal);
+      lim_gated_kernel<2, P, 1, 1, false, false><<<grid, 128, 0, c->st>>>(la, sens, c->X, c->nbr, U, c->scal);
+    }
+    c->counter += 1;
+  } else {
+    if (c->limiter == DGB_LIM_M2I)
+      lim_gated_kernel<1, P, 2, 0, false, false><<<g, 128, 0, c->st>>>(la, sens, U, c->nbr, c->X, c->scal);
+    else if (pri)
+      lim_gated_kernel<1, P, 1, 0, true, true><<<g, 128, 0, c->st>>>(la, sens, U, c->nbr, c->X, c->scal);
+    else
+      lim_gated_kernel<1, P, 1, 0, false, false><<<g, 128, 0, c->st>>>(la, sens, U, c->nbr, c->X, c->scal);
+    cudaMemcpyAsync(U, c->X, c->nstate * sizeof(double), cudaMemcpyDeviceToDevice, c->st);
+  }
+  return 0;
+}
+
+// prl: HR of the primitive variables (all elements converted there and back)
+template <int D, int P>
+void launch_prl(dgb_ctx* c, double* U) {
+  constexpr int NS = D == 2 ? (P + 1) * (P + 1) : P + 1;
+  const LimArgs la{c->ld, c->ne};
+  const int g = (c->ne + 255) / 256;
+  {
+    ProfScope ps(c, KC_LIMITER);
+    convert_state_kernel<D, NS, true><<<g, 256, 0, c->st>>>(la, U, c->scal);
+  }
+  if (D == 2) launch_lim2d<P, 1>(c, U);
+  else launch_lim1d<P, 1>(c, U);
+  {
+    ProfScope ps(c, KC_LIMITER);
+    convert_state_kernel<D, NS, false><<<g, 256, 0, c->st>>>(la, U, c->scal);
+  }
+}
+
 // in-place limiting of a state buffer with the context's limiter
 int limit_dispatch(dgb_ctx* c, double* U) {
   if (c->limiter == 0) return 0;
+  if (c->limiter == DGB_LIM_PRL) {
+    const int k = c->D * 10 + c->p;
+    switch (k) {
+      case 11: launch_prl<1, 1>(c, U); return 0;
+      case 12: launch_prl<1, 2>(c, U); return 0;
+      case 13: launch_prl<1, 3>(c, U); return 0;
+      case 21: launch_prl<2, 1>(c, U); return 0;
+      case 22: launch_prl<2, 2>(c, U); return 0;
+      case 23: launch_prl<2, 3>(c, U); return 0;
+      default: return set_error(DGB_ERR_UNSUPPORTED, "order outside 1..3");
+    }
+  }
+  if (c->gated) {
+    const int k = c->D * 10 + c->p;
+    switch (k) {
+      case 11: return launch_gated<1, 1>(c, U);
+      case 12: return launch_gated<1, 2>(c, U);
+      case 13: return launch_gated<1, 3>(c, U);
+      case 21: return launch_gated<2, 1>(c, U);
+      case 22: return launch_gated<2, 2>(c, U);
+      case 23: return launch_gated<2, 3>(c, U);
+      default: return set_error(DGB_ERR_UNSUPPORTED, "order outside 1..3");
+    }
+  }
   const int key = c->p * 10 + c->limiter;
 #define L2(P, M) case P * 10 + M: launch_lim2d<P, M>(c, U); return 0;
 #define L1(P, M) case P * 10 + M: launch_lim1d<P, M>(c, U); return 0;
@@ -503,8 +595,7 @@ extern "C" int dgb_create(const dgb_problem* prob, int device, dgb_ctx** out) {
   if (!P.gpu_ok) return set_error(DGB_ERR_UNSUPPORTED, P.gpu_reason);
   if (P.D == 2 && P.flux == DGB_FLUX_HLL)
     return set_error(DGB_ERR_UNSUPPORTED, "2D HLL is a stub in the reference (twod_multifluid_fluxes.h:119-141)");
-  if (P.limiter != 0 && P.limiter != 1 && P.limiter != 2)
-    return set_error(DGB_ERR_UNSUPPORTED, "device limiters: none, hrl, m2l");
+  if (P.limiter < 0 || P.limiter > 7) return set_error(DGB_ERR_UNSUPPORTED, "unknown limiter code");
   int ndev = 0;
   if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return set_error(DGB_ERR_NO_DEVICE, "no CUDA device");
   if (device < 0 || device >= ndev) return set_error(DGB_ERR_ARG, "bad device index");
@@ -574,6 +665,38 @@ extern "C" int dgb_create(const dgb_problem* prob, int device, dgb_ctx** out) {
   cudaMemcpy(c->nbr, nb.data(), nb.size() * sizeof(int), cudaMemcpyHostToDevice);
   if ((e = cudaMalloc(&c->perm, c->ns * sizeof(int))) != cudaSuccess) return fail(e, "perm");
   cudaMemcpy(c->perm, P.tensor_perm.data(), c->ns * sizeof(int), cudaMemcpyHostToDevice);
+  c->gated = P.limiter == DGB_LIM_HRI || P.limiter == DGB_LIM_M2I || P.limiter == DGB_LIM_PRI || P.limiter == DGB_LIM_P0I;
+  c->has_sensors = c->gated || !P.thresholds.empty();
+  if (c->has_sensors) {
+    // sensor work arrays; the reference's node order for the cell means; p0i weights
+    if ((e = cudaMalloc(&c->smean, (size_t)c->nf * c->ld * sizeof(double))) != cudaSuccess) return fail(e, "sensor means");
+    if ((e = cudaMalloc(&c->sint, ((size_t)6 * c->ld + 64) * sizeof(int))) != cudaSuccess) return fail(e, "sensor arrays");
+    cudaMemset(c->sint, 0, ((size_t)6 * c->ld + 64) * sizeof(int));
+    std::vector<int> ip(c->ns);
+    for (int t = 0; t < c->ns; ++t) ip[P.tensor_perm[t]] = t;
+    if ((e = cudaMalloc(&c->iperm, c->ns * sizeof(int))) != cudaSuccess) return fail(e, "iperm");
+    cudaMemcpy(c->iperm, ip.data(), c->ns * sizeof(int), cudaMemcpyHostToDevice);
+    SensorLaunch& sl = c->sl;
+    std::memset(&sl, 0, sizeof(sl));
+    sl.D = c->D; sl.ns = c->ns; sl.nf = c->nf; sl.n_elem = c->ne; sl.ld = c->ld; sl.n_nbr = P.N_N;
+    sl.iperm = c->iperm; sl.nbr = c->nbr; sl.mean = c->smean;
+    sl.target = c->sint; sl.type = c->sint + c->ld; sl.processed = c->sint + 2 * (size_t)c->ld;
+    sl.mask = c->sint + 3 * (size_t)c->ld; sl.list = c->sint + 4 * (size_t)c->ld; sl.sens = c->sint + 5 * (size_t)c->ld;
+    sl.count = c->sint + 6 * (size_t)c->ld;
+    for (int k = 0; k < 3; ++k) {
+      sl.on[k] = k < (int)P.thresholds.size();
+      sl.th[k] = sl.on[k] ? P.thresholds[k] : 0.0;
+    }
+    // cell average = sum_g sum_i phi_w[i*N_G + g] U_i / |reference element| (4 for quads; lines: 2)
+    std::memset(&c->p0w, 0, sizeof(c->p0w));
+    const double area = P.D == 2 ? 4.0 : 2.0;
+    for (int t = 0; t < c->ns; ++t) {
+      const int i = P.tensor_perm[t];
+      double w = 0;
+      for (int g = 0; g < P.N_G; ++g) w += P.phi_w[(size_t)i * P.N_G + g];
+      c->p0w.w[t] = w / area;
+    }
+  }
   if ((e = cudaMalloc(&c->scal, sizeof(DevScalars))) != cudaSuccess) return fail(e, "scalars");
   cudaMemset(c->scal, 0, sizeof(DevScalars));
   if ((e = cudaMallocHost(&c->h_scal, sizeof(DevScalars))) != cudaSuccess) return fail(e, "pinned scalars");
@@ -600,6 +723,9 @@ extern "C" void dgb_destroy(dgb_ctx* c) {
   for (double* b : {c->A, c->B, c->C, c->DU, c->X, c->ref}) if (b) cudaFree(b);
   if (c->nbr) cudaFree(c->nbr);
   if (c->perm) cudaFree(c->perm);
+  if (c->iperm) cudaFree(c->iperm);
+  if (c->smean) cudaFree(c->smean);
+  if (c->sint) cudaFree(c->sint);
   if (c->scal) cudaFree(c->scal);
   if (c->h_scal) cudaFreeHost(c->h_scal);
   for (auto ev : c->ev_pool) cudaEventDestroy(ev);
@@ -682,6 +808,19 @@ extern "C" int dgb_limit(dgb_ctx* c, double* U) {
   if (int rc = limit_dispatch(c, c->B)) return rc;
   DGB_CUDA(cudaGetLastError());
   return download(c, c->B, U);
+}
+
+extern "C" int dgb_sensors(dgb_ctx* c, const double* U, int* flags) {
+  if (!c || !U || !flags) return set_error(DGB_ERR_ARG, "null argument");
+  if (!c->has_sensors) return set_error(DGB_ERR_ARG, "the problem has no sensor thresholds");
+  DGB_CUDA(cudaSetDevice(c->device));
+  if (int rc = upload(c, U, c->B)) return rc;
+  SensorLaunch s = c->sl;
+  s.U = c->B;
+  if (int rc = launch_sensors(s, c->st)) return set_error(DGB_ERR_CUDA, std::string("sensors: ") + cudaGetErrorString((cudaError_t)rc));
+  DGB_CUDA(cudaMemcpyAsync(flags, s.sens, (size_t)c->ne * sizeof(int), cudaMemcpyDeviceToHost, c->st));
+  DGB_CUDA(cudaStreamSynchronize(c->st));
+  return DGB_OK;
 }
 
 extern "C" int dgb_dt_from_cfl(dgb_ctx* c, const double* U, double* dt) {

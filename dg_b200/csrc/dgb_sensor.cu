@@ -1,0 +1,202 @@
+// Troubled-cell sensors (contact / shock / gamma-jump), B200 form of SENSOR::sensing
+// (code/src/sensors/sensor.cc:11-35) and calc_sensors (code/src/sensors/sensor_kernels.cu:19-165).
+//
+// The reference visits elements in index order.  An element that an earlier element already
+// flagged skips its own tests; otherwise it tests its neighbours in order (left, right[, bottom,
+// top]) and the first hit flags both cells with the sensor's number and ends its loop; a boundary
+// neighbour flags the element alone with 1.  That order is part of the result, so it is reproduced
+// exactly, in parallel:
+//   1. cell means (the reference's "average solution", a plain nodal mean);
+//   2. per element, the first hit of its own neighbour loop: target T(e) and sensor type;
+//   3. "processed" P(j) = no earlier neighbour i < j with P(i) and T(i) = j.  Only the few elements
+//      that such a forward edge reaches need work; the edges form a DAG (i < j), so in-place sweeps
+//      over that list reach the unique fixed point after at most (longest chain + 1) sweeps, and a
+//      sweep that changes nothing proves it.  One CTA runs the sweeps (the list is short: cells
+//      next to discontinuities); the sweep count is bounded by the list length + 2;
+//   4. each element's final flag = the value of its last writer in index order (itself, when
+//      processed and hit, or any processed neighbour whose target it is).
+// This file is compiled with -fmad=false: the tests below are evaluated with separately rounded
+// multiplies and adds, like the reference on x86-64, so no threshold decision can differ.
+#include <cuda_runtime.h>
+
+#include "device/sensor.h"
+
+namespace dgb {
+namespace {
+
+template <int NS>
+__global__ void __launch_bounds__(256) cell_means_kernel(const double* __restrict__ U, const int* __restrict__ iperm,
+                                                          int n_elem, int nf, int ld, double* __restrict__ M) {
+  const int e = blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= n_elem) return;
+  for (int f = 0; f < nf; ++f) {
+    double s = U[(size_t)(f * NS + iperm[0]) * ld + e];
+#pragma unroll
+    for (int i = 1; i < NS; ++i) s = s + U[(size_t)(f * NS + iperm[i]) * ld + e];
+    M[(size_t)f * ld + e] = s * (1.0 / NS);
+  }
+}
+
+struct Cell {
+  double rho, vx, vy, al, gam, p, ie, a, H;
+};
+
+template <int D>
+__device__ __forceinline__ Cell cell_state(const double* __restrict__ M, int e, int ld) {
+  Cell c;
+  c.rho = M[e];
+  c.vx = M[(size_t)ld + e] / c.rho;
+  c.vy = D == 2 ? M[(size_t)2 * ld + e] / c.rho : 0.0;
+  const double Et = M[(size_t)(D + 1) * ld + e];
+  c.al = M[(size_t)(D + 2) * ld + e];
+  c.gam = 1.0 + 1.0 / c.al;
+  const double pinf = (1 - 1.0 / c.gam) * 0.0;  // stiffened-gas term of the reference, zero here
+  c.p = (c.gam - 1) * (Et - 0.0 - 0.5 * c.rho * (c.vx * c.vx + c.vy * c.vy));
+  c.ie = c.p * c.al;
+  c.a = sqrt((c.gam * (c.p + pinf)) / c.rho);
+  c.H = (Et + c.p) / c.rho;
+  return c;
+}
+
+struct DetectArgs {
+  int n_elem, ld, n_nbr;
+  int on1, on2, on3;
+  double t1, t2, t3;
+};
+
+// first hit of each element's own neighbour loop (calc_sensors, sensor_kernels.cu:48-160)
+template <int D>
+__global__ void __launch_bounds__(256) sensor_detect_kernel(const DetectArgs a, const double* __restrict__ M,
+                                                             const int* __restrict__ nbr, int* __restrict__ T,
+                                                             int* __restrict__ typ) {
+  const int e = blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= a.n_elem) return;
+  const Cell L = cell_state<D>(M, e, a.ld);
+  int target = -1, kind = 0;
+  for (int nn = 0; nn < a.n_nbr; ++nn) {
+    const int r = nbr[(size_t)nn * a.ld + e];
+    if (r < 0) {  // boundary neighbour: flag this element alone
+      kind = 1;
+      break;
+    }
+    const Cell R = cell_state<D>(M, r, a.ld);
+    const double RT = sqrt(R.rho / L.rho);
+    const double vx = (L.vx + RT * R.vx) / (1 + RT);
+    const double vy = (L.vy + RT * R.vy) / (1 + RT);
+    const double alpha = (L.al + RT * R.al) / (1 + RT);
+    const double gamma = 1 + 1.0 / alpha;
+    const double H = (L.H + RT * R.H) / (1 + RT);
+    const double c = sqrt((gamma - 1) * (H - 0.5 * (vx * vx + vy * vy)));
+    const double i = (L.ie + RT * R.ie) / (1 + RT);
+    if (a.on1) {  // contact sensor on the density wave strength
+      const double drho = R.rho - L.rho;
+      const double dp = (gamma - 1) * (gamma - 1) * (alpha * (R.ie - L.ie) - i * (R.al - L.al));
+      const double dV2 = drho - dp / (c * c);
+      const double G = fabs(dV2) / (L.rho + R.rho);
+      const double PHI = 2 * G / ((1 + G) * (1 + G));
+      if (PHI > a.t1) { target = r; kind = 1; break; }
+    }
+    if (a.on2) {  // shock sensor: converging acoustic characteristics and a pressure jump
+      if (((L.vx - L.a > vx - c) && (vx - c > R.vx - R.a)) || ((L.vy - L.a > vy - c) && (vy - c > R.vy - R.a))) {
+        const double PSI = fabs(R.p - L.p) / (L.p + R.p);
+        const double W = 2 * PSI / ((1 + PSI) * (1 + PSI));
+        if (W > a.t2) { target = r; kind = 2; break; }
+      }
+    }
+    if (a.on3) {  // contact sensor on the gamma jump
+      const double G = fabs(R.gam - L.gam) / (L.gam + R.gam);
+      const double PHI = 2 * G / ((1 + G) * (1 + G));
+      if (PHI > a.t3) { target = r; kind = 3; break; }
+    }
+  }
+  T[e] = target;
+  typ[e] = kind;
+}
+
+// forward edges i -> j (i < j, T(i) = j): mask of the neighbour slots they come from
+__global__ void __launch_bounds__(256) sensor_edges_kernel(int n_elem, int ld, int n_nbr, const int* __restrict__ nbr,
+                                                            const int* __restrict__ T, int* __restrict__ P,
+                                                            int* __restrict__ mask, int* __restrict__ list,
+                                                            int* __restrict__ count) {
+  const int j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= n_elem) return;
+  int m = 0;
+  for (int k = 0; k < n_nbr; ++k) {
+    const int i = nbr[(size_t)k * ld + j];
+    if (i >= 0 && i < j && T[i] == j) m |= 1 << k;
+  }
+  P[j] = 1;
+  mask[j] = m;
+  if (m) list[atomicAdd(count, 1)] = j;
+}
+
+// P(j) = not (any forward predecessor i with P(i)); in-place sweeps until nothing changes
+__global__ void __launch_bounds__(1024) sensor_resolve_kernel(int ld, int n_nbr, const int* __restrict__ nbr,
+                                                               const int* __restrict__ mask,
+                                                               const int* __restrict__ list,
+                                                               const int* __restrict__ count, volatile int* P) {
+  __shared__ int changed;
+  const int n = *count;
+  for (int sweep = 0; sweep < n + 2; ++sweep) {
+    if (threadIdx.x == 0) changed = 0;
+    __syncthreads();
+    for (int idx = threadIdx.x; idx < n; idx += blockDim.x) {
+      const int j = list[idx];
+      const int m = mask[j];
+      int any = 0;
+      for (int k = 0; k < n_nbr; ++k)
+        if ((m >> k) & 1) any |= P[nbr[(size_t)k * ld + j]];
+      const int np = any ? 0 : 1;
+      if (np != P[j]) {
+        P[j] = np;
+        changed = 1;
+      }
+    }
+    __syncthreads();
+    const int done = (changed == 0);
+    __syncthreads();
+    if (done) return;
+  }
+}
+
+// final flag = the value of the last writer in index order
+__global__ void __launch_bounds__(256) sensor_finalize_kernel(int n_elem, int ld, int n_nbr,
+                                                               const int* __restrict__ nbr, const int* __restrict__ T,
+                                                               const int* __restrict__ typ,
+                                                               const int* __restrict__ P, int* __restrict__ sens) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= n_elem) return;
+  int last = -1, val = 0;
+  if (P[k] && typ[k]) { last = k; val = typ[k]; }
+  for (int s = 0; s < n_nbr; ++s) {
+    const int i = nbr[(size_t)s * ld + k];
+    if (i >= 0 && i > last && P[i] && typ[i] && T[i] == k) { last = i; val = typ[i]; }
+  }
+  sens[k] = val;
+}
+
+}  // namespace
+
+int launch_sensors(const SensorLaunch& s, cudaStream_t st) {
+  const int g = (s.n_elem + 255) / 256;
+  switch (s.ns) {
+    case 2: cell_means_kernel<2><<<g, 256, 0, st>>>(s.U, s.iperm, s.n_elem, s.nf, s.ld, s.mean); break;
+    case 3: cell_means_kernel<3><<<g, 256, 0, st>>>(s.U, s.iperm, s.n_elem, s.nf, s.ld, s.mean); break;
+    case 4: cell_means_kernel<4><<<g, 256, 0, st>>>(s.U, s.iperm, s.n_elem, s.nf, s.ld, s.mean); break;
+    case 9: cell_means_kernel<9><<<g, 256, 0, st>>>(s.U, s.iperm, s.n_elem, s.nf, s.ld, s.mean); break;
+    case 16: cell_means_kernel<16><<<g, 256, 0, st>>>(s.U, s.iperm, s.n_elem, s.nf, s.ld, s.mean); break;
+    default: return (int)cudaErrorInvalidValue;
+  }
+  DetectArgs a{s.n_elem, s.ld, s.n_nbr, s.on[0], s.on[1], s.on[2], s.th[0], s.th[1], s.th[2]};
+  if (s.D == 2) sensor_detect_kernel<2><<<g, 256, 0, st>>>(a, s.mean, s.nbr, s.target, s.type);
+  else sensor_detect_kernel<1><<<g, 256, 0, st>>>(a, s.mean, s.nbr, s.target, s.type);
+  cudaError_t e = cudaMemsetAsync(s.count, 0, sizeof(int), st);
+  if (e != cudaSuccess) return (int)e;
+  sensor_edges_kernel<<<g, 256, 0, st>>>(s.n_elem, s.ld, s.n_nbr, s.nbr, s.target, s.processed, s.mask, s.list,
+                                         s.count);
+  sensor_resolve_kernel<<<1, 1024, 0, st>>>(s.ld, s.n_nbr, s.nbr, s.mask, s.list, s.count, s.processed);
+  sensor_finalize_kernel<<<g, 256, 0, st>>>(s.n_elem, s.ld, s.n_nbr, s.nbr, s.target, s.type, s.processed, s.sens);
+  return (int)cudaGetLastError();
+}
+
+}  // namespace dgb

@@ -154,6 +154,12 @@ class DGSolver:
         F.check(F.lib().dgb_limit(self._h, F.dptr(V)))
         return V
 
+    def sensors(self, U) -> np.ndarray:
+        """Troubled-cell flags of U (SENSOR::sensing): 0 or the number of the sensor that fired."""
+        flags = np.zeros(self.problem.info.n_elem, np.int32)
+        F.check(F.lib().dgb_sensors(self._h, F.dptr(self._arr(U)), flags.ctypes.data_as(C.POINTER(C.c_int))))
+        return flags
+
     def dt_from_cfl(self, U) -> float:
         dt = C.c_double()
         F.check(F.lib().dgb_dt_from_cfl(self._h, F.dptr(self._arr(U)), C.byref(dt)))

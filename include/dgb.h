@@ -14,7 +14,8 @@
  *   2. Device context (CUDA, sm_100a).  Replaces the reference's device-side path:
  *      DG_SOLVER::dg_solver (code/src/dg/dg_solver.h:292), Lsolver
  *      (code/src/time_integration/rk_kernels.cu:182), Limiting::HRlimiting/M2limiting
- *      (code/src/limiting/limiting.cc:11, 123), RK::DtFromCFL (code/src/time_integration/rk.cc:250)
+ *      (code/src/limiting/limiting.cc:11, 123, 596-742), SENSOR::sensing (code/src/sensors/sensor.cc:11),
+ *      RK::DtFromCFL (code/src/time_integration/rk.cc:250)
  *      and RK::RK_integration (rk.cc:11).
  *
  * Conventions (all entry points):
@@ -166,6 +167,11 @@ int dgb_residual(dgb_ctx* c, const double* U_host, double* f_host);
 int dgb_solve(dgb_ctx* c, double dt, const double* U_host, double* DU_host);
 /* In-place limiting with the problem's limiter (Limiting::*limiting, limiting.cc). */
 int dgb_limit(dgb_ctx* c, double* U_host);
+/* Troubled-cell flags of U with the deck's sensor thresholds (SENSOR::sensing, sensor.cc:11 with
+ * calc_sensors, sensor_kernels.cu:19): flags[e] = 0 (not flagged) or 1..3 (contact, shock, gamma
+ * sensor), identical to the reference's sequential CPU evaluation.  Needs thresholds in the
+ * problem or a sensor-gated limiter (hri, m2i, pri, p0i). */
+int dgb_sensors(dgb_ctx* c, const double* U_host, int* flags_host);
 /* Dt = CFL_scaled / max_nodes(|u|+a) (RK::DtFromCFL, rk.cc:250-272). */
 int dgb_dt_from_cfl(dgb_ctx* c, const double* U_host, double* dt);
 

@@ -107,3 +107,10 @@ def test_tiled_kernel_matches_generic_kernel(flux, limiter, order, monkeypatch):
     assert rel_err(tiled.get_state(), generic.get_state()) < 1e-12
     tiled.close()
     generic.close()
+
+
+@pytest.mark.parametrize("name", [c for c in CASES if "thresholds" in load_golden(c)[0]])
+def test_sensors(solvers, name):
+    """Troubled-cell flags equal the reference's exactly (integer output)."""
+    meta, d, s = solvers(name)
+    assert np.array_equal(s.sensors(d["Uraw"]), d["sens"])
