@@ -212,6 +212,8 @@ def main(argv=None) -> int:
     ap.add_argument("--e2e-steps", type=int, default=10)
     ap.add_argument("--nx", type=int, default=NX, help="elements in x (profiling cases; default the workload)")
     ap.add_argument("--ny", type=int, default=NY)
+    ap.add_argument("--form", default="fp64", choices=["fp64", "mixed"],
+                    help="arithmetic of the residual (fp64: the plain parity form)")
     args = ap.parse_args(argv)
     if args.impl == "reference":
         return run_reference(args)
@@ -229,6 +231,7 @@ def main(argv=None) -> int:
 
     prob, U0 = build_problem(args.nx, args.ny)
     solver = dgb.DGSolver(prob, device=dev)
+    solver.set_form(args.form)
     U0 = solver.limit(U0)  # the reference limits the initial condition when CFL > 0 (rk.cc:108-114)
     solver.set_state(U0)
     dof = prob.info.n_elem * prob.info.n_s * prob.info.n_fields
@@ -304,13 +307,16 @@ def main(argv=None) -> int:
     if rank == 0 and ws == 1 and not args.no_cpu_baseline and (args.nx, args.ny) == (NX, NY):
         cpu = cpu_baseline(U0)
 
+    form_cfg = {"form": "plain FP64" if args.form == "fp64" else
+                "mixed: FP32 contractions/Rusanov flux on FP64 anchors, FP64 pressure, state and update"}
     if rank == 0:
         line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": dev_ms / args.steps, "higher_is_better": True,
-                "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-                "config": config() if (args.nx, args.ny) == (NX, NY) else config(
+                "scaling": "weak", "vs_baseline": None, "dtype": "f64" if args.form == "fp64" else "f64+f32",
+                "data": "synthetic",
+                "config": config(form_cfg) if (args.nx, args.ny) == (NX, NY) else config(
                     {"workload": f"profiling case {args.nx}x{args.ny} (not the benchmark workload)",
-                     "n_elem": args.nx * args.ny, "dof": dof}),
+                     "n_elem": args.nx * args.ny, "dof": dof, **form_cfg}),
                 "e2e": e2e,
                 "roofline": {"bound": "hbm", "achieved": achieved_gbs, "peak": peak, "unit": "GB/s",
                              "frac": achieved_gbs / peak, "traffic": traffic,

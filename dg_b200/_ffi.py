@@ -14,6 +14,7 @@ OK, ERR_ARG, ERR_IO, ERR_MESH, ERR_UNSUPPORTED, ERR_CUDA, ERR_NONFINITE, ERR_DT_
 FLUX = {"rusanov": 0, "rus": 0, "llf": 0, "hll": 1, "roe": 2}
 LIMITER = {"none": 0, "hrl": 1, "m2l": 2, "hri": 3, "m2i": 4, "prl": 5, "pri": 6, "p0i": 7}
 SSPRK3, RK4 = 3, 4
+FORM = {"fp64": 0, "mixed": 1}
 BC = {"periodic": 1, "transmissive": 2, "reflective": 3, "frozen": 4}
 
 # every exported entry point of include/dgb.h
@@ -24,7 +25,7 @@ EXPORTS = [
     "dgb_destroy", "dgb_set_state", "dgb_get_state", "dgb_set_state_device", "dgb_get_state_device",
     "dgb_residual", "dgb_solve", "dgb_limit", "dgb_dt_from_cfl", "dgb_advance", "dgb_last_dt",
     "dgb_conservation", "dgb_last_timing", "dgb_set_profiling", "dgb_kernel_timing", "dgb_limit_noalloc",
-    "dgb_sensors",
+    "dgb_sensors", "dgb_set_form",
 ]
 
 
@@ -87,6 +88,7 @@ def lib() -> C.CDLL:
         "dgb_solve": [vp, C.c_double, dp, dp],
         "dgb_limit": [vp, dp],
         "dgb_sensors": [vp, dp, C.POINTER(C.c_int)],
+        "dgb_set_form": [vp, ip],
         "dgb_dt_from_cfl": [vp, dp, dp],
         "dgb_advance": [vp, ip, ip, C.c_double, dp],
         "dgb_last_dt": [vp, dp],

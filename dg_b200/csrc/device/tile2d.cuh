@@ -85,13 +85,21 @@ struct TileDims {
 
 enum { FLAG_TIMEOUT = 4u };
 
+// Unrolling of the outer quadrature-column loop of the volume terms.  Fully unrolled, the
+// straight-line kernel body outgrows the instruction cache once several warps per scheduler run
+// different parts of it; kept rolled, the column index is warp-uniform and the tables stay
+// constant-bank operands.
+#ifndef DGB_VOL_UNROLL
+#define DGB_VOL_UNROLL 1
+#endif
+constexpr int kVolUnroll = DGB_VOL_UNROLL;
+
 template <int P, int FLUX, int MODE, int TW, int TH>
 __global__ void __launch_bounds__(TW * TH, 2)
     residual2d_tile_kernel(const TileArgs a, const __grid_constant__ CUtensorMap mapU,
                            const __grid_constant__ CUtensorMap mapB) {
   using Dm = TileDims<P, TW, TH>;
   constexpr int N1 = Dm::N1, NS = Dm::NS, NF = 5, NT = Dm::NT, NXF = Dm::NXF, NYF = Dm::NYF;
-  constexpr int NG = Tab2<P>::NG;
   extern __shared__ __align__(128) unsigned char smraw[];
   uint64_t* bar = reinterpret_cast<uint64_t*>(smraw);
   int* s_ok = reinterpret_cast<int*>(smraw + 8);
@@ -287,7 +295,7 @@ __global__ void __launch_bounds__(TW * TH, 2)
   // volume terms: collocation sum-factorised (x-contraction per quadrature column gx, then y per
   // point), lift accumulated per point with the tensor-product derivative tables
   const double* us = Us + tid;  // thread-private column of the tile: us[(f*NS + t)*NT]
-#pragma unroll
+#pragma unroll(kVolUnroll)
   for (int gx = 0; gx < NG1; ++gx) {
     double Tc[NF][N1], dT[N1];  // column values: sum_ix l_ix(x_gx) u(ix, iy), and of l' for alpha
 #pragma unroll

@@ -20,6 +20,7 @@
 #include "device/tile2d.cuh"
 #include "device/limiter2d_tile.cuh"
 #include "device/limiter_gated.cuh"
+#include "device/tile2d_mixed.cuh"
 #include "device/sensor.h"
 #include "host/host.h"
 
@@ -151,6 +152,28 @@ Tab2<P> make_tab2(const Consts& c) {
   return T;
 }
 
+template <int P>
+Tab2f<P> make_tab2f(const Tab2<P>& d) {
+  Tab2f<P> T;
+  std::memset(&T, 0, sizeof(T));
+  constexpr int N1 = Tab2<P>::N1, NG1 = Tab2<P>::NG1, NS = Tab2<P>::NS, NG = Tab2<P>::NG;
+  for (int g = 0; g < NG; ++g) {
+    T.W[g] = (float)d.W[g];
+    for (int t = 0; t < NS; ++t) {
+      T.dPx[g][t] = (float)d.dPx[g][t];
+      T.dPy[g][t] = (float)d.dPy[g][t];
+      T.Phi[g][t] = (float)d.Phi[g][t];
+    }
+  }
+  for (int i = 0; i < N1; ++i) {
+    T.wf[i] = (float)d.wf[i];
+    for (int j = 0; j < N1; ++j) { T.Bf[i][j] = (float)d.Bf[i][j]; T.M1i[i][j] = (float)d.M1i[i][j]; }
+  }
+  for (int g = 0; g < NG1; ++g)
+    for (int i = 0; i < N1; ++i) { T.B1[g][i] = (float)d.B1[g][i]; T.D1[g][i] = (float)d.D1[g][i]; }
+  return T;
+}
+
 // structured row-major grid test: interior neighbours are e-1, e+1, e-nx, e+nx
 bool is_row_major_grid(const Problem& P) {
   if (P.D != 2 || P.nx <= 0 || P.ny <= 0 || (long)P.nx * P.ny != P.N_E) return false;
@@ -175,6 +198,7 @@ struct dgb_ctx {
   int D = 1, p = 1, nf = 4, ns = 2, ne = 0, ld = 0, flux = 2, limiter = 0;
   int nx = 0, ny = 0;
   bool tiled = false;     // structured row-major grid with tile-multiple extents: tiled residual kernel
+  int form = DGB_FORM_FP64;  // arithmetic of the residual: plain FP64 or mixed FP32/FP64
   bool rowmajor = false;  // structured row-major grid: tiled limiter passes
   CUtensorMap mapA, mapB, mapC;  // TMA descriptors of the state buffers (tiled kernel)
   double hx = 0, hy = 0;
@@ -284,6 +308,30 @@ void launch_tile2d(dgb_ctx* c, const StageArgs& s) {
   k<<<grid, TILE_W * TILE_H, smem, c->st>>>(a, mu, mb);
 }
 
+template <int P, int FLUX, int MODE>
+void launch_tile2d_mixed(dgb_ctx* c, const StageArgs& s) {
+  constexpr size_t smem = TileDimsMixed<P, TILE_W, TILE_H>::smem_bytes;
+  auto k = residual2d_tile_mixed_kernel<P, FLUX, MODE, TILE_W, TILE_H>;
+  static bool attr = false;
+  if (!attr) { cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem); attr = true; }
+  TileArgs a;
+  a.U = s.U; a.Ubase = s.Ubase; a.out = s.out; a.Uacc = s.Uacc; a.nbr = s.nbr; a.scal = s.scal;
+  a.errflag = &c->scal->flags;
+  a.a = s.a; a.b = s.b; a.dt_override = s.dt_override;
+  a.J = c->cs.J;
+  a.invJ = 1.0 / c->cs.J;
+  a.cx = c->cs.J * c->cs.ixx;
+  a.cy = c->cs.J * c->cs.iyy;
+  a.sx = c->cs.ixx;
+  a.sy = c->cs.iyy;
+  a.JFx = c->cs.JFx;
+  a.JFy = c->cs.JFy;
+  a.nx = c->nx; a.ny = c->ny; a.ld = c->ld;
+  dim3 grid(c->nx / TILE_W, c->ny / TILE_H);
+  ProfScope ps(c, KC_RESIDUAL);
+  k<<<grid, TILE_W * TILE_H, smem, c->st>>>(a, map_of(c, s.U));
+}
+
 // TMA descriptor of a state buffer viewed as (x: nx, y: ny, z: N_F*N_s rows of stride ld)
 bool encode_state_map(dgb_ctx* c, double* ptr, CUtensorMap* map) {
   static PFN_cuTensorMapEncodeTiled_v12000 encode = nullptr;
@@ -307,6 +355,16 @@ bool encode_state_map(dgb_ctx* c, double* ptr, CUtensorMap* map) {
 
 template <int MODE>
 int residual_dispatch(dgb_ctx* c, const StageArgs& a) {
+  if (c->tiled && c->form == DGB_FORM_MIXED) {
+    const int key = c->p * 10 + c->flux;
+    switch (key) {
+      case 10: launch_tile2d_mixed<1, 0, MODE>(c, a); return 0;
+      case 12: launch_tile2d_mixed<1, 2, MODE>(c, a); return 0;
+      case 20: launch_tile2d_mixed<2, 0, MODE>(c, a); return 0;
+      case 22: launch_tile2d_mixed<2, 2, MODE>(c, a); return 0;
+      default: return set_error(DGB_ERR_UNSUPPORTED, "mixed form: p = 1, 2 with Rusanov or Roe");
+    }
+  }
   if (c->tiled) {
     const int key = c->p * 10 + c->flux;
     switch (key) {
@@ -637,9 +695,24 @@ extern "C" int dgb_create(const dgb_problem* prob, int device, dgb_ctx** out) {
   }
   if (P.D == 2) {
     cudaError_t et = cudaSuccess;
-    if (P.p == 1) { auto t = make_tab2<1>(c->cs); et = cudaMemcpyToSymbol(c_tab2_p1, &t, sizeof(t)); }
-    if (P.p == 2) { auto t = make_tab2<2>(c->cs); et = cudaMemcpyToSymbol(c_tab2_p2, &t, sizeof(t)); }
-    if (P.p == 3) { auto t = make_tab2<3>(c->cs); et = cudaMemcpyToSymbol(c_tab2_p3, &t, sizeof(t)); }
+    if (P.p == 1) {
+      auto t = make_tab2<1>(c->cs);
+      auto tf = make_tab2f<1>(t);
+      et = cudaMemcpyToSymbol(c_tab2_p1, &t, sizeof(t));
+      if (et == cudaSuccess) et = cudaMemcpyToSymbol(c_tab2f_p1, &tf, sizeof(tf));
+    }
+    if (P.p == 2) {
+      auto t = make_tab2<2>(c->cs);
+      auto tf = make_tab2f<2>(t);
+      et = cudaMemcpyToSymbol(c_tab2_p2, &t, sizeof(t));
+      if (et == cudaSuccess) et = cudaMemcpyToSymbol(c_tab2f_p2, &tf, sizeof(tf));
+    }
+    if (P.p == 3) {
+      auto t = make_tab2<3>(c->cs);
+      auto tf = make_tab2f<3>(t);
+      et = cudaMemcpyToSymbol(c_tab2_p3, &t, sizeof(t));
+      if (et == cudaSuccess) et = cudaMemcpyToSymbol(c_tab2f_p3, &tf, sizeof(tf));
+    }
     if (et != cudaSuccess) { delete c; return set_error(DGB_ERR_CUDA, std::string("constant tables: ") + cudaGetErrorString(et)); }
   }
   auto fail = [&](cudaError_t e, const char* what) {
@@ -808,6 +881,23 @@ extern "C" int dgb_limit(dgb_ctx* c, double* U) {
   if (int rc = limit_dispatch(c, c->B)) return rc;
   DGB_CUDA(cudaGetLastError());
   return download(c, c->B, U);
+}
+
+extern "C" int dgb_set_form(dgb_ctx* c, int form) {
+  if (!c) return set_error(DGB_ERR_ARG, "null argument");
+  if (form != DGB_FORM_FP64 && form != DGB_FORM_MIXED) return set_error(DGB_ERR_ARG, "unknown form");
+  if (form == DGB_FORM_MIXED && !(c->tiled && c->p <= 2))
+    return set_error(DGB_ERR_UNSUPPORTED,
+                     "the mixed form needs a structured 2D grid with extents multiples of 32 x 4 and p <= 2");
+  if (form != c->form) {
+    DGB_CUDA(cudaSetDevice(c->device));
+    DGB_CUDA(cudaStreamSynchronize(c->st));
+    for (auto& row : c->graphs)
+      for (auto& g : row)
+        if (g) { cudaGraphExecDestroy(g); g = nullptr; }
+    c->form = form;
+  }
+  return DGB_OK;
 }
 
 extern "C" int dgb_sensors(dgb_ctx* c, const double* U, int* flags) {

@@ -154,6 +154,11 @@ class DGSolver:
         F.check(F.lib().dgb_limit(self._h, F.dptr(V)))
         return V
 
+    def set_form(self, form: str) -> None:
+        """Arithmetic of the residual: "fp64" (plain, the parity form) or "mixed" (FP32 contractions
+        and fluxes on FP64 anchors, FP64 pressure recovery and stage update)."""
+        F.check(F.lib().dgb_set_form(self._h, F.FORM[form]))
+
     def sensors(self, U) -> np.ndarray:
         """Troubled-cell flags of U (SENSOR::sensing): 0 or the number of the sensor that fired."""
         flags = np.zeros(self.problem.info.n_elem, np.int32)

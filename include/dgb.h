@@ -62,6 +62,11 @@ enum dgb_limiter {
   DGB_LIM_M2I = 4, DGB_LIM_PRL = 5, DGB_LIM_PRI = 6, DGB_LIM_P0I = 7
 };
 
+/* Arithmetic of the residual kernels.  FP64: plain double precision (the parity form).  MIXED:
+ * basis contractions, Rusanov flux and lift in FP32 on deviations from a per-element FP64 anchor;
+ * state, pressure recovery, Roe solver and stage update in FP64 (structured 2D grids, p <= 2). */
+enum dgb_form { DGB_FORM_FP64 = 0, DGB_FORM_MIXED = 1 };
+
 /* Time integrators: classical RK4 (reference rk.h:44-57) and Shu-Osher SSP-RK3 (new). */
 enum dgb_scheme { DGB_SSPRK3 = 3, DGB_RK4 = 4 };
 
@@ -172,6 +177,9 @@ int dgb_limit(dgb_ctx* c, double* U_host);
  * sensor), identical to the reference's sequential CPU evaluation.  Needs thresholds in the
  * problem or a sensor-gated limiter (hri, m2i, pri, p0i). */
 int dgb_sensors(dgb_ctx* c, const double* U_host, int* flags_host);
+/* Selects the arithmetic of the residual kernels (enum dgb_form) for later calls; no counterpart
+ * in the reference, which is FP64 only. */
+int dgb_set_form(dgb_ctx* c, int form);
 /* Dt = CFL_scaled / max_nodes(|u|+a) (RK::DtFromCFL, rk.cc:250-272). */
 int dgb_dt_from_cfl(dgb_ctx* c, const double* U_host, double* dt);
 

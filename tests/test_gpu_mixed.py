@@ -1,0 +1,74 @@
+"""The mixed-precision form (FP32 contractions / Rusanov flux on FP64 anchors, FP64 pressure
+recovery, Roe solver and stage update) against the plain FP64 form.
+
+Per operator, the mixed residual must stay within 1e-5 of the FP64 residual per field (relative to
+that field's max |f|, momentum components scaled together); after 50 SSP-RK3 steps of the shock-bubble the per-field relative L1 error
+of the state must stay below 1e-6.  Both are printed per field.
+"""
+import numpy as np
+import pytest
+
+from conftest import perturbed_state
+
+pytestmark = pytest.mark.gpu
+WALLS = ("reflective", "transmissive", "reflective", "transmissive")
+
+
+def per_field(a, b, info, norm="max"):
+    """Per-field error of a against b; the two momentum components are scaled together (by the
+    momentum magnitude), since one of them is nearly zero in these flows."""
+    A = np.asarray(a).reshape(info.n_elem, info.n_fields, info.n_s)
+    B = np.asarray(b).reshape(info.n_elem, info.n_fields, info.n_s)
+    red = (lambda x: np.abs(x).max()) if norm == "max" else (lambda x: np.abs(x).sum())
+    out = []
+    for f in range(info.n_fields):
+        scale = red(B[:, f]) if f not in (1, 2) else max(red(B[:, 1]), red(B[:, 2]))
+        out.append(float(red(A[:, f] - B[:, f]) / scale))
+    return out
+
+
+@pytest.mark.parametrize("flux,order", [("rusanov", 2), ("roe", 2), ("rusanov", 1)])
+def test_mixed_residual_close_to_fp64(flux, order):
+    import dg_b200 as dgb
+    prob = dgb.Problem.structured(2, order, 64, 32, 0.0, 2.0, 0.0, 1.0, WALLS, flux=flux, limiter="m2l", cfl=0.3)
+    s = dgb.DGSolver(prob)
+    try:
+        U0 = s.limit(perturbed_state(prob, "shock_bubble", 5))
+        f64 = s.dg_solver(U0)
+        s.set_form("mixed")
+        fmx = s.dg_solver(U0)
+        err = per_field(fmx, f64, prob.info)
+        print(f"mixed residual, per-field max error / max |f| ({flux}, p={order}):", err)
+        assert max(err) < 1e-5
+    finally:
+        s.close()
+
+
+def test_mixed_steps_close_to_fp64():
+    import dg_b200 as dgb
+    prob = dgb.Problem.structured(2, 2, 128, 64, 0.0, 2.0, 0.0, 1.0, WALLS, flux="rusanov", limiter="m2l", cfl=0.3)
+    ref = dgb.DGSolver(prob)
+    mix = dgb.DGSolver(prob)
+    try:
+        U0 = ref.limit(prob.init_state("shock_bubble", seed=7))
+        mix.set_form("mixed")
+        for s in (ref, mix):
+            s.set_state(U0)
+            s.advance(50, 0.0, scheme=dgb.SSPRK3)
+        err = per_field(mix.get_state(), ref.get_state(), prob.info, norm="l1")
+        print("mixed vs FP64 after 50 SSP-RK3 steps, per-field relative L1:", err)
+        assert max(err) < 1e-6
+    finally:
+        ref.close()
+        mix.close()
+
+
+def test_mixed_form_rejected_where_not_built():
+    import dg_b200 as dgb
+    prob = dgb.Problem.structured(2, 3, 64, 32, flux="roe", limiter="m2l")
+    s = dgb.DGSolver(prob)
+    try:
+        with pytest.raises(dgb.DGBError):
+            s.set_form("mixed")
+    finally:
+        s.close()
