@@ -93,6 +93,13 @@ enum { FLAG_TIMEOUT = 4u };
 #define DGB_VOL_UNROLL 1
 #endif
 constexpr int kVolUnroll = DGB_VOL_UNROLL;
+// Lift of the volume terms: sum-factorised (1) -- per quadrature column, contract over the
+// points of the column first, then one rank-1 update per node -- or direct (0) with the
+// tensor-product tables dPx, dPy, Phi.
+#ifndef DGB_SF_LIFT
+#define DGB_SF_LIFT 1
+#endif
+constexpr bool kSfLift = DGB_SF_LIFT != 0;
 
 template <int P, int FLUX, int MODE, int TW, int TH>
 __global__ void __launch_bounds__(TW * TH, 2)
@@ -312,6 +319,13 @@ __global__ void __launch_bounds__(TW * TH, 2)
       for (int ix = 0; ix < N1; ++ix) sd += DGB_TAB2(P, D1[gx][ix]) * us[(4 * NS + ix + N1 * iy) * NT];
       dT[iy] = sd;
     }
+    double Ax[4][N1], Ay[4][N1], As[N1];  // column sums of the sum-factorised lift
+#pragma unroll
+    for (int iy = 0; iy < N1; ++iy) {
+      As[iy] = 0.0;
+#pragma unroll
+      for (int f = 0; f < 4; ++f) Ax[f][iy] = Ay[f][iy] = 0.0;
+    }
 #pragma unroll
     for (int gy = 0; gy < NG1; ++gy) {
       const int g = gx * NG1 + gy;
@@ -334,12 +348,35 @@ __global__ void __launch_bounds__(TW * TH, 2)
       const double gxv[4] = {mx, mx * uu + wx * p, mx * vv, wx * ((Et + p) * uu)};
       const double gyv[4] = {my, my * uu, my * vv + wy * p, wy * ((Et + p) * vv)};
       const double gs = (DGB_TAB2(P, W[g]) * a.J) * (-uu * dax * a.sx - vv * day * a.sy);
+      if constexpr (kSfLift) {
 #pragma unroll
-      for (int t = 0; t < NS; ++t) {
+        for (int iy = 0; iy < N1; ++iy) {
+          const double b = DGB_TAB2(P, B1[gy][iy]), d = DGB_TAB2(P, D1[gy][iy]);
 #pragma unroll
-        for (int f = 0; f < 4; ++f) r[f][t] += DGB_TAB2(P, dPx[g][t]) * gxv[f] + DGB_TAB2(P, dPy[g][t]) * gyv[f];
-        r[4][t] += DGB_TAB2(P, Phi[g][t]) * gs;
+          for (int f = 0; f < 4; ++f) { Ax[f][iy] += b * gxv[f]; Ay[f][iy] += d * gyv[f]; }
+          As[iy] += b * gs;
+        }
+      } else {
+#pragma unroll
+        for (int t = 0; t < NS; ++t) {
+#pragma unroll
+          for (int f = 0; f < 4; ++f) r[f][t] += DGB_TAB2(P, dPx[g][t]) * gxv[f] + DGB_TAB2(P, dPy[g][t]) * gyv[f];
+          r[4][t] += DGB_TAB2(P, Phi[g][t]) * gs;
+        }
       }
+    }
+    if constexpr (kSfLift) {
+      // dPx = l'_ix(x_gx) l_iy(x_gy), dPy = l_ix(x_gx) l'_iy(x_gy), Phi = l_ix(x_gx) l_iy(x_gy)
+#pragma unroll
+      for (int iy = 0; iy < N1; ++iy)
+#pragma unroll
+        for (int ix = 0; ix < N1; ++ix) {
+          const double dx = DGB_TAB2(P, D1[gx][ix]), bx = DGB_TAB2(P, B1[gx][ix]);
+          const int t = ix + N1 * iy;
+#pragma unroll
+          for (int f = 0; f < 4; ++f) r[f][t] += dx * Ax[f][iy] + bx * Ay[f][iy];
+          r[4][t] += bx * As[iy];
+        }
     }
   }
   if (MODE == MODE_RESIDUAL) {

@@ -273,6 +273,13 @@ __global__ void __launch_bounds__(TW * TH, 3)
         sd += DGB_TAB2F(P, D1[gx][ix]) * (float)(us[(4 * NS + ix + N1 * iy) * NT] - anc[4]);
       dT[iy] = sd;
     }
+    float Ax[4][N1], Ay[4][N1], As[N1];
+#pragma unroll
+    for (int iy = 0; iy < N1; ++iy) {
+      As[iy] = 0.f;
+#pragma unroll
+      for (int f = 0; f < 4; ++f) Ax[f][iy] = Ay[f][iy] = 0.f;
+    }
 #pragma unroll
     for (int gy = 0; gy < NG1; ++gy) {
       const int g = gx * NG1 + gy;
@@ -299,12 +306,34 @@ __global__ void __launch_bounds__(TW * TH, 3)
       const float gxv[4] = {mx, mx * uu + wx * p, mx * vv, wx * ((Et + p) * uu)};
       const float gyv[4] = {my, my * uu, my * vv + wy * p, wy * ((Et + p) * vv)};
       const float gs = (wq * cJ) * (-uu * dax * sx - vv * day * sy);
+      if constexpr (kSfLift) {
 #pragma unroll
-      for (int t = 0; t < NS; ++t) {
+        for (int iy = 0; iy < N1; ++iy) {
+          const float b = DGB_TAB2F(P, B1[gy][iy]), d = DGB_TAB2F(P, D1[gy][iy]);
 #pragma unroll
-        for (int f = 0; f < 4; ++f) r[f][t] += DGB_TAB2F(P, dPx[g][t]) * gxv[f] + DGB_TAB2F(P, dPy[g][t]) * gyv[f];
-        r[4][t] += DGB_TAB2F(P, Phi[g][t]) * gs;
+          for (int f = 0; f < 4; ++f) { Ax[f][iy] += b * gxv[f]; Ay[f][iy] += d * gyv[f]; }
+          As[iy] += b * gs;
+        }
+      } else {
+#pragma unroll
+        for (int t = 0; t < NS; ++t) {
+#pragma unroll
+          for (int f = 0; f < 4; ++f) r[f][t] += DGB_TAB2F(P, dPx[g][t]) * gxv[f] + DGB_TAB2F(P, dPy[g][t]) * gyv[f];
+          r[4][t] += DGB_TAB2F(P, Phi[g][t]) * gs;
+        }
       }
+    }
+    if constexpr (kSfLift) {
+#pragma unroll
+      for (int iy = 0; iy < N1; ++iy)
+#pragma unroll
+        for (int ix = 0; ix < N1; ++ix) {
+          const float dx = DGB_TAB2F(P, D1[gx][ix]), bx = DGB_TAB2F(P, B1[gx][ix]);
+          const int t = ix + N1 * iy;
+#pragma unroll
+          for (int f = 0; f < 4; ++f) r[f][t] += dx * Ax[f][iy] + bx * Ay[f][iy];
+          r[4][t] += bx * As[iy];
+        }
     }
   }
   if (MODE == MODE_RESIDUAL) {
