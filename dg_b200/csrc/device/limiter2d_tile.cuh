@@ -212,3 +212,226 @@ __global__ void __launch_bounds__(32 * 6) lim2d_ypass_tile_kernel(const LimArgs 
 }
 
 }  // namespace dgb
+
+namespace dgb {
+
+template <int P, int METHOD>
+constexpr size_t lim2d_fused_smem_bytes() {
+  return ((size_t)5 * (P + 1) * (P + 1) * 32 + (size_t)3 * (METHOD == 2 ? 6 : 5) * (P + 1) * (P + 1) * 32) *
+         sizeof(double);
+}
+
+// Both limiter passes in one kernel.  A CTA owns a strip of 30 element columns and H element rows
+// and walks up the strip one row at a time: the x pass of row r (threads: element slot incl. the
+// left/right neighbour slots, y-slice) writes its x-limited Lagrange values into a three-row ring
+// buffer in shared memory, then the y pass of row r-1 (threads: element slot, x-column) reads
+// rows r-2, r-1, r from the ring and writes the limited state.  The rows below and above the strip
+// are x-limited too (2/H extra x work), so the x-limited intermediate never goes to HBM.  Rows
+// beyond the domain edges come from the neighbour table (periodic wrap) or are absent (walls,
+// transmissive boundaries: the y pass then needs no neighbour).  Same arithmetic as
+// lim2d_xpass_tile_kernel followed by lim2d_ypass_tile_kernel.  Uout must not alias U.
+template <int P, int METHOD, int H>
+__global__ void __launch_bounds__(32 * (P + 1)) lim2d_fused_tile_kernel(const LimArgs la, int nx, int ny,
+                                                                       const double* __restrict__ U,
+                                                                       const int* __restrict__ nbr,
+                                                                       double* __restrict__ Uout,
+                                                                       const DevScalars* __restrict__ scal) {
+  constexpr int N1 = P + 1, NS = N1 * N1, NQ = 5, NQS = METHOD == 2 ? 6 : 5, TWI = 30;
+  extern __shared__ __align__(16) double lsm[];
+  auto A = reinterpret_cast<double(*)[N1][N1][32]>(lsm);                 // [q][slice][m][slot]
+  auto XR = reinterpret_cast<double(*)[NQS][NS][32]>(lsm + NQ * N1 * N1 * 32);  // [row % 3][q][node][slot]
+  if (scal && scal->flags) return;
+  const int ld = la.ld;
+  const int tx = threadIdx.x, sl = threadIdx.y;
+  const int x0 = blockIdx.x * TWI, y0 = blockIdx.y * H;
+  const int nrow = min(H, ny - y0);
+  const int ex = x0 - 1 + tx;
+  const bool icol = tx >= 1 && tx <= TWI && ex < nx;
+  // element of column x (0 <= x < nx) in strip row s (s = 0: the row below, s = nrow + 1: above)
+  auto row_elem = [&](int s, int x) -> int {
+    if (s >= 1 && s <= nrow) return (y0 + s - 1) * nx + x;
+    if (s == 0) return __ldg(nbr + (size_t)2 * ld + y0 * nx + x);
+    return __ldg(nbr + (size_t)3 * ld + (y0 + nrow - 1) * nx + x);
+  };
+  auto lane_elem = [&](int s) -> int {
+    if (icol) return row_elem(s, ex);
+    if (tx == 0) {
+      const int e1 = row_elem(s, x0);
+      return e1 >= 0 ? __ldg(nbr + e1) : -1;
+    }
+    if (ex - 1 < nx && ex - 1 >= 0) {
+      const int el = row_elem(s, ex - 1);
+      return el >= 0 ? __ldg(nbr + (size_t)ld + el) : -1;
+    }
+    return -1;
+  };
+  double v[5][N1];  // raw values of this lane's slice in the current row (prefetched)
+  int e = lane_elem(0);
+  if (e >= 0) {
+#pragma unroll
+    for (int f = 0; f < 5; ++f)
+#pragma unroll
+      for (int ix = 0; ix < N1; ++ix) v[f][ix] = __ldg(U + (size_t)(f * NS + ix + N1 * sl) * ld + e);
+  }
+  for (int s = 0; s <= nrow + 1; ++s) {
+    // ---- x pass of strip row s: monomial coefficients of every slot ----
+    double Em[N1];
+    if (e >= 0) {
+      double q[NQ][N1];
+#pragma unroll
+      for (int ix = 0; ix < N1; ++ix) {
+        if constexpr (METHOD == 1) {
+#pragma unroll
+          for (int f = 0; f < 5; ++f) q[f][ix] = v[f][ix];
+        } else {
+          q[0][ix] = v[0][ix];
+          q[1][ix] = v[1][ix];
+          q[2][ix] = v[2][ix];
+          q[3][ix] = v[4][ix];
+          const double ru = v[1][ix], rv = v[2][ix];
+          q[4][ix] = (1.0 / v[4][ix]) * (v[3][ix] - 0.5 * (ru * ru + rv * rv) / v[0][ix]);
+        }
+      }
+#pragma unroll
+      for (int k = 0; k < NQ; ++k) {
+        double am[N1];
+        to_mono<P>(q[k], am);
+#pragma unroll
+        for (int m = 0; m < N1; ++m) A[k][sl][m][tx] = am[m];
+      }
+      if constexpr (METHOD == 2) to_mono<P>(v[3], Em);
+    }
+    __syncthreads();
+    // ---- x pass: limit the interior slots, x-limited Lagrange values into the ring ----
+    const int slot = s % 3;
+    if (icol && e >= 0) {
+      const int phys = boundary_code(__ldg(nbr + e), __ldg(nbr + (size_t)ld + e));
+      double lim[NQ][N1];
+#pragma unroll
+      for (int k = 0; k < NQ; ++k) {
+        double aL[N1], aC[N1], aR[N1];
+#pragma unroll
+        for (int m = 0; m < N1; ++m) aC[m] = A[k][sl][m][tx];
+        const int ph = (METHOD == 1 && phys == 3 && k == 1) ? 5 : phys;
+        if (ph == 0) {
+#pragma unroll
+          for (int m = 0; m < N1; ++m) { aL[m] = A[k][sl][m][tx - 1]; aR[m] = A[k][sl][m][tx + 1]; }
+          limit_monomial<P>(aL, aC, aR, lim[k]);
+        } else if (ph == 2 || ph == 3) {
+          average_monomial<P>(aC, lim[k]);
+        } else {
+#pragma unroll
+          for (int m = 0; m < N1; ++m) lim[k][m] = aC[m];
+        }
+      }
+      if constexpr (METHOD == 1) {
+#pragma unroll
+        for (int k = 0; k < NQ; ++k) {
+          double out[N1];
+          to_lag<P>(lim[k], out);
+#pragma unroll
+          for (int ix = 0; ix < N1; ++ix) XR[slot][k][ix + N1 * sl][tx] = out[ix];
+        }
+      } else {
+        double r_[N1], u_[N1], v_[N1], a_[N1], p_[N1], K[N1], Km[N1], El[N1], E_[N1];
+        to_lag<P>(lim[0], r_);
+        to_lag<P>(lim[1], u_);
+        to_lag<P>(lim[2], v_);
+        to_lag<P>(lim[3], a_);
+        to_lag<P>(lim[4], p_);
+#pragma unroll
+        for (int ix = 0; ix < N1; ++ix) K[ix] = 0.5 * (u_[ix] * u_[ix] + v_[ix] * v_[ix]) / r_[ix];
+        to_mono<P>(K, Km);
+        reconstruct_energy<P>(lim[4], lim[3], Km, Em, El);
+        to_lag<P>(El, E_);
+#pragma unroll
+        for (int ix = 0; ix < N1; ++ix) {
+          const int t = ix + N1 * sl;
+          XR[slot][0][t][tx] = r_[ix];
+          XR[slot][1][t][tx] = u_[ix];
+          XR[slot][2][t][tx] = v_[ix];
+          XR[slot][3][t][tx] = a_[ix];
+          XR[slot][4][t][tx] = p_[ix];
+          XR[slot][5][t][tx] = E_[ix];
+        }
+      }
+    }
+    __syncthreads();
+    // prefetch the next row's raw values while the y pass runs
+    if (s <= nrow) {
+      e = lane_elem(s + 1);
+      if (e >= 0) {
+#pragma unroll
+        for (int f = 0; f < 5; ++f)
+#pragma unroll
+          for (int ix = 0; ix < N1; ++ix) v[f][ix] = __ldg(U + (size_t)(f * NS + ix + N1 * sl) * ld + e);
+      }
+    }
+    // ---- y pass of strip row s - 1 (threads: slot, x-column ix = threadIdx.y) ----
+    if (s >= 2 && icol) {
+      const int ix = sl;
+      const int ec = (y0 + s - 2) * nx + ex;
+      const int phys = boundary_code(__ldg(nbr + (size_t)2 * ld + ec), __ldg(nbr + (size_t)3 * ld + ec));
+      const int cD = (s - 2) % 3, cC = (s - 1) % 3, cU = s % 3;
+      double lim[NQ][N1], Emy[N1];
+#pragma unroll
+      for (int k = 0; k < NQ; ++k) {
+        double col[N1], aC[N1];
+#pragma unroll
+        for (int iy = 0; iy < N1; ++iy) col[iy] = XR[cC][k][ix + N1 * iy][tx];
+        to_mono<P>(col, aC);
+        const int ph = (METHOD == 1 && phys == 3 && k == 2) ? 5 : phys;
+        if (ph == 0) {
+          double aD[N1], aU[N1];
+#pragma unroll
+          for (int iy = 0; iy < N1; ++iy) col[iy] = XR[cD][k][ix + N1 * iy][tx];
+          to_mono<P>(col, aD);
+#pragma unroll
+          for (int iy = 0; iy < N1; ++iy) col[iy] = XR[cU][k][ix + N1 * iy][tx];
+          to_mono<P>(col, aU);
+          limit_monomial<P>(aD, aC, aU, lim[k]);
+        } else if (ph == 2 || ph == 3) {
+          average_monomial<P>(aC, lim[k]);
+        } else {
+#pragma unroll
+          for (int m = 0; m < N1; ++m) lim[k][m] = aC[m];
+        }
+      }
+      if constexpr (METHOD == 1) {
+#pragma unroll
+        for (int k = 0; k < NQ; ++k) {
+          double out[N1];
+          to_lag<P>(lim[k], out);
+#pragma unroll
+          for (int iy = 0; iy < N1; ++iy) Uout[(size_t)(k * NS + ix + N1 * iy) * ld + ec] = out[iy];
+        }
+      } else {
+        double col[N1];
+#pragma unroll
+        for (int iy = 0; iy < N1; ++iy) col[iy] = XR[cC][5][ix + N1 * iy][tx];
+        to_mono<P>(col, Emy);
+        double r_[N1], u_[N1], v_[N1], a_[N1], K[N1], Km[N1], El[N1], E_[N1];
+        to_lag<P>(lim[0], r_);
+        to_lag<P>(lim[1], u_);
+        to_lag<P>(lim[2], v_);
+        to_lag<P>(lim[3], a_);
+#pragma unroll
+        for (int iy = 0; iy < N1; ++iy) K[iy] = 0.5 * (u_[iy] * u_[iy] + v_[iy] * v_[iy]) / r_[iy];
+        to_mono<P>(K, Km);
+        reconstruct_energy<P>(lim[4], lim[3], Km, Emy, El);
+        to_lag<P>(El, E_);
+#pragma unroll
+        for (int iy = 0; iy < N1; ++iy) {
+          const size_t o = (size_t)(ix + N1 * iy) * ld + ec;
+          Uout[o + (size_t)0 * NS * ld] = r_[iy];
+          Uout[o + (size_t)1 * NS * ld] = u_[iy];
+          Uout[o + (size_t)2 * NS * ld] = v_[iy];
+          Uout[o + (size_t)3 * NS * ld] = E_[iy];
+          Uout[o + (size_t)4 * NS * ld] = a_[iy];
+        }
+      }
+    }
+  }
+}
+
+}  // namespace dgb

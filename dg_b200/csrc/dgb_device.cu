@@ -200,6 +200,7 @@ struct dgb_ctx {
   bool tiled = false;     // structured row-major grid with tile-multiple extents: tiled residual kernel
   int form = DGB_FORM_FP64;  // arithmetic of the residual: plain FP64 or mixed FP32/FP64
   bool rowmajor = false;  // structured row-major grid: tiled limiter passes
+  bool fused_lim = false; // row-major grid, hrl / m2l: both limiter passes in one kernel (opt-in)
   CUtensorMap mapA, mapB, mapC;  // TMA descriptors of the state buffers (tiled kernel)
   double hx = 0, hy = 0;
   size_t nstate = 0;
@@ -394,8 +395,28 @@ int residual_dispatch(dgb_ctx* c, const StageArgs& a) {
   return set_error(DGB_ERR_UNSUPPORTED, "no residual kernel for this (dim, p, flux)");
 }
 
+constexpr int LIM_STRIP_H = 8;
+
+// fused x+y limiter on a row-major grid, out of place (in != out)
+template <int P, int METHOD>
+void launch_lim2d_fused(dgb_ctx* c, const double* in, double* out) {
+  ProfScope ps(c, KC_LIMITER);
+  const LimArgs la{c->ld, c->ne};
+  constexpr size_t smem = lim2d_fused_smem_bytes<P, METHOD>();
+  auto k = lim2d_fused_tile_kernel<P, METHOD, LIM_STRIP_H>;
+  static bool attr = false;
+  if (!attr) { cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem); attr = true; }
+  dim3 grid((c->nx + 29) / 30, (c->ny + LIM_STRIP_H - 1) / LIM_STRIP_H), block(32, P + 1);
+  k<<<grid, block, smem, c->st>>>(la, c->nx, c->ny, in, c->nbr, out, c->scal);
+}
+
 template <int P, int METHOD>
 void launch_lim2d(dgb_ctx* c, double* U) {
+  if (c->fused_lim) {
+    cudaMemcpyAsync(c->X, U, c->nstate * sizeof(double), cudaMemcpyDeviceToDevice, c->st);
+    launch_lim2d_fused<P, METHOD>(c, c->X, U);
+    return;
+  }
   ProfScope ps(c, KC_LIMITER);
   const LimArgs la{c->ld, c->ne};
   if (c->rowmajor) {
@@ -481,6 +502,20 @@ void launch_prl(dgb_ctx* c, double* U) {
   }
 }
 
+// out-of-place fused limiting (row-major grids, hrl / m2l): in -> out, in != out
+int limit_to(dgb_ctx* c, const double* in, double* out) {
+  const int key = c->p * 10 + c->limiter;
+  switch (key) {
+    case 11: launch_lim2d_fused<1, 1>(c, in, out); return 0;
+    case 12: launch_lim2d_fused<1, 2>(c, in, out); return 0;
+    case 21: launch_lim2d_fused<2, 1>(c, in, out); return 0;
+    case 22: launch_lim2d_fused<2, 2>(c, in, out); return 0;
+    case 31: launch_lim2d_fused<3, 1>(c, in, out); return 0;
+    case 32: launch_lim2d_fused<3, 2>(c, in, out); return 0;
+    default: return set_error(DGB_ERR_UNSUPPORTED, "fused limiter: hrl / m2l, p = 1..3");
+  }
+}
+
 // in-place limiting of a state buffer with the context's limiter
 int limit_dispatch(dgb_ctx* c, double* U) {
   if (c->limiter == 0) return 0;
@@ -557,11 +592,15 @@ int step_ssprk3(dgb_ctx* c, bool cfl) {
   for (int s = 0; s < 3; ++s) {
     a.U = in[s];
     a.Ubase = c->A;
-    a.out = out[s];
+    a.out = c->fused_lim ? c->X : out[s];  // the fused limiter then writes the stage output
     a.a = coef[s][0];
     a.b = coef[s][1];
     if (int rc = residual_dispatch<MODE_SSP>(c, a)) return rc;
-    if (int rc = limit_dispatch(c, out[s])) return rc;
+    if (c->fused_lim) {
+      if (int rc = limit_to(c, c->X, out[s])) return rc;
+    } else if (int rc = limit_dispatch(c, out[s])) {
+      return rc;
+    }
   }
   return 0;
 }
@@ -674,6 +713,9 @@ extern "C" int dgb_create(const dgb_problem* prob, int device, dgb_ctx** out) {
   c->hy = P.hy;
   c->rowmajor = P.D == 2 && is_row_major_grid(P) && std::getenv("DGB_NO_TILE") == nullptr;
   c->tiled = c->rowmajor && P.p <= 2 && P.nx % TILE_W == 0 && P.ny % TILE_H == 0;
+  // opt-in: measured slower than the two tiled passes on 512 x 256, p = 2 (64 vs 55 us per stage)
+  c->fused_lim = c->rowmajor && (P.limiter == DGB_LIM_HRL || P.limiter == DGB_LIM_M2L) &&
+                 std::getenv("DGB_FUSED_LIMITER") != nullptr;
   {
     cudaError_t el = cudaSuccess;
     auto fill = [&](auto& t, int n1) {

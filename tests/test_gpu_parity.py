@@ -114,3 +114,26 @@ def test_sensors(solvers, name):
     """Troubled-cell flags equal the reference's exactly (integer output)."""
     meta, d, s = solvers(name)
     assert np.array_equal(s.sensors(d["Uraw"]), d["sens"])
+
+
+@pytest.mark.parametrize("limiter,order,bc", [("m2l", 2, ("periodic",) * 4), ("hrl", 1, ("reflective",) * 4),
+                                              ("m2l", 3, ("reflective", "transmissive", "reflective", "transmissive"))])
+def test_fused_limiter_matches_two_pass_limiter(limiter, order, bc, monkeypatch):
+    """The opt-in single-kernel limiter (x and y passes fused) equals the two tiled passes."""
+    import dg_b200 as dgb
+    prob = dgb.Problem.structured(2, order, 70, 29, 0.0, 2.0, 0.0, 1.0, bc, flux="rusanov", limiter=limiter, cfl=0.3)
+    U0 = prob.init_state("shock_bubble", seed=9)
+    two = dgb.DGSolver(prob)
+    monkeypatch.setenv("DGB_FUSED_LIMITER", "1")
+    fused = dgb.DGSolver(prob)
+    monkeypatch.delenv("DGB_FUSED_LIMITER")
+    try:
+        assert rel_err(fused.limit(U0), two.limit(U0)) < 1e-13
+        U1 = two.limit(U0)
+        for s in (two, fused):
+            s.set_state(U1)
+            s.advance(4, 0.0, scheme=dgb.SSPRK3)
+        assert rel_err(fused.get_state(), two.get_state()) < 1e-12
+    finally:
+        two.close()
+        fused.close()
