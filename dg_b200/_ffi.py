@@ -25,7 +25,8 @@ EXPORTS = [
     "dgb_destroy", "dgb_set_state", "dgb_get_state", "dgb_set_state_device", "dgb_get_state_device",
     "dgb_residual", "dgb_solve", "dgb_limit", "dgb_dt_from_cfl", "dgb_advance", "dgb_last_dt",
     "dgb_conservation", "dgb_last_timing", "dgb_set_profiling", "dgb_kernel_timing", "dgb_limit_noalloc",
-    "dgb_sensors", "dgb_set_form",
+    "dgb_sensors", "dgb_set_form", "dgb_mlp_param_count", "dgb_indicator_features", "dgb_indicator_labels",
+    "dgb_mlp_forward", "dgb_mlp_backward", "dgb_mlp_adam", "dgb_set_indicator", "dgb_indicator_scores",
 ]
 
 
@@ -89,6 +90,13 @@ def lib() -> C.CDLL:
         "dgb_limit": [vp, dp],
         "dgb_sensors": [vp, dp, C.POINTER(C.c_int)],
         "dgb_set_form": [vp, ip],
+        "dgb_indicator_features": [vp, vp],
+        "dgb_indicator_labels": [vp, vp],
+        "dgb_mlp_forward": [vp, vp, ip, vp, vp, vp],
+        "dgb_mlp_backward": [vp, vp, vp, C.c_float, ip, vp, vp, vp, vp, vp, vp],
+        "dgb_mlp_adam": [vp, vp, vp, vp, ip, C.c_float, vp],
+        "dgb_set_indicator": [vp, vp, C.c_float],
+        "dgb_indicator_scores": [vp, dp, C.POINTER(C.c_float), C.POINTER(C.c_int)],
         "dgb_dt_from_cfl": [vp, dp, dp],
         "dgb_advance": [vp, ip, ip, C.c_double, dp],
         "dgb_last_dt": [vp, dp],
@@ -102,6 +110,8 @@ def lib() -> C.CDLL:
         f = getattr(L, name)
         f.argtypes = args
         f.restype = ip
+    L.dgb_mlp_param_count.argtypes = []
+    L.dgb_mlp_param_count.restype = ip
     L.dgb_problem_destroy.argtypes = [vp]
     L.dgb_problem_destroy.restype = None
     L.dgb_destroy.argtypes = [vp]

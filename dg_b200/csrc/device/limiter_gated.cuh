@@ -36,26 +36,45 @@ __device__ __forceinline__ void prim_to_cons(double* q) {
   q[D + 1] = p * al + 0.5 * rho * (u * u + v * v);
 }
 
+// Sparse form (learned indicator): the elements come from a list; pass 0 reads the raw state U and
+// writes X for the listed elements only; pass 1 reads X for listed (flagged) elements and the raw
+// state `alt` for the others, and writes the listed elements of `out` (= alt): flagged entries of
+// alt are written but never read in that pass.
+struct GateSparse {
+  const int* list = nullptr;
+  const int* count = nullptr;
+  const unsigned char* flag = nullptr;
+  const double* alt = nullptr;
+};
+
 // One pass of hri / pri (METHOD 1) or m2i (METHOD 2).  PASS 0: x slices (row iy = blockIdx.y,
 // neighbours left/right); PASS 1: y slices (column ix = blockIdx.y, neighbours bottom/top); 1D: the
 // element is the slice.  IN_PRIM converts loaded values to primitive variables, OUT_CONS converts
 // stored values back.  out must not alias U.
-template <int D, int P, int METHOD, int PASS, bool IN_PRIM, bool OUT_CONS>
+template <int D, int P, int METHOD, int PASS, bool IN_PRIM, bool OUT_CONS, bool SPARSE = false>
 __global__ void __launch_bounds__(128) lim_gated_kernel(const LimArgs la, const int* __restrict__ sens,
-                                                        const double* __restrict__ U, const int* __restrict__ nbr,
-                                                        double* __restrict__ out, const DevScalars* __restrict__ scal) {
+                                                        const double* U, const int* __restrict__ nbr,
+                                                        double* out, const DevScalars* __restrict__ scal,
+                                                        const GateSparse sp = GateSparse()) {
   constexpr int N1 = P + 1, NS = D == 2 ? N1 * N1 : N1, NF = D + 3, IE = D + 1, IA = D + 2;
   constexpr int UN = (D == 2 && PASS == 1) ? 2 : 1;  // wall-normal momentum of this pass
   if (scal && scal->flags) return;
-  const int ld = la.ld, e = blockIdx.x * blockDim.x + threadIdx.x, sl = blockIdx.y;
-  if (e >= la.n_elem) return;
+  const int ld = la.ld, sl = blockIdx.y;
+  int e = blockIdx.x * blockDim.x + threadIdx.x;
+  if (SPARSE) {
+    if (e >= *sp.count) return;
+    e = sp.list[e];
+  } else if (e >= la.n_elem) {
+    return;
+  }
   auto node = [&](int k) { return D == 1 ? k : (PASS == 0 ? k + N1 * sl : sl + N1 * k); };
   auto load = [&](int el, double (*v)[N1]) {
+    const double* src = (SPARSE && PASS == 1 && el != e && !sp.flag[el]) ? sp.alt : U;
 #pragma unroll
     for (int k = 0; k < N1; ++k) {
       double q[NF];
 #pragma unroll
-      for (int f = 0; f < NF; ++f) q[f] = __ldg(U + (size_t)(f * NS + node(k)) * ld + el);
+      for (int f = 0; f < NF; ++f) q[f] = src[(size_t)(f * NS + node(k)) * ld + el];
       if (IN_PRIM) cons_to_prim<D>(q);
 #pragma unroll
       for (int f = 0; f < NF; ++f) v[f][k] = q[f];
@@ -74,7 +93,7 @@ __global__ void __launch_bounds__(128) lim_gated_kernel(const LimArgs la, const 
   };
   double c[NF][N1];
   load(e, c);
-  if (!__ldg(sens + e)) {
+  if (!SPARSE && !__ldg(sens + e)) {
     store(c);
     return;
   }

@@ -21,6 +21,7 @@
 #include "device/limiter2d_tile.cuh"
 #include "device/limiter_gated.cuh"
 #include "device/tile2d_mixed.cuh"
+#include "device/learned.cuh"
 #include "device/sensor.h"
 #include "host/host.h"
 
@@ -209,6 +210,15 @@ struct dgb_ctx {
   int *nbr = nullptr, *perm = nullptr;
   // sensor-gated limiters (hri, m2i, pri, p0i): sensor work arrays and flags
   bool gated = false, has_sensors = false;
+  bool ind_on = false;          // learned indicator gates the limiter (dgb_set_indicator)
+  float ind_threshold = 0.2f;
+  float* ind_params = nullptr;  // FP32 parameters (MLP_NPARAM)
+  __nv_bfloat16* ind_w = nullptr;  // W1 [64][IND_KPAD] then W2 [64][64], BF16
+  float* ind_vec = nullptr;     // b1, b2, w3, b3
+  float* ind_modes = nullptr;   // [N_E][IND_MODES]
+  float* ind_score = nullptr;   // [N_E]
+  unsigned char* ind_flag = nullptr;
+  int* ind_list = nullptr;      // [N_E] + count
   SensorLaunch sl;
   int* iperm = nullptr;
   double* smean = nullptr;
@@ -516,9 +526,44 @@ int limit_to(dgb_ctx* c, const double* in, double* out) {
   }
 }
 
+// learned indicator: scores and flags of U (modes, then the BF16 tensor-core MLP)
+void launch_indicator(dgb_ctx* c, const double* U) {
+  ProfScope ps(c, KC_LIMITER);
+  indicator_modes_kernel<2><<<(c->ne + 127) / 128, 128, 0, c->st>>>(U, c->ld, c->ne, c->ind_modes);
+  cudaMemsetAsync(c->ind_list + c->ld, 0, sizeof(int), c->st);
+  IndicatorArgs a;
+  a.n_elem = c->ne; a.ld = c->ld; a.threshold = c->ind_threshold; a.nbr = c->nbr; a.modes = c->ind_modes;
+  a.w1 = c->ind_w; a.w2 = c->ind_w + MLP_H * IND_KPAD; a.vec = c->ind_vec;
+  a.score = c->ind_score; a.flag = c->ind_flag; a.list = c->ind_list; a.count = c->ind_list + c->ld; a.scal = c->scal;
+  const int ntiles = (c->ne + 15) / 16;
+  const int grid = std::min((ntiles + 3) / 4, 148 * 4);
+  indicator_infer_kernel<<<grid, 128, 0, c->st>>>(a);
+  c->counter += 2;
+}
+
+// learned-indicator-gated m2 limiter (m2i arithmetic on the flagged elements only), in place
+void launch_learned_limiter(dgb_ctx* c, double* U) {
+  launch_indicator(c, U);
+  ProfScope ps(c, KC_LIMITER);
+  const LimArgs la{c->ld, c->ne};
+  GateSparse sp;
+  sp.list = c->ind_list;
+  sp.count = c->ind_list + c->ld;
+  sp.flag = c->ind_flag;
+  sp.alt = U;
+  dim3 grid((c->ne + 127) / 128, 3);
+  lim_gated_kernel<2, 2, 2, 0, false, false, true><<<grid, 128, 0, c->st>>>(la, nullptr, U, c->nbr, c->X, c->scal, sp);
+  lim_gated_kernel<2, 2, 2, 1, false, false, true><<<grid, 128, 0, c->st>>>(la, nullptr, c->X, c->nbr, U, c->scal, sp);
+  c->counter += 1;
+}
+
 // in-place limiting of a state buffer with the context's limiter
 int limit_dispatch(dgb_ctx* c, double* U) {
   if (c->limiter == 0) return 0;
+  if (c->ind_on) {
+    launch_learned_limiter(c, U);
+    return 0;
+  }
   if (c->limiter == DGB_LIM_PRL) {
     const int k = c->D * 10 + c->p;
     switch (k) {
@@ -592,11 +637,12 @@ int step_ssprk3(dgb_ctx* c, bool cfl) {
   for (int s = 0; s < 3; ++s) {
     a.U = in[s];
     a.Ubase = c->A;
-    a.out = c->fused_lim ? c->X : out[s];  // the fused limiter then writes the stage output
+    const bool fused = c->fused_lim && !c->ind_on;
+    a.out = fused ? c->X : out[s];  // the fused limiter then writes the stage output
     a.a = coef[s][0];
     a.b = coef[s][1];
     if (int rc = residual_dispatch<MODE_SSP>(c, a)) return rc;
-    if (c->fused_lim) {
+    if (fused) {
       if (int rc = limit_to(c, c->X, out[s])) return rc;
     } else if (int rc = limit_dispatch(c, out[s])) {
       return rc;
@@ -839,6 +885,9 @@ extern "C" void dgb_destroy(dgb_ctx* c) {
   if (c->nbr) cudaFree(c->nbr);
   if (c->perm) cudaFree(c->perm);
   if (c->iperm) cudaFree(c->iperm);
+  for (void* q : {(void*)c->ind_params, (void*)c->ind_w, (void*)c->ind_vec, (void*)c->ind_modes, (void*)c->ind_score,
+                  (void*)c->ind_flag, (void*)c->ind_list})
+    if (q) cudaFree(q);
   if (c->smean) cudaFree(c->smean);
   if (c->sint) cudaFree(c->sint);
   if (c->scal) cudaFree(c->scal);
@@ -923,6 +972,145 @@ extern "C" int dgb_limit(dgb_ctx* c, double* U) {
   if (int rc = limit_dispatch(c, c->B)) return rc;
   DGB_CUDA(cudaGetLastError());
   return download(c, c->B, U);
+}
+
+// ------------------------------------------------------------------------------------------
+// learned troubled-cell indicator: dataset and training
+// ------------------------------------------------------------------------------------------
+extern "C" int dgb_mlp_param_count(void) { return MLP_NPARAM; }
+
+extern "C" int dgb_indicator_features(dgb_ctx* c, float* X_dev) {
+  if (!c || !X_dev) return set_error(DGB_ERR_ARG, "null argument");
+  if (c->D != 2 || c->p != 2) return set_error(DGB_ERR_UNSUPPORTED, "the indicator is built for 2D, p = 2");
+  DGB_CUDA(cudaSetDevice(c->device));
+  indicator_features_kernel<2><<<(c->ne + 127) / 128, 128, 0, c->st>>>(c->A, c->ld, c->ne, c->nbr, X_dev);
+  DGB_CUDA(cudaGetLastError());
+  DGB_CUDA(cudaStreamSynchronize(c->st));
+  return DGB_OK;
+}
+
+extern "C" int dgb_indicator_labels(dgb_ctx* c, float* y_dev) {
+  if (!c || !y_dev) return set_error(DGB_ERR_ARG, "null argument");
+  if (c->D != 2 || c->p != 2) return set_error(DGB_ERR_UNSUPPORTED, "the indicator is built for 2D, p = 2");
+  if (c->limiter == 0) return set_error(DGB_ERR_ARG, "labels need a limiter");
+  DGB_CUDA(cudaSetDevice(c->device));
+  if (int rc = reset_scalars(c, 0.0)) return rc;
+  DGB_CUDA(cudaMemcpyAsync(c->B, c->A, c->nstate * sizeof(double), cudaMemcpyDeviceToDevice, c->st));
+  const bool ind = c->ind_on;
+  c->ind_on = false;  // labels come from the problem's own (full) limiter
+  const int rc = limit_dispatch(c, c->B);
+  c->ind_on = ind;
+  if (rc) return rc;
+  indicator_labels_kernel<2><<<(c->ne + 127) / 128, 128, 0, c->st>>>(c->A, c->B, c->ld, c->ne, y_dev);
+  DGB_CUDA(cudaGetLastError());
+  DGB_CUDA(cudaStreamSynchronize(c->st));
+  return DGB_OK;
+}
+
+extern "C" int dgb_mlp_forward(const float* params, const float* X, int n, float* cache, float* prob, void* stream) {
+  if (!params || !X || !prob || n < 0) return set_error(DGB_ERR_ARG, "bad argument");
+  if (n == 0) return DGB_OK;
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  const size_t smem = MLP_NPARAM * sizeof(float);
+  static bool attr = false;
+  if (!attr) { cudaFuncSetAttribute(mlp_forward_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem); attr = true; }
+  mlp_forward_kernel<<<(n + 127) / 128, 128, smem, st>>>(params, X, n, cache, prob);
+  DGB_CUDA(cudaGetLastError());
+  return DGB_OK;
+}
+
+extern "C" int dgb_mlp_backward(const float* params, const float* X, const float* y, float pos_weight, int n,
+                                const float* cache, const float* prob, float* grad, float* loss, float* work,
+                                void* stream) {
+  if (!params || !X || !y || !cache || !prob || !grad || !loss || !work || n <= 0)
+    return set_error(DGB_ERR_ARG, "bad argument");
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  float* dz = work;
+  float* dA2 = work + n;
+  float* dA1 = dA2 + (size_t)n * MLP_H;
+  DGB_CUDA(cudaMemsetAsync(loss, 0, sizeof(float), st));
+  mlp_delta_kernel<<<(n + 127) / 128, 128, 0, st>>>(params, y, pos_weight, n, cache, prob, dz, dA2, dA1, loss);
+  const dim3 b(16, 16);
+  auto red = [&](const float* Pm, int ldp, int R, const float* Qm, int ldq, int C, float* G) {
+    const dim3 g((C + 15) / 16, (R + 15) / 16);
+    outer_reduce_kernel<<<g, b, 0, st>>>(n, Pm, ldp, R, Qm, ldq, C, G);
+  };
+  red(dA1, MLP_H, MLP_H, X, MLP_IN, MLP_IN, grad + MLP_W1);            // dW1 = dA1^T X
+  red(dA1, MLP_H, MLP_H, nullptr, 0, 1, grad + MLP_B1);                // db1
+  red(dA2, MLP_H, MLP_H, cache + MLP_H, MLP_CACHE, MLP_H, grad + MLP_W2);  // dW2 = dA2^T H1
+  red(dA2, MLP_H, MLP_H, nullptr, 0, 1, grad + MLP_B2);                // db2
+  red(cache + 3 * MLP_H, MLP_CACHE, MLP_H, dz, 1, 1, grad + MLP_W3);   // dw3 = H2^T dz
+  red(dz, 1, 1, nullptr, 0, 1, grad + MLP_B3);                         // db3
+  DGB_CUDA(cudaGetLastError());
+  return DGB_OK;
+}
+
+extern "C" int dgb_mlp_adam(float* params, const float* grad, float* m, float* v, int t, float lr, void* stream) {
+  if (!params || !grad || !m || !v || t < 1) return set_error(DGB_ERR_ARG, "bad argument");
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  mlp_adam_kernel<<<(MLP_NPARAM + 255) / 256, 256, 0, st>>>(params, grad, m, v, MLP_NPARAM, t, lr, 0.9f, 0.999f, 1e-8f);
+  DGB_CUDA(cudaGetLastError());
+  return DGB_OK;
+}
+
+extern "C" int dgb_set_indicator(dgb_ctx* c, const float* params, float threshold) {
+  if (!c) return set_error(DGB_ERR_ARG, "null argument");
+  DGB_CUDA(cudaSetDevice(c->device));
+  DGB_CUDA(cudaStreamSynchronize(c->st));
+  for (auto& row : c->graphs)
+    for (auto& g : row)
+      if (g) { cudaGraphExecDestroy(g); g = nullptr; }
+  if (!params) {
+    c->ind_on = false;
+    return DGB_OK;
+  }
+  if (c->D != 2 || c->p != 2 || c->limiter != DGB_LIM_M2L)
+    return set_error(DGB_ERR_UNSUPPORTED, "the learned indicator gates the m2l limiter of 2D p = 2 problems");
+  if (!c->ind_params) {
+    cudaError_t e;
+    if ((e = cudaMalloc(&c->ind_params, MLP_NPARAM * sizeof(float))) != cudaSuccess ||
+        (e = cudaMalloc(&c->ind_w, (size_t)(MLP_H * IND_KPAD + MLP_H * MLP_H) * sizeof(__nv_bfloat16))) != cudaSuccess ||
+        (e = cudaMalloc(&c->ind_vec, (3 * MLP_H + 1) * sizeof(float))) != cudaSuccess ||
+        (e = cudaMalloc(&c->ind_modes, (size_t)c->ld * IND_MODES * sizeof(float))) != cudaSuccess ||
+        (e = cudaMalloc(&c->ind_score, (size_t)c->ld * sizeof(float))) != cudaSuccess ||
+        (e = cudaMalloc(&c->ind_flag, (size_t)c->ld)) != cudaSuccess ||
+        (e = cudaMalloc(&c->ind_list, ((size_t)c->ld + 1) * sizeof(int))) != cudaSuccess)
+      return set_error(DGB_ERR_CUDA, std::string("indicator buffers: ") + cudaGetErrorString(e));
+  }
+  std::vector<__nv_bfloat16> w((size_t)MLP_H * IND_KPAD + MLP_H * MLP_H, __float2bfloat16(0.f));
+  for (int j = 0; j < MLP_H; ++j)
+    for (int k = 0; k < MLP_IN; ++k) w[(size_t)j * IND_KPAD + k] = __float2bfloat16(params[MLP_W1 + j * MLP_IN + k]);
+  for (int j = 0; j < MLP_H; ++j)
+    for (int i = 0; i < MLP_H; ++i) w[(size_t)MLP_H * IND_KPAD + j * MLP_H + i] = __float2bfloat16(params[MLP_W2 + j * MLP_H + i]);
+  std::vector<float> vec(3 * MLP_H + 1);
+  for (int j = 0; j < MLP_H; ++j) {
+    vec[j] = params[MLP_B1 + j];
+    vec[MLP_H + j] = params[MLP_B2 + j];
+    vec[2 * MLP_H + j] = params[MLP_W3 + j];
+  }
+  vec[3 * MLP_H] = params[MLP_B3];
+  DGB_CUDA(cudaMemcpy(c->ind_params, params, MLP_NPARAM * sizeof(float), cudaMemcpyHostToDevice));
+  DGB_CUDA(cudaMemcpy(c->ind_w, w.data(), w.size() * sizeof(__nv_bfloat16), cudaMemcpyHostToDevice));
+  DGB_CUDA(cudaMemcpy(c->ind_vec, vec.data(), vec.size() * sizeof(float), cudaMemcpyHostToDevice));
+  c->ind_threshold = threshold;
+  c->ind_on = true;
+  return DGB_OK;
+}
+
+extern "C" int dgb_indicator_scores(dgb_ctx* c, const double* U, float* score, int* n_flagged) {
+  if (!c || !U || !score) return set_error(DGB_ERR_ARG, "null argument");
+  if (!c->ind_on) return set_error(DGB_ERR_ARG, "no indicator set (dgb_set_indicator)");
+  DGB_CUDA(cudaSetDevice(c->device));
+  if (int rc = upload(c, U, c->B)) return rc;
+  if (int rc = reset_scalars(c, 0.0)) return rc;
+  launch_indicator(c, c->B);
+  DGB_CUDA(cudaGetLastError());
+  DGB_CUDA(cudaMemcpyAsync(score, c->ind_score, (size_t)c->ne * sizeof(float), cudaMemcpyDeviceToHost, c->st));
+  int cnt = 0;
+  DGB_CUDA(cudaMemcpyAsync(&cnt, c->ind_list + c->ld, sizeof(int), cudaMemcpyDeviceToHost, c->st));
+  DGB_CUDA(cudaStreamSynchronize(c->st));
+  if (n_flagged) *n_flagged = cnt;
+  return DGB_OK;
 }
 
 extern "C" int dgb_set_form(dgb_ctx* c, int form) {

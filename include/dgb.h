@@ -206,6 +206,36 @@ int dgb_set_profiling(dgb_ctx* c, int on);
 int dgb_kernel_timing(dgb_ctx* c, const char* name, double* ms, long long* launches);
 
 /* ------------------------------------------------------------------------------------
+ * Learned troubled-cell indicator (no counterpart in the reference)
+ * ------------------------------------------------------------------------------------
+ * A 225 -> 64 -> 64 -> 1 MLP (GELU, sigmoid) reads each element's and its four neighbours'
+ * normalised scaled-Taylor modes (2D, p = 2; each input compressed by asinh(x / 1e-7) / asinh(1e7))
+ * and predicts whether the problem's limiter would change the element.  Parameters: one FP32 array of dgb_mlp_param_count() values laid out as
+ * W1[64][225], b1[64], W2[64][64], b2[64], w3[64], b3.  Pointers marked _dev are device memory. */
+int dgb_mlp_param_count(void);
+/* Features [N_E][225] (FP32, row-major) of the context's current state. */
+int dgb_indicator_features(dgb_ctx* c, float* X_dev);
+/* Labels [N_E] (0 / 1) of the context's current state from the problem's own limiter. */
+int dgb_indicator_labels(dgb_ctx* c, float* y_dev);
+/* Training kernels (FP32).  forward: probabilities, and the activations needed by backward in
+ * cache_dev ([n][256], may be NULL); backward: weighted binary cross-entropy (positive samples
+ * weighted by pos_weight, mean over n) into *loss_dev and its gradient into grad_dev; work_dev
+ * holds n*129 floats.  adam: one bias-corrected Adam update (beta 0.9 / 0.999), step t >= 1. */
+int dgb_mlp_forward(const float* params_dev, const float* X_dev, int n, float* cache_dev, float* prob_dev,
+                    void* stream);
+int dgb_mlp_backward(const float* params_dev, const float* X_dev, const float* y_dev, float pos_weight, int n,
+                     const float* cache_dev, const float* prob_dev, float* grad_dev, float* loss_dev,
+                     float* work_dev, void* stream);
+int dgb_mlp_adam(float* params_dev, const float* grad_dev, float* m_dev, float* v_dev, int t, float lr,
+                 void* stream);
+/* Gates the limiter with the network: the limiter (m2l problems, 2D, p = 2) then runs on elements
+ * scoring above `threshold` only (per-element m2 arithmetic), scored with BF16 tensor-core MMAs
+ * every time the limiter runs.  params_host = NULL switches back to the full limiter. */
+int dgb_set_indicator(dgb_ctx* c, const float* params_host, float threshold);
+/* Scores [N_E] of U (reference layout, host) with the indicator set, and the flagged count. */
+int dgb_indicator_scores(dgb_ctx* c, const double* U_host, float* score_host, int* n_flagged);
+
+/* ------------------------------------------------------------------------------------
  * Allocation-free limiter (no counterpart in the reference)
  * ------------------------------------------------------------------------------------
  * For callers that cannot allocate device memory themselves -- an application that manages a

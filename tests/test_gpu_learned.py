@@ -1,0 +1,104 @@
+"""Learned troubled-cell indicator on the GPU against the numpy oracle (oracle/mlp_oracle.py):
+features and labels of a solver state, the FP32 training kernels (forward, backward, Adam), the
+BF16 tensor-core scoring inside the limiter, and the sparse gated m2 limiter it drives.
+
+Tolerances: features 1e-5 relative (FP32 storage); labels agree on >= 99.5% of elements (a label
+is a 1e-8-relative threshold test on limiter changes, so FP64 rounding can flip a borderline one);
+forward 1e-5, gradients 1e-4 relative (FP32 vs FP64); BF16 scores within 0.03 of the FP64 network;
+gated limiter 1e-12 relative.
+"""
+import ctypes as C
+
+import numpy as np
+import pytest
+
+from conftest import rel_err
+from oracle import dg_oracle as O
+from oracle import mlp_oracle as M
+
+pytestmark = pytest.mark.gpu
+
+
+def quadrant_state(nx=32, ny=32, seed=3, steps=5):
+    import dg_b200 as dgb
+    prob = dgb.Problem.structured(2, 2, nx, ny, flux="rusanov", limiter="m2l", cfl=0.3)
+    s = dgb.DGSolver(prob)
+    s.set_state(s.limit(prob.init_state("quadrants", seed=seed)))
+    if steps:
+        s.advance(steps, 0.0)
+    return prob, s
+
+
+def test_features_and_labels_match_oracle():
+    import torch
+    from dg_b200 import learned as L
+    prob, s = quadrant_state()
+    try:
+        X, y = L.snapshot_samples(s)
+        U = s.get_state()
+    finally:
+        s.close()
+    S = O.Setup.from_problem(prob)
+    perm = prob.array("tensor_perm")
+    Xo = M.features(S, U, perm)
+    yo = M.labels(S, U, perm)
+    assert rel_err(X.cpu().numpy(), Xo) < 1e-5
+    agree = float(np.mean(y.cpu().numpy() == yo))
+    assert agree >= 0.995, agree
+    assert 0 < yo.sum() < yo.size
+
+
+def test_training_kernels_match_oracle():
+    import torch
+    from dg_b200 import _ffi as F
+    from dg_b200 import learned as L
+    rng = np.random.default_rng(1)
+    n = 300
+    p = L.init_params(4)
+    X = rng.standard_normal((n, 225)).astype(np.float32)
+    y = (rng.uniform(size=n) > 0.8).astype(np.float32)
+    tr = L.Trainer(p, batch=n)
+    Xd, yd = torch.from_numpy(X).cuda(), torch.from_numpy(y).cuda()
+    prob = tr.predict(Xd).cpu().numpy()
+    po, _ = M.forward(p, X.astype(np.float64))
+    assert rel_err(prob, po) < 1e-5
+    tr.step(Xd, yd, lr=1e-3, pos_weight=4.0)
+    lo, go = M.loss_and_grad(p, X.astype(np.float64), y.astype(np.float64), 4.0)
+    assert abs(tr.loss.item() - lo) < 1e-5 * max(1.0, lo)
+    assert rel_err(tr.g.cpu().numpy(), go) < 1e-4
+    # Adam, first step: p - lr * g / (|g| + eps)
+    expect = p - 1e-3 * go / (np.abs(go) + 1e-8)
+    assert rel_err(tr.params(), expect) < 1e-5
+
+
+def test_bf16_scores_match_fp64_network():
+    from dg_b200 import learned as L
+    prob, s = quadrant_state(seed=7)
+    try:
+        params = L.init_params(2) * 3.0
+        L.set_indicator(s, params, 0.5)
+        U = s.get_state()
+        sc, cnt = L.scores(s, U)
+    finally:
+        s.close()
+    S = O.Setup.from_problem(prob)
+    po, _ = M.forward(params, M.features(S, U, prob.array("tensor_perm")))
+    assert np.abs(sc - po).max() < 0.03
+    assert cnt == int(np.sum(sc > 0.5))
+
+
+@pytest.mark.parametrize("threshold", [-1.0, 0.5])
+def test_gated_limiter_matches_oracle(threshold):
+    from dg_b200 import learned as L
+    prob, s = quadrant_state(seed=11, steps=3)
+    try:
+        params = L.init_params(5) * 3.0
+        U = s.get_state()
+        L.set_indicator(s, params, threshold)
+        sc, _ = L.scores(s, U)
+        out = s.limit(U)
+    finally:
+        s.close()
+    S = O.Setup.from_problem(prob)
+    flags = sc > threshold
+    assert rel_err(out, M.gated_m2(S, U, flags)) < 1e-12

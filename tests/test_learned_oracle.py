@@ -1,0 +1,37 @@
+"""The numpy restatement of the indicator MLP (oracle/mlp_oracle.py) checks itself: its gradient
+against central finite differences, and basic properties of its features."""
+import numpy as np
+
+from oracle import mlp_oracle as M
+
+
+def test_oracle_gradient_matches_finite_differences():
+    rng = np.random.default_rng(0)
+    p = rng.standard_normal(18689) * 0.1
+    X = rng.standard_normal((37, 225))
+    y = (rng.uniform(size=37) > 0.7).astype(float)
+    _, g = M.loss_and_grad(p, X, y, 3.0)
+    for k in (0, 5000, 14400, 14470, 18600, 18688):
+        e = np.zeros_like(p)
+        e[k] = 1e-6
+        fd = (M.loss_and_grad(p + e, X, y, 3.0)[0] - M.loss_and_grad(p - e, X, y, 3.0)[0]) / 2e-6
+        assert abs(fd - g[k]) <= 1e-6 * max(1.0, abs(g[k]))
+
+
+def test_taylor_transform_reproduces_monomials():
+    T = M.taylor_transform(2)
+    x = np.linspace(-1, 1, 3)
+    assert np.allclose(T @ (x ** 2 / 2.0), [0, 0, 1])
+    assert np.allclose(T @ np.ones(3), [1, 0, 0])
+
+
+def test_features_of_uniform_state_are_trivial():
+    import dg_b200 as dgb
+    from oracle import dg_oracle as O
+    prob = dgb.Problem.structured(2, 2, 6, 4, flux="rusanov", limiter="m2l", cfl=0.3)
+    U = prob.init_state("quadrants", params=(10.0, 10.0), seed=1)  # split outside: one state
+    S = O.Setup.from_problem(prob)
+    X = M.features(S, U, prob.array("tensor_perm")).reshape(-1, 5, 5, 9)
+    assert np.allclose(X[:, :, :, 1:], 0.0, atol=1e-12)      # no slopes anywhere
+    assert np.allclose(X[:, :, :, 0], 0.0, atol=1e-12)       # neighbours' means equal the element's
+    assert np.all(M.labels(S, U, prob.array("tensor_perm")) == 0)
