@@ -202,6 +202,107 @@ def run_reference(args):
     return 0
 
 
+def time_steps(dgb, solver, steps, warmup, flush):
+    """Device time (ms) and launches of `steps` SSP-RK3 steps, L2 flushed before each one."""
+    import torch
+    for _ in range(warmup):
+        solver.advance(1, 0.0, scheme=dgb.SSPRK3)
+    torch.cuda.synchronize()
+    dev_ms, launches = 0.0, 0
+    for _ in range(steps):
+        flush.fill_(1.0)
+        torch.cuda.synchronize()
+        solver.advance(1, 0.0, scheme=dgb.SSPRK3)
+        ms, n = solver.last_timing()
+        dev_ms += ms
+        launches += n
+    torch.cuda.synchronize()
+    return dev_ms, launches
+
+
+def cell_means(prob, U, field=0):
+    """Cell averages of one field: sum_i w_i U_i with w_i = sum_g phi_w[g, i] / |reference element|."""
+    i = prob.info
+    w = prob.array("phi_w").reshape(i.n_s, i.n_g).sum(axis=1) / 4.0
+    return U.reshape(i.n_elem, i.n_fields, i.n_s)[:, field, :] @ w
+
+
+def compare_forms(dgb, U0_coarse, dev, steps, warmup, flush, acc_steps=200):
+    """The forms of the solver on the benchmark workload: throughput of plain FP64, mixed and
+    mixed + learned indicator (same timing protocol as the headline), and their L1 density error
+    after `acc_steps` fixed steps against a 2x-refined plain FP64 solution (1024 x 512, half the
+    step) projected on the 512 x 256 cells."""
+    from dg_b200 import learned as L
+    params, meta = L.load()
+    prob, _ = build_problem()
+    out = {}
+    solvers = {}
+    for name, form, learned in (("fp64", "fp64", False), ("mixed", "mixed", False), ("mixed_learned", "mixed", True)):
+        s = dgb.DGSolver(prob, device=dev)
+        s.set_form(form)
+        if learned:
+            L.set_indicator(s, params, 0.2)
+        s.set_state(U0_coarse)
+        ms, n = time_steps(dgb, s, steps, warmup, flush)
+        dof = prob.info.n_elem * prob.info.n_s * prob.info.n_fields
+        out[name] = {"value": dof * STAGES_PER_STEP * steps / (ms / 1e3), "ms_per_step": ms / steps,
+                     "gpu_launches_per_step": n / steps}
+        solvers[name] = s
+    base = out["fp64"]["value"]
+    for k in out:
+        out[k]["speedup_vs_fp64"] = out[k]["value"] / base
+    # accuracy at a fixed step
+    ref = solvers["fp64"]
+    dt = 0.8 * ref.dt_from_cfl(U0_coarse)
+    finals = {}
+    for name, s in solvers.items():
+        s.set_state(U0_coarse)
+        try:
+            s.advance(acc_steps, dt, scheme=dgb.SSPRK3)
+            finals[name] = s.get_state()
+        except dgb.DGBError as e:
+            finals[name] = None
+            out[name]["failed"] = str(e)
+    if finals.get("mixed_learned") is not None:
+        sc, cnt = L.scores(solvers["mixed_learned"], finals["mixed_learned"])
+        out["mixed_learned"]["flagged_fraction_final"] = cnt / prob.info.n_elem
+    for s in solvers.values():
+        s.close()
+    fprob, fU0 = build_problem(2 * NX, 2 * NY)
+    fs = dgb.DGSolver(fprob, device=dev)
+    fs.set_state(fs.limit(fU0))
+    fs.advance(2 * acc_steps, 0.5 * dt, scheme=dgb.SSPRK3)
+    fine = cell_means(fprob, fs.get_state()).reshape(2 * NY, 2 * NX)
+    fs.close()
+    truth = 0.25 * (fine[0::2, 0::2] + fine[1::2, 0::2] + fine[0::2, 1::2] + fine[1::2, 1::2]).reshape(-1)
+    for name, U in finals.items():
+        if U is None:
+            continue
+        err = float(np.abs(cell_means(prob, U) - truth).sum() / np.abs(truth).sum())
+        out[name]["l1_density_error_vs_refined_fp64"] = err
+    if "l1_density_error_vs_refined_fp64" in out["fp64"]:
+        e0 = out["fp64"]["l1_density_error_vs_refined_fp64"]
+        for k in out:
+            if "l1_density_error_vs_refined_fp64" in out[k]:
+                out[k]["l1_error_ratio_vs_fp64"] = out[k]["l1_density_error_vs_refined_fp64"] / e0
+    if finals.get("fp64") is not None:
+        i = prob.info
+        for k in ("mixed", "mixed_learned"):
+            if finals.get(k) is None:
+                continue
+            A = finals[k].reshape(i.n_elem, i.n_fields, i.n_s)
+            B = finals["fp64"].reshape(i.n_elem, i.n_fields, i.n_s)
+            mom = max(np.abs(B[:, 1]).sum(), np.abs(B[:, 2]).sum())
+            out[k]["per_field_rel_l1_vs_fp64"] = [
+                float(np.abs(A[:, f] - B[:, f]).sum() / (mom if f in (1, 2) else np.abs(B[:, f]).sum()))
+                for f in range(i.n_fields)]
+    out["protocol"] = (f"{steps} timed SSP-RK3 steps each (L2 flushed); accuracy: {acc_steps} steps of dt = 0.8 x "
+                       f"the initial CFL step, truth = plain FP64 on 1024x512 with dt/2, cell-averaged onto "
+                       f"512x256; learned threshold 0.2, network {meta.get('samples')} samples, held-out recall "
+                       f"{meta.get('held_out', {}).get('0.2', {}).get('recall')}")
+    return out
+
+
 def main(argv=None) -> int:
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -214,6 +315,8 @@ def main(argv=None) -> int:
     ap.add_argument("--ny", type=int, default=NY)
     ap.add_argument("--form", default="fp64", choices=["fp64", "mixed"],
                     help="arithmetic of the residual (fp64: the plain parity form)")
+    ap.add_argument("--learned", action="store_true", help="gate the limiter with the learned indicator")
+    ap.add_argument("--no-forms", action="store_true", help="skip the mixed / learned form comparison")
     args = ap.parse_args(argv)
     if args.impl == "reference":
         return run_reference(args)
@@ -233,6 +336,9 @@ def main(argv=None) -> int:
     solver = dgb.DGSolver(prob, device=dev)
     solver.set_form(args.form)
     U0 = solver.limit(U0)  # the reference limits the initial condition when CFL > 0 (rk.cc:108-114)
+    if args.learned:
+        from dg_b200 import learned as L
+        L.set_indicator(solver, L.load()[0], 0.2)
     solver.set_state(U0)
     dof = prob.info.n_elem * prob.info.n_s * prob.info.n_fields
 
@@ -306,9 +412,13 @@ def main(argv=None) -> int:
     cpu = None
     if rank == 0 and ws == 1 and not args.no_cpu_baseline and (args.nx, args.ny) == (NX, NY):
         cpu = cpu_baseline(U0)
+    forms = None
+    if ws == 1 and not args.no_forms and (args.nx, args.ny) == (NX, NY):
+        forms = compare_forms(dgb, U0, dev, args.steps, args.warmup, flush)
 
-    form_cfg = {"form": "plain FP64" if args.form == "fp64" else
-                "mixed: FP32 contractions/Rusanov flux on FP64 anchors, FP64 pressure, state and update"}
+    form_cfg = {"form": ("plain FP64" if args.form == "fp64" else
+                         "mixed: FP32 contractions/Rusanov flux on FP64 anchors, FP64 pressure, state and update")
+                + (" + learned indicator (threshold 0.2)" if args.learned else "")}
     if rank == 0:
         line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": dev_ms / args.steps, "higher_is_better": True,
@@ -325,7 +435,7 @@ def main(argv=None) -> int:
                              "avg_launch_ms": res_avg_s * 1e3, "peak_source": "MEASURED_PEAKS.json hbm_gbs (measured copy)"},
                 "kernel_ms_per_step": {"residual": res_ms / args.steps, "limiter": lim_ms / args.steps,
                                        "dt": dt_ms / args.steps},
-                "cpu_baseline": cpu, "clocks": clocks, "gpu_launches": launches}
+                "cpu_baseline": cpu, "clocks": clocks, "gpu_launches": launches, "forms": forms}
         print(json.dumps(line))
     solver.close()
     if ws > 1:

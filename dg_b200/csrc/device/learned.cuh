@@ -5,9 +5,9 @@
 // bottom and top neighbours (the element itself where a neighbour is a boundary), minus e's own
 // cell value on the constant mode and divided by e's field scale (|mode 0| for rho, E, alpha;
 // sqrt(|rho_0 E_0|) for both momenta): x[(n*5 + f)*9 + k], n = self, L, R, D, U.
-// Each input is then compressed by the fixed signed logarithm asinh(x / 1e-7) / asinh(1e7): the
-// values span many decades (smooth cells have slopes ~1e-15, troubled ones ~1e-7 and up) and the
-// decision lives in their magnitude.
+// Each input is then compressed by the fixed signed logarithm sign(x) log(1 + |x| / 1e-7) /
+// log(1 + 1e7): the values span many decades (smooth cells have slopes ~1e-15, troubled ones ~1e-7
+// and up) and the decision lives in their magnitude.
 // Label: 1 when the full limiter of the problem changes any non-constant mode of any field of
 // the element by more than 1e-8 of that field's scale.
 // Parameters (FP32, one flat array): W1[64][225], b1[64], W2[64][64], b2[64], w3[64], b3.
@@ -25,11 +25,10 @@ constexpr int MLP_W1 = 0, MLP_B1 = MLP_W1 + MLP_H * MLP_IN, MLP_W2 = MLP_B1 + ML
 constexpr int MLP_CACHE = 4 * MLP_H;  // per sample: A1, H1, A2, H2
 constexpr double IND_LABEL_TOL = 1e-8;
 constexpr double IND_FEAT_S0 = 1e-7;                        // compression scale of the inputs
-constexpr double IND_FEAT_NORM = 16.811242831518268;       // asinh(1 / IND_FEAT_S0)
+constexpr double IND_FEAT_NORM = 16.118095750958314;       // log(1 + 1 / IND_FEAT_S0)
 
-__device__ __forceinline__ double feature_compress(double x) { return asinh(x / IND_FEAT_S0) / IND_FEAT_NORM; }
-__device__ __forceinline__ float feature_compress_f(float x) {
-  return asinhf(x * (float)(1.0 / IND_FEAT_S0)) * (float)(1.0 / IND_FEAT_NORM);
+__device__ __forceinline__ double feature_compress(double x) {
+  return copysign(log1p(fabs(x) / IND_FEAT_S0) / IND_FEAT_NORM, x);
 }
 
 __device__ __forceinline__ float gelu_f(float x) { return 0.5f * x * (1.f + erff(x * 0.70710678118654752f)); }
@@ -234,12 +233,17 @@ namespace dgb {
 // ---------------------------------------------------------------------------------------------
 // inference inside the limiter
 // ---------------------------------------------------------------------------------------------
-constexpr int IND_KPAD = 240;            // 225 inputs padded to 15 k-tiles of 16
+// The scoring kernel lays the inputs out with each neighbour's 45 values padded to 48 (k' = 48 n +
+// 9 f + m; 240 = 15 k-tiles of 16), so that a lane writes one neighbour's values with 16-byte
+// stores; W1 is stored with the same padded column order.
+constexpr int IND_KPAD = 240, IND_NSEG = 48;
 constexpr int IND_W1S = IND_KPAD + 8;    // shared row strides (bf16) that keep the fragment loads
-constexpr int IND_W2S = MLP_H + 8;       // free of bank conflicts
-// per element (56 floats = 224 bytes): the 5 constant modes as FP64 (neighbour differences of
-// nearly equal means must not cancel in FP32), the 40 other modes and the 5 inverse field scales
-constexpr int IND_MODES = 56;
+constexpr int IND_FTS = 264;             // free of bank conflicts (and 16-byte aligned rows)
+constexpr int IND_W2S = MLP_H + 8;
+// per element, 64 floats = 256 bytes, 16-byte aligned parts: [0, 10) the 5 constant modes as
+// FP64 (neighbour differences of nearly equal means must not cancel in FP32), [16, 56) the other
+// 40 modes (field f at 16 + 8 f), [56, 61) the 5 inverse field scales
+constexpr int IND_MODES = 64, IND_M_SLOPE = 16, IND_M_ISCALE = 56;
 
 // modes and scales of every element (FP64 transform)
 template <int P>
@@ -257,8 +261,8 @@ __global__ void __launch_bounds__(128) indicator_modes_kernel(const double* __re
   for (int f = 0; f < 5; ++f) {
     m0[f] = a[f][0];
 #pragma unroll
-    for (int k = 1; k < NS; ++k) m[10 + f * (NS - 1) + k - 1] = (float)a[f][k];
-    m[10 + 5 * (NS - 1) + f] = (float)(1.0 / s[f]);
+    for (int k = 1; k < NS; ++k) m[IND_M_SLOPE + f * (NS - 1) + k - 1] = (float)a[f][k];
+    m[IND_M_ISCALE + f] = (float)(1.0 / s[f]);
   }
 }
 
@@ -290,28 +294,37 @@ struct IndicatorArgs {
   const DevScalars* scal;
 };
 
-// feature value k of the element whose five element indices are el[5] (self, L, R, D, U)
-__device__ __forceinline__ float indicator_feature(const float* __restrict__ M, const int el[5], int k) {
-  const int n = k / 45, r = k % 45, f = r / 9, m = r % 9;
-  const float* ms = M + (size_t)el[0] * IND_MODES;
-  const float* mn = M + (size_t)el[n] * IND_MODES;
-  float v;
-  if (m == 0)
-    v = (float)(__ldg(reinterpret_cast<const double*>(mn) + f) - __ldg(reinterpret_cast<const double*>(ms) + f));
-  else
-    v = __ldg(mn + 10 + f * 8 + m - 1);
-  return feature_compress_f(v * __ldg(ms + 50 + f));
+// the input compression in FP32 with the hardware base-2 logarithm
+__device__ __forceinline__ float feature_compress_fast(float x) {
+  const float l = __log2f(fmaf(fabsf(x), (float)(1.0 / IND_FEAT_S0), 1.f));
+  return copysignf(l * (float)(0.69314718055994531 / IND_FEAT_NORM), x);
+}
+
+// GELU in its tanh form with the hardware tanh (scoring only; inputs are BF16 anyway)
+__device__ __forceinline__ float gelu_fast(float x) {
+  const float u = 0.7978845608028654f * fmaf(0.044715f * x, x * x, x);
+  float th;
+  asm("tanh.approx.f32 %0, %1;" : "=f"(th) : "f"(u));
+  return 0.5f * x * (1.f + th);
 }
 
 // MLP scores on BF16 tensor cores (mma.sync m16n8k16, FP32 accumulation): a warp scores 16
 // elements; layer-1 accumulators become layer-2 A fragments without leaving registers.
 // Persistent CTAs of 4 warps; weights staged once per CTA.  Elements scoring above the threshold
 // are flagged and appended to the list.
+constexpr size_t IND_SMEM_BYTES =
+    ((size_t)MLP_H * IND_W1S + (size_t)MLP_H * IND_W2S + (size_t)4 * 16 * IND_FTS) * sizeof(__nv_bfloat16) +
+    (3 * MLP_H + 4) * sizeof(float) + 4 * 80 * sizeof(int);
+
 __global__ void __launch_bounds__(128) indicator_infer_kernel(const IndicatorArgs a) {
-  __shared__ __align__(16) __nv_bfloat16 w1s[MLP_H * IND_W1S];
-  __shared__ __align__(16) __nv_bfloat16 w2s[MLP_H * IND_W2S];
-  __shared__ float vs[3 * MLP_H + 1];
+  extern __shared__ __align__(16) unsigned char ism[];
+  __nv_bfloat16* w1s = reinterpret_cast<__nv_bfloat16*>(ism);          // [64][IND_W1S]
+  __nv_bfloat16* w2s = w1s + MLP_H * IND_W1S;                           // [64][IND_W2S]
+  __nv_bfloat16* fts0 = w2s + MLP_H * IND_W2S;                          // per warp: [16][IND_W1S]
+  float* vs = reinterpret_cast<float*>(fts0 + 4 * 16 * IND_FTS);        // b1, b2, w3, b3
+  int* eidx0 = reinterpret_cast<int*>(vs + 3 * MLP_H + 4);              // per warp: [16][5]
   if (a.scal && a.scal->flags) return;
+  for (int i = threadIdx.x; i < 4 * 16 * IND_FTS; i += blockDim.x) fts0[i] = __float2bfloat16(0.f);
   for (int i = threadIdx.x; i < MLP_H * IND_KPAD; i += blockDim.x)
     w1s[(i / IND_KPAD) * IND_W1S + i % IND_KPAD] = a.w1[i];
   for (int i = threadIdx.x; i < MLP_H * MLP_H; i += blockDim.x) w2s[(i / MLP_H) * IND_W2S + i % MLP_H] = a.w2[i];
@@ -321,32 +334,74 @@ __global__ void __launch_bounds__(128) indicator_infer_kernel(const IndicatorArg
   const uint32_t* w1w = reinterpret_cast<const uint32_t*>(w1s);
   const uint32_t* w2w = reinterpret_cast<const uint32_t*>(w2s);
   const int ntiles = (a.n_elem + 15) / 16;
+  __syncthreads();
+  __nv_bfloat16* ft = fts0 + warp * 16 * IND_FTS;
+  const uint32_t* ftw = reinterpret_cast<const uint32_t*>(ft);
   for (int tile = blockIdx.x * 4 + warp; tile < ntiles; tile += gridDim.x * 4) {
     const int r0 = tile * 16 + g, r1 = r0 + 8;
-    int el0[5], el1[5];
     const bool ok0 = r0 < a.n_elem, ok1 = r1 < a.n_elem;
-    el0[0] = ok0 ? r0 : 0;
-    el1[0] = ok1 ? r1 : 0;
-#pragma unroll
-    for (int q = 1; q < 5; ++q) {
-      const int n0 = ok0 ? __ldg(a.nbr + (size_t)(q - 1) * a.ld + r0) : -1;
-      const int n1 = ok1 ? __ldg(a.nbr + (size_t)(q - 1) * a.ld + r1) : -1;
-      el0[q] = n0 >= 0 ? n0 : el0[0];
-      el1[q] = n1 >= 0 ? n1 : el1[0];
+    // element indices of the 16 rows (self, L, R, D, U), then the features into shared memory:
+    // 25 (neighbour, field) groups of 9 modes per row, several groups in flight per lane
+    int* eidx = eidx0 + warp * 80;
+    for (int q = lane; q < 80; q += 32) {
+      const int row = q / 5, n = q - 5 * row, es = tile * 16 + row;
+      int v = es < a.n_elem ? es : -1;
+      if (v >= 0 && n > 0) {
+        const int nb = __ldg(a.nbr + (size_t)(n - 1) * a.ld + es);
+        v = nb >= 0 ? nb : es;
+      }
+      eidx[q] = v;
     }
+    __syncwarp();
+    // one lane per (row, neighbour): the neighbour's whole record by 16-byte loads, 45 features out
+    for (int q = lane; q < 80; q += 32) {
+      const int row = q / 5, n = q - 5 * row;
+      const int es = eidx[row * 5], en = eidx[row * 5 + n];
+      uint4* dst = reinterpret_cast<uint4*>(ft + row * IND_FTS + n * IND_NSEG);
+      if (es < 0) {
+#pragma unroll
+        for (int j = 0; j < IND_NSEG / 8; ++j) dst[j] = make_uint4(0u, 0u, 0u, 0u);
+        continue;
+      }
+      const float4* rs = reinterpret_cast<const float4*>(a.modes + (size_t)es * IND_MODES);
+      const float4* rn = reinterpret_cast<const float4*>(a.modes + (size_t)en * IND_MODES);
+      float4 sv[3], nv[3], sl[10], isc[2];
+#pragma unroll
+      for (int k = 0; k < 3; ++k) { sv[k] = __ldg(rs + k); nv[k] = __ldg(rn + k); }
+#pragma unroll
+      for (int k = 0; k < 10; ++k) sl[k] = __ldg(rn + IND_M_SLOPE / 4 + k);
+#pragma unroll
+      for (int k = 0; k < 2; ++k) isc[k] = __ldg(rs + IND_M_ISCALE / 4 + k);
+      const double* s0 = reinterpret_cast<const double*>(sv);
+      const double* n0 = reinterpret_cast<const double*>(nv);
+      const float* slp = reinterpret_cast<const float*>(sl);
+      const float* is = reinterpret_cast<const float*>(isc);
+      float v[IND_NSEG];
+#pragma unroll
+      for (int f = 0; f < 5; ++f) {
+        v[f * 9] = feature_compress_fast((float)(n0[f] - s0[f]) * is[f]);
+#pragma unroll
+        for (int m = 1; m < 9; ++m) v[f * 9 + m] = feature_compress_fast(slp[f * 8 + m - 1] * is[f]);
+      }
+      v[45] = v[46] = v[47] = 0.f;
+#pragma unroll
+      for (int j = 0; j < IND_NSEG / 8; ++j)
+        dst[j] = make_uint4(pack_bf16(v[8 * j], v[8 * j + 1]), pack_bf16(v[8 * j + 2], v[8 * j + 3]),
+                            pack_bf16(v[8 * j + 4], v[8 * j + 5]), pack_bf16(v[8 * j + 6], v[8 * j + 7]));
+    }
+    __syncwarp();
     // layer 1: [16 x 240] x [240 x 64]
     float h[8][4];
 #pragma unroll
     for (int j = 0; j < 8; ++j) h[j][0] = h[j][1] = h[j][2] = h[j][3] = 0.f;
-#pragma unroll 1
+#pragma unroll 5
     for (int kk = 0; kk < IND_KPAD / 16; ++kk) {
       const int k0 = kk * 16 + 2 * t, k1 = k0 + 8;
-      auto fv = [&](const int* el, bool ok, int k) { return (ok && k < MLP_IN) ? indicator_feature(a.modes, el, k) : 0.f; };
       uint32_t af[4];
-      af[0] = pack_bf16(fv(el0, ok0, k0), fv(el0, ok0, k0 + 1));
-      af[1] = pack_bf16(fv(el1, ok1, k0), fv(el1, ok1, k0 + 1));
-      af[2] = pack_bf16(fv(el0, ok0, k1), fv(el0, ok0, k1 + 1));
-      af[3] = pack_bf16(fv(el1, ok1, k1), fv(el1, ok1, k1 + 1));
+      af[0] = ftw[(g * IND_FTS + k0) >> 1];
+      af[1] = ftw[((g + 8) * IND_FTS + k0) >> 1];
+      af[2] = ftw[(g * IND_FTS + k1) >> 1];
+      af[3] = ftw[((g + 8) * IND_FTS + k1) >> 1];
 #pragma unroll
       for (int j = 0; j < 8; ++j) {
         const int n = 8 * j + g;
@@ -356,10 +411,10 @@ __global__ void __launch_bounds__(128) indicator_infer_kernel(const IndicatorArg
 #pragma unroll
     for (int j = 0; j < 8; ++j) {
       const int c = 8 * j + 2 * t;
-      h[j][0] = gelu_f(h[j][0] + vs[c]);
-      h[j][1] = gelu_f(h[j][1] + vs[c + 1]);
-      h[j][2] = gelu_f(h[j][2] + vs[c]);
-      h[j][3] = gelu_f(h[j][3] + vs[c + 1]);
+      h[j][0] = gelu_fast(h[j][0] + vs[c]);
+      h[j][1] = gelu_fast(h[j][1] + vs[c + 1]);
+      h[j][2] = gelu_fast(h[j][2] + vs[c]);
+      h[j][3] = gelu_fast(h[j][3] + vs[c + 1]);
     }
     // layer 2: [16 x 64] x [64 x 64], A fragments from the layer-1 accumulators
     float h2[8][4];
@@ -384,30 +439,39 @@ __global__ void __launch_bounds__(128) indicator_infer_kernel(const IndicatorArg
 #pragma unroll
     for (int j = 0; j < 8; ++j) {
       const int c = 8 * j + 2 * t;
-      z0 += gelu_f(h2[j][0] + vs[MLP_H + c]) * vs[2 * MLP_H + c] + gelu_f(h2[j][1] + vs[MLP_H + c + 1]) * vs[2 * MLP_H + c + 1];
-      z1 += gelu_f(h2[j][2] + vs[MLP_H + c]) * vs[2 * MLP_H + c] + gelu_f(h2[j][3] + vs[MLP_H + c + 1]) * vs[2 * MLP_H + c + 1];
+      z0 += gelu_fast(h2[j][0] + vs[MLP_H + c]) * vs[2 * MLP_H + c] + gelu_fast(h2[j][1] + vs[MLP_H + c + 1]) * vs[2 * MLP_H + c + 1];
+      z1 += gelu_fast(h2[j][2] + vs[MLP_H + c]) * vs[2 * MLP_H + c] + gelu_fast(h2[j][3] + vs[MLP_H + c + 1]) * vs[2 * MLP_H + c + 1];
     }
     z0 += __shfl_xor_sync(0xffffffffu, z0, 1);
     z0 += __shfl_xor_sync(0xffffffffu, z0, 2);
     z1 += __shfl_xor_sync(0xffffffffu, z1, 1);
     z1 += __shfl_xor_sync(0xffffffffu, z1, 2);
+    // decisions; flagged rows appended to the list with one atomic per warp
+    const float b3 = vs[3 * MLP_H];
+    bool f0 = false, f1 = false;
     if (t == 0) {
-      const float b3 = vs[3 * MLP_H];
       if (ok0) {
         const float sc = 1.f / (1.f + expf(-(z0 + b3)));
         a.score[r0] = sc;
-        const bool f = sc > a.threshold;
-        a.flag[r0] = f;
-        if (f) a.list[atomicAdd(a.count, 1)] = r0;
+        f0 = sc > a.threshold;
+        a.flag[r0] = f0;
       }
       if (ok1) {
         const float sc = 1.f / (1.f + expf(-(z1 + b3)));
         a.score[r1] = sc;
-        const bool f = sc > a.threshold;
-        a.flag[r1] = f;
-        if (f) a.list[atomicAdd(a.count, 1)] = r1;
+        f1 = sc > a.threshold;
+        a.flag[r1] = f1;
       }
     }
+    const unsigned m0 = __ballot_sync(0xffffffffu, f0), m1 = __ballot_sync(0xffffffffu, f1);
+    const int n0 = __popc(m0), ntot = n0 + __popc(m1);
+    int base = 0;
+    if (lane == 0 && ntot) base = atomicAdd(a.count, ntot);
+    base = __shfl_sync(0xffffffffu, base, 0);
+    const unsigned below = (1u << lane) - 1u;
+    if (f0) a.list[base + __popc(m0 & below)] = r0;
+    if (f1) a.list[base + n0 + __popc(m1 & below)] = r1;
+    __syncwarp();
   }
 }
 

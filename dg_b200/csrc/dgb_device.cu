@@ -536,8 +536,13 @@ void launch_indicator(dgb_ctx* c, const double* U) {
   a.w1 = c->ind_w; a.w2 = c->ind_w + MLP_H * IND_KPAD; a.vec = c->ind_vec;
   a.score = c->ind_score; a.flag = c->ind_flag; a.list = c->ind_list; a.count = c->ind_list + c->ld; a.scal = c->scal;
   const int ntiles = (c->ne + 15) / 16;
-  const int grid = std::min((ntiles + 3) / 4, 148 * 4);
-  indicator_infer_kernel<<<grid, 128, 0, c->st>>>(a);
+  const int grid = std::min((ntiles + 3) / 4, 148 * 3);  // persistent: 3 CTAs of 73 KB per SM
+  static bool attr = false;
+  if (!attr) {
+    cudaFuncSetAttribute(indicator_infer_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)IND_SMEM_BYTES);
+    attr = true;
+  }
+  indicator_infer_kernel<<<grid, 128, IND_SMEM_BYTES, c->st>>>(a);
   c->counter += 2;
 }
 
@@ -1079,7 +1084,8 @@ extern "C" int dgb_set_indicator(dgb_ctx* c, const float* params, float threshol
   }
   std::vector<__nv_bfloat16> w((size_t)MLP_H * IND_KPAD + MLP_H * MLP_H, __float2bfloat16(0.f));
   for (int j = 0; j < MLP_H; ++j)
-    for (int k = 0; k < MLP_IN; ++k) w[(size_t)j * IND_KPAD + k] = __float2bfloat16(params[MLP_W1 + j * MLP_IN + k]);
+    for (int k = 0; k < MLP_IN; ++k)  // input k = 45 n + r sits at column 48 n + r
+      w[(size_t)j * IND_KPAD + IND_NSEG * (k / 45) + k % 45] = __float2bfloat16(params[MLP_W1 + j * MLP_IN + k]);
   for (int j = 0; j < MLP_H; ++j)
     for (int i = 0; i < MLP_H; ++i) w[(size_t)MLP_H * IND_KPAD + j * MLP_H + i] = __float2bfloat16(params[MLP_W2 + j * MLP_H + i]);
   std::vector<float> vec(3 * MLP_H + 1);

@@ -209,7 +209,7 @@ int dgb_kernel_timing(dgb_ctx* c, const char* name, double* ms, long long* launc
  * Learned troubled-cell indicator (no counterpart in the reference)
  * ------------------------------------------------------------------------------------
  * A 225 -> 64 -> 64 -> 1 MLP (GELU, sigmoid) reads each element's and its four neighbours'
- * normalised scaled-Taylor modes (2D, p = 2; each input compressed by asinh(x / 1e-7) / asinh(1e7))
+ * normalised scaled-Taylor modes (2D, p = 2; each input compressed by sign(x) log(1 + |x| / 1e-7) / log(1 + 1e7))
  * and predicts whether the problem's limiter would change the element.  Parameters: one FP32 array of dgb_mlp_param_count() values laid out as
  * W1[64][225], b1[64], W2[64][64], b2[64], w3[64], b3.  Pointers marked _dev are device memory. */
 int dgb_mlp_param_count(void);

@@ -95,8 +95,8 @@ FEAT_S0 = 1e-7
 
 
 def compress(x):
-    """The fixed signed-log compression of the inputs: asinh(x / 1e-7) / asinh(1e7)."""
-    return np.arcsinh(x / FEAT_S0) / np.arcsinh(1.0 / FEAT_S0)
+    """The fixed signed-log compression of the inputs: sign(x) log(1 + |x| / 1e-7) / log(1 + 1e7)."""
+    return np.sign(x) * np.log1p(np.abs(x) / FEAT_S0) / np.log1p(1.0 / FEAT_S0)
 
 
 def features(S: O.Setup, U, perm):

@@ -102,3 +102,45 @@ def test_gated_limiter_matches_oracle(threshold):
     S = O.Setup.from_problem(prob)
     flags = sc > threshold
     assert rel_err(out, M.gated_m2(S, U, flags)) < 1e-12
+
+
+def test_trained_indicator_gain():
+    """What the trained network (dg_b200/data/indicator_p2.npz) buys: on held-out four-quadrant
+    problems it finds >= 95% of the cells the full limiter changes while flagging at most 1.3x as
+    many cells as there are troubled ones; on the shock-bubble it limits a minority of cells and
+    stays within 1e-4 (relative L1 density) of the full-limiter solution after 100 steps, while
+    dropping the limiter altogether departs from it by far more (or fails)."""
+    import dg_b200 as dgb
+    from dg_b200 import learned as L
+    params, meta = L.load()
+    X, y = L.generate_dataset([20001, 20002], 64, 64)
+    ev = L.evaluate(params, X, y, 0.2)
+    assert ev["recall"] >= 0.95
+    assert ev["flagged_fraction"] <= 1.3 * ev["label_fraction"]
+
+    walls = ("reflective", "transmissive", "reflective", "transmissive")
+    prob = dgb.Problem.structured(2, 2, 128, 64, 0.0, 2.0, 0.0, 1.0, walls, flux="rusanov", limiter="m2l", cfl=0.3)
+    none = dgb.Problem.structured(2, 2, 128, 64, 0.0, 2.0, 0.0, 1.0, walls, flux="rusanov", limiter="none", cfl=0.3)
+    full, learned, plain = dgb.DGSolver(prob), dgb.DGSolver(prob), dgb.DGSolver(none)
+    try:
+        U0 = full.limit(prob.init_state("shock_bubble", seed=7))
+        dt = 0.8 * full.dt_from_cfl(U0)
+        L.set_indicator(learned, params, 0.2)
+        out = {}
+        for name, s in (("full", full), ("learned", learned), ("none", plain)):
+            s.set_state(U0)
+            try:
+                s.advance(100, dt)
+                out[name] = s.get_state()
+            except dgb.DGBError:
+                out[name] = None
+        i = prob.info
+        rho = {k: (v.reshape(i.n_elem, i.n_fields, i.n_s)[:, 0] if v is not None else None) for k, v in out.items()}
+        dev = lambda k: float(np.abs(rho[k] - rho["full"]).sum() / np.abs(rho["full"]).sum())
+        assert rho["learned"] is not None and dev("learned") < 1e-4
+        _, cnt = L.scores(learned, out["learned"])
+        assert cnt < 0.5 * i.n_elem
+        assert rho["none"] is None or not np.all(np.isfinite(rho["none"])) or dev("none") > 10 * dev("learned")
+    finally:
+        for s in (full, learned, plain):
+            s.close()
