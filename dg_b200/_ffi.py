@@ -27,6 +27,7 @@ EXPORTS = [
     "dgb_conservation", "dgb_last_timing", "dgb_set_profiling", "dgb_kernel_timing", "dgb_limit_noalloc",
     "dgb_sensors", "dgb_set_form", "dgb_mlp_param_count", "dgb_indicator_features", "dgb_indicator_labels",
     "dgb_mlp_forward", "dgb_mlp_backward", "dgb_mlp_adam", "dgb_set_indicator", "dgb_indicator_scores",
+    "dgb_cfl_dt",
 ]
 
 
@@ -90,6 +91,7 @@ def lib() -> C.CDLL:
         "dgb_limit": [vp, dp],
         "dgb_sensors": [vp, dp, C.POINTER(C.c_int)],
         "dgb_set_form": [vp, ip],
+        "dgb_cfl_dt": [vp, dp],
         "dgb_indicator_features": [vp, vp],
         "dgb_indicator_labels": [vp, vp],
         "dgb_mlp_forward": [vp, vp, ip, vp, vp, vp],

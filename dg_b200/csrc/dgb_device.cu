@@ -1149,6 +1149,19 @@ extern "C" int dgb_sensors(dgb_ctx* c, const double* U, int* flags) {
   return DGB_OK;
 }
 
+extern "C" int dgb_cfl_dt(dgb_ctx* c, double* dt) {
+  if (!c || !dt) return set_error(DGB_ERR_ARG, "null argument");
+  DGB_CUDA(cudaSetDevice(c->device));
+  if (int rc = reset_scalars(c, 0.0)) return rc;
+  launch_dt(c, c->A, true);
+  DGB_CUDA(cudaGetLastError());
+  if (int rc = read_scalars(c)) return rc;
+  if (c->h_scal->flags & FLAG_NONFINITE) return set_error(DGB_ERR_NONFINITE, "time step is NaN");
+  if (c->h_scal->flags & FLAG_DT_SMALL) return set_error(DGB_ERR_DT_SMALL, "next time step is too small (< 1e-14)");
+  *dt = c->h_scal->dt;
+  return DGB_OK;
+}
+
 extern "C" int dgb_dt_from_cfl(dgb_ctx* c, const double* U, double* dt) {
   if (!c || !U || !dt) return set_error(DGB_ERR_ARG, "null argument");
   DGB_CUDA(cudaSetDevice(c->device));

@@ -65,6 +65,8 @@ struct Problem {
   std::vector<double> output_times;
   double final_time = 0.0;
   std::string deck_dir;
+  std::string deck_ic;                // "#initial condition" of the deck ("" for built problems)
+  std::vector<double> deck_ic_inputs; // "#ic inputs"
   // sizes
   int N_E = 0, N_s = 0, N_G = 0, M_T = 0, M_s = 0, M_G = 0, N_N = 0, M_B = 0;
   int elem_type = 0, face_type = 0;

@@ -86,6 +86,8 @@ extern "C" int dgb_problem_from_deck(const char* deck_path, dgb_problem** out) {
                           d.thresholds, outt, tf, pr->P);
   if (!st.ok()) { delete pr; return set_error(st.code, st.msg); }
   pr->P.deck_dir = dir;
+  pr->P.deck_ic = d.ic;
+  pr->P.deck_ic_inputs = d.ic_inputs;
   *out = pr;
   return DGB_OK;
 }
@@ -204,9 +206,13 @@ extern "C" int dgb_problem_get_array(const dgb_problem* p, const char* name, voi
 
 extern "C" int dgb_problem_init_state(const dgb_problem* p, const char* ic, const double* params, int nparams,
                                       uint64_t seed, double* U) {
-  if (!p || !ic || !U || (nparams > 0 && !params)) return set_error(DGB_ERR_ARG, "null argument");
+  if (!p || !U || (nparams > 0 && !params)) return set_error(DGB_ERR_ARG, "null argument");
   std::vector<double> prm(params, params + std::max(0, nparams));
-  dgb::Status st = dgb::init_state(p->P, ic, prm, seed, U);
+  if (!ic) {  // the deck's own initial condition and inputs
+    if (p->P.deck_ic.empty()) return set_error(DGB_ERR_ARG, "the problem has no deck initial condition");
+    if (nparams == 0) prm = p->P.deck_ic_inputs;
+  }
+  dgb::Status st = dgb::init_state(p->P, ic ? std::string(ic) : p->P.deck_ic, prm, seed, U);
   return st.ok() ? DGB_OK : set_error(st.code, st.msg);
 }
 

@@ -141,6 +141,7 @@ int dgb_problem_get_array(const dgb_problem* p, const char* name, void* dst, siz
  * perturbation of the radius), "quadrants" (four-quadrant Riemann problem, seeded states). */
 int dgb_problem_init_state(const dgb_problem* p, const char* ic, const double* params, int nparams,
                            uint64_t seed, double* U);
+/* (ic == NULL selects the deck's "#initial condition" and, when nparams == 0, its "#ic inputs".) */
 
 /* Output in the reference .pos format (code/src/mesh/simpleMesh.cc:322-376 via
  * code/src/printer/printer.cc:77): one file per primitive field, <dir>/<name><step>.pos. */
@@ -180,6 +181,8 @@ int dgb_sensors(dgb_ctx* c, const double* U_host, int* flags_host);
 /* Selects the arithmetic of the residual kernels (enum dgb_form) for later calls; no counterpart
  * in the reference, which is FP64 only. */
 int dgb_set_form(dgb_ctx* c, int form);
+/* CFL step of the context's current (device-resident) state, as dgb_dt_from_cfl computes it. */
+int dgb_cfl_dt(dgb_ctx* c, double* dt);
 /* Dt = CFL_scaled / max_nodes(|u|+a) (RK::DtFromCFL, rk.cc:250-272). */
 int dgb_dt_from_cfl(dgb_ctx* c, const double* U_host, double* dt);
 

@@ -144,7 +144,40 @@ def make_case(c: dict, seed: int) -> dict:
     return out
 
 
+def read_pos(path: Path):
+    """(name, time, step, values [N_E][nodes]) of a Gmsh ElementNodeData file."""
+    lines = path.read_text().split("\n")
+    name = lines[5].strip().strip('"')
+    time = float(lines[7])
+    step = int(lines[9])
+    ne = int(lines[11])
+    vals = [[float(x) for x in lines[13 + e].split()[2:]] for e in range(ne)]
+    return name, time, step, np.array(vals)
+
+
+# the reference executable's own time loop and output on a deck (the drop-in check of dgbexec)
+DRIVER = dict(name="driver_d1_sodtube_roe_m2l", dim=1, order=2, nx=60, dom=(-0.5, 0.5), flux="roe", limiter="m2l",
+              cfl=0.4, output_times=(0.0, 0.02, 0.05, 0.08))
+
+
+def make_driver_fixture() -> dict:
+    c = DRIVER
+    ref = RefCase(c["dim"], c["order"], c["nx"], 1, c["dom"][0], c["dom"][1], 0.0, 1.0, ("transmissive",) * 4,
+                  c["flux"], c["limiter"], cfl=c["cfl"], output_times=c["output_times"])
+    ref.write_deck()
+    ref.run("none")
+    out = {"deck": np.array((ref.workdir / "deck.inp").read_text())}
+    for f in sorted(ref.workdir.glob("*.pos")):
+        name, time, step, vals = read_pos(f)
+        out[f"pos_{f.stem}"] = vals
+        out[f"time_{f.stem}"] = np.array([time])
+    out["meta"] = np.array(json.dumps(c))
+    return out
+
+
 def main() -> int:
+    np.savez_compressed(OUT / f"{DRIVER['name']}.npz", **make_driver_fixture())
+    print(f"wrote {DRIVER['name']}.npz")
     for k, c in enumerate(CASES):
         data = make_case(c, seed=100 + k)
         np.savez_compressed(OUT / f"{c['name']}.npz", **data)
