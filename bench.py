@@ -202,6 +202,22 @@ def run_reference(args):
     return 0
 
 
+def max_over_ranks(value: float, ws: int, device: str) -> float:
+    """Max of a per-rank time over all ranks (identity on one rank); every rank must call it."""
+    if ws <= 1:
+        return value
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([value], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def whole_job_rate(ws: int, dof: int, steps: int, t_max_s: float) -> float:
+    """DOF*stages/s of all replicas together: every rank advances its own copy of the workload."""
+    return ws * dof * STAGES_PER_STEP * steps / t_max_s
+
+
 def time_steps(dgb, solver, steps, warmup, flush):
     """Device time (ms) and launches of `steps` SSP-RK3 steps, L2 flushed before each one."""
     import torch
@@ -366,12 +382,8 @@ def main(argv=None) -> int:
     if ws > 1:
         dist.barrier()
     clocks = clk.summary()
-    t_s = dev_ms / 1e3
-    if ws > 1:
-        tt = torch.tensor([t_s], device=f"cuda:{dev}")
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        t_s = float(tt.item())
-    value = ws * dof * STAGES_PER_STEP * args.steps / t_s
+    t_s = max_over_ranks(dev_ms / 1e3, ws, f"cuda:{dev}")
+    value = whole_job_rate(ws, dof, args.steps, t_s)
 
     # per-kernel device time (profiled pass over the same number of steps, same state evolution)
     solver.set_profiling(True)
@@ -401,11 +413,8 @@ def main(argv=None) -> int:
         solver.advance(1, 0.0, scheme=dgb.SSPRK3)
         hostv[:] = solver.get_state()
     e2e_s = time.perf_counter() - t0
-    if ws > 1:
-        tt = torch.tensor([e2e_s], device=f"cuda:{dev}")
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        e2e_s = float(tt.item())
-    e2e = {"value": ws * dof * STAGES_PER_STEP * args.e2e_steps / e2e_s, "unit": UNIT,
+    e2e_s = max_over_ranks(e2e_s, ws, f"cuda:{dev}")
+    e2e = {"value": whole_job_rate(ws, dof, args.e2e_steps, e2e_s), "unit": UNIT,
            "h2d_bytes_per_step": n_state * 8, "d2h_bytes_per_step": n_state * 8,
            "steps": args.e2e_steps}
 
