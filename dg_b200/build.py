@@ -32,6 +32,8 @@ NVFLAGS = ["-std=c++17", "-O3", "-lineinfo", "-Xcompiler", "-fPIC", "--expt-rela
 # per-file additions: the sensors take threshold decisions that must see the same separately
 # rounded products and sums as the reference's CPU arithmetic, so no multiply-add contraction there
 FILE_NVFLAGS = {"dgb_sensor.cu": ["-fmad=false"]}
+SHIMS = [(1, "rus"), (1, "hll"), (1, "roe"), (2, "rus"), (2, "roe")]
+SHIM_FLUX = {"rus": 0, "hll": 1, "roe": 2}
 
 
 def _deps_digest(paths: list[Path]) -> str:
@@ -59,7 +61,7 @@ def build(force: bool = False, verbose: bool = False) -> Path:
     objs = []
     jobs = []
     for src in sorted(SRC.rglob("*.cc")) + sorted(SRC.rglob("*.cu")):
-        if src.name == "dgbexec.cc":
+        if src.name == "dgbexec.cc" or "shim" in src.parts:
             continue
         key = hashlib.sha1((hdr + src.read_text()).encode()).hexdigest()[:12]
         obj = BUILD / f"{src.stem}.{key}.o"
@@ -78,7 +80,7 @@ def build(force: bool = False, verbose: bool = False) -> Path:
             for f in [ex.submit(_run, j, verbose) for j in jobs]:
                 f.result()
     for stale in BUILD.glob("*.o"):
-        if stale not in objs:
+        if stale not in objs and not stale.name.startswith("dgb_shim_"):
             stale.unlink()
     stamp = hashlib.sha1("".join(str(o) for o in objs).encode()).hexdigest()
     stamp_file = BUILD / "libdgb.stamp"
@@ -87,6 +89,19 @@ def build(force: bool = False, verbose: bool = False) -> Path:
         _run([NVCC] + ARCH + ["-shared", "-o", str(tmp)] + [str(o) for o in objs], verbose)
         os.replace(tmp, LIB)
         stamp_file.write_text(stamp)
+    # link-compatible shims of the reference's kernel launchers, one per (dimension, flux)
+    shim_src = SRC / "shim" / "dgb_shim.cu"
+    sensor_obj = next(o for o in objs if o.name.startswith("dgb_sensor."))
+    for d, flux in SHIMS:
+        out = LIBDIR / f"libdgb_shim_{d}d_{flux}.so"
+        key = hashlib.sha1((hdr + shim_src.read_text() + str(sensor_obj)).encode()).hexdigest()[:12]
+        obj = BUILD / f"dgb_shim_{d}d_{flux}.{key}.o"
+        if force or not obj.exists():
+            _run([NVCC] + NVFLAGS + [f"-DDGB_SHIM_D={d}", f"-DDGB_SHIM_FLUX={SHIM_FLUX[flux]}", f"-I{INC}", f"-I{SRC}",
+                                     "-c", str(shim_src), "-o", str(obj)], verbose)
+            _run([NVCC] + ARCH + ["-shared", "-o", str(out), str(obj), str(sensor_obj)], verbose)
+        elif not out.exists():
+            _run([NVCC] + ARCH + ["-shared", "-o", str(out), str(obj), str(sensor_obj)], verbose)
     drv = SRC / "dgbexec.cc"
     if drv.exists() and (force or not EXE.exists() or EXE.stat().st_mtime < max(LIB.stat().st_mtime, drv.stat().st_mtime)):
         _run(["g++", "-std=c++17", "-O2", f"-I{INC}", str(drv), "-o", str(EXE), f"-L{LIBDIR}", "-ldgb",

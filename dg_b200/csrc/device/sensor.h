@@ -23,5 +23,7 @@ struct SensorLaunch {
 
 // Enqueues the sensor evaluation on `st`; returns 0 or a cudaError_t value.
 int launch_sensors(const SensorLaunch& s, cudaStream_t st);
+// Same, from cell means already in s.mean (mean[f*ld + e]); s.U and s.iperm are not used.
+int launch_sensors_from_means(const SensorLaunch& s, cudaStream_t st);
 
 }  // namespace dgb

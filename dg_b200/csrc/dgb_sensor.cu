@@ -179,6 +179,7 @@ __global__ void __launch_bounds__(256) sensor_finalize_kernel(int n_elem, int ld
 
 int launch_sensors(const SensorLaunch& s, cudaStream_t st) {
   const int g = (s.n_elem + 255) / 256;
+  if (s.U == nullptr) return launch_sensors_from_means(s, st);
   switch (s.ns) {
     case 2: cell_means_kernel<2><<<g, 256, 0, st>>>(s.U, s.iperm, s.n_elem, s.nf, s.ld, s.mean); break;
     case 3: cell_means_kernel<3><<<g, 256, 0, st>>>(s.U, s.iperm, s.n_elem, s.nf, s.ld, s.mean); break;
@@ -187,6 +188,11 @@ int launch_sensors(const SensorLaunch& s, cudaStream_t st) {
     case 16: cell_means_kernel<16><<<g, 256, 0, st>>>(s.U, s.iperm, s.n_elem, s.nf, s.ld, s.mean); break;
     default: return (int)cudaErrorInvalidValue;
   }
+  return launch_sensors_from_means(s, st);
+}
+
+int launch_sensors_from_means(const SensorLaunch& s, cudaStream_t st) {
+  const int g = (s.n_elem + 255) / 256;
   DetectArgs a{s.n_elem, s.ld, s.n_nbr, s.on[0], s.on[1], s.on[2], s.th[0], s.th[1], s.th[2]};
   if (s.D == 2) sensor_detect_kernel<2><<<g, 256, 0, st>>>(a, s.mean, s.nbr, s.target, s.type);
   else sensor_detect_kernel<1><<<g, 256, 0, st>>>(a, s.mean, s.nbr, s.target, s.type);
