@@ -15,6 +15,10 @@ device-side CFL step.  DOF = N_E * N_s * N_F = 5,898,240.
              on average for SSP-RK3) / its average device time from a profiled pass of the same steps
   cpu_baseline  the reference CPU build (oracle/_ref, compiled from the reference sources) on a
              bounded sample of the same workload, one process on one core
+  forms      plain FP64, mixed and mixed + learned indicator at equal L1 error (same protocol)
+  ensemble   the batched ensemble (256 independent cases of uneven sizes, dgb_batch): aggregate
+             DOF*stages/s against the same cases advanced one after another, autotuned tiling,
+             per-case completion times for a common end time
 
 --impl reference runs the reference CPU implementation (oracle/_ref) on the host cores: one process
 per core, each advancing its own copy of the workload; a bench step there is one SSP-RK3 stage
@@ -319,6 +323,89 @@ def compare_forms(dgb, U0_coarse, dev, steps, warmup, flush, acc_steps=200):
     return out
 
 
+ENSEMBLE_SEED = 11
+ENSEMBLE_T_END = 1e-4
+
+
+def ensemble_cases(dgb, seed=ENSEMBLE_SEED):
+    """The batched-ensemble workload: 192 1D two-fluid Riemann problems on [0,1] with element counts
+    log-uniform in [200, 20000] and p uniform in {1, 2, 3}, and 64 2D four-quadrant Riemann problems
+    on the unit square with square meshes of side log-uniform in [64, 512] (rounded to a multiple
+    of 32), p = 2; all Rusanov, m2l, CFL 0.3, FP64, transmissive boundaries; seeded left/right and
+    quadrant states (rho, p ~ U[0.1, 2], u, v ~ U[-1, 1], gamma in {1.4, 1.67})."""
+    rng = np.random.default_rng(seed)
+    cases = []
+    for k in range(192):
+        ne = int(round(np.exp(rng.uniform(np.log(200), np.log(20000)))))
+        p = int(rng.integers(1, 4))
+        prob = dgb.Problem.structured(1, p, ne, 1, 0.0, 1.0, bc=("transmissive",) * 2, flux="rusanov",
+                                      limiter="m2l", cfl=CFL)
+        cases.append((prob, prob.init_state("riemann", seed=1000 + k)))
+    for k in range(64):
+        n = int(32 * round(np.exp(rng.uniform(np.log(64), np.log(512))) / 32))
+        prob = dgb.Problem.structured(2, 2, n, n, 0.0, 1.0, 0.0, 1.0, bc=("transmissive",) * 4, flux="rusanov",
+                                      limiter="m2l", cfl=CFL)
+        cases.append((prob, prob.init_state("quadrants", seed=2000 + k)))
+    return cases
+
+
+def ensemble(dgb, dev, steps, warmup):
+    """Batched ensemble: all cases in one dgb_batch (a persistent launch per element class and
+    operator, one CUDA graph per step), autotuned; against the same cases advanced one after another
+    with dgb_advance.  Device time (CUDA events) over `steps` steps, each case with its own CFL
+    step; then every case run to t = ENSEMBLE_T_END for the per-case completion times."""
+    t0 = time.perf_counter()
+    cases = ensemble_cases(dgb)
+    setup_s = time.perf_counter() - t0
+    solvers, starts = [], []
+    for prob, U0 in cases:
+        s = dgb.DGSolver(prob, device=dev)
+        U = s.limit(U0)  # the reference limits the initial condition (rk.cc:108-114)
+        s.set_state(U)
+        solvers.append(s)
+        starts.append(U)
+    dof = np.array([p.info.n_elem * p.info.n_s * p.info.n_fields for p, _ in cases], dtype=np.float64)
+    b = dgb.DGBatch(solvers)
+    classes = b.autotune(5)
+    b.advance(warmup)
+    b.advance(steps)
+    ms, launches = b.last_timing()
+    _, case_steps, _ = b.case_stats()
+    value = float((dof * case_steps).sum() * STAGES_PER_STEP / (ms / 1e3))
+    # completion time of every case for a common end time
+    for s, U in zip(solvers, starts):
+        s.set_state(U)
+    n_end = b.advance(100000, ENSEMBLE_T_END)
+    end_ms, _ = b.last_timing()
+    t_case, st_case, wall = b.case_stats()
+    b.close()
+    # the same cases one after another, each through its own context and graph
+    seq_ms = 0.0
+    for s, U in zip(solvers, starts):
+        s.set_state(U)
+        s.advance(warmup, 0.0, scheme=dgb.SSPRK3)
+        s.advance(steps, 0.0, scheme=dgb.SSPRK3)
+        seq_ms += s.last_timing()[0]
+    for s in solvers:
+        s.close()
+    seq_value = float(dof.sum() * steps * STAGES_PER_STEP / (seq_ms / 1e3))
+    w = np.sort(wall[wall >= 0])
+    return {"workload": "192 1D Riemann (N_E log-uniform 200..20000, p 1-3) + 64 2D quadrants (64^2..512^2, p=2), "
+                        "Rusanov, m2l, SSP-RK3, CFL 0.3 per case, FP64",
+            "cases": len(cases), "dof_total": int(dof.sum()), "dof_1d": int(dof[:192].sum()),
+            "dof_2d": int(dof[192:].sum()), "steps": steps,
+            "value": value, "unit": UNIT, "ms_per_step": ms / steps, "gpu_launches_per_step": launches / max(steps, 1),
+            "one_after_another": {"value": seq_value, "ms_per_step": seq_ms / steps},
+            "speedup_vs_one_after_another": value / seq_value,
+            "hbm_algorithmic_gbs": value * BYTES_PER_DOF_STAGE / 1e9,
+            "classes": classes,
+            "to_t_end": {"t_end": ENSEMBLE_T_END, "graph_steps": n_end, "ms": end_ms,
+                         "case_steps_min_median_max": [int(st_case.min()), float(np.median(st_case)), int(st_case.max())],
+                         "case_wall_ms_min_median_max": [float(w[0]), float(np.median(w)), float(w[-1])] if w.size else None,
+                         "all_at_t_end": bool(np.all(t_case == ENSEMBLE_T_END))},
+            "host_setup_s": setup_s}
+
+
 def main(argv=None) -> int:
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -333,6 +420,8 @@ def main(argv=None) -> int:
                     help="arithmetic of the residual (fp64: the plain parity form)")
     ap.add_argument("--learned", action="store_true", help="gate the limiter with the learned indicator")
     ap.add_argument("--no-forms", action="store_true", help="skip the mixed / learned form comparison")
+    ap.add_argument("--no-ensemble", action="store_true", help="skip the batched-ensemble measurement")
+    ap.add_argument("--ensemble-only", action="store_true", help="print only the batched-ensemble measurement")
     args = ap.parse_args(argv)
     if args.impl == "reference":
         return run_reference(args)
@@ -347,6 +436,11 @@ def main(argv=None) -> int:
         dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=120))
     torch.cuda.set_device(local)
     dev = local
+
+    if args.ensemble_only:
+        if rank == 0:
+            print(json.dumps({"ensemble": ensemble(dgb, dev, min(args.steps, 20), args.warmup)}))
+        return 0
 
     prob, U0 = build_problem(args.nx, args.ny)
     solver = dgb.DGSolver(prob, device=dev)
@@ -425,6 +519,10 @@ def main(argv=None) -> int:
     if ws == 1 and not args.no_forms and (args.nx, args.ny) == (NX, NY):
         forms = compare_forms(dgb, U0, dev, args.steps, args.warmup, flush)
 
+    ens = None
+    if ws == 1 and not args.no_ensemble and (args.nx, args.ny) == (NX, NY):
+        ens = ensemble(dgb, dev, min(args.steps, 20), args.warmup)
+
     form_cfg = {"form": ("plain FP64" if args.form == "fp64" else
                          "mixed: FP32 contractions/Rusanov flux on FP64 anchors, FP64 pressure, state and update")
                 + (" + learned indicator (threshold 0.2)" if args.learned else "")}
@@ -444,7 +542,8 @@ def main(argv=None) -> int:
                              "avg_launch_ms": res_avg_s * 1e3, "peak_source": "MEASURED_PEAKS.json hbm_gbs (measured copy)"},
                 "kernel_ms_per_step": {"residual": res_ms / args.steps, "limiter": lim_ms / args.steps,
                                        "dt": dt_ms / args.steps},
-                "cpu_baseline": cpu, "clocks": clocks, "gpu_launches": launches, "forms": forms}
+                "cpu_baseline": cpu, "clocks": clocks, "gpu_launches": launches, "forms": forms,
+                "ensemble": ens}
         print(json.dumps(line))
     solver.close()
     if ws > 1:

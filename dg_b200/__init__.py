@@ -5,6 +5,6 @@ The compute path is ``lib/libdgb.so`` (C++ host setup + sm_100a CUDA kernels) be
 fail when the library or the GPU is missing.
 """
 from ._ffi import DGBError, RK4, SSPRK3  # noqa: F401
-from .solver import DGSolver, Problem, write_msh  # noqa: F401
+from .solver import DGBatch, DGSolver, Problem, write_msh  # noqa: F401
 
-__all__ = ["DGSolver", "Problem", "write_msh", "DGBError", "RK4", "SSPRK3"]
+__all__ = ["DGBatch", "DGSolver", "Problem", "write_msh", "DGBError", "RK4", "SSPRK3"]

@@ -27,7 +27,8 @@ EXPORTS = [
     "dgb_conservation", "dgb_last_timing", "dgb_set_profiling", "dgb_kernel_timing", "dgb_limit_noalloc",
     "dgb_sensors", "dgb_set_form", "dgb_mlp_param_count", "dgb_indicator_features", "dgb_indicator_labels",
     "dgb_mlp_forward", "dgb_mlp_backward", "dgb_mlp_adam", "dgb_set_indicator", "dgb_indicator_scores",
-    "dgb_cfl_dt",
+    "dgb_cfl_dt", "dgb_batch_create", "dgb_batch_destroy", "dgb_batch_n_classes", "dgb_batch_class_info",
+    "dgb_batch_autotune", "dgb_batch_set_tuning", "dgb_batch_advance", "dgb_batch_case_stats", "dgb_batch_last_timing",
 ]
 
 
@@ -107,6 +108,14 @@ def lib() -> C.CDLL:
         "dgb_set_profiling": [vp, ip],
         "dgb_kernel_timing": [vp, cp, dp, C.POINTER(C.c_longlong)],
         "dgb_limit_noalloc": [vp, vp, vp, vp],
+        "dgb_batch_create": [C.POINTER(vp), ip, C.POINTER(vp)],
+        "dgb_batch_n_classes": [vp],
+        "dgb_batch_class_info": [vp, ip, C.POINTER(C.c_int)],
+        "dgb_batch_autotune": [vp, ip],
+        "dgb_batch_set_tuning": [vp, ip, ip, ip, ip, ip],
+        "dgb_batch_advance": [vp, ip, C.c_double, C.POINTER(C.c_int)],
+        "dgb_batch_case_stats": [vp, dp, C.POINTER(C.c_int), dp],
+        "dgb_batch_last_timing": [vp, dp, C.POINTER(C.c_longlong)],
     }
     for name, args in sig.items():
         f = getattr(L, name)
@@ -118,6 +127,8 @@ def lib() -> C.CDLL:
     L.dgb_problem_destroy.restype = None
     L.dgb_destroy.argtypes = [vp]
     L.dgb_destroy.restype = None
+    L.dgb_batch_destroy.argtypes = [vp]
+    L.dgb_batch_destroy.restype = None
     _lib = L
     return L
 

@@ -1,0 +1,75 @@
+// The device context of one problem (the opaque dgb_ctx of include/dgb.h), shared by the
+// single-problem entry points (dgb_device.cu) and the batched ensemble (dgb_batch.cu).
+#pragma once
+#include <cuda.h>
+#include <cuda_bf16.h>
+#include <cuda_runtime.h>
+
+#include <string>
+#include <utility>
+#include <vector>
+
+#include "../../include/dgb.h"
+#include "device/common.cuh"
+#include "device/limiter_gated.cuh"
+#include "device/sensor.h"
+
+namespace dgb {
+enum { KC_RESIDUAL = 0, KC_LIMITER = 1, KC_DT = 2, KC_OTHER = 3, KC_N = 4 };
+}
+
+struct dgb_ctx {
+  int device = 0;
+  cudaStream_t st = nullptr;
+  int D = 1, p = 1, nf = 4, ns = 2, ne = 0, ld = 0, flux = 2, limiter = 0;
+  int nx = 0, ny = 0;
+  bool tiled = false;     // structured row-major grid with tile-multiple extents: tiled residual kernel
+  int form = DGB_FORM_FP64;  // arithmetic of the residual: plain FP64 or mixed FP32/FP64
+  bool rowmajor = false;  // structured row-major grid: tiled limiter passes
+  bool fused_lim = false; // row-major grid, hrl / m2l: both limiter passes in one kernel (opt-in)
+  CUtensorMap mapA, mapB, mapC;  // TMA descriptors of the state buffers (tiled kernel)
+  double hx = 0, hy = 0;
+  size_t nstate = 0;
+  dgb::Consts cs;
+  double *A = nullptr, *B = nullptr, *C = nullptr, *DU = nullptr, *X = nullptr, *ref = nullptr;
+  int *nbr = nullptr, *perm = nullptr;
+  // sensor-gated limiters (hri, m2i, pri, p0i): sensor work arrays and flags
+  bool gated = false, has_sensors = false;
+  bool ind_on = false;          // learned indicator gates the limiter (dgb_set_indicator)
+  float ind_threshold = 0.2f;
+  float* ind_params = nullptr;  // FP32 parameters (MLP_NPARAM)
+  __nv_bfloat16* ind_w = nullptr;  // W1 [64][IND_KPAD] then W2 [64][64], BF16
+  float* ind_vec = nullptr;     // b1, b2, w3, b3
+  float* ind_modes = nullptr;   // [N_E][IND_MODES]
+  float* ind_score = nullptr;   // [N_E]
+  unsigned char* ind_flag = nullptr;
+  int* ind_list = nullptr;      // [N_E] + count
+  dgb::SensorLaunch sl;
+  int* iperm = nullptr;
+  double* smean = nullptr;
+  int* sint = nullptr;          // target, type, processed, mask, list (ld each), count, flags (ld)
+  dgb::CellAverageWeights p0w;       // p0i: cell-average weights in internal node order
+  dgb::DevScalars* scal = nullptr;
+  dgb::DevScalars* h_scal = nullptr;  // pinned
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  double last_ms = 0.0;
+  long long last_launches = 0;
+  long long launches_per_step = 0;
+  cudaGraphExec_t graphs[2][2] = {{nullptr, nullptr}, {nullptr, nullptr}};
+  long long graph_launches[2][2] = {{0, 0}, {0, 0}};
+  // profiling (per kernel class)
+  bool prof = false;
+  std::vector<std::pair<int, std::pair<cudaEvent_t, cudaEvent_t>>> pev;
+  std::vector<cudaEvent_t> ev_pool;
+  size_t ev_used = 0;
+  double kc_ms[dgb::KC_N] = {0, 0, 0, 0};
+  long long kc_n[dgb::KC_N] = {0, 0, 0, 0};
+  long long counter = 0;  // launches issued since the last reset
+};
+
+
+namespace dgb {
+int set_error(int code, const std::string& msg);
+// TMA descriptor of one of the context's state buffers with a tw x th element box
+bool encode_state_map(dgb_ctx* c, double* ptr, CUtensorMap* map, int tw, int th);
+}

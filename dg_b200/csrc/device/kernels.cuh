@@ -255,15 +255,11 @@ __global__ void __launch_bounds__(NT) residual2d_kernel(const Consts cin, const 
 // ------------------------------------------------------------------------------------------
 // 1D: one thread per element, everything in registers
 // ------------------------------------------------------------------------------------------
+// element e (< c.n_elem) with the problem constants c (in shared memory) and dt
 template <int P, int FLUX, int MODE>
-__global__ void __launch_bounds__(128) residual1d_kernel(const Consts cin, const StageArgs a) {
+__device__ __forceinline__ void res1d_body(const Consts& c, const StageArgs& a, int e, double dt) {
   constexpr int N1 = P + 1, NG = P + 1, NF = 4;
-  __shared__ Consts c;
-  copy_consts(c, cin);
-  if (a.scal && a.scal->flags) return;
-  __syncthreads();
-  const int ld = c.ld, e = blockIdx.x * blockDim.x + threadIdx.x;
-  if (e >= c.n_elem) return;
+  const int ld = c.ld;
   double u[NF][N1], r[NF][N1];
 #pragma unroll
   for (int f = 0; f < NF; ++f)
@@ -322,7 +318,6 @@ __global__ void __launch_bounds__(128) residual1d_kernel(const Consts cin, const
       for (int t = 0; t < N1; ++t) a.out[(size_t)(f * N1 + t) * ld + e] = r[f][t];
     return;
   }
-  const double dt = a.dt_override > 0 ? a.dt_override : a.scal->dt;
 #pragma unroll
   for (int f = 0; f < NF; ++f)
 #pragma unroll
@@ -340,6 +335,18 @@ __global__ void __launch_bounds__(128) residual1d_kernel(const Consts cin, const
         if (a.Uacc) a.Uacc[gi] += a.b * du;
       }
     }
+}
+
+template <int P, int FLUX, int MODE>
+__global__ void __launch_bounds__(128) residual1d_kernel(const Consts cin, const StageArgs a) {
+  __shared__ Consts c;
+  copy_consts(c, cin);
+  if (a.scal && a.scal->flags) return;
+  __syncthreads();
+  const int e = blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= c.n_elem) return;
+  const double dt = MODE == MODE_RESIDUAL ? 0.0 : (a.dt_override > 0 ? a.dt_override : a.scal->dt);
+  res1d_body<P, FLUX, MODE>(c, a, e, dt);
 }
 
 // ------------------------------------------------------------------------------------------
@@ -564,13 +571,9 @@ __global__ void __launch_bounds__(128) lim2d_ypass_kernel(const LimArgs la, cons
 
 // 1D HR / m2 limiter, one thread per element (reads U, writes Uout).
 template <int P, int METHOD>
-__global__ void __launch_bounds__(128) lim1d_kernel(const LimArgs la, const double* __restrict__ U,
-                                                    const int* __restrict__ nbr, double* __restrict__ Uout,
-                                                    const DevScalars* __restrict__ scal) {
+__device__ __forceinline__ void lim1d_body(int ld, int e, const double* __restrict__ U, const int* __restrict__ nbr,
+                                           double* __restrict__ Uout) {
   constexpr int N1 = P + 1;
-  if (scal && scal->flags) return;
-  const int ld = la.ld, e = blockIdx.x * blockDim.x + threadIdx.x;
-  if (e >= la.n_elem) return;
   const int nL = __ldg(nbr + e), nR = __ldg(nbr + (size_t)ld + e);
   const int phys = boundary_code(nL, nR);
   double v[3][4][N1];
@@ -628,6 +631,16 @@ __global__ void __launch_bounds__(128) lim1d_kernel(const LimArgs la, const doub
       Uout[(size_t)(3 * N1 + i) * ld + e] = a_[i];
     }
   }
+}
+
+template <int P, int METHOD>
+__global__ void __launch_bounds__(128) lim1d_kernel(const LimArgs la, const double* __restrict__ U,
+                                                    const int* __restrict__ nbr, double* __restrict__ Uout,
+                                                    const DevScalars* __restrict__ scal) {
+  if (scal && scal->flags) return;
+  const int e = blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= la.n_elem) return;
+  lim1d_body<P, METHOD>(la.ld, e, U, nbr, Uout);
 }
 
 // ------------------------------------------------------------------------------------------

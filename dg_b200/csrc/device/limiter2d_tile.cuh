@@ -15,18 +15,16 @@
 
 namespace dgb {
 
+// x pass over one block of the row ey starting at element column x0 (a multiple of 30); the CTA
+// returns from here together, after its last barrier
 template <int P, int METHOD>
-__global__ void __launch_bounds__(32 * (P + 1)) lim2d_xpass_tile_kernel(const LimArgs la, int nx,
-                                                                      const double* __restrict__ U,
-                                                                      const int* __restrict__ nbr,
-                                                                      double* __restrict__ X,
-                                                                      const DevScalars* __restrict__ scal) {
+__device__ __forceinline__ void lim2d_xpass_body(const LimArgs la, int nx, const double* __restrict__ U,
+                                                 const int* __restrict__ nbr, double* __restrict__ X, int x0,
+                                                 int ey) {
   constexpr int N1 = P + 1, NS = N1 * N1, NQ = 5, TWI = 30;
   __shared__ double A[NQ][N1][N1][32];  // [quantity][slice][coefficient][slot]
-  if (scal && scal->flags) return;
   const int ld = la.ld;
   const int tx = threadIdx.x, sl = threadIdx.y;
-  const int ey = blockIdx.y, x0 = blockIdx.x * TWI;
   const int ex = x0 - 1 + tx;
   // element held by this slot: interior element, or the neighbour of the adjacent interior one
   const bool interior = tx >= 1 && tx <= TWI && ex < nx;
@@ -121,18 +119,26 @@ __global__ void __launch_bounds__(32 * (P + 1)) lim2d_xpass_tile_kernel(const Li
 }
 
 template <int P, int METHOD>
-__global__ void __launch_bounds__(32 * 6) lim2d_ypass_tile_kernel(const LimArgs la, int nx, int ny,
-                                                                  const double* __restrict__ X,
-                                                                  const int* __restrict__ nbr,
-                                                                  double* __restrict__ Uout,
-                                                                  const DevScalars* __restrict__ scal) {
+__global__ void __launch_bounds__(32 * (P + 1)) lim2d_xpass_tile_kernel(const LimArgs la, int nx,
+                                                                      const double* __restrict__ U,
+                                                                      const int* __restrict__ nbr,
+                                                                      double* __restrict__ X,
+                                                                      const DevScalars* __restrict__ scal) {
+  if (scal && scal->flags) return;
+  lim2d_xpass_body<P, METHOD>(la, nx, U, nbr, X, blockIdx.x * 30, blockIdx.y);
+}
+
+// y pass over the 32 x 4 element block at (x0, y0) for the node column ix; the CTA returns from
+// here together, after its last barrier
+template <int P, int METHOD>
+__device__ __forceinline__ void lim2d_ypass_body(const LimArgs la, int nx, int ny, const double* __restrict__ X,
+                                                 const int* __restrict__ nbr, double* __restrict__ Uout, int x0,
+                                                 int y0, int ix) {
   constexpr int N1 = P + 1, NS = N1 * N1, NQ = 5, THI = 4;
   __shared__ double B[NQ][N1][THI + 2][32];  // [quantity][coefficient][row slot][x slot]
-  if (scal && scal->flags) return;
   const int ld = la.ld;
-  const int tx = threadIdx.x, ty = threadIdx.y, ix = blockIdx.z;
-  const int x = blockIdx.x * 32 + tx;
-  const int y0 = blockIdx.y * THI;
+  const int tx = threadIdx.x, ty = threadIdx.y;
+  const int x = x0 + tx;
   const int yy = y0 - 1 + ty;
   const bool interior = ty >= 1 && ty <= THI && yy < ny && x < nx;
   int e = -1;
@@ -209,6 +215,16 @@ __global__ void __launch_bounds__(32 * 6) lim2d_ypass_tile_kernel(const LimArgs 
       Uout[o + (size_t)4 * NS * ld] = a_[iy];
     }
   }
+}
+
+template <int P, int METHOD>
+__global__ void __launch_bounds__(32 * 6) lim2d_ypass_tile_kernel(const LimArgs la, int nx, int ny,
+                                                                  const double* __restrict__ X,
+                                                                  const int* __restrict__ nbr,
+                                                                  double* __restrict__ Uout,
+                                                                  const DevScalars* __restrict__ scal) {
+  if (scal && scal->flags) return;
+  lim2d_ypass_body<P, METHOD>(la, nx, ny, X, nbr, Uout, blockIdx.x * 32, blockIdx.y * 4, blockIdx.z);
 }
 
 }  // namespace dgb

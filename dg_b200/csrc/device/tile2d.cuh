@@ -101,13 +101,14 @@ constexpr int kVolUnroll = DGB_VOL_UNROLL;
 #endif
 constexpr bool kSfLift = DGB_SF_LIFT != 0;
 
-template <int P, int FLUX, int MODE, int TW, int TH>
-__global__ void __launch_bounds__(TW * TH, 2)
-    residual2d_tile_kernel(const TileArgs a, const __grid_constant__ CUtensorMap mapU,
-                           const __grid_constant__ CUtensorMap mapB) {
+// The work of one tile (origin tx0, ty0).  The caller has initialised the mbarrier at the start of
+// shared memory; `phase` counts its completed phases (a persistent caller runs many tiles on one
+// barrier).  Every early return is taken by the whole CTA, after its last barrier.
+template <int P, int FLUX, int MODE, int TW, int TH, int UNROLL>
+__device__ __forceinline__ void tile2d_body(const TileArgs& a, const CUtensorMap* mapU, const CUtensorMap* mapB,
+                                            int tx0, int ty0, unsigned char* smraw, uint32_t& phase) {
   using Dm = TileDims<P, TW, TH>;
   constexpr int N1 = Dm::N1, NS = Dm::NS, NF = 5, NT = Dm::NT, NXF = Dm::NXF, NYF = Dm::NYF;
-  extern __shared__ __align__(128) unsigned char smraw[];
   uint64_t* bar = reinterpret_cast<uint64_t*>(smraw);
   int* s_ok = reinterpret_cast<int*>(smraw + 8);
   int* codes = reinterpret_cast<int*>(smraw + Dm::head_bytes);  // [L: TH][R: TH][D: TW][U: TW]
@@ -118,17 +119,11 @@ __global__ void __launch_bounds__(TW * TH, 2)
   double* HU = HD + TW * NF * N1;          // [TW][NF][N1]
   double* Fs = reinterpret_cast<double*>(smraw + Dm::off_face);  // [NXF + NYF][6] F[5], nc
 
-  if (a.scal && a.scal->flags) return;
   const int tid = threadIdx.x;
-  const int tx0 = blockIdx.x * TW, ty0 = blockIdx.y * TH;
   const int ld = a.ld, nx = a.nx;
   constexpr bool kPrefetch = MODE != MODE_RESIDUAL;
 
   // ---------------- phase 0: stage the tile (TMA) and the neighbour strips ----------------
-  if (tid == 0) {
-    mbar_init(bar, 1);
-    fence_mbar_init();
-  }
   for (int k = tid; k < Dm::NCODE; k += NT) {
     int face, eo;
     if (k < TH) { face = 0; eo = (ty0 + k) * nx + tx0; }
@@ -144,7 +139,7 @@ __global__ void __launch_bounds__(TW * TH, 2)
   if (tid == 0) {
     if (tma_ok) {
       mbar_arrive_expect_tx(bar, Dm::tile_bytes);
-      tma_load_3d(Us, &mapU, tx0, ty0, 0, bar);
+      tma_load_3d(Us, mapU, tx0, ty0, 0, bar);
     } else {
       atomicOr(a.errflag, (unsigned)FLAG_TIMEOUT);
     }
@@ -168,13 +163,14 @@ __global__ void __launch_bounds__(TW * TH, 2)
     (side == 0 ? HD : HU)[r] = v;
   }
   if (tid == 0) {
-    bool ok = tma_ok && mbar_wait(bar, 0);
+    bool ok = tma_ok && mbar_wait(bar, phase & 1);
     if (tma_ok && !ok) {
       atomicOr(a.errflag, (unsigned)FLAG_TIMEOUT);
-      mbar_wait(bar, 0);
+      mbar_wait(bar, phase & 1);
     }
     *s_ok = ok ? 1 : 0;
   }
+  if (tma_ok) ++phase;
   __syncthreads();
   if (!*s_ok) return;
 
@@ -295,14 +291,14 @@ __global__ void __launch_bounds__(TW * TH, 2)
     __syncthreads();
     if (tid == 0 && need) {
       mbar_arrive_expect_tx(bar, Dm::tile_bytes);
-      tma_load_3d(Ub, &mapB, tx0, ty0, 0, bar);
+      tma_load_3d(Ub, mapB, tx0, ty0, 0, bar);
     }
   }
 
   // volume terms: collocation sum-factorised (x-contraction per quadrature column gx, then y per
   // point), lift accumulated per point with the tensor-product derivative tables
   const double* us = Us + tid;  // thread-private column of the tile: us[(f*NS + t)*NT]
-#pragma unroll(kVolUnroll)
+#pragma unroll(UNROLL)
   for (int gx = 0; gx < NG1; ++gx) {
     double Tc[NF][N1], dT[N1];  // column values: sum_ix l_ix(x_gx) u(ix, iy), and of l' for alpha
 #pragma unroll
@@ -388,13 +384,14 @@ __global__ void __launch_bounds__(TW * TH, 2)
   }
   if (need) {
     if (tid == 0) {
-      bool ok = mbar_wait(bar, 1);
+      bool ok = mbar_wait(bar, phase & 1);
       if (!ok) {
         atomicOr(a.errflag, (unsigned)FLAG_TIMEOUT);
-        mbar_wait(bar, 1);
+        mbar_wait(bar, phase & 1);
       }
       *s_ok = ok ? 1 : 0;
     }
+    ++phase;
     __syncthreads();
     if (!*s_ok) return;
   }
@@ -432,6 +429,20 @@ __global__ void __launch_bounds__(TW * TH, 2)
         }
       }
   }
+}
+
+template <int P, int FLUX, int MODE, int TW, int TH>
+__global__ void __launch_bounds__(TW * TH, 2)
+    residual2d_tile_kernel(const TileArgs a, const __grid_constant__ CUtensorMap mapU,
+                           const __grid_constant__ CUtensorMap mapB) {
+  extern __shared__ __align__(128) unsigned char smraw[];
+  if (a.scal && a.scal->flags) return;
+  if (threadIdx.x == 0) {
+    mbar_init(reinterpret_cast<uint64_t*>(smraw), 1);
+    fence_mbar_init();
+  }
+  uint32_t phase = 0;
+  tile2d_body<P, FLUX, MODE, TW, TH, kVolUnroll>(a, &mapU, &mapB, blockIdx.x * TW, blockIdx.y * TH, smraw, phase);
 }
 
 }  // namespace dgb

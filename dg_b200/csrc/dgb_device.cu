@@ -22,8 +22,10 @@
 #include "device/limiter_gated.cuh"
 #include "device/tile2d_mixed.cuh"
 #include "device/learned.cuh"
+#include "device/tables.cuh"
 #include "device/sensor.h"
 #include "host/host.h"
+#include "ctx.h"
 
 namespace dgb {
 int set_error(int code, const std::string& msg);
@@ -43,8 +45,6 @@ namespace {
 
 constexpr int RES2D_TE = 16;
 constexpr int RES2D_NT = 256;
-
-enum { KC_RESIDUAL = 0, KC_LIMITER = 1, KC_DT = 2, KC_OTHER = 3, KC_N = 4 };
 
 double fact(int n) { double f = 1; for (int i = 2; i <= n; ++i) f *= i; return f; }
 
@@ -118,63 +118,6 @@ Consts make_consts(const Problem& P, int ld) {
   return c;
 }
 
-template <int P>
-Tab2<P> make_tab2(const Consts& c) {
-  Tab2<P> T;
-  std::memset(&T, 0, sizeof(T));
-  constexpr int N1 = Tab2<P>::N1, NG1 = Tab2<P>::NG1;
-  for (int gx = 0; gx < NG1; ++gx)
-    for (int gy = 0; gy < NG1; ++gy) {
-      const int g = gx * NG1 + gy;
-      T.W[g] = c.wq[gx] * c.wq[gy];
-      for (int iy = 0; iy < N1; ++iy)
-        for (int ix = 0; ix < N1; ++ix) {
-          const int t = ix + N1 * iy;
-          T.Phi[g][t] = c.Bq[gx][ix] * c.Bq[gy][iy];
-          T.dPx[g][t] = c.Dq[gx][ix] * c.Bq[gy][iy];
-          T.dPy[g][t] = c.Bq[gx][ix] * c.Dq[gy][iy];
-        }
-    }
-  for (int g = 0; g < N1; ++g) {
-    T.wf[g] = c.wf[g];
-    for (int j = 0; j < N1; ++j) T.Bf[g][j] = c.Bf[g][j];
-  }
-  for (int g = 0; g < NG1; ++g) {
-    T.W1[g] = c.wq[g];
-    for (int i = 0; i < N1; ++i) { T.B1[g][i] = c.Bq[g][i]; T.D1[g][i] = c.Dq[g][i]; }
-  }
-  std::vector<double> M((size_t)N1 * N1, 0.0);
-  for (int i = 0; i < N1; ++i)
-    for (int j = 0; j < N1; ++j)
-      for (int g = 0; g < NG1; ++g) M[i + (size_t)j * N1] += c.wq[g] * c.Bq[g][i] * c.Bq[g][j];
-  invert(M, N1);
-  for (int i = 0; i < N1; ++i)
-    for (int j = 0; j < N1; ++j) T.M1i[i][j] = M[i + (size_t)j * N1];
-  return T;
-}
-
-template <int P>
-Tab2f<P> make_tab2f(const Tab2<P>& d) {
-  Tab2f<P> T;
-  std::memset(&T, 0, sizeof(T));
-  constexpr int N1 = Tab2<P>::N1, NG1 = Tab2<P>::NG1, NS = Tab2<P>::NS, NG = Tab2<P>::NG;
-  for (int g = 0; g < NG; ++g) {
-    T.W[g] = (float)d.W[g];
-    for (int t = 0; t < NS; ++t) {
-      T.dPx[g][t] = (float)d.dPx[g][t];
-      T.dPy[g][t] = (float)d.dPy[g][t];
-      T.Phi[g][t] = (float)d.Phi[g][t];
-    }
-  }
-  for (int i = 0; i < N1; ++i) {
-    T.wf[i] = (float)d.wf[i];
-    for (int j = 0; j < N1; ++j) { T.Bf[i][j] = (float)d.Bf[i][j]; T.M1i[i][j] = (float)d.M1i[i][j]; }
-  }
-  for (int g = 0; g < NG1; ++g)
-    for (int i = 0; i < N1; ++i) { T.B1[g][i] = (float)d.B1[g][i]; T.D1[g][i] = (float)d.D1[g][i]; }
-  return T;
-}
-
 // structured row-major grid test: interior neighbours are e-1, e+1, e-nx, e+nx
 bool is_row_major_grid(const Problem& P) {
   if (P.D != 2 || P.nx <= 0 || P.ny <= 0 || (long)P.nx * P.ny != P.N_E) return false;
@@ -193,54 +136,6 @@ bool is_row_major_grid(const Problem& P) {
 
 }  // namespace
 
-struct dgb_ctx {
-  int device = 0;
-  cudaStream_t st = nullptr;
-  int D = 1, p = 1, nf = 4, ns = 2, ne = 0, ld = 0, flux = 2, limiter = 0;
-  int nx = 0, ny = 0;
-  bool tiled = false;     // structured row-major grid with tile-multiple extents: tiled residual kernel
-  int form = DGB_FORM_FP64;  // arithmetic of the residual: plain FP64 or mixed FP32/FP64
-  bool rowmajor = false;  // structured row-major grid: tiled limiter passes
-  bool fused_lim = false; // row-major grid, hrl / m2l: both limiter passes in one kernel (opt-in)
-  CUtensorMap mapA, mapB, mapC;  // TMA descriptors of the state buffers (tiled kernel)
-  double hx = 0, hy = 0;
-  size_t nstate = 0;
-  Consts cs;
-  double *A = nullptr, *B = nullptr, *C = nullptr, *DU = nullptr, *X = nullptr, *ref = nullptr;
-  int *nbr = nullptr, *perm = nullptr;
-  // sensor-gated limiters (hri, m2i, pri, p0i): sensor work arrays and flags
-  bool gated = false, has_sensors = false;
-  bool ind_on = false;          // learned indicator gates the limiter (dgb_set_indicator)
-  float ind_threshold = 0.2f;
-  float* ind_params = nullptr;  // FP32 parameters (MLP_NPARAM)
-  __nv_bfloat16* ind_w = nullptr;  // W1 [64][IND_KPAD] then W2 [64][64], BF16
-  float* ind_vec = nullptr;     // b1, b2, w3, b3
-  float* ind_modes = nullptr;   // [N_E][IND_MODES]
-  float* ind_score = nullptr;   // [N_E]
-  unsigned char* ind_flag = nullptr;
-  int* ind_list = nullptr;      // [N_E] + count
-  SensorLaunch sl;
-  int* iperm = nullptr;
-  double* smean = nullptr;
-  int* sint = nullptr;          // target, type, processed, mask, list (ld each), count, flags (ld)
-  CellAverageWeights p0w;       // p0i: cell-average weights in internal node order
-  DevScalars* scal = nullptr;
-  DevScalars* h_scal = nullptr;  // pinned
-  cudaEvent_t e0 = nullptr, e1 = nullptr;
-  double last_ms = 0.0;
-  long long last_launches = 0;
-  long long launches_per_step = 0;
-  cudaGraphExec_t graphs[2][2] = {{nullptr, nullptr}, {nullptr, nullptr}};
-  long long graph_launches[2][2] = {{0, 0}, {0, 0}};
-  // profiling (per kernel class)
-  bool prof = false;
-  std::vector<std::pair<int, std::pair<cudaEvent_t, cudaEvent_t>>> pev;
-  std::vector<cudaEvent_t> ev_pool;
-  size_t ev_used = 0;
-  double kc_ms[KC_N] = {0, 0, 0, 0};
-  long long kc_n[KC_N] = {0, 0, 0, 0};
-  long long counter = 0;  // launches issued since the last reset
-};
 
 namespace {
 
@@ -343,8 +238,11 @@ void launch_tile2d_mixed(dgb_ctx* c, const StageArgs& s) {
   k<<<grid, TILE_W * TILE_H, smem, c->st>>>(a, map_of(c, s.U));
 }
 
-// TMA descriptor of a state buffer viewed as (x: nx, y: ny, z: N_F*N_s rows of stride ld)
-bool encode_state_map(dgb_ctx* c, double* ptr, CUtensorMap* map) {
+}  // namespace
+
+// TMA descriptor of a state buffer viewed as (x: nx, y: ny, z: N_F*N_s rows of stride ld), box
+// tw x th x N_F*N_s
+bool dgb::encode_state_map(dgb_ctx* c, double* ptr, CUtensorMap* map, int tw, int th) {
   static PFN_cuTensorMapEncodeTiled_v12000 encode = nullptr;
   if (!encode) {
     cudaDriverEntryPointQueryResult q;
@@ -356,13 +254,15 @@ bool encode_state_map(dgb_ctx* c, double* ptr, CUtensorMap* map) {
   }
   const cuuint64_t dims[3] = {(cuuint64_t)c->nx, (cuuint64_t)c->ny, (cuuint64_t)(c->nf * c->ns)};
   const cuuint64_t strides[2] = {(cuuint64_t)c->nx * sizeof(double), (cuuint64_t)c->ld * sizeof(double)};
-  const cuuint32_t box[3] = {(cuuint32_t)TILE_W, (cuuint32_t)TILE_H, (cuuint32_t)(c->nf * c->ns)};
+  const cuuint32_t box[3] = {(cuuint32_t)tw, (cuuint32_t)th, (cuuint32_t)(c->nf * c->ns)};
   const cuuint32_t estr[3] = {1, 1, 1};
   CUresult r = encode(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 3, ptr, dims, strides, box, estr,
                       CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
                       CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
   return r == CUDA_SUCCESS;
 }
+
+namespace {
 
 template <int MODE>
 int residual_dispatch(dgb_ctx* c, const StageArgs& a) {
@@ -767,47 +667,7 @@ extern "C" int dgb_create(const dgb_problem* prob, int device, dgb_ctx** out) {
   // opt-in: measured slower than the two tiled passes on 512 x 256, p = 2 (64 vs 55 us per stage)
   c->fused_lim = c->rowmajor && (P.limiter == DGB_LIM_HRL || P.limiter == DGB_LIM_M2L) &&
                  std::getenv("DGB_FUSED_LIMITER") != nullptr;
-  {
-    cudaError_t el = cudaSuccess;
-    auto fill = [&](auto& t, int n1) {
-      std::memset(&t, 0, sizeof(t));
-      for (int m = 0; m < n1; ++m)
-        for (int i = 0; i < n1; ++i) {
-          t.T[m][i] = c->cs.T[m][i];
-          t.Tinv[m][i] = c->cs.Tinv[m][i];
-          t.imd[m][i] = c->cs.imd[m][i];
-          t.imdL[m][i] = c->cs.imdL[m][i];
-          t.imdR[m][i] = c->cs.imdR[m][i];
-        }
-      for (int k = 0; k < n1 + 2; ++k) t.ifact[k] = c->cs.ifact[k];
-    };
-    if (P.p == 1) { LimTab<1> t; fill(t, 2); el = cudaMemcpyToSymbol(c_lim_p1, &t, sizeof(t)); }
-    if (P.p == 2) { LimTab<2> t; fill(t, 3); el = cudaMemcpyToSymbol(c_lim_p2, &t, sizeof(t)); }
-    if (P.p == 3) { LimTab<3> t; fill(t, 4); el = cudaMemcpyToSymbol(c_lim_p3, &t, sizeof(t)); }
-    if (el != cudaSuccess) { delete c; return set_error(DGB_ERR_CUDA, std::string("limiter tables: ") + cudaGetErrorString(el)); }
-  }
-  if (P.D == 2) {
-    cudaError_t et = cudaSuccess;
-    if (P.p == 1) {
-      auto t = make_tab2<1>(c->cs);
-      auto tf = make_tab2f<1>(t);
-      et = cudaMemcpyToSymbol(c_tab2_p1, &t, sizeof(t));
-      if (et == cudaSuccess) et = cudaMemcpyToSymbol(c_tab2f_p1, &tf, sizeof(tf));
-    }
-    if (P.p == 2) {
-      auto t = make_tab2<2>(c->cs);
-      auto tf = make_tab2f<2>(t);
-      et = cudaMemcpyToSymbol(c_tab2_p2, &t, sizeof(t));
-      if (et == cudaSuccess) et = cudaMemcpyToSymbol(c_tab2f_p2, &tf, sizeof(tf));
-    }
-    if (P.p == 3) {
-      auto t = make_tab2<3>(c->cs);
-      auto tf = make_tab2f<3>(t);
-      et = cudaMemcpyToSymbol(c_tab2_p3, &t, sizeof(t));
-      if (et == cudaSuccess) et = cudaMemcpyToSymbol(c_tab2f_p3, &tf, sizeof(tf));
-    }
-    if (et != cudaSuccess) { delete c; return set_error(DGB_ERR_CUDA, std::string("constant tables: ") + cudaGetErrorString(et)); }
-  }
+  if (int rc = upload_tables(c->cs, P.D, P.p)) { delete c; return rc; }
   auto fail = [&](cudaError_t e, const char* what) {
     dgb_destroy(c);
     return set_error(DGB_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
@@ -868,8 +728,8 @@ extern "C" int dgb_create(const dgb_problem* prob, int device, dgb_ctx** out) {
   if ((e = cudaMallocHost(&c->h_scal, sizeof(DevScalars))) != cudaSuccess) return fail(e, "pinned scalars");
   if (c->tiled) {
     // row starts must be 16-byte aligned for TMA: nx is a multiple of TILE_W (32) and ld of 64
-    if (!(encode_state_map(c, c->A, &c->mapA) && encode_state_map(c, c->B, &c->mapB) &&
-          encode_state_map(c, c->C, &c->mapC)))
+    if (!(encode_state_map(c, c->A, &c->mapA, TILE_W, TILE_H) && encode_state_map(c, c->B, &c->mapB, TILE_W, TILE_H) &&
+          encode_state_map(c, c->C, &c->mapC, TILE_W, TILE_H)))
       c->tiled = false;
   }
   cudaEventCreate(&c->e0);

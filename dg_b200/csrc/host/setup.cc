@@ -585,6 +585,27 @@ Status init_state(const Problem& P, const std::string& ic, const std::vector<dou
     }
     return Status();
   }
+  if (ic == "riemann" && D == 1) {
+    // two-fluid Riemann problem split at params[0] (default domain centre): left and right
+    // rho, p ~ U[0.1, 2], u ~ U[-1, 1], gamma in {1.4, 1.67}, seeded; element-wise constant
+    double xmin = 1e300, xmax = -1e300;
+    for (size_t k = 0; k < P.mesh.x.size(); ++k) { xmin = std::min(xmin, P.mesh.x[k]); xmax = std::max(xmax, P.mesh.x[k]); }
+    const double xs = prm.size() > 0 ? prm[0] : 0.5 * (xmin + xmax);
+    double q[2][4];
+    for (int k = 0; k < 2; ++k) {
+      q[k][0] = 0.1 + 1.9 * U01(rng);
+      q[k][1] = -1.0 + 2.0 * U01(rng);
+      q[k][2] = 0.1 + 1.9 * U01(rng);
+      q[k][3] = U01(rng) < 0.5 ? 1.4 : 1.67;
+    }
+    for (int e = 0; e < NE; ++e) {
+      double cx = 0;
+      for (int k = 0; k < NS; ++k) cx += X(k, e, 0);
+      cx /= NS;
+      for (int i = 0; i < NS; ++i) set(e, i, q[cx >= xs ? 1 : 0]);
+    }
+    return Status();
+  }
   if (ic == "shock_bubble" && D == 2) {
     // Mach-1.5 shock in air (gamma 1.4, pre-shock rho 1, p 1) at x = params[0] (default 0.2)
     // moving in +x into a circular bubble of radius 0.2 at (0.5, 0.5): gamma 1.67, rho 0.138,

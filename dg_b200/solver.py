@@ -195,3 +195,59 @@ class DGSolver:
         tot = np.zeros(self.problem.info.n_fields)
         F.check(F.lib().dgb_conservation(self._h, F.dptr(tot)))
         return tot
+
+
+class DGBatch:
+    """Batched ensemble (dgb_batch_*): independent problems, one DGSolver each, advanced together
+    with SSP-RK3, every case with its own CFL step.  The solvers stay usable on their own (states
+    are set and read through them) and must outlive the batch."""
+
+    CLASS_KEYS = ("dim", "order", "flux", "limiter", "cases", "tile_w", "tile_h", "unroll", "ctas_per_sm",
+                  "tuned_ns")
+
+    def __init__(self, solvers: Sequence["DGSolver"]):
+        self.solvers = list(solvers)
+        arr = (C.c_void_p * len(self.solvers))(*[s._h for s in self.solvers])
+        self._h = C.c_void_p()
+        F.check(F.lib().dgb_batch_create(arr, len(self.solvers), C.byref(self._h)))
+
+    def close(self):
+        if getattr(self, "_h", None):
+            F.lib().dgb_batch_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        self.close()
+
+    def classes(self) -> list[dict]:
+        out = []
+        for k in range(F.lib().dgb_batch_n_classes(self._h)):
+            info = (C.c_int * 10)()
+            F.check(F.lib().dgb_batch_class_info(self._h, k, info))
+            out.append(dict(zip(self.CLASS_KEYS, list(info))))
+        return out
+
+    def autotune(self, reps: int = 5) -> list[dict]:
+        F.check(F.lib().dgb_batch_autotune(self._h, int(reps)))
+        return self.classes()
+
+    def set_tuning(self, k: int, tile_w: int, tile_h: int = 1, unroll: int = 1, ctas_per_sm: int = 0) -> None:
+        F.check(F.lib().dgb_batch_set_tuning(self._h, int(k), int(tile_w), int(tile_h), int(unroll), int(ctas_per_sm)))
+
+    def advance(self, nsteps: int, t_end: float = 0.0) -> int:
+        n = C.c_int()
+        F.check(F.lib().dgb_batch_advance(self._h, int(nsteps), float(t_end), C.byref(n)))
+        return n.value
+
+    def case_stats(self) -> tuple[np.ndarray, np.ndarray, np.ndarray]:
+        """(simulated time, steps, wall ms to the stop at t_end or -1) per case of the last run."""
+        n = len(self.solvers)
+        t, w = np.zeros(n), np.zeros(n)
+        s = np.zeros(n, np.int32)
+        F.check(F.lib().dgb_batch_case_stats(self._h, F.dptr(t), s.ctypes.data_as(C.POINTER(C.c_int)), F.dptr(w)))
+        return t, s, w
+
+    def last_timing(self) -> tuple[float, int]:
+        ms, n = C.c_double(), C.c_longlong()
+        F.check(F.lib().dgb_batch_last_timing(self._h, C.byref(ms), C.byref(n)))
+        return ms.value, n.value

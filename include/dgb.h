@@ -138,7 +138,8 @@ int dgb_problem_get_array(const dgb_problem* p, const char* name, void* dst, siz
 /* Seeded initial states (reference layout).  Names: "sodtube" (reference init_cond.cc:400),
  * "tube_noise" (two-fluid tube split at params[0] with +-params[1] uniform noise on rho),
  * "shock_bubble" (Mach-1.5 shock hitting a gamma=1.67 bubble, 1% seeded Fourier
- * perturbation of the radius), "quadrants" (four-quadrant Riemann problem, seeded states). */
+ * perturbation of the radius), "quadrants" (four-quadrant Riemann problem, seeded states),
+ * "riemann" (1D two-fluid Riemann problem split at params[0], seeded left/right states). */
 int dgb_problem_init_state(const dgb_problem* p, const char* ic, const double* params, int nparams,
                            uint64_t seed, double* U);
 /* (ic == NULL selects the deck's "#initial condition" and, when nparams == 0, its "#ic inputs".) */
@@ -237,6 +238,46 @@ int dgb_mlp_adam(float* params_dev, const float* grad_dev, float* m_dev, float* 
 int dgb_set_indicator(dgb_ctx* c, const float* params_host, float threshold);
 /* Scores [N_E] of U (reference layout, host) with the indicator set, and the flagged count. */
 int dgb_indicator_scores(dgb_ctx* c, const double* U_host, float* score_host, int* n_flagged);
+
+/* ------------------------------------------------------------------------------------
+ * Batched ensemble (no counterpart in the reference, which runs one problem per process)
+ * ------------------------------------------------------------------------------------
+ * Many independent problems advanced together with SSP-RK3, each with its own CFL step.  The
+ * cases are contexts made by dgb_create (owned by the caller, all on one device, outliving the
+ * batch; states set and read with dgb_set_state / dgb_get_state on each).  They are grouped by
+ * (dimension, order, flux, limiter); per group and operator one persistent launch walks the work
+ * items of all its cases, and one step of the whole ensemble is a CUDA graph whose group branches
+ * run concurrently.  A case advanced in a batch matches dgb_advance on it alone: bit for bit in
+ * 1D, to a few ulps in 2D (the same arithmetic, with fused multiply-adds formed differently).
+ * Supported: plain FP64 form, limiter none / hrl / m2l, positive CFL; 2D cases on structured
+ * row-major grids with p <= 2, nx a multiple of 32 and ny of 4 (DGB_ERR_UNSUPPORTED otherwise). */
+typedef struct dgb_batch dgb_batch;
+int dgb_batch_create(dgb_ctx* const* cases, int n_cases, dgb_batch** out);
+void dgb_batch_destroy(dgb_batch* b);
+/* Number of element groups and, per group k, info[10] = {dim, order, flux, limiter, cases,
+ * tile width (2D; 1D: elements per CTA), tile height (1D: 1), quadrature-loop unrolling (2D),
+ * CTAs per SM of the residual launch (0 = occupancy limit), tuned stage time in ns (0 = untuned)}. */
+int dgb_batch_n_classes(dgb_batch* b);
+int dgb_batch_class_info(dgb_batch* b, int k, int* info);
+/* Autotuner: per group, times every candidate residual configuration (tile shape and unrolling
+ * for 2D, elements per CTA for 1D, persistent grid size) `reps` times on the cases' current
+ * states (left unchanged) and keeps the fastest. */
+int dgb_batch_autotune(dgb_batch* b, int reps);
+/* Sets group k's residual configuration by hand: 2D: a tile shape among the tuner's candidates
+ * (tile_w x tile_h = 32x4, 32x2 or 16x8 dividing every case's grid; unroll 1, or 2 with 32x4);
+ * 1D: tile_w = elements per CTA (64, 128 or 256), tile_h and unroll ignored.  ctas_per_sm caps the
+ * persistent grid (0 = occupancy limit).  DGB_ERR_ARG for anything else. */
+int dgb_batch_set_tuning(dgb_batch* b, int k, int tile_w, int tile_h, int unroll, int ctas_per_sm);
+/* Up to nsteps steps of every case, each with its own CFL step; times restart at 0.  t_end > 0:
+ * a case stops at time t_end (its last step shortened to land on it) and the run ends early once
+ * every case has stopped.  *steps_run = graph steps launched.  A case whose step fails stops; the
+ * first failure is the returned status (DGB_ERR_NONFINITE / _DT_SMALL / _TIMEOUT). */
+int dgb_batch_advance(dgb_batch* b, int nsteps, double t_end, int* steps_run);
+/* Per case of the last run: simulated time, steps taken, and (t_end > 0) device wall-clock ms
+ * from the start of the run to the step at which the case stopped (-1 if it did not stop). */
+int dgb_batch_case_stats(dgb_batch* b, double* time, int* steps, double* wall_ms);
+/* Device time (ms, CUDA events) and kernel launches of the last dgb_batch_advance. */
+int dgb_batch_last_timing(dgb_batch* b, double* ms, long long* launches);
 
 /* ------------------------------------------------------------------------------------
  * Allocation-free limiter (no counterpart in the reference)
