@@ -180,6 +180,9 @@ void launch_res1d(dgb_ctx* c, const StageArgs& a) {
 }
 
 constexpr int TILE_W = 32, TILE_H = 4;
+// p = 3 tiles are two element rows high: the per-element register state (80 nodal values per
+// field set) and the shared tile then leave room for two (FP64) or three (mixed) CTAs per SM
+constexpr int tile_h_for(int p) { return p == 3 ? 2 : TILE_H; }
 
 const CUtensorMap& map_of(dgb_ctx* c, const double* p) {
   if (p == c->B) return c->mapB;
@@ -189,9 +192,10 @@ const CUtensorMap& map_of(dgb_ctx* c, const double* p) {
 
 template <int P, int FLUX, int MODE>
 void launch_tile2d(dgb_ctx* c, const StageArgs& s) {
-  using Dm = TileDims<P, TILE_W, TILE_H>;
+  constexpr int TH = tile_h_for(P);
+  using Dm = TileDims<P, TILE_W, TH>;
   constexpr size_t smem = Dm::smem_bytes;
-  auto k = residual2d_tile_kernel<P, FLUX, MODE, TILE_W, TILE_H>;
+  auto k = residual2d_tile_kernel<P, FLUX, MODE, TILE_W, TH>;
   static bool attr = false;
   if (!attr) { cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem); attr = true; }
   TileArgs a;
@@ -209,15 +213,16 @@ void launch_tile2d(dgb_ctx* c, const StageArgs& s) {
   a.nx = c->nx; a.ny = c->ny; a.ld = c->ld;
   const CUtensorMap& mu = map_of(c, s.U);
   const CUtensorMap& mb = MODE == MODE_SSP ? map_of(c, s.Ubase) : MODE == MODE_RK4 && s.Uacc ? map_of(c, s.Uacc) : mu;
-  dim3 grid(c->nx / TILE_W, c->ny / TILE_H);
+  dim3 grid(c->nx / TILE_W, c->ny / TH);
   ProfScope ps(c, KC_RESIDUAL);
-  k<<<grid, TILE_W * TILE_H, smem, c->st>>>(a, mu, mb);
+  k<<<grid, TILE_W * TH, smem, c->st>>>(a, mu, mb);
 }
 
 template <int P, int FLUX, int MODE>
 void launch_tile2d_mixed(dgb_ctx* c, const StageArgs& s) {
-  constexpr size_t smem = TileDimsMixed<P, TILE_W, TILE_H>::smem_bytes;
-  auto k = residual2d_tile_mixed_kernel<P, FLUX, MODE, TILE_W, TILE_H>;
+  constexpr int TH = tile_h_for(P);
+  constexpr size_t smem = TileDimsMixed<P, TILE_W, TH>::smem_bytes;
+  auto k = residual2d_tile_mixed_kernel<P, FLUX, MODE, TILE_W, TH>;
   static bool attr = false;
   if (!attr) { cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem); attr = true; }
   TileArgs a;
@@ -233,9 +238,9 @@ void launch_tile2d_mixed(dgb_ctx* c, const StageArgs& s) {
   a.JFx = c->cs.JFx;
   a.JFy = c->cs.JFy;
   a.nx = c->nx; a.ny = c->ny; a.ld = c->ld;
-  dim3 grid(c->nx / TILE_W, c->ny / TILE_H);
+  dim3 grid(c->nx / TILE_W, c->ny / TH);
   ProfScope ps(c, KC_RESIDUAL);
-  k<<<grid, TILE_W * TILE_H, smem, c->st>>>(a, map_of(c, s.U));
+  k<<<grid, TILE_W * TH, smem, c->st>>>(a, map_of(c, s.U));
 }
 
 }  // namespace
@@ -273,7 +278,9 @@ int residual_dispatch(dgb_ctx* c, const StageArgs& a) {
       case 12: launch_tile2d_mixed<1, 2, MODE>(c, a); return 0;
       case 20: launch_tile2d_mixed<2, 0, MODE>(c, a); return 0;
       case 22: launch_tile2d_mixed<2, 2, MODE>(c, a); return 0;
-      default: return set_error(DGB_ERR_UNSUPPORTED, "mixed form: p = 1, 2 with Rusanov or Roe");
+      case 30: launch_tile2d_mixed<3, 0, MODE>(c, a); return 0;
+      case 32: launch_tile2d_mixed<3, 2, MODE>(c, a); return 0;
+      default: return set_error(DGB_ERR_UNSUPPORTED, "mixed form: p = 1..3 with Rusanov or Roe");
     }
   }
   if (c->tiled) {
@@ -283,6 +290,8 @@ int residual_dispatch(dgb_ctx* c, const StageArgs& a) {
       case 12: launch_tile2d<1, 2, MODE>(c, a); return 0;
       case 20: launch_tile2d<2, 0, MODE>(c, a); return 0;
       case 22: launch_tile2d<2, 2, MODE>(c, a); return 0;
+      case 30: launch_tile2d<3, 0, MODE>(c, a); return 0;
+      case 32: launch_tile2d<3, 2, MODE>(c, a); return 0;
       default: break;
     }
   }
@@ -663,7 +672,7 @@ extern "C" int dgb_create(const dgb_problem* prob, int device, dgb_ctx** out) {
   c->hx = P.hx;
   c->hy = P.hy;
   c->rowmajor = P.D == 2 && is_row_major_grid(P) && std::getenv("DGB_NO_TILE") == nullptr;
-  c->tiled = c->rowmajor && P.p <= 2 && P.nx % TILE_W == 0 && P.ny % TILE_H == 0;
+  c->tiled = c->rowmajor && P.p <= 3 && P.nx % TILE_W == 0 && P.ny % tile_h_for(P.p) == 0;
   // opt-in: measured slower than the two tiled passes on 512 x 256, p = 2 (64 vs 55 us per stage)
   c->fused_lim = c->rowmajor && (P.limiter == DGB_LIM_HRL || P.limiter == DGB_LIM_M2L) &&
                  std::getenv("DGB_FUSED_LIMITER") != nullptr;
@@ -728,8 +737,9 @@ extern "C" int dgb_create(const dgb_problem* prob, int device, dgb_ctx** out) {
   if ((e = cudaMallocHost(&c->h_scal, sizeof(DevScalars))) != cudaSuccess) return fail(e, "pinned scalars");
   if (c->tiled) {
     // row starts must be 16-byte aligned for TMA: nx is a multiple of TILE_W (32) and ld of 64
-    if (!(encode_state_map(c, c->A, &c->mapA, TILE_W, TILE_H) && encode_state_map(c, c->B, &c->mapB, TILE_W, TILE_H) &&
-          encode_state_map(c, c->C, &c->mapC, TILE_W, TILE_H)))
+    const int th = tile_h_for(P.p);
+    if (!(encode_state_map(c, c->A, &c->mapA, TILE_W, th) && encode_state_map(c, c->B, &c->mapB, TILE_W, th) &&
+          encode_state_map(c, c->C, &c->mapC, TILE_W, th)))
       c->tiled = false;
   }
   cudaEventCreate(&c->e0);
@@ -982,9 +992,10 @@ extern "C" int dgb_indicator_scores(dgb_ctx* c, const double* U, float* score, i
 extern "C" int dgb_set_form(dgb_ctx* c, int form) {
   if (!c) return set_error(DGB_ERR_ARG, "null argument");
   if (form != DGB_FORM_FP64 && form != DGB_FORM_MIXED) return set_error(DGB_ERR_ARG, "unknown form");
-  if (form == DGB_FORM_MIXED && !(c->tiled && c->p <= 2))
+  if (form == DGB_FORM_MIXED && !(c->tiled && c->flux != DGB_FLUX_HLL))
     return set_error(DGB_ERR_UNSUPPORTED,
-                     "the mixed form needs a structured 2D grid with extents multiples of 32 x 4 and p <= 2");
+                     "the mixed form needs a structured 2D grid with nx a multiple of 32 and ny of 4 (p = 3: 2), "
+                     "Rusanov or Roe");
   if (form != c->form) {
     DGB_CUDA(cudaSetDevice(c->device));
     DGB_CUDA(cudaStreamSynchronize(c->st));

@@ -64,7 +64,7 @@ enum dgb_limiter {
 
 /* Arithmetic of the residual kernels.  FP64: plain double precision (the parity form).  MIXED:
  * basis contractions, Rusanov flux and lift in FP32 on deviations from a per-element FP64 anchor;
- * state, pressure recovery, Roe solver and stage update in FP64 (structured 2D grids, p <= 2). */
+ * state, pressure recovery, Roe solver and stage update in FP64 (structured 2D grids, p <= 3). */
 enum dgb_form { DGB_FORM_FP64 = 0, DGB_FORM_MIXED = 1 };
 
 /* Time integrators: classical RK4 (reference rk.h:44-57) and Shu-Osher SSP-RK3 (new). */
