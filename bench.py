@@ -16,6 +16,8 @@ device-side CFL step.  DOF = N_E * N_s * N_F = 5,898,240.
   cpu_baseline  the reference CPU build (oracle/_ref, compiled from the reference sources) on a
              bounded sample of the same workload, one process on one core
   forms      plain FP64, mixed and mixed + learned indicator at equal L1 error (same protocol)
+  mixed_p3   the 2048x1024 p=3 Roe shock-bubble: FP64 and mixed throughput, per-field L1 / Linf of
+             the mixed form against the FP64 run and the conserved totals after 300 steps
   ensemble   the batched ensemble (256 independent cases of uneven sizes, dgb_batch): aggregate
              DOF*stages/s against the same cases advanced one after another, autotuned tiling,
              per-case completion times for a common end time
@@ -406,6 +408,65 @@ def ensemble(dgb, dev, steps, warmup):
             "host_setup_s": setup_s}
 
 
+P3_NX, P3_NY, P3_STEPS = 2048, 1024, 300
+
+
+def mixed_p3(dgb, dev, steps=P3_STEPS, timed=10):
+    """The p=3 configuration: shock-bubble on 2048 x 1024 quads, p = 3, Roe, m2l, SSP-RK3, CFL 0.3.
+    Throughput of the plain FP64 and the mixed form (same protocol as the headline, without the L2
+    flush: the 2.7 GB state is 21x the L2), then both advanced `steps` CFL steps from the same
+    state: per-field relative L1 and Linf error of the mixed form against the FP64 run, and the
+    conserved totals (domain integrals of the five fields) of both at the start and the end."""
+    prob = dgb.Problem.structured(2, 3, P3_NX, P3_NY, *DOMAIN, bc=BC, flux="roe", limiter="m2l", cfl=CFL)
+    info = prob.info
+    dof = info.n_elem * info.n_s * info.n_fields
+    U0 = None
+    out = {"workload": "2D shock-bubble 2048x1024 quads, p=3, Roe, m2l, SSP-RK3, CFL 0.3", "dof": dof}
+    finals, totals = {}, {}
+    for form in ("fp64", "mixed"):
+        s = dgb.DGSolver(prob, device=dev)
+        s.set_form(form)
+        if U0 is None:
+            U0 = s.limit(prob.init_state("shock_bubble", seed=SEED))
+        s.set_state(U0)
+        s.advance(3, 0.0, scheme=dgb.SSPRK3)
+        s.advance(timed, 0.0, scheme=dgb.SSPRK3)
+        ms, _ = s.last_timing()
+        out[form] = {"value": dof * STAGES_PER_STEP * timed / (ms / 1e3), "ms_per_step": ms / timed}
+        s.set_state(U0)
+        c0 = s.conservation()
+        try:
+            t = s.advance(steps, 0.0, scheme=dgb.SSPRK3)
+            finals[form] = s.get_state()
+            totals[form] = (c0, s.conservation())
+            out[form]["time_after_steps"] = t
+        except dgb.DGBError as e:
+            out[form]["failed"] = str(e)
+        s.close()
+    out["speedup_mixed_vs_fp64"] = out["mixed"]["value"] / out["fp64"]["value"]
+    if len(finals) == 2:
+        A = finals["mixed"].reshape(info.n_elem, info.n_fields, info.n_s)
+        B = finals["fp64"].reshape(info.n_elem, info.n_fields, info.n_s)
+        names = ("rho", "rho_u", "rho_v", "E", "alpha")
+        l1, li = {}, {}
+        for f, nm in enumerate(names):
+            sc1 = np.abs(B[:, f]).sum() if f not in (1, 2) else max(np.abs(B[:, 1]).sum(), np.abs(B[:, 2]).sum())
+            sci = np.abs(B[:, f]).max() if f not in (1, 2) else max(np.abs(B[:, 1]).max(), np.abs(B[:, 2]).max())
+            l1[nm] = float(np.abs(A[:, f] - B[:, f]).sum() / sc1)
+            li[nm] = float(np.abs(A[:, f] - B[:, f]).max() / sci)
+        c0, r1 = totals["fp64"]
+        _, m1 = totals["mixed"]
+        scale = np.abs(c0).copy()
+        scale[1:3] = np.abs(c0).max()
+        out["after_steps"] = steps
+        out["rel_l1_mixed_vs_fp64"] = l1
+        out["rel_linf_mixed_vs_fp64"] = li
+        out["conserved_totals"] = {"start": c0.tolist(), "fp64_end": r1.tolist(), "mixed_end": m1.tolist(),
+                                   "mixed_minus_fp64_rel": ((m1 - r1) / scale).tolist(),
+                                   "note": "totals change through the open (transmissive) x boundaries in both forms"}
+    return out
+
+
 def main(argv=None) -> int:
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -422,6 +483,8 @@ def main(argv=None) -> int:
     ap.add_argument("--no-forms", action="store_true", help="skip the mixed / learned form comparison")
     ap.add_argument("--no-ensemble", action="store_true", help="skip the batched-ensemble measurement")
     ap.add_argument("--ensemble-only", action="store_true", help="print only the batched-ensemble measurement")
+    ap.add_argument("--no-p3", action="store_true", help="skip the 2048x1024 p=3 FP64 / mixed comparison")
+    ap.add_argument("--p3-only", action="store_true", help="print only the 2048x1024 p=3 FP64 / mixed comparison")
     args = ap.parse_args(argv)
     if args.impl == "reference":
         return run_reference(args)
@@ -437,6 +500,10 @@ def main(argv=None) -> int:
     torch.cuda.set_device(local)
     dev = local
 
+    if args.p3_only:
+        if rank == 0:
+            print(json.dumps({"mixed_p3": mixed_p3(dgb, dev)}))
+        return 0
     if args.ensemble_only:
         if rank == 0:
             print(json.dumps({"ensemble": ensemble(dgb, dev, min(args.steps, 20), args.warmup)}))
@@ -522,6 +589,9 @@ def main(argv=None) -> int:
     ens = None
     if ws == 1 and not args.no_ensemble and (args.nx, args.ny) == (NX, NY):
         ens = ensemble(dgb, dev, min(args.steps, 20), args.warmup)
+    p3 = None
+    if ws == 1 and not args.no_p3 and (args.nx, args.ny) == (NX, NY):
+        p3 = mixed_p3(dgb, dev)
 
     form_cfg = {"form": ("plain FP64" if args.form == "fp64" else
                          "mixed: FP32 contractions/Rusanov flux on FP64 anchors, FP64 pressure, state and update")
@@ -543,7 +613,7 @@ def main(argv=None) -> int:
                 "kernel_ms_per_step": {"residual": res_ms / args.steps, "limiter": lim_ms / args.steps,
                                        "dt": dt_ms / args.steps},
                 "cpu_baseline": cpu, "clocks": clocks, "gpu_launches": launches, "forms": forms,
-                "ensemble": ens}
+                "ensemble": ens, "mixed_p3": p3}
         print(json.dumps(line))
     solver.close()
     if ws > 1:
