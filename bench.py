@@ -16,6 +16,8 @@ device-side CFL step.  DOF = N_E * N_s * N_F = 5,898,240.
   cpu_baseline  the reference CPU build (oracle/_ref, compiled from the reference sources) on a
              bounded sample of the same workload, one process on one core
   forms      plain FP64, mixed and mixed + learned indicator at equal L1 error (same protocol)
+  learned_deploy  the learned indicator on a 1024x1024 four-quadrant problem: FP64 / mixed / mixed +
+             gated limiter, time per step and L1 density distance from the FP64 full-limiter run
   mixed_p3   the 2048x1024 p=3 Roe shock-bubble: FP64 and mixed throughput, per-field L1 / Linf of
              the mixed form against the FP64 run and the conserved totals after 300 steps
   ensemble   the batched ensemble (256 independent cases of uneven sizes, dgb_batch): aggregate
@@ -408,6 +410,56 @@ def ensemble(dgb, dev, steps, warmup):
             "host_setup_s": setup_s}
 
 
+DEPLOY_N, DEPLOY_STEPS, DEPLOY_SEED = 1024, 100, 4097
+
+
+def learned_deploy(dgb, dev, timed=20, warmup=3, steps=DEPLOY_STEPS):
+    """The learned indicator on its deployment problem: a seeded four-quadrant Riemann problem on
+    1024 x 1024 quads, p = 2, Rusanov, m2l, SSP-RK3, CFL 0.3 (states as in the training set, a
+    problem outside it).  Plain FP64 with the full limiter, mixed with the full limiter and mixed
+    with the indicator-gated limiter (threshold 0.2, band of face neighbours, scored once per
+    step): device time per step, and after `steps` fixed steps the L1 density distance of each
+    run from the plain FP64 full-limiter run (the judge) and the flagged / band fractions."""
+    from dg_b200 import learned as L
+    params, _ = L.load()
+    prob = dgb.Problem.structured(2, 2, DEPLOY_N, DEPLOY_N, 0.0, 1.0, 0.0, 1.0, bc=("transmissive",) * 4,
+                                  flux="rusanov", limiter="m2l", cfl=CFL)
+    info = prob.info
+    dof = info.n_elem * info.n_s * info.n_fields
+    out = {"workload": "2D four-quadrant Riemann problem 1024x1024 quads, p=2, Rusanov, m2l, SSP-RK3, CFL 0.3",
+           "dof": dof}
+    U0, dt, finals = None, None, {}
+    for name, form, learned in (("fp64", "fp64", False), ("mixed", "mixed", False), ("mixed_learned", "mixed", True)):
+        s = dgb.DGSolver(prob, device=dev)
+        s.set_form(form)
+        if U0 is None:
+            U0 = s.limit(prob.init_state("quadrants", seed=DEPLOY_SEED))
+            dt = 0.8 * s.dt_from_cfl(U0)
+        if learned:
+            L.set_indicator(s, params, 0.2)
+        s.set_state(U0)
+        s.advance(warmup, 0.0, scheme=dgb.SSPRK3)
+        s.advance(timed, 0.0, scheme=dgb.SSPRK3)
+        ms, n = s.last_timing()
+        out[name] = {"value": dof * STAGES_PER_STEP * timed / (ms / 1e3), "ms_per_step": ms / timed,
+                     "gpu_launches_per_step": n / timed}
+        s.set_state(U0)
+        s.advance(steps, dt, scheme=dgb.SSPRK3)
+        finals[name] = s.get_state()
+        if learned:
+            sc, cnt = L.scores(s, finals[name])
+            out[name]["flagged_fraction_final"] = cnt / info.n_elem
+        s.close()
+    base = out["fp64"]["value"]
+    rho = {k: v.reshape(info.n_elem, info.n_fields, info.n_s)[:, 0] for k, v in finals.items()}
+    for k in out:
+        if isinstance(out[k], dict) and "value" in out[k]:
+            out[k]["speedup_vs_fp64"] = out[k]["value"] / base
+            out[k]["l1_density_vs_fp64_full_limiter"] = float(np.abs(rho[k] - rho["fp64"]).sum() / np.abs(rho["fp64"]).sum())
+    out["protocol"] = f"{timed} timed CFL steps after {warmup}; accuracy after {steps} steps of dt = 0.8 x the initial CFL step"
+    return out
+
+
 P3_NX, P3_NY, P3_STEPS = 2048, 1024, 300
 
 
@@ -484,6 +536,8 @@ def main(argv=None) -> int:
     ap.add_argument("--no-ensemble", action="store_true", help="skip the batched-ensemble measurement")
     ap.add_argument("--ensemble-only", action="store_true", help="print only the batched-ensemble measurement")
     ap.add_argument("--no-p3", action="store_true", help="skip the 2048x1024 p=3 FP64 / mixed comparison")
+    ap.add_argument("--no-deploy", action="store_true", help="skip the learned indicator's 1024x1024 deployment")
+    ap.add_argument("--deploy-only", action="store_true", help="print only the learned indicator's deployment")
     ap.add_argument("--p3-only", action="store_true", help="print only the 2048x1024 p=3 FP64 / mixed comparison")
     args = ap.parse_args(argv)
     if args.impl == "reference":
@@ -500,6 +554,10 @@ def main(argv=None) -> int:
     torch.cuda.set_device(local)
     dev = local
 
+    if args.deploy_only:
+        if rank == 0:
+            print(json.dumps({"learned_deploy": learned_deploy(dgb, dev)}))
+        return 0
     if args.p3_only:
         if rank == 0:
             print(json.dumps({"mixed_p3": mixed_p3(dgb, dev)}))
@@ -592,6 +650,9 @@ def main(argv=None) -> int:
     p3 = None
     if ws == 1 and not args.no_p3 and (args.nx, args.ny) == (NX, NY):
         p3 = mixed_p3(dgb, dev)
+    deploy = None
+    if ws == 1 and not args.no_deploy and (args.nx, args.ny) == (NX, NY):
+        deploy = learned_deploy(dgb, dev)
 
     form_cfg = {"form": ("plain FP64" if args.form == "fp64" else
                          "mixed: FP32 contractions/Rusanov flux on FP64 anchors, FP64 pressure, state and update")
@@ -613,7 +674,7 @@ def main(argv=None) -> int:
                 "kernel_ms_per_step": {"residual": res_ms / args.steps, "limiter": lim_ms / args.steps,
                                        "dt": dt_ms / args.steps},
                 "cpu_baseline": cpu, "clocks": clocks, "gpu_launches": launches, "forms": forms,
-                "ensemble": ens, "mixed_p3": p3}
+                "ensemble": ens, "mixed_p3": p3, "learned_deploy": deploy}
         print(json.dumps(line))
     solver.close()
     if ws > 1:

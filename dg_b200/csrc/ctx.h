@@ -44,6 +44,8 @@ struct dgb_ctx {
   float* ind_score = nullptr;   // [N_E]
   unsigned char* ind_flag = nullptr;
   int* ind_list = nullptr;      // [N_E] + count
+  unsigned char* ind_band = nullptr;  // flagged elements and their neighbours
+  int* ind_blist = nullptr;     // [N_E] + count: the band as a list
   dgb::SensorLaunch sl;
   int* iperm = nullptr;
   double* smean = nullptr;

@@ -310,21 +310,23 @@ __device__ __forceinline__ float gelu_fast(float x) {
 
 // MLP scores on BF16 tensor cores (mma.sync m16n8k16, FP32 accumulation): a warp scores 16
 // elements; layer-1 accumulators become layer-2 A fragments without leaving registers.
-// Persistent CTAs of 4 warps; weights staged once per CTA.  Elements scoring above the threshold
+// Persistent CTAs of IND_WARPS warps sharing one copy of the weights (2 CTAs, 16 warps per SM: the
+// feature gathers are latency-bound and need the warps).  Elements scoring above the threshold
 // are flagged and appended to the list.
+constexpr int IND_WARPS = 8;
 constexpr size_t IND_SMEM_BYTES =
-    ((size_t)MLP_H * IND_W1S + (size_t)MLP_H * IND_W2S + (size_t)4 * 16 * IND_FTS) * sizeof(__nv_bfloat16) +
-    (3 * MLP_H + 4) * sizeof(float) + 4 * 80 * sizeof(int);
+    ((size_t)MLP_H * IND_W1S + (size_t)MLP_H * IND_W2S + (size_t)IND_WARPS * 16 * IND_FTS) * sizeof(__nv_bfloat16) +
+    (3 * MLP_H + 4) * sizeof(float) + IND_WARPS * 80 * sizeof(int);
 
-__global__ void __launch_bounds__(128) indicator_infer_kernel(const IndicatorArgs a) {
+__global__ void __launch_bounds__(32 * IND_WARPS, 2) indicator_infer_kernel(const IndicatorArgs a) {
   extern __shared__ __align__(16) unsigned char ism[];
   __nv_bfloat16* w1s = reinterpret_cast<__nv_bfloat16*>(ism);          // [64][IND_W1S]
   __nv_bfloat16* w2s = w1s + MLP_H * IND_W1S;                           // [64][IND_W2S]
   __nv_bfloat16* fts0 = w2s + MLP_H * IND_W2S;                          // per warp: [16][IND_W1S]
-  float* vs = reinterpret_cast<float*>(fts0 + 4 * 16 * IND_FTS);        // b1, b2, w3, b3
+  float* vs = reinterpret_cast<float*>(fts0 + IND_WARPS * 16 * IND_FTS);  // b1, b2, w3, b3
   int* eidx0 = reinterpret_cast<int*>(vs + 3 * MLP_H + 4);              // per warp: [16][5]
   if (a.scal && a.scal->flags) return;
-  for (int i = threadIdx.x; i < 4 * 16 * IND_FTS; i += blockDim.x) fts0[i] = __float2bfloat16(0.f);
+  for (int i = threadIdx.x; i < IND_WARPS * 16 * IND_FTS; i += blockDim.x) fts0[i] = __float2bfloat16(0.f);
   for (int i = threadIdx.x; i < MLP_H * IND_KPAD; i += blockDim.x)
     w1s[(i / IND_KPAD) * IND_W1S + i % IND_KPAD] = a.w1[i];
   for (int i = threadIdx.x; i < MLP_H * MLP_H; i += blockDim.x) w2s[(i / MLP_H) * IND_W2S + i % MLP_H] = a.w2[i];
@@ -337,7 +339,7 @@ __global__ void __launch_bounds__(128) indicator_infer_kernel(const IndicatorArg
   __syncthreads();
   __nv_bfloat16* ft = fts0 + warp * 16 * IND_FTS;
   const uint32_t* ftw = reinterpret_cast<const uint32_t*>(ft);
-  for (int tile = blockIdx.x * 4 + warp; tile < ntiles; tile += gridDim.x * 4) {
+  for (int tile = blockIdx.x * IND_WARPS + warp; tile < ntiles; tile += gridDim.x * IND_WARPS) {
     const int r0 = tile * 16 + g, r1 = r0 + 8;
     const bool ok0 = r0 < a.n_elem, ok1 = r1 < a.n_elem;
     // element indices of the 16 rows (self, L, R, D, U), then the features into shared memory:
@@ -473,6 +475,31 @@ __global__ void __launch_bounds__(128) indicator_infer_kernel(const IndicatorArg
     if (f1) a.list[base + n0 + __popc(m1 & below)] = r1;
     __syncwarp();
   }
+}
+
+// The band: flagged elements and their face neighbours (the flags are taken once per step on the
+// step's initial state; a discontinuity moves well under one element per step at CFL < 1).
+__global__ void __launch_bounds__(256) indicator_band_kernel(int n_elem, int ld, int n_nbr, const int* __restrict__ nbr,
+                                                             const unsigned char* __restrict__ flag,
+                                                             unsigned char* __restrict__ band, int* __restrict__ list,
+                                                             int* __restrict__ count, const DevScalars* __restrict__ scal) {
+  if (scal && scal->flags) return;
+  const int e = blockIdx.x * blockDim.x + threadIdx.x;
+  bool b = false;
+  if (e < n_elem) {
+    b = flag[e] != 0;
+    for (int k = 0; k < n_nbr && !b; ++k) {
+      const int n = __ldg(nbr + (size_t)k * ld + e);
+      b = n >= 0 && flag[n] != 0;
+    }
+    band[e] = b;
+  }
+  const unsigned m = __ballot_sync(0xffffffffu, b);
+  const int lane = threadIdx.x & 31;
+  int base = 0;
+  if (lane == 0 && m) base = atomicAdd(count, __popc(m));
+  base = __shfl_sync(0xffffffffu, base, 0);
+  if (b) list[base + __popc(m & ((1u << lane) - 1u))] = e;
 }
 
 }  // namespace dgb

@@ -435,7 +435,8 @@ int limit_to(dgb_ctx* c, const double* in, double* out) {
   }
 }
 
-// learned indicator: scores and flags of U (modes, then the BF16 tensor-core MLP)
+// learned indicator: scores and flags of U (modes, then the BF16 tensor-core MLP), then the band
+// (flagged elements and their face neighbours) that the sparse limiter works on
 void launch_indicator(dgb_ctx* c, const double* U) {
   ProfScope ps(c, KC_LIMITER);
   indicator_modes_kernel<2><<<(c->ne + 127) / 128, 128, 0, c->st>>>(U, c->ld, c->ne, c->ind_modes);
@@ -445,25 +446,29 @@ void launch_indicator(dgb_ctx* c, const double* U) {
   a.w1 = c->ind_w; a.w2 = c->ind_w + MLP_H * IND_KPAD; a.vec = c->ind_vec;
   a.score = c->ind_score; a.flag = c->ind_flag; a.list = c->ind_list; a.count = c->ind_list + c->ld; a.scal = c->scal;
   const int ntiles = (c->ne + 15) / 16;
-  const int grid = std::min((ntiles + 3) / 4, 148 * 3);  // persistent: 3 CTAs of 73 KB per SM
+  const int grid = std::min((ntiles + IND_WARPS - 1) / IND_WARPS, 148 * 2);  // persistent: 2 CTAs per SM
   static bool attr = false;
   if (!attr) {
     cudaFuncSetAttribute(indicator_infer_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)IND_SMEM_BYTES);
     attr = true;
   }
-  indicator_infer_kernel<<<grid, 128, IND_SMEM_BYTES, c->st>>>(a);
-  c->counter += 2;
+  indicator_infer_kernel<<<grid, 32 * IND_WARPS, IND_SMEM_BYTES, c->st>>>(a);
+  cudaMemsetAsync(c->ind_blist + c->ld, 0, sizeof(int), c->st);
+  indicator_band_kernel<<<(c->ne + 255) / 256, 256, 0, c->st>>>(c->ne, c->ld, 4, c->nbr, c->ind_flag, c->ind_band,
+                                                                c->ind_blist, c->ind_blist + c->ld, c->scal);
+  c->counter += 3;
 }
 
-// learned-indicator-gated m2 limiter (m2i arithmetic on the flagged elements only), in place
-void launch_learned_limiter(dgb_ctx* c, double* U) {
-  launch_indicator(c, U);
+// learned-indicator-gated m2 limiter (m2i arithmetic on the band only), in place; score = false
+// reuses the band of the last scoring (the time steppers score once per step)
+void launch_learned_limiter(dgb_ctx* c, double* U, bool score) {
+  if (score) launch_indicator(c, U);
   ProfScope ps(c, KC_LIMITER);
   const LimArgs la{c->ld, c->ne};
   GateSparse sp;
-  sp.list = c->ind_list;
-  sp.count = c->ind_list + c->ld;
-  sp.flag = c->ind_flag;
+  sp.list = c->ind_blist;
+  sp.count = c->ind_blist + c->ld;
+  sp.flag = c->ind_band;
   sp.alt = U;
   dim3 grid((c->ne + 127) / 128, 3);
   lim_gated_kernel<2, 2, 2, 0, false, false, true><<<grid, 128, 0, c->st>>>(la, nullptr, U, c->nbr, c->X, c->scal, sp);
@@ -471,11 +476,12 @@ void launch_learned_limiter(dgb_ctx* c, double* U) {
   c->counter += 1;
 }
 
-// in-place limiting of a state buffer with the context's limiter
-int limit_dispatch(dgb_ctx* c, double* U) {
+// in-place limiting of a state buffer with the context's limiter (rescore: the learned indicator
+// scores U first; the time steppers score once per step and pass false)
+int limit_dispatch(dgb_ctx* c, double* U, bool rescore = true) {
   if (c->limiter == 0) return 0;
   if (c->ind_on) {
-    launch_learned_limiter(c, U);
+    launch_learned_limiter(c, U, rescore);
     return 0;
   }
   if (c->limiter == DGB_LIM_PRL) {
@@ -544,6 +550,7 @@ StageArgs stage_args(dgb_ctx* c) {
 // One SSP-RK3 step on c->A (Shu-Osher form); limiter after every stage.
 int step_ssprk3(dgb_ctx* c, bool cfl) {
   launch_dt(c, c->A, cfl);
+  if (c->ind_on) launch_indicator(c, c->A);  // the learned indicator's band, once per step
   StageArgs a = stage_args(c);
   const double coef[3][2] = {{0.0, 1.0}, {0.75, 0.25}, {1.0 / 3.0, 2.0 / 3.0}};
   double* in[3] = {c->A, c->B, c->C};
@@ -558,7 +565,7 @@ int step_ssprk3(dgb_ctx* c, bool cfl) {
     if (int rc = residual_dispatch<MODE_SSP>(c, a)) return rc;
     if (fused) {
       if (int rc = limit_to(c, c->X, out[s])) return rc;
-    } else if (int rc = limit_dispatch(c, out[s])) {
+    } else if (int rc = limit_dispatch(c, out[s], false)) {
       return rc;
     }
   }
@@ -568,6 +575,7 @@ int step_ssprk3(dgb_ctx* c, bool cfl) {
 // One classical RK4 step in the reference's form (rk.cc:155-209): A = U, B = Us, C = Ustar.
 int step_rk4(dgb_ctx* c, bool cfl) {
   launch_dt(c, c->A, cfl);
+  if (c->ind_on) launch_indicator(c, c->A);  // the learned indicator's band, once per step
   const double beta[4] = {0.0, 0.5, 0.5, 1.0};
   const double gam[4] = {1.0 / 6.0, 2.0 / 6.0, 2.0 / 6.0, 1.0 / 6.0};
   cudaMemcpyAsync(c->B, c->A, c->nstate * sizeof(double), cudaMemcpyDeviceToDevice, c->st);
@@ -580,7 +588,7 @@ int step_rk4(dgb_ctx* c, bool cfl) {
         ProfScope ps(c, KC_OTHER);
         axpy_kernel<<<grid, 256, 0, c->st>>>(c->B, c->DU, beta[k], c->C, c->nstate, c->scal);
       }
-      if (int rc = limit_dispatch(c, c->C)) return rc;
+      if (int rc = limit_dispatch(c, c->C, false)) return rc;
       in = c->C;
     }
     a.U = in;
@@ -589,7 +597,7 @@ int step_rk4(dgb_ctx* c, bool cfl) {
     a.b = gam[k];
     if (int rc = residual_dispatch<MODE_RK4>(c, a)) return rc;
   }
-  return limit_dispatch(c, c->A);
+  return limit_dispatch(c, c->A, false);
 }
 
 int to_internal(dgb_ctx* c, const double* Uref_dev, double* Uint) {
@@ -761,7 +769,7 @@ extern "C" void dgb_destroy(dgb_ctx* c) {
   if (c->perm) cudaFree(c->perm);
   if (c->iperm) cudaFree(c->iperm);
   for (void* q : {(void*)c->ind_params, (void*)c->ind_w, (void*)c->ind_vec, (void*)c->ind_modes, (void*)c->ind_score,
-                  (void*)c->ind_flag, (void*)c->ind_list})
+                  (void*)c->ind_flag, (void*)c->ind_list, (void*)c->ind_band, (void*)c->ind_blist})
     if (q) cudaFree(q);
   if (c->smean) cudaFree(c->smean);
   if (c->sint) cudaFree(c->sint);
@@ -949,7 +957,9 @@ extern "C" int dgb_set_indicator(dgb_ctx* c, const float* params, float threshol
         (e = cudaMalloc(&c->ind_modes, (size_t)c->ld * IND_MODES * sizeof(float))) != cudaSuccess ||
         (e = cudaMalloc(&c->ind_score, (size_t)c->ld * sizeof(float))) != cudaSuccess ||
         (e = cudaMalloc(&c->ind_flag, (size_t)c->ld)) != cudaSuccess ||
-        (e = cudaMalloc(&c->ind_list, ((size_t)c->ld + 1) * sizeof(int))) != cudaSuccess)
+        (e = cudaMalloc(&c->ind_list, ((size_t)c->ld + 1) * sizeof(int))) != cudaSuccess ||
+        (e = cudaMalloc(&c->ind_band, (size_t)c->ld)) != cudaSuccess ||
+        (e = cudaMalloc(&c->ind_blist, ((size_t)c->ld + 1) * sizeof(int))) != cudaSuccess)
       return set_error(DGB_ERR_CUDA, std::string("indicator buffers: ") + cudaGetErrorString(e));
   }
   std::vector<__nv_bfloat16> w((size_t)MLP_H * IND_KPAD + MLP_H * MLP_H, __float2bfloat16(0.f));

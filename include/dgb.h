@@ -232,9 +232,11 @@ int dgb_mlp_backward(const float* params_dev, const float* X_dev, const float* y
                      float* work_dev, void* stream);
 int dgb_mlp_adam(float* params_dev, const float* grad_dev, float* m_dev, float* v_dev, int t, float lr,
                  void* stream);
-/* Gates the limiter with the network: the limiter (m2l problems, 2D, p = 2) then runs on elements
- * scoring above `threshold` only (per-element m2 arithmetic), scored with BF16 tensor-core MMAs
- * every time the limiter runs.  params_host = NULL switches back to the full limiter. */
+/* Gates the limiter with the network: the limiter (m2l problems, 2D, p = 2) then runs only on the
+ * band -- elements scoring above `threshold` and their face neighbours -- with per-element m2
+ * arithmetic.  Scores (BF16 tensor-core MMAs) are taken once per time step on the step's initial
+ * state (a discontinuity moves well under one element per step at CFL < 1), and on the given
+ * state by dgb_limit.  params_host = NULL switches back to the full limiter. */
 int dgb_set_indicator(dgb_ctx* c, const float* params_host, float threshold);
 /* Scores [N_E] of U (reference layout, host) with the indicator set, and the flagged count. */
 int dgb_indicator_scores(dgb_ctx* c, const double* U_host, float* score_host, int* n_flagged);

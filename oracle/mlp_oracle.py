@@ -120,6 +120,19 @@ def labels(S: O.Setup, U, perm, tol=1e-8):
     return (np.abs(b - a)[:, :, 1:] > tol * s[:, :, None]).any(axis=(1, 2)).astype(np.float64)
 
 
+def band(S: O.Setup, flags):
+    """The flagged elements and their face neighbours: the set the gated limiter works on when the
+    flags are taken once per time step (dg_b200/csrc/device/learned.cuh, indicator_band_kernel)."""
+    f = np.asarray(flags, bool)
+    nb = S.a["neighbors"].reshape(S.N_E, S.N_N)
+    b = f.copy()
+    for k in range(S.N_N):
+        n = nb[:, k]
+        ok = n >= 0
+        b[ok] |= f[n[ok]]
+    return b
+
+
 def gated_m2(S: O.Setup, U, flags):
     """The m2 limiter on the flagged elements only (m2i arithmetic, x then y pass), given flags."""
     U = np.asarray(U, np.float64)

@@ -35,3 +35,20 @@ def test_features_of_uniform_state_are_trivial():
     assert np.allclose(X[:, :, :, 1:], 0.0, atol=1e-12)      # no slopes anywhere
     assert np.allclose(X[:, :, :, 0], 0.0, atol=1e-12)       # neighbours' means equal the element's
     assert np.all(M.labels(S, U, prob.array("tensor_perm")) == 0)
+
+
+def test_band_adds_face_neighbours():
+    """The gated limiter's working set: flagged cells and their face neighbours (not diagonal
+    cells), clipped at walls and wrapped by periodic boundaries."""
+    import dg_b200 as dgb
+    from oracle import dg_oracle as O
+    from oracle import mlp_oracle as M
+    prob = dgb.Problem.structured(2, 2, 8, 6, bc=("reflective", "periodic", "reflective", "periodic"), flux="rusanov",
+                                  limiter="m2l")
+    S = O.Setup.from_problem(prob)
+    f = np.zeros(S.N_E, bool)
+    f[3 * 8 + 4] = True   # interior cell (x 4, y 3)
+    f[0 * 8 + 0] = True   # corner cell
+    b = M.band(S, f)
+    exp = {3 * 8 + 4, 3 * 8 + 3, 3 * 8 + 5, 2 * 8 + 4, 4 * 8 + 4, 0, 1, 8, 7}  # corner: right, up, periodic left
+    assert set(np.nonzero(b)[0].tolist()) == exp
