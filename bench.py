@@ -519,6 +519,57 @@ def mixed_p3(dgb, dev, steps=P3_STEPS, timed=10):
     return out
 
 
+PROFILE_CASES = ("p3fp64", "p3mixed", "batch", "indicator")
+
+
+def profile_case(dgb, dev, name):
+    """A small run of one kernel family for an ncu capture (inputs larger than L2, a few launches,
+    no timing): p3fp64 / p3mixed -- 2 SSP-RK3 steps of the 1024 x 512 p=3 Roe shock-bubble in the
+    FP64 / mixed form; batch -- 2 batched steps of 8 2D quadrant problems (256^2, p=2) and 8 1D
+    Riemann problems (5000 elements, p=2); indicator -- 3 scorings of the 1024 x 512 p=2
+    shock-bubble (after 10 steps) by the trained network."""
+    if name in ("p3fp64", "p3mixed"):
+        prob = dgb.Problem.structured(2, 3, 1024, 512, *DOMAIN, bc=BC, flux="roe", limiter="m2l", cfl=CFL)
+        s = dgb.DGSolver(prob, device=dev)
+        s.set_form("fp64" if name == "p3fp64" else "mixed")
+        s.set_state(s.limit(prob.init_state("shock_bubble", seed=SEED)))
+        s.advance(2, 0.0, scheme=dgb.SSPRK3)
+        s.close()
+    elif name == "batch":
+        solvers = []
+        for k in range(8):
+            prob = dgb.Problem.structured(2, 2, 256, 256, 0.0, 1.0, 0.0, 1.0, bc=("transmissive",) * 4,
+                                          flux="rusanov", limiter="m2l", cfl=CFL)
+            s = dgb.DGSolver(prob, device=dev)
+            s.set_state(s.limit(prob.init_state("quadrants", seed=300 + k)))
+            solvers.append(s)
+        for k in range(8):
+            prob = dgb.Problem.structured(1, 2, 5000, 1, 0.0, 1.0, bc=("transmissive",) * 2, flux="rusanov",
+                                          limiter="m2l", cfl=CFL)
+            s = dgb.DGSolver(prob, device=dev)
+            s.set_state(s.limit(prob.init_state("riemann", seed=400 + k)))
+            solvers.append(s)
+        b = dgb.DGBatch(solvers)
+        b.advance(2)
+        b.close()
+        for s in solvers:
+            s.close()
+    elif name == "indicator":
+        from dg_b200 import learned as L
+        prob, U0 = build_problem(1024, 512)
+        s = dgb.DGSolver(prob, device=dev)
+        s.set_state(s.limit(U0))
+        s.advance(10, 0.0, scheme=dgb.SSPRK3)
+        U = s.get_state()
+        L.set_indicator(s, L.load()[0], 0.2)
+        for _ in range(3):
+            L.scores(s, U)
+        s.close()
+    else:
+        raise ValueError(name)
+    return 0
+
+
 def main(argv=None) -> int:
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -538,6 +589,7 @@ def main(argv=None) -> int:
     ap.add_argument("--no-p3", action="store_true", help="skip the 2048x1024 p=3 FP64 / mixed comparison")
     ap.add_argument("--no-deploy", action="store_true", help="skip the learned indicator's 1024x1024 deployment")
     ap.add_argument("--deploy-only", action="store_true", help="print only the learned indicator's deployment")
+    ap.add_argument("--profile-case", choices=PROFILE_CASES, help="run a small case of one kernel family for ncu")
     ap.add_argument("--p3-only", action="store_true", help="print only the 2048x1024 p=3 FP64 / mixed comparison")
     args = ap.parse_args(argv)
     if args.impl == "reference":
@@ -554,6 +606,8 @@ def main(argv=None) -> int:
     torch.cuda.set_device(local)
     dev = local
 
+    if args.profile_case:
+        return profile_case(dgb, dev, args.profile_case)
     if args.deploy_only:
         if rank == 0:
             print(json.dumps({"learned_deploy": learned_deploy(dgb, dev)}))
