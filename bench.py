@@ -16,6 +16,8 @@ device-side CFL step.  DOF = N_E * N_s * N_F = 5,898,240.
   cpu_baseline  the reference CPU build (oracle/_ref, compiled from the reference sources) on a
              bounded sample of the same workload, one process on one core
   forms      plain FP64, mixed and mixed + learned indicator at equal L1 error (same protocol)
+  tube_1d    the 1D two-fluid shock tube (1000 elements, p=2, Roe, RK4, CFL 0.4, 2000 steps): device
+             time, distance from the reference's own run, the reference CPU build's time
   learned_deploy  the learned indicator on a 1024x1024 four-quadrant problem: FP64 / mixed / mixed +
              gated limiter, time per step and L1 density distance from the FP64 full-limiter run
   mixed_p3   the 2048x1024 p=3 Roe shock-bubble: FP64 and mixed throughput, per-field L1 / Linf of
@@ -410,6 +412,49 @@ def ensemble(dgb, dev, steps, warmup):
             "host_setup_s": setup_s}
 
 
+TUBE_FIXTURE = ROOT / "tests" / "golden" / "run_d1_tube_p2_roe_m2l_1000.npz"
+
+
+def tube_1d(dgb, dev, with_reference=True):
+    """The 1D two-fluid shock tube: 1000 elements on [0, 1], p = 2, Roe, m2l, RK4 with the CFL step
+    (CFL 0.4), transmissive ends, seeded +-1e-3 density noise, 2000 steps from the limited initial
+    state.  Device time of the 2000 steps (one dgb_advance call, CUDA graph replays), the relative L1
+    density distance from the reference's own 2000-step run (committed fixture), and the reference
+    CPU build's wall time for the same 2000 steps (one process, one core)."""
+    d = np.load(TUBE_FIXTURE)
+    c = json.loads(str(d["meta"]))
+    prob = dgb.Problem.structured(1, c["order"], c["nx"], 1, 0.0, 1.0, bc=("transmissive",) * 2, flux=c["flux"],
+                                  limiter=c["limiter"], cfl=c["cfl"])
+    info = prob.info
+    dof = info.n_elem * info.n_s * info.n_fields
+    s = dgb.DGSolver(prob, device=dev)
+    s.set_state(d["U0"])
+    s.advance(20, 0.0, scheme=dgb.RK4)  # warm-up (graph capture)
+    s.set_state(d["U0"])
+    t = s.advance(2000, 0.0, scheme=dgb.RK4)
+    ms, launches = s.last_timing()
+    U = s.get_state()
+    s.close()
+    A = U.reshape(info.n_elem, info.n_fields, info.n_s)[:, 0]
+    B = d["U2000"].reshape(info.n_elem, info.n_fields, info.n_s)[:, 0]
+    out = {"workload": "1D two-fluid shock tube, 1000 elements, p=2, Roe, m2l, RK4, CFL 0.4, 2000 steps",
+           "dof": dof, "value": dof * 4 * 2000 / (ms / 1e3), "unit": UNIT, "ms_total": ms,
+           "us_per_step": 1e3 * ms / 2000, "gpu_launches_per_step": launches / 2000, "time_reached": t,
+           "rel_l1_density_vs_reference_run": float(np.abs(A - B).sum() / np.abs(B).sum())}
+    if with_reference:
+        from oracle.ref_run import RefCase, available
+        if available(1, "roe"):
+            case = RefCase(1, c["order"], c["nx"], 1, 0.0, 1.0, 0.0, 1.0, ("transmissive",) * 4, c["flux"],
+                           c["limiter"])
+            case.write_deck(cfl=c["cfl"])
+            _, log = case.run("rk4n", d["U0"], dt=0.0, nsteps=2000, timeout=600)
+            wall = float(log.split("DGREF_WALL_S")[1].split()[0])
+            out["reference_cpu"] = {"value": dof * 4 * 2000 / wall, "unit": UNIT, "cores": 1, "kind": "reference",
+                                    "wall_s": wall, "sample": "the same 2000 RK4 steps, reference step body, 1 process"}
+            out["speedup_vs_reference_cpu"] = out["value"] / out["reference_cpu"]["value"]
+    return out
+
+
 DEPLOY_N, DEPLOY_STEPS, DEPLOY_SEED = 1024, 100, 4097
 
 
@@ -590,6 +635,8 @@ def main(argv=None) -> int:
     ap.add_argument("--no-deploy", action="store_true", help="skip the learned indicator's 1024x1024 deployment")
     ap.add_argument("--deploy-only", action="store_true", help="print only the learned indicator's deployment")
     ap.add_argument("--profile-case", choices=PROFILE_CASES, help="run a small case of one kernel family for ncu")
+    ap.add_argument("--no-tube", action="store_true", help="skip the 1D shock-tube run")
+    ap.add_argument("--tube-only", action="store_true", help="print only the 1D shock-tube run")
     ap.add_argument("--p3-only", action="store_true", help="print only the 2048x1024 p=3 FP64 / mixed comparison")
     args = ap.parse_args(argv)
     if args.impl == "reference":
@@ -608,6 +655,10 @@ def main(argv=None) -> int:
 
     if args.profile_case:
         return profile_case(dgb, dev, args.profile_case)
+    if args.tube_only:
+        if rank == 0:
+            print(json.dumps({"tube_1d": tube_1d(dgb, dev)}))
+        return 0
     if args.deploy_only:
         if rank == 0:
             print(json.dumps({"learned_deploy": learned_deploy(dgb, dev)}))
@@ -707,6 +758,9 @@ def main(argv=None) -> int:
     deploy = None
     if ws == 1 and not args.no_deploy and (args.nx, args.ny) == (NX, NY):
         deploy = learned_deploy(dgb, dev)
+    tube = None
+    if ws == 1 and not args.no_tube and (args.nx, args.ny) == (NX, NY):
+        tube = tube_1d(dgb, dev, with_reference=rank == 0 and not args.no_cpu_baseline)
 
     form_cfg = {"form": ("plain FP64" if args.form == "fp64" else
                          "mixed: FP32 contractions/Rusanov flux on FP64 anchors, FP64 pressure, state and update")
@@ -728,7 +782,7 @@ def main(argv=None) -> int:
                 "kernel_ms_per_step": {"residual": res_ms / args.steps, "limiter": lim_ms / args.steps,
                                        "dt": dt_ms / args.steps},
                 "cpu_baseline": cpu, "clocks": clocks, "gpu_launches": launches, "forms": forms,
-                "ensemble": ens, "mixed_p3": p3, "learned_deploy": deploy}
+                "ensemble": ens, "mixed_p3": p3, "learned_deploy": deploy, "tube_1d": tube}
         print(json.dumps(line))
     solver.close()
     if ws > 1:

@@ -18,7 +18,7 @@ def pytest_configure(config):
 
 def golden_cases():
     """Operator fixtures (the driver_* fixtures hold whole reference runs instead)."""
-    return sorted(p.stem for p in GOLDEN.glob("*.npz") if not p.stem.startswith("driver_"))
+    return sorted(p.stem for p in GOLDEN.glob("*.npz") if not p.stem.startswith(("driver_", "run_")))
 
 
 def load_golden(name: str):

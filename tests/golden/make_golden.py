@@ -175,7 +175,33 @@ def make_driver_fixture() -> dict:
     return out
 
 
+# the 1D two-fluid shock tube of the benchmark configurations, run by the reference itself: 1000
+# elements on [0, 1], p = 2, Roe, m2l, RK4 with the CFL step (CFL 0.4), transmissive ends, seeded
+# +-1e-3 noise on the nodal density, 2000 steps (the reference's step body, rk.cc:155-209)
+TUBE = dict(name="run_d1_tube_p2_roe_m2l_1000", dim=1, order=2, nx=1000, flux="roe", limiter="m2l", cfl=0.4,
+            ic="tube_noise", seed=2024, steps=(100, 2000))
+
+
+def make_tube_fixture() -> dict:
+    c = TUBE
+    ref = RefCase(1, c["order"], c["nx"], 1, 0.0, 1.0, 0.0, 1.0, ("transmissive",) * 4, c["flux"], c["limiter"],
+                  cfl=c["cfl"])
+    prob = dgb.Problem.structured(1, c["order"], c["nx"], 1, 0.0, 1.0, bc=("transmissive",) * 2, flux=c["flux"],
+                                  limiter=c["limiter"], cfl=c["cfl"])
+    U0 = ref.limit(prob.init_state(c["ic"], seed=c["seed"]))  # the reference limits the initial state
+    out = {"U0": U0}
+    U, done = U0, 0
+    for n in c["steps"]:
+        U = ref.rk4(U, 0.0, n - done, cfl=c["cfl"])
+        done = n
+        out[f"U{n}"] = U
+    out["meta"] = np.array(json.dumps(c))
+    return out
+
+
 def main() -> int:
+    np.savez_compressed(OUT / f"{TUBE['name']}.npz", **make_tube_fixture())
+    print(f"wrote {TUBE['name']}.npz")
     np.savez_compressed(OUT / f"{DRIVER['name']}.npz", **make_driver_fixture())
     print(f"wrote {DRIVER['name']}.npz")
     for k, c in enumerate(CASES):

@@ -10,7 +10,7 @@ per operator and 1e-11 after the multi-step runs.
 import numpy as np
 import pytest
 
-from conftest import golden_cases, load_golden, rel_err
+from conftest import GOLDEN, golden_cases, load_golden, rel_err
 from oracle import dg_oracle as O
 
 CASES = golden_cases()
@@ -77,3 +77,18 @@ def test_oracle_sensors(name):
     """SENSOR::sensing flags (sequential CPU semantics) on the raw state, exactly."""
     meta, d, S = setup_for(name)
     assert np.array_equal(O.sensors(S, d["Uraw"]), d["sens"])
+
+
+def test_tube_fixture_starts_from_the_limited_initial_state():
+    """The 2000-step tube fixture's U0 is the reference limiter applied to the seeded initial state
+    (the oracle's m2 limiter reproduces it)."""
+    import json
+    import dg_b200 as dgb
+    d = np.load(GOLDEN / "run_d1_tube_p2_roe_m2l_1000.npz")
+    c = json.loads(str(d["meta"]))
+    prob = dgb.Problem.structured(1, c["order"], c["nx"], 1, 0.0, 1.0, bc=("transmissive",) * 2, flux=c["flux"],
+                                  limiter=c["limiter"], cfl=c["cfl"])
+    S = O.Setup.from_problem(prob)
+    U = O.limit(S, prob.init_state(c["ic"], seed=c["seed"]))
+    assert rel_err(U, d["U0"]) < 1e-12
+    assert all(np.isfinite(d[k]).all() for k in ("U100", "U2000"))
