@@ -92,16 +92,21 @@ def build(force: bool = False, verbose: bool = False) -> Path:
     # link-compatible shims of the reference's kernel launchers, one per (dimension, flux)
     shim_src = SRC / "shim" / "dgb_shim.cu"
     sensor_obj = next(o for o in objs if o.name.startswith("dgb_sensor."))
+    shim_objs = []
     for d, flux in SHIMS:
         out = LIBDIR / f"libdgb_shim_{d}d_{flux}.so"
         key = hashlib.sha1((hdr + shim_src.read_text() + str(sensor_obj)).encode()).hexdigest()[:12]
         obj = BUILD / f"dgb_shim_{d}d_{flux}.{key}.o"
+        shim_objs.append(obj)
         if force or not obj.exists():
             _run([NVCC] + NVFLAGS + [f"-DDGB_SHIM_D={d}", f"-DDGB_SHIM_FLUX={SHIM_FLUX[flux]}", f"-I{INC}", f"-I{SRC}",
                                      "-c", str(shim_src), "-o", str(obj)], verbose)
             _run([NVCC] + ARCH + ["-shared", "-o", str(out), str(obj), str(sensor_obj)], verbose)
         elif not out.exists():
             _run([NVCC] + ARCH + ["-shared", "-o", str(out), str(obj), str(sensor_obj)], verbose)
+    for stale in BUILD.glob("dgb_shim_*.o"):
+        if stale not in shim_objs:
+            stale.unlink()
     drv = SRC / "dgbexec.cc"
     if drv.exists() and (force or not EXE.exists() or EXE.stat().st_mtime < max(LIB.stat().st_mtime, drv.stat().st_mtime)):
         _run(["g++", "-std=c++17", "-O2", f"-I{INC}", str(drv), "-o", str(EXE), f"-L{LIBDIR}", "-ldgb",

@@ -311,7 +311,7 @@ __device__ __forceinline__ void res1d_body(const Consts& c, const StageArgs& a, 
 #pragma unroll
     for (int f = 0; f < NF; ++f) r[f][to] += sgn * F[f] + (f == 3 ? nc : 0.0);
   }
-  if (MODE == MODE_RESIDUAL) {
+  if constexpr (MODE == MODE_RESIDUAL) {
 #pragma unroll
     for (int f = 0; f < NF; ++f)
 #pragma unroll

@@ -87,12 +87,14 @@ enum { FLAG_TIMEOUT = 4u };
 
 // Unrolling of the outer quadrature-column loop of the volume terms.  Fully unrolled, the
 // straight-line kernel body outgrows the instruction cache once several warps per scheduler run
-// different parts of it; kept rolled, the column index is warp-uniform and the tables stay
-// constant-bank operands.
+// different parts of it; rolled, the column index is warp-uniform and the tables stay
+// constant-bank operands.  Measured at p = 2 (512 x 256): rolled 85.4 us, unrolled by 2 84.1 us
+// per launch; the other orders keep the loop rolled.
 #ifndef DGB_VOL_UNROLL
-#define DGB_VOL_UNROLL 1
+#define DGB_VOL_UNROLL 0
 #endif
-constexpr int kVolUnroll = DGB_VOL_UNROLL;
+template <int P>
+constexpr int vol_unroll() { return DGB_VOL_UNROLL > 0 ? DGB_VOL_UNROLL : (P == 2 ? 2 : 1); }
 // Lift of the volume terms: sum-factorised (1) -- per quadrature column, contract over the
 // points of the column first, then one rank-1 update per node -- or direct (0) with the
 // tensor-product tables dPx, dPy, Phi.
@@ -442,7 +444,7 @@ __global__ void __launch_bounds__(TW * TH, 2)
     fence_mbar_init();
   }
   uint32_t phase = 0;
-  tile2d_body<P, FLUX, MODE, TW, TH, kVolUnroll>(a, &mapU, &mapB, blockIdx.x * TW, blockIdx.y * TH, smraw, phase);
+  tile2d_body<P, FLUX, MODE, TW, TH, vol_unroll<P>()>(a, &mapU, &mapB, blockIdx.x * TW, blockIdx.y * TH, smraw, phase);
 }
 
 }  // namespace dgb

@@ -254,7 +254,7 @@ __global__ void __launch_bounds__(TW * TH, 3)
 #pragma unroll
   for (int f = 0; f < NF; ++f) anc[f] = us[(f * NS) * NT];
   const float cx = (float)a.cx, cy = (float)a.cy, cJ = (float)a.J, sx = (float)a.sx, sy = (float)a.sy;
-#pragma unroll(kVolUnroll)
+#pragma unroll 1  // rolled quadrature-column loop (instruction cache), as in the FP64 kernel
   for (int gx = 0; gx < NG1; ++gx) {
     float Tc[NF][N1], dT[N1];
 #pragma unroll

@@ -131,8 +131,15 @@ class DGSolver:
     def set_state(self, U) -> None:
         F.check(F.lib().dgb_set_state(self._h, F.dptr(self._arr(U))))
 
-    def get_state(self) -> np.ndarray:
-        U = np.zeros(self.n)
+    def get_state(self, out: np.ndarray | None = None) -> np.ndarray:
+        """The resident state (reference layout).  `out`: a contiguous float64 array of the state's
+        size to read into (pinned host memory makes the device-to-host copy a direct DMA)."""
+        if out is None:
+            U = np.empty(self.n)
+        else:
+            U = out
+            if U.dtype != np.float64 or U.size != self.n or not U.flags.c_contiguous:
+                raise ValueError(f"out must be a contiguous float64 array of {self.n} values")
         F.check(F.lib().dgb_get_state(self._h, F.dptr(U)))
         return U
 
