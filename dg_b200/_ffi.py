@@ -40,7 +40,7 @@ class MeshSpec(C.Structure):
 
 class Options(C.Structure):
     _fields_ = [("flux", C.c_int), ("limiter", C.c_int), ("cfl", C.c_double),
-                ("thresholds", C.c_double * 3), ("n_thresholds", C.c_int)]
+                ("thresholds", C.c_double * 3), ("n_thresholds", C.c_int), ("n_mass", C.c_int)]
 
 
 class Info(C.Structure):

@@ -255,10 +255,11 @@ __global__ void __launch_bounds__(NT) residual2d_kernel(const Consts cin, const 
 // ------------------------------------------------------------------------------------------
 // 1D: one thread per element, everything in registers
 // ------------------------------------------------------------------------------------------
-// element e (< c.n_elem) with the problem constants c (in shared memory) and dt
-template <int P, int FLUX, int MODE>
+// element e (< c.n_elem) with the problem constants c (in shared memory) and dt; NY passive mass
+// fractions follow the four gamma-model fields
+template <int P, int FLUX, int MODE, int NY = 0>
 __device__ __forceinline__ void res1d_body(const Consts& c, const StageArgs& a, int e, double dt) {
-  constexpr int N1 = P + 1, NG = P + 1, NF = 4;
+  constexpr int N1 = P + 1, NG = P + 1, NF = 4 + NY;
   const int ld = c.ld;
   double u[NF][N1], r[NF][N1];
 #pragma unroll
@@ -268,7 +269,9 @@ __device__ __forceinline__ void res1d_body(const Consts& c, const StageArgs& a, 
   // volume
 #pragma unroll
   for (int g = 0; g < NG; ++g) {
-    double ug[NF] = {0, 0, 0, 0}, da = 0;
+    double ug[NF], da = 0;
+#pragma unroll
+    for (int f = 0; f < NF; ++f) ug[f] = 0.0;
 #pragma unroll
     for (int t = 0; t < N1; ++t) {
 #pragma unroll
@@ -286,6 +289,8 @@ __device__ __forceinline__ void res1d_body(const Consts& c, const StageArgs& a, 
 #pragma unroll
       for (int f = 0; f < 3; ++f) r[f][t] += c.Dq[g][t] * (cx * fx[f]);
       r[3][t] += c.Bq[g][t] * s;
+#pragma unroll
+      for (int k = 0; k < NY; ++k) r[4 + k][t] += c.Dq[g][t] * (cx * (ug[4 + k] * vx));  // physics.cu:130-134
     }
   }
   // faces: left (node 0, x = -1) and right (node P, x = +1)
@@ -307,7 +312,7 @@ __device__ __forceinline__ void res1d_body(const Consts& c, const StageArgs& a, 
 #pragma unroll
     for (int f = 0; f < NF; ++f) { L[f] = swapLR ? un[f] : uo[f]; R[f] = swapLR ? uo[f] : un[f]; }
     double F[NF], nc;
-    phys::riemann1d<FLUX>(L[0], R[0], L[1] / L[0], R[1] / R[0], L[2], R[2], L[3], R[3], nx, F, nc);
+    phys::riemann1d<FLUX, NY>(L[0], R[0], L[1] / L[0], R[1] / R[0], L[2], R[2], L[3], R[3], nx, F, nc, L + 4, R + 4);
 #pragma unroll
     for (int f = 0; f < NF; ++f) r[f][to] += sgn * F[f] + (f == 3 ? nc : 0.0);
   }
@@ -337,7 +342,7 @@ __device__ __forceinline__ void res1d_body(const Consts& c, const StageArgs& a, 
     }
 }
 
-template <int P, int FLUX, int MODE>
+template <int P, int FLUX, int MODE, int NY = 0>
 __global__ void __launch_bounds__(128) residual1d_kernel(const Consts cin, const StageArgs a) {
   __shared__ Consts c;
   copy_consts(c, cin);
@@ -346,7 +351,7 @@ __global__ void __launch_bounds__(128) residual1d_kernel(const Consts cin, const
   const int e = blockIdx.x * blockDim.x + threadIdx.x;
   if (e >= c.n_elem) return;
   const double dt = MODE == MODE_RESIDUAL ? 0.0 : (a.dt_override > 0 ? a.dt_override : a.scal->dt);
-  res1d_body<P, FLUX, MODE>(c, a, e, dt);
+  res1d_body<P, FLUX, MODE, NY>(c, a, e, dt);
 }
 
 // ------------------------------------------------------------------------------------------
@@ -569,26 +574,27 @@ __global__ void __launch_bounds__(128) lim2d_ypass_kernel(const LimArgs la, cons
   }
 }
 
-// 1D HR / m2 limiter, one thread per element (reads U, writes Uout).
-template <int P, int METHOD>
+// 1D HR / m2 limiter, one thread per element (reads U, writes Uout).  Mass fractions are limited
+// like the density (HR: every field; m2: the MACRO block of M2limiting, limiting.cc:186-193).
+template <int P, int METHOD, int NY = 0>
 __device__ __forceinline__ void lim1d_body(int ld, int e, const double* __restrict__ U, const int* __restrict__ nbr,
                                            double* __restrict__ Uout) {
-  constexpr int N1 = P + 1;
+  constexpr int N1 = P + 1, NF = 4 + NY;
   const int nL = __ldg(nbr + e), nR = __ldg(nbr + (size_t)ld + e);
   const int phys = boundary_code(nL, nR);
-  double v[3][4][N1];
+  double v[3][NF][N1];
 #pragma unroll
   for (int s = 0; s < 3; ++s) {
     const int el = s == 0 ? nL : s == 1 ? e : nR;
     if (s != 1 && phys != 0) continue;
 #pragma unroll
-    for (int f = 0; f < 4; ++f)
+    for (int f = 0; f < NF; ++f)
 #pragma unroll
       for (int i = 0; i < N1; ++i) v[s][f][i] = __ldg(U + (size_t)(f * N1 + i) * ld + el);
   }
   if constexpr (METHOD == 1) {
 #pragma unroll
-    for (int f = 0; f < 4; ++f) {
+    for (int f = 0; f < NF; ++f) {
       double lim[N1], out[N1];
       const int ph = (phys == 3 && f == 1) ? 5 : phys;
       limit_slice<P>(ph, v[0][f], v[1][f], v[2][f], lim);
@@ -630,17 +636,25 @@ __device__ __forceinline__ void lim1d_body(int ld, int e, const double* __restri
       Uout[(size_t)(2 * N1 + i) * ld + e] = E_[i];
       Uout[(size_t)(3 * N1 + i) * ld + e] = a_[i];
     }
+#pragma unroll
+    for (int k = 4; k < NF; ++k) {
+      double ly[N1], y_[N1];
+      limit_slice<P>(phys, v[0][k], v[1][k], v[2][k], ly);
+      to_lag<P>(ly, y_);
+#pragma unroll
+      for (int i = 0; i < N1; ++i) Uout[(size_t)(k * N1 + i) * ld + e] = y_[i];
+    }
   }
 }
 
-template <int P, int METHOD>
+template <int P, int METHOD, int NY = 0>
 __global__ void __launch_bounds__(128) lim1d_kernel(const LimArgs la, const double* __restrict__ U,
                                                     const int* __restrict__ nbr, double* __restrict__ Uout,
                                                     const DevScalars* __restrict__ scal) {
   if (scal && scal->flags) return;
   const int e = blockIdx.x * blockDim.x + threadIdx.x;
   if (e >= la.n_elem) return;
-  lim1d_body<P, METHOD>(la.ld, e, U, nbr, Uout);
+  lim1d_body<P, METHOD, NY>(la.ld, e, U, nbr, Uout);
 }
 
 // ------------------------------------------------------------------------------------------

@@ -17,11 +17,13 @@ namespace dgb {
 
 // x pass over one block of the row ey starting at element column x0 (a multiple of 30); the CTA
 // returns from here together, after its last barrier
-template <int P, int METHOD>
+// NY mass fractions: limited like the density (m2: the MACRO blocks of M2limiting,
+// limiting.cc:327-331 and 398-404; HR: every field); in X after E (m2) or as fields (HR).
+template <int P, int METHOD, int NY = 0>
 __device__ __forceinline__ void lim2d_xpass_body(const LimArgs la, int nx, const double* __restrict__ U,
                                                  const int* __restrict__ nbr, double* __restrict__ X, int x0,
                                                  int ey) {
-  constexpr int N1 = P + 1, NS = N1 * N1, NQ = 5, TWI = 30;
+  constexpr int N1 = P + 1, NS = N1 * N1, NQ = 5 + NY, NF = 5 + NY, TWI = 30;
   __shared__ double A[NQ][N1][N1][32];  // [quantity][slice][coefficient][slot]
   const int ld = la.ld;
   const int tx = threadIdx.x, sl = threadIdx.y;
@@ -32,16 +34,18 @@ __device__ __forceinline__ void lim2d_xpass_body(const LimArgs la, int nx, const
   if (interior) e = ey * nx + ex;
   else if (tx == 0) e = __ldg(nbr + (size_t)0 * ld + ey * nx + x0);
   else if (ex - 1 < nx && ex - 1 >= 0) e = __ldg(nbr + (size_t)1 * ld + ey * nx + ex - 1);
-  double v[5][N1];
+  double v[NF][N1];
   double Em[N1];
   if (e >= 0) {
 #pragma unroll
-    for (int f = 0; f < 5; ++f)
+    for (int f = 0; f < NF; ++f)
 #pragma unroll
       for (int ix = 0; ix < N1; ++ix) v[f][ix] = __ldg(U + (size_t)(f * NS + ix + N1 * sl) * ld + e);
     double q[NQ][N1];
 #pragma unroll
     for (int ix = 0; ix < N1; ++ix) {
+#pragma unroll
+      for (int k = 5; k < NQ; ++k) q[k][ix] = v[k][ix];
       if constexpr (METHOD == 1) {
 #pragma unroll
         for (int f = 0; f < 5; ++f) q[f][ix] = v[f][ix];
@@ -115,26 +119,35 @@ __device__ __forceinline__ void lim2d_xpass_body(const LimArgs la, int nx, const
       X[o + (size_t)4 * NS * ld] = p_[ix];
       X[o + (size_t)5 * NS * ld] = E_[ix];
     }
+#pragma unroll
+    for (int k = 5; k < NQ; ++k) {
+      double y_[N1];
+      to_lag<P>(lim[k], y_);
+#pragma unroll
+      for (int ix = 0; ix < N1; ++ix) X[(size_t)((k + 1) * NS + ix + N1 * sl) * ld + e] = y_[ix];
+    }
   }
 }
 
-template <int P, int METHOD>
+template <int P, int METHOD, int NY = 0>
 __global__ void __launch_bounds__(32 * (P + 1)) lim2d_xpass_tile_kernel(const LimArgs la, int nx,
                                                                       const double* __restrict__ U,
                                                                       const int* __restrict__ nbr,
                                                                       double* __restrict__ X,
                                                                       const DevScalars* __restrict__ scal) {
   if (scal && scal->flags) return;
-  lim2d_xpass_body<P, METHOD>(la, nx, U, nbr, X, blockIdx.x * 30, blockIdx.y);
+  lim2d_xpass_body<P, METHOD, NY>(la, nx, U, nbr, X, blockIdx.x * 30, blockIdx.y);
 }
 
 // y pass over the 32 x 4 element block at (x0, y0) for the node column ix; the CTA returns from
 // here together, after its last barrier
-template <int P, int METHOD>
+template <int P, int METHOD, int NY = 0>
 __device__ __forceinline__ void lim2d_ypass_body(const LimArgs la, int nx, int ny, const double* __restrict__ X,
                                                  const int* __restrict__ nbr, double* __restrict__ Uout, int x0,
                                                  int y0, int ix) {
-  constexpr int N1 = P + 1, NS = N1 * N1, NQ = 5, THI = 4;
+  constexpr int N1 = P + 1, NS = N1 * N1, NQ = 5 + NY, THI = 4;
+  // row of quantity k in X: HR -> field k; m2 -> [rho, rhou, rhov, alpha, p, E, rho Y_k]
+  auto xrow = [](int k) { return (METHOD == 2 && k >= 5) ? k + 1 : k; };
   __shared__ double B[NQ][N1][THI + 2][32];  // [quantity][coefficient][row slot][x slot]
   const int ld = la.ld;
   const int tx = threadIdx.x, ty = threadIdx.y;
@@ -153,7 +166,7 @@ __device__ __forceinline__ void lim2d_ypass_body(const LimArgs la, int nx, int n
     for (int k = 0; k < NQ; ++k) {
       double col[N1], a[N1];
 #pragma unroll
-      for (int iy = 0; iy < N1; ++iy) col[iy] = __ldg(X + (size_t)(k * NS + ix + N1 * iy) * ld + e);
+      for (int iy = 0; iy < N1; ++iy) col[iy] = __ldg(X + (size_t)(xrow(k) * NS + ix + N1 * iy) * ld + e);
       to_mono<P>(col, a);
 #pragma unroll
       for (int m = 0; m < N1; ++m) B[k][m][ty][tx] = a[m];
@@ -214,17 +227,24 @@ __device__ __forceinline__ void lim2d_ypass_body(const LimArgs la, int nx, int n
       Uout[o + (size_t)3 * NS * ld] = E_[iy];
       Uout[o + (size_t)4 * NS * ld] = a_[iy];
     }
+#pragma unroll
+    for (int k = 5; k < NQ; ++k) {
+      double y_[N1];
+      to_lag<P>(lim[k], y_);
+#pragma unroll
+      for (int iy = 0; iy < N1; ++iy) Uout[(size_t)(k * NS + ix + N1 * iy) * ld + e] = y_[iy];
+    }
   }
 }
 
-template <int P, int METHOD>
+template <int P, int METHOD, int NY = 0>
 __global__ void __launch_bounds__(32 * 6) lim2d_ypass_tile_kernel(const LimArgs la, int nx, int ny,
                                                                   const double* __restrict__ X,
                                                                   const int* __restrict__ nbr,
                                                                   double* __restrict__ Uout,
                                                                   const DevScalars* __restrict__ scal) {
   if (scal && scal->flags) return;
-  lim2d_ypass_body<P, METHOD>(la, nx, ny, X, nbr, Uout, blockIdx.x * 32, blockIdx.y * 4, blockIdx.z);
+  lim2d_ypass_body<P, METHOD, NY>(la, nx, ny, X, nbr, Uout, blockIdx.x * 32, blockIdx.y * 4, blockIdx.z);
 }
 
 }  // namespace dgb

@@ -2,7 +2,9 @@
 //
 // State per point: 1D (rho, rho u, E, alpha), 2D (rho, rho u, rho v, E, alpha) with
 // alpha = 1/(gamma-1) carried non-conservatively (no flux; volume source -u.grad(alpha);
-// interface term ncterm).  Formulas restate the reference's:
+// interface term ncterm), then NY passive mass fractions rho*Y_k (conservative: flux rho*Y_k u,
+// interface fluxes of the MACRO blocks that follow each flux function in the reference's
+// face_fluxes headers).  Formulas restate the reference's:
 //   volume flux/source   evaluate_sf   code/src/physics/physics.cu:96-143 (1D), 248-301 (2D)
 //   Rusanov              oned_multifluid_rusanov  code/src/face_fluxes/oned_multifluid_fluxes.h:30-94
 //                        twod_multifluid_rusanov  code/src/face_fluxes/twod_multifluid_fluxes.h:30-97
@@ -22,9 +24,10 @@ enum { FLUX_RUS = 0, FLUX_HLL = 1, FLUX_ROE = 2 };
 // ---------------------------------------------------------------- 1D -------------------------
 // Interface flux F[4] and ncterm for the alpha equation (F[3] holds the alpha dissipation).
 // Caller forms q_L = -F + nc (element on side L) and q_R = F + nc (physics.cu:800-804).
-template <int FLUX>
+template <int FLUX, int NY = 0>
 __device__ __forceinline__ void riemann1d(double rhoL, double rhoR, double vxL, double vxR, double EtL, double EtR,
-                                          double alphaL, double alphaR, double nx, double F[4], double& nc) {
+                                          double alphaL, double alphaR, double nx, double* F, double& nc,
+                                          const double* YL = nullptr, const double* YR = nullptr) {
   const double gammaL = 1.0 + 1.0 / alphaL;
   const double gammaR = 1.0 + 1.0 / alphaR;
   const double pL = (gammaL - 1) * (EtL - 0.5 * rhoL * vxL * vxL);
@@ -38,6 +41,9 @@ __device__ __forceinline__ void riemann1d(double rhoL, double rhoR, double vxL, 
     F[2] = 0.5 * (((EtL + pL) * vxL + (EtR + pR) * vxR) * nx - maxvap * (EtR - EtL));
     F[3] = 0.5 * (-maxvap * (alphaR - alphaL));
     nc = -0.5 * 0.5 * (vxL + vxR) * (alphaR - alphaL) * nx;
+    // the reference's mass-fraction line has its dissipation outside the 1/2 (fluxes.h:90-91)
+#pragma unroll
+    for (int k = 0; k < NY; ++k) F[4 + k] = 0.5 * (YL[k] * vxL + YR[k] * vxR) * nx - maxvap * (YR[k] - YL[k]);
   } else if (FLUX == FLUX_HLL) {
     // Davis wave-speed estimates (Toro 10.48); fhll of basic_fluxes.h:22-27.  The momentum
     // component passes the velocities as its state jump, and no branch is taken when SL == 0,
@@ -50,21 +56,29 @@ __device__ __forceinline__ void riemann1d(double rhoL, double rhoR, double vxL, 
       return (SRv * FL - SLv * FR + SLv * SRv * (UR - UL)) / fabs(SRv - SLv);
     };
     F[0] = F[1] = F[2] = F[3] = 0.0;
+#pragma unroll
+    for (int k = 0; k < NY; ++k) F[4 + k] = 0.0;
     if (SL > 0) {
       F[0] = rhoL * vxL * nx;
       F[1] = (rhoL * vxL * vxL + pL) * nx;
       F[2] = (EtL + pL) * vxL * nx;
       F[3] = -0.5 * vncabs;
+#pragma unroll
+      for (int k = 0; k < NY; ++k) F[4 + k] = YL[k] * vxL * nx;
     } else if ((SL < 0) && (SR > 0)) {
       F[0] = fhll(rhoL, SL, rhoL * vxL * nx, rhoR, SR, rhoR * vxR * nx);
       F[1] = fhll(vxL, SL, (rhoL * vxL * vxL + pL) * nx, vxR, SR, (rhoR * vxR * vxR + pR) * nx);
       F[2] = fhll(EtL, SL, (EtL + pL) * vxL * nx, EtR, SR, (EtR + pR) * vxR * nx);
       F[3] = fhll(alphaL, SL, 0, alphaR, SR, 0) - 0.5 * fabs(SR + SL) / fabs(SR - SL) * vncabs;
+#pragma unroll
+      for (int k = 0; k < NY; ++k) F[4 + k] = fhll(YL[k], SL, YL[k] * vxL * nx, YR[k], SR, YR[k] * vxR * nx);
     } else if (SR < 0) {
       F[0] = rhoR * vxR * nx;
       F[1] = (rhoR * vxR * vxR + pR) * nx;
       F[2] = (EtR + pR) * vxR * nx;
       F[3] = 0.5 * vncabs;
+#pragma unroll
+      for (int k = 0; k < NY; ++k) F[4 + k] = YR[k] * vxR * nx;
     }
     nc = -0.5 * vnc;
   } else {
@@ -95,14 +109,22 @@ __device__ __forceinline__ void riemann1d(double rhoL, double rhoR, double vxL, 
            0.5 * (ws0 * dV0 * (H - v * a) + ws1 * dV1 * (0.5 * v * v) + ws2 * dV2 * (H + v * a) + ws3 * dV3 * p);
     F[3] = 0 + -0.5 * (ws0 * dV0 * 0 + ws1 * dV1 * 0 + ws2 * dV2 * 0 + ws3 * dV3 * 1);
     nc = -0.5 * v * (alphaR - alphaL) * nx;
+    // mass fractions: Roe-averaged Y and its wave strength (oned_multifluid_fluxes.h:358-370)
+#pragma unroll
+    for (int k = 0; k < NY; ++k) {
+      const double Y = (YL[k] / rhoL + RT * YR[k] / rhoR) / (1 + RT);
+      const double dVY = YR[k] - YL[k] - (dV0 + dV1 + dV2) * Y;
+      F[4 + k] = 0.5 * (YL[k] * vxL + YR[k] * vxR) * nx - 0.5 * (ws0 * dV0 * Y + ws1 * dV1 * Y + ws1 * dVY * 1 + ws2 * dV2 * Y);
+    }
   }
 }
 
 // ---------------------------------------------------------------- 2D -------------------------
-template <int FLUX>
+template <int FLUX, int NY = 0>
 __device__ __forceinline__ void riemann2d(double rhoL, double rhoR, double vxL, double vxR, double vyL, double vyR,
                                           double EtL, double EtR, double alphaL, double alphaR, double nx, double ny,
-                                          double F[5], double& nc) {
+                                          double* F, double& nc, const double* YL = nullptr,
+                                          const double* YR = nullptr) {
   const double vnL = vxL * nx + vyL * ny;
   const double vnR = vxR * nx + vyR * ny;
   const double gammaL = 1.0 + 1.0 / alphaL;
@@ -151,6 +173,13 @@ __device__ __forceinline__ void riemann2d(double rhoL, double rhoR, double vxL, 
                   ws3 * dV3 * (H + vn * a) + ws4 * dV4 * p);
     F[4] = 0 + -0.5 * (ws0 * dV0 * 0 + ws1 * dV1 * 0 + ws2 * dV2 * 0 + ws3 * dV3 * 0 + ws4 * dV4 * 1);
     nc = -0.5 * vn * (alphaR - alphaL);
+    // mass fractions (twod_multifluid_fluxes.h:307-319)
+#pragma unroll
+    for (int k = 0; k < NY; ++k) {
+      const double Y = (YL[k] / rhoL + RT * YR[k] / rhoR) / (1 + RT);
+      const double dVY = YR[k] - YL[k] - (dV0 + dV2 + dV3) * Y;
+      F[5 + k] = 0.5 * (YL[k] * vnL + YR[k] * vnR) - 0.5 * (ws0 * dV0 * Y + ws2 * dV2 * Y + ws1 * dVY * 1 + ws3 * dV3 * Y);
+    }
   } else {
     // Rusanov (2D HLL is a stub in the reference, twod_multifluid_fluxes.h:119-141; the host
     // rejects it before any launch)
@@ -161,6 +190,9 @@ __device__ __forceinline__ void riemann2d(double rhoL, double rhoR, double vxL, 
     F[3] = 0.5 * (rhoL * vnL * HL + rhoR * vnR * HR - maxvap * (EtR - EtL));
     F[4] = 0.5 * (-maxvap * (alphaR - alphaL));
     nc = -0.5 * 0.5 * (vnL + vnR) * (alphaR - alphaL);
+    // the reference's mass-fraction line has its dissipation outside the 1/2 (fluxes.h:91-94)
+#pragma unroll
+    for (int k = 0; k < NY; ++k) F[5 + k] = 0.5 * (YL[k] * vnL + YR[k] * vnR) - maxvap * (YR[k] - YL[k]);
   }
 }
 
@@ -188,8 +220,8 @@ namespace phys {
 // The same 2D interface fluxes evaluated with one reciprocal per state instead of repeated
 // divisions (x/rho -> x * (1/rho), gamma-1 = 1/alpha).  Agrees with riemann2d to a few ulp,
 // far inside the 1e-12 parity bound; used by the tiled kernel.
-template <int FLUX>
-__device__ __forceinline__ void riemann2d_rcp(const double* L, const double* R, double nx, double ny, double F[5],
+template <int FLUX, int NY = 0>
+__device__ __forceinline__ void riemann2d_rcp(const double* L, const double* R, double nx, double ny, double* F,
                                               double& nc) {
   const double rhoL = L[0], rhoR = R[0];
   const double irL = __drcp_rn(rhoL), irR = __drcp_rn(rhoR);
@@ -243,6 +275,12 @@ __device__ __forceinline__ void riemann2d_rcp(const double* L, const double* R, 
            0.5 * (w0 * (H - vn * a) + w1 * (vt * a) + w2 * (0.5 * (vx * vx + vy * vy)) + w3 * (H + vn * a) + w4 * p);
     F[4] = -0.5 * w4;
     nc = -0.5 * vn * (alphaR - alphaL);
+#pragma unroll
+    for (int k = 0; k < NY; ++k) {
+      const double Y = (L[5 + k] * irL + RT * R[5 + k] * irR) * i1;
+      const double dVY = R[5 + k] - L[5 + k] - (dV0 + dV2 + dV3) * Y;
+      F[5 + k] = 0.5 * (L[5 + k] * vnL + R[5 + k] * vnR) - 0.5 * (w0 * Y + w2 * Y + ws1 * dVY * 1 + w3 * Y);
+    }
   } else {
     const double maxvap = fmax(fabs(vnL) + aL, fabs(vnR) + aR);
     F[0] = 0.5 * (rhoL * vnL + rhoR * vnR - maxvap * (rhoR - rhoL));
@@ -251,6 +289,8 @@ __device__ __forceinline__ void riemann2d_rcp(const double* L, const double* R, 
     F[3] = 0.5 * (rhoL * vnL * HL + rhoR * vnR * HR - maxvap * (EtR - EtL));
     F[4] = 0.5 * (-maxvap * (alphaR - alphaL));
     nc = -0.5 * 0.5 * (vnL + vnR) * (alphaR - alphaL);
+#pragma unroll
+    for (int k = 0; k < NY; ++k) F[5 + k] = 0.5 * (L[5 + k] * vnL + R[5 + k] * vnR) - maxvap * (R[5 + k] - L[5 + k]);
   }
 }
 

@@ -61,9 +61,9 @@ struct TileArgs {
   int nx, ny, ld;
 };
 
-template <int P, int TW, int TH>
+template <int P, int TW, int TH, int NY = 0>
 struct TileDims {
-  static constexpr int N1 = P + 1, NS = N1 * N1, NF = 5, NT = TW * TH;
+  static constexpr int N1 = P + 1, NS = N1 * N1, NF = 5 + NY, NT = TW * TH;
   static constexpr int NXF = (TW + 1) * TH * N1;  // x-face points
   static constexpr int NYF = TW * (TH + 1) * N1;  // y-face points
   static constexpr int NCODE = 2 * TH + 2 * TW;   // boundary codes / neighbours of the tile edges
@@ -72,7 +72,7 @@ struct TileDims {
   static constexpr size_t tile_doubles = (size_t)NF * NS * NT;
   static constexpr uint32_t tile_bytes = (uint32_t)(tile_doubles * 8);
   static constexpr size_t halo_doubles = (size_t)2 * TH * NF * N1 + (size_t)2 * TW * NF * N1;
-  static constexpr size_t face_doubles = (size_t)6 * (NXF + NYF);
+  static constexpr size_t face_doubles = (size_t)(NF + 1) * (NXF + NYF);  // NF fluxes + ncterm per point
   // the face buffer is reused for the prefetched stage base, so it is at least one tile
   static constexpr size_t fbuf_doubles = face_doubles > tile_doubles ? face_doubles : tile_doubles;
   // byte offsets; every region a TMA copy lands in starts on a 128-byte boundary
@@ -106,11 +106,16 @@ constexpr bool kSfLift = DGB_SF_LIFT != 0;
 // The work of one tile (origin tx0, ty0).  The caller has initialised the mbarrier at the start of
 // shared memory; `phase` counts its completed phases (a persistent caller runs many tiles on one
 // barrier).  Every early return is taken by the whole CTA, after its last barrier.
-template <int P, int FLUX, int MODE, int TW, int TH, int UNROLL>
+// NY passive mass fractions rho*Y_k follow the five gamma-model fields: conservative volume flux
+// rho*Y_k (u, v) (physics.cu:293-298) and the interface fluxes of phys::riemann2d_rcp.
+template <int P, int FLUX, int MODE, int TW, int TH, int UNROLL, int NY = 0>
 __device__ __forceinline__ void tile2d_body(const TileArgs& a, const CUtensorMap* mapU, const CUtensorMap* mapB,
                                             int tx0, int ty0, unsigned char* smraw, uint32_t& phase) {
-  using Dm = TileDims<P, TW, TH>;
-  constexpr int N1 = Dm::N1, NS = Dm::NS, NF = 5, NT = Dm::NT, NXF = Dm::NXF, NYF = Dm::NYF;
+  using Dm = TileDims<P, TW, TH, NY>;
+  constexpr int N1 = Dm::N1, NS = Dm::NS, NF = Dm::NF, NT = Dm::NT, NXF = Dm::NXF, NYF = Dm::NYF;
+  constexpr int FS = NF + 1;      // face record: NF fluxes, ncterm
+  constexpr int NFL = 4 + NY;     // fields with a volume flux: rho, rho u, rho v, E, rho Y_k
+  auto fld = [](int k) { return k < 4 ? k : k + 1; };
   uint64_t* bar = reinterpret_cast<uint64_t*>(smraw);
   int* s_ok = reinterpret_cast<int*>(smraw + 8);
   int* codes = reinterpret_cast<int*>(smraw + Dm::head_bytes);  // [L: TH][R: TH][D: TW][U: TW]
@@ -242,12 +247,12 @@ __device__ __forceinline__ void tile2d_body(const TileArgs& a, const CUtensorMap
       R[f] = sr;
     }
     double F[NF], nc;
-    phys::riemann2d_rcp<FLUX>(L, R, nxv, nyv, F, nc);
+    phys::riemann2d_rcp<FLUX, NY>(L, R, nxv, nyv, F, nc);
     // boundary faces seen from the right/top element store -F so that every consumer forms
     // (+F + nc) on its left/bottom face and (-F + nc) on its right/top face
 #pragma unroll
-    for (int f = 0; f < NF; ++f) Fs[k * 6 + f] = sgn * F[f];
-    Fs[k * 6 + 5] = nc;
+    for (int f = 0; f < NF; ++f) Fs[k * FS + f] = sgn * F[f];
+    Fs[k * FS + NF] = nc;
   }
   __syncthreads();
 
@@ -271,11 +276,11 @@ __device__ __forceinline__ void tile2d_body(const TileArgs& a, const CUtensorMap
     else { base = NXF + ((ty + 1) * TW + tx) * N1; s = -1.0; jw = a.JFy; }
 #pragma unroll
     for (int g = 0; g < N1; ++g) {
-      const double* fp = Fs + (base + g) * 6;
+      const double* fp = Fs + (base + g) * FS;
       const double w = jw * DGB_TAB2(P, wf[g]);
       double c[NF];
 #pragma unroll
-      for (int f = 0; f < NF; ++f) c[f] = (s * fp[f] + (f == 4 ? fp[5] : 0.0)) * w;
+      for (int f = 0; f < NF; ++f) c[f] = (s * fp[f] + (f == 4 ? fp[NF] : 0.0)) * w;
 #pragma unroll
       for (int j = 0; j < N1; ++j) {
         const int t = kf == 0 ? N1 * j : kf == 1 ? P + N1 * j : kf == 2 ? j : j + N1 * P;
@@ -317,12 +322,12 @@ __device__ __forceinline__ void tile2d_body(const TileArgs& a, const CUtensorMap
       for (int ix = 0; ix < N1; ++ix) sd += DGB_TAB2(P, D1[gx][ix]) * us[(4 * NS + ix + N1 * iy) * NT];
       dT[iy] = sd;
     }
-    double Ax[4][N1], Ay[4][N1], As[N1];  // column sums of the sum-factorised lift
+    double Ax[NFL][N1], Ay[NFL][N1], As[N1];  // column sums of the sum-factorised lift
 #pragma unroll
     for (int iy = 0; iy < N1; ++iy) {
       As[iy] = 0.0;
 #pragma unroll
-      for (int f = 0; f < 4; ++f) Ax[f][iy] = Ay[f][iy] = 0.0;
+      for (int f = 0; f < NFL; ++f) Ax[f][iy] = Ay[f][iy] = 0.0;
     }
 #pragma unroll
     for (int gy = 0; gy < NG1; ++gy) {
@@ -343,22 +348,24 @@ __device__ __forceinline__ void tile2d_body(const TileArgs& a, const CUtensorMap
       const double p = gm1 * (Et - 0.5 * rho * (uu * uu + vv * vv));
       const double wx = DGB_TAB2(P, W[g]) * a.cx, wy = DGB_TAB2(P, W[g]) * a.cy;
       const double mx = ug[1] * wx, my = ug[2] * wy;
-      const double gxv[4] = {mx, mx * uu + wx * p, mx * vv, wx * ((Et + p) * uu)};
-      const double gyv[4] = {my, my * uu, my * vv + wy * p, wy * ((Et + p) * vv)};
+      double gxv[NFL] = {mx, mx * uu + wx * p, mx * vv, wx * ((Et + p) * uu)};
+      double gyv[NFL] = {my, my * uu, my * vv + wy * p, wy * ((Et + p) * vv)};
+#pragma unroll
+      for (int k = 0; k < NY; ++k) { gxv[4 + k] = wx * (ug[5 + k] * uu); gyv[4 + k] = wy * (ug[5 + k] * vv); }
       const double gs = (DGB_TAB2(P, W[g]) * a.J) * (-uu * dax * a.sx - vv * day * a.sy);
       if constexpr (kSfLift) {
 #pragma unroll
         for (int iy = 0; iy < N1; ++iy) {
           const double b = DGB_TAB2(P, B1[gy][iy]), d = DGB_TAB2(P, D1[gy][iy]);
 #pragma unroll
-          for (int f = 0; f < 4; ++f) { Ax[f][iy] += b * gxv[f]; Ay[f][iy] += d * gyv[f]; }
+          for (int f = 0; f < NFL; ++f) { Ax[f][iy] += b * gxv[f]; Ay[f][iy] += d * gyv[f]; }
           As[iy] += b * gs;
         }
       } else {
 #pragma unroll
         for (int t = 0; t < NS; ++t) {
 #pragma unroll
-          for (int f = 0; f < 4; ++f) r[f][t] += DGB_TAB2(P, dPx[g][t]) * gxv[f] + DGB_TAB2(P, dPy[g][t]) * gyv[f];
+          for (int f = 0; f < NFL; ++f) r[fld(f)][t] += DGB_TAB2(P, dPx[g][t]) * gxv[f] + DGB_TAB2(P, dPy[g][t]) * gyv[f];
           r[4][t] += DGB_TAB2(P, Phi[g][t]) * gs;
         }
       }
@@ -372,7 +379,7 @@ __device__ __forceinline__ void tile2d_body(const TileArgs& a, const CUtensorMap
           const double dx = DGB_TAB2(P, D1[gx][ix]), bx = DGB_TAB2(P, B1[gx][ix]);
           const int t = ix + N1 * iy;
 #pragma unroll
-          for (int f = 0; f < 4; ++f) r[f][t] += dx * Ax[f][iy] + bx * Ay[f][iy];
+          for (int f = 0; f < NFL; ++f) r[fld(f)][t] += dx * Ax[f][iy] + bx * Ay[f][iy];
           r[4][t] += bx * As[iy];
         }
     }
@@ -433,7 +440,7 @@ __device__ __forceinline__ void tile2d_body(const TileArgs& a, const CUtensorMap
   }
 }
 
-template <int P, int FLUX, int MODE, int TW, int TH>
+template <int P, int FLUX, int MODE, int TW, int TH, int NY = 0>
 __global__ void __launch_bounds__(TW * TH, 2)
     residual2d_tile_kernel(const TileArgs a, const __grid_constant__ CUtensorMap mapU,
                            const __grid_constant__ CUtensorMap mapB) {
@@ -444,7 +451,8 @@ __global__ void __launch_bounds__(TW * TH, 2)
     fence_mbar_init();
   }
   uint32_t phase = 0;
-  tile2d_body<P, FLUX, MODE, TW, TH, vol_unroll<P>()>(a, &mapU, &mapB, blockIdx.x * TW, blockIdx.y * TH, smraw, phase);
+  tile2d_body<P, FLUX, MODE, TW, TH, vol_unroll<P>(), NY>(a, &mapU, &mapB, blockIdx.x * TW, blockIdx.y * TH, smraw,
+                                                         phase);
 }
 
 }  // namespace dgb

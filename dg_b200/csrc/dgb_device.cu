@@ -172,11 +172,11 @@ void launch_res2d(dgb_ctx* c, const StageArgs& a) {
   k<<<grid, RES2D_NT, smem, c->st>>>(c->cs, a);
 }
 
-template <int P, int FLUX, int MODE>
+template <int P, int FLUX, int MODE, int NY = 0>
 void launch_res1d(dgb_ctx* c, const StageArgs& a) {
   const int grid = (c->ne + 127) / 128;
   ProfScope ps(c, KC_RESIDUAL);
-  residual1d_kernel<P, FLUX, MODE><<<grid, 128, 0, c->st>>>(c->cs, a);
+  residual1d_kernel<P, FLUX, MODE, NY><<<grid, 128, 0, c->st>>>(c->cs, a);
 }
 
 constexpr int TILE_W = 32, TILE_H = 4;
@@ -190,12 +190,12 @@ const CUtensorMap& map_of(dgb_ctx* c, const double* p) {
   return c->mapA;
 }
 
-template <int P, int FLUX, int MODE>
+template <int P, int FLUX, int MODE, int NY = 0>
 void launch_tile2d(dgb_ctx* c, const StageArgs& s) {
   constexpr int TH = tile_h_for(P);
-  using Dm = TileDims<P, TILE_W, TH>;
+  using Dm = TileDims<P, TILE_W, TH, NY>;
   constexpr size_t smem = Dm::smem_bytes;
-  auto k = residual2d_tile_kernel<P, FLUX, MODE, TILE_W, TH>;
+  auto k = residual2d_tile_kernel<P, FLUX, MODE, TILE_W, TH, NY>;
   static bool attr = false;
   if (!attr) { cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem); attr = true; }
   TileArgs a;
@@ -283,6 +283,25 @@ int residual_dispatch(dgb_ctx* c, const StageArgs& a) {
       default: return set_error(DGB_ERR_UNSUPPORTED, "mixed form: p = 1..3 with Rusanov or Roe");
     }
   }
+  if (c->tiled && c->nmass == 1) {
+    switch (c->p * 10 + c->flux) {
+      case 10: launch_tile2d<1, 0, MODE, 1>(c, a); return 0;
+      case 12: launch_tile2d<1, 2, MODE, 1>(c, a); return 0;
+      case 20: launch_tile2d<2, 0, MODE, 1>(c, a); return 0;
+      case 22: launch_tile2d<2, 2, MODE, 1>(c, a); return 0;
+      case 30: launch_tile2d<3, 0, MODE, 1>(c, a); return 0;
+      case 32: launch_tile2d<3, 2, MODE, 1>(c, a); return 0;
+      default: return set_error(DGB_ERR_UNSUPPORTED, "no residual kernel for this (p, flux) with a mass fraction");
+    }
+  }
+  if (c->D == 1 && c->nmass == 1) {
+#define R1Y(P, F) case P * 10 + F: launch_res1d<P, F, MODE, 1>(c, a); return 0;
+    switch (c->p * 10 + c->flux) {
+      R1Y(1, 0) R1Y(1, 1) R1Y(1, 2) R1Y(2, 0) R1Y(2, 1) R1Y(2, 2) R1Y(3, 0) R1Y(3, 1) R1Y(3, 2)
+      default: return set_error(DGB_ERR_UNSUPPORTED, "no residual kernel for this (p, flux) with a mass fraction");
+    }
+#undef R1Y
+  }
   if (c->tiled) {
     const int key = c->p * 10 + c->flux;
     switch (key) {
@@ -329,9 +348,9 @@ void launch_lim2d_fused(dgb_ctx* c, const double* in, double* out) {
   k<<<grid, block, smem, c->st>>>(la, c->nx, c->ny, in, c->nbr, out, c->scal);
 }
 
-template <int P, int METHOD>
+template <int P, int METHOD, int NY = 0>
 void launch_lim2d(dgb_ctx* c, double* U) {
-  if (c->fused_lim) {
+  if (NY == 0 && c->fused_lim) {
     cudaMemcpyAsync(c->X, U, c->nstate * sizeof(double), cudaMemcpyDeviceToDevice, c->st);
     launch_lim2d_fused<P, METHOD>(c, c->X, U);
     return;
@@ -340,10 +359,10 @@ void launch_lim2d(dgb_ctx* c, double* U) {
   const LimArgs la{c->ld, c->ne};
   if (c->rowmajor) {
     dim3 gx((c->nx + 29) / 30, c->ny), bx(32, P + 1);
-    lim2d_xpass_tile_kernel<P, METHOD><<<gx, bx, 0, c->st>>>(la, c->nx, U, c->nbr, c->X, c->scal);
+    lim2d_xpass_tile_kernel<P, METHOD, NY><<<gx, bx, 0, c->st>>>(la, c->nx, U, c->nbr, c->X, c->scal);
     dim3 gy((c->nx + 31) / 32, (c->ny + 3) / 4, P + 1), by(32, 6);
-    lim2d_ypass_tile_kernel<P, METHOD><<<gy, by, 0, c->st>>>(la, c->nx, c->ny, c->X, c->nbr, U, c->scal);
-  } else {
+    lim2d_ypass_tile_kernel<P, METHOD, NY><<<gy, by, 0, c->st>>>(la, c->nx, c->ny, c->X, c->nbr, U, c->scal);
+  } else if (NY == 0) {
     dim3 grid((c->ne + 127) / 128, P + 1);
     lim2d_xpass_kernel<P, METHOD><<<grid, 128, 0, c->st>>>(la, U, c->nbr, c->X, c->scal);
     lim2d_ypass_kernel<P, METHOD><<<grid, 128, 0, c->st>>>(la, c->X, c->nbr, U, c->scal);
@@ -351,13 +370,13 @@ void launch_lim2d(dgb_ctx* c, double* U) {
   c->counter++;
 }
 
-template <int P, int METHOD>
+template <int P, int METHOD, int NY = 0>
 void launch_lim1d(dgb_ctx* c, double* U) {
   const int grid = (c->ne + 127) / 128;
   {
     ProfScope ps(c, KC_LIMITER);
     const LimArgs la{c->ld, c->ne};
-    lim1d_kernel<P, METHOD><<<grid, 128, 0, c->st>>>(la, U, c->nbr, c->X, c->scal);
+    lim1d_kernel<P, METHOD, NY><<<grid, 128, 0, c->st>>>(la, U, c->nbr, c->X, c->scal);
   }
   cudaMemcpyAsync(U, c->X, c->nstate * sizeof(double), cudaMemcpyDeviceToDevice, c->st);
 }
@@ -509,6 +528,18 @@ int limit_dispatch(dgb_ctx* c, double* U, bool rescore = true) {
     }
   }
   const int key = c->p * 10 + c->limiter;
+  if (c->nmass == 1) {
+#define L2Y(P, M) case P * 10 + M: launch_lim2d<P, M, 1>(c, U); return 0;
+#define L1Y(P, M) case P * 10 + M: launch_lim1d<P, M, 1>(c, U); return 0;
+    if (c->D == 2) {
+      switch (key) { L2Y(1, 1) L2Y(1, 2) L2Y(2, 1) L2Y(2, 2) L2Y(3, 1) L2Y(3, 2) default: break; }
+    } else {
+      switch (key) { L1Y(1, 1) L1Y(1, 2) L1Y(2, 1) L1Y(2, 2) L1Y(3, 1) L1Y(3, 2) default: break; }
+    }
+#undef L2Y
+#undef L1Y
+    return set_error(DGB_ERR_UNSUPPORTED, "limiter not available with a mass fraction");
+  }
 #define L2(P, M) case P * 10 + M: launch_lim2d<P, M>(c, U); return 0;
 #define L1(P, M) case P * 10 + M: launch_lim1d<P, M>(c, U); return 0;
   if (c->D == 2) {
@@ -683,7 +714,18 @@ extern "C" int dgb_create(const dgb_problem* prob, int device, dgb_ctx** out) {
   c->tiled = c->rowmajor && P.p <= 3 && P.nx % TILE_W == 0 && P.ny % tile_h_for(P.p) == 0;
   // opt-in: measured slower than the two tiled passes on 512 x 256, p = 2 (64 vs 55 us per stage)
   c->fused_lim = c->rowmajor && (P.limiter == DGB_LIM_HRL || P.limiter == DGB_LIM_M2L) &&
-                 std::getenv("DGB_FUSED_LIMITER") != nullptr;
+                 std::getenv("DGB_FUSED_LIMITER") != nullptr && P.N_Y == 0;
+  c->nmass = P.N_Y;
+  if (P.N_Y > 1) { delete c; return set_error(DGB_ERR_UNSUPPORTED, "at most one mass fraction on the device path"); }
+  if (P.N_Y == 1 && P.D == 2 && !c->tiled) {
+    delete c;
+    return set_error(DGB_ERR_UNSUPPORTED, "mass fractions in 2D need a structured row-major grid with nx a multiple "
+                                          "of 32 and ny of 4 (p = 3: 2)");
+  }
+  if (P.N_Y == 1 && P.limiter != DGB_LIM_NONE && P.limiter != DGB_LIM_HRL && P.limiter != DGB_LIM_M2L) {
+    delete c;
+    return set_error(DGB_ERR_UNSUPPORTED, "with a mass fraction the limiter is none, hrl or m2l");
+  }
   if (int rc = upload_tables(c->cs, P.D, P.p)) { delete c; return rc; }
   auto fail = [&](cudaError_t e, const char* what) {
     dgb_destroy(c);
@@ -697,7 +739,7 @@ extern "C" int dgb_create(const dgb_problem* prob, int device, dgb_ctx** out) {
     if ((e = cudaMalloc(b, sb)) != cudaSuccess) return fail(e, "state allocation");
     cudaMemset(*b, 0, sb);
   }
-  const size_t xb = (size_t)6 * c->ns * c->ld * sizeof(double);
+  const size_t xb = (size_t)(6 + c->nmass) * c->ns * c->ld * sizeof(double);  // m2 x pass: 6 quantities + Y_k
   if ((e = cudaMalloc(&c->X, std::max(xb, sb))) != cudaSuccess) return fail(e, "limiter scratch");
   cudaMemset(c->X, 0, std::max(xb, sb));
   if ((e = cudaMalloc(&c->ref, (size_t)c->ne * c->nf * c->ns * sizeof(double))) != cudaSuccess) return fail(e, "staging");
@@ -864,7 +906,8 @@ extern "C" int dgb_mlp_param_count(void) { return MLP_NPARAM; }
 
 extern "C" int dgb_indicator_features(dgb_ctx* c, float* X_dev) {
   if (!c || !X_dev) return set_error(DGB_ERR_ARG, "null argument");
-  if (c->D != 2 || c->p != 2) return set_error(DGB_ERR_UNSUPPORTED, "the indicator is built for 2D, p = 2");
+  if (c->D != 2 || c->p != 2 || c->nmass != 0)
+    return set_error(DGB_ERR_UNSUPPORTED, "the indicator is built for 2D, p = 2, without mass fractions");
   DGB_CUDA(cudaSetDevice(c->device));
   indicator_features_kernel<2><<<(c->ne + 127) / 128, 128, 0, c->st>>>(c->A, c->ld, c->ne, c->nbr, X_dev);
   DGB_CUDA(cudaGetLastError());
@@ -874,7 +917,8 @@ extern "C" int dgb_indicator_features(dgb_ctx* c, float* X_dev) {
 
 extern "C" int dgb_indicator_labels(dgb_ctx* c, float* y_dev) {
   if (!c || !y_dev) return set_error(DGB_ERR_ARG, "null argument");
-  if (c->D != 2 || c->p != 2) return set_error(DGB_ERR_UNSUPPORTED, "the indicator is built for 2D, p = 2");
+  if (c->D != 2 || c->p != 2 || c->nmass != 0)
+    return set_error(DGB_ERR_UNSUPPORTED, "the indicator is built for 2D, p = 2, without mass fractions");
   if (c->limiter == 0) return set_error(DGB_ERR_ARG, "labels need a limiter");
   DGB_CUDA(cudaSetDevice(c->device));
   if (int rc = reset_scalars(c, 0.0)) return rc;
@@ -947,8 +991,9 @@ extern "C" int dgb_set_indicator(dgb_ctx* c, const float* params, float threshol
     c->ind_on = false;
     return DGB_OK;
   }
-  if (c->D != 2 || c->p != 2 || c->limiter != DGB_LIM_M2L)
-    return set_error(DGB_ERR_UNSUPPORTED, "the learned indicator gates the m2l limiter of 2D p = 2 problems");
+  if (c->D != 2 || c->p != 2 || c->limiter != DGB_LIM_M2L || c->nmass != 0)
+    return set_error(DGB_ERR_UNSUPPORTED,
+                     "the learned indicator gates the m2l limiter of 2D p = 2 problems without mass fractions");
   if (!c->ind_params) {
     cudaError_t e;
     if ((e = cudaMalloc(&c->ind_params, MLP_NPARAM * sizeof(float))) != cudaSuccess ||
@@ -1002,7 +1047,7 @@ extern "C" int dgb_indicator_scores(dgb_ctx* c, const double* U, float* score, i
 extern "C" int dgb_set_form(dgb_ctx* c, int form) {
   if (!c) return set_error(DGB_ERR_ARG, "null argument");
   if (form != DGB_FORM_FP64 && form != DGB_FORM_MIXED) return set_error(DGB_ERR_ARG, "unknown form");
-  if (form == DGB_FORM_MIXED && !(c->tiled && c->flux != DGB_FLUX_HLL))
+  if (form == DGB_FORM_MIXED && !(c->tiled && c->flux != DGB_FLUX_HLL && c->nmass == 0))
     return set_error(DGB_ERR_UNSUPPORTED,
                      "the mixed form needs a structured 2D grid with nx a multiple of 32 and ny of 4 (p = 3: 2), "
                      "Rusanov or Roe");

@@ -59,9 +59,9 @@ extern "C" int dgb_problem_from_deck(const char* deck_path, dgb_problem** out) {
     else if (mo->second == "ROE") flux = DGB_FLUX_ROE;
     else return set_error(DGB_ERR_ARG, "unknown FLUX " + mo->second);
   }
+  int n_mass = 0;
   mo = d.make_options.find("MASS");
-  if (mo != d.make_options.end() && std::atoi(mo->second.c_str()) != 0)
-    return set_error(DGB_ERR_UNSUPPORTED, "mass fractions (MASS>0) are outside the device path");
+  if (mo != d.make_options.end()) n_mass = std::atoi(mo->second.c_str());
   mo = d.make_options.find("GAMM");
   if (mo != d.make_options.end() && mo->second != "GAMNCON")
     return set_error(DGB_ERR_UNSUPPORTED, "only the GAMNCON gamma model is on the device path");
@@ -83,7 +83,7 @@ extern "C" int dgb_problem_from_deck(const char* deck_path, dgb_problem** out) {
   if (!st.ok()) return set_error(st.code, st.msg);
   auto* pr = new dgb_problem();
   st = dgb::build_problem(std::move(m), dim, d.order, d.elem_type, flux, limiter_code(d.limiter), d.cfl,
-                          d.thresholds, outt, tf, pr->P);
+                          d.thresholds, outt, tf, pr->P, n_mass);
   if (!st.ok()) { delete pr; return set_error(st.code, st.msg); }
   pr->P.deck_dir = dir;
   pr->P.deck_ic = d.ic;
@@ -116,10 +116,11 @@ extern "C" int dgb_problem_structured(const dgb_mesh_spec* mesh, const dgb_optio
   if (rc) return rc;
   if (opt->flux < 0 || opt->flux > 2) return set_error(DGB_ERR_ARG, "bad flux");
   if (opt->limiter < 0 || opt->limiter > 7) return set_error(DGB_ERR_ARG, "bad limiter");
+  if (opt->n_mass < 0 || opt->n_mass > 10) return set_error(DGB_ERR_ARG, "n_mass must be 0..10");
   std::vector<double> th(opt->thresholds, opt->thresholds + std::max(0, std::min(3, opt->n_thresholds)));
   auto* pr = new dgb_problem();
   dgb::Status st = dgb::build_problem(mesh_from_spec(mesh), mesh->dim, mesh->order, mesh->dim == 1 ? "lin" : "qua",
-                                      opt->flux, opt->limiter, opt->cfl, th, {}, 0.0, pr->P);
+                                      opt->flux, opt->limiter, opt->cfl, th, {}, 0.0, pr->P, opt->n_mass);
   if (!st.ok()) { delete pr; return set_error(st.code, st.msg); }
   *out = pr;
   return DGB_OK;

@@ -110,15 +110,17 @@ Status fail(int code, const std::string& msg) { Status s; s.code = code; s.msg =
 
 Status build_problem(Mesh&& mesh, int dim, int p, const std::string& kind, int flux, int limiter, double cfl,
                      const std::vector<double>& thresholds, const std::vector<double>& out_times, double final_time,
-                     Problem& P) {
+                     Problem& P, int n_mass) {
   P = Problem();
   if (dim != 1 && dim != 2) return fail(1, "dimension must be 1 or 2");
+  if (n_mass < 0 || n_mass > 10) return fail(1, "mass fractions: 0..10 (MASS of the reference Makefile)");
   if (p < 1 || p > 4) return fail(4, "polynomial order must be 1..4");
   if (dim == 1 && kind != "lin") return fail(4, "1D problems use 'lin' elements");
   if (dim == 2 && kind != "qua") return fail(4, "2D problems use 'qua' elements (triangles are outside this path)");
   P.D = dim;
   P.p = p;
-  P.N_F = dim == 1 ? 4 : 5;
+  P.N_Y = n_mass;
+  P.N_F = (dim == 1 ? 4 : 5) + n_mass;
   P.flux = flux;
   P.limiter = limiter;
   P.cfl = cfl;
@@ -543,7 +545,14 @@ Status build_problem(Mesh&& mesh, int dim, int p, const std::string& kind, int f
 Status init_state(const Problem& P, const std::string& ic, const std::vector<double>& prm, uint64_t seed, double* U) {
   const int NS = P.N_s, NF = P.N_F, NE = P.N_E, D = P.D;
   auto X = [&](int i, int e, int a) { return P.xyz_nodes[i + (size_t)(e * D + a) * NS]; };
+  // passive mass fractions: rho*Y_k with Y_k = the region indicator `ymark` of the state set last
+  // (1 for the first / left / bubble region, 0 elsewhere; every Y_k alike)
+  double ymark = 0.0;
+  auto setY = [&](int e, int i, double rho) {
+    for (int k = 0; k < P.N_Y; ++k) U[(e * NF + NF - P.N_Y + k) * NS + i] = rho * ymark;
+  };
   auto set = [&](int e, int i, const double* prim) {  // prim = rho, u, v, p, gamma (1D: rho,u,p,gamma)
+    setY(e, i, prim[0]);
     double* u = U;
     if (D == 1) {
       const double rho = prim[0], vx = prim[1], pr = prim[2], g = prim[3];
@@ -567,7 +576,10 @@ Status init_state(const Problem& P, const std::string& ic, const std::vector<dou
     // first node at x < 1e-8 (buildLRstates_multifluid, init_cond.cc:351-398)
     const double L[4] = {1.0, 0.0, 1.0, 1.4}, R[4] = {0.125, 0.0, 0.1, 1.6};
     for (int e = 0; e < NE; ++e)
-      for (int i = 0; i < NS; ++i) set(e, i, X(0, e, 0) < 1e-8 ? L : R);
+      for (int i = 0; i < NS; ++i) {
+        ymark = X(0, e, 0) < 1e-8 ? 1.0 : 0.0;
+        set(e, i, X(0, e, 0) < 1e-8 ? L : R);
+      }
     return Status();
   }
   if (ic == "tube_noise" && D == 1) {
@@ -580,6 +592,7 @@ Status init_state(const Problem& P, const std::string& ic, const std::vector<dou
       for (int i = 0; i < NS; ++i) {
         double s[4] = {left ? 1.0 : 0.125, 0.0, left ? 1.0 : 0.1, left ? 1.4 : 1.6};
         s[0] += amp * (2.0 * U01(rng) - 1.0);
+        ymark = left ? 1.0 : 0.0;
         set(e, i, s);
       }
     }
@@ -602,6 +615,7 @@ Status init_state(const Problem& P, const std::string& ic, const std::vector<dou
       double cx = 0;
       for (int k = 0; k < NS; ++k) cx += X(k, e, 0);
       cx /= NS;
+      ymark = cx >= xs ? 0.0 : 1.0;
       for (int i = 0; i < NS; ++i) set(e, i, q[cx >= xs ? 1 : 0]);
     }
     return Status();
@@ -626,8 +640,9 @@ Status init_state(const Problem& P, const std::string& ic, const std::vector<dou
         double r = 0.2;
         for (int k = 0; k < 8; ++k) r += amp[k] * std::cos((k + 2) * th + ph[k]);
         double s[5];
+        ymark = 0.0;
         if (x < xs) { s[0] = rho2; s[1] = u2; s[2] = 0; s[3] = p2; s[4] = g; }
-        else if (dx * dx + dy * dy < r * r) { s[0] = 0.138; s[1] = 0; s[2] = 0; s[3] = p1; s[4] = 1.67; }
+        else if (dx * dx + dy * dy < r * r) { s[0] = 0.138; s[1] = 0; s[2] = 0; s[3] = p1; s[4] = 1.67; ymark = 1.0; }
         else { s[0] = rho1; s[1] = 0; s[2] = 0; s[3] = p1; s[4] = g; }
         set(e, i, s);
       }
@@ -656,6 +671,7 @@ Status init_state(const Problem& P, const std::string& ic, const std::vector<dou
       for (int k = 0; k < 4; ++k) { cx += X(k, e, 0); cy += X(k, e, 1); }
       cx /= 4; cy /= 4;
       const int k = (cx >= xc ? 1 : 0) + (cy >= yc ? 2 : 0);
+      ymark = (k == 0 || k == 3) ? 1.0 : 0.0;
       for (int i = 0; i < NS; ++i) set(e, i, q[k]);
     }
     return Status();
@@ -670,9 +686,12 @@ Status init_state(const Problem& P, const std::string& ic, const std::vector<dou
 // .pos output / restart (simpleMesh::writeSolution / readSolution, simpleMesh.cc:322-459;
 // field formatting of printer_{oned,twod}_multifluid.cu, names of printer.cc:11-74)
 // ---------------------------------------------------------------------------------------
-static std::vector<std::pair<std::string, std::string>> pos_names(int D) {
-  if (D == 1) return {{"Rho", "rho"}, {"Ux", "ux"}, {"G", "g"}, {"P", "p"}};
-  return {{"Rho", "rho"}, {"Ux", "ux"}, {"Uy", "uy"}, {"G", "g"}, {"P", "p"}};
+static std::vector<std::pair<std::string, std::string>> pos_names(int D, int NY) {
+  std::vector<std::pair<std::string, std::string>> n;
+  if (D == 1) n = {{"Rho", "rho"}, {"Ux", "ux"}, {"G", "g"}, {"P", "p"}};
+  else n = {{"Rho", "rho"}, {"Ux", "ux"}, {"Uy", "uy"}, {"G", "g"}, {"P", "p"}};
+  for (int k = 0; k < NY; ++k) n.push_back({"Y" + std::to_string(k), "y" + std::to_string(k)});  // printer.cc:65-71
+  return n;
 }
 
 Status write_pos(const Problem& P, const double* U, int step, double time, const std::string& dir) {
@@ -699,8 +718,9 @@ Status write_pos(const Problem& P, const double* U, int step, double time, const
         out[(e * NF + 3) * NS + i] = g;
         out[(e * NF + 4) * NS + i] = (g - 1) * (et - 0.5 * (ux * ux + uy * uy) * rho);
       }
+      for (int k = NF - P.N_Y; k < NF; ++k) out[(e * NF + k) * NS + i] = U[(e * NF + k) * NS + i] / rho;
     }
-  const auto names = pos_names(P.D);
+  const auto names = pos_names(P.D, P.N_Y);
   for (int fc = 0; fc < NF; ++fc) {
     char stepstr[32];
     snprintf(stepstr, sizeof stepstr, "%010d", step);
@@ -723,7 +743,7 @@ Status write_pos(const Problem& P, const double* U, int step, double time, const
 Status read_pos(const Problem& P, int step, const std::string& dir, double& time, double* U) {
   const int NS = P.N_s, NF = P.N_F, NE = P.N_E;
   std::vector<double> out((size_t)NS * NE * NF);
-  const auto names = pos_names(P.D);
+  const auto names = pos_names(P.D, P.N_Y);
   for (int fc = 0; fc < NF; ++fc) {
     char stepstr[32];
     snprintf(stepstr, sizeof stepstr, "%010d", step);
@@ -765,6 +785,7 @@ Status read_pos(const Problem& P, int step, const std::string& dir, double& time
         U[(e * NF + 3) * NS + i] = pr / (g - 1) + 0.5 * rho * (ux * ux + uy * uy);
         U[(e * NF + 4) * NS + i] = 1.0 / (g - 1);
       }
+      for (int k = NF - P.N_Y; k < NF; ++k) U[(e * NF + k) * NS + i] = rho * out[(e * NF + k) * NS + i];
     }
   return Status();
 }

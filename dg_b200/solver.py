@@ -38,9 +38,10 @@ class Problem:
     def structured(cls, dim: int, order: int, nx: int, ny: int = 1, x0: float = 0.0, x1: float = 1.0,
                    y0: float = 0.0, y1: float = 1.0, bc: Sequence[str | int] = ("transmissive",) * 4,
                    flux: str = "roe", limiter: str = "m2l", cfl: float = -1.0,
-                   thresholds: Iterable[float] = ()) -> "Problem":
+                   thresholds: Iterable[float] = (), n_mass: int = 0) -> "Problem":
         spec = mesh_spec(dim, order, nx, ny, x0, x1, y0, y1, bc)
         opt = F.Options()
+        opt.n_mass = int(n_mass)
         opt.flux = F.FLUX[flux.lower()]
         opt.limiter = F.LIMITER[limiter.lower()]
         opt.cfl = cfl

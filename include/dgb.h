@@ -38,7 +38,7 @@
 extern "C" {
 #endif
 
-#define DGB_ABI_VERSION 1
+#define DGB_ABI_VERSION 2
 
 enum dgb_status {
   DGB_OK = 0,
@@ -99,11 +99,14 @@ typedef struct {
   double cfl;          /* deck CFL; < 0 selects a fixed step (rk.cc:136-139) */
   double thresholds[3];/* sensor thresholds (sensor.h:35-45); n_thresholds of them are set */
   int n_thresholds;
+  int n_mass;          /* passive mass fractions rho*Y_k appended to the state (MASS of the
+                        * reference Makefile; N_F = 4 (1D) / 5 (2D) + n_mass) */
 } dgb_options;
 
 /* Reads a reference input deck (format of code/src/deck/deck.cc:11-64) and the Gmsh 2.2 mesh
  * it names (path relative to the deck's directory).  The flux comes from the deck's optional
- * "#Make options" block (FLUX=ROE|RUS|HLL, the block tests/runtests.py:80-87 reads), else ROE. */
+ * "#Make options" block (FLUX=ROE|RUS|HLL, the block tests/runtests.py:80-87 reads), else ROE;
+ * MASS=n there gives n passive mass fractions. */
 int dgb_problem_from_deck(const char* deck_path, dgb_problem** out);
 /* Builds the same problem from an in-memory structured mesh (identical to reading the file
  * that dgb_mesh_write_msh writes for the same spec). */

@@ -8,7 +8,8 @@ set with oracle/ref_harness.cc into ``oracle/_ref/dgref_<variant>``.  Outputs go
 
 Compile-time configuration follows code/Makefile:147-156 (DEFINES) for the gamma-model
 multifluid build: USE_CPU, USE_DOUBLE, MULTIFLUID, GAMNCON, NO_MPI, N_Y=0, and
-N_F=4 (1D) / 5 (2D), D=1/2, DF=1, with the flux flag ROE, RUS or HLL.
+N_F=4 (1D) / 5 (2D), D=1/2, DF=1, with the flux flag ROE, RUS or HLL; and the same with one
+passive mass fraction (N_Y=1, N_F=5 / 6; variants *_y1).
 
 Out-of-tree additions (none of them touch reference arithmetic):
   * an empty ``gsl/gsl_integration.h`` (code/src/ic/init_cond.cc:10 includes it, never calls it);
@@ -41,6 +42,12 @@ VARIANTS = {
     "1d_hll": dict(dims="ONED", nf=4, d=1, flux="HLL"),
     "2d_roe": dict(dims="TWOD", nf=5, d=2, flux="ROE"),
     "2d_rus": dict(dims="TWOD", nf=5, d=2, flux="RUS"),
+    # one passive mass fraction (MASS=1 in code/Makefile: N_Y=1, one more field)
+    "1d_roe_y1": dict(dims="ONED", nf=5, d=1, flux="ROE", ny=1),
+    "1d_rus_y1": dict(dims="ONED", nf=5, d=1, flux="RUS", ny=1),
+    "1d_hll_y1": dict(dims="ONED", nf=5, d=1, flux="HLL", ny=1),
+    "2d_roe_y1": dict(dims="TWOD", nf=6, d=2, flux="ROE", ny=1),
+    "2d_rus_y1": dict(dims="TWOD", nf=6, d=2, flux="RUS", ny=1),
 }
 
 RK_SYM = ("_ZN2RK14RK_integrationEdiiiiiiiPdS0_R8LimitingbR9DG_SOLVERR12COMMUNICATORR7PRINTER"
@@ -49,7 +56,7 @@ RK_SYM = ("_ZN2RK14RK_integrationEdiiiiiiiPdS0_R8LimitingbR9DG_SOLVERR12COMMUNIC
 
 def defines(v: dict) -> list[str]:
     return ["-DHAVE_BLAS", "-DHAVE_LAPACK", "-DUSE_CPU", "-DHOME", "-DUSE_DOUBLE", "-DMULTIFLUID",
-            "-DGAMNCON", f"-D{v['flux']}", f"-D{v['dims']}", "-DNO_MPI", "-DN_Y=0", f"-DN_F={v['nf']}",
+            "-DGAMNCON", f"-D{v['flux']}", f"-D{v['dims']}", "-DNO_MPI", f"-DN_Y={v.get('ny', 0)}", f"-DN_F={v['nf']}",
             "-DNOERROR", "-DNOCONS", f"-DD={v['d']}", "-DDF=1"]
 
 

@@ -96,8 +96,10 @@ class Setup:
 # interface Riemann solvers (vectorised over face points); each returns (F, nc) with shape (N_F, n)
 # ---------------------------------------------------------------------------------------------
 
-def _twod_rusanov(rhoL, rhoR, vxL, vxR, vyL, vyR, EtL, EtR, alL, alR, nx, ny):
-    """twod_multifluid_rusanov, code/src/face_fluxes/twod_multifluid_fluxes.h:30-97 (GAMNCON)."""
+def _twod_rusanov(rhoL, rhoR, vxL, vxR, vyL, vyR, EtL, EtR, alL, alR, nx, ny, YL=(), YR=()):
+    """twod_multifluid_rusanov, code/src/face_fluxes/twod_multifluid_fluxes.h:30-97 (GAMNCON); the
+    mass fractions rho*Y_k (YL, YR) by the MACRO block at :89-94, whose dissipation term sits
+    outside the 1/2."""
     vnL = vxL * nx + vyL * ny
     vnR = vxR * nx + vyR * ny
     gL = 1.0 + 1.0 / alL
@@ -109,8 +111,10 @@ def _twod_rusanov(rhoL, rhoR, vxL, vxR, vyL, vyR, EtL, EtR, alL, alR, nx, ny):
     HL = (EtL + pL) / rhoL
     HR = (EtR + pR) / rhoR
     lam = np.maximum(np.abs(vnL) + aL, np.abs(vnR) + aR)
-    F = np.zeros((5,) + np.shape(rhoL))
+    F = np.zeros((5 + len(YL),) + np.shape(rhoL))
     nc = np.zeros_like(F)
+    for k in range(len(YL)):
+        F[5 + k] = 0.5 * (YL[k] * vnL + YR[k] * vnR) - lam * (YR[k] - YL[k])
     F[0] = 0.5 * (rhoL * vnL + rhoR * vnR - lam * (rhoR - rhoL))
     F[1] = 0.5 * ((rhoL * vnL * vxL + pL * nx) + (rhoR * vnR * vxR + pR * nx) - lam * (rhoR * vxR - rhoL * vxL))
     F[2] = 0.5 * ((rhoL * vnL * vyL + pL * ny) + (rhoR * vnR * vyR + pR * ny) - lam * (rhoR * vyR - rhoL * vyL))
@@ -120,9 +124,10 @@ def _twod_rusanov(rhoL, rhoR, vxL, vxR, vyL, vyR, EtL, EtR, alL, alR, nx, ny):
     return F, nc
 
 
-def _twod_roe(rhoL, rhoR, vxL, vxR, vyL, vyR, EtL, EtR, alL, alR, nx, ny):
+def _twod_roe(rhoL, rhoR, vxL, vxR, vyL, vyR, EtL, EtR, alL, alR, nx, ny, YL=(), YR=()):
     """twod_multifluid_roe, twod_multifluid_fluxes.h:151-342 (GAMNCON): Roe averages, wave
-    strengths dV0..dV4 and right eigenvectors R of the gamma-model system."""
+    strengths dV0..dV4 and right eigenvectors R of the gamma-model system; mass fractions by the
+    Roe-averaged Y and its wave strength (:307-319)."""
     tx, ty = -ny, nx
     vnL = vxL * nx + vyL * ny
     vnR = vxR * nx + vyR * ny
@@ -167,8 +172,13 @@ def _twod_roe(rhoL, rhoR, vxL, vxR, vyL, vyR, EtL, EtR, alL, alR, nx, ny):
         return ws[0] * dV[0] * R[0][c] + ws[1] * dV[1] * R[1][c] + ws[2] * dV[2] * R[2][c] + \
             ws[3] * dV[3] * R[3][c] + ws[4] * dV[4] * R[4][c]
 
-    F = np.zeros((5,) + np.shape(rhoL))
+    F = np.zeros((5 + len(YL),) + np.shape(rhoL))
     nc = np.zeros_like(F)
+    for k in range(len(YL)):
+        Y = (YL[k] / rhoL + RT * YR[k] / rhoR) / (1 + RT)
+        dVY = YR[k] - YL[k] - (dV[0] + dV[2] + dV[3]) * Y
+        F[5 + k] = 0.5 * (YL[k] * vnL + YR[k] * vnR) - 0.5 * (ws[0] * dV[0] * Y + ws[2] * dV[2] * Y + ws[1] * dVY * 1 +
+                                                                ws[3] * dV[3] * Y)
     F[0] = 0.5 * (rhoL * vnL + rhoR * vnR) - 0.5 * diss(0)
     F[1] = 0.5 * ((rhoL * vnL * vxL + pL * nx) + (rhoR * vnR * vxR + pR * nx)) - 0.5 * diss(1)
     F[2] = 0.5 * ((rhoL * vnL * vyL + pL * ny) + (rhoR * vnR * vyR + pR * ny)) - 0.5 * diss(2)
@@ -178,8 +188,9 @@ def _twod_roe(rhoL, rhoR, vxL, vxR, vyL, vyR, EtL, EtR, alL, alR, nx, ny):
     return F, nc
 
 
-def _oned_rusanov(rhoL, rhoR, vxL, vxR, EtL, EtR, alL, alR, nx):
-    """oned_multifluid_rusanov, code/src/face_fluxes/oned_multifluid_fluxes.h:30-94 (GAMNCON)."""
+def _oned_rusanov(rhoL, rhoR, vxL, vxR, EtL, EtR, alL, alR, nx, YL=(), YR=()):
+    """oned_multifluid_rusanov, code/src/face_fluxes/oned_multifluid_fluxes.h:30-94 (GAMNCON); mass
+    fractions by the MACRO block at :88-92 (dissipation outside the 1/2)."""
     gL = 1.0 + 1.0 / alL
     gR = 1.0 + 1.0 / alR
     pL = (gL - 1) * (EtL - 0.5 * rhoL * vxL * vxL)
@@ -187,8 +198,10 @@ def _oned_rusanov(rhoL, rhoR, vxL, vxR, EtL, EtR, alL, alR, nx):
     aL = np.sqrt((gL * pL) / rhoL)
     aR = np.sqrt((gR * pR) / rhoR)
     lam = np.maximum(np.abs(vxL) + aL, np.abs(vxR) + aR)
-    F = np.zeros((4,) + np.shape(rhoL))
+    F = np.zeros((4 + len(YL),) + np.shape(rhoL))
     nc = np.zeros_like(F)
+    for k in range(len(YL)):
+        F[4 + k] = 0.5 * (YL[k] * vxL + YR[k] * vxR) * nx - lam * (YR[k] - YL[k])
     F[0] = 0.5 * ((rhoL * vxL + rhoR * vxR) * nx - lam * (rhoR - rhoL))
     F[1] = 0.5 * ((rhoL * vxL * vxL + pL + rhoR * vxR * vxR + pR) * nx - lam * (rhoR * vxR - rhoL * vxL))
     F[2] = 0.5 * (((EtL + pL) * vxL + (EtR + pR) * vxR) * nx - lam * (EtR - EtL))
@@ -202,7 +215,7 @@ def _fhll(UL, SL, FL, UR, SR, FR):
     return (SR * FL - SL * FR + SL * SR * (UR - UL)) / np.abs(SR - SL)
 
 
-def _oned_hll(rhoL, rhoR, vxL, vxR, EtL, EtR, alL, alR, nx):
+def _oned_hll(rhoL, rhoR, vxL, vxR, EtL, EtR, alL, alR, nx, YL=(), YR=()):
     """oned_multifluid_hll, oned_multifluid_fluxes.h:117-226 (GAMNCON, wave-speed estimate Toro
     10.48).  As in the reference, the momentum row's HLL jump uses the velocities vxL, vxR
     (oned_multifluid_fluxes.h:196), and a face with SL == 0 or SR == 0 keeps a zero flux."""
@@ -224,19 +237,25 @@ def _oned_hll(rhoL, rhoR, vxL, vxR, EtL, EtR, alL, alR, nx):
                _fhll(alL, SL, 0.0, alR, SR, 0.0) - 0.5 * np.abs(SR + SL) / np.abs(SR - SL) * vncabs]
     left = [fL[0], fL[1], fL[2], -0.5 * vncabs]
     right = [fR[0], fR[1], fR[2], 0.5 * vncabs]
+    for k in range(len(YL)):  # mass fractions (oned_multifluid_fluxes.h:186-219)
+        fYL, fYR = YL[k] * vxL * nx, YR[k] * vxR * nx
+        with np.errstate(divide="ignore", invalid="ignore"):
+            mid.append(_fhll(YL[k], SL, fYL, YR[k], SR, fYR))
+        left.append(fYL)
+        right.append(fYR)
     cL = SL > 0
     cM = (SL < 0) & (SR > 0)
     cR = (SR < 0) & ~cL & ~cM
-    F = np.zeros((4,) + np.shape(rhoL))
+    F = np.zeros((4 + len(YL),) + np.shape(rhoL))
     nc = np.zeros_like(F)
-    for k in range(4):
+    for k in range(4 + len(YL)):
         F[k] = np.where(cL, left[k], np.where(cM, mid[k], np.where(cR, right[k], 0.0)))
     nc[3] = -0.5 * vnc
     return F, nc
 
 
-def _oned_roe(rhoL, rhoR, vxL, vxR, EtL, EtR, alL, alR, nx):
-    """oned_multifluid_roe, oned_multifluid_fluxes.h:237-382 (GAMNCON)."""
+def _oned_roe(rhoL, rhoR, vxL, vxR, EtL, EtR, alL, alR, nx, YL=(), YR=()):
+    """oned_multifluid_roe, oned_multifluid_fluxes.h:237-382 (GAMNCON); mass fractions :358-370."""
     gL = 1.0 + 1.0 / alL
     gR = 1.0 + 1.0 / alR
     pL = (gL - 1) * (EtL - 0.5 * rhoL * vxL * vxL)
@@ -265,8 +284,13 @@ def _oned_roe(rhoL, rhoR, vxL, vxR, EtL, EtR, alL, alR, nx):
     def diss(c):
         return ws[0] * dV[0] * R[0][c] + ws[1] * dV[1] * R[1][c] + ws[2] * dV[2] * R[2][c] + ws[3] * dV[3] * R[3][c]
 
-    F = np.zeros((4,) + np.shape(rhoL))
+    F = np.zeros((4 + len(YL),) + np.shape(rhoL))
     nc = np.zeros_like(F)
+    for k in range(len(YL)):
+        Y = (YL[k] / rhoL + RT * YR[k] / rhoR) / (1 + RT)
+        dVY = YR[k] - YL[k] - (dV[0] + dV[1] + dV[2]) * Y
+        F[4 + k] = 0.5 * (YL[k] * vxL + YR[k] * vxR) * nx - 0.5 * (ws[0] * dV[0] * Y + ws[1] * dV[1] * Y +
+                                                                     ws[1] * dVY * 1 + ws[2] * dV[2] * Y)
     F[0] = 0.5 * (rhoL * vxL + rhoR * vxR) * nx - 0.5 * diss(0)
     F[1] = 0.5 * (rhoL * vxL * vxL + pL + rhoR * vxR * vxR + pR) * nx - 0.5 * diss(1)
     F[2] = 0.5 * ((EtL + pL) * vxL + (EtR + pR) * vxR) * nx - 0.5 * diss(2)
@@ -317,6 +341,8 @@ def _evaluate_sf(S: Setup, Ug, dUg, invJac):
         f[:, 1, :, 0] = rho * u * u + p
         f[:, 2, :, 0] = (Et + p) * u
         s[:, 3] = -u * dUg[:, 3, :, 0] * invJac.reshape(NE, NG)
+        for k in range(4, NF):  # mass fractions: flux rho*Y_k u (physics.cu:130-134)
+            f[:, k, :, 0] = Ug[:, k] * u
         return s, f
     u = Ug[:, 1] / rho
     v = Ug[:, 2] / rho
@@ -339,6 +365,9 @@ def _evaluate_sf(S: Setup, Ug, dUg, invJac):
     for al in range(D):
         vg += -u * dUg[:, 4, :, al] * iJ[:, :, 0, al] - v * dUg[:, 4, :, al] * iJ[:, :, 1, al]
     s[:, 4] = vg
+    for k in range(5, NF):  # mass fractions: flux rho*Y_k (u, v) (physics.cu:293-298)
+        f[:, k, :, 0] = Ug[:, k] * u
+        f[:, k, :, 1] = Ug[:, k] * v
     return s, f
 
 
@@ -350,12 +379,14 @@ def _evaluate_q(S: Setup, UgF):
     nx = n[:, 0][:, None]
     if S.D == 1:
         fn = {"rusanov": _oned_rusanov, "hll": _oned_hll, "roe": _oned_roe}[S.flux]
-        F, nc = fn(L[:, 0], R[:, 0], L[:, 1] / L[:, 0], R[:, 1] / R[:, 0], L[:, 2], R[:, 2], L[:, 3], R[:, 3], nx)
+        F, nc = fn(L[:, 0], R[:, 0], L[:, 1] / L[:, 0], R[:, 1] / R[:, 0], L[:, 2], R[:, 2], L[:, 3], R[:, 3], nx,
+                   [L[:, k] for k in range(4, S.N_F)], [R[:, k] for k in range(4, S.N_F)])
     else:
         ny = n[:, 1][:, None]
         fn = {"rusanov": _twod_rusanov, "roe": _twod_roe}[S.flux]
         F, nc = fn(L[:, 0], R[:, 0], L[:, 1] / L[:, 0], R[:, 1] / R[:, 0], L[:, 2] / L[:, 0], R[:, 2] / R[:, 0],
-                   L[:, 3], R[:, 3], L[:, 4], R[:, 4], nx, ny)
+                   L[:, 3], R[:, 3], L[:, 4], R[:, 4], nx, ny, [L[:, k] for k in range(5, S.N_F)],
+                   [R[:, k] for k in range(5, S.N_F)])
     F = np.moveaxis(F, 0, 1)    # (M_T, N_F, M_G)
     nc = np.moveaxis(nc, 0, 1)
     q = np.empty_like(UgF)
@@ -616,6 +647,8 @@ def _m2(S: Setup, U: np.ndarray) -> np.ndarray:
         E = _apply(M2L, _reconstruct_energy(rhoe, K, EM), Ns)
         out = np.empty_like(V)
         out[:, 0], out[:, 1], out[:, 2], out[:, 3] = rho, rhou, E, gam
+        for k in range(4, NF):  # mass fractions like the density (limiting.cc:184-193)
+            out[:, k] = _apply(M2L, lim(V[:, k]), Ns)
         return out.reshape(-1)
     n1 = S.order + 1
     L2MX, MX2L, L2MY, MY2L = a["Lag2MonoX"], a["MonoX2Lag"], a["Lag2MonoY"], a["MonoY2Lag"]
@@ -626,7 +659,9 @@ def _m2(S: Setup, U: np.ndarray) -> np.ndarray:
     # x slices
     lims = {}
     nodal = {}
-    for name, x in (("rho", V[:, 0]), ("rhou", V[:, 1]), ("rhov", V[:, 2]), ("g", V[:, 4])):
+    ynames = [f"y{k}" for k in range(5, NF)]  # mass fractions like the density (limiting.cc:323-331, 396-404)
+    for name, x in (("rho", V[:, 0]), ("rhou", V[:, 1]), ("rhov", V[:, 2]), ("g", V[:, 4])) + tuple(
+            (f"y{k}", V[:, k]) for k in range(5, NF)):
         lims[name] = hrl1d(S, mono(L2MX, x), 0, False)
         nodal[name] = _apply(MX2L, lims[name], Ns)
     rho, ru, rv = V[:, 0], V[:, 1], V[:, 2]
@@ -637,7 +672,7 @@ def _m2(S: Setup, U: np.ndarray) -> np.ndarray:
     rhoe = _internal_energy(pL, lims["g"])
     E = _apply(MX2L, _reconstruct_energy(rhoe, K, mono(L2MX, V[:, 3])), Ns)
     # y slices of the x-limited fields
-    for name in ("rho", "rhou", "rhov", "g"):
+    for name in ("rho", "rhou", "rhov", "g", *ynames):
         lims[name] = hrl1d(S, mono(L2MY, nodal[name]), 2, False)
         nodal[name] = _apply(MY2L, lims[name], Ns)
     pL = hrl1d(S, mono(L2MY, pres), 2, False)
@@ -646,6 +681,8 @@ def _m2(S: Setup, U: np.ndarray) -> np.ndarray:
     E = _apply(MY2L, _reconstruct_energy(rhoe, K, mono(L2MY, E)), Ns)
     out = np.empty_like(V)
     out[:, 0], out[:, 1], out[:, 2], out[:, 3], out[:, 4] = nodal["rho"], nodal["rhou"], nodal["rhov"], E, nodal["g"]
+    for k in range(5, NF):
+        out[:, k] = nodal[f"y{k}"]
     return out.reshape(-1)
 
 

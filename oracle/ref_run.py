@@ -22,12 +22,13 @@ FLUX_TAG = {"rusanov": "rus", "rus": "rus", "roe": "roe", "hll": "hll"}
 BC_TAG = {"periodic": 1, "transmissive": 2, "reflective": 3, "frozen": 4}
 
 
-def binary(dim: int, flux: str) -> Path:
-    return REF_DIR / f"dgref_{dim}d_{FLUX_TAG[flux.lower()]}"
+def binary(dim: int, flux: str, n_mass: int = 0) -> Path:
+    """The reference build for (dimension, flux) with N_Y = n_mass (0 or 1) mass fractions."""
+    return REF_DIR / (f"dgref_{dim}d_{FLUX_TAG[flux.lower()]}" + (f"_y{n_mass}" if n_mass else ""))
 
 
-def available(dim: int = 2, flux: str = "rusanov") -> bool:
-    return binary(dim, flux).exists()
+def available(dim: int = 2, flux: str = "rusanov", n_mass: int = 0) -> bool:
+    return binary(dim, flux, n_mass).exists()
 
 
 @dataclass
@@ -46,6 +47,7 @@ class RefCase:
     cfl: float = -1.0
     output_times: tuple = (0.0, 1e-3)
     thresholds: tuple = ()
+    n_mass: int = 0
     workdir: Path | None = None
     _tmp: object = field(default=None, repr=False)
 
@@ -76,7 +78,7 @@ class RefCase:
 
     def run(self, cmd: str, U: np.ndarray | None = None, dt: float = 0.0, nsteps: int = 1,
             repeat: int = 1, timeout: float = 600.0, extra_env: dict | None = None) -> tuple[np.ndarray, str]:
-        exe = binary(self.dim, self.flux)
+        exe = binary(self.dim, self.flux, self.n_mass)
         if not exe.exists():
             raise FileNotFoundError(f"{exe} missing: run python oracle/build_ref.py")
         args = [str(exe), "-d", "deck.inp", "--cmd", cmd, "--dt", repr(float(dt)), "--nsteps", str(nsteps),

@@ -14,7 +14,7 @@ when the case has no limiter).  The reference binaries of oracle/build_ref.py
 plus the reference's setup arrays (phi, ..., Minv, neighbours) for the host-setup pins.
 
 Run from the repository root after `python oracle/build_ref.py` and `python -m dg_b200.build`:
-    python tests/golden/make_golden.py
+    python tests/golden/make_golden.py [name ...]     (no names: every fixture)
 """
 from __future__ import annotations
 
@@ -84,6 +84,20 @@ CASES = [
          flux="rusanov", limiter="pri", ic="tube_noise", cfl=0.3, dt=2e-4, nsteps=4, thresholds=(0.001,)),
     dict(name="s1_p2_rus_prl", dim=1, order=2, nx=30, ny=1, dom=(0, 1, 0, 1), bc=("transmissive",) * 2,
          flux="rusanov", limiter="prl", ic="tube_noise", cfl=0.3, dt=2e-4, nsteps=4),
+    # one passive mass fraction (the reference built with MASS=1: N_Y = 1)
+    dict(name="y1_p2_roe_m2l", dim=1, order=2, nx=24, ny=1, dom=(0, 1, 0, 1), bc=("transmissive",) * 2,
+         flux="roe", limiter="m2l", ic="tube_noise", cfl=0.4, dt=4e-4, nsteps=5, n_mass=1),
+    dict(name="y1_p3_hll_hrl_wall", dim=1, order=3, nx=20, ny=1, dom=(0, 1, 0, 1), bc=("reflective",) * 2,
+         flux="hll", limiter="hrl", ic="tube_noise", cfl=0.2, dt=2e-4, nsteps=5, n_mass=1),
+    dict(name="y1_p1_rus_m2l_periodic", dim=1, order=1, nx=30, ny=1, dom=(0, 1, 0, 1), bc=("periodic",) * 2,
+         flux="rusanov", limiter="m2l", ic="riemann", cfl=0.4, dt=4e-4, nsteps=5, n_mass=1),
+    dict(name="y2_p2_rus_m2l_walls", dim=2, order=2, nx=32, ny=8, dom=(0, 2, 0, 1),
+         bc=("reflective", "transmissive", "reflective", "transmissive"), flux="rusanov", limiter="m2l",
+         ic="shock_bubble", cfl=0.3, dt=5e-4, nsteps=4, n_mass=1),
+    dict(name="y2_p2_roe_hrl_periodic", dim=2, order=2, nx=32, ny=8, dom=(0, 1, 0, 1), bc=("periodic",) * 4,
+         flux="roe", limiter="hrl", ic="quadrants", cfl=0.3, dt=5e-4, nsteps=4, n_mass=1),
+    dict(name="y2_p1_roe_m2l_box", dim=2, order=1, nx=32, ny=4, dom=(0, 1, 0, 1), bc=("reflective",) * 4,
+         flux="roe", limiter="m2l", ic="quadrants", cfl=0.3, dt=5e-4, nsteps=4, n_mass=1),
 ]
 
 
@@ -105,10 +119,11 @@ def make_case(c: dict, seed: int) -> dict:
     x0, x1, y0, y1 = c["dom"]
     bc = tuple(c["bc"]) + ("transmissive",) * (4 - len(c["bc"]))
     th = tuple(c.get("thresholds", ()))
+    nm = c.get("n_mass", 0)
     ref = RefCase(c["dim"], c["order"], c["nx"], c["ny"], x0, x1, y0, y1, bc, c["flux"], c["limiter"],
-                  thresholds=th)
+                  thresholds=th, n_mass=nm)
     prob = dgb.Problem.structured(c["dim"], c["order"], c["nx"], c["ny"], x0, x1, y0, y1, bc, flux=c["flux"],
-                                  limiter=c["limiter"], cfl=c["cfl"], thresholds=th)
+                                  limiter=c["limiter"], cfl=c["cfl"], thresholds=th, n_mass=nm)
     Uraw = perturbed_state(prob, c["ic"], seed)
     out = dict(Uraw=Uraw)
     if th:
@@ -199,7 +214,14 @@ def make_tube_fixture() -> dict:
     return out
 
 
-def main() -> int:
+def main(argv=None) -> int:
+    only = set((argv if argv is not None else sys.argv[1:]))
+    if only:  # regenerate the named fixtures only
+        for k, c in enumerate(CASES):
+            if c["name"] in only:
+                np.savez_compressed(OUT / f"{c['name']}.npz", **make_case(c, seed=100 + k))
+                print(f"wrote {c['name']}.npz")
+        return 0
     np.savez_compressed(OUT / f"{TUBE['name']}.npz", **make_tube_fixture())
     print(f"wrote {TUBE['name']}.npz")
     np.savez_compressed(OUT / f"{DRIVER['name']}.npz", **make_driver_fixture())

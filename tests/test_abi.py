@@ -24,7 +24,7 @@ def test_library_exports_every_declared_symbol():
     missing = [n for n in declared() if not hasattr(lib, n)]
     assert not missing, missing
     assert sorted(_ffi.EXPORTS) == declared()
-    assert lib.dgb_abi_version() == 1
+    assert lib.dgb_abi_version() == 2
 
 
 def test_device_calls_fail_loudly_without_gpu():
