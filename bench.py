@@ -16,6 +16,7 @@ device-side CFL step.  DOF = N_E * N_s * N_F = 5,898,240.
   cpu_baseline  the reference CPU build (oracle/_ref, compiled from the reference sources) on a
              bounded sample of the same workload, one process on one core
   forms      plain FP64, mixed and mixed + learned indicator at equal L1 error (same protocol)
+  mass_fraction  the workload with one passive mass fraction (6 fields): time per step
   tube_1d    the 1D two-fluid shock tube (1000 elements, p=2, Roe, RK4, CFL 0.4, 2000 steps): device
              time, distance from the reference's own run, the reference CPU build's time
   learned_deploy  the learned indicator on a 1024x1024 four-quadrant problem: FP64 / mixed / mixed +
@@ -505,6 +506,29 @@ def learned_deploy(dgb, dev, timed=20, warmup=3, steps=DEPLOY_STEPS):
     return out
 
 
+def mass_fraction(dgb, dev, base_ms, steps=20, warmup=3):
+    """The benchmark workload with one passive mass fraction marking the bubble (rho Y = rho inside;
+    6 fields): device time per step against the plain workload's (same protocol, L2 flushed by
+    the 47 MB+ state being read once per stage; no extra flush here), and the Y total carried."""
+    x0, x1, y0, y1 = DOMAIN
+    prob = dgb.Problem.structured(2, ORDER, NX, NY, x0, x1, y0, y1, BC, flux="rusanov", limiter="m2l", cfl=CFL,
+                                  n_mass=1)
+    info = prob.info
+    dof = info.n_elem * info.n_s * info.n_fields
+    s = dgb.DGSolver(prob, device=dev)
+    s.set_state(s.limit(prob.init_state("shock_bubble", seed=SEED)))
+    c0 = s.conservation()
+    s.advance(warmup, 0.0, scheme=dgb.SSPRK3)
+    s.advance(steps, 0.0, scheme=dgb.SSPRK3)
+    ms, _ = s.last_timing()
+    c1 = s.conservation()
+    s.close()
+    return {"workload": "2D shock-bubble 512x256, p=2, Rusanov, m2l, SSP-RK3, CFL 0.3, one mass fraction (6 fields)",
+            "dof": dof, "value": dof * STAGES_PER_STEP * steps / (ms / 1e3), "unit": UNIT,
+            "ms_per_step": ms / steps, "ms_per_step_without": base_ms,
+            "rhoY_total_start_end": [float(c0[5]), float(c1[5])]}
+
+
 P3_NX, P3_NY, P3_STEPS = 2048, 1024, 300
 
 
@@ -758,6 +782,9 @@ def main(argv=None) -> int:
     deploy = None
     if ws == 1 and not args.no_deploy and (args.nx, args.ny) == (NX, NY):
         deploy = learned_deploy(dgb, dev)
+    mf = None
+    if ws == 1 and not args.no_tube and (args.nx, args.ny) == (NX, NY):
+        mf = mass_fraction(dgb, dev, dev_ms / args.steps)
     tube = None
     if ws == 1 and not args.no_tube and (args.nx, args.ny) == (NX, NY):
         tube = tube_1d(dgb, dev, with_reference=rank == 0 and not args.no_cpu_baseline)
@@ -782,7 +809,7 @@ def main(argv=None) -> int:
                 "kernel_ms_per_step": {"residual": res_ms / args.steps, "limiter": lim_ms / args.steps,
                                        "dt": dt_ms / args.steps},
                 "cpu_baseline": cpu, "clocks": clocks, "gpu_launches": launches, "forms": forms,
-                "ensemble": ens, "mixed_p3": p3, "learned_deploy": deploy, "tube_1d": tube}
+                "ensemble": ens, "mixed_p3": p3, "learned_deploy": deploy, "tube_1d": tube, "mass_fraction": mf}
         print(json.dumps(line))
     solver.close()
     if ws > 1:

@@ -1,8 +1,9 @@
 """CUDA path (through the C ABI) against the numpy oracle at sizes and seeds the golden fixtures
 do not cover: ragged grids (extents not multiples of the 32 x 4 element tile), tile-aligned grids
 (tiled kernels), p = 1..3, all fluxes, both limiters, walls / periodic / transmissive
-boundaries, the 1D shock-tube workload (1000 elements, p=2, Roe, m2l, RK4) and the 2D
-shock-bubble workload at its full size (512 x 256 elements, p=2, Rusanov, m2l, SSP-RK3).
+boundaries, one passive mass fraction, the 1D shock-tube workload (1000 elements, p=2, Roe, m2l,
+RK4) and the 2D shock-bubble workload at its full size (512 x 256 elements, p=2, Rusanov, m2l,
+SSP-RK3).
 
 Tolerances: 1e-12 relative per operator (residual, limiter, Minv solve, CFL step), 1e-10
 relative after a few RK steps, and 1e-10 in relative L1 density after 100 steps.
@@ -29,6 +30,12 @@ CASES = [
     ("1d_p3_hll_hrl_walls", 1, 3, 301, 1, ("reflective",) * 2, "hll", "hrl", "tube_noise", 0.15),
     ("1d_p1_rus_m2l_periodic", 1, 1, 257, 1, ("periodic",) * 2, "rusanov", "m2l", "tube_noise"),
     ("1d_p2_roe_none", 1, 2, 123, 1, ("transmissive",) * 2, "roe", "none", "tube_noise"),
+    # one passive mass fraction (last entry: n_mass)
+    ("2d_p2_roe_m2l_tiled_walls_y1", 2, 2, 64, 16, WALLS, "roe", "m2l", "shock_bubble", 0.3, 1),
+    ("2d_p3_rus_hrl_tiled_periodic_y1", 2, 3, 32, 8, ("periodic",) * 4, "rusanov", "hrl", "quadrants", 0.3, 1),
+    ("2d_p1_rus_m2l_tiled_box_y1", 2, 1, 64, 12, ("reflective",) * 4, "rusanov", "m2l", "quadrants", 0.3, 1),
+    ("1d_p2_rus_m2l_y1", 1, 2, 201, 1, ("transmissive",) * 2, "rusanov", "m2l", "tube_noise", 0.3, 1),
+    ("1d_p3_hll_hrl_walls_y1", 1, 3, 97, 1, ("reflective",) * 2, "hll", "hrl", "riemann", 0.15, 1),
 ]
 
 
@@ -36,8 +43,10 @@ def make(case, seed):
     import dg_b200 as dgb
     _, dim, order, nx, ny, bc, flux, limiter, ic = case[:9]
     cfl = case[9] if len(case) > 9 else 0.3
+    n_mass = case[10] if len(case) > 10 else 0
     x1 = 2.0 if dim == 2 and ic == "shock_bubble" else 1.0
-    prob = dgb.Problem.structured(dim, order, nx, ny, 0.0, x1, 0.0, 1.0, bc, flux=flux, limiter=limiter, cfl=cfl)
+    prob = dgb.Problem.structured(dim, order, nx, ny, 0.0, x1, 0.0, 1.0, bc, flux=flux, limiter=limiter, cfl=cfl,
+                                  n_mass=n_mass)
     S = O.Setup.from_problem(prob)
     U0 = O.limit(S, perturbed_state(prob, ic, seed))
     return prob, S, U0
@@ -113,6 +122,58 @@ def test_shock_bubble_small_100_steps_l1_density():
     Uo = O.ssprk3_steps(S, U0, 0.0, 100)
     i = prob.info
     assert l1_density_error(Ug, Uo, i.n_elem, i.n_fields, i.n_s) < 1e-10
+
+
+def test_shock_bubble_mass_fraction_100_steps_l1():
+    """The 2D shock-bubble with the bubble marked by a mass fraction (rho Y = rho inside), 64 x 32
+    grid, p=2, Roe, m2l, SSP-RK3, CFL step, 100 steps: relative L1 of density and of rho Y."""
+    import dg_b200 as dgb
+    prob = dgb.Problem.structured(2, 2, 64, 32, 0.0, 2.0, 0.0, 1.0, WALLS, flux="roe", limiter="m2l", cfl=0.3,
+                                  n_mass=1)
+    S = O.Setup.from_problem(prob)
+    U0 = O.limit(S, prob.init_state("shock_bubble", seed=7))
+    s = dgb.DGSolver(prob)
+    try:
+        s.set_state(U0)
+        s.advance(100, 0.0, scheme=dgb.SSPRK3)
+        Ug = s.get_state()
+    finally:
+        s.close()
+    Uo = O.ssprk3_steps(S, U0, 0.0, 100)
+    i = prob.info
+    assert i.n_fields == 6
+    assert l1_density_error(Ug, Uo, i.n_elem, i.n_fields, i.n_s) < 1e-10
+    A = Ug.reshape(i.n_elem, i.n_fields, i.n_s)[:, 5]
+    B = Uo.reshape(i.n_elem, i.n_fields, i.n_s)[:, 5]
+    assert np.abs(A - B).sum() / np.abs(B).sum() < 1e-10
+    # the marker is carried, not created: its total changes only through the open x boundaries
+    assert B.sum() > 0
+
+
+def test_mass_fraction_configurations_outside_the_device_path_are_rejected():
+    import dg_b200 as dgb
+    bad = [dict(dim=2, order=2, nx=40, ny=8, limiter="m2l"),       # 2D grid not tile-aligned
+           dict(dim=1, order=2, nx=50, ny=1, limiter="m2i", thresholds=(0.05,)),  # sensor-gated limiter
+           dict(dim=1, order=2, nx=50, ny=1, limiter="prl")]
+    for kw in bad:
+        th = kw.pop("thresholds", ())
+        prob = dgb.Problem.structured(kw["dim"], kw["order"], kw["nx"], kw["ny"], flux="rusanov", limiter=kw["limiter"],
+                                      cfl=0.3, thresholds=th, n_mass=1)
+        with pytest.raises(dgb.DGBError) as e:
+            dgb.DGSolver(prob)
+        assert e.value.code == 4
+    prob = dgb.Problem.structured(2, 2, 32, 8, flux="rusanov", limiter="m2l", cfl=0.3, n_mass=2)
+    with pytest.raises(dgb.DGBError):
+        dgb.DGSolver(prob)
+    prob = dgb.Problem.structured(2, 2, 32, 8, flux="rusanov", limiter="m2l", cfl=0.3, n_mass=1)
+    s = dgb.DGSolver(prob)
+    try:
+        with pytest.raises(dgb.DGBError):
+            s.set_form("mixed")
+        with pytest.raises(dgb.DGBError):
+            dgb.DGBatch([s])
+    finally:
+        s.close()
 
 
 def test_shock_bubble_full_size_one_step():

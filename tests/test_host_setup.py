@@ -80,3 +80,35 @@ def test_pos_roundtrip(tmp_path):
     V, t = p.read_pos(3, tmp_path)
     assert t == 0.125
     assert np.abs(U - V).max() <= 1e-14 * np.abs(U).max()
+
+
+def test_mass_fraction_state_and_pos_round_trip(tmp_path):
+    """One passive mass fraction: N_F grows by one, the initial states carry rho Y = rho times the
+    region marker, and the .pos output (field y0 = Y, printer.cc:65-71) reads back exactly."""
+    import dg_b200 as dgb
+    prob = dgb.Problem.structured(2, 2, 8, 4, 0.0, 2.0, 0.0, 1.0, ("transmissive",) * 4, flux="roe", limiter="m2l",
+                                  cfl=0.3, n_mass=1)
+    i = prob.info
+    assert i.n_fields == 6
+    U = prob.init_state("shock_bubble", seed=3)
+    V = U.reshape(i.n_elem, i.n_fields, i.n_s)
+    Y = V[:, 5] / V[:, 0]
+    assert set(np.unique(Y)) <= {0.0, 1.0} and Y.max() == 1.0 and Y.min() == 0.0
+    prob.write_pos(U, 7, 0.25, tmp_path)
+    assert (tmp_path / "y00000000007.pos").exists()
+    assert '"Y0"' in (tmp_path / "y00000000007.pos").read_text()
+    U2, t = prob.read_pos(7, tmp_path)
+    assert t == 0.25
+    assert np.abs(U2 - U).max() <= 1e-15 * np.abs(U).max()
+
+
+def test_deck_mass_option(tmp_path):
+    """MASS=1 in the deck's "#Make options" block gives one mass fraction."""
+    import dg_b200 as dgb
+    dgb.write_msh(tmp_path / "mesh.msh", 1, 2, 20, 1, 0.0, 1.0, 0.0, 1.0, ("transmissive",) * 4)
+    (tmp_path / "deck.inp").write_text(
+        "#Make options\nFLUX=RUS\nMASS=1\n#Code options\n#time integration\nrk4\n#output time step size\n0.1\n"
+        "#final time\n0.1\n#Courant-Friedrichs-Lewy condition\n0.4\n#order\n2\n#mesh file\nmesh.msh\nlin\n"
+        "#limiter\nm2l\n#initial condition\nsodtube\n")
+    prob = dgb.Problem.from_deck(tmp_path / "deck.inp")
+    assert prob.info.n_fields == 5
