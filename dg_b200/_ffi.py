@@ -28,7 +28,7 @@ EXPORTS = [
     "dgb_sensors", "dgb_set_form", "dgb_mlp_param_count", "dgb_indicator_features", "dgb_indicator_labels",
     "dgb_mlp_forward", "dgb_mlp_backward", "dgb_mlp_adam", "dgb_set_indicator", "dgb_indicator_scores",
     "dgb_cfl_dt", "dgb_batch_create", "dgb_batch_destroy", "dgb_batch_n_classes", "dgb_batch_class_info",
-    "dgb_batch_autotune", "dgb_batch_set_tuning", "dgb_batch_advance", "dgb_batch_case_stats", "dgb_batch_last_timing",
+    "dgb_batch_autotune", "dgb_batch_set_tuning", "dgb_batch_advance", "dgb_problem_error_norms", "dgb_batch_case_stats", "dgb_batch_last_timing",
 ]
 
 
@@ -48,7 +48,7 @@ class Info(C.Structure):
                 "dim order n_fields n_elem n_s n_g n_ifaces m_s m_g n_n n_reflective cartesian "
                 "gpu_supported flux limiter nx ny".split()] + \
                [(n, C.c_double) for n in "cfl dx_min cfl_scaled final_time".split()] + \
-               [("n_output_times", C.c_int)]
+               [("n_output_times", C.c_int), ("error_output", C.c_int)]
 
 
 class DGBError(RuntimeError):
@@ -82,6 +82,7 @@ def lib() -> C.CDLL:
         "dgb_problem_init_state": [vp, cp, dp, ip, C.c_uint64, dp],
         "dgb_write_pos": [vp, dp, ip, C.c_double, cp],
         "dgb_read_pos": [vp, ip, cp, dp, dp],
+        "dgb_problem_error_norms": [vp, dp, dp, dp],
         "dgb_create": [vp, ip, C.POINTER(vp)],
         "dgb_set_state": [vp, dp],
         "dgb_get_state": [vp, dp],

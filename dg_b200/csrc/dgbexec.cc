@@ -7,7 +7,8 @@
 //     on the final time (rk.cc:134-149, 207-228);
 //   * CFL < 0: a fixed step of output_times[1] - output_times[0], clipped to the final time, and
 //     no output (rk.cc:136-139);
-//   * output in the reference's .pos format (one file per field and output step) in --out.
+//   * output in the reference's .pos format (one file per field and output step) in --out;
+//   * with "#Make options" ERRR=ERROR, error.dat (main.cc:909-1038) in --out after the run.
 // A NaN or too small time step ends the run with exit status 1 and the reference's message.
 //
 // usage: dgbexec [-d deck.inp] [--out DIR] [--scheme rk4|ssprk3] [--form fp64|mixed] [--device N]
@@ -118,6 +119,23 @@ int main(int argc, char** argv) {
       ++count;
       if ((size_t)count < times.size()) tout = times[count];
     }
+  }
+  if (info.error_output) {
+    // the ERROR block of the reference driver (main.cc:909-1038): final state against the deck's
+    // initial condition re-evaluated, written as error.dat (dx, then L1 / L2 / Linf per field)
+    std::vector<double> Uex(n), err(1 + 3 * (size_t)info.n_fields);
+    if (dgb_get_state(ctx, U.data())) return fail("state");
+    if (dgb_problem_init_state(prob, nullptr, nullptr, 0, 0, Uex.data())) return fail("initial condition");
+    if (dgb_problem_error_norms(prob, U.data(), Uex.data(), err.data())) return fail("error norms");
+    const std::string fn = out + "/error.dat";
+    FILE* f = std::fopen(fn.c_str(), "w");
+    if (!f) { std::fprintf(stderr, "dgbexec: cannot write %s\n", fn.c_str()); return 2; }
+    for (int row = 0; row < 3; ++row) {
+      std::fprintf(f, "%12.7f\t", err[0]);
+      for (int fc = 0; fc < info.n_fields; ++fc) std::fprintf(f, "%20.16E\t", err[1 + row * info.n_fields + fc]);
+      std::fprintf(f, "\n");
+    }
+    std::fclose(f);
   }
   dgb_destroy(ctx);
   dgb_problem_destroy(prob);

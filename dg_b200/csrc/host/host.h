@@ -61,6 +61,7 @@ struct Problem {
   int D = 1, p = 1, N_F = 4;
   int N_Y = 0;                        // passive mass fractions rho*Y_k, fields D+3 .. N_F-1
   int flux = 2, limiter = 0;
+  bool error_output = false;          // deck "#Make options" ERRR=ERROR: error.dat after the run
   double cfl = -1.0;
   std::vector<double> thresholds;
   std::vector<double> output_times;
@@ -121,6 +122,8 @@ Status build_problem(Mesh&& mesh, int dim, int order, const std::string& elem_ki
 Status init_state(const Problem& P, const std::string& ic, const std::vector<double>& params, uint64_t seed,
                   double* U);
 Status write_pos(const Problem& P, const double* U, int step, double time, const std::string& dir);
+// the ERROR diagnostic of the reference driver: [dx, L1(N_F), L2(N_F), Linf(N_F)]
+Status error_norms(const Problem& P, const double* U, const double* Uexact, double* out);
 Status read_pos(const Problem& P, int step, const std::string& dir, double& time, double* U);
 
 }  // namespace dgb

@@ -86,6 +86,8 @@ extern "C" int dgb_problem_from_deck(const char* deck_path, dgb_problem** out) {
                           d.thresholds, outt, tf, pr->P, n_mass);
   if (!st.ok()) { delete pr; return set_error(st.code, st.msg); }
   pr->P.deck_dir = dir;
+  mo = d.make_options.find("ERRR");
+  pr->P.error_output = mo != d.make_options.end() && mo->second == "ERROR";
   pr->P.deck_ic = d.ic;
   pr->P.deck_ic_inputs = d.ic_inputs;
   *out = pr;
@@ -151,6 +153,7 @@ extern "C" int dgb_problem_info(const dgb_problem* p, dgb_info* o) {
   o->cfl = P.cfl; o->dx_min = P.dx_min; o->cfl_scaled = P.cfl_scaled;
   o->final_time = P.final_time;
   o->n_output_times = (int)P.output_times.size();
+  o->error_output = P.error_output ? 1 : 0;
   return DGB_OK;
 }
 
@@ -231,3 +234,10 @@ extern "C" int dgb_read_pos(const dgb_problem* p, int step, const char* dir, dou
 
 // access for the device layer
 const dgb::Problem& dgb_problem_ref(const dgb_problem* p) { return p->P; }
+
+extern "C" int dgb_problem_error_norms(const dgb_problem* p, const double* U, const double* U_exact, double* out) {
+  if (!p || !U || !U_exact || !out) return set_error(DGB_ERR_ARG, "null argument");
+  dgb::Status st = dgb::error_norms(p->P, U, U_exact, out);
+  if (!st.ok()) return set_error(st.code, st.msg);
+  return DGB_OK;
+}

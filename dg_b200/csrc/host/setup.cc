@@ -620,6 +620,29 @@ Status init_state(const Problem& P, const std::string& ic, const std::vector<dou
     }
     return Status();
   }
+  if (ic == "sinegam") {
+    // init_dg_sinegam_multifluid (code/src/ic/init_cond.cc:551-618): uniform velocity 1 (1D; (1, 1)
+    // in 2D) and pressure 1, density 1 + 0.2 sin(4 pi x) and gamma 1.4 + 0.2 sin(2 pi x) (1D), or
+    // both perturbations 0.2 sin(2 pi x) sin(2 pi y) (2D): pure advection, periodic on the unit
+    // interval / square
+    const double rho0 = 1.0, u0 = 1.0, g0 = 1.4, Ag = 0.20, Ar = 0.20, p0 = 1.0;
+    for (int e = 0; e < NE; ++e)
+      for (int i = 0; i < NS; ++i) {
+        const double x = X(i, e, 0);
+        if (D == 1) {
+          const double sr = Ar * std::sin(4 * M_PI * x), sg = Ag * std::sin(2 * M_PI * x);
+          const double s[4] = {rho0 + sr, u0, p0, g0 + sg};
+          set(e, i, s);
+        } else {
+          const double y = X(i, e, 1);
+          const double sr = Ar * std::sin(2.0 * M_PI * x) * std::sin(2.0 * M_PI * y);
+          const double sg = Ag * std::sin(2.0 * M_PI * x) * std::sin(2.0 * M_PI * y);
+          const double s[5] = {rho0 + sr, u0, 1.0, p0, g0 + sg};
+          set(e, i, s);
+        }
+      }
+    return Status();
+  }
   if (ic == "shock_bubble" && D == 2) {
     // Mach-1.5 shock in air (gamma 1.4, pre-shock rho 1, p 1) at x = params[0] (default 0.2)
     // moving in +x into a circular bubble of radius 0.2 at (0.5, 0.5): gamma 1.67, rho 0.138,
@@ -680,6 +703,55 @@ Status init_state(const Problem& P, const std::string& ic, const std::vector<dou
   s.code = 1;
   s.msg = "unknown initial condition '" + ic + "' for this dimension";
   return s;
+}
+
+// ---------------------------------------------------------------------------------------
+// ERROR diagnostic of the reference driver (code/src/main.cc:909-1038, built with ERRR=ERROR):
+// both states go to (rho, u, (E - rho u^2/2)/alpha, alpha) on their fields 0..3 (the reference
+// applies this 1D formula on the same field indices in 2D as well), the cell integrals of every
+// field at the element quadrature points are divided by the width dx of element 0 (its nodes 0
+// and 1), and the differences give L1 = sum|E|/N_E, L2 = sqrt(sum E^2/N_E), Linf = max|E| per field.
+// ---------------------------------------------------------------------------------------
+Status error_norms(const Problem& P, const double* U, const double* Uexact, double* out) {
+  const int NS = P.N_s, NF = P.N_F, NE = P.N_E, NG = P.N_G, D = P.D;
+  auto prim = [&](const double* src) {
+    std::vector<double> V(src, src + (size_t)NE * NF * NS);
+    for (int e = 0; e < NE; ++e)
+      for (int i = 0; i < NS; ++i) {
+        double* f = &V[(size_t)e * NF * NS + i];
+        f[1 * NS] = f[1 * NS] / f[0];
+        f[2 * NS] = 1.0 / f[3 * NS] * (f[2 * NS] - 0.5 * f[0] * f[1 * NS] * f[1 * NS]);
+      }
+    return V;
+  };
+  const std::vector<double> A = prim(U), B = prim(Uexact);
+  auto averages = [&](const std::vector<double>& V) {
+    std::vector<double> avg((size_t)NE * NF, 0.0);
+    for (int e = 0; e < NE; ++e)
+      for (int fc = 0; fc < NF; ++fc)
+        for (int g = 0; g < NG; ++g) {
+          double ug = 0.0;
+          for (int i = 0; i < NS; ++i) ug += P.phi[g + (size_t)i * NG] * V[((size_t)e * NF + fc) * NS + i];
+          avg[(size_t)e * NF + fc] += ug * P.J[e] * P.qw[g];
+        }
+    return avg;
+  };
+  const std::vector<double> a = averages(A), b = averages(B);
+  const double dx = P.xyz_nodes[1 + (size_t)(0 * D + 0) * NS] - P.xyz_nodes[0 + (size_t)(0 * D + 0) * NS];
+  out[0] = dx;
+  for (int fc = 0; fc < NF; ++fc) {
+    double e1 = 0.0, e2 = 0.0, ei = 0.0;
+    for (int e = 0; e < NE; ++e) {
+      const double E = b[(size_t)e * NF + fc] / dx - a[(size_t)e * NF + fc] / dx;
+      e1 += std::fabs(E);
+      e2 += E * E;
+      if (ei < std::fabs(E)) ei = std::fabs(E);
+    }
+    out[1 + fc] = e1 / (double)NE;
+    out[1 + NF + fc] = std::sqrt(e2 / (double)NE);
+    out[1 + 2 * NF + fc] = ei;
+  }
+  return Status();
 }
 
 // ---------------------------------------------------------------------------------------

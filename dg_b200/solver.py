@@ -79,6 +79,16 @@ class Problem:
                                                int(prm.size), int(seed), F.dptr(U)))
         return U
 
+    def error_norms(self, U, U_exact) -> dict:
+        """The reference driver's ERROR diagnostic (main.cc:909-1038): dx and the L1, L2, Linf per
+        field of the cell averages of U against U_exact."""
+        U = np.ascontiguousarray(U, np.float64)
+        Ue = np.ascontiguousarray(U_exact, np.float64)
+        nf = self.info.n_fields
+        out = np.zeros(1 + 3 * nf)
+        F.check(F.lib().dgb_problem_error_norms(self._h, F.dptr(U), F.dptr(Ue), F.dptr(out)))
+        return {"dx": out[0], "l1": out[1:1 + nf], "l2": out[1 + nf:1 + 2 * nf], "linf": out[1 + 2 * nf:]}
+
     def write_pos(self, U: np.ndarray, step: int, time: float, directory: str | Path) -> None:
         U = np.ascontiguousarray(U, np.float64)
         F.check(F.lib().dgb_write_pos(self._h, F.dptr(U), int(step), float(time), str(directory).encode()))

@@ -127,6 +127,7 @@ typedef struct {
   double cfl, dx_min, cfl_scaled;/* cfl_scaled = CFL*Dx/(2p+1) (main.cc:896-897) */
   double final_time;
   int n_output_times;
+  int error_output;              /* deck "#Make options" ERRR=ERROR: error.dat after the run */
 } dgb_info;
 
 int dgb_problem_info(const dgb_problem* p, dgb_info* out);
@@ -145,11 +146,16 @@ int dgb_problem_get_array(const dgb_problem* p, const char* name, void* dst, siz
  * "riemann" (1D two-fluid Riemann problem split at params[0], seeded left/right states). */
 int dgb_problem_init_state(const dgb_problem* p, const char* ic, const double* params, int nparams,
                            uint64_t seed, double* U);
-/* (ic == NULL selects the deck's "#initial condition" and, when nparams == 0, its "#ic inputs".) */
+/* (ic == NULL selects the deck's "#initial condition" and, when nparams == 0, its "#ic inputs".)
+ * "sinegam" is the reference's smooth advection test (init_cond.cc:551-618). */
 
 /* Output in the reference .pos format (code/src/mesh/simpleMesh.cc:322-376 via
  * code/src/printer/printer.cc:77): one file per primitive field, <dir>/<name><step>.pos. */
 int dgb_write_pos(const dgb_problem* p, const double* U, int step, double time, const char* dir);
+/* The ERROR diagnostic of the reference driver (main.cc:909-1038): out = [dx, L1 (N_F), L2 (N_F),
+ * Linf (N_F)] of the cell averages of U against U_exact (both host, reference layout), after both
+ * are turned into (rho, u, (E - rho u^2/2) alpha^-1, alpha) on fields 0..3 as the reference does. */
+int dgb_problem_error_norms(const dgb_problem* p, const double* U, const double* U_exact, double* out);
 /* Restart read of the same files (printer.cc:108, simpleMesh.cc:378). */
 int dgb_read_pos(const dgb_problem* p, int step, const char* dir, double* time, double* U);
 

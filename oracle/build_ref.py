@@ -48,6 +48,8 @@ VARIANTS = {
     "1d_hll_y1": dict(dims="ONED", nf=5, d=1, flux="HLL", ny=1),
     "2d_roe_y1": dict(dims="TWOD", nf=6, d=2, flux="ROE", ny=1),
     "2d_rus_y1": dict(dims="TWOD", nf=6, d=2, flux="RUS", ny=1),
+    # the ERROR diagnostic compiled in (ERRR=ERROR in code/Makefile): error.dat after the run
+    "1d_rus_err": dict(dims="ONED", nf=4, d=1, flux="RUS", err=True),
 }
 
 RK_SYM = ("_ZN2RK14RK_integrationEdiiiiiiiPdS0_R8LimitingbR9DG_SOLVERR12COMMUNICATORR7PRINTER"
@@ -57,7 +59,7 @@ RK_SYM = ("_ZN2RK14RK_integrationEdiiiiiiiPdS0_R8LimitingbR9DG_SOLVERR12COMMUNIC
 def defines(v: dict) -> list[str]:
     return ["-DHAVE_BLAS", "-DHAVE_LAPACK", "-DUSE_CPU", "-DHOME", "-DUSE_DOUBLE", "-DMULTIFLUID",
             "-DGAMNCON", f"-D{v['flux']}", f"-D{v['dims']}", "-DNO_MPI", f"-DN_Y={v.get('ny', 0)}", f"-DN_F={v['nf']}",
-            "-DNOERROR", "-DNOCONS", f"-DD={v['d']}", "-DDF=1"]
+            "-DERROR" if v.get("err") else "-DNOERROR", "-DNOCONS", f"-DD={v['d']}", "-DDF=1"]
 
 
 def sources(ref: Path) -> list[Path]:

@@ -35,7 +35,7 @@ import numpy as np
 # setup
 # ---------------------------------------------------------------------------------------------
 
-ARRAY_NAMES = ("phi", "dphi", "phi_w", "dphi_w", "psi", "psi_w", "J", "invJac", "JF", "normals", "Minv",
+ARRAY_NAMES = ("phi", "dphi", "phi_w", "dphi_w", "psi", "psi_w", "weight", "J", "invJac", "JF", "normals", "Minv",
                "map", "invmap", "boundaryMap", "neighbors", "Lag2Mono", "Mono2Lag", "Lag2MonoX",
                "MonoX2MonoY", "MonoY2Lag", "MonoX2Lag", "Lag2MonoY")
 
@@ -962,3 +962,32 @@ def _sensor_gated(S: Setup, U: np.ndarray) -> np.ndarray:
     for off, L2M, M2L, n1 in passes:
         W = np.where(fl, fn(S, W, off, L2M, M2L, n1), W)
     return prim2cons(S, W) if S.limiter == "pri" else W
+
+
+# ---------------------------------------------------------------------------------------------
+# ERROR diagnostic of the reference driver (code/src/main.cc:909-1038)
+# ---------------------------------------------------------------------------------------------
+
+def error_norms(S: Setup, U: np.ndarray, Uex: np.ndarray, xyz0: tuple[float, float]) -> np.ndarray:
+    """[dx, L1, L2, Linf per field] of the quadrature cell integrals / dx of U against Uex after
+    both go to (rho, u, (E - rho u^2/2)/alpha, alpha) on fields 0..3; xyz0 = x of nodes 0 and 1
+    of element 0 (dx = their difference, main.cc:992)."""
+    NE, NF, Ns, NG = S.N_E, S.N_F, S.N_s, S.N_G
+
+    def prim(X):
+        V = np.array(X, np.float64, copy=True).reshape(NE, NF, Ns)
+        V[:, 1] = V[:, 1] / V[:, 0]
+        V[:, 2] = 1.0 / V[:, 3] * (V[:, 2] - 0.5 * V[:, 0] * V[:, 1] * V[:, 1])
+        return V
+
+    phi = S.a["phi"].reshape(Ns, NG)  # phi[i*N_G + g] (column-major N_G x N_s)
+    w = S.a["weight"].reshape(-1)[:NG]
+    J = S.a["J"].reshape(NE)
+
+    def avg(V):
+        Ug = np.einsum("efi,ig->efg", V, phi)
+        return np.einsum("efg,g->ef", Ug, w) * J[:, None]
+
+    dx = xyz0[1] - xyz0[0]
+    E = avg(prim(Uex)) / dx - avg(prim(U)) / dx
+    return np.concatenate([[dx], np.abs(E).sum(0) / NE, np.sqrt((E * E).sum(0) / NE), np.abs(E).max(0)])

@@ -22,9 +22,11 @@ FLUX_TAG = {"rusanov": "rus", "rus": "rus", "roe": "roe", "hll": "hll"}
 BC_TAG = {"periodic": 1, "transmissive": 2, "reflective": 3, "frozen": 4}
 
 
-def binary(dim: int, flux: str, n_mass: int = 0) -> Path:
-    """The reference build for (dimension, flux) with N_Y = n_mass (0 or 1) mass fractions."""
-    return REF_DIR / (f"dgref_{dim}d_{FLUX_TAG[flux.lower()]}" + (f"_y{n_mass}" if n_mass else ""))
+def binary(dim: int, flux: str, n_mass: int = 0, error: bool = False) -> Path:
+    """The reference build for (dimension, flux) with N_Y = n_mass (0 or 1) mass fractions, or with
+    the ERROR diagnostic compiled in."""
+    return REF_DIR / (f"dgref_{dim}d_{FLUX_TAG[flux.lower()]}" + (f"_y{n_mass}" if n_mass else "") +
+                      ("_err" if error else ""))
 
 
 def available(dim: int = 2, flux: str = "rusanov", n_mass: int = 0) -> bool:
@@ -48,6 +50,9 @@ class RefCase:
     output_times: tuple = (0.0, 1e-3)
     thresholds: tuple = ()
     n_mass: int = 0
+    ic: str = ""                  # deck "#initial condition" (default sodtube / sodcirc)
+    make_options: tuple = ()      # "#Make options" KEY=VALUE lines (read by dgbexec, ignored by the reference)
+    error: bool = False           # run the build with the ERROR diagnostic
     workdir: Path | None = None
     _tmp: object = field(default=None, repr=False)
 
@@ -65,11 +70,12 @@ class RefCase:
     def write_deck(self, cfl: float | None = None, output_times=None) -> Path:
         cfl = self.cfl if cfl is None else cfl
         out = self.output_times if output_times is None else output_times
-        lines = ["#Code options", "#time integration", "rk4", "#output time array",
+        lines = (["#Make options", *self.make_options] if self.make_options else []) + [
+                 "#Code options", "#time integration", "rk4", "#output time array",
                  " ".join(repr(float(t)) for t in out), "#final time", repr(float(out[-1])),
                  "#Courant-Friedrichs-Lewy condition", repr(float(cfl)), "#order", str(self.order),
                  "#mesh file", "mesh.msh", "lin" if self.dim == 1 else "qua", "#limiter", self.limiter,
-                 "#initial condition", "sodtube" if self.dim == 1 else "sodcirc"]
+                 "#initial condition", self.ic or ("sodtube" if self.dim == 1 else "sodcirc")]
         if self.thresholds:
             lines += ["#sensor thresholds", " ".join(repr(float(t)) for t in self.thresholds)]
         p = self.workdir / "deck.inp"
@@ -78,7 +84,7 @@ class RefCase:
 
     def run(self, cmd: str, U: np.ndarray | None = None, dt: float = 0.0, nsteps: int = 1,
             repeat: int = 1, timeout: float = 600.0, extra_env: dict | None = None) -> tuple[np.ndarray, str]:
-        exe = binary(self.dim, self.flux, self.n_mass)
+        exe = binary(self.dim, self.flux, self.n_mass, self.error)
         if not exe.exists():
             raise FileNotFoundError(f"{exe} missing: run python oracle/build_ref.py")
         args = [str(exe), "-d", "deck.inp", "--cmd", cmd, "--dt", repr(float(dt)), "--nsteps", str(nsteps),

@@ -214,8 +214,35 @@ def make_tube_fixture() -> dict:
     return out
 
 
+# the reference's ERROR diagnostic on its smooth advection test: sinegam on the periodic unit
+# interval, 40 elements, p = 2, Rusanov, no limiter, RK4 at CFL 0.2 to t = 1 (one period), built
+# with ERRR=ERROR; the reference's error.dat and its final .pos output are stored
+ERRCASE = dict(name="driver_d1_sinegam_rus_err", dim=1, order=2, nx=40, flux="rusanov", limiter="none", cfl=0.2,
+               output_times=(0.0, 0.5, 1.0), ic="sinegam")
+
+
+def make_error_fixture() -> dict:
+    c = ERRCASE
+    ref = RefCase(1, c["order"], c["nx"], 1, 0.0, 1.0, 0.0, 1.0, ("periodic",) * 4, c["flux"], c["limiter"],
+                  cfl=c["cfl"], output_times=c["output_times"], ic=c["ic"], make_options=("FLUX=RUS", "ERRR=ERROR"),
+                  error=True)
+    ref.write_deck()
+    ref.run("none", timeout=1800)
+    out = {"deck": np.array((ref.workdir / "deck.inp").read_text()),
+           "error_dat": np.loadtxt(ref.workdir / "error.dat")}
+    for f in sorted(ref.workdir.glob("*.pos")):
+        name, time, step, vals = read_pos(f)
+        out[f"pos_{f.stem}"] = vals
+        out[f"time_{f.stem}"] = np.array([time])
+    out["meta"] = np.array(json.dumps(c))
+    return out
+
+
 def main(argv=None) -> int:
     only = set((argv if argv is not None else sys.argv[1:]))
+    if ERRCASE["name"] in only:
+        np.savez_compressed(OUT / f"{ERRCASE['name']}.npz", **make_error_fixture())
+        print(f"wrote {ERRCASE['name']}.npz")
     if only:  # regenerate the named fixtures only
         for k, c in enumerate(CASES):
             if c["name"] in only:
@@ -224,6 +251,8 @@ def main(argv=None) -> int:
         return 0
     np.savez_compressed(OUT / f"{TUBE['name']}.npz", **make_tube_fixture())
     print(f"wrote {TUBE['name']}.npz")
+    np.savez_compressed(OUT / f"{ERRCASE['name']}.npz", **make_error_fixture())
+    print(f"wrote {ERRCASE['name']}.npz")
     np.savez_compressed(OUT / f"{DRIVER['name']}.npz", **make_driver_fixture())
     print(f"wrote {DRIVER['name']}.npz")
     for k, c in enumerate(CASES):

@@ -38,3 +38,26 @@ def test_dgbexec_reproduces_reference_run(tmp_path):
         rv = d[f"pos_{stem}"]
         assert vals.shape == rv.shape
         assert np.abs(vals - rv).max() <= 1e-10 * np.abs(rv).max(), stem
+
+
+def test_dgbexec_error_diagnostic_matches_reference(tmp_path):
+    """The reference's ERROR build on its smooth advection deck (sinegam, periodic, 40 elements,
+    p=2, Rusanov, no limiter, RK4 to one period): dgbexec's error.dat against the reference's.
+    The density and 1/(gamma-1) errors (3e-6, 1.5e-5) agree to 1e-4 relative; the velocity and
+    pressure columns are rounding noise (~1e-14) in both runs."""
+    import dg_b200 as dgb
+    d = np.load(GOLDEN / "driver_d1_sinegam_rus_err.npz")
+    c = json.loads(str(d["meta"]))
+    dgb.write_msh(tmp_path / "mesh.msh", 1, c["order"], c["nx"], 1, 0.0, 1.0, 0.0, 1.0, ("periodic",) * 4)
+    (tmp_path / "deck.inp").write_text(str(d["deck"]))
+    exe = ROOT / "dg_b200" / "lib" / "dgbexec"
+    r = subprocess.run([str(exe), "-d", "deck.inp", "--out", "."], cwd=tmp_path, capture_output=True, text=True,
+                       timeout=300)
+    assert r.returncode == 0, r.stdout + r.stderr
+    mine = np.loadtxt(tmp_path / "error.dat")
+    ref = d["error_dat"]
+    assert mine.shape == ref.shape == (3, 5)
+    assert np.all(mine[:, 0] == ref[:, 0])  # dx
+    for col in (1, 4):                      # rho, 1/(gamma-1)
+        assert np.allclose(mine[:, col], ref[:, col], rtol=1e-4, atol=0), (col, mine[:, col], ref[:, col])
+    assert np.all(np.abs(mine[:, 2:4]) < 1e-12) and np.all(np.abs(ref[:, 2:4]) < 1e-12)

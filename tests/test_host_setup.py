@@ -112,3 +112,38 @@ def test_deck_mass_option(tmp_path):
         "#limiter\nm2l\n#initial condition\nsodtube\n")
     prob = dgb.Problem.from_deck(tmp_path / "deck.inp")
     assert prob.info.n_fields == 5
+
+
+def test_error_norms_match_the_oracle():
+    """dgb_problem_error_norms (the reference driver's ERROR block) against its numpy restatement,
+    on the smooth advection state and a perturbed copy."""
+    import dg_b200 as dgb
+    from oracle import dg_oracle as O
+    for dim, nx, ny in ((1, 24, 1), (2, 8, 6)):
+        prob = dgb.Problem.structured(dim, 2, nx, ny, 0.0, 1.0, 0.0, 1.0, ("periodic",) * 4, flux="rusanov",
+                                      limiter="none", cfl=0.2)
+        Uex = prob.init_state("sinegam")
+        rng = np.random.default_rng(4)
+        U = Uex * (1 + 1e-3 * rng.uniform(-1, 1, Uex.shape))
+        mine = prob.error_norms(U, Uex)
+        S = O.Setup.from_problem(prob)
+        xyz = prob.array("xyz_nodes")
+        ref = O.error_norms(S, U, Uex, (xyz[0], xyz[1]))
+        assert abs(mine["dx"] - ref[0]) == 0
+        nf = prob.info.n_fields
+        got = np.concatenate([mine["l1"], mine["l2"], mine["linf"]])
+        assert np.allclose(got, ref[1:], rtol=1e-12, atol=0), (got, ref[1:])
+        assert mine["l1"][0] > 0
+
+
+def test_sinegam_initial_state():
+    """The reference's smooth advection test: uniform velocity and pressure, rho and gamma perturbed."""
+    import dg_b200 as dgb
+    prob = dgb.Problem.structured(1, 2, 16, 1, 0.0, 1.0, 0.0, 1.0, ("periodic",) * 2, flux="rusanov", limiter="none")
+    i = prob.info
+    V = prob.init_state("sinegam").reshape(i.n_elem, i.n_fields, i.n_s)
+    rho, u = V[:, 0], V[:, 1] / V[:, 0]
+    gam = 1 + 1 / V[:, 3]
+    p = (gam - 1) * (V[:, 2] - 0.5 * rho * u * u)
+    assert np.allclose(u, 1.0, atol=1e-15) and np.allclose(p, 1.0, atol=1e-14)
+    assert 0.79 < rho.min() < 0.81 and 1.19 < rho.max() < 1.21 and 1.19 < gam.min() and gam.max() < 1.61
