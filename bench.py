@@ -17,6 +17,7 @@ device-side CFL step.  DOF = N_E * N_s * N_F = 5,898,240.
              bounded sample of the same workload, one process on one core
   forms      plain FP64, mixed and mixed + learned indicator at equal L1 error (same protocol)
   mass_fraction  the workload with one passive mass fraction (6 fields): time per step
+  gamma_model  the workload grid with Roe + hrl in both gamma models (GAMNCON, GAMCONS): time per step
   tube_1d    the 1D two-fluid shock tube (1000 elements, p=2, Roe, RK4, CFL 0.4, 2000 steps): device
              time, distance from the reference's own run, the reference CPU build's time
   learned_deploy  the learned indicator on a 1024x1024 four-quadrant problem: FP64 / mixed / mixed +
@@ -529,6 +530,32 @@ def mass_fraction(dgb, dev, base_ms, steps=20, warmup=3):
             "rhoY_total_start_end": [float(c0[5]), float(c1[5])]}
 
 
+def gamma_models(dgb, dev, steps=20, warmup=3):
+    """The benchmark grid (512 x 256, p=2, SSP-RK3, CFL 0.3) with Roe and hrl in both gamma models:
+    GAMNCON (1/(gamma-1) with its non-conservative source) and GAMCONS (rho/(gamma-1) transported
+    conservatively; the reference's M2limiting stops for it, hence hrl for both).  Device time per
+    step and the total of the gamma-model field at the start and the end (conserved for GAMCONS up
+    to the open x boundaries)."""
+    x0, x1, y0, y1 = DOMAIN
+    out = {"workload": "2D shock-bubble 512x256, p=2, Roe, hrl, SSP-RK3, CFL 0.3"}
+    for gm in ("gamncon", "gamcons"):
+        prob = dgb.Problem.structured(2, ORDER, NX, NY, x0, x1, y0, y1, BC, flux="roe", limiter="hrl", cfl=CFL,
+                                      gamma_model=gm)
+        info = prob.info
+        dof = info.n_elem * info.n_s * info.n_fields
+        s = dgb.DGSolver(prob, device=dev)
+        s.set_state(s.limit(prob.init_state("shock_bubble", seed=SEED)))
+        c0 = s.conservation()
+        s.advance(warmup, 0.0, scheme=dgb.SSPRK3)
+        s.advance(steps, 0.0, scheme=dgb.SSPRK3)
+        ms, _ = s.last_timing()
+        c1 = s.conservation()
+        s.close()
+        out[gm] = {"value": dof * STAGES_PER_STEP * steps / (ms / 1e3), "unit": UNIT, "ms_per_step": ms / steps,
+                   "gamma_field_total_start_end": [float(c0[4]), float(c1[4])]}
+    return out
+
+
 P3_NX, P3_NY, P3_STEPS = 2048, 1024, 300
 
 
@@ -662,6 +689,8 @@ def main(argv=None) -> int:
     ap.add_argument("--no-tube", action="store_true", help="skip the 1D shock-tube run")
     ap.add_argument("--tube-only", action="store_true", help="print only the 1D shock-tube run")
     ap.add_argument("--p3-only", action="store_true", help="print only the 2048x1024 p=3 FP64 / mixed comparison")
+    ap.add_argument("--models-only", action="store_true",
+                    help="print only the mass-fraction and gamma-model lines (512x256, p=2)")
     args = ap.parse_args(argv)
     if args.impl == "reference":
         return run_reference(args)
@@ -690,6 +719,10 @@ def main(argv=None) -> int:
     if args.p3_only:
         if rank == 0:
             print(json.dumps({"mixed_p3": mixed_p3(dgb, dev)}))
+        return 0
+    if args.models_only:
+        if rank == 0:
+            print(json.dumps({"mass_fraction": mass_fraction(dgb, dev, None), "gamma_model": gamma_models(dgb, dev)}))
         return 0
     if args.ensemble_only:
         if rank == 0:
@@ -785,6 +818,9 @@ def main(argv=None) -> int:
     mf = None
     if ws == 1 and not args.no_tube and (args.nx, args.ny) == (NX, NY):
         mf = mass_fraction(dgb, dev, dev_ms / args.steps)
+    gms = None
+    if ws == 1 and not args.no_tube and (args.nx, args.ny) == (NX, NY):
+        gms = gamma_models(dgb, dev)
     tube = None
     if ws == 1 and not args.no_tube and (args.nx, args.ny) == (NX, NY):
         tube = tube_1d(dgb, dev, with_reference=rank == 0 and not args.no_cpu_baseline)
@@ -809,7 +845,8 @@ def main(argv=None) -> int:
                 "kernel_ms_per_step": {"residual": res_ms / args.steps, "limiter": lim_ms / args.steps,
                                        "dt": dt_ms / args.steps},
                 "cpu_baseline": cpu, "clocks": clocks, "gpu_launches": launches, "forms": forms,
-                "ensemble": ens, "mixed_p3": p3, "learned_deploy": deploy, "tube_1d": tube, "mass_fraction": mf}
+                "ensemble": ens, "mixed_p3": p3, "learned_deploy": deploy, "tube_1d": tube, "mass_fraction": mf,
+                "gamma_model": gms}
         print(json.dumps(line))
     solver.close()
     if ws > 1:

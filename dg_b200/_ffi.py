@@ -15,6 +15,7 @@ FLUX = {"rusanov": 0, "rus": 0, "llf": 0, "hll": 1, "roe": 2}
 LIMITER = {"none": 0, "hrl": 1, "m2l": 2, "hri": 3, "m2i": 4, "prl": 5, "pri": 6, "p0i": 7}
 SSPRK3, RK4 = 3, 4
 FORM = {"fp64": 0, "mixed": 1}
+GAMMA_MODEL = {"gamncon": 0, "gamcons": 1}
 BC = {"periodic": 1, "transmissive": 2, "reflective": 3, "frozen": 4}
 
 # every exported entry point of include/dgb.h
@@ -40,7 +41,8 @@ class MeshSpec(C.Structure):
 
 class Options(C.Structure):
     _fields_ = [("flux", C.c_int), ("limiter", C.c_int), ("cfl", C.c_double),
-                ("thresholds", C.c_double * 3), ("n_thresholds", C.c_int), ("n_mass", C.c_int)]
+                ("thresholds", C.c_double * 3), ("n_thresholds", C.c_int), ("n_mass", C.c_int),
+                ("gamma_model", C.c_int)]
 
 
 class Info(C.Structure):
@@ -48,7 +50,7 @@ class Info(C.Structure):
                 "dim order n_fields n_elem n_s n_g n_ifaces m_s m_g n_n n_reflective cartesian "
                 "gpu_supported flux limiter nx ny".split()] + \
                [(n, C.c_double) for n in "cfl dx_min cfl_scaled final_time".split()] + \
-               [("n_output_times", C.c_int), ("error_output", C.c_int)]
+               [("n_output_times", C.c_int), ("error_output", C.c_int), ("gamma_model", C.c_int)]
 
 
 class DGBError(RuntimeError):

@@ -24,6 +24,7 @@ struct dgb_ctx {
   int D = 1, p = 1, nf = 4, ns = 2, ne = 0, ld = 0, flux = 2, limiter = 0;
   int nx = 0, ny = 0;
   int nmass = 0;          // passive mass fractions (fields D+3 .. nf-1)
+  bool gamcons = false;   // GAMCONS gamma model (fifth field rho/(gamma-1), conservative)
   bool tiled = false;     // structured row-major grid with tile-multiple extents: tiled residual kernel
   int form = DGB_FORM_FP64;  // arithmetic of the residual: plain FP64 or mixed FP32/FP64
   bool rowmajor = false;  // structured row-major grid: tiled limiter passes

@@ -257,7 +257,8 @@ __global__ void __launch_bounds__(NT) residual2d_kernel(const Consts cin, const 
 // ------------------------------------------------------------------------------------------
 // element e (< c.n_elem) with the problem constants c (in shared memory) and dt; NY passive mass
 // fractions follow the four gamma-model fields
-template <int P, int FLUX, int MODE, int NY = 0>
+// GC: the GAMCONS model (fields rho, rho u, E, rho/(gamma-1)): conservative alpha flux, no source
+template <int P, int FLUX, int MODE, int NY = 0, bool GC = false>
 __device__ __forceinline__ void res1d_body(const Consts& c, const StageArgs& a, int e, double dt) {
   constexpr int N1 = P + 1, NG = P + 1, NF = 4 + NY;
   const int ld = c.ld;
@@ -279,16 +280,18 @@ __device__ __forceinline__ void res1d_body(const Consts& c, const StageArgs& a, 
       da += c.Dq[g][t] * u[3][t];
     }
     const double rho = ug[0], vx = ug[1] / rho, Et = ug[2];
-    const double gamma = 1 + 1.0 / ug[3];
+    const double gamma = GC ? 1 + rho / ug[3] : 1 + 1.0 / ug[3];  // physics.cu:100-104
     const double p = (gamma - 1) * (Et - 0.5 * rho * vx * vx);
     const double cx = c.wq[g] * (c.ixx * c.J);
     const double fx[3] = {rho * vx, rho * vx * vx + p, (Et + p) * vx};
     const double s = (c.wq[g] * c.J) * (-vx * da * c.ixx);  // physics.cu:126-127
+    const double fa = rho * vx * (1 / (gamma - 1));           // GAMCONS alpha flux, physics.cu:122-124
 #pragma unroll
     for (int t = 0; t < N1; ++t) {
 #pragma unroll
       for (int f = 0; f < 3; ++f) r[f][t] += c.Dq[g][t] * (cx * fx[f]);
-      r[3][t] += c.Bq[g][t] * s;
+      if (GC) r[3][t] += c.Dq[g][t] * (cx * fa);
+      else r[3][t] += c.Bq[g][t] * s;
 #pragma unroll
       for (int k = 0; k < NY; ++k) r[4 + k][t] += c.Dq[g][t] * (cx * (ug[4 + k] * vx));  // physics.cu:130-134
     }
@@ -312,7 +315,8 @@ __device__ __forceinline__ void res1d_body(const Consts& c, const StageArgs& a, 
 #pragma unroll
     for (int f = 0; f < NF; ++f) { L[f] = swapLR ? un[f] : uo[f]; R[f] = swapLR ? uo[f] : un[f]; }
     double F[NF], nc;
-    phys::riemann1d<FLUX, NY>(L[0], R[0], L[1] / L[0], R[1] / R[0], L[2], R[2], L[3], R[3], nx, F, nc, L + 4, R + 4);
+    phys::riemann1d<FLUX, NY, GC>(L[0], R[0], L[1] / L[0], R[1] / R[0], L[2], R[2], L[3], R[3], nx, F, nc, L + 4,
+                                  R + 4);
 #pragma unroll
     for (int f = 0; f < NF; ++f) r[f][to] += sgn * F[f] + (f == 3 ? nc : 0.0);
   }
@@ -342,7 +346,7 @@ __device__ __forceinline__ void res1d_body(const Consts& c, const StageArgs& a, 
     }
 }
 
-template <int P, int FLUX, int MODE, int NY = 0>
+template <int P, int FLUX, int MODE, int NY = 0, bool GC = false>
 __global__ void __launch_bounds__(128) residual1d_kernel(const Consts cin, const StageArgs a) {
   __shared__ Consts c;
   copy_consts(c, cin);
@@ -351,7 +355,7 @@ __global__ void __launch_bounds__(128) residual1d_kernel(const Consts cin, const
   const int e = blockIdx.x * blockDim.x + threadIdx.x;
   if (e >= c.n_elem) return;
   const double dt = MODE == MODE_RESIDUAL ? 0.0 : (a.dt_override > 0 ? a.dt_override : a.scal->dt);
-  res1d_body<P, FLUX, MODE, NY>(c, a, e, dt);
+  res1d_body<P, FLUX, MODE, NY, GC>(c, a, e, dt);
 }
 
 // ------------------------------------------------------------------------------------------
@@ -660,7 +664,7 @@ __global__ void __launch_bounds__(128) lim1d_kernel(const LimArgs la, const doub
 // ------------------------------------------------------------------------------------------
 // CFL step: max over nodes of the wave speed, then dt = CFL_scaled / max (on the device)
 // ------------------------------------------------------------------------------------------
-template <int DIM, int NS>
+template <int DIM, int NS, bool GC = false>
 __global__ void __launch_bounds__(256) wavespeed_kernel(const double* __restrict__ U, int n_elem, int ld,
                                                         DevScalars* __restrict__ scal) {
   if (scal->flags) return;
@@ -671,10 +675,10 @@ __global__ void __launch_bounds__(256) wavespeed_kernel(const double* __restrict
     for (int t = 0; t < NS; ++t) {
       double w;
       if (DIM == 1)
-        w = phys::wave_speed1d(__ldg(U + (size_t)(0 * NS + t) * ld + e), __ldg(U + (size_t)(1 * NS + t) * ld + e),
-                               __ldg(U + (size_t)(2 * NS + t) * ld + e), __ldg(U + (size_t)(3 * NS + t) * ld + e));
+        w = phys::wave_speed1d<GC>(__ldg(U + (size_t)(0 * NS + t) * ld + e), __ldg(U + (size_t)(1 * NS + t) * ld + e),
+                                   __ldg(U + (size_t)(2 * NS + t) * ld + e), __ldg(U + (size_t)(3 * NS + t) * ld + e));
       else
-        w = phys::wave_speed2d(__ldg(U + (size_t)(0 * NS + t) * ld + e), __ldg(U + (size_t)(1 * NS + t) * ld + e),
+        w = phys::wave_speed2d<GC>(__ldg(U + (size_t)(0 * NS + t) * ld + e), __ldg(U + (size_t)(1 * NS + t) * ld + e),
                                __ldg(U + (size_t)(2 * NS + t) * ld + e), __ldg(U + (size_t)(3 * NS + t) * ld + e),
                                __ldg(U + (size_t)(4 * NS + t) * ld + e));
       if (!(w == w)) bad = true;

@@ -4,7 +4,9 @@
 // alpha = 1/(gamma-1) carried non-conservatively (no flux; volume source -u.grad(alpha);
 // interface term ncterm), then NY passive mass fractions rho*Y_k (conservative: flux rho*Y_k u,
 // interface fluxes of the MACRO blocks that follow each flux function in the reference's
-// face_fluxes headers).  Formulas restate the reference's:
+// face_fluxes headers).  GC selects the reference's GAMCONS model: the fifth field is
+// rho/(gamma-1), carried conservatively (flux rho u/(gamma-1), no source, ncterm 0); the flux
+// functions divide it by rho on entry as the reference does.  Formulas restate the reference's:
 //   volume flux/source   evaluate_sf   code/src/physics/physics.cu:96-143 (1D), 248-301 (2D)
 //   Rusanov              oned_multifluid_rusanov  code/src/face_fluxes/oned_multifluid_fluxes.h:30-94
 //                        twod_multifluid_rusanov  code/src/face_fluxes/twod_multifluid_fluxes.h:30-97
@@ -24,10 +26,14 @@ enum { FLUX_RUS = 0, FLUX_HLL = 1, FLUX_ROE = 2 };
 // ---------------------------------------------------------------- 1D -------------------------
 // Interface flux F[4] and ncterm for the alpha equation (F[3] holds the alpha dissipation).
 // Caller forms q_L = -F + nc (element on side L) and q_R = F + nc (physics.cu:800-804).
-template <int FLUX, int NY = 0>
+template <int FLUX, int NY = 0, bool GC = false>
 __device__ __forceinline__ void riemann1d(double rhoL, double rhoR, double vxL, double vxR, double EtL, double EtR,
                                           double alphaL, double alphaR, double nx, double* F, double& nc,
                                           const double* YL = nullptr, const double* YR = nullptr) {
+  if (GC) {
+    alphaL = alphaL / rhoL;
+    alphaR = alphaR / rhoR;
+  }
   const double gammaL = 1.0 + 1.0 / alphaL;
   const double gammaR = 1.0 + 1.0 / alphaR;
   const double pL = (gammaL - 1) * (EtL - 0.5 * rhoL * vxL * vxL);
@@ -39,8 +45,13 @@ __device__ __forceinline__ void riemann1d(double rhoL, double rhoR, double vxL, 
     F[0] = 0.5 * ((rhoL * vxL + rhoR * vxR) * nx - maxvap * (rhoR - rhoL));
     F[1] = 0.5 * ((rhoL * vxL * vxL + pL + rhoR * vxR * vxR + pR) * nx - maxvap * (rhoR * vxR - rhoL * vxL));
     F[2] = 0.5 * (((EtL + pL) * vxL + (EtR + pR) * vxR) * nx - maxvap * (EtR - EtL));
-    F[3] = 0.5 * (-maxvap * (alphaR - alphaL));
-    nc = -0.5 * 0.5 * (vxL + vxR) * (alphaR - alphaL) * nx;
+    if (GC) {  // oned_multifluid_fluxes.h:79-81
+      F[3] = 0.5 * ((rhoL * vxL * alphaL + rhoR * vxR * alphaR) * nx - maxvap * (rhoR * alphaR - rhoL * alphaL));
+      nc = 0.0;
+    } else {
+      F[3] = 0.5 * (-maxvap * (alphaR - alphaL));
+      nc = -0.5 * 0.5 * (vxL + vxR) * (alphaR - alphaL) * nx;
+    }
     // the reference's mass-fraction line has its dissipation outside the 1/2 (fluxes.h:90-91)
 #pragma unroll
     for (int k = 0; k < NY; ++k) F[4 + k] = 0.5 * (YL[k] * vxL + YR[k] * vxR) * nx - maxvap * (YR[k] - YL[k]);
@@ -62,25 +73,27 @@ __device__ __forceinline__ void riemann1d(double rhoL, double rhoR, double vxL, 
       F[0] = rhoL * vxL * nx;
       F[1] = (rhoL * vxL * vxL + pL) * nx;
       F[2] = (EtL + pL) * vxL * nx;
-      F[3] = -0.5 * vncabs;
+      F[3] = GC ? rhoL * vxL * alphaL * nx : -0.5 * vncabs;
 #pragma unroll
       for (int k = 0; k < NY; ++k) F[4 + k] = YL[k] * vxL * nx;
     } else if ((SL < 0) && (SR > 0)) {
       F[0] = fhll(rhoL, SL, rhoL * vxL * nx, rhoR, SR, rhoR * vxR * nx);
       F[1] = fhll(vxL, SL, (rhoL * vxL * vxL + pL) * nx, vxR, SR, (rhoR * vxR * vxR + pR) * nx);
       F[2] = fhll(EtL, SL, (EtL + pL) * vxL * nx, EtR, SR, (EtR + pR) * vxR * nx);
-      F[3] = fhll(alphaL, SL, 0, alphaR, SR, 0) - 0.5 * fabs(SR + SL) / fabs(SR - SL) * vncabs;
+      // GAMCONS: the jump term takes the divided alpha, as oned_multifluid_fluxes.h:196 does
+      F[3] = GC ? fhll(alphaL, SL, rhoL * vxL * alphaL * nx, alphaR, SR, rhoR * vxR * alphaR * nx)
+                : fhll(alphaL, SL, 0, alphaR, SR, 0) - 0.5 * fabs(SR + SL) / fabs(SR - SL) * vncabs;
 #pragma unroll
       for (int k = 0; k < NY; ++k) F[4 + k] = fhll(YL[k], SL, YL[k] * vxL * nx, YR[k], SR, YR[k] * vxR * nx);
     } else if (SR < 0) {
       F[0] = rhoR * vxR * nx;
       F[1] = (rhoR * vxR * vxR + pR) * nx;
       F[2] = (EtR + pR) * vxR * nx;
-      F[3] = 0.5 * vncabs;
+      F[3] = GC ? rhoR * vxR * alphaR * nx : 0.5 * vncabs;
 #pragma unroll
       for (int k = 0; k < NY; ++k) F[4 + k] = YR[k] * vxR * nx;
     }
-    nc = -0.5 * vnc;
+    nc = GC ? 0.0 : -0.5 * vnc;
   } else {
     const double RT = sqrt(rhoR / rhoL);
     const double rho = RT * rhoL;
@@ -107,8 +120,9 @@ __device__ __forceinline__ void riemann1d(double rhoL, double rhoR, double vxL, 
            0.5 * (ws0 * dV0 * (v - a) + ws1 * dV1 * v + ws2 * dV2 * (v + a) + ws3 * dV3 * 0);
     F[2] = 0.5 * ((EtL + pL) * vxL + (EtR + pR) * vxR) * nx -
            0.5 * (ws0 * dV0 * (H - v * a) + ws1 * dV1 * (0.5 * v * v) + ws2 * dV2 * (H + v * a) + ws3 * dV3 * p);
-    F[3] = 0 + -0.5 * (ws0 * dV0 * 0 + ws1 * dV1 * 0 + ws2 * dV2 * 0 + ws3 * dV3 * 1);
-    nc = -0.5 * v * (alphaR - alphaL) * nx;
+    F[3] = (GC ? 0.5 * (rhoL * vxL * alphaL + rhoR * vxR * alphaR) * nx : 0) +
+           -0.5 * (ws0 * dV0 * 0 + ws1 * dV1 * 0 + ws2 * dV2 * 0 + ws3 * dV3 * 1);
+    nc = GC ? 0.0 : -0.5 * v * (alphaR - alphaL) * nx;
     // mass fractions: Roe-averaged Y and its wave strength (oned_multifluid_fluxes.h:358-370)
 #pragma unroll
     for (int k = 0; k < NY; ++k) {
@@ -120,11 +134,19 @@ __device__ __forceinline__ void riemann1d(double rhoL, double rhoR, double vxL, 
 }
 
 // ---------------------------------------------------------------- 2D -------------------------
-template <int FLUX, int NY = 0>
+template <int FLUX, int NY = 0, bool GC = false>
 __device__ __forceinline__ void riemann2d(double rhoL, double rhoR, double vxL, double vxR, double vyL, double vyR,
                                           double EtL, double EtR, double alphaL, double alphaR, double nx, double ny,
                                           double* F, double& nc, const double* YL = nullptr,
                                           const double* YR = nullptr) {
+  if (GC) {
+    // twod_multifluid_rusanov runs alphaL = alphaL/rhoL; alphaR = alphaL/rhoL (fluxes.h:50-53),
+    // so its right alpha is the left one divided twice by rhoL; the Roe solver divides each by
+    // its own density (:175-178)
+    const double aLd = alphaL / rhoL;
+    alphaR = FLUX == FLUX_ROE ? alphaR / rhoR : aLd / rhoL;
+    alphaL = aLd;
+  }
   const double vnL = vxL * nx + vyL * ny;
   const double vnR = vxR * nx + vyR * ny;
   const double gammaL = 1.0 + 1.0 / alphaL;
@@ -171,8 +193,9 @@ __device__ __forceinline__ void riemann2d(double rhoL, double rhoR, double vxL, 
     F[3] = 0.5 * (rhoL * vnL * HL + rhoR * vnR * HR) -
            0.5 * (ws0 * dV0 * (H - vn * a) + ws1 * dV1 * (vt * a) + ws2 * dV2 * (0.5 * (vx * vx + vy * vy)) +
                   ws3 * dV3 * (H + vn * a) + ws4 * dV4 * p);
-    F[4] = 0 + -0.5 * (ws0 * dV0 * 0 + ws1 * dV1 * 0 + ws2 * dV2 * 0 + ws3 * dV3 * 0 + ws4 * dV4 * 1);
-    nc = -0.5 * vn * (alphaR - alphaL);
+    F[4] = (GC ? 0.5 * (rhoL * vnL * alphaL + rhoR * vnR * alphaR) : 0) +
+           -0.5 * (ws0 * dV0 * 0 + ws1 * dV1 * 0 + ws2 * dV2 * 0 + ws3 * dV3 * 0 + ws4 * dV4 * 1);
+    nc = GC ? 0.0 : -0.5 * vn * (alphaR - alphaL);
     // mass fractions (twod_multifluid_fluxes.h:307-319)
 #pragma unroll
     for (int k = 0; k < NY; ++k) {
@@ -188,8 +211,13 @@ __device__ __forceinline__ void riemann2d(double rhoL, double rhoR, double vxL, 
     F[1] = 0.5 * ((rhoL * vnL * vxL + pL * nx) + (rhoR * vnR * vxR + pR * nx) - maxvap * (rhoR * vxR - rhoL * vxL));
     F[2] = 0.5 * ((rhoL * vnL * vyL + pL * ny) + (rhoR * vnR * vyR + pR * ny) - maxvap * (rhoR * vyR - rhoL * vyL));
     F[3] = 0.5 * (rhoL * vnL * HL + rhoR * vnR * HR - maxvap * (EtR - EtL));
-    F[4] = 0.5 * (-maxvap * (alphaR - alphaL));
-    nc = -0.5 * 0.5 * (vnL + vnR) * (alphaR - alphaL);
+    if (GC) {  // twod_multifluid_fluxes.h:82-84
+      F[4] = 0.5 * (rhoL * vnL * alphaL + rhoR * vnR * alphaR - maxvap * (rhoR * alphaR - rhoL * alphaL));
+      nc = 0.0;
+    } else {
+      F[4] = 0.5 * (-maxvap * (alphaR - alphaL));
+      nc = -0.5 * 0.5 * (vnL + vnR) * (alphaR - alphaL);
+    }
     // the reference's mass-fraction line has its dissipation outside the 1/2 (fluxes.h:91-94)
 #pragma unroll
     for (int k = 0; k < NY; ++k) F[5 + k] = 0.5 * (YL[k] * vnL + YR[k] * vnR) - maxvap * (YR[k] - YL[k]);
@@ -197,13 +225,17 @@ __device__ __forceinline__ void riemann2d(double rhoL, double rhoR, double vxL, 
 }
 
 // max(|u|+a, |v|+a) at a node (upa.h:61-85)
+template <bool GC = false>
 __device__ __forceinline__ double wave_speed1d(double rho, double rhou, double E, double alpha) {
+  if (GC) alpha = alpha / rho;  // upa.h:65-67
   const double u = rhou / rho;
   const double gamma = 1.0 + 1.0 / alpha;
   const double p = (gamma - 1) * (E - 0.5 * rho * u * u);
   return fabs(u) + sqrt(gamma * p / rho);
 }
+template <bool GC = false>
 __device__ __forceinline__ double wave_speed2d(double rho, double rhou, double rhov, double E, double alpha) {
+  if (GC) alpha = alpha / rho;  // upa.h:78-80
   const double u = rhou / rho, v = rhov / rho;
   const double gamma = 1.0 + 1.0 / alpha;
   const double p = (gamma - 1) * (E - 0.5 * rho * (u * u + v * v));
@@ -220,13 +252,17 @@ namespace phys {
 // The same 2D interface fluxes evaluated with one reciprocal per state instead of repeated
 // divisions (x/rho -> x * (1/rho), gamma-1 = 1/alpha).  Agrees with riemann2d to a few ulp,
 // far inside the 1e-12 parity bound; used by the tiled kernel.
-template <int FLUX, int NY = 0>
+template <int FLUX, int NY = 0, bool GC = false>
 __device__ __forceinline__ void riemann2d_rcp(const double* L, const double* R, double nx, double ny, double* F,
                                               double& nc) {
   const double rhoL = L[0], rhoR = R[0];
   const double irL = __drcp_rn(rhoL), irR = __drcp_rn(rhoR);
   const double vxL = L[1] * irL, vyL = L[2] * irL, vxR = R[1] * irR, vyR = R[2] * irR;
-  const double EtL = L[3], EtR = R[3], alphaL = L[4], alphaR = R[4];
+  const double EtL = L[3], EtR = R[3];
+  // GAMCONS: divided by rho on entry; the Rusanov solver's right alpha is the left one divided
+  // twice by rhoL (see riemann2d)
+  const double alphaL = GC ? L[4] * irL : L[4];
+  const double alphaR = GC ? (FLUX == FLUX_ROE ? R[4] * irR : alphaL * irL) : R[4];
   const double gm1L = __drcp_rn(alphaL), gm1R = __drcp_rn(alphaR);
   const double vnL = vxL * nx + vyL * ny;
   const double vnR = vxR * nx + vyR * ny;
@@ -273,8 +309,8 @@ __device__ __forceinline__ void riemann2d_rcp(const double* L, const double* R, 
            0.5 * (w0 * (vy - a * ny) + w1 * (a * ty) + w2 * vy + w3 * (vy + a * ny));
     F[3] = 0.5 * (rhoL * vnL * HL + rhoR * vnR * HR) -
            0.5 * (w0 * (H - vn * a) + w1 * (vt * a) + w2 * (0.5 * (vx * vx + vy * vy)) + w3 * (H + vn * a) + w4 * p);
-    F[4] = -0.5 * w4;
-    nc = -0.5 * vn * (alphaR - alphaL);
+    F[4] = GC ? 0.5 * (rhoL * vnL * alphaL + rhoR * vnR * alphaR) + -0.5 * w4 : -0.5 * w4;
+    nc = GC ? 0.0 : -0.5 * vn * (alphaR - alphaL);
 #pragma unroll
     for (int k = 0; k < NY; ++k) {
       const double Y = (L[5 + k] * irL + RT * R[5 + k] * irR) * i1;
@@ -287,8 +323,13 @@ __device__ __forceinline__ void riemann2d_rcp(const double* L, const double* R, 
     F[1] = 0.5 * ((rhoL * vnL * vxL + pL * nx) + (rhoR * vnR * vxR + pR * nx) - maxvap * (R[1] - L[1]));
     F[2] = 0.5 * ((rhoL * vnL * vyL + pL * ny) + (rhoR * vnR * vyR + pR * ny) - maxvap * (R[2] - L[2]));
     F[3] = 0.5 * (rhoL * vnL * HL + rhoR * vnR * HR - maxvap * (EtR - EtL));
-    F[4] = 0.5 * (-maxvap * (alphaR - alphaL));
-    nc = -0.5 * 0.5 * (vnL + vnR) * (alphaR - alphaL);
+    if (GC) {
+      F[4] = 0.5 * (rhoL * vnL * alphaL + rhoR * vnR * alphaR - maxvap * (rhoR * alphaR - rhoL * alphaL));
+      nc = 0.0;
+    } else {
+      F[4] = 0.5 * (-maxvap * (alphaR - alphaL));
+      nc = -0.5 * 0.5 * (vnL + vnR) * (alphaR - alphaL);
+    }
 #pragma unroll
     for (int k = 0; k < NY; ++k) F[5 + k] = 0.5 * (L[5 + k] * vnL + R[5 + k] * vnR) - maxvap * (R[5 + k] - L[5 + k]);
   }

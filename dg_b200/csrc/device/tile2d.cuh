@@ -108,14 +108,17 @@ constexpr bool kSfLift = DGB_SF_LIFT != 0;
 // barrier).  Every early return is taken by the whole CTA, after its last barrier.
 // NY passive mass fractions rho*Y_k follow the five gamma-model fields: conservative volume flux
 // rho*Y_k (u, v) (physics.cu:293-298) and the interface fluxes of phys::riemann2d_rcp.
-template <int P, int FLUX, int MODE, int TW, int TH, int UNROLL, int NY = 0>
+// GC: the GAMCONS model (fifth field rho/(gamma-1), conservative flux rho u/(gamma-1), no source;
+// physics.cu:253-281), with NY = 0.
+template <int P, int FLUX, int MODE, int TW, int TH, int UNROLL, int NY = 0, bool GC = false>
 __device__ __forceinline__ void tile2d_body(const TileArgs& a, const CUtensorMap* mapU, const CUtensorMap* mapB,
                                             int tx0, int ty0, unsigned char* smraw, uint32_t& phase) {
+  static_assert(!(GC && NY > 0), "GAMCONS with mass fractions is not built");
   using Dm = TileDims<P, TW, TH, NY>;
   constexpr int N1 = Dm::N1, NS = Dm::NS, NF = Dm::NF, NT = Dm::NT, NXF = Dm::NXF, NYF = Dm::NYF;
-  constexpr int FS = NF + 1;      // face record: NF fluxes, ncterm
-  constexpr int NFL = 4 + NY;     // fields with a volume flux: rho, rho u, rho v, E, rho Y_k
-  auto fld = [](int k) { return k < 4 ? k : k + 1; };
+  constexpr int FS = NF + 1;             // face record: NF fluxes, ncterm
+  constexpr int NFL = 4 + NY + (GC ? 1 : 0);  // fields with a volume flux (rho, rho u, rho v, E, alpha | rho Y_k)
+  auto fld = [](int k) { return (GC || k < 4) ? k : k + 1; };
   uint64_t* bar = reinterpret_cast<uint64_t*>(smraw);
   int* s_ok = reinterpret_cast<int*>(smraw + 8);
   int* codes = reinterpret_cast<int*>(smraw + Dm::head_bytes);  // [L: TH][R: TH][D: TW][U: TW]
@@ -247,7 +250,7 @@ __device__ __forceinline__ void tile2d_body(const TileArgs& a, const CUtensorMap
       R[f] = sr;
     }
     double F[NF], nc;
-    phys::riemann2d_rcp<FLUX, NY>(L, R, nxv, nyv, F, nc);
+    phys::riemann2d_rcp<FLUX, NY, GC>(L, R, nxv, nyv, F, nc);
     // boundary faces seen from the right/top element store -F so that every consumer forms
     // (+F + nc) on its left/bottom face and (-F + nc) on its right/top face
 #pragma unroll
@@ -344,7 +347,7 @@ __device__ __forceinline__ void tile2d_body(const TileArgs& a, const CUtensorMap
       for (int iy = 0; iy < N1; ++iy) { dax += DGB_TAB2(P, B1[gy][iy]) * dT[iy]; day += DGB_TAB2(P, D1[gy][iy]) * Tc[4][iy]; }
       const double rho = ug[0], irho = __drcp_rn(rho);
       const double uu = ug[1] * irho, vv = ug[2] * irho, Et = ug[3];
-      const double gm1 = __drcp_rn(ug[4]);
+      const double gm1 = GC ? rho * __drcp_rn(ug[4]) : __drcp_rn(ug[4]);  // gamma - 1
       const double p = gm1 * (Et - 0.5 * rho * (uu * uu + vv * vv));
       const double wx = DGB_TAB2(P, W[g]) * a.cx, wy = DGB_TAB2(P, W[g]) * a.cy;
       const double mx = ug[1] * wx, my = ug[2] * wy;
@@ -352,6 +355,7 @@ __device__ __forceinline__ void tile2d_body(const TileArgs& a, const CUtensorMap
       double gyv[NFL] = {my, my * uu, my * vv + wy * p, wy * ((Et + p) * vv)};
 #pragma unroll
       for (int k = 0; k < NY; ++k) { gxv[4 + k] = wx * (ug[5 + k] * uu); gyv[4 + k] = wy * (ug[5 + k] * vv); }
+      if constexpr (GC) { gxv[4] = wx * (ug[4] * uu); gyv[4] = wy * (ug[4] * vv); }
       const double gs = (DGB_TAB2(P, W[g]) * a.J) * (-uu * dax * a.sx - vv * day * a.sy);
       if constexpr (kSfLift) {
 #pragma unroll
@@ -359,14 +363,14 @@ __device__ __forceinline__ void tile2d_body(const TileArgs& a, const CUtensorMap
           const double b = DGB_TAB2(P, B1[gy][iy]), d = DGB_TAB2(P, D1[gy][iy]);
 #pragma unroll
           for (int f = 0; f < NFL; ++f) { Ax[f][iy] += b * gxv[f]; Ay[f][iy] += d * gyv[f]; }
-          As[iy] += b * gs;
+          if (!GC) As[iy] += b * gs;
         }
       } else {
 #pragma unroll
         for (int t = 0; t < NS; ++t) {
 #pragma unroll
           for (int f = 0; f < NFL; ++f) r[fld(f)][t] += DGB_TAB2(P, dPx[g][t]) * gxv[f] + DGB_TAB2(P, dPy[g][t]) * gyv[f];
-          r[4][t] += DGB_TAB2(P, Phi[g][t]) * gs;
+          if (!GC) r[4][t] += DGB_TAB2(P, Phi[g][t]) * gs;
         }
       }
     }
@@ -380,7 +384,7 @@ __device__ __forceinline__ void tile2d_body(const TileArgs& a, const CUtensorMap
           const int t = ix + N1 * iy;
 #pragma unroll
           for (int f = 0; f < NFL; ++f) r[fld(f)][t] += dx * Ax[f][iy] + bx * Ay[f][iy];
-          r[4][t] += bx * As[iy];
+          if (!GC) r[4][t] += bx * As[iy];
         }
     }
   }
@@ -440,7 +444,7 @@ __device__ __forceinline__ void tile2d_body(const TileArgs& a, const CUtensorMap
   }
 }
 
-template <int P, int FLUX, int MODE, int TW, int TH, int NY = 0>
+template <int P, int FLUX, int MODE, int TW, int TH, int NY = 0, bool GC = false>
 __global__ void __launch_bounds__(TW * TH, 2)
     residual2d_tile_kernel(const TileArgs a, const __grid_constant__ CUtensorMap mapU,
                            const __grid_constant__ CUtensorMap mapB) {
@@ -451,8 +455,8 @@ __global__ void __launch_bounds__(TW * TH, 2)
     fence_mbar_init();
   }
   uint32_t phase = 0;
-  tile2d_body<P, FLUX, MODE, TW, TH, vol_unroll<P>(), NY>(a, &mapU, &mapB, blockIdx.x * TW, blockIdx.y * TH, smraw,
-                                                         phase);
+  tile2d_body<P, FLUX, MODE, TW, TH, vol_unroll<P>(), NY, GC>(a, &mapU, &mapB, blockIdx.x * TW, blockIdx.y * TH,
+                                                             smraw, phase);
 }
 
 }  // namespace dgb

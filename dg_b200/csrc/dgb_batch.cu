@@ -369,7 +369,8 @@ extern "C" int dgb_batch_create(dgb_ctx* const* cases, int n, dgb_batch** out) {
     if (c->device != dev) return fail(set_error(DGB_ERR_ARG, "batch: cases on different devices"));
     for (int j = 0; j < i; ++j)
       if (cases[j] == c) return fail(set_error(DGB_ERR_ARG, "batch: a context appears twice"));
-    if (c->nmass != 0) return fail(set_error(DGB_ERR_UNSUPPORTED, "batch: cases without mass fractions"));
+    if (c->nmass != 0 || c->gamcons)
+      return fail(set_error(DGB_ERR_UNSUPPORTED, "batch: GAMNCON cases without mass fractions"));
     if (c->form != DGB_FORM_FP64 || c->ind_on || c->fused_lim)
       return fail(set_error(DGB_ERR_UNSUPPORTED, "batch: plain FP64 form with the two-pass limiter only"));
     if (c->limiter != DGB_LIM_NONE && c->limiter != DGB_LIM_HRL && c->limiter != DGB_LIM_M2L)

@@ -172,11 +172,11 @@ void launch_res2d(dgb_ctx* c, const StageArgs& a) {
   k<<<grid, RES2D_NT, smem, c->st>>>(c->cs, a);
 }
 
-template <int P, int FLUX, int MODE, int NY = 0>
+template <int P, int FLUX, int MODE, int NY = 0, bool GC = false>
 void launch_res1d(dgb_ctx* c, const StageArgs& a) {
   const int grid = (c->ne + 127) / 128;
   ProfScope ps(c, KC_RESIDUAL);
-  residual1d_kernel<P, FLUX, MODE, NY><<<grid, 128, 0, c->st>>>(c->cs, a);
+  residual1d_kernel<P, FLUX, MODE, NY, GC><<<grid, 128, 0, c->st>>>(c->cs, a);
 }
 
 constexpr int TILE_W = 32, TILE_H = 4;
@@ -190,12 +190,12 @@ const CUtensorMap& map_of(dgb_ctx* c, const double* p) {
   return c->mapA;
 }
 
-template <int P, int FLUX, int MODE, int NY = 0>
+template <int P, int FLUX, int MODE, int NY = 0, bool GC = false>
 void launch_tile2d(dgb_ctx* c, const StageArgs& s) {
   constexpr int TH = tile_h_for(P);
   using Dm = TileDims<P, TILE_W, TH, NY>;
   constexpr size_t smem = Dm::smem_bytes;
-  auto k = residual2d_tile_kernel<P, FLUX, MODE, TILE_W, TH, NY>;
+  auto k = residual2d_tile_kernel<P, FLUX, MODE, TILE_W, TH, NY, GC>;
   static bool attr = false;
   if (!attr) { cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem); attr = true; }
   TileArgs a;
@@ -282,6 +282,25 @@ int residual_dispatch(dgb_ctx* c, const StageArgs& a) {
       case 32: launch_tile2d_mixed<3, 2, MODE>(c, a); return 0;
       default: return set_error(DGB_ERR_UNSUPPORTED, "mixed form: p = 1..3 with Rusanov or Roe");
     }
+  }
+  if (c->gamcons) {  // GAMCONS: tiled 2D or 1D, FP64 form, no mass fractions (checked at create)
+    if (c->D == 2) {
+      switch (c->p * 10 + c->flux) {
+        case 10: launch_tile2d<1, 0, MODE, 0, true>(c, a); return 0;
+        case 12: launch_tile2d<1, 2, MODE, 0, true>(c, a); return 0;
+        case 20: launch_tile2d<2, 0, MODE, 0, true>(c, a); return 0;
+        case 22: launch_tile2d<2, 2, MODE, 0, true>(c, a); return 0;
+        case 30: launch_tile2d<3, 0, MODE, 0, true>(c, a); return 0;
+        case 32: launch_tile2d<3, 2, MODE, 0, true>(c, a); return 0;
+        default: return set_error(DGB_ERR_UNSUPPORTED, "no GAMCONS residual kernel for this (p, flux)");
+      }
+    }
+#define R1G(P, F) case P * 10 + F: launch_res1d<P, F, MODE, 0, true>(c, a); return 0;
+    switch (c->p * 10 + c->flux) {
+      R1G(1, 0) R1G(1, 1) R1G(1, 2) R1G(2, 0) R1G(2, 1) R1G(2, 2) R1G(3, 0) R1G(3, 1) R1G(3, 2)
+      default: return set_error(DGB_ERR_UNSUPPORTED, "no GAMCONS residual kernel for this (p, flux)");
+    }
+#undef R1G
   }
   if (c->tiled && c->nmass == 1) {
     switch (c->p * 10 + c->flux) {
@@ -556,6 +575,17 @@ void launch_dt(dgb_ctx* c, const double* U, bool cfl) {
   ProfScope ps(c, KC_DT);
   if (cfl) {
     const int grid = std::max(1, std::min(4 * 148, (c->ne + 255) / 256));
+    if (c->gamcons) {
+      switch (c->D * 100 + c->ns) {
+        case 102: wavespeed_kernel<1, 2, true><<<grid, 256, 0, c->st>>>(U, c->ne, c->ld, c->scal); break;
+        case 103: wavespeed_kernel<1, 3, true><<<grid, 256, 0, c->st>>>(U, c->ne, c->ld, c->scal); break;
+        case 104: wavespeed_kernel<1, 4, true><<<grid, 256, 0, c->st>>>(U, c->ne, c->ld, c->scal); break;
+        case 204: wavespeed_kernel<2, 4, true><<<grid, 256, 0, c->st>>>(U, c->ne, c->ld, c->scal); break;
+        case 209: wavespeed_kernel<2, 9, true><<<grid, 256, 0, c->st>>>(U, c->ne, c->ld, c->scal); break;
+        case 216: wavespeed_kernel<2, 16, true><<<grid, 256, 0, c->st>>>(U, c->ne, c->ld, c->scal); break;
+        default: break;
+      }
+    } else
     switch (c->D * 100 + c->ns) {
       case 102: wavespeed_kernel<1, 2><<<grid, 256, 0, c->st>>>(U, c->ne, c->ld, c->scal); break;
       case 103: wavespeed_kernel<1, 3><<<grid, 256, 0, c->st>>>(U, c->ne, c->ld, c->scal); break;
@@ -716,6 +746,21 @@ extern "C" int dgb_create(const dgb_problem* prob, int device, dgb_ctx** out) {
   c->fused_lim = c->rowmajor && (P.limiter == DGB_LIM_HRL || P.limiter == DGB_LIM_M2L) &&
                  std::getenv("DGB_FUSED_LIMITER") != nullptr && P.N_Y == 0;
   c->nmass = P.N_Y;
+  c->gamcons = P.gamcons;
+  if (P.gamcons) {
+    const char* why = nullptr;
+    if (P.N_Y != 0) why = "GAMCONS with mass fractions is not on the device path";
+    else if (P.D == 2 && !c->tiled)
+      why = "GAMCONS in 2D needs a structured row-major grid with nx a multiple of 32 and ny of 4 (p = 3: 2)";
+    else if (P.limiter == DGB_LIM_M2L)  // M2limiting stops there too (limiting.cc:193-194, 410-411)
+      why = "M2L is only implemented for gamncon";
+    else if (P.limiter != DGB_LIM_NONE && P.limiter != DGB_LIM_HRL)
+      why = "with GAMCONS the limiter is none or hrl";
+    else if (!P.thresholds.empty())
+      why = "the troubled-cell sensors are built for GAMNCON";
+    if (why) { delete c; return set_error(DGB_ERR_UNSUPPORTED, why); }
+    c->fused_lim = false;
+  }
   if (P.N_Y > 1) { delete c; return set_error(DGB_ERR_UNSUPPORTED, "at most one mass fraction on the device path"); }
   if (P.N_Y == 1 && P.D == 2 && !c->tiled) {
     delete c;
@@ -906,8 +951,8 @@ extern "C" int dgb_mlp_param_count(void) { return MLP_NPARAM; }
 
 extern "C" int dgb_indicator_features(dgb_ctx* c, float* X_dev) {
   if (!c || !X_dev) return set_error(DGB_ERR_ARG, "null argument");
-  if (c->D != 2 || c->p != 2 || c->nmass != 0)
-    return set_error(DGB_ERR_UNSUPPORTED, "the indicator is built for 2D, p = 2, without mass fractions");
+  if (c->D != 2 || c->p != 2 || c->nmass != 0 || c->gamcons)
+    return set_error(DGB_ERR_UNSUPPORTED, "the indicator is built for 2D, p = 2, GAMNCON, without mass fractions");
   DGB_CUDA(cudaSetDevice(c->device));
   indicator_features_kernel<2><<<(c->ne + 127) / 128, 128, 0, c->st>>>(c->A, c->ld, c->ne, c->nbr, X_dev);
   DGB_CUDA(cudaGetLastError());
@@ -917,8 +962,8 @@ extern "C" int dgb_indicator_features(dgb_ctx* c, float* X_dev) {
 
 extern "C" int dgb_indicator_labels(dgb_ctx* c, float* y_dev) {
   if (!c || !y_dev) return set_error(DGB_ERR_ARG, "null argument");
-  if (c->D != 2 || c->p != 2 || c->nmass != 0)
-    return set_error(DGB_ERR_UNSUPPORTED, "the indicator is built for 2D, p = 2, without mass fractions");
+  if (c->D != 2 || c->p != 2 || c->nmass != 0 || c->gamcons)
+    return set_error(DGB_ERR_UNSUPPORTED, "the indicator is built for 2D, p = 2, GAMNCON, without mass fractions");
   if (c->limiter == 0) return set_error(DGB_ERR_ARG, "labels need a limiter");
   DGB_CUDA(cudaSetDevice(c->device));
   if (int rc = reset_scalars(c, 0.0)) return rc;
@@ -991,7 +1036,7 @@ extern "C" int dgb_set_indicator(dgb_ctx* c, const float* params, float threshol
     c->ind_on = false;
     return DGB_OK;
   }
-  if (c->D != 2 || c->p != 2 || c->limiter != DGB_LIM_M2L || c->nmass != 0)
+  if (c->D != 2 || c->p != 2 || c->limiter != DGB_LIM_M2L || c->nmass != 0 || c->gamcons)
     return set_error(DGB_ERR_UNSUPPORTED,
                      "the learned indicator gates the m2l limiter of 2D p = 2 problems without mass fractions");
   if (!c->ind_params) {
@@ -1047,7 +1092,7 @@ extern "C" int dgb_indicator_scores(dgb_ctx* c, const double* U, float* score, i
 extern "C" int dgb_set_form(dgb_ctx* c, int form) {
   if (!c) return set_error(DGB_ERR_ARG, "null argument");
   if (form != DGB_FORM_FP64 && form != DGB_FORM_MIXED) return set_error(DGB_ERR_ARG, "unknown form");
-  if (form == DGB_FORM_MIXED && !(c->tiled && c->flux != DGB_FLUX_HLL && c->nmass == 0))
+  if (form == DGB_FORM_MIXED && !(c->tiled && c->flux != DGB_FLUX_HLL && c->nmass == 0 && !c->gamcons))
     return set_error(DGB_ERR_UNSUPPORTED,
                      "the mixed form needs a structured 2D grid with nx a multiple of 32 and ny of 4 (p = 3: 2), "
                      "Rusanov or Roe");

@@ -154,7 +154,8 @@ extern "C" int dgb_limit_noalloc(const dgb_problem* prob, const double* U_in_dev
   if (!prob || !U_in_dev || !U_out_dev) return set_error(DGB_ERR_ARG, "null argument");
   const Problem& P = dgb_problem_ref(prob);
   if (!P.gpu_ok) return set_error(DGB_ERR_UNSUPPORTED, P.gpu_reason);
-  if (P.N_Y != 0) return set_error(DGB_ERR_UNSUPPORTED, "dgb_limit_noalloc: problems without mass fractions");
+  if (P.N_Y != 0 || P.gamcons)
+    return set_error(DGB_ERR_UNSUPPORTED, "dgb_limit_noalloc: GAMNCON problems without mass fractions");
   if (P.limiter != DGB_LIM_HRL && P.limiter != DGB_LIM_M2L)
     return set_error(DGB_ERR_UNSUPPORTED, "dgb_limit_noalloc supports the hrl and m2l limiters");
   const int ld = (P.N_E + 63) / 64 * 64;

@@ -62,6 +62,7 @@ struct Problem {
   int N_Y = 0;                        // passive mass fractions rho*Y_k, fields D+3 .. N_F-1
   int flux = 2, limiter = 0;
   bool error_output = false;          // deck "#Make options" ERRR=ERROR: error.dat after the run
+  bool gamcons = false;               // GAMCONS gamma model: field D+2 holds rho/(gamma-1)
   double cfl = -1.0;
   std::vector<double> thresholds;
   std::vector<double> output_times;
@@ -118,7 +119,7 @@ bool invert(std::vector<double>& A, int n);  // column-major in-place inverse (p
 // setup.cc
 Status build_problem(Mesh&& mesh, int dim, int order, const std::string& elem_kind, int flux, int limiter,
                      double cfl, const std::vector<double>& thresholds, const std::vector<double>& out_times,
-                     double final_time, Problem& P, int n_mass = 0);
+                     double final_time, Problem& P, int n_mass = 0, bool gamcons = false);
 Status init_state(const Problem& P, const std::string& ic, const std::vector<double>& params, uint64_t seed,
                   double* U);
 Status write_pos(const Problem& P, const double* U, int step, double time, const std::string& dir);

@@ -62,9 +62,12 @@ extern "C" int dgb_problem_from_deck(const char* deck_path, dgb_problem** out) {
   int n_mass = 0;
   mo = d.make_options.find("MASS");
   if (mo != d.make_options.end()) n_mass = std::atoi(mo->second.c_str());
+  bool gamcons = false;
   mo = d.make_options.find("GAMM");
-  if (mo != d.make_options.end() && mo->second != "GAMNCON")
-    return set_error(DGB_ERR_UNSUPPORTED, "only the GAMNCON gamma model is on the device path");
+  if (mo != d.make_options.end()) {
+    if (mo->second == "GAMCONS") gamcons = true;
+    else if (mo->second != "GAMNCON") return set_error(DGB_ERR_ARG, "unknown GAMM " + mo->second);
+  }
   if (d.order < 1) return set_error(DGB_ERR_UNSUPPORTED, "order 0 is outside the device path");
   // output times (RK constructor, rk.h:61-84); the intended (int)(Tf/DtOut)+1 count is used
   std::vector<double> outt = d.output_times;
@@ -83,7 +86,7 @@ extern "C" int dgb_problem_from_deck(const char* deck_path, dgb_problem** out) {
   if (!st.ok()) return set_error(st.code, st.msg);
   auto* pr = new dgb_problem();
   st = dgb::build_problem(std::move(m), dim, d.order, d.elem_type, flux, limiter_code(d.limiter), d.cfl,
-                          d.thresholds, outt, tf, pr->P, n_mass);
+                          d.thresholds, outt, tf, pr->P, n_mass, gamcons);
   if (!st.ok()) { delete pr; return set_error(st.code, st.msg); }
   pr->P.deck_dir = dir;
   mo = d.make_options.find("ERRR");
@@ -119,10 +122,12 @@ extern "C" int dgb_problem_structured(const dgb_mesh_spec* mesh, const dgb_optio
   if (opt->flux < 0 || opt->flux > 2) return set_error(DGB_ERR_ARG, "bad flux");
   if (opt->limiter < 0 || opt->limiter > 7) return set_error(DGB_ERR_ARG, "bad limiter");
   if (opt->n_mass < 0 || opt->n_mass > 10) return set_error(DGB_ERR_ARG, "n_mass must be 0..10");
+  if (opt->gamma_model != DGB_GAMNCON && opt->gamma_model != DGB_GAMCONS) return set_error(DGB_ERR_ARG, "bad gamma model");
   std::vector<double> th(opt->thresholds, opt->thresholds + std::max(0, std::min(3, opt->n_thresholds)));
   auto* pr = new dgb_problem();
   dgb::Status st = dgb::build_problem(mesh_from_spec(mesh), mesh->dim, mesh->order, mesh->dim == 1 ? "lin" : "qua",
-                                      opt->flux, opt->limiter, opt->cfl, th, {}, 0.0, pr->P, opt->n_mass);
+                                      opt->flux, opt->limiter, opt->cfl, th, {}, 0.0, pr->P, opt->n_mass,
+                                      opt->gamma_model == DGB_GAMCONS);
   if (!st.ok()) { delete pr; return set_error(st.code, st.msg); }
   *out = pr;
   return DGB_OK;
@@ -154,6 +159,7 @@ extern "C" int dgb_problem_info(const dgb_problem* p, dgb_info* o) {
   o->final_time = P.final_time;
   o->n_output_times = (int)P.output_times.size();
   o->error_output = P.error_output ? 1 : 0;
+  o->gamma_model = P.gamcons ? DGB_GAMCONS : DGB_GAMNCON;
   return DGB_OK;
 }
 

@@ -110,7 +110,7 @@ Status fail(int code, const std::string& msg) { Status s; s.code = code; s.msg =
 
 Status build_problem(Mesh&& mesh, int dim, int p, const std::string& kind, int flux, int limiter, double cfl,
                      const std::vector<double>& thresholds, const std::vector<double>& out_times, double final_time,
-                     Problem& P, int n_mass) {
+                     Problem& P, int n_mass, bool gamcons) {
   P = Problem();
   if (dim != 1 && dim != 2) return fail(1, "dimension must be 1 or 2");
   if (n_mass < 0 || n_mass > 10) return fail(1, "mass fractions: 0..10 (MASS of the reference Makefile)");
@@ -120,6 +120,7 @@ Status build_problem(Mesh&& mesh, int dim, int p, const std::string& kind, int f
   P.D = dim;
   P.p = p;
   P.N_Y = n_mass;
+  P.gamcons = gamcons;
   P.N_F = (dim == 1 ? 4 : 5) + n_mass;
   P.flux = flux;
   P.limiter = limiter;
@@ -559,14 +560,14 @@ Status init_state(const Problem& P, const std::string& ic, const std::vector<dou
       u[(e * NF + 0) * NS + i] = rho;
       u[(e * NF + 1) * NS + i] = rho * vx;
       u[(e * NF + 2) * NS + i] = 1.0 / (g - 1.0) * pr + 0.5 * rho * vx * vx;
-      u[(e * NF + 3) * NS + i] = 1.0 / (g - 1.0);
+      u[(e * NF + 3) * NS + i] = P.gamcons ? rho / (g - 1.0) : 1.0 / (g - 1.0);
     } else {
       const double rho = prim[0], vx = prim[1], vy = prim[2], pr = prim[3], g = prim[4];
       u[(e * NF + 0) * NS + i] = rho;
       u[(e * NF + 1) * NS + i] = rho * vx;
       u[(e * NF + 2) * NS + i] = rho * vy;
       u[(e * NF + 3) * NS + i] = 1.0 / (g - 1.0) * pr + 0.5 * rho * (vx * vx + vy * vy);
-      u[(e * NF + 4) * NS + i] = 1.0 / (g - 1.0);
+      u[(e * NF + 4) * NS + i] = P.gamcons ? rho / (g - 1.0) : 1.0 / (g - 1.0);
     }
   };
   std::mt19937_64 rng(seed);
@@ -720,6 +721,7 @@ Status error_norms(const Problem& P, const double* U, const double* Uexact, doub
       for (int i = 0; i < NS; ++i) {
         double* f = &V[(size_t)e * NF * NS + i];
         f[1 * NS] = f[1 * NS] / f[0];
+        if (P.gamcons) f[3 * NS] = f[3 * NS] / f[0];
         f[2 * NS] = 1.0 / f[3 * NS] * (f[2 * NS] - 0.5 * f[0] * f[1 * NS] * f[1 * NS]);
       }
     return V;
@@ -775,7 +777,7 @@ Status write_pos(const Problem& P, const double* U, int step, double time, const
       const double ux = U[(e * NF + 1) * NS + i] / rho;
       if (P.D == 1) {
         const double et = U[(e * NF + 2) * NS + i];
-        const double g = 1 + 1.0 / U[(e * NF + 3) * NS + i];
+        const double g = P.gamcons ? 1 + rho / U[(e * NF + 3) * NS + i] : 1 + 1.0 / U[(e * NF + 3) * NS + i];
         out[(e * NF + 0) * NS + i] = rho;
         out[(e * NF + 1) * NS + i] = ux;
         out[(e * NF + 2) * NS + i] = g;
@@ -783,7 +785,7 @@ Status write_pos(const Problem& P, const double* U, int step, double time, const
       } else {
         const double uy = U[(e * NF + 2) * NS + i] / rho;
         const double et = U[(e * NF + 3) * NS + i];
-        const double g = 1 + 1.0 / U[(e * NF + 4) * NS + i];
+        const double g = P.gamcons ? 1 + rho / U[(e * NF + 4) * NS + i] : 1 + 1.0 / U[(e * NF + 4) * NS + i];
         out[(e * NF + 0) * NS + i] = rho;
         out[(e * NF + 1) * NS + i] = ux;
         out[(e * NF + 2) * NS + i] = uy;
@@ -848,14 +850,14 @@ Status read_pos(const Problem& P, int step, const std::string& dir, double& time
         U[(e * NF + 0) * NS + i] = rho;
         U[(e * NF + 1) * NS + i] = rho * ux;
         U[(e * NF + 2) * NS + i] = pr / (g - 1) + 0.5 * rho * ux * ux;
-        U[(e * NF + 3) * NS + i] = 1.0 / (g - 1);
+        U[(e * NF + 3) * NS + i] = P.gamcons ? rho / (g - 1) : 1.0 / (g - 1);
       } else {
         const double uy = out[(e * NF + 2) * NS + i], g = out[(e * NF + 3) * NS + i], pr = out[(e * NF + 4) * NS + i];
         U[(e * NF + 0) * NS + i] = rho;
         U[(e * NF + 1) * NS + i] = rho * ux;
         U[(e * NF + 2) * NS + i] = rho * uy;
         U[(e * NF + 3) * NS + i] = pr / (g - 1) + 0.5 * rho * (ux * ux + uy * uy);
-        U[(e * NF + 4) * NS + i] = 1.0 / (g - 1);
+        U[(e * NF + 4) * NS + i] = P.gamcons ? rho / (g - 1) : 1.0 / (g - 1);
       }
       for (int k = NF - P.N_Y; k < NF; ++k) U[(e * NF + k) * NS + i] = rho * out[(e * NF + k) * NS + i];
     }

@@ -38,10 +38,11 @@ class Problem:
     def structured(cls, dim: int, order: int, nx: int, ny: int = 1, x0: float = 0.0, x1: float = 1.0,
                    y0: float = 0.0, y1: float = 1.0, bc: Sequence[str | int] = ("transmissive",) * 4,
                    flux: str = "roe", limiter: str = "m2l", cfl: float = -1.0,
-                   thresholds: Iterable[float] = (), n_mass: int = 0) -> "Problem":
+                   thresholds: Iterable[float] = (), n_mass: int = 0, gamma_model: str = "gamncon") -> "Problem":
         spec = mesh_spec(dim, order, nx, ny, x0, x1, y0, y1, bc)
         opt = F.Options()
         opt.n_mass = int(n_mass)
+        opt.gamma_model = F.GAMMA_MODEL[gamma_model.lower()]
         opt.flux = F.FLUX[flux.lower()]
         opt.limiter = F.LIMITER[limiter.lower()]
         opt.cfl = cfl

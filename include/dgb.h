@@ -67,6 +67,10 @@ enum dgb_limiter {
  * state, pressure recovery, Roe solver and stage update in FP64 (structured 2D grids, p <= 3). */
 enum dgb_form { DGB_FORM_FP64 = 0, DGB_FORM_MIXED = 1 };
 
+/* Gamma model (GAMM of the reference Makefile): GAMNCON carries alpha = 1/(gamma-1) with a
+ * non-conservative source, GAMCONS carries rho/(gamma-1) conservatively. */
+enum dgb_gamma_model { DGB_GAMNCON = 0, DGB_GAMCONS = 1 };
+
 /* Time integrators: classical RK4 (reference rk.h:44-57) and Shu-Osher SSP-RK3 (new). */
 enum dgb_scheme { DGB_SSPRK3 = 3, DGB_RK4 = 4 };
 
@@ -101,12 +105,13 @@ typedef struct {
   int n_thresholds;
   int n_mass;          /* passive mass fractions rho*Y_k appended to the state (MASS of the
                         * reference Makefile; N_F = 4 (1D) / 5 (2D) + n_mass) */
+  int gamma_model;     /* enum dgb_gamma_model */
 } dgb_options;
 
 /* Reads a reference input deck (format of code/src/deck/deck.cc:11-64) and the Gmsh 2.2 mesh
  * it names (path relative to the deck's directory).  The flux comes from the deck's optional
  * "#Make options" block (FLUX=ROE|RUS|HLL, the block tests/runtests.py:80-87 reads), else ROE;
- * MASS=n there gives n passive mass fractions. */
+ * MASS=n there gives n passive mass fractions, GAMM=GAMCONS the conservative gamma model. */
 int dgb_problem_from_deck(const char* deck_path, dgb_problem** out);
 /* Builds the same problem from an in-memory structured mesh (identical to reading the file
  * that dgb_mesh_write_msh writes for the same spec). */
@@ -128,6 +133,7 @@ typedef struct {
   double final_time;
   int n_output_times;
   int error_output;              /* deck "#Make options" ERRR=ERROR: error.dat after the run */
+  int gamma_model;               /* enum dgb_gamma_model */
 } dgb_info;
 
 int dgb_problem_info(const dgb_problem* p, dgb_info* out);

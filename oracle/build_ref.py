@@ -9,7 +9,8 @@ set with oracle/ref_harness.cc into ``oracle/_ref/dgref_<variant>``.  Outputs go
 Compile-time configuration follows code/Makefile:147-156 (DEFINES) for the gamma-model
 multifluid build: USE_CPU, USE_DOUBLE, MULTIFLUID, GAMNCON, NO_MPI, N_Y=0, and
 N_F=4 (1D) / 5 (2D), D=1/2, DF=1, with the flux flag ROE, RUS or HLL; and the same with one
-passive mass fraction (N_Y=1, N_F=5 / 6; variants *_y1).
+passive mass fraction (N_Y=1, N_F=5 / 6; variants *_y1); GAMCONS in place of GAMNCON (variants
+*_gc); ERROR in place of NOERROR (variant 1d_rus_err).
 
 Out-of-tree additions (none of them touch reference arithmetic):
   * an empty ``gsl/gsl_integration.h`` (code/src/ic/init_cond.cc:10 includes it, never calls it);
@@ -50,6 +51,12 @@ VARIANTS = {
     "2d_rus_y1": dict(dims="TWOD", nf=6, d=2, flux="RUS", ny=1),
     # the ERROR diagnostic compiled in (ERRR=ERROR in code/Makefile): error.dat after the run
     "1d_rus_err": dict(dims="ONED", nf=4, d=1, flux="RUS", err=True),
+    # the conservative gamma model (GAMM=GAMCONS in code/Makefile): rho/(gamma-1) as the field
+    "1d_roe_gc": dict(dims="ONED", nf=4, d=1, flux="ROE", gc=True),
+    "1d_rus_gc": dict(dims="ONED", nf=4, d=1, flux="RUS", gc=True),
+    "1d_hll_gc": dict(dims="ONED", nf=4, d=1, flux="HLL", gc=True),
+    "2d_roe_gc": dict(dims="TWOD", nf=5, d=2, flux="ROE", gc=True),
+    "2d_rus_gc": dict(dims="TWOD", nf=5, d=2, flux="RUS", gc=True),
 }
 
 RK_SYM = ("_ZN2RK14RK_integrationEdiiiiiiiPdS0_R8LimitingbR9DG_SOLVERR12COMMUNICATORR7PRINTER"
@@ -58,7 +65,7 @@ RK_SYM = ("_ZN2RK14RK_integrationEdiiiiiiiPdS0_R8LimitingbR9DG_SOLVERR12COMMUNIC
 
 def defines(v: dict) -> list[str]:
     return ["-DHAVE_BLAS", "-DHAVE_LAPACK", "-DUSE_CPU", "-DHOME", "-DUSE_DOUBLE", "-DMULTIFLUID",
-            "-DGAMNCON", f"-D{v['flux']}", f"-D{v['dims']}", "-DNO_MPI", f"-DN_Y={v.get('ny', 0)}", f"-DN_F={v['nf']}",
+            "-DGAMCONS" if v.get("gc") else "-DGAMNCON", f"-D{v['flux']}", f"-D{v['dims']}", "-DNO_MPI", f"-DN_Y={v.get('ny', 0)}", f"-DN_F={v['nf']}",
             "-DERROR" if v.get("err") else "-DNOERROR", "-DNOCONS", f"-DD={v['d']}", "-DDF=1"]
 
 

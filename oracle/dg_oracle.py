@@ -4,7 +4,9 @@ TEST INFRASTRUCTURE ONLY.  This module is the checker: only ``tests/``, ``__graf
 and the ``cpu_baseline`` leg of ``bench.py`` import it.  The product (``dg_b200``) never calls it
 and has no CPU fallback.
 
-It restates, for the gamma-model (GAMNCON, N_Y = 0) multifluid Euler equations in 1D and 2D,
+It restates, for the gamma-model multifluid Euler equations in 1D and 2D (GAMNCON, where the
+last gamma-model field is 1/(gamma-1) with a non-conservative source, and GAMCONS, where it is
+rho/(gamma-1) transported conservatively; with passive mass fractions rho*Y_k appended),
 the arithmetic of the reference's CPU build, operating on the reference's own setup arrays
 (phi, dphi, psi, J, invJac, JF, normals, map, invmap, boundaryMap, neighbors, Minv and the
 Lagrange<->monomial transforms) in the reference's own layouts:
@@ -60,6 +62,7 @@ class Setup:
     gx: float = 0.0          # constants::GLOBAL_GX / GLOBAL_GY (zero unless an IC sets gravity)
     gy: float = 0.0
     thresholds: tuple = ()   # "#sensor thresholds" of the deck (sensor.h:35-45)
+    gamcons: bool = False    # GAMCONS gamma model (Makefile GAMM=GAMCONS)
 
     @property
     def order(self) -> int:
@@ -73,7 +76,7 @@ class Setup:
         return cls(D=rm["D"], N_F=rm["N_F"], N_E=rm["N_E"], N_s=rm["N_s"], N_G=rm["N_G"], M_T=rm["M_T"],
                    M_s=rm["M_s"], M_G=rm["M_G"], N_N=rm["N_N"], flux=meta["flux"], limiter=meta["limiter"],
                    cfl_scaled=rm["cfl_scaled"], n_reflective=rm.get("rflctive", 0), a=arrays,
-                   thresholds=tuple(meta.get("thresholds", ())))
+                   thresholds=tuple(meta.get("thresholds", ())), gamcons=meta.get("gamma_model") == "gamcons")
 
     @classmethod
     def from_problem(cls, prob, thresholds=()) -> "Setup":
@@ -89,17 +92,21 @@ class Setup:
                 pass
         return cls(D=i.dim, N_F=i.n_fields, N_E=i.n_elem, N_s=i.n_s, N_G=i.n_g, M_T=i.n_ifaces, M_s=i.m_s,
                    M_G=i.m_g, N_N=i.n_n, flux=names[i.flux], limiter=lims[i.limiter], cfl_scaled=i.cfl_scaled,
-                   n_reflective=i.n_reflective, a=arrays, thresholds=tuple(thresholds))
+                   n_reflective=i.n_reflective, a=arrays, thresholds=tuple(thresholds),
+                   gamcons=getattr(i, "gamma_model", 0) == 1)
 
 
 # ---------------------------------------------------------------------------------------------
 # interface Riemann solvers (vectorised over face points); each returns (F, nc) with shape (N_F, n)
 # ---------------------------------------------------------------------------------------------
 
-def _twod_rusanov(rhoL, rhoR, vxL, vxR, vyL, vyR, EtL, EtR, alL, alR, nx, ny, YL=(), YR=()):
-    """twod_multifluid_rusanov, code/src/face_fluxes/twod_multifluid_fluxes.h:30-97 (GAMNCON); the
-    mass fractions rho*Y_k (YL, YR) by the MACRO block at :89-94, whose dissipation term sits
-    outside the 1/2."""
+def _twod_rusanov(rhoL, rhoR, vxL, vxR, vyL, vyR, EtL, EtR, alL, alR, nx, ny, YL=(), YR=(), gc=False):
+    """twod_multifluid_rusanov, code/src/face_fluxes/twod_multifluid_fluxes.h:30-97; the mass
+    fractions rho*Y_k (YL, YR) by the MACRO block at :89-94, whose dissipation term sits outside
+    the 1/2.  gc (GAMCONS): alL, alR are the stored rho/(gamma-1) divided by the density by the
+    caller (:50-53, where the right alpha is set to the already divided left one divided by rhoL
+    again, which the caller reproduces), and the fifth flux is the conservative rho*alpha*vn with its dissipation
+    (:82-84), with no non-conservative term."""
     vnL = vxL * nx + vyL * ny
     vnR = vxR * nx + vyR * ny
     gL = 1.0 + 1.0 / alL
@@ -119,15 +126,19 @@ def _twod_rusanov(rhoL, rhoR, vxL, vxR, vyL, vyR, EtL, EtR, alL, alR, nx, ny, YL
     F[1] = 0.5 * ((rhoL * vnL * vxL + pL * nx) + (rhoR * vnR * vxR + pR * nx) - lam * (rhoR * vxR - rhoL * vxL))
     F[2] = 0.5 * ((rhoL * vnL * vyL + pL * ny) + (rhoR * vnR * vyR + pR * ny) - lam * (rhoR * vyR - rhoL * vyL))
     F[3] = 0.5 * (rhoL * vnL * HL + rhoR * vnR * HR - lam * (EtR - EtL))
-    F[4] = 0.5 * (-lam * (alR - alL))
-    nc[4] = -0.5 * 0.5 * (vnL + vnR) * (alR - alL)
+    if gc:
+        F[4] = 0.5 * (rhoL * vnL * alL + rhoR * vnR * alR - lam * (rhoR * alR - rhoL * alL))
+    else:
+        F[4] = 0.5 * (-lam * (alR - alL))
+        nc[4] = -0.5 * 0.5 * (vnL + vnR) * (alR - alL)
     return F, nc
 
 
-def _twod_roe(rhoL, rhoR, vxL, vxR, vyL, vyR, EtL, EtR, alL, alR, nx, ny, YL=(), YR=()):
-    """twod_multifluid_roe, twod_multifluid_fluxes.h:151-342 (GAMNCON): Roe averages, wave
-    strengths dV0..dV4 and right eigenvectors R of the gamma-model system; mass fractions by the
-    Roe-averaged Y and its wave strength (:307-319)."""
+def _twod_roe(rhoL, rhoR, vxL, vxR, vyL, vyR, EtL, EtR, alL, alR, nx, ny, YL=(), YR=(), gc=False):
+    """twod_multifluid_roe, twod_multifluid_fluxes.h:151-342: Roe averages, wave strengths
+    dV0..dV4 and right eigenvectors R of the gamma-model system; mass fractions by the
+    Roe-averaged Y and its wave strength (:307-319).  gc (GAMCONS): divided alphas (:175-178) and
+    the central part 0.5 (rho alpha vn)_L + (rho alpha vn)_R in the fifth flux (:294-299)."""
     tx, ty = -ny, nx
     vnL = vxL * nx + vyL * ny
     vnR = vxR * nx + vyR * ny
@@ -183,14 +194,18 @@ def _twod_roe(rhoL, rhoR, vxL, vxR, vyL, vyR, EtL, EtR, alL, alR, nx, ny, YL=(),
     F[1] = 0.5 * ((rhoL * vnL * vxL + pL * nx) + (rhoR * vnR * vxR + pR * nx)) - 0.5 * diss(1)
     F[2] = 0.5 * ((rhoL * vnL * vyL + pL * ny) + (rhoR * vnR * vyR + pR * ny)) - 0.5 * diss(2)
     F[3] = 0.5 * (rhoL * vnL * HL + rhoR * vnR * HR) - 0.5 * diss(3)
-    F[4] = -0.5 * diss(4)
-    nc[4] = -0.5 * vn * (alR - alL)
+    if gc:
+        F[4] = 0.5 * (rhoL * vnL * alL + rhoR * vnR * alR) - 0.5 * diss(4)
+    else:
+        F[4] = -0.5 * diss(4)
+        nc[4] = -0.5 * vn * (alR - alL)
     return F, nc
 
 
-def _oned_rusanov(rhoL, rhoR, vxL, vxR, EtL, EtR, alL, alR, nx, YL=(), YR=()):
-    """oned_multifluid_rusanov, code/src/face_fluxes/oned_multifluid_fluxes.h:30-94 (GAMNCON); mass
-    fractions by the MACRO block at :88-92 (dissipation outside the 1/2)."""
+def _oned_rusanov(rhoL, rhoR, vxL, vxR, EtL, EtR, alL, alR, nx, YL=(), YR=(), gc=False):
+    """oned_multifluid_rusanov, code/src/face_fluxes/oned_multifluid_fluxes.h:30-94; mass fractions
+    by the MACRO block at :88-92 (dissipation outside the 1/2).  gc (GAMCONS; alphas divided by
+    the caller, :46-49): conservative rho*alpha*u flux with its dissipation (:78-81)."""
     gL = 1.0 + 1.0 / alL
     gR = 1.0 + 1.0 / alR
     pL = (gL - 1) * (EtL - 0.5 * rhoL * vxL * vxL)
@@ -205,8 +220,11 @@ def _oned_rusanov(rhoL, rhoR, vxL, vxR, EtL, EtR, alL, alR, nx, YL=(), YR=()):
     F[0] = 0.5 * ((rhoL * vxL + rhoR * vxR) * nx - lam * (rhoR - rhoL))
     F[1] = 0.5 * ((rhoL * vxL * vxL + pL + rhoR * vxR * vxR + pR) * nx - lam * (rhoR * vxR - rhoL * vxL))
     F[2] = 0.5 * (((EtL + pL) * vxL + (EtR + pR) * vxR) * nx - lam * (EtR - EtL))
-    F[3] = 0.5 * (-lam * (alR - alL))
-    nc[3] = -0.5 * 0.5 * (vxL + vxR) * (alR - alL) * nx
+    if gc:
+        F[3] = 0.5 * ((rhoL * vxL * alL + rhoR * vxR * alR) * nx - lam * (rhoR * alR - rhoL * alL))
+    else:
+        F[3] = 0.5 * (-lam * (alR - alL))
+        nc[3] = -0.5 * 0.5 * (vxL + vxR) * (alR - alL) * nx
     return F, nc
 
 
@@ -215,10 +233,12 @@ def _fhll(UL, SL, FL, UR, SR, FR):
     return (SR * FL - SL * FR + SL * SR * (UR - UL)) / np.abs(SR - SL)
 
 
-def _oned_hll(rhoL, rhoR, vxL, vxR, EtL, EtR, alL, alR, nx, YL=(), YR=()):
-    """oned_multifluid_hll, oned_multifluid_fluxes.h:117-226 (GAMNCON, wave-speed estimate Toro
-    10.48).  As in the reference, the momentum row's HLL jump uses the velocities vxL, vxR
-    (oned_multifluid_fluxes.h:196), and a face with SL == 0 or SR == 0 keeps a zero flux."""
+def _oned_hll(rhoL, rhoR, vxL, vxR, EtL, EtR, alL, alR, nx, YL=(), YR=(), gc=False):
+    """oned_multifluid_hll, oned_multifluid_fluxes.h:117-226 (wave-speed estimate Toro 10.48).  As
+    in the reference, the momentum row's HLL jump uses the velocities vxL, vxR
+    (oned_multifluid_fluxes.h:196), and a face with SL == 0 or SR == 0 keeps a zero flux.  gc
+    (GAMCONS; alphas divided by the caller, :131-134): the alpha row is the HLL flux of
+    rho*alpha*u whose state jump is the divided alpha (:180-182, 195-197, 210-212)."""
     gL = 1.0 + 1.0 / alL
     gR = 1.0 + 1.0 / alR
     pL = (gL - 1) * (EtL - 0.5 * rhoL * vxL * vxL)
@@ -233,10 +253,17 @@ def _oned_hll(rhoL, rhoR, vxL, vxR, EtL, EtR, alL, alR, nx, YL=(), YR=()):
     fR = [rhoR * vxR * nx, (rhoR * vxR * vxR + pR) * nx, (EtR + pR) * vxR * nx]
     with np.errstate(divide="ignore", invalid="ignore"):
         mid = [_fhll(rhoL, SL, fL[0], rhoR, SR, fR[0]), _fhll(vxL, SL, fL[1], vxR, SR, fR[1]),
-               _fhll(EtL, SL, fL[2], EtR, SR, fR[2]),
-               _fhll(alL, SL, 0.0, alR, SR, 0.0) - 0.5 * np.abs(SR + SL) / np.abs(SR - SL) * vncabs]
-    left = [fL[0], fL[1], fL[2], -0.5 * vncabs]
-    right = [fR[0], fR[1], fR[2], 0.5 * vncabs]
+               _fhll(EtL, SL, fL[2], EtR, SR, fR[2])]
+        if gc:
+            mid.append(_fhll(alL, SL, rhoL * vxL * alL * nx, alR, SR, rhoR * vxR * alR * nx))
+        else:
+            mid.append(_fhll(alL, SL, 0.0, alR, SR, 0.0) - 0.5 * np.abs(SR + SL) / np.abs(SR - SL) * vncabs)
+    if gc:
+        left = [fL[0], fL[1], fL[2], rhoL * vxL * alL * nx]
+        right = [fR[0], fR[1], fR[2], rhoR * vxR * alR * nx]
+    else:
+        left = [fL[0], fL[1], fL[2], -0.5 * vncabs]
+        right = [fR[0], fR[1], fR[2], 0.5 * vncabs]
     for k in range(len(YL)):  # mass fractions (oned_multifluid_fluxes.h:186-219)
         fYL, fYR = YL[k] * vxL * nx, YR[k] * vxR * nx
         with np.errstate(divide="ignore", invalid="ignore"):
@@ -250,12 +277,15 @@ def _oned_hll(rhoL, rhoR, vxL, vxR, EtL, EtR, alL, alR, nx, YL=(), YR=()):
     nc = np.zeros_like(F)
     for k in range(4 + len(YL)):
         F[k] = np.where(cL, left[k], np.where(cM, mid[k], np.where(cR, right[k], 0.0)))
-    nc[3] = -0.5 * vnc
+    if not gc:
+        nc[3] = -0.5 * vnc
     return F, nc
 
 
-def _oned_roe(rhoL, rhoR, vxL, vxR, EtL, EtR, alL, alR, nx, YL=(), YR=()):
-    """oned_multifluid_roe, oned_multifluid_fluxes.h:237-382 (GAMNCON); mass fractions :358-370."""
+def _oned_roe(rhoL, rhoR, vxL, vxR, EtL, EtR, alL, alR, nx, YL=(), YR=(), gc=False):
+    """oned_multifluid_roe, oned_multifluid_fluxes.h:237-382; mass fractions :358-370.  gc
+    (GAMCONS; alphas divided by the caller, :252-255): central rho*alpha*u part in the alpha row
+    (:348-350), no non-conservative term."""
     gL = 1.0 + 1.0 / alL
     gR = 1.0 + 1.0 / alR
     pL = (gL - 1) * (EtL - 0.5 * rhoL * vxL * vxL)
@@ -294,8 +324,11 @@ def _oned_roe(rhoL, rhoR, vxL, vxR, EtL, EtR, alL, alR, nx, YL=(), YR=()):
     F[0] = 0.5 * (rhoL * vxL + rhoR * vxR) * nx - 0.5 * diss(0)
     F[1] = 0.5 * (rhoL * vxL * vxL + pL + rhoR * vxR * vxR + pR) * nx - 0.5 * diss(1)
     F[2] = 0.5 * ((EtL + pL) * vxL + (EtR + pR) * vxR) * nx - 0.5 * diss(2)
-    F[3] = -0.5 * diss(3)
-    nc[3] = -0.5 * v * (alR - alL) * nx
+    if gc:
+        F[3] = 0.5 * (rhoL * vxL * alL + rhoR * vxR * alR) * nx - 0.5 * diss(3)
+    else:
+        F[3] = -0.5 * diss(3)
+        nc[3] = -0.5 * v * (alR - alL) * nx
     return F, nc
 
 
@@ -325,7 +358,9 @@ def _reflect(S: Setup, UF: np.ndarray) -> None:
 
 
 def _evaluate_sf(S: Setup, Ug, dUg, invJac):
-    """evaluate_sf, code/src/physics/physics.cu:27-363 (1D multifluid :96-143, 2D :248-301)."""
+    """evaluate_sf, code/src/physics/physics.cu:27-363 (1D multifluid :96-143, 2D :248-301).  GAMCONS:
+    gamma = 1 + rho/(stored field) and the conservative flux rho*u/(gamma-1) with no source
+    (:100-104, :122-124; 2D :253-257, :278-281)."""
     NE, NF, NG, D = S.N_E, S.N_F, S.N_G, S.D
     s = np.zeros((NE, NF, NG))
     f = np.zeros((NE, NF, NG, D))
@@ -333,21 +368,24 @@ def _evaluate_sf(S: Setup, Ug, dUg, invJac):
     if D == 1:
         u = Ug[:, 1] / rho
         Et = Ug[:, 2]
-        gam = 1 + 1.0 / Ug[:, 3]
+        gam = 1 + (rho if S.gamcons else 1.0) / Ug[:, 3]
         p = (gam - 1) * (Et - 0.5 * rho * u * u)
         s[:, 1] = rho * S.gx
         s[:, 2] = rho * u * S.gx
         f[:, 0, :, 0] = rho * u
         f[:, 1, :, 0] = rho * u * u + p
         f[:, 2, :, 0] = (Et + p) * u
-        s[:, 3] = -u * dUg[:, 3, :, 0] * invJac.reshape(NE, NG)
+        if S.gamcons:
+            f[:, 3, :, 0] = rho * u * (1 / (gam - 1))
+        else:
+            s[:, 3] = -u * dUg[:, 3, :, 0] * invJac.reshape(NE, NG)
         for k in range(4, NF):  # mass fractions: flux rho*Y_k u (physics.cu:130-134)
             f[:, k, :, 0] = Ug[:, k] * u
         return s, f
     u = Ug[:, 1] / rho
     v = Ug[:, 2] / rho
     Et = Ug[:, 3]
-    gam = 1 + 1.0 / Ug[:, 4]
+    gam = 1 + (rho if S.gamcons else 1.0) / Ug[:, 4]
     p = (gam - 1) * (Et - 0.5 * rho * (u * u + v * v))
     s[:, 1] = rho * S.gx
     s[:, 2] = rho * S.gy
@@ -360,11 +398,15 @@ def _evaluate_sf(S: Setup, Ug, dUg, invJac):
     f[:, 1, :, 1] = rho * u * v
     f[:, 2, :, 1] = rho * v * v + p
     f[:, 3, :, 1] = (Et + p) * v
-    iJ = invJac.reshape(NE, NG, D, D)  # [e, g, alpha, a]: d xi_a / d x_alpha
-    vg = np.zeros((NE, NG))
-    for al in range(D):
-        vg += -u * dUg[:, 4, :, al] * iJ[:, :, 0, al] - v * dUg[:, 4, :, al] * iJ[:, :, 1, al]
-    s[:, 4] = vg
+    if S.gamcons:
+        f[:, 4, :, 0] = rho * u * (1 / (gam - 1))
+        f[:, 4, :, 1] = rho * v * (1 / (gam - 1))
+    else:
+        iJ = invJac.reshape(NE, NG, D, D)  # [e, g, alpha, a]: d xi_a / d x_alpha
+        vg = np.zeros((NE, NG))
+        for al in range(D):
+            vg += -u * dUg[:, 4, :, al] * iJ[:, :, 0, al] - v * dUg[:, 4, :, al] * iJ[:, :, 1, al]
+        s[:, 4] = vg
     for k in range(5, NF):  # mass fractions: flux rho*Y_k (u, v) (physics.cu:293-298)
         f[:, k, :, 0] = Ug[:, k] * u
         f[:, k, :, 1] = Ug[:, k] * v
@@ -377,16 +419,22 @@ def _evaluate_q(S: Setup, UgF):
     n = S.a["normals"].reshape(S.M_T, S.D)
     L, R = UgF[:, :, 0, :], UgF[:, :, 1, :]  # (M_T, N_F, M_G)
     nx = n[:, 0][:, None]
+    ka = S.D + 2                              # the gamma-model field
+    alL, alR = L[:, ka], R[:, ka]
+    if S.gamcons:                             # divided by the density inside each flux function
+        alL, alR = alL / L[:, 0], alR / R[:, 0]
+        if S.D == 2 and S.flux == "rusanov":  # twod_multifluid_fluxes.h:51-52: alphaL = alphaL/rhoL;
+            alR = alL / L[:, 0]                 # alphaR = alphaL/rhoL (the divided left alpha, again)
     if S.D == 1:
         fn = {"rusanov": _oned_rusanov, "hll": _oned_hll, "roe": _oned_roe}[S.flux]
-        F, nc = fn(L[:, 0], R[:, 0], L[:, 1] / L[:, 0], R[:, 1] / R[:, 0], L[:, 2], R[:, 2], L[:, 3], R[:, 3], nx,
-                   [L[:, k] for k in range(4, S.N_F)], [R[:, k] for k in range(4, S.N_F)])
+        F, nc = fn(L[:, 0], R[:, 0], L[:, 1] / L[:, 0], R[:, 1] / R[:, 0], L[:, 2], R[:, 2], alL, alR, nx,
+                   [L[:, k] for k in range(4, S.N_F)], [R[:, k] for k in range(4, S.N_F)], gc=S.gamcons)
     else:
         ny = n[:, 1][:, None]
         fn = {"rusanov": _twod_rusanov, "roe": _twod_roe}[S.flux]
         F, nc = fn(L[:, 0], R[:, 0], L[:, 1] / L[:, 0], R[:, 1] / R[:, 0], L[:, 2] / L[:, 0], R[:, 2] / R[:, 0],
-                   L[:, 3], R[:, 3], L[:, 4], R[:, 4], nx, ny, [L[:, k] for k in range(5, S.N_F)],
-                   [R[:, k] for k in range(5, S.N_F)])
+                   L[:, 3], R[:, 3], alL, alR, nx, ny, [L[:, k] for k in range(5, S.N_F)],
+                   [R[:, k] for k in range(5, S.N_F)], gc=S.gamcons)
     F = np.moveaxis(F, 0, 1)    # (M_T, N_F, M_G)
     nc = np.moveaxis(nc, 0, 1)
     q = np.empty_like(UgF)
@@ -449,13 +497,13 @@ def dt_from_cfl(S: Setup, U: np.ndarray, cfl_scaled: float | None = None) -> flo
     rho = V[:, 0]
     if S.D == 1:
         u = V[:, 1] / rho
-        g = 1.0 + 1.0 / V[:, 3]
+        g = 1.0 + (rho if S.gamcons else 1.0) / V[:, 3]     # upa.h:61-70
         p = (g - 1) * (V[:, 2] - 0.5 * rho * u * u)
         upa = np.abs(u) + np.sqrt(g * p / rho)
     else:
         u = V[:, 1] / rho
         v = V[:, 2] / rho
-        g = 1.0 + 1.0 / V[:, 4]
+        g = 1.0 + (rho if S.gamcons else 1.0) / V[:, 4]     # upa.h:72-85
         p = (g - 1) * (V[:, 3] - 0.5 * rho * (u * u + v * v))
         a = np.sqrt(g * p / rho)
         upa = np.maximum(np.abs(u) + a, np.abs(v) + a)
@@ -598,6 +646,8 @@ def limit(S: Setup, U: np.ndarray) -> np.ndarray:
     if S.limiter == "hrl":
         return _hr(S, U)
     if S.limiter == "m2l":
+        if S.gamcons:  # limiting.cc:193-194 / 410-411 stop the run
+            raise NotImplementedError("M2L is only implemented for gamncon")
         return _m2(S, U)
     if S.limiter == "prl":
         return prim2cons(S, _hr(S, cons2prim(S, U)))
@@ -970,13 +1020,16 @@ def _sensor_gated(S: Setup, U: np.ndarray) -> np.ndarray:
 
 def error_norms(S: Setup, U: np.ndarray, Uex: np.ndarray, xyz0: tuple[float, float]) -> np.ndarray:
     """[dx, L1, L2, Linf per field] of the quadrature cell integrals / dx of U against Uex after
-    both go to (rho, u, (E - rho u^2/2)/alpha, alpha) on fields 0..3; xyz0 = x of nodes 0 and 1
-    of element 0 (dx = their difference, main.cc:992)."""
+    both go to (rho, u, (E - rho u^2/2)/alpha, alpha) on fields 0..3, alpha = 1/(gamma-1) (the
+    stored field divided by rho for GAMCONS, main.cc:963-966); xyz0 = x of nodes 0 and 1 of
+    element 0 (dx = their difference, main.cc:992)."""
     NE, NF, Ns, NG = S.N_E, S.N_F, S.N_s, S.N_G
 
     def prim(X):
         V = np.array(X, np.float64, copy=True).reshape(NE, NF, Ns)
         V[:, 1] = V[:, 1] / V[:, 0]
+        if S.gamcons:
+            V[:, 3] = V[:, 3] / V[:, 0]
         V[:, 2] = 1.0 / V[:, 3] * (V[:, 2] - 0.5 * V[:, 0] * V[:, 1] * V[:, 1])
         return V
 

@@ -31,7 +31,7 @@ def problem_for(meta, **over):
     import dg_b200 as dgb
     x0, x1, y0, y1 = meta["dom"]
     kw = dict(flux=meta["flux"], limiter=meta["limiter"], cfl=meta["cfl"], thresholds=tuple(meta.get("thresholds", ())),
-              n_mass=meta.get("n_mass", 0))
+              n_mass=meta.get("n_mass", 0), gamma_model=meta.get("gamma_model", "gamncon"))
     kw.update(over)
     return dgb.Problem.structured(meta["dim"], meta["order"], meta["nx"], meta["ny"], x0, x1, y0, y1,
                                   tuple(meta["bc"]), **kw)

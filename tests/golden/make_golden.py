@@ -98,6 +98,21 @@ CASES = [
          flux="roe", limiter="hrl", ic="quadrants", cfl=0.3, dt=5e-4, nsteps=4, n_mass=1),
     dict(name="y2_p1_roe_m2l_box", dim=2, order=1, nx=32, ny=4, dom=(0, 1, 0, 1), bc=("reflective",) * 4,
          flux="roe", limiter="m2l", ic="quadrants", cfl=0.3, dt=5e-4, nsteps=4, n_mass=1),
+    # the conservative gamma model (the reference built with GAMM=GAMCONS); its M2limiting stops
+    # the run for this model, so the limiters are hrl and none
+    dict(name="g1_p2_roe_hrl", dim=1, order=2, nx=24, ny=1, dom=(0, 1, 0, 1), bc=("transmissive",) * 2,
+         flux="roe", limiter="hrl", ic="tube_noise", cfl=0.4, dt=4e-4, nsteps=5, gamma_model="gamcons"),
+    dict(name="g1_p3_hll_none_wall", dim=1, order=3, nx=20, ny=1, dom=(0, 1, 0, 1), bc=("reflective",) * 2,
+         flux="hll", limiter="none", ic="tube_noise", cfl=0.05, dt=2e-4, nsteps=5, gamma_model="gamcons"),
+    dict(name="g1_p1_rus_hrl_periodic", dim=1, order=1, nx=30, ny=1, dom=(0, 1, 0, 1), bc=("periodic",) * 2,
+         flux="rusanov", limiter="hrl", ic="riemann", cfl=0.4, dt=4e-4, nsteps=5, gamma_model="gamcons"),
+    dict(name="g2_p2_rus_hrl_walls", dim=2, order=2, nx=32, ny=8, dom=(0, 2, 0, 1),
+         bc=("reflective", "transmissive", "reflective", "transmissive"), flux="rusanov", limiter="hrl",
+         ic="shock_bubble", cfl=0.3, dt=5e-4, nsteps=4, gamma_model="gamcons"),
+    dict(name="g2_p1_roe_none_periodic", dim=2, order=1, nx=32, ny=4, dom=(0, 1, 0, 1), bc=("periodic",) * 4,
+         flux="roe", limiter="none", ic="quadrants", cfl=0.1, dt=5e-4, nsteps=4, gamma_model="gamcons"),
+    dict(name="g2_p3_roe_hrl", dim=2, order=3, nx=32, ny=4, dom=(0, 2, 0, 1), bc=("transmissive",) * 4,
+         flux="roe", limiter="hrl", ic="shock_bubble", cfl=0.3, dt=2.5e-4, nsteps=4, gamma_model="gamcons"),
 ]
 
 
@@ -120,10 +135,11 @@ def make_case(c: dict, seed: int) -> dict:
     bc = tuple(c["bc"]) + ("transmissive",) * (4 - len(c["bc"]))
     th = tuple(c.get("thresholds", ()))
     nm = c.get("n_mass", 0)
+    gm = c.get("gamma_model", "gamncon")
     ref = RefCase(c["dim"], c["order"], c["nx"], c["ny"], x0, x1, y0, y1, bc, c["flux"], c["limiter"],
-                  thresholds=th, n_mass=nm)
+                  thresholds=th, n_mass=nm, gamcons=gm == "gamcons")
     prob = dgb.Problem.structured(c["dim"], c["order"], c["nx"], c["ny"], x0, x1, y0, y1, bc, flux=c["flux"],
-                                  limiter=c["limiter"], cfl=c["cfl"], thresholds=th, n_mass=nm)
+                                  limiter=c["limiter"], cfl=c["cfl"], thresholds=th, n_mass=nm, gamma_model=gm)
     Uraw = perturbed_state(prob, c["ic"], seed)
     out = dict(Uraw=Uraw)
     if th:

@@ -69,3 +69,31 @@ def test_shim_exports_reference_launchers(d, flux):
     lib = ctypes.CDLL(str(ROOT / "dg_b200" / "lib" / f"libdgb_shim_{d}d_{flux}.so"))
     missing = [n for n in SHIM_LAUNCHERS if not hasattr(lib, n)]
     assert not missing, missing
+
+
+def test_ctypes_structs_match_the_header_layout(tmp_path):
+    """Size and every field offset of dgb_mesh_spec, dgb_options and dgb_info as a C compiler lays
+    them out from include/dgb.h, against the ctypes mirrors in dg_b200/_ffi.py."""
+    import ctypes
+    import shutil
+    import subprocess
+    from dg_b200 import _ffi
+    if shutil.which("gcc") is None:
+        pytest.skip("no C compiler")
+    structs = {"dgb_mesh_spec": _ffi.MeshSpec, "dgb_options": _ffi.Options, "dgb_info": _ffi.Info}
+    lines = ["#include <stdio.h>", "#include <stddef.h>", '#include "dgb.h"', "int main(void) {"]
+    for cname, py in structs.items():
+        lines.append(f'  printf("{cname} size %zu\\n", sizeof({cname}));')
+        for fname, _ in py._fields_:
+            lines.append(f'  printf("{cname} {fname} %zu\\n", offsetof({cname}, {fname}));')
+    lines += ["  return 0;", "}"]
+    src = tmp_path / "layout.c"
+    src.write_text("\n".join(lines) + "\n")
+    exe = tmp_path / "layout"
+    subprocess.run(["gcc", "-std=c99", f"-I{ROOT / 'include'}", str(src), "-o", str(exe)], check=True)
+    out = subprocess.run([str(exe)], check=True, capture_output=True, text=True).stdout.split("\n")
+    got = {tuple(l.split()[:2]): int(l.split()[2]) for l in out if l}
+    for cname, py in structs.items():
+        assert got[(cname, "size")] == ctypes.sizeof(py), cname
+        for fname, _ in py._fields_:
+            assert got[(cname, fname)] == getattr(py, fname).offset, (cname, fname)

@@ -1,7 +1,7 @@
 """CUDA path (through the C ABI) against the numpy oracle at sizes and seeds the golden fixtures
 do not cover: ragged grids (extents not multiples of the 32 x 4 element tile), tile-aligned grids
 (tiled kernels), p = 1..3, all fluxes, both limiters, walls / periodic / transmissive
-boundaries, one passive mass fraction, the 1D shock-tube workload (1000 elements, p=2, Roe, m2l,
+boundaries, one passive mass fraction, the GAMCONS gamma model, the 1D shock-tube workload (1000 elements, p=2, Roe, m2l,
 RK4) and the 2D shock-bubble workload at its full size (512 x 256 elements, p=2, Rusanov, m2l,
 SSP-RK3).
 
@@ -36,6 +36,14 @@ CASES = [
     ("2d_p1_rus_m2l_tiled_box_y1", 2, 1, 64, 12, ("reflective",) * 4, "rusanov", "m2l", "quadrants", 0.3, 1),
     ("1d_p2_rus_m2l_y1", 1, 2, 201, 1, ("transmissive",) * 2, "rusanov", "m2l", "tube_noise", 0.3, 1),
     ("1d_p3_hll_hrl_walls_y1", 1, 3, 97, 1, ("reflective",) * 2, "hll", "hrl", "riemann", 0.15, 1),
+    # the GAMCONS gamma model (last entry); limiters hrl and none (the reference's M2limiting stops
+    # for this model)
+    ("2d_p2_rus_hrl_tiled_walls_gc", 2, 2, 64, 16, WALLS, "rusanov", "hrl", "shock_bubble", 0.3, 0, "gamcons"),
+    ("2d_p1_roe_hrl_tiled_periodic_gc", 2, 1, 64, 8, ("periodic",) * 4, "roe", "hrl", "quadrants", 0.3, 0, "gamcons"),
+    ("2d_p3_roe_none_tiled_box_gc", 2, 3, 32, 6, ("reflective",) * 4, "roe", "none", "quadrants", 0.1, 0, "gamcons"),
+    ("1d_p2_roe_hrl_gc", 1, 2, 211, 1, ("transmissive",) * 2, "roe", "hrl", "tube_noise", 0.3, 0, "gamcons"),
+    ("1d_p1_hll_hrl_periodic_gc", 1, 1, 150, 1, ("periodic",) * 2, "hll", "hrl", "riemann", 0.3, 0, "gamcons"),
+    ("1d_p3_rus_none_walls_gc", 1, 3, 77, 1, ("reflective",) * 2, "rusanov", "none", "tube_noise", 0.05, 0, "gamcons"),
 ]
 
 
@@ -44,9 +52,10 @@ def make(case, seed):
     _, dim, order, nx, ny, bc, flux, limiter, ic = case[:9]
     cfl = case[9] if len(case) > 9 else 0.3
     n_mass = case[10] if len(case) > 10 else 0
+    gamma_model = case[11] if len(case) > 11 else "gamncon"
     x1 = 2.0 if dim == 2 and ic == "shock_bubble" else 1.0
     prob = dgb.Problem.structured(dim, order, nx, ny, 0.0, x1, 0.0, 1.0, bc, flux=flux, limiter=limiter, cfl=cfl,
-                                  n_mass=n_mass)
+                                  n_mass=n_mass, gamma_model=gamma_model)
     S = O.Setup.from_problem(prob)
     U0 = O.limit(S, perturbed_state(prob, ic, seed))
     return prob, S, U0
@@ -166,6 +175,82 @@ def test_mass_fraction_configurations_outside_the_device_path_are_rejected():
     with pytest.raises(dgb.DGBError):
         dgb.DGSolver(prob)
     prob = dgb.Problem.structured(2, 2, 32, 8, flux="rusanov", limiter="m2l", cfl=0.3, n_mass=1)
+    s = dgb.DGSolver(prob)
+    try:
+        with pytest.raises(dgb.DGBError):
+            s.set_form("mixed")
+        with pytest.raises(dgb.DGBError):
+            dgb.DGBatch([s])
+    finally:
+        s.close()
+
+
+def test_gamcons_shock_bubble_100_steps_l1():
+    """The 2D shock-bubble in the GAMCONS model (64 x 32, p=2, Roe, hrl, SSP-RK3, CFL step), 100
+    steps: relative L1 of density and of rho/(gamma-1)."""
+    import dg_b200 as dgb
+    prob = dgb.Problem.structured(2, 2, 64, 32, 0.0, 2.0, 0.0, 1.0, WALLS, flux="roe", limiter="hrl", cfl=0.3,
+                                  gamma_model="gamcons")
+    assert prob.info.gamma_model == 1
+    S = O.Setup.from_problem(prob)
+    assert S.gamcons
+    U0 = O.limit(S, prob.init_state("shock_bubble", seed=7))
+    s = dgb.DGSolver(prob)
+    try:
+        s.set_state(U0)
+        s.advance(100, 0.0, scheme=dgb.SSPRK3)
+        Ug = s.get_state()
+    finally:
+        s.close()
+    Uo = O.ssprk3_steps(S, U0, 0.0, 100)
+    i = prob.info
+    assert l1_density_error(Ug, Uo, i.n_elem, i.n_fields, i.n_s) < 1e-10
+    A = Ug.reshape(i.n_elem, i.n_fields, i.n_s)[:, 4]
+    B = Uo.reshape(i.n_elem, i.n_fields, i.n_s)[:, 4]
+    assert np.abs(A - B).sum() / np.abs(B).sum() < 1e-10
+
+
+def test_gamcons_rusanov_2d_breaks_down_like_the_reference():
+    """The reference's 2D GAMCONS Rusanov flux takes the right alpha as the left one divided twice
+    by rhoL (twod_multifluid_fluxes.h:50-53); on the shock-bubble its own arithmetic (the oracle)
+    turns NaN at step 16.  The device path follows it step for step and then stops with the NaN
+    time-step error instead of returning a NaN state."""
+    import dg_b200 as dgb
+    prob = dgb.Problem.structured(2, 2, 64, 32, 0.0, 2.0, 0.0, 1.0, WALLS, flux="rusanov", limiter="hrl", cfl=0.3,
+                                  gamma_model="gamcons")
+    S = O.Setup.from_problem(prob)
+    U0 = O.limit(S, prob.init_state("shock_bubble", seed=7))
+    s = dgb.DGSolver(prob)
+    try:
+        s.set_state(U0)
+        s.advance(8, 0.0, scheme=dgb.SSPRK3)
+        assert rel_err(s.get_state(), O.ssprk3_steps(S, U0, 0.0, 8)) < 1e-9
+        with pytest.raises(dgb.DGBError) as e:
+            s.advance(40, 0.0, scheme=dgb.SSPRK3)
+        assert e.value.code == 6
+    finally:
+        s.close()
+
+
+def test_gamcons_configurations_outside_the_device_path_are_rejected():
+    """M2L stops with GAMCONS (as in the reference), and the device path has no GAMCONS variant of
+    the sensors, of mass fractions, of the mixed form or of untiled 2D grids."""
+    import dg_b200 as dgb
+    bad = [dict(dim=2, order=2, nx=32, ny=8, limiter="m2l"),
+           dict(dim=1, order=2, nx=50, ny=1, limiter="m2l"),
+           dict(dim=2, order=2, nx=40, ny=8, limiter="hrl"),               # 2D grid not tile-aligned
+           dict(dim=1, order=2, nx=50, ny=1, limiter="hri", thresholds=(0.05,)),
+           dict(dim=1, order=2, nx=50, ny=1, limiter="prl"),
+           dict(dim=1, order=2, nx=50, ny=1, limiter="hrl", n_mass=1)]
+    for kw in bad:
+        th = kw.pop("thresholds", ())
+        nm = kw.pop("n_mass", 0)
+        prob = dgb.Problem.structured(kw["dim"], kw["order"], kw["nx"], kw["ny"], flux="rusanov", limiter=kw["limiter"],
+                                      cfl=0.3, thresholds=th, n_mass=nm, gamma_model="gamcons")
+        with pytest.raises(dgb.DGBError) as e:
+            dgb.DGSolver(prob)
+        assert e.value.code == 4, kw
+    prob = dgb.Problem.structured(2, 2, 32, 8, flux="rusanov", limiter="hrl", cfl=0.3, gamma_model="gamcons")
     s = dgb.DGSolver(prob)
     try:
         with pytest.raises(dgb.DGBError):
