@@ -50,7 +50,8 @@ class Info(C.Structure):
                 "dim order n_fields n_elem n_s n_g n_ifaces m_s m_g n_n n_reflective cartesian "
                 "gpu_supported flux limiter nx ny".split()] + \
                [(n, C.c_double) for n in "cfl dx_min cfl_scaled final_time".split()] + \
-               [("n_output_times", C.c_int), ("error_output", C.c_int), ("gamma_model", C.c_int)]
+               [("n_output_times", C.c_int), ("error_output", C.c_int), ("gamma_model", C.c_int),
+                                            ("cons_output", C.c_int)]
 
 
 class DGBError(RuntimeError):

@@ -269,6 +269,31 @@ bool dgb::encode_state_map(dgb_ctx* c, double* ptr, CUtensorMap* map, int tw, in
 
 namespace {
 
+// NY passive mass fractions (1D or tiled 2D, FP64 form; checked at create)
+template <int MODE, int NY>
+int residual_ny(dgb_ctx* c, const StageArgs& a) {
+  if (c->tiled) {
+    switch (c->p * 10 + c->flux) {
+      case 10: launch_tile2d<1, 0, MODE, NY>(c, a); return 0;
+      case 12: launch_tile2d<1, 2, MODE, NY>(c, a); return 0;
+      case 20: launch_tile2d<2, 0, MODE, NY>(c, a); return 0;
+      case 22: launch_tile2d<2, 2, MODE, NY>(c, a); return 0;
+      case 30: launch_tile2d<3, 0, MODE, NY>(c, a); return 0;
+      case 32: launch_tile2d<3, 2, MODE, NY>(c, a); return 0;
+      default: return set_error(DGB_ERR_UNSUPPORTED, "no residual kernel for this (p, flux) with mass fractions");
+    }
+  }
+  if (c->D == 1) {
+#define R1Y(P, F) case P * 10 + F: launch_res1d<P, F, MODE, NY>(c, a); return 0;
+    switch (c->p * 10 + c->flux) {
+      R1Y(1, 0) R1Y(1, 1) R1Y(1, 2) R1Y(2, 0) R1Y(2, 1) R1Y(2, 2) R1Y(3, 0) R1Y(3, 1) R1Y(3, 2)
+      default: break;
+    }
+#undef R1Y
+  }
+  return set_error(DGB_ERR_UNSUPPORTED, "no residual kernel for this (p, flux) with mass fractions");
+}
+
 template <int MODE>
 int residual_dispatch(dgb_ctx* c, const StageArgs& a) {
   if (c->tiled && c->form == DGB_FORM_MIXED) {
@@ -302,24 +327,13 @@ int residual_dispatch(dgb_ctx* c, const StageArgs& a) {
     }
 #undef R1G
   }
-  if (c->tiled && c->nmass == 1) {
-    switch (c->p * 10 + c->flux) {
-      case 10: launch_tile2d<1, 0, MODE, 1>(c, a); return 0;
-      case 12: launch_tile2d<1, 2, MODE, 1>(c, a); return 0;
-      case 20: launch_tile2d<2, 0, MODE, 1>(c, a); return 0;
-      case 22: launch_tile2d<2, 2, MODE, 1>(c, a); return 0;
-      case 30: launch_tile2d<3, 0, MODE, 1>(c, a); return 0;
-      case 32: launch_tile2d<3, 2, MODE, 1>(c, a); return 0;
-      default: return set_error(DGB_ERR_UNSUPPORTED, "no residual kernel for this (p, flux) with a mass fraction");
+  if (c->nmass > 0) {
+    switch (c->nmass) {
+      case 1: return residual_ny<MODE, 1>(c, a);
+      case 2: return residual_ny<MODE, 2>(c, a);
+      case 3: return residual_ny<MODE, 3>(c, a);
+      default: return set_error(DGB_ERR_UNSUPPORTED, "at most three mass fractions on the device path");
     }
-  }
-  if (c->D == 1 && c->nmass == 1) {
-#define R1Y(P, F) case P * 10 + F: launch_res1d<P, F, MODE, 1>(c, a); return 0;
-    switch (c->p * 10 + c->flux) {
-      R1Y(1, 0) R1Y(1, 1) R1Y(1, 2) R1Y(2, 0) R1Y(2, 1) R1Y(2, 2) R1Y(3, 0) R1Y(3, 1) R1Y(3, 2)
-      default: return set_error(DGB_ERR_UNSUPPORTED, "no residual kernel for this (p, flux) with a mass fraction");
-    }
-#undef R1Y
   }
   if (c->tiled) {
     const int key = c->p * 10 + c->flux;
@@ -516,6 +530,21 @@ void launch_learned_limiter(dgb_ctx* c, double* U, bool score) {
 
 // in-place limiting of a state buffer with the context's limiter (rescore: the learned indicator
 // scores U first; the time steppers score once per step and pass false)
+// hrl / m2l with NY passive mass fractions; key = p * 10 + limiter
+template <int NY>
+int limit_ny(dgb_ctx* c, double* U, int key) {
+#define L2Y(P, M) case P * 10 + M: launch_lim2d<P, M, NY>(c, U); return 0;
+#define L1Y(P, M) case P * 10 + M: launch_lim1d<P, M, NY>(c, U); return 0;
+  if (c->D == 2) {
+    switch (key) { L2Y(1, 1) L2Y(1, 2) L2Y(2, 1) L2Y(2, 2) L2Y(3, 1) L2Y(3, 2) default: break; }
+  } else {
+    switch (key) { L1Y(1, 1) L1Y(1, 2) L1Y(2, 1) L1Y(2, 2) L1Y(3, 1) L1Y(3, 2) default: break; }
+  }
+#undef L2Y
+#undef L1Y
+  return set_error(DGB_ERR_UNSUPPORTED, "limiter not available with mass fractions");
+}
+
 int limit_dispatch(dgb_ctx* c, double* U, bool rescore = true) {
   if (c->limiter == 0) return 0;
   if (c->ind_on) {
@@ -547,17 +576,12 @@ int limit_dispatch(dgb_ctx* c, double* U, bool rescore = true) {
     }
   }
   const int key = c->p * 10 + c->limiter;
-  if (c->nmass == 1) {
-#define L2Y(P, M) case P * 10 + M: launch_lim2d<P, M, 1>(c, U); return 0;
-#define L1Y(P, M) case P * 10 + M: launch_lim1d<P, M, 1>(c, U); return 0;
-    if (c->D == 2) {
-      switch (key) { L2Y(1, 1) L2Y(1, 2) L2Y(2, 1) L2Y(2, 2) L2Y(3, 1) L2Y(3, 2) default: break; }
-    } else {
-      switch (key) { L1Y(1, 1) L1Y(1, 2) L1Y(2, 1) L1Y(2, 2) L1Y(3, 1) L1Y(3, 2) default: break; }
-    }
-#undef L2Y
-#undef L1Y
-    return set_error(DGB_ERR_UNSUPPORTED, "limiter not available with a mass fraction");
+  switch (c->nmass) {
+    case 0: break;
+    case 1: return limit_ny<1>(c, U, key);
+    case 2: return limit_ny<2>(c, U, key);
+    case 3: return limit_ny<3>(c, U, key);
+    default: return set_error(DGB_ERR_UNSUPPORTED, "at most three mass fractions on the device path");
   }
 #define L2(P, M) case P * 10 + M: launch_lim2d<P, M>(c, U); return 0;
 #define L1(P, M) case P * 10 + M: launch_lim1d<P, M>(c, U); return 0;
@@ -761,15 +785,15 @@ extern "C" int dgb_create(const dgb_problem* prob, int device, dgb_ctx** out) {
     if (why) { delete c; return set_error(DGB_ERR_UNSUPPORTED, why); }
     c->fused_lim = false;
   }
-  if (P.N_Y > 1) { delete c; return set_error(DGB_ERR_UNSUPPORTED, "at most one mass fraction on the device path"); }
-  if (P.N_Y == 1 && P.D == 2 && !c->tiled) {
+  if (P.N_Y > 3) { delete c; return set_error(DGB_ERR_UNSUPPORTED, "at most three mass fractions on the device path"); }
+  if (P.N_Y > 0 && P.D == 2 && !c->tiled) {
     delete c;
     return set_error(DGB_ERR_UNSUPPORTED, "mass fractions in 2D need a structured row-major grid with nx a multiple "
                                           "of 32 and ny of 4 (p = 3: 2)");
   }
-  if (P.N_Y == 1 && P.limiter != DGB_LIM_NONE && P.limiter != DGB_LIM_HRL && P.limiter != DGB_LIM_M2L) {
+  if (P.N_Y > 0 && P.limiter != DGB_LIM_NONE && P.limiter != DGB_LIM_HRL && P.limiter != DGB_LIM_M2L) {
     delete c;
-    return set_error(DGB_ERR_UNSUPPORTED, "with a mass fraction the limiter is none, hrl or m2l");
+    return set_error(DGB_ERR_UNSUPPORTED, "with mass fractions the limiter is none, hrl or m2l");
   }
   if (int rc = upload_tables(c->cs, P.D, P.p)) { delete c; return rc; }
   auto fail = [&](cudaError_t e, const char* what) {

@@ -8,7 +8,11 @@
 //   * CFL < 0: a fixed step of output_times[1] - output_times[0], clipped to the final time, and
 //     no output (rk.cc:136-139);
 //   * output in the reference's .pos format (one file per field and output step) in --out;
-//   * with "#Make options" ERRR=ERROR, error.dat (main.cc:909-1038) in --out after the run.
+//   * with "#Make options" ERRR=ERROR, error.dat (main.cc:909-1038) in --out after the run;
+//   * with "#Make options" CONS=CONS, one line of conservation.dat in --out (appended, as the
+//     reference opens it, dg_solver.h:238-240) after the initial limiting and at every output
+//     time: the time and the domain integral of each field (DG_SOLVER::conservation,
+//     dg_solver.h:367-389; rk.cc:120-121, 228-229).
 // A NaN or too small time step ends the run with exit status 1 and the reference's message.
 //
 // usage: dgbexec [-d deck.inp] [--out DIR] [--scheme rk4|ssprk3] [--form fp64|mixed] [--device N]
@@ -26,6 +30,20 @@ namespace {
 int fail(const char* what) {
   std::fprintf(stderr, "dgbexec: %s: %s\n", what, dgb_last_error());
   return 2;
+}
+
+// one line of conservation.dat: "%20.16E\t" for the time and for each field total
+int write_conservation(dgb_ctx* ctx, int nf, double T, const std::string& dir) {
+  std::vector<double> tot(nf);
+  if (dgb_conservation(ctx, tot.data())) return fail("conservation");
+  const std::string fn = dir + "/conservation.dat";
+  FILE* f = std::fopen(fn.c_str(), "a");
+  if (!f) { std::fprintf(stderr, "dgbexec: cannot write %s\n", fn.c_str()); return 2; }
+  std::fprintf(f, "%20.16E\t", T);
+  for (int k = 0; k < nf; ++k) std::fprintf(f, "%20.16E\t", tot[k]);
+  std::fprintf(f, "\n");
+  std::fclose(f);
+  return 0;
 }
 
 }  // namespace
@@ -79,6 +97,8 @@ int main(int argc, char** argv) {
     if (info.limiter != DGB_LIM_NONE && dgb_limit(ctx, U.data())) return fail("limiter");
   }
   if (dgb_set_state(ctx, U.data())) return fail("state");
+  if (cfl >= 0 && info.cons_output)
+    if (int rc = write_conservation(ctx, info.n_fields, T, out)) return rc;
   ++count;
   double tout = times[std::min<size_t>(count, times.size() - 1)];
   bool done = false;
@@ -116,6 +136,8 @@ int main(int argc, char** argv) {
       if (dgb_get_state(ctx, U.data())) return fail("state");
       if (dgb_write_pos(prob, U.data(), count, T, out.c_str())) return fail("output");
       std::printf("Solution written to file at step %7ld and time %e.\n", steps, T);
+      if (info.cons_output)
+        if (int rc = write_conservation(ctx, info.n_fields, T, out)) return rc;
       ++count;
       if ((size_t)count < times.size()) tout = times[count];
     }

@@ -62,6 +62,7 @@ struct Problem {
   int N_Y = 0;                        // passive mass fractions rho*Y_k, fields D+3 .. N_F-1
   int flux = 2, limiter = 0;
   bool error_output = false;          // deck "#Make options" ERRR=ERROR: error.dat after the run
+  bool cons_output = false;           // deck "#Make options" CONS=CONS: conservation.dat at outputs
   bool gamcons = false;               // GAMCONS gamma model: field D+2 holds rho/(gamma-1)
   double cfl = -1.0;
   std::vector<double> thresholds;

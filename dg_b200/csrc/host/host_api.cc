@@ -91,6 +91,8 @@ extern "C" int dgb_problem_from_deck(const char* deck_path, dgb_problem** out) {
   pr->P.deck_dir = dir;
   mo = d.make_options.find("ERRR");
   pr->P.error_output = mo != d.make_options.end() && mo->second == "ERROR";
+  mo = d.make_options.find("CONS");
+  pr->P.cons_output = mo != d.make_options.end() && mo->second == "CONS";
   pr->P.deck_ic = d.ic;
   pr->P.deck_ic_inputs = d.ic_inputs;
   *out = pr;
@@ -159,6 +161,7 @@ extern "C" int dgb_problem_info(const dgb_problem* p, dgb_info* o) {
   o->final_time = P.final_time;
   o->n_output_times = (int)P.output_times.size();
   o->error_output = P.error_output ? 1 : 0;
+  o->cons_output = P.cons_output ? 1 : 0;
   o->gamma_model = P.gamcons ? DGB_GAMCONS : DGB_GAMNCON;
   return DGB_OK;
 }

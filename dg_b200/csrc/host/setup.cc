@@ -546,11 +546,11 @@ Status build_problem(Mesh&& mesh, int dim, int p, const std::string& kind, int f
 Status init_state(const Problem& P, const std::string& ic, const std::vector<double>& prm, uint64_t seed, double* U) {
   const int NS = P.N_s, NF = P.N_F, NE = P.N_E, D = P.D;
   auto X = [&](int i, int e, int a) { return P.xyz_nodes[i + (size_t)(e * D + a) * NS]; };
-  // passive mass fractions: rho*Y_k with Y_k = the region indicator `ymark` of the state set last
-  // (1 for the first / left / bubble region, 0 elsewhere; every Y_k alike)
+  // passive mass fractions: rho*Y_k with Y_k the region indicator `ymark` of the state set last (1
+  // for the first / left / bubble region, 0 elsewhere) for even k and its complement for odd k
   double ymark = 0.0;
   auto setY = [&](int e, int i, double rho) {
-    for (int k = 0; k < P.N_Y; ++k) U[(e * NF + NF - P.N_Y + k) * NS + i] = rho * ymark;
+    for (int k = 0; k < P.N_Y; ++k) U[(e * NF + NF - P.N_Y + k) * NS + i] = rho * (k % 2 ? 1.0 - ymark : ymark);
   };
   auto set = [&](int e, int i, const double* prim) {  // prim = rho, u, v, p, gamma (1D: rho,u,p,gamma)
     setY(e, i, prim[0]);

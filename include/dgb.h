@@ -104,7 +104,8 @@ typedef struct {
   double thresholds[3];/* sensor thresholds (sensor.h:35-45); n_thresholds of them are set */
   int n_thresholds;
   int n_mass;          /* passive mass fractions rho*Y_k appended to the state (MASS of the
-                        * reference Makefile; N_F = 4 (1D) / 5 (2D) + n_mass) */
+                        * reference Makefile, 0..10; N_F = 4 (1D) / 5 (2D) + n_mass; the device
+                        * path takes 0..3) */
   int gamma_model;     /* enum dgb_gamma_model */
 } dgb_options;
 
@@ -134,6 +135,7 @@ typedef struct {
   int n_output_times;
   int error_output;              /* deck "#Make options" ERRR=ERROR: error.dat after the run */
   int gamma_model;               /* enum dgb_gamma_model */
+  int cons_output;               /* deck "#Make options" CONS=CONS: conservation.dat at each output */
 } dgb_info;
 
 int dgb_problem_info(const dgb_problem* p, dgb_info* out);

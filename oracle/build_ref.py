@@ -9,8 +9,9 @@ set with oracle/ref_harness.cc into ``oracle/_ref/dgref_<variant>``.  Outputs go
 Compile-time configuration follows code/Makefile:147-156 (DEFINES) for the gamma-model
 multifluid build: USE_CPU, USE_DOUBLE, MULTIFLUID, GAMNCON, NO_MPI, N_Y=0, and
 N_F=4 (1D) / 5 (2D), D=1/2, DF=1, with the flux flag ROE, RUS or HLL; and the same with one
-passive mass fraction (N_Y=1, N_F=5 / 6; variants *_y1); GAMCONS in place of GAMNCON (variants
-*_gc); ERROR in place of NOERROR (variant 1d_rus_err).
+passive mass fraction (N_Y=1, N_F=5 / 6; variants *_y1) and with two or three (*_y2, *_y3); GAMCONS in place of GAMNCON (variants
+*_gc); ERROR in place of NOERROR (variant 1d_rus_err); CONS in place of NOCONS (variant
+1d_roe_cons).
 
 Out-of-tree additions (none of them touch reference arithmetic):
   * an empty ``gsl/gsl_integration.h`` (code/src/ic/init_cond.cc:10 includes it, never calls it);
@@ -49,6 +50,11 @@ VARIANTS = {
     "1d_hll_y1": dict(dims="ONED", nf=5, d=1, flux="HLL", ny=1),
     "2d_roe_y1": dict(dims="TWOD", nf=6, d=2, flux="ROE", ny=1),
     "2d_rus_y1": dict(dims="TWOD", nf=6, d=2, flux="RUS", ny=1),
+    # two and three mass fractions (MASS=2, MASS=3)
+    "1d_roe_y2": dict(dims="ONED", nf=6, d=1, flux="ROE", ny=2),
+    "1d_hll_y3": dict(dims="ONED", nf=7, d=1, flux="HLL", ny=3),
+    "2d_rus_y2": dict(dims="TWOD", nf=7, d=2, flux="RUS", ny=2),
+    "2d_roe_y3": dict(dims="TWOD", nf=8, d=2, flux="ROE", ny=3),
     # the ERROR diagnostic compiled in (ERRR=ERROR in code/Makefile): error.dat after the run
     "1d_rus_err": dict(dims="ONED", nf=4, d=1, flux="RUS", err=True),
     # the conservative gamma model (GAMM=GAMCONS in code/Makefile): rho/(gamma-1) as the field
@@ -57,6 +63,8 @@ VARIANTS = {
     "1d_hll_gc": dict(dims="ONED", nf=4, d=1, flux="HLL", gc=True),
     "2d_roe_gc": dict(dims="TWOD", nf=5, d=2, flux="ROE", gc=True),
     "2d_rus_gc": dict(dims="TWOD", nf=5, d=2, flux="RUS", gc=True),
+    # the conservation diagnostic compiled in (CONS=CONS in code/Makefile): conservation.dat
+    "1d_roe_cons": dict(dims="ONED", nf=4, d=1, flux="ROE", cons=True),
 }
 
 RK_SYM = ("_ZN2RK14RK_integrationEdiiiiiiiPdS0_R8LimitingbR9DG_SOLVERR12COMMUNICATORR7PRINTER"
@@ -66,7 +74,7 @@ RK_SYM = ("_ZN2RK14RK_integrationEdiiiiiiiPdS0_R8LimitingbR9DG_SOLVERR12COMMUNIC
 def defines(v: dict) -> list[str]:
     return ["-DHAVE_BLAS", "-DHAVE_LAPACK", "-DUSE_CPU", "-DHOME", "-DUSE_DOUBLE", "-DMULTIFLUID",
             "-DGAMCONS" if v.get("gc") else "-DGAMNCON", f"-D{v['flux']}", f"-D{v['dims']}", "-DNO_MPI", f"-DN_Y={v.get('ny', 0)}", f"-DN_F={v['nf']}",
-            "-DERROR" if v.get("err") else "-DNOERROR", "-DNOCONS", f"-DD={v['d']}", "-DDF=1"]
+            "-DERROR" if v.get("err") else "-DNOERROR", "-DCONS" if v.get("cons") else "-DNOCONS", f"-DD={v['d']}", "-DDF=1"]
 
 
 def sources(ref: Path) -> list[Path]:

@@ -22,11 +22,12 @@ FLUX_TAG = {"rusanov": "rus", "rus": "rus", "roe": "roe", "hll": "hll"}
 BC_TAG = {"periodic": 1, "transmissive": 2, "reflective": 3, "frozen": 4}
 
 
-def binary(dim: int, flux: str, n_mass: int = 0, error: bool = False, gamcons: bool = False) -> Path:
+def binary(dim: int, flux: str, n_mass: int = 0, error: bool = False, gamcons: bool = False,
+           cons: bool = False) -> Path:
     """The reference build for (dimension, flux) with N_Y = n_mass (0 or 1) mass fractions, with
-    the ERROR diagnostic compiled in, or with the GAMCONS gamma model."""
+    the ERROR or CONS diagnostic compiled in, or with the GAMCONS gamma model."""
     return REF_DIR / (f"dgref_{dim}d_{FLUX_TAG[flux.lower()]}" + (f"_y{n_mass}" if n_mass else "") +
-                      ("_err" if error else "") + ("_gc" if gamcons else ""))
+                      ("_err" if error else "") + ("_gc" if gamcons else "") + ("_cons" if cons else ""))
 
 
 def available(dim: int = 2, flux: str = "rusanov", n_mass: int = 0, gamcons: bool = False) -> bool:
@@ -54,6 +55,7 @@ class RefCase:
     make_options: tuple = ()      # "#Make options" KEY=VALUE lines (read by dgbexec, ignored by the reference)
     error: bool = False           # run the build with the ERROR diagnostic
     gamcons: bool = False         # run the GAMCONS build
+    cons: bool = False            # run the build with the CONS diagnostic
     workdir: Path | None = None
     _tmp: object = field(default=None, repr=False)
 
@@ -85,7 +87,7 @@ class RefCase:
 
     def run(self, cmd: str, U: np.ndarray | None = None, dt: float = 0.0, nsteps: int = 1,
             repeat: int = 1, timeout: float = 600.0, extra_env: dict | None = None) -> tuple[np.ndarray, str]:
-        exe = binary(self.dim, self.flux, self.n_mass, self.error, self.gamcons)
+        exe = binary(self.dim, self.flux, self.n_mass, self.error, self.gamcons, self.cons)
         if not exe.exists():
             raise FileNotFoundError(f"{exe} missing: run python oracle/build_ref.py")
         args = [str(exe), "-d", "deck.inp", "--cmd", cmd, "--dt", repr(float(dt)), "--nsteps", str(nsteps),

@@ -98,6 +98,17 @@ CASES = [
          flux="roe", limiter="hrl", ic="quadrants", cfl=0.3, dt=5e-4, nsteps=4, n_mass=1),
     dict(name="y2_p1_roe_m2l_box", dim=2, order=1, nx=32, ny=4, dom=(0, 1, 0, 1), bc=("reflective",) * 4,
          flux="roe", limiter="m2l", ic="quadrants", cfl=0.3, dt=5e-4, nsteps=4, n_mass=1),
+    # two and three mass fractions (MASS=2, MASS=3; Y_k marks the region for even k, its complement
+    # for odd k)
+    dict(name="m2_d1_p2_roe_m2l", dim=1, order=2, nx=24, ny=1, dom=(0, 1, 0, 1), bc=("transmissive",) * 2,
+         flux="roe", limiter="m2l", ic="tube_noise", cfl=0.4, dt=4e-4, nsteps=5, n_mass=2),
+    dict(name="m3_d1_p3_hll_hrl_wall", dim=1, order=3, nx=20, ny=1, dom=(0, 1, 0, 1), bc=("reflective",) * 2,
+         flux="hll", limiter="hrl", ic="riemann", cfl=0.2, dt=2e-4, nsteps=5, n_mass=3),
+    dict(name="m2_d2_p2_rus_m2l_walls", dim=2, order=2, nx=32, ny=8, dom=(0, 2, 0, 1),
+         bc=("reflective", "transmissive", "reflective", "transmissive"), flux="rusanov", limiter="m2l",
+         ic="shock_bubble", cfl=0.3, dt=5e-4, nsteps=4, n_mass=2),
+    dict(name="m3_d2_p1_roe_hrl_periodic", dim=2, order=1, nx=32, ny=4, dom=(0, 1, 0, 1), bc=("periodic",) * 4,
+         flux="roe", limiter="hrl", ic="quadrants", cfl=0.3, dt=5e-4, nsteps=4, n_mass=3),
     # the conservative gamma model (the reference built with GAMM=GAMCONS); its M2limiting stops
     # the run for this model, so the limiters are hrl and none
     dict(name="g1_p2_roe_hrl", dim=1, order=2, nx=24, ny=1, dom=(0, 1, 0, 1), bc=("transmissive",) * 2,
@@ -254,11 +265,34 @@ def make_error_fixture() -> dict:
     return out
 
 
+# the reference's CONS diagnostic on the driver deck (sodtube, 60 elements, p = 2, Roe, m2l, CFL
+# 0.4), built with CONS=CONS: conservation.dat (time and the integral of each field after the
+# initial limiting and at every output time)
+CONSCASE = dict(name="driver_d1_sodtube_roe_cons", dim=1, order=2, nx=60, dom=(-0.5, 0.5), flux="roe",
+                limiter="m2l", cfl=0.4, output_times=(0.0, 0.02, 0.05, 0.08))
+
+
+def make_cons_fixture() -> dict:
+    c = CONSCASE
+    ref = RefCase(c["dim"], c["order"], c["nx"], 1, c["dom"][0], c["dom"][1], 0.0, 1.0, ("transmissive",) * 4,
+                  c["flux"], c["limiter"], cfl=c["cfl"], output_times=c["output_times"],
+                  make_options=("FLUX=ROE", "CONS=CONS"), cons=True)
+    ref.write_deck()
+    ref.run("none")
+    out = {"deck": np.array((ref.workdir / "deck.inp").read_text()),
+           "conservation_dat": np.loadtxt(ref.workdir / "conservation.dat")}
+    out["meta"] = np.array(json.dumps(c))
+    return out
+
+
 def main(argv=None) -> int:
     only = set((argv if argv is not None else sys.argv[1:]))
     if ERRCASE["name"] in only:
         np.savez_compressed(OUT / f"{ERRCASE['name']}.npz", **make_error_fixture())
         print(f"wrote {ERRCASE['name']}.npz")
+    if CONSCASE["name"] in only:
+        np.savez_compressed(OUT / f"{CONSCASE['name']}.npz", **make_cons_fixture())
+        print(f"wrote {CONSCASE['name']}.npz")
     if only:  # regenerate the named fixtures only
         for k, c in enumerate(CASES):
             if c["name"] in only:
@@ -271,6 +305,8 @@ def main(argv=None) -> int:
     print(f"wrote {ERRCASE['name']}.npz")
     np.savez_compressed(OUT / f"{DRIVER['name']}.npz", **make_driver_fixture())
     print(f"wrote {DRIVER['name']}.npz")
+    np.savez_compressed(OUT / f"{CONSCASE['name']}.npz", **make_cons_fixture())
+    print(f"wrote {CONSCASE['name']}.npz")
     for k, c in enumerate(CASES):
         data = make_case(c, seed=100 + k)
         np.savez_compressed(OUT / f"{c['name']}.npz", **data)

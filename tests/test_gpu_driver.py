@@ -61,3 +61,30 @@ def test_dgbexec_error_diagnostic_matches_reference(tmp_path):
     for col in (1, 4):                      # rho, 1/(gamma-1)
         assert np.allclose(mine[:, col], ref[:, col], rtol=1e-4, atol=0), (col, mine[:, col], ref[:, col])
     assert np.all(np.abs(mine[:, 2:4]) < 1e-12) and np.all(np.abs(ref[:, 2:4]) < 1e-12)
+
+
+def test_dgbexec_conservation_output_matches_reference(tmp_path):
+    """The reference's CONS build on the driver deck: conservation.dat (time and the domain
+    integral of each field after the initial limiting and at every output time) written by
+    dgbexec against the reference's, within 1e-10 relative per field."""
+    import dg_b200 as dgb
+    d = np.load(GOLDEN / "driver_d1_sodtube_roe_cons.npz")
+    c = json.loads(str(d["meta"]))
+    dgb.write_msh(tmp_path / "mesh.msh", c["dim"], c["order"], c["nx"], 1, c["dom"][0], c["dom"][1], 0.0, 1.0,
+                  ("transmissive",) * 4)
+    (tmp_path / "deck.inp").write_text(str(d["deck"]))
+    assert dgb.Problem.from_deck(tmp_path / "deck.inp").info.cons_output == 1
+    exe = ROOT / "dg_b200" / "lib" / "dgbexec"
+    r = subprocess.run([str(exe), "-d", "deck.inp", "--out", "."], cwd=tmp_path, capture_output=True, text=True,
+                       timeout=300)
+    assert r.returncode == 0, r.stdout + r.stderr
+    mine = np.loadtxt(tmp_path / "conservation.dat")
+    ref = d["conservation_dat"]
+    assert mine.shape == ref.shape == (len(c["output_times"]), 5)
+    assert np.abs(mine[:, 0] - ref[:, 0]).max() <= 1e-15
+    for col in range(1, 5):
+        scale = np.abs(ref[:, col]).max()
+        if scale == 0:
+            assert np.abs(mine[:, col]).max() <= 1e-14
+        else:
+            assert np.abs(mine[:, col] - ref[:, col]).max() <= 1e-10 * scale, (col, mine[:, col], ref[:, col])

@@ -115,6 +115,10 @@ def test_deck_mass_option(tmp_path):
         "#limiter\nm2l\n#initial condition\nsodtube\n")
     prob = dgb.Problem.from_deck(tmp_path / "deck.inp")
     assert prob.info.n_fields == 5
+    assert prob.info.cons_output == 0 and prob.info.error_output == 0
+    (tmp_path / "deck.inp").write_text((tmp_path / "deck.inp").read_text().replace("MASS=1", "CONS=CONS\nERRR=ERROR"))
+    i = dgb.Problem.from_deck(tmp_path / "deck.inp").info
+    assert (i.n_fields, i.cons_output, i.error_output) == (4, 1, 1)
 
 
 def test_gamcons_state_pos_and_deck(tmp_path):
