@@ -29,7 +29,9 @@ EXPORTS = [
     "dgb_sensors", "dgb_set_form", "dgb_mlp_param_count", "dgb_indicator_features", "dgb_indicator_labels",
     "dgb_mlp_forward", "dgb_mlp_backward", "dgb_mlp_adam", "dgb_set_indicator", "dgb_indicator_scores",
     "dgb_cfl_dt", "dgb_batch_create", "dgb_batch_destroy", "dgb_batch_n_classes", "dgb_batch_class_info",
-    "dgb_batch_autotune", "dgb_batch_set_tuning", "dgb_batch_advance", "dgb_problem_error_norms", "dgb_batch_case_stats", "dgb_batch_last_timing",
+    "dgb_batch_autotune", "dgb_batch_set_tuning", "dgb_batch_advance", "dgb_problem_error_norms", "dgb_batch_case_stats",
+    "dgb_batch_last_timing", "dgb_slab_ghost_rows", "dgb_step_begin", "dgb_step_wavespeed_word", "dgb_step_stage",
+    "dgb_step_end", "dgb_halo_count", "dgb_halo_pack", "dgb_halo_unpack", "dgb_stream", "dgb_set_cfl_scale",
 ]
 
 
@@ -120,6 +122,16 @@ def lib() -> C.CDLL:
         "dgb_batch_advance": [vp, ip, C.c_double, C.POINTER(C.c_int)],
         "dgb_batch_case_stats": [vp, dp, C.POINTER(C.c_int), dp],
         "dgb_batch_last_timing": [vp, dp, C.POINTER(C.c_longlong)],
+        "dgb_slab_ghost_rows": [vp, ip, ip],
+        "dgb_step_begin": [vp, ip, C.c_double],
+        "dgb_step_wavespeed_word": [vp, C.POINTER(vp)],
+        "dgb_step_stage": [vp, ip],
+        "dgb_step_end": [vp, dp],
+        "dgb_halo_count": [vp, ip, C.POINTER(C.c_size_t)],
+        "dgb_halo_pack": [vp, ip, vp],
+        "dgb_halo_unpack": [vp, ip, vp],
+        "dgb_stream": [vp, C.POINTER(vp)],
+        "dgb_set_cfl_scale": [vp, C.c_double],
     }
     for name, args in sig.items():
         f = getattr(L, name)

@@ -25,6 +25,12 @@ struct dgb_ctx {
   int nx = 0, ny = 0;
   int nmass = 0;          // passive mass fractions (fields D+3 .. nf-1)
   bool gamcons = false;   // GAMCONS gamma model (fifth field rho/(gamma-1), conservative)
+  // slab mode (dgb_slab_ghost_rows): ghost rows at the bottom / top of a structured grid, filled by
+  // the caller's halo exchange; the phase-level step (dgb_step_*) and its position
+  int halo_lo = 0, halo_hi = 0;
+  double* slab_cur = nullptr;   // the buffer the next stage reads (packed / unpacked by dgb_halo_*)
+  int slab_scheme = 0, slab_next = -1;
+  bool slab_cfl = false;
   bool tiled = false;     // structured row-major grid with tile-multiple extents: tiled residual kernel
   int form = DGB_FORM_FP64;  // arithmetic of the residual: plain FP64 or mixed FP32/FP64
   bool rowmajor = false;  // structured row-major grid: tiled limiter passes

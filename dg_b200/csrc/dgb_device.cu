@@ -595,32 +595,40 @@ int limit_dispatch(dgb_ctx* c, double* U, bool rescore = true) {
   return set_error(DGB_ERR_UNSUPPORTED, "limiter not available on the device path");
 }
 
-void launch_dt(dgb_ctx* c, const double* U, bool cfl) {
-  ProfScope ps(c, KC_DT);
-  if (cfl) {
-    const int grid = std::max(1, std::min(4 * 148, (c->ne + 255) / 256));
+// the wave-speed reduction into scal->umax over the elements the context owns (all of them, or
+// in slab mode the rows between the ghost rows)
+void launch_wavespeed(dgb_ctx* c, const double* Uall) {
+  const int e0 = c->halo_lo * c->nx, n = c->ne - (c->halo_lo + c->halo_hi) * c->nx;
+  const double* U = Uall + e0;  // element offset inside every (field, node) plane of stride ld
+  const int grid = std::max(1, std::min(4 * 148, (n + 255) / 256));
+  {
     if (c->gamcons) {
       switch (c->D * 100 + c->ns) {
-        case 102: wavespeed_kernel<1, 2, true><<<grid, 256, 0, c->st>>>(U, c->ne, c->ld, c->scal); break;
-        case 103: wavespeed_kernel<1, 3, true><<<grid, 256, 0, c->st>>>(U, c->ne, c->ld, c->scal); break;
-        case 104: wavespeed_kernel<1, 4, true><<<grid, 256, 0, c->st>>>(U, c->ne, c->ld, c->scal); break;
-        case 204: wavespeed_kernel<2, 4, true><<<grid, 256, 0, c->st>>>(U, c->ne, c->ld, c->scal); break;
-        case 209: wavespeed_kernel<2, 9, true><<<grid, 256, 0, c->st>>>(U, c->ne, c->ld, c->scal); break;
-        case 216: wavespeed_kernel<2, 16, true><<<grid, 256, 0, c->st>>>(U, c->ne, c->ld, c->scal); break;
+        case 102: wavespeed_kernel<1, 2, true><<<grid, 256, 0, c->st>>>(U, n, c->ld, c->scal); break;
+        case 103: wavespeed_kernel<1, 3, true><<<grid, 256, 0, c->st>>>(U, n, c->ld, c->scal); break;
+        case 104: wavespeed_kernel<1, 4, true><<<grid, 256, 0, c->st>>>(U, n, c->ld, c->scal); break;
+        case 204: wavespeed_kernel<2, 4, true><<<grid, 256, 0, c->st>>>(U, n, c->ld, c->scal); break;
+        case 209: wavespeed_kernel<2, 9, true><<<grid, 256, 0, c->st>>>(U, n, c->ld, c->scal); break;
+        case 216: wavespeed_kernel<2, 16, true><<<grid, 256, 0, c->st>>>(U, n, c->ld, c->scal); break;
         default: break;
       }
     } else
     switch (c->D * 100 + c->ns) {
-      case 102: wavespeed_kernel<1, 2><<<grid, 256, 0, c->st>>>(U, c->ne, c->ld, c->scal); break;
-      case 103: wavespeed_kernel<1, 3><<<grid, 256, 0, c->st>>>(U, c->ne, c->ld, c->scal); break;
-      case 104: wavespeed_kernel<1, 4><<<grid, 256, 0, c->st>>>(U, c->ne, c->ld, c->scal); break;
-      case 204: wavespeed_kernel<2, 4><<<grid, 256, 0, c->st>>>(U, c->ne, c->ld, c->scal); break;
-      case 209: wavespeed_kernel<2, 9><<<grid, 256, 0, c->st>>>(U, c->ne, c->ld, c->scal); break;
-      case 216: wavespeed_kernel<2, 16><<<grid, 256, 0, c->st>>>(U, c->ne, c->ld, c->scal); break;
+      case 102: wavespeed_kernel<1, 2><<<grid, 256, 0, c->st>>>(U, n, c->ld, c->scal); break;
+      case 103: wavespeed_kernel<1, 3><<<grid, 256, 0, c->st>>>(U, n, c->ld, c->scal); break;
+      case 104: wavespeed_kernel<1, 4><<<grid, 256, 0, c->st>>>(U, n, c->ld, c->scal); break;
+      case 204: wavespeed_kernel<2, 4><<<grid, 256, 0, c->st>>>(U, n, c->ld, c->scal); break;
+      case 209: wavespeed_kernel<2, 9><<<grid, 256, 0, c->st>>>(U, n, c->ld, c->scal); break;
+      case 216: wavespeed_kernel<2, 16><<<grid, 256, 0, c->st>>>(U, n, c->ld, c->scal); break;
       default: break;
     }
     c->counter++;
   }
+}
+
+void launch_dt(dgb_ctx* c, const double* U, bool cfl) {
+  ProfScope ps(c, KC_DT);
+  if (cfl) launch_wavespeed(c, U);
   finish_dt_kernel<<<1, 1, 0, c->st>>>(c->scal, c->cs.cfl_scaled);
 }
 
@@ -632,57 +640,63 @@ StageArgs stage_args(dgb_ctx* c) {
   return a;
 }
 
-// One SSP-RK3 step on c->A (Shu-Osher form); limiter after every stage.
-int step_ssprk3(dgb_ctx* c, bool cfl) {
-  launch_dt(c, c->A, cfl);
-  if (c->ind_on) launch_indicator(c, c->A);  // the learned indicator's band, once per step
-  StageArgs a = stage_args(c);
+// Stage s (0..2) of an SSP-RK3 step on c->A (Shu-Osher form), limiter included: reads
+// {A, B, C}[s], writes {B, C, A}[s].
+int ssp_stage(dgb_ctx* c, int s) {
   const double coef[3][2] = {{0.0, 1.0}, {0.75, 0.25}, {1.0 / 3.0, 2.0 / 3.0}};
   double* in[3] = {c->A, c->B, c->C};
   double* out[3] = {c->B, c->C, c->A};
-  for (int s = 0; s < 3; ++s) {
-    a.U = in[s];
-    a.Ubase = c->A;
-    const bool fused = c->fused_lim && !c->ind_on;
-    a.out = fused ? c->X : out[s];  // the fused limiter then writes the stage output
-    a.a = coef[s][0];
-    a.b = coef[s][1];
-    if (int rc = residual_dispatch<MODE_SSP>(c, a)) return rc;
-    if (fused) {
-      if (int rc = limit_to(c, c->X, out[s])) return rc;
-    } else if (int rc = limit_dispatch(c, out[s], false)) {
-      return rc;
-    }
-  }
+  StageArgs a = stage_args(c);
+  a.U = in[s];
+  a.Ubase = c->A;
+  const bool fused = c->fused_lim && !c->ind_on;
+  a.out = fused ? c->X : out[s];  // the fused limiter then writes the stage output
+  a.a = coef[s][0];
+  a.b = coef[s][1];
+  if (int rc = residual_dispatch<MODE_SSP>(c, a)) return rc;
+  if (fused) return limit_to(c, c->X, out[s]);
+  return limit_dispatch(c, out[s], false);
+}
+
+// One SSP-RK3 step on c->A; limiter after every stage.
+int step_ssprk3(dgb_ctx* c, bool cfl) {
+  launch_dt(c, c->A, cfl);
+  if (c->ind_on) launch_indicator(c, c->A);  // the learned indicator's band, once per step
+  for (int s = 0; s < 3; ++s)
+    if (int rc = ssp_stage(c, s)) return rc;
   return 0;
 }
 
-// One classical RK4 step in the reference's form (rk.cc:155-209): A = U, B = Us, C = Ustar.
+// Stage k (0..3) of a classical RK4 step in the reference's form (rk.cc:155-209): A = U, B = Us,
+// C = Ustar.  The residual of the stage input (B for k = 0, C after) is accumulated into A; then
+// the next stage's input C = Us + beta DU is formed and limited, or after the last stage A is
+// limited.
+int rk4_stage(dgb_ctx* c, int k) {
+  const double beta[4] = {0.0, 0.5, 0.5, 1.0};
+  const double gam[4] = {1.0 / 6.0, 2.0 / 6.0, 2.0 / 6.0, 1.0 / 6.0};
+  StageArgs a = stage_args(c);
+  a.U = k == 0 ? c->B : c->C;
+  a.out = c->DU;
+  a.Uacc = c->A;
+  a.b = gam[k];
+  if (int rc = residual_dispatch<MODE_RK4>(c, a)) return rc;
+  if (k == 3) return limit_dispatch(c, c->A, false);
+  const int grid = (int)std::min<size_t>((c->nstate + 255) / 256, 148 * 16);
+  {
+    ProfScope ps(c, KC_OTHER);
+    axpy_kernel<<<grid, 256, 0, c->st>>>(c->B, c->DU, beta[k + 1], c->C, c->nstate, c->scal);
+  }
+  return limit_dispatch(c, c->C, false);
+}
+
+// One classical RK4 step.
 int step_rk4(dgb_ctx* c, bool cfl) {
   launch_dt(c, c->A, cfl);
   if (c->ind_on) launch_indicator(c, c->A);  // the learned indicator's band, once per step
-  const double beta[4] = {0.0, 0.5, 0.5, 1.0};
-  const double gam[4] = {1.0 / 6.0, 2.0 / 6.0, 2.0 / 6.0, 1.0 / 6.0};
   cudaMemcpyAsync(c->B, c->A, c->nstate * sizeof(double), cudaMemcpyDeviceToDevice, c->st);
-  StageArgs a = stage_args(c);
-  for (int k = 0; k < 4; ++k) {
-    const double* in = c->B;
-    if (k > 0) {
-      const int grid = (int)std::min<size_t>((c->nstate + 255) / 256, 148 * 16);
-      {
-        ProfScope ps(c, KC_OTHER);
-        axpy_kernel<<<grid, 256, 0, c->st>>>(c->B, c->DU, beta[k], c->C, c->nstate, c->scal);
-      }
-      if (int rc = limit_dispatch(c, c->C, false)) return rc;
-      in = c->C;
-    }
-    a.U = in;
-    a.out = c->DU;
-    a.Uacc = c->A;
-    a.b = gam[k];
-    if (int rc = residual_dispatch<MODE_RK4>(c, a)) return rc;
-  }
-  return limit_dispatch(c, c->A, false);
+  for (int k = 0; k < 4; ++k)
+    if (int rc = rk4_stage(c, k)) return rc;
+  return 0;
 }
 
 int to_internal(dgb_ctx* c, const double* Uref_dev, double* Uint) {
@@ -1218,6 +1232,157 @@ extern "C" int dgb_advance(dgb_ctx* c, int scheme, int nsteps, double dt, double
   if (c->h_scal->flags & FLAG_TIMEOUT) return set_error(DGB_ERR_TIMEOUT, "a bounded device wait expired");
   if (c->h_scal->flags & FLAG_NONFINITE) return set_error(DGB_ERR_NONFINITE, "time step is NaN");
   if (c->h_scal->flags & FLAG_DT_SMALL) return set_error(DGB_ERR_DT_SMALL, "next time step is too small (< 1e-14)");
+  return DGB_OK;
+}
+
+// ------------------------------------------------------------------------------------------
+// Slab mode: a y-slab of a larger structured grid with ghost rows, stepped phase by phase so that
+// the caller can exchange the ghost rows between the stages (the reference's ghost exchange,
+// COMMUNICATOR::CommunicateGhosts before every residual and limiter pass, rk.cc:108-114, 173,
+// 203-209, done here per slab boundary instead of per ghost element)
+// ------------------------------------------------------------------------------------------
+extern "C" int dgb_slab_ghost_rows(dgb_ctx* c, int lo, int hi) {
+  if (!c) return set_error(DGB_ERR_ARG, "null context");
+  if (!c->rowmajor) return set_error(DGB_ERR_UNSUPPORTED, "slab mode needs a structured row-major 2D grid");
+  const int owned = c->ny - lo - hi;
+  if (lo < 0 || hi < 0 || owned < 1 || owned < lo || owned < hi)
+    return set_error(DGB_ERR_ARG, "ghost rows: 0 <= lo, hi and at least max(lo, hi, 1) owned rows");
+  if (c->ind_on) return set_error(DGB_ERR_UNSUPPORTED, "slab mode does not take the learned indicator");
+  if (c->limiter != DGB_LIM_NONE && c->limiter != DGB_LIM_HRL && c->limiter != DGB_LIM_M2L &&
+      c->limiter != DGB_LIM_PRL)
+    return set_error(DGB_ERR_UNSUPPORTED, "slab mode: the sensor-gated limiters reach three rows; use none, hrl, m2l or prl");
+  c->halo_lo = lo;
+  c->halo_hi = hi;
+  return DGB_OK;
+}
+
+namespace {
+int nstages(int scheme) { return scheme == DGB_RK4 ? 4 : 3; }
+double* slab_state(dgb_ctx* c) { return c->slab_cur ? c->slab_cur : c->A; }
+}  // namespace
+
+extern "C" int dgb_set_cfl_scale(dgb_ctx* c, double cfl_scaled) {
+  if (!c) return set_error(DGB_ERR_ARG, "null context");
+  if (!std::isfinite(cfl_scaled)) return set_error(DGB_ERR_ARG, "CFL scale must be finite");
+  c->cs.cfl_scaled = cfl_scaled;
+  for (auto& row : c->graphs)  // captured steps hold the old value
+    for (auto& g : row)
+      if (g) { cudaGraphExecDestroy(g); g = nullptr; }
+  return DGB_OK;
+}
+
+extern "C" int dgb_step_begin(dgb_ctx* c, int scheme, double dt) {
+  if (!c) return set_error(DGB_ERR_ARG, "null context");
+  if (scheme != DGB_SSPRK3 && scheme != DGB_RK4) return set_error(DGB_ERR_ARG, "scheme must be 3 or 4");
+  if (!(dt > 0) && !(c->cs.cfl_scaled > 0)) return set_error(DGB_ERR_ARG, "no fixed dt and no positive CFL");
+  if (c->ind_on) return set_error(DGB_ERR_UNSUPPORTED, "the phase-level step does not take the learned indicator");
+  if (c->slab_next >= 0) return set_error(DGB_ERR_ARG, "a step is already open (dgb_step_end first)");
+  DGB_CUDA(cudaSetDevice(c->device));
+  c->slab_cfl = !(dt > 0);
+  if (int rc = reset_scalars(c, c->slab_cfl ? 0.0 : dt)) return rc;
+  c->slab_scheme = scheme;
+  c->slab_next = 0;
+  c->slab_cur = c->A;
+  c->counter = 0;
+  DGB_CUDA(cudaEventRecord(c->e0, c->st));
+  if (c->slab_cfl) {
+    ProfScope ps(c, KC_DT);
+    launch_wavespeed(c, c->A);  // owned rows only
+  }
+  DGB_CUDA(cudaGetLastError());
+  return DGB_OK;
+}
+
+extern "C" int dgb_step_wavespeed_word(dgb_ctx* c, void** umax_dev) {
+  if (!c || !umax_dev) return set_error(DGB_ERR_ARG, "null argument");
+  *umax_dev = &c->scal->umax;
+  return DGB_OK;
+}
+
+extern "C" int dgb_step_stage(dgb_ctx* c, int k) {
+  if (!c) return set_error(DGB_ERR_ARG, "null context");
+  if (c->slab_next < 0 || k != c->slab_next || k >= nstages(c->slab_scheme))
+    return set_error(DGB_ERR_ARG, "stages run in order 0.. after dgb_step_begin");
+  if (k == 0) {
+    {
+      ProfScope ps(c, KC_DT);
+      finish_dt_kernel<<<1, 1, 0, c->st>>>(c->scal, c->cs.cfl_scaled);
+    }
+    if (c->slab_scheme == DGB_RK4)
+      DGB_CUDA(cudaMemcpyAsync(c->B, c->A, c->nstate * sizeof(double), cudaMemcpyDeviceToDevice, c->st));
+  }
+  int rc;
+  if (c->slab_scheme == DGB_RK4) {
+    rc = rk4_stage(c, k);
+    c->slab_cur = k < 3 ? c->C : c->A;
+  } else {
+    rc = ssp_stage(c, k);
+    c->slab_cur = k == 0 ? c->B : (k == 1 ? c->C : c->A);
+  }
+  if (rc) return rc;
+  c->slab_next = k + 1;
+  DGB_CUDA(cudaGetLastError());
+  return DGB_OK;
+}
+
+extern "C" int dgb_step_end(dgb_ctx* c, double* time) {
+  if (!c) return set_error(DGB_ERR_ARG, "null context");
+  if (c->slab_next != nstages(c->slab_scheme)) return set_error(DGB_ERR_ARG, "the step's stages have not all run");
+  c->slab_next = -1;
+  c->slab_cur = nullptr;
+  DGB_CUDA(cudaEventRecord(c->e1, c->st));
+  if (int rc = read_scalars(c)) return rc;
+  float ms = 0;
+  cudaEventElapsedTime(&ms, c->e0, c->e1);
+  c->last_ms = ms;
+  c->last_launches = c->counter;
+  if (time) *time += c->h_scal->time;
+  if (c->h_scal->flags & FLAG_TIMEOUT) return set_error(DGB_ERR_TIMEOUT, "a bounded device wait expired");
+  if (c->h_scal->flags & FLAG_NONFINITE) return set_error(DGB_ERR_NONFINITE, "time step is NaN");
+  if (c->h_scal->flags & FLAG_DT_SMALL) return set_error(DGB_ERR_DT_SMALL, "next time step is too small (< 1e-14)");
+  return DGB_OK;
+}
+
+extern "C" int dgb_halo_count(dgb_ctx* c, int side, size_t* n) {
+  if (!c || !n) return set_error(DGB_ERR_ARG, "null argument");
+  if (side != 0 && side != 1) return set_error(DGB_ERR_ARG, "side is 0 (bottom) or 1 (top)");
+  *n = (size_t)(side == 0 ? c->halo_lo : c->halo_hi) * c->nx * c->nf * c->ns;
+  return DGB_OK;
+}
+
+// rows r0 .. r0 + g - 1 of every (field, node) plane <-> buf[(plane * g + row) * nx + col]
+static int halo_copy(dgb_ctx* c, int r0, int g, double* buf, bool pack) {
+  double* U = slab_state(c);
+  const size_t w = (size_t)g * c->nx * sizeof(double), planes = (size_t)c->nf * c->ns;
+  if (g == 0) return DGB_OK;
+  DGB_CUDA(cudaSetDevice(c->device));
+  if (pack)
+    DGB_CUDA(cudaMemcpy2DAsync(buf, w, U + (size_t)r0 * c->nx, (size_t)c->ld * sizeof(double), w, planes,
+                               cudaMemcpyDeviceToDevice, c->st));
+  else
+    DGB_CUDA(cudaMemcpy2DAsync(U + (size_t)r0 * c->nx, (size_t)c->ld * sizeof(double), buf, w, w, planes,
+                               cudaMemcpyDeviceToDevice, c->st));
+  return DGB_OK;
+}
+
+extern "C" int dgb_halo_pack(dgb_ctx* c, int side, double* dst_dev) {
+  if (!c || !dst_dev) return set_error(DGB_ERR_ARG, "null argument");
+  if (side != 0 && side != 1) return set_error(DGB_ERR_ARG, "side is 0 (bottom) or 1 (top)");
+  // the owned rows next to the side, as many as that side has ghost rows
+  return side == 0 ? halo_copy(c, c->halo_lo, c->halo_lo, dst_dev, true)
+                   : halo_copy(c, c->ny - 2 * c->halo_hi, c->halo_hi, dst_dev, true);
+}
+
+extern "C" int dgb_halo_unpack(dgb_ctx* c, int side, const double* src_dev) {
+  if (!c || !src_dev) return set_error(DGB_ERR_ARG, "null argument");
+  if (side != 0 && side != 1) return set_error(DGB_ERR_ARG, "side is 0 (bottom) or 1 (top)");
+  double* src = const_cast<double*>(src_dev);
+  return side == 0 ? halo_copy(c, 0, c->halo_lo, src, false) : halo_copy(c, c->ny - c->halo_hi, c->halo_hi, src, false);
+}
+
+extern "C" int dgb_stream(dgb_ctx* c, void** stream) {
+  if (!c || !stream) return set_error(DGB_ERR_ARG, "null argument");
+  *stream = (void*)c->st;
   return DGB_OK;
 }
 

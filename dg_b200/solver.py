@@ -215,6 +215,48 @@ class DGSolver:
         F.check(F.lib().dgb_conservation(self._h, F.dptr(tot)))
         return tot
 
+    # --- slab mode and the phase-level step (dgb_slab_ghost_rows, dgb_step_*, dgb_halo_*) ---------
+    def set_ghost_rows(self, lo: int, hi: int) -> None:
+        F.check(F.lib().dgb_slab_ghost_rows(self._h, int(lo), int(hi)))
+
+    def set_cfl_scale(self, cfl_scaled: float) -> None:
+        F.check(F.lib().dgb_set_cfl_scale(self._h, float(cfl_scaled)))
+
+    def step_begin(self, scheme: int, dt: float) -> None:
+        F.check(F.lib().dgb_step_begin(self._h, int(scheme), float(dt)))
+
+    def wavespeed_word(self) -> int:
+        """Device address of the step's max-wave-speed word (uint64 bits of a non-negative double)."""
+        p = C.c_void_p()
+        F.check(F.lib().dgb_step_wavespeed_word(self._h, C.byref(p)))
+        return int(p.value)
+
+    def step_stage(self, k: int) -> None:
+        F.check(F.lib().dgb_step_stage(self._h, int(k)))
+
+    def step_end(self) -> tuple[int, float]:
+        """(status, dt of the step); the status is not raised so that slabs can agree on it first."""
+        t = C.c_double(0.0)
+        rc = F.lib().dgb_step_end(self._h, C.byref(t))
+        return rc, t.value
+
+    def halo_count(self, side: int) -> int:
+        n = C.c_size_t()
+        F.check(F.lib().dgb_halo_count(self._h, int(side), C.byref(n)))
+        return n.value
+
+    def halo_pack(self, side: int, dst_ptr: int) -> None:
+        F.check(F.lib().dgb_halo_pack(self._h, int(side), C.c_void_p(dst_ptr)))
+
+    def halo_unpack(self, side: int, src_ptr: int) -> None:
+        F.check(F.lib().dgb_halo_unpack(self._h, int(side), C.c_void_p(src_ptr)))
+
+    def stream(self) -> int:
+        """The context's cudaStream_t as an integer."""
+        p = C.c_void_p()
+        F.check(F.lib().dgb_stream(self._h, C.byref(p)))
+        return int(p.value or 0)
+
 
 class DGBatch:
     """Batched ensemble (dgb_batch_*): independent problems, one DGSolver each, advanced together

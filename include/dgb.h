@@ -215,6 +215,37 @@ int dgb_advance(dgb_ctx* c, int scheme, int nsteps, double dt, double* time);
 /* Last step size used by dgb_advance (host copy). */
 int dgb_last_dt(dgb_ctx* c, double* dt);
 
+/* ------------------------------------------------------------------------------------
+ * Slab mode: one y-slab of a larger structured 2D grid per context (the reference's MPI
+ * decomposition, simpleMesh.cc:1006-1074, with its per-element ghost exchange,
+ * communicator_cpu.cc:14-59, replaced by whole ghost rows).  The context's grid is the slab
+ * plus `lo` ghost rows below and `hi` above (rows of elements, nx each); a stage reaches two rows
+ * deep (residual, then the limiter's y pass), so a slab neighbour needs 2 ghost rows.  The caller
+ * moves the rows between slabs (NCCL, peer copies, or in one process):
+ *   dgb_step_begin                    local CFL wave speed over the owned rows
+ *   [MAX-reduce the word of dgb_step_wavespeed_word over the slabs, as 64-bit integers]
+ *   for k in 0 .. stages-1:           (SSP-RK3: 3, RK4: 4)
+ *     [dgb_halo_pack both sides, send / receive, dgb_halo_unpack both sides]
+ *     dgb_step_stage(k)                residual, stage update, limiter
+ *   dgb_step_end                       status and the step's dt added to *time
+ * Pack / unpack act on the buffer the next stage reads (outside a step: the resident state);
+ * all work is queued on the context's stream (dgb_stream).  Interior slabs give the same
+ * result as the whole grid advanced by dgb_advance. */
+int dgb_slab_ghost_rows(dgb_ctx* c, int lo, int hi);
+/* Replaces the CFL scale CFL * Dx / (2p+1) of the context's CFL step (main.cc:896-897): the slabs
+ * of one grid take one value (their own meshes can give it one ulp apart). */
+int dgb_set_cfl_scale(dgb_ctx* c, double cfl_scaled);
+int dgb_step_begin(dgb_ctx* c, int scheme, double dt);
+int dgb_step_wavespeed_word(dgb_ctx* c, void** umax_dev);  /* device uint64: bits of max |u|+a */
+int dgb_step_stage(dgb_ctx* c, int k);
+int dgb_step_end(dgb_ctx* c, double* time);
+/* doubles per side (0 bottom, 1 top): ghost rows x nx x N_F x N_s, laid out
+ * buf[((f * N_s + node) * rows + row) * nx + col] */
+int dgb_halo_count(dgb_ctx* c, int side, size_t* n);
+int dgb_halo_pack(dgb_ctx* c, int side, double* dst_dev);
+int dgb_halo_unpack(dgb_ctx* c, int side, const double* src_dev);
+int dgb_stream(dgb_ctx* c, void** stream);  /* the context's cudaStream_t */
+
 /* Conserved totals sum_e sum_g U_g J w_g per field (DG_SOLVER::conservation, dg_solver.h:367). */
 int dgb_conservation(dgb_ctx* c, double* totals /* N_F */);
 
