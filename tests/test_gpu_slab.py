@@ -2,7 +2,7 @@
 process on its own device context, ghost rows refreshed before every stage by device-to-device
 copies and the CFL wave speed max-reduced over the slabs (dg_b200.slab.LocalTransport), against the
 whole grid advanced by dgb_advance.  Walls, periodic and transmissive y boundaries; p = 1..3;
-SSP-RK3 and RK4; CFL and fixed steps; hrl, m2l, none; a mass fraction.  The owned rows must match
+SSP-RK3 and RK4; CFL and fixed steps; hrl, m2l, none; a mass fraction; GAMCONS.  The owned rows must match
 the whole-grid run within 1e-13 of the state's scale (the slabs' meshes and the whole grid's differ
 in the last bit of their coordinates on non-dyadic extents), and the time advanced must agree.
 Without the exchange the slabs drift apart from the whole-grid run (negative control)."""
@@ -25,6 +25,8 @@ CASES = [
     ("p1_rus_none_walls_4", 1, 64, 32, 4, WALLS, "rusanov", "none", "quadrants", dgb.SSPRK3, 2e-4, 10, {}),
     ("p2_rus_m2l_periodic_2", 2, 32, 24, 2, PERIODIC_Y, "rusanov", "m2l", "quadrants", dgb.SSPRK3, 0.0, 8, {}),
     ("p2_roe_m2l_walls_3_y1", 2, 64, 40, 3, WALLS, "roe", "m2l", "shock_bubble", dgb.SSPRK3, 0.0, 8, {"n_mass": 1}),
+    ("p2_roe_hrl_walls_2_gamcons", 2, 64, 32, 2, WALLS, "roe", "hrl", "shock_bubble", dgb.RK4, 0.0, 6,
+     {"gamma_model": "gamcons"}),
 ]
 
 
