@@ -31,6 +31,9 @@ struct StageArgs {
   const double* __restrict__ Ubase;  // SSP: U^n
   double* __restrict__ out;
   double* __restrict__ Uacc;         // RK4 accumulator (may be null)
+  double* __restrict__ Unext;        // RK4 (1D): the next stage input Us + beta_next * DU, or null
+  const double* __restrict__ Us;     //   its Us
+  double beta_next;
   const int* __restrict__ nbr;       // [face][ld] neighbours, boundary codes < 0
   const DevScalars* __restrict__ scal;
   double a, b;
@@ -342,6 +345,7 @@ __device__ __forceinline__ void res1d_body(const Consts& c, const StageArgs& a, 
       } else {
         a.out[gi] = du;
         if (a.Uacc) a.Uacc[gi] += a.b * du;
+        if (a.Unext) a.Unext[gi] = __ldg(a.Us + gi) + a.beta_next * du;  // rk.cc:164-170
       }
     }
 }
@@ -664,9 +668,12 @@ __global__ void __launch_bounds__(128) lim1d_kernel(const LimArgs la, const doub
 // ------------------------------------------------------------------------------------------
 // CFL step: max over nodes of the wave speed, then dt = CFL_scaled / max (on the device)
 // ------------------------------------------------------------------------------------------
+// copy_to (1D RK4, or null): the nf fields of every element read are also written there (the
+// step's accumulator starts as the state)
 template <int DIM, int NS, bool GC = false>
 __global__ void __launch_bounds__(256) wavespeed_kernel(const double* __restrict__ U, int n_elem, int ld,
-                                                        DevScalars* __restrict__ scal) {
+                                                        DevScalars* __restrict__ scal,
+                                                        double* __restrict__ copy_to, int nf) {
   if (scal->flags) return;
   double m = 0.0;
   bool bad = false;
@@ -683,6 +690,8 @@ __global__ void __launch_bounds__(256) wavespeed_kernel(const double* __restrict
                                __ldg(U + (size_t)(4 * NS + t) * ld + e));
       if (!(w == w)) bad = true;
       else m = fmax(m, fabs(w));
+      if (copy_to)
+        for (int f = 0; f < nf; ++f) copy_to[(size_t)(f * NS + t) * ld + e] = __ldg(U + (size_t)(f * NS + t) * ld + e);
     }
   }
 #pragma unroll

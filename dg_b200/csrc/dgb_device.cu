@@ -597,38 +597,38 @@ int limit_dispatch(dgb_ctx* c, double* U, bool rescore = true) {
 
 // the wave-speed reduction into scal->umax over the elements the context owns (all of them, or
 // in slab mode the rows between the ghost rows)
-void launch_wavespeed(dgb_ctx* c, const double* Uall) {
+void launch_wavespeed(dgb_ctx* c, const double* Uall, double* copy_to = nullptr) {
   const int e0 = c->halo_lo * c->nx, n = c->ne - (c->halo_lo + c->halo_hi) * c->nx;
   const double* U = Uall + e0;  // element offset inside every (field, node) plane of stride ld
   const int grid = std::max(1, std::min(4 * 148, (n + 255) / 256));
   {
     if (c->gamcons) {
       switch (c->D * 100 + c->ns) {
-        case 102: wavespeed_kernel<1, 2, true><<<grid, 256, 0, c->st>>>(U, n, c->ld, c->scal); break;
-        case 103: wavespeed_kernel<1, 3, true><<<grid, 256, 0, c->st>>>(U, n, c->ld, c->scal); break;
-        case 104: wavespeed_kernel<1, 4, true><<<grid, 256, 0, c->st>>>(U, n, c->ld, c->scal); break;
-        case 204: wavespeed_kernel<2, 4, true><<<grid, 256, 0, c->st>>>(U, n, c->ld, c->scal); break;
-        case 209: wavespeed_kernel<2, 9, true><<<grid, 256, 0, c->st>>>(U, n, c->ld, c->scal); break;
-        case 216: wavespeed_kernel<2, 16, true><<<grid, 256, 0, c->st>>>(U, n, c->ld, c->scal); break;
+        case 102: wavespeed_kernel<1, 2, true><<<grid, 256, 0, c->st>>>(U, n, c->ld, c->scal, copy_to, c->nf); break;
+        case 103: wavespeed_kernel<1, 3, true><<<grid, 256, 0, c->st>>>(U, n, c->ld, c->scal, copy_to, c->nf); break;
+        case 104: wavespeed_kernel<1, 4, true><<<grid, 256, 0, c->st>>>(U, n, c->ld, c->scal, copy_to, c->nf); break;
+        case 204: wavespeed_kernel<2, 4, true><<<grid, 256, 0, c->st>>>(U, n, c->ld, c->scal, copy_to, c->nf); break;
+        case 209: wavespeed_kernel<2, 9, true><<<grid, 256, 0, c->st>>>(U, n, c->ld, c->scal, copy_to, c->nf); break;
+        case 216: wavespeed_kernel<2, 16, true><<<grid, 256, 0, c->st>>>(U, n, c->ld, c->scal, copy_to, c->nf); break;
         default: break;
       }
     } else
     switch (c->D * 100 + c->ns) {
-      case 102: wavespeed_kernel<1, 2><<<grid, 256, 0, c->st>>>(U, n, c->ld, c->scal); break;
-      case 103: wavespeed_kernel<1, 3><<<grid, 256, 0, c->st>>>(U, n, c->ld, c->scal); break;
-      case 104: wavespeed_kernel<1, 4><<<grid, 256, 0, c->st>>>(U, n, c->ld, c->scal); break;
-      case 204: wavespeed_kernel<2, 4><<<grid, 256, 0, c->st>>>(U, n, c->ld, c->scal); break;
-      case 209: wavespeed_kernel<2, 9><<<grid, 256, 0, c->st>>>(U, n, c->ld, c->scal); break;
-      case 216: wavespeed_kernel<2, 16><<<grid, 256, 0, c->st>>>(U, n, c->ld, c->scal); break;
+      case 102: wavespeed_kernel<1, 2><<<grid, 256, 0, c->st>>>(U, n, c->ld, c->scal, copy_to, c->nf); break;
+      case 103: wavespeed_kernel<1, 3><<<grid, 256, 0, c->st>>>(U, n, c->ld, c->scal, copy_to, c->nf); break;
+      case 104: wavespeed_kernel<1, 4><<<grid, 256, 0, c->st>>>(U, n, c->ld, c->scal, copy_to, c->nf); break;
+      case 204: wavespeed_kernel<2, 4><<<grid, 256, 0, c->st>>>(U, n, c->ld, c->scal, copy_to, c->nf); break;
+      case 209: wavespeed_kernel<2, 9><<<grid, 256, 0, c->st>>>(U, n, c->ld, c->scal, copy_to, c->nf); break;
+      case 216: wavespeed_kernel<2, 16><<<grid, 256, 0, c->st>>>(U, n, c->ld, c->scal, copy_to, c->nf); break;
       default: break;
     }
     c->counter++;
   }
 }
 
-void launch_dt(dgb_ctx* c, const double* U, bool cfl) {
+void launch_dt(dgb_ctx* c, const double* U, bool cfl, double* copy_to = nullptr) {
   ProfScope ps(c, KC_DT);
-  if (cfl) launch_wavespeed(c, U);
+  if (cfl) launch_wavespeed(c, U, copy_to);
   finish_dt_kernel<<<1, 1, 0, c->st>>>(c->scal, c->cs.cfl_scaled);
 }
 
@@ -658,8 +658,90 @@ int ssp_stage(dgb_ctx* c, int s) {
   return limit_dispatch(c, out[s], false);
 }
 
+// 1D hrl / m2l limiter from `in` into `out` (no copy back): the 1D steps write the limited stage
+// output straight into the buffer the next stage reads
+template <int P, int METHOD, int NY>
+void launch_lim1d_to(dgb_ctx* c, const double* in, double* out) {
+  ProfScope ps(c, KC_LIMITER);
+  const LimArgs la{c->ld, c->ne};
+  lim1d_kernel<P, METHOD, NY><<<(c->ne + 127) / 128, 128, 0, c->st>>>(la, in, c->nbr, out, c->scal);
+}
+
+template <int NY>
+int limit1d_to_ny(dgb_ctx* c, const double* in, double* out) {
+  switch (c->p * 10 + c->limiter) {
+    case 11: launch_lim1d_to<1, 1, NY>(c, in, out); return 0;
+    case 12: launch_lim1d_to<1, 2, NY>(c, in, out); return 0;
+    case 21: launch_lim1d_to<2, 1, NY>(c, in, out); return 0;
+    case 22: launch_lim1d_to<2, 2, NY>(c, in, out); return 0;
+    case 31: launch_lim1d_to<3, 1, NY>(c, in, out); return 0;
+    case 32: launch_lim1d_to<3, 2, NY>(c, in, out); return 0;
+    default: return set_error(DGB_ERR_UNSUPPORTED, "limiter not available on the device path");
+  }
+}
+
+int limit1d_to(dgb_ctx* c, const double* in, double* out) {
+  switch (c->nmass) {
+    case 0: return limit1d_to_ny<0>(c, in, out);
+    case 1: return limit1d_to_ny<1>(c, in, out);
+    case 2: return limit1d_to_ny<2>(c, in, out);
+    case 3: return limit1d_to_ny<3>(c, in, out);
+    default: return set_error(DGB_ERR_UNSUPPORTED, "at most three mass fractions on the device path");
+  }
+}
+
+// 1D with the plain hrl / m2l limiter: steps without device copies (the multi-kernel step of a
+// small 1D problem is launch-latency bound, so every graph node counts)
+bool lim1d_direct(const dgb_ctx* c) {
+  return c->D == 1 && !c->gated && !c->ind_on && (c->limiter == DGB_LIM_HRL || c->limiter == DGB_LIM_M2L);
+}
+
+// SSP-RK3, 1D: stage inputs A, X, B; unlimited outputs B, C, X; limited into X, B, A
+int step1d_ssprk3(dgb_ctx* c, bool cfl) {
+  launch_dt(c, c->A, cfl);
+  const double coef[3][2] = {{0.0, 1.0}, {0.75, 0.25}, {1.0 / 3.0, 2.0 / 3.0}};
+  const double* in[3] = {c->A, c->X, c->B};
+  double* raw[3] = {c->B, c->C, c->X};
+  double* lim[3] = {c->X, c->B, c->A};
+  for (int s = 0; s < 3; ++s) {
+    StageArgs a = stage_args(c);
+    a.U = in[s];
+    a.Ubase = c->A;
+    a.out = raw[s];
+    a.a = coef[s][0];
+    a.b = coef[s][1];
+    if (int rc = residual_dispatch<MODE_SSP>(c, a)) return rc;
+    if (int rc = limit1d_to(c, raw[s], lim[s])) return rc;
+  }
+  return 0;
+}
+
+// RK4, 1D: Us = A unchanged through the step, accumulator X (copied from A by the CFL reduction),
+// stage k's residual also forms the next input C = Us + beta DU, limited into B; the last stage's
+// accumulator is limited into A
+int step1d_rk4(dgb_ctx* c, bool cfl) {
+  launch_dt(c, c->A, cfl, cfl ? c->X : nullptr);
+  if (!cfl) cudaMemcpyAsync(c->X, c->A, c->nstate * sizeof(double), cudaMemcpyDeviceToDevice, c->st);
+  const double beta[4] = {0.0, 0.5, 0.5, 1.0};
+  const double gam[4] = {1.0 / 6.0, 2.0 / 6.0, 2.0 / 6.0, 1.0 / 6.0};
+  for (int k = 0; k < 4; ++k) {
+    StageArgs a = stage_args(c);
+    a.U = k == 0 ? c->A : c->B;
+    a.out = c->DU;
+    a.Uacc = c->X;
+    a.b = gam[k];
+    a.Unext = k < 3 ? c->C : nullptr;
+    a.Us = c->A;
+    a.beta_next = k < 3 ? beta[k + 1] : 0.0;
+    if (int rc = residual_dispatch<MODE_RK4>(c, a)) return rc;
+    if (int rc = limit1d_to(c, k < 3 ? c->C : c->X, k < 3 ? c->B : c->A)) return rc;
+  }
+  return 0;
+}
+
 // One SSP-RK3 step on c->A; limiter after every stage.
 int step_ssprk3(dgb_ctx* c, bool cfl) {
+  if (lim1d_direct(c)) return step1d_ssprk3(c, cfl);
   launch_dt(c, c->A, cfl);
   if (c->ind_on) launch_indicator(c, c->A);  // the learned indicator's band, once per step
   for (int s = 0; s < 3; ++s)
@@ -691,6 +773,7 @@ int rk4_stage(dgb_ctx* c, int k) {
 
 // One classical RK4 step.
 int step_rk4(dgb_ctx* c, bool cfl) {
+  if (lim1d_direct(c)) return step1d_rk4(c, cfl);
   launch_dt(c, c->A, cfl);
   if (c->ind_on) launch_indicator(c, c->A);  // the learned indicator's band, once per step
   cudaMemcpyAsync(c->B, c->A, c->nstate * sizeof(double), cudaMemcpyDeviceToDevice, c->st);
