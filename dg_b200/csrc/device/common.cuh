@@ -45,7 +45,7 @@ struct DevScalars {
   double time;                 // accumulated time
   unsigned long long umax;     // max wave speed as ordered bits (non-negative doubles)
   unsigned int flags;          // bit 0: NaN wave speed / dt, bit 1: dt < 1e-14
-  unsigned int pad_;
+  unsigned int blocks_done;    // CTAs of a wave-speed reduction that have added their maximum
   double dt_fixed;             // fixed step (> 0) or 0 for the CFL step
 };
 

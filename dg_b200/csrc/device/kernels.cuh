@@ -668,12 +668,35 @@ __global__ void __launch_bounds__(128) lim1d_kernel(const LimArgs la, const doub
 // ------------------------------------------------------------------------------------------
 // CFL step: max over nodes of the wave speed, then dt = CFL_scaled / max (on the device)
 // ------------------------------------------------------------------------------------------
+// The step dt from scal->umax (and the checks of rk.cc:146-149): by finish_dt_kernel, or by the
+// last CTA of a wave-speed reduction.
+// The scalars are read through volatile loads: in the last CTA of a reduction this SM may hold a
+// line of them from before the other CTAs' atomics.
+__device__ __forceinline__ void finish_dt(DevScalars* scal, double cfl_scaled) {
+  volatile DevScalars* v = scal;
+  if (v->flags) return;
+  double dt;
+  if (v->dt_fixed > 0) dt = v->dt_fixed;
+  else {
+    const double umax = __longlong_as_double((long long)v->umax);
+    dt = cfl_scaled / umax;
+    if (!(dt == dt)) atomicOr(&scal->flags, (unsigned)FLAG_NONFINITE);
+    else if (dt < 1e-14) atomicOr(&scal->flags, (unsigned)FLAG_DT_SMALL);
+  }
+  v->umax = 0ull;
+  if (v->flags) return;
+  v->dt = dt;
+  v->time = v->time + dt;
+}
+
 // copy_to (1D RK4, or null): the nf fields of every element read are also written there (the
-// step's accumulator starts as the state)
+// step's accumulator starts as the state).  finish > 0: the last CTA to add its maximum forms the
+// step from it (that CFL scale), so no separate finish launch is needed; 0 leaves umax for a caller
+// that reduces it further (slab mode).
 template <int DIM, int NS, bool GC = false>
 __global__ void __launch_bounds__(256) wavespeed_kernel(const double* __restrict__ U, int n_elem, int ld,
                                                         DevScalars* __restrict__ scal,
-                                                        double* __restrict__ copy_to, int nf) {
+                                                        double* __restrict__ copy_to, int nf, double finish) {
   if (scal->flags) return;
   double m = 0.0;
   bool bad = false;
@@ -705,24 +728,18 @@ __global__ void __launch_bounds__(256) wavespeed_kernel(const double* __restrict
     double mm = 0.0;
     for (int k = 0; k < (int)(blockDim.x >> 5); ++k) mm = fmax(mm, wm[k]);
     atomicMax(&scal->umax, (unsigned long long)__double_as_longlong(mm));
+    if (finish > 0) {
+      __threadfence();  // this CTA's maximum and flags before its count
+      if (atomicAdd(&scal->blocks_done, 1u) == gridDim.x - 1) {
+        __threadfence();  // every other CTA's maximum is in umax
+        scal->blocks_done = 0;
+        finish_dt(scal, finish);
+      }
+    }
   }
 }
 
-static __global__ void finish_dt_kernel(DevScalars* scal, double cfl_scaled) {
-  if (scal->flags) return;
-  double dt;
-  if (scal->dt_fixed > 0) dt = scal->dt_fixed;
-  else {
-    const double umax = __longlong_as_double((long long)scal->umax);
-    dt = cfl_scaled / umax;
-    if (!(dt == dt)) atomicOr(&scal->flags, (unsigned)FLAG_NONFINITE);
-    else if (dt < 1e-14) atomicOr(&scal->flags, (unsigned)FLAG_DT_SMALL);
-  }
-  scal->umax = 0ull;
-  if (scal->flags) return;
-  scal->dt = dt;
-  scal->time += dt;
-}
+static __global__ void finish_dt_kernel(DevScalars* scal, double cfl_scaled) { finish_dt(scal, cfl_scaled); }
 
 // ------------------------------------------------------------------------------------------
 // Layout conversion (API boundary only), RK4 helpers

@@ -597,39 +597,46 @@ int limit_dispatch(dgb_ctx* c, double* U, bool rescore = true) {
 
 // the wave-speed reduction into scal->umax over the elements the context owns (all of them, or
 // in slab mode the rows between the ghost rows)
-void launch_wavespeed(dgb_ctx* c, const double* Uall, double* copy_to = nullptr) {
+// finish > 0: the reduction's last CTA also forms the step dt with that CFL scale
+void launch_wavespeed(dgb_ctx* c, const double* Uall, double* copy_to = nullptr, double finish = 0.0) {
   const int e0 = c->halo_lo * c->nx, n = c->ne - (c->halo_lo + c->halo_hi) * c->nx;
   const double* U = Uall + e0;  // element offset inside every (field, node) plane of stride ld
   const int grid = std::max(1, std::min(4 * 148, (n + 255) / 256));
   {
     if (c->gamcons) {
       switch (c->D * 100 + c->ns) {
-        case 102: wavespeed_kernel<1, 2, true><<<grid, 256, 0, c->st>>>(U, n, c->ld, c->scal, copy_to, c->nf); break;
-        case 103: wavespeed_kernel<1, 3, true><<<grid, 256, 0, c->st>>>(U, n, c->ld, c->scal, copy_to, c->nf); break;
-        case 104: wavespeed_kernel<1, 4, true><<<grid, 256, 0, c->st>>>(U, n, c->ld, c->scal, copy_to, c->nf); break;
-        case 204: wavespeed_kernel<2, 4, true><<<grid, 256, 0, c->st>>>(U, n, c->ld, c->scal, copy_to, c->nf); break;
-        case 209: wavespeed_kernel<2, 9, true><<<grid, 256, 0, c->st>>>(U, n, c->ld, c->scal, copy_to, c->nf); break;
-        case 216: wavespeed_kernel<2, 16, true><<<grid, 256, 0, c->st>>>(U, n, c->ld, c->scal, copy_to, c->nf); break;
+        case 102: wavespeed_kernel<1, 2, true><<<grid, 256, 0, c->st>>>(U, n, c->ld, c->scal, copy_to, c->nf, finish); break;
+        case 103: wavespeed_kernel<1, 3, true><<<grid, 256, 0, c->st>>>(U, n, c->ld, c->scal, copy_to, c->nf, finish); break;
+        case 104: wavespeed_kernel<1, 4, true><<<grid, 256, 0, c->st>>>(U, n, c->ld, c->scal, copy_to, c->nf, finish); break;
+        case 204: wavespeed_kernel<2, 4, true><<<grid, 256, 0, c->st>>>(U, n, c->ld, c->scal, copy_to, c->nf, finish); break;
+        case 209: wavespeed_kernel<2, 9, true><<<grid, 256, 0, c->st>>>(U, n, c->ld, c->scal, copy_to, c->nf, finish); break;
+        case 216: wavespeed_kernel<2, 16, true><<<grid, 256, 0, c->st>>>(U, n, c->ld, c->scal, copy_to, c->nf, finish); break;
         default: break;
       }
     } else
     switch (c->D * 100 + c->ns) {
-      case 102: wavespeed_kernel<1, 2><<<grid, 256, 0, c->st>>>(U, n, c->ld, c->scal, copy_to, c->nf); break;
-      case 103: wavespeed_kernel<1, 3><<<grid, 256, 0, c->st>>>(U, n, c->ld, c->scal, copy_to, c->nf); break;
-      case 104: wavespeed_kernel<1, 4><<<grid, 256, 0, c->st>>>(U, n, c->ld, c->scal, copy_to, c->nf); break;
-      case 204: wavespeed_kernel<2, 4><<<grid, 256, 0, c->st>>>(U, n, c->ld, c->scal, copy_to, c->nf); break;
-      case 209: wavespeed_kernel<2, 9><<<grid, 256, 0, c->st>>>(U, n, c->ld, c->scal, copy_to, c->nf); break;
-      case 216: wavespeed_kernel<2, 16><<<grid, 256, 0, c->st>>>(U, n, c->ld, c->scal, copy_to, c->nf); break;
+      case 102: wavespeed_kernel<1, 2><<<grid, 256, 0, c->st>>>(U, n, c->ld, c->scal, copy_to, c->nf, finish); break;
+      case 103: wavespeed_kernel<1, 3><<<grid, 256, 0, c->st>>>(U, n, c->ld, c->scal, copy_to, c->nf, finish); break;
+      case 104: wavespeed_kernel<1, 4><<<grid, 256, 0, c->st>>>(U, n, c->ld, c->scal, copy_to, c->nf, finish); break;
+      case 204: wavespeed_kernel<2, 4><<<grid, 256, 0, c->st>>>(U, n, c->ld, c->scal, copy_to, c->nf, finish); break;
+      case 209: wavespeed_kernel<2, 9><<<grid, 256, 0, c->st>>>(U, n, c->ld, c->scal, copy_to, c->nf, finish); break;
+      case 216: wavespeed_kernel<2, 16><<<grid, 256, 0, c->st>>>(U, n, c->ld, c->scal, copy_to, c->nf, finish); break;
       default: break;
     }
-    c->counter++;
   }
 }
 
 void launch_dt(dgb_ctx* c, const double* U, bool cfl, double* copy_to = nullptr) {
   ProfScope ps(c, KC_DT);
-  if (cfl) launch_wavespeed(c, U, copy_to);
-  finish_dt_kernel<<<1, 1, 0, c->st>>>(c->scal, c->cs.cfl_scaled);
+  if (cfl && c->cs.cfl_scaled > 0) {
+    launch_wavespeed(c, U, copy_to, c->cs.cfl_scaled);
+  } else {
+    if (cfl) {
+      launch_wavespeed(c, U, copy_to);
+      c->counter++;  // two launches in this scope
+    }
+    finish_dt_kernel<<<1, 1, 0, c->st>>>(c->scal, c->cs.cfl_scaled);
+  }
 }
 
 StageArgs stage_args(dgb_ctx* c) {
