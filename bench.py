@@ -18,6 +18,9 @@ device-side CFL step.  DOF = N_E * N_s * N_F = 5,898,240.
   forms      plain FP64, mixed and mixed + learned indicator at equal L1 error (same protocol)
   mass_fraction  the workload with one passive mass fraction (6 fields): time per step
   gamma_model  the workload grid with Roe + hrl in both gamma models (GAMNCON, GAMCONS): time per step
+  slab_local  the workload split into y-slabs with ghost rows, all in this process on one GPU
+             (dg_b200.slab, LocalTransport): time per step against the whole grid, and the owned
+             rows' distance from it
   tube_1d    the 1D two-fluid shock tube (1000 elements, p=2, Roe, RK4, CFL 0.4, 2000 steps): device
              time, distance from the reference's own run, the reference CPU build's time
   learned_deploy  the learned indicator on a 1024x1024 four-quadrant problem: FP64 / mixed / mixed +
@@ -530,6 +533,47 @@ def mass_fraction(dgb, dev, base_ms, steps=20, warmup=3):
             "rhoY_total_start_end": [float(c0[5]), float(c1[5])]}
 
 
+def slab_local(dgb, dev, steps=10, warmup=3):
+    """The benchmark workload as 2 and 4 y-slabs (2 ghost rows a side), every slab a context in
+    this process on one GPU, ghost rows refreshed before every stage by device copies with the
+    slabs' streams synchronised around each exchange, the CFL wave speed max-reduced over the
+    slabs.  Wall time per step (host synchronisation is part of this transport), against the
+    whole grid's device time per step, and the max distance of the owned rows from the whole grid
+    after the same steps."""
+    import time
+    import torch
+    from dg_b200 import slab as S
+    x0, x1, y0, y1 = DOMAIN
+    out = {"workload": "2D shock-bubble 512x256, p=2, Rusanov, m2l, SSP-RK3, CFL 0.3"}
+    prob = dgb.Problem.structured(2, ORDER, NX, NY, x0, x1, y0, y1, BC, flux="rusanov", limiter="m2l", cfl=CFL)
+    whole = dgb.DGSolver(prob, device=dev)
+    U0 = whole.limit(prob.init_state("shock_bubble", seed=SEED))
+    whole.set_state(U0)
+    whole.advance(warmup, 0.0, scheme=dgb.SSPRK3)
+    whole.advance(steps, 0.0, scheme=dgb.SSPRK3)
+    ms, _ = whole.last_timing()
+    ref = whole.get_state()
+    whole.close()
+    out["whole_ms_per_step"] = ms / steps
+    for ns in (2, 4):
+        dec = S.Decomposition(ORDER, NX, NY, ns, x0, x1, y0, y1, BC, flux="rusanov", limiter="m2l", cfl=CFL)
+        run = S.SlabRun(dec, range(ns), S.LocalTransport(), device=dev)
+        try:
+            run.set_global_state(U0)
+            run.advance(warmup, 0.0, scheme=dgb.SSPRK3)
+            torch.cuda.synchronize(dev)
+            t0 = time.perf_counter()
+            run.advance(steps, 0.0, scheme=dgb.SSPRK3)
+            torch.cuda.synchronize(dev)
+            wall = (time.perf_counter() - t0) * 1e3 / steps
+            got = run.global_state()
+        finally:
+            run.close()
+        out[f"slabs_{ns}"] = {"rows": [r1 - r0 for r0, r1 in dec.ranges], "ms_per_step_wall": wall,
+                              "max_abs_diff_vs_whole": float(np.abs(got - ref).max())}
+    return out
+
+
 def gamma_models(dgb, dev, steps=20, warmup=3):
     """The benchmark grid (512 x 256, p=2, SSP-RK3, CFL 0.3) with Roe and hrl in both gamma models:
     GAMNCON (1/(gamma-1) with its non-conservative source) and GAMCONS (rho/(gamma-1) transported
@@ -689,6 +733,8 @@ def main(argv=None) -> int:
     ap.add_argument("--no-tube", action="store_true", help="skip the 1D shock-tube run")
     ap.add_argument("--tube-only", action="store_true", help="print only the 1D shock-tube run")
     ap.add_argument("--p3-only", action="store_true", help="print only the 2048x1024 p=3 FP64 / mixed comparison")
+    ap.add_argument("--slab-only", action="store_true",
+                    help="print only the one-GPU slab-mode line (512x256 as 2 and 4 slabs)")
     ap.add_argument("--models-only", action="store_true",
                     help="print only the mass-fraction and gamma-model lines (512x256, p=2)")
     args = ap.parse_args(argv)
@@ -719,6 +765,10 @@ def main(argv=None) -> int:
     if args.p3_only:
         if rank == 0:
             print(json.dumps({"mixed_p3": mixed_p3(dgb, dev)}))
+        return 0
+    if args.slab_only:
+        if rank == 0:
+            print(json.dumps({"slab_local": slab_local(dgb, dev)}))
         return 0
     if args.models_only:
         if rank == 0:
@@ -821,6 +871,9 @@ def main(argv=None) -> int:
     gms = None
     if ws == 1 and not args.no_tube and (args.nx, args.ny) == (NX, NY):
         gms = gamma_models(dgb, dev)
+    slabs = None
+    if ws == 1 and not args.no_tube and (args.nx, args.ny) == (NX, NY):
+        slabs = slab_local(dgb, dev)
     tube = None
     if ws == 1 and not args.no_tube and (args.nx, args.ny) == (NX, NY):
         tube = tube_1d(dgb, dev, with_reference=rank == 0 and not args.no_cpu_baseline)
@@ -846,7 +899,7 @@ def main(argv=None) -> int:
                                        "dt": dt_ms / args.steps},
                 "cpu_baseline": cpu, "clocks": clocks, "gpu_launches": launches, "forms": forms,
                 "ensemble": ens, "mixed_p3": p3, "learned_deploy": deploy, "tube_1d": tube, "mass_fraction": mf,
-                "gamma_model": gms}
+                "gamma_model": gms, "slab_local": slabs}
         print(json.dumps(line))
     solver.close()
     if ws > 1:
