@@ -233,14 +233,28 @@ __device__ __forceinline__ double wave_speed1d(double rho, double rhou, double E
   const double p = (gamma - 1) * (E - 0.5 * rho * u * u);
   return fabs(u) + sqrt(gamma * p / rho);
 }
-template <bool GC = false>
-__device__ __forceinline__ double wave_speed2d(double rho, double rhou, double rhov, double E, double alpha) {
-  if (GC) alpha = alpha / rho;  // upa.h:78-80
+// twod_multifluid_upa (upa.h:72-85) as the reference writes it, with its divisions (the launcher
+// shim's LfindUPA)
+__device__ __forceinline__ double wave_speed2d_quotients(double rho, double rhou, double rhov, double E,
+                                                         double alpha) {
   const double u = rhou / rho, v = rhov / rho;
   const double gamma = 1.0 + 1.0 / alpha;
   const double p = (gamma - 1) * (E - 0.5 * rho * (u * u + v * v));
   const double a = sqrt(gamma * p / rho);
   return fmax(fabs(u) + a, fabs(v) + a);
+}
+
+template <bool GC = false>
+__device__ __forceinline__ double wave_speed2d(double rho, double rhou, double rhov, double E, double alpha) {
+  // upa.h:72-85 with correctly rounded reciprocals in place of the four divisions (within an ulp
+  // or two of the quotient form; the reduction reads every node of the state each step)
+  const double ir = __drcp_rn(rho);
+  if (GC) alpha = alpha * ir;  // upa.h:78-80
+  const double u = rhou * ir, v = rhov * ir;
+  const double gm1 = __drcp_rn(alpha);
+  const double p = gm1 * (E - 0.5 * rho * (u * u + v * v));
+  const double a = sqrt((1.0 + gm1) * p * ir);
+  return fmax(fabs(u), fabs(v)) + a;
 }
 
 }  // namespace phys
