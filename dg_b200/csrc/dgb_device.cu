@@ -1340,7 +1340,8 @@ extern "C" int dgb_slab_ghost_rows(dgb_ctx* c, int lo, int hi) {
   if (c->ind_on) return set_error(DGB_ERR_UNSUPPORTED, "slab mode does not take the learned indicator");
   if (c->limiter != DGB_LIM_NONE && c->limiter != DGB_LIM_HRL && c->limiter != DGB_LIM_M2L &&
       c->limiter != DGB_LIM_PRL)
-    return set_error(DGB_ERR_UNSUPPORTED, "slab mode: the sensor-gated limiters reach three rows; use none, hrl, m2l or prl");
+    return set_error(DGB_ERR_UNSUPPORTED, "slab mode: the sensors follow the reference's sequential element order, "
+                                          "which no ghost depth reproduces; use none, hrl, m2l or prl");
   c->halo_lo = lo;
   c->halo_hi = hi;
   return DGB_OK;

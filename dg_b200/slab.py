@@ -8,7 +8,9 @@ the reference's ghost exchange before every residual and limiter pass (rk.cc:108
 203-209; communicator_cpu.cc:14-59), done per slab boundary instead of per ghost element -- and
 the CFL wave speed is max-reduced over the slabs before the step's dt is formed (RK::DtFromCFL over
 the whole mesh).  A stage reaches two rows deep (the residual, then the limiter's y pass), so two
-ghost rows make every owned row's result the one of the whole grid advanced at once.
+ghost rows make every owned row's result the one of the whole grid advanced at once.  (The
+sensor-gated limiters are not available here: their flags follow the reference's sequential element
+order, a recurrence that can cross any number of rows.)
 
 Transports move the rows:
   LocalTransport  every slab in this process on one device (device-to-device copies)

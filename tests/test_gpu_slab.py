@@ -93,7 +93,7 @@ def test_slab_mode_rejections_and_phase_order():
     s = dgb.DGSolver(prob)
     try:
         with pytest.raises(dgb.DGBError):
-            s.set_ghost_rows(2, 2)  # the sensor-gated limiters reach three rows
+            s.set_ghost_rows(2, 2)  # sensor flags follow the reference's element order across rows
     finally:
         s.close()
     prob = dgb.Problem.structured(2, 2, 32, 16, flux="rusanov", limiter="m2l", cfl=0.3)
