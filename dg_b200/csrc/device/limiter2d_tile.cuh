@@ -54,9 +54,10 @@ __device__ __forceinline__ void lim2d_xpass_body(const LimArgs la, int nx, const
         q[1][ix] = v[1][ix];
         q[2][ix] = v[2][ix];
         q[3][ix] = v[4][ix];
-        // pressure from the unlimited state (pressure kernel, physics.cu:891-958)
+        // pressure from the unlimited state (pressure kernel, physics.cu:891-958), with correctly
+        // rounded reciprocals in place of its divisions
         const double ru = v[1][ix], rv = v[2][ix];
-        q[4][ix] = (1.0 / v[4][ix]) * (v[3][ix] - 0.5 * (ru * ru + rv * rv) / v[0][ix]);
+        q[4][ix] = __drcp_rn(v[4][ix]) * (v[3][ix] - 0.5 * (ru * ru + rv * rv) * __drcp_rn(v[0][ix]));
       }
     }
 #pragma unroll
@@ -105,7 +106,7 @@ __device__ __forceinline__ void lim2d_xpass_body(const LimArgs la, int nx, const
     to_lag<P>(lim[3], a_);
     to_lag<P>(lim[4], p_);
 #pragma unroll
-    for (int ix = 0; ix < N1; ++ix) K[ix] = 0.5 * (u_[ix] * u_[ix] + v_[ix] * v_[ix]) / r_[ix];
+    for (int ix = 0; ix < N1; ++ix) K[ix] = 0.5 * (u_[ix] * u_[ix] + v_[ix] * v_[ix]) * __drcp_rn(r_[ix]);
     to_mono<P>(K, Km);
     reconstruct_energy<P>(lim[4], lim[3], Km, Em, El);
     to_lag<P>(El, E_);
@@ -214,7 +215,7 @@ __device__ __forceinline__ void lim2d_ypass_body(const LimArgs la, int nx, int n
     to_lag<P>(lim[2], v_);
     to_lag<P>(lim[3], a_);
 #pragma unroll
-    for (int iy = 0; iy < N1; ++iy) K[iy] = 0.5 * (u_[iy] * u_[iy] + v_[iy] * v_[iy]) / r_[iy];
+    for (int iy = 0; iy < N1; ++iy) K[iy] = 0.5 * (u_[iy] * u_[iy] + v_[iy] * v_[iy]) * __drcp_rn(r_[iy]);
     to_mono<P>(K, Km);
     reconstruct_energy<P>(lim[4], lim[3], Km, Em, El);
     to_lag<P>(El, E_);
@@ -325,7 +326,7 @@ __global__ void __launch_bounds__(32 * (P + 1)) lim2d_fused_tile_kernel(const Li
           q[2][ix] = v[2][ix];
           q[3][ix] = v[4][ix];
           const double ru = v[1][ix], rv = v[2][ix];
-          q[4][ix] = (1.0 / v[4][ix]) * (v[3][ix] - 0.5 * (ru * ru + rv * rv) / v[0][ix]);
+          q[4][ix] = __drcp_rn(v[4][ix]) * (v[3][ix] - 0.5 * (ru * ru + rv * rv) * __drcp_rn(v[0][ix]));
         }
       }
 #pragma unroll
@@ -376,7 +377,7 @@ __global__ void __launch_bounds__(32 * (P + 1)) lim2d_fused_tile_kernel(const Li
         to_lag<P>(lim[3], a_);
         to_lag<P>(lim[4], p_);
 #pragma unroll
-        for (int ix = 0; ix < N1; ++ix) K[ix] = 0.5 * (u_[ix] * u_[ix] + v_[ix] * v_[ix]) / r_[ix];
+        for (int ix = 0; ix < N1; ++ix) K[ix] = 0.5 * (u_[ix] * u_[ix] + v_[ix] * v_[ix]) * __drcp_rn(r_[ix]);
         to_mono<P>(K, Km);
         reconstruct_energy<P>(lim[4], lim[3], Km, Em, El);
         to_lag<P>(El, E_);
@@ -452,7 +453,7 @@ __global__ void __launch_bounds__(32 * (P + 1)) lim2d_fused_tile_kernel(const Li
         to_lag<P>(lim[2], v_);
         to_lag<P>(lim[3], a_);
 #pragma unroll
-        for (int iy = 0; iy < N1; ++iy) K[iy] = 0.5 * (u_[iy] * u_[iy] + v_[iy] * v_[iy]) / r_[iy];
+        for (int iy = 0; iy < N1; ++iy) K[iy] = 0.5 * (u_[iy] * u_[iy] + v_[iy] * v_[iy]) * __drcp_rn(r_[iy]);
         to_mono<P>(K, Km);
         reconstruct_energy<P>(lim[4], lim[3], Km, Emy, El);
         to_lag<P>(El, E_);
