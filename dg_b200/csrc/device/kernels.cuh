@@ -282,13 +282,14 @@ __device__ __forceinline__ void res1d_body(const Consts& c, const StageArgs& a, 
       for (int f = 0; f < NF; ++f) ug[f] += c.Bq[g][t] * u[f][t];
       da += c.Dq[g][t] * u[3][t];
     }
-    const double rho = ug[0], vx = ug[1] / rho, Et = ug[2];
-    const double gamma = GC ? 1 + rho / ug[3] : 1 + 1.0 / ug[3];  // physics.cu:100-104
-    const double p = (gamma - 1) * (Et - 0.5 * rho * vx * vx);
+    // physics.cu:96-104 with correctly rounded reciprocals in place of its divisions
+    const double rho = ug[0], vx = ug[1] * __drcp_rn(rho), Et = ug[2];
+    const double gm1 = GC ? rho * __drcp_rn(ug[3]) : __drcp_rn(ug[3]);  // gamma - 1
+    const double p = gm1 * (Et - 0.5 * rho * vx * vx);
     const double cx = c.wq[g] * (c.ixx * c.J);
     const double fx[3] = {rho * vx, rho * vx * vx + p, (Et + p) * vx};
     const double s = (c.wq[g] * c.J) * (-vx * da * c.ixx);  // physics.cu:126-127
-    const double fa = rho * vx * (1 / (gamma - 1));           // GAMCONS alpha flux, physics.cu:122-124
+    const double fa = rho * vx * __drcp_rn(gm1);              // GAMCONS alpha flux, physics.cu:122-124
 #pragma unroll
     for (int t = 0; t < N1; ++t) {
 #pragma unroll
@@ -318,8 +319,8 @@ __device__ __forceinline__ void res1d_body(const Consts& c, const StageArgs& a, 
 #pragma unroll
     for (int f = 0; f < NF; ++f) { L[f] = swapLR ? un[f] : uo[f]; R[f] = swapLR ? uo[f] : un[f]; }
     double F[NF], nc;
-    phys::riemann1d<FLUX, NY, GC>(L[0], R[0], L[1] / L[0], R[1] / R[0], L[2], R[2], L[3], R[3], nx, F, nc, L + 4,
-                                  R + 4);
+    phys::riemann1d<FLUX, NY, GC>(L[0], R[0], L[1] * __drcp_rn(L[0]), R[1] * __drcp_rn(R[0]), L[2], R[2], L[3], R[3],
+                                  nx, F, nc, L + 4, R + 4);
 #pragma unroll
     for (int f = 0; f < NF; ++f) r[f][to] += sgn * F[f] + (f == 3 ? nc : 0.0);
   }

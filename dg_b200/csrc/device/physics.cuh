@@ -30,16 +30,20 @@ template <int FLUX, int NY = 0, bool GC = false>
 __device__ __forceinline__ void riemann1d(double rhoL, double rhoR, double vxL, double vxR, double EtL, double EtR,
                                           double alphaL, double alphaR, double nx, double* F, double& nc,
                                           const double* YL = nullptr, const double* YR = nullptr) {
+  // the reference's divisions as correctly rounded reciprocals (shorter dependency chains; within
+  // an ulp or two of the quotients)
+  const double irL = __drcp_rn(rhoL), irR = __drcp_rn(rhoR);
   if (GC) {
-    alphaL = alphaL / rhoL;
-    alphaR = alphaR / rhoR;
+    alphaL = alphaL * irL;
+    alphaR = alphaR * irR;
   }
-  const double gammaL = 1.0 + 1.0 / alphaL;
-  const double gammaR = 1.0 + 1.0 / alphaR;
-  const double pL = (gammaL - 1) * (EtL - 0.5 * rhoL * vxL * vxL);
-  const double pR = (gammaR - 1) * (EtR - 0.5 * rhoR * vxR * vxR);
-  const double aL = sqrt((gammaL * pL) / rhoL);
-  const double aR = sqrt((gammaR * pR) / rhoR);
+  const double gm1L = __drcp_rn(alphaL), gm1R = __drcp_rn(alphaR);  // gamma - 1 = 1/alpha
+  const double gammaL = 1.0 + gm1L;
+  const double gammaR = 1.0 + gm1R;
+  const double pL = gm1L * (EtL - 0.5 * rhoL * vxL * vxL);
+  const double pR = gm1R * (EtR - 0.5 * rhoR * vxR * vxR);
+  const double aL = sqrt(gammaL * pL * irL);
+  const double aR = sqrt(gammaR * pR * irR);
   if (FLUX == FLUX_RUS) {
     const double maxvap = fmax(fabs(vxL) + aL, fabs(vxR) + aR);
     F[0] = 0.5 * ((rhoL * vxL + rhoR * vxR) * nx - maxvap * (rhoR - rhoL));
@@ -63,8 +67,9 @@ __device__ __forceinline__ void riemann1d(double rhoL, double rhoR, double vxL, 
     const double SR = fmax(vxL * nx + aL, vxR * nx + aR);
     const double vnc = -0.5 * (vxL * nx + vxR * nx) * (alphaL - alphaR);
     const double vncabs = -0.5 * fabs(vxL * nx + vxR * nx) * (alphaL - alphaR);
-    auto fhll = [](double UL, double SLv, double FL, double UR, double SRv, double FR) {
-      return (SRv * FL - SLv * FR + SLv * SRv * (UR - UL)) / fabs(SRv - SLv);
+    const double iw = __drcp_rn(fabs(SR - SL));
+    auto fhll = [iw](double UL, double SLv, double FL, double UR, double SRv, double FR) {
+      return (SRv * FL - SLv * FR + SLv * SRv * (UR - UL)) * iw;
     };
     F[0] = F[1] = F[2] = F[3] = 0.0;
 #pragma unroll
@@ -82,7 +87,7 @@ __device__ __forceinline__ void riemann1d(double rhoL, double rhoR, double vxL, 
       F[2] = fhll(EtL, SL, (EtL + pL) * vxL * nx, EtR, SR, (EtR + pR) * vxR * nx);
       // GAMCONS: the jump term takes the divided alpha, as oned_multifluid_fluxes.h:196 does
       F[3] = GC ? fhll(alphaL, SL, rhoL * vxL * alphaL * nx, alphaR, SR, rhoR * vxR * alphaR * nx)
-                : fhll(alphaL, SL, 0, alphaR, SR, 0) - 0.5 * fabs(SR + SL) / fabs(SR - SL) * vncabs;
+                : fhll(alphaL, SL, 0, alphaR, SR, 0) - 0.5 * fabs(SR + SL) * iw * vncabs;
 #pragma unroll
       for (int k = 0; k < NY; ++k) F[4 + k] = fhll(YL[k], SL, YL[k] * vxL * nx, YR[k], SR, YR[k] * vxR * nx);
     } else if (SR < 0) {
@@ -95,23 +100,26 @@ __device__ __forceinline__ void riemann1d(double rhoL, double rhoR, double vxL, 
     }
     nc = GC ? 0.0 : -0.5 * vnc;
   } else {
-    const double RT = sqrt(rhoR / rhoL);
+    const double RT = sqrt(rhoR * irL);
     const double rho = RT * rhoL;
-    const double v = (vxL + RT * vxR) / (1 + RT);
-    const double HL = (EtL + pL) / rhoL;
-    const double HR = (EtR + pR) / rhoR;
-    const double H = (HL + RT * HR) / (1 + RT);
-    const double alpha = (alphaL + RT * alphaR) / (1 + RT);
-    const double gamma = 1 + 1.0 / alpha;
-    const double a = sqrt((gamma - 1) * (H - 0.5 * v * v));
+    const double i1 = __drcp_rn(1 + RT);
+    const double v = (vxL + RT * vxR) * i1;
+    const double HL = (EtL + pL) * irL;
+    const double HR = (EtR + pR) * irR;
+    const double H = (HL + RT * HR) * i1;
+    const double alpha = (alphaL + RT * alphaR) * i1;
+    const double gm1 = __drcp_rn(alpha);  // gamma - 1
+    const double a = sqrt(gm1 * (H - 0.5 * v * v));
     const double iL = pL * alphaL;
     const double iR = pR * alphaR;
-    const double i = (sqrt(rhoL) * iL + sqrt(rhoR) * iR) / (sqrt(rhoL) + sqrt(rhoR));
-    const double Dp = (gamma - 1) * (gamma - 1) * (alpha * (iR - iL) - i * (alphaR - alphaL));
-    const double p = (gamma - 1) * i;
-    const double dV0 = (Dp - rho * a * (vxR - vxL)) / (2 * a * a);
-    const double dV1 = (rhoR - rhoL) - Dp / (a * a);
-    const double dV2 = (Dp + rho * a * (vxR - vxL)) / (2 * a * a);
+    const double sL = sqrt(rhoL), sR = sqrt(rhoR);
+    const double i = (sL * iL + sR * iR) * __drcp_rn(sL + sR);
+    const double Dp = gm1 * gm1 * (alpha * (iR - iL) - i * (alphaR - alphaL));
+    const double p = gm1 * i;
+    const double ia2 = __drcp_rn(a * a);
+    const double dV0 = (Dp - rho * a * (vxR - vxL)) * (0.5 * ia2);
+    const double dV1 = (rhoR - rhoL) - Dp * ia2;
+    const double dV2 = (Dp + rho * a * (vxR - vxL)) * (0.5 * ia2);
     const double dV3 = alphaR - alphaL;
     const double ws0 = fabs(v - a), ws1 = fabs(v), ws2 = fabs(v + a), ws3 = fabs(v);
     // right eigenvectors R0=(1, v-a, H-va, 0), R1=(1, v, v^2/2, 0), R2=(1, v+a, H+va, 0), R3=(0,0,p,1)
@@ -126,7 +134,7 @@ __device__ __forceinline__ void riemann1d(double rhoL, double rhoR, double vxL, 
     // mass fractions: Roe-averaged Y and its wave strength (oned_multifluid_fluxes.h:358-370)
 #pragma unroll
     for (int k = 0; k < NY; ++k) {
-      const double Y = (YL[k] / rhoL + RT * YR[k] / rhoR) / (1 + RT);
+      const double Y = (YL[k] * irL + RT * YR[k] * irR) * i1;
       const double dVY = YR[k] - YL[k] - (dV0 + dV1 + dV2) * Y;
       F[4 + k] = 0.5 * (YL[k] * vxL + YR[k] * vxR) * nx - 0.5 * (ws0 * dV0 * Y + ws1 * dV1 * Y + ws1 * dVY * 1 + ws2 * dV2 * Y);
     }
@@ -227,7 +235,16 @@ __device__ __forceinline__ void riemann2d(double rhoL, double rhoR, double vxL, 
 // max(|u|+a, |v|+a) at a node (upa.h:61-85)
 template <bool GC = false>
 __device__ __forceinline__ double wave_speed1d(double rho, double rhou, double E, double alpha) {
-  if (GC) alpha = alpha / rho;  // upa.h:65-67
+  // upa.h:61-70 with correctly rounded reciprocals in place of its divisions
+  const double ir = __drcp_rn(rho);
+  if (GC) alpha = alpha * ir;  // upa.h:65-67
+  const double u = rhou * ir;
+  const double gm1 = __drcp_rn(alpha);
+  const double p = gm1 * (E - 0.5 * rho * u * u);
+  return fabs(u) + sqrt((1.0 + gm1) * p * ir);
+}
+// oned_multifluid_upa (upa.h:61-70) as the reference writes it (the launcher shim's LfindUPA)
+__device__ __forceinline__ double wave_speed1d_quotients(double rho, double rhou, double E, double alpha) {
   const double u = rhou / rho;
   const double gamma = 1.0 + 1.0 / alpha;
   const double p = (gamma - 1) * (E - 0.5 * rho * u * u);

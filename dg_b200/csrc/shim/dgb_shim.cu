@@ -198,7 +198,7 @@ __global__ void find_upa(int N_s, int N_E, const scalar* U, scalar* UPA) {
   const long e = k / N_s;
   const int i = (int)(k % N_s);
   auto u = [&](int fc) { return U[(e * N_F + fc) * N_s + i]; };
-  UPA[k] = D == 1 ? dgb::phys::wave_speed1d(u(0), u(1), u(2), u(3))
+  UPA[k] = D == 1 ? dgb::phys::wave_speed1d_quotients(u(0), u(1), u(2), u(3))
                   : dgb::phys::wave_speed2d_quotients(u(0), u(1), u(2), u(3), u(4));
 }
 
