@@ -129,7 +129,7 @@ __global__ void __launch_bounds__(128) lim_gated_kernel(const LimArgs la, const 
 #pragma unroll
       for (int k = 0; k < N1; ++k) {
         const double kin = v[1][k] * v[1][k] + (D == 2 ? v[2][k] * v[2][k] : 0.0);
-        p[k] = (v[IE][k] - 0.5 * kin / v[0][k]) / v[IA][k];
+        p[k] = (v[IE][k] - 0.5 * kin * __drcp_rn(v[0][k])) * __drcp_rn(v[IA][k]);  // reciprocals for divisions
       }
     };
     press(c, pc);
@@ -159,7 +159,7 @@ __global__ void __launch_bounds__(128) lim_gated_kernel(const LimArgs la, const 
 #pragma unroll
     for (int k = 0; k < N1; ++k) {
       const double kin = res[1][k] * res[1][k] + (D == 2 ? res[2][k] * res[2][k] : 0.0);
-      K[k] = 0.5 * kin / res[0][k];
+      K[k] = 0.5 * kin * __drcp_rn(res[0][k]);
     }
     to_mono<P>(K, Km);
     to_mono<P>(c[IE], Em);
