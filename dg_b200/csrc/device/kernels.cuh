@@ -329,26 +329,26 @@ __device__ __forceinline__ void res1d_body(const Consts& c, const StageArgs& a, 
     for (int f = 0; f < NF; ++f)
 #pragma unroll
       for (int t = 0; t < N1; ++t) a.out[(size_t)(f * N1 + t) * ld + e] = r[f][t];
-    return;
-  }
+  } else {
 #pragma unroll
-  for (int f = 0; f < NF; ++f)
+    for (int f = 0; f < NF; ++f)
 #pragma unroll
-    for (int t = 0; t < N1; ++t) {
-      double s = 0.0;
+      for (int t = 0; t < N1; ++t) {
+        double s = 0.0;
 #pragma unroll
-      for (int tt = 0; tt < N1; ++tt) s += c.Minv[t][tt] * r[f][tt];
-      const double du = dt * s;
-      const size_t gi = (size_t)(f * N1 + t) * ld + e;
-      if (MODE == MODE_SSP) {
-        const double base = a.a != 0.0 ? a.a * __ldg(a.Ubase + gi) : 0.0;
-        a.out[gi] = base + a.b * (u[f][t] + du);
-      } else {
-        a.out[gi] = du;
-        if (a.Uacc) a.Uacc[gi] += a.b * du;
-        if (a.Unext) a.Unext[gi] = __ldg(a.Us + gi) + a.beta_next * du;  // rk.cc:164-170
+        for (int tt = 0; tt < N1; ++tt) s += c.Minv[t][tt] * r[f][tt];
+        const double du = dt * s;
+        const size_t gi = (size_t)(f * N1 + t) * ld + e;
+        if (MODE == MODE_SSP) {
+          const double base = a.a != 0.0 ? a.a * __ldg(a.Ubase + gi) : 0.0;
+          a.out[gi] = base + a.b * (u[f][t] + du);
+        } else {
+          a.out[gi] = du;
+          if (a.Uacc) a.Uacc[gi] += a.b * du;
+          if (a.Unext) a.Unext[gi] = __ldg(a.Us + gi) + a.beta_next * du;  // rk.cc:164-170
+        }
       }
-    }
+  }
 }
 
 template <int P, int FLUX, int MODE, int NY = 0, bool GC = false>
