@@ -267,7 +267,12 @@ class DistTransport:
         self._init(run)
         (s,) = run.slabs
         with s.stream():
-            dist.all_reduce(s.umax(), op=dist.ReduceOp.MAX, group=self.group)
+            # reduced in a copy the torch allocator owns (the word itself is the library's memory,
+            # which the collective's stream bookkeeping should not be given), then written back
+            word = s.umax()
+            t = word.clone()
+            dist.all_reduce(t, op=dist.ReduceOp.MAX, group=self.group)
+            word.copy_(t)
 
     def reduce_status(self, run: "SlabRun", code: int) -> int:
         import torch
