@@ -31,7 +31,10 @@ struct dgb_ctx {
   double* slab_cur = nullptr;   // the buffer the next stage reads (packed / unpacked by dgb_halo_*)
   int slab_scheme = 0, slab_next = -1;
   bool slab_cfl = false;
-  bool tiled = false;     // structured row-major grid with tile-multiple extents: tiled residual kernel
+  bool tiled = false;     // structured row-major grid with at least one full tile: tiled residual kernel
+  bool tiled_full = false;  // ... and extents that are tile multiples (no leftover strips)
+  int* left = nullptr;    // the elements outside the full tiles (generic residual kernel), nleft of them
+  int nleft = 0;
   int form = DGB_FORM_FP64;  // arithmetic of the residual: plain FP64 or mixed FP32/FP64
   bool rowmajor = false;  // structured row-major grid: tiled limiter passes
   bool fused_lim = false; // row-major grid, hrl / m2l: both limiter passes in one kernel (opt-in)

@@ -34,6 +34,8 @@ struct StageArgs {
   double* __restrict__ Unext;        // RK4 (1D): the next stage input Us + beta_next * DU, or null
   const double* __restrict__ Us;     //   its Us
   double beta_next;
+  const int* __restrict__ elist;     // 2D generic residual: the elements to do (null: all of them)
+  int nlist;
   const int* __restrict__ nbr;       // [face][ld] neighbours, boundary codes < 0
   const DevScalars* __restrict__ scal;
   double a, b;
@@ -96,8 +98,15 @@ __global__ void __launch_bounds__(NT) residual2d_kernel(const Consts cin, const 
   copy_consts(c, cin);
   if (a.scal && a.scal->flags) return;  // a failed CFL step stops the integration here
   __syncthreads();
-  const int ld = c.ld, NE = c.n_elem;
+  const int ld = c.ld;
   const int e0 = blockIdx.x * TE;
+  // the element of slot el: the grid's e0 + el, or the listed one (the strips the tiled kernel
+  // leaves on a grid whose extents are not tile multiples); -1 past the end
+  const int NL = a.elist ? a.nlist : c.n_elem;
+  auto elem = [&](int el) -> int {
+    const int k = e0 + el;
+    return k < NL ? (a.elist ? __ldg(a.elist + k) : k) : -1;
+  };
   for (int i = tid; i < NG * NS; i += NT) {
     const int g = i / NS, t = i % NS, gx = g / NG1, gy = g % NG1, ix = t % N1, iy = t / N1;
     Phi[i] = c.Bq[gx][ix] * c.Bq[gy][iy];
@@ -106,17 +115,17 @@ __global__ void __launch_bounds__(NT) residual2d_kernel(const Consts cin, const 
   }
   // ---- stage the tile's state and the neighbours' face traces ----
   for (int i = tid; i < NF * NS * TE; i += NT) {
-    const int el = i % TE, ft = i / TE, e = e0 + el;
-    Us[i] = e < NE ? __ldg(a.U + (size_t)ft * ld + e) : 0.0;
+    const int el = i % TE, ft = i / TE, e = elem(el);
+    Us[i] = e >= 0 ? __ldg(a.U + (size_t)ft * ld + e) : 0.0;
   }
   for (int i = tid; i < 4 * NF * N1 * TE; i += NT) {
     const int el = i % TE;
     int r = i / TE;
     const int j = r % N1;
     r /= N1;
-    const int f = r % NF, k = r / NF, e = e0 + el;
+    const int f = r % NF, k = r / NF, e = elem(el);
     double v = 0.0;
-    if (e < NE) {
+    if (e >= 0) {
       const int nb = __ldg(a.nbr + (size_t)k * ld + e);
       if (nb >= 0) v = __ldg(a.U + (size_t)(f * NS + across_node<P>(k, j)) * ld + nb);
       else {
@@ -132,7 +141,7 @@ __global__ void __launch_bounds__(NT) residual2d_kernel(const Consts cin, const 
   // ---- volume: states, fluxes and the alpha source at the quadrature points ----
   for (int i = tid; i < NG * TE; i += NT) {
     const int el = i % TE, g = i / TE;
-    if (e0 + el >= NE) continue;
+    if (elem(el) < 0) continue;
     double ug[NF] = {0, 0, 0, 0, 0}, dax = 0, day = 0;
 #pragma unroll
     for (int t = 0; t < NS; ++t) {
@@ -178,8 +187,8 @@ __global__ void __launch_bounds__(NT) residual2d_kernel(const Consts cin, const 
   __syncthreads();
   // ---- faces: Riemann flux at the face quadrature points ----
   for (int i = tid; i < 4 * N1 * TE; i += NT) {
-    const int el = i % TE, r = i / TE, g = r % N1, k = r / N1, e = e0 + el;
-    if (e >= NE) continue;
+    const int el = i % TE, r = i / TE, g = r % N1, k = r / N1, e = elem(el);
+    if (e < 0) continue;
     double uo[NF], un[NF];
 #pragma unroll
     for (int f = 0; f < NF; ++f) {
@@ -217,7 +226,7 @@ __global__ void __launch_bounds__(NT) residual2d_kernel(const Consts cin, const 
   __syncthreads();
   // ---- face lift and total ----
   for (int i = tid; i < NF * NS * TE; i += NT) {
-    const int el = i % TE, ft = i / TE, f = ft / NS, t = ft % NS, e = e0 + el;
+    const int el = i % TE, ft = i / TE, f = ft / NS, t = ft % NS, e = elem(el);
     const int ix = t % N1, iy = t / N1;
     double r = Rs[i];
 #pragma unroll
@@ -228,7 +237,7 @@ __global__ void __launch_bounds__(NT) residual2d_kernel(const Consts cin, const 
       if (iy == P) r += c.Bf[g][ix] * G[((f * 4 + 3) * N1 + g) * TE + el];
     }
     if (MODE == MODE_RESIDUAL) {
-      if (e < NE) a.out[(size_t)ft * ld + e] = r;
+      if (e >= 0) a.out[(size_t)ft * ld + e] = r;
     } else {
       Rs[i] = r;
     }
@@ -238,8 +247,8 @@ __global__ void __launch_bounds__(NT) residual2d_kernel(const Consts cin, const 
   // ---- epilogue: DU = dt Minv R and the stage update ----
   const double dt = a.dt_override > 0 ? a.dt_override : a.scal->dt;
   for (int i = tid; i < NF * NS * TE; i += NT) {
-    const int el = i % TE, ft = i / TE, f = ft / NS, t = ft % NS, e = e0 + el;
-    if (e >= NE) continue;
+    const int el = i % TE, ft = i / TE, f = ft / NS, t = ft % NS, e = elem(el);
+    if (e < 0) continue;
     double s = 0.0;
 #pragma unroll
     for (int tt = 0; tt < NS; ++tt) s += c.Minv[t][tt] * Rs[(f * NS + tt) * TE + el];

@@ -375,7 +375,7 @@ extern "C" int dgb_batch_create(dgb_ctx* const* cases, int n, dgb_batch** out) {
       return fail(set_error(DGB_ERR_UNSUPPORTED, "batch: plain FP64 form with the two-pass limiter only"));
     if (c->limiter != DGB_LIM_NONE && c->limiter != DGB_LIM_HRL && c->limiter != DGB_LIM_M2L)
       return fail(set_error(DGB_ERR_UNSUPPORTED, "batch: limiter none, hrl or m2l"));
-    if (c->D == 2 && (!c->tiled || c->p > 2))
+    if (c->D == 2 && (!c->tiled_full || c->p > 2))
       return fail(set_error(DGB_ERR_UNSUPPORTED,
                             "batch: 2D cases must be structured row-major grids, p <= 2, nx % 32 == 0, ny % 4 == 0"));
     if (!(c->cs.cfl_scaled > 0)) return fail(set_error(DGB_ERR_ARG, "batch: every case needs a positive CFL"));

@@ -161,15 +161,19 @@ struct ProfScope {
   }
 };
 
+// generic 2D residual over every element, or over the listed ones (elist, n)
 template <int P, int FLUX, int MODE>
-void launch_res2d(dgb_ctx* c, const StageArgs& a) {
+void launch_res2d(dgb_ctx* c, const StageArgs& a, const int* elist = nullptr, int n = 0) {
   constexpr size_t smem = residual2d_smem_doubles<P, RES2D_TE>() * sizeof(double);
   auto k = residual2d_kernel<P, FLUX, MODE, RES2D_TE, RES2D_NT>;
   static bool attr = false;
   if (!attr) { cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem); attr = true; }
-  const int grid = (c->ne + RES2D_TE - 1) / RES2D_TE;
+  StageArgs s = a;
+  s.elist = elist;
+  s.nlist = n;
+  const int grid = ((elist ? n : c->ne) + RES2D_TE - 1) / RES2D_TE;
   ProfScope ps(c, KC_RESIDUAL);
-  k<<<grid, RES2D_NT, smem, c->st>>>(c->cs, a);
+  k<<<grid, RES2D_NT, smem, c->st>>>(c->cs, s);
 }
 
 template <int P, int FLUX, int MODE, int NY = 0, bool GC = false>
@@ -272,7 +276,7 @@ namespace {
 // NY passive mass fractions (1D or tiled 2D, FP64 form; checked at create)
 template <int MODE, int NY>
 int residual_ny(dgb_ctx* c, const StageArgs& a) {
-  if (c->tiled) {
+  if (c->tiled_full) {
     switch (c->p * 10 + c->flux) {
       case 10: launch_tile2d<1, 0, MODE, NY>(c, a); return 0;
       case 12: launch_tile2d<1, 2, MODE, NY>(c, a); return 0;
@@ -294,9 +298,19 @@ int residual_ny(dgb_ctx* c, const StageArgs& a) {
   return set_error(DGB_ERR_UNSUPPORTED, "no residual kernel for this (p, flux) with mass fractions");
 }
 
+// the full tiles with the tiled kernel, then the elements outside them (right and top strips of a
+// grid whose extents are not tile multiples) with the generic kernel; disjoint outputs, both read
+// the stage input's neighbours from global memory
+template <int P, int FLUX, int MODE>
+int tiles_then_strips(dgb_ctx* c, const StageArgs& a) {
+  launch_tile2d<P, FLUX, MODE>(c, a);
+  if (c->nleft) launch_res2d<P, FLUX, MODE>(c, a, c->left, c->nleft);
+  return 0;
+}
+
 template <int MODE>
 int residual_dispatch(dgb_ctx* c, const StageArgs& a) {
-  if (c->tiled && c->form == DGB_FORM_MIXED) {
+  if (c->tiled_full && c->form == DGB_FORM_MIXED) {
     const int key = c->p * 10 + c->flux;
     switch (key) {
       case 10: launch_tile2d_mixed<1, 0, MODE>(c, a); return 0;
@@ -338,12 +352,12 @@ int residual_dispatch(dgb_ctx* c, const StageArgs& a) {
   if (c->tiled) {
     const int key = c->p * 10 + c->flux;
     switch (key) {
-      case 10: launch_tile2d<1, 0, MODE>(c, a); return 0;
-      case 12: launch_tile2d<1, 2, MODE>(c, a); return 0;
-      case 20: launch_tile2d<2, 0, MODE>(c, a); return 0;
-      case 22: launch_tile2d<2, 2, MODE>(c, a); return 0;
-      case 30: launch_tile2d<3, 0, MODE>(c, a); return 0;
-      case 32: launch_tile2d<3, 2, MODE>(c, a); return 0;
+      case 10: return tiles_then_strips<1, 0, MODE>(c, a);
+      case 12: return tiles_then_strips<1, 2, MODE>(c, a);
+      case 20: return tiles_then_strips<2, 0, MODE>(c, a);
+      case 22: return tiles_then_strips<2, 2, MODE>(c, a);
+      case 30: return tiles_then_strips<3, 0, MODE>(c, a);
+      case 32: return tiles_then_strips<3, 2, MODE>(c, a);
       default: break;
     }
   }
@@ -869,7 +883,10 @@ extern "C" int dgb_create(const dgb_problem* prob, int device, dgb_ctx** out) {
   c->hx = P.hx;
   c->hy = P.hy;
   c->rowmajor = P.D == 2 && is_row_major_grid(P) && std::getenv("DGB_NO_TILE") == nullptr;
-  c->tiled = c->rowmajor && P.p <= 3 && P.nx % TILE_W == 0 && P.ny % tile_h_for(P.p) == 0;
+  // tiled residual over the full tiles (the tensor map's row stride nx * 8 bytes must be a multiple
+  // of 16: nx even); the strips left over on other extents go to the generic kernel
+  c->tiled = c->rowmajor && P.p <= 3 && P.nx % 2 == 0 && P.nx >= TILE_W && P.ny >= tile_h_for(P.p);
+  c->tiled_full = c->tiled && P.nx % TILE_W == 0 && P.ny % tile_h_for(P.p) == 0;
   // opt-in: measured slower than the two tiled passes on 512 x 256, p = 2 (64 vs 55 us per stage)
   c->fused_lim = c->rowmajor && (P.limiter == DGB_LIM_HRL || P.limiter == DGB_LIM_M2L) &&
                  std::getenv("DGB_FUSED_LIMITER") != nullptr && P.N_Y == 0;
@@ -878,7 +895,7 @@ extern "C" int dgb_create(const dgb_problem* prob, int device, dgb_ctx** out) {
   if (P.gamcons) {
     const char* why = nullptr;
     if (P.N_Y != 0) why = "GAMCONS with mass fractions is not on the device path";
-    else if (P.D == 2 && !c->tiled)
+    else if (P.D == 2 && !c->tiled_full)
       why = "GAMCONS in 2D needs a structured row-major grid with nx a multiple of 32 and ny of 4 (p = 3: 2)";
     else if (P.limiter == DGB_LIM_M2L)  // M2limiting stops there too (limiting.cc:193-194, 410-411)
       why = "M2L is only implemented for gamncon";
@@ -890,7 +907,7 @@ extern "C" int dgb_create(const dgb_problem* prob, int device, dgb_ctx** out) {
     c->fused_lim = false;
   }
   if (P.N_Y > 3) { delete c; return set_error(DGB_ERR_UNSUPPORTED, "at most three mass fractions on the device path"); }
-  if (P.N_Y > 0 && P.D == 2 && !c->tiled) {
+  if (P.N_Y > 0 && P.D == 2 && !c->tiled_full) {
     delete c;
     return set_error(DGB_ERR_UNSUPPORTED, "mass fractions in 2D need a structured row-major grid with nx a multiple "
                                           "of 32 and ny of 4 (p = 3: 2)");
@@ -959,11 +976,23 @@ extern "C" int dgb_create(const dgb_problem* prob, int device, dgb_ctx** out) {
   cudaMemset(c->scal, 0, sizeof(DevScalars));
   if ((e = cudaMallocHost(&c->h_scal, sizeof(DevScalars))) != cudaSuccess) return fail(e, "pinned scalars");
   if (c->tiled) {
-    // row starts must be 16-byte aligned for TMA: nx is a multiple of TILE_W (32) and ld of 64
+    // row starts must be 16-byte aligned for TMA: nx is even and ld a multiple of 64
     const int th = tile_h_for(P.p);
     if (!(encode_state_map(c, c->A, &c->mapA, TILE_W, th) && encode_state_map(c, c->B, &c->mapB, TILE_W, th) &&
-          encode_state_map(c, c->C, &c->mapC, TILE_W, th)))
-      c->tiled = false;
+          encode_state_map(c, c->C, &c->mapC, TILE_W, th))) {
+      if (P.N_Y > 0 || P.gamcons) return fail(cudaErrorInvalidValue, "tensor maps for the tiled residual");
+      c->tiled = c->tiled_full = false;
+    }
+  }
+  if (c->tiled && !c->tiled_full) {
+    // the right strip (rows of the full tiles) and the top strip (all columns), in element order
+    const int th = tile_h_for(P.p), nxt = P.nx / TILE_W * TILE_W, nyt = P.ny / th * th;
+    std::vector<int> left;
+    for (int y = 0; y < P.ny; ++y)
+      for (int x = (y < nyt ? nxt : 0); x < P.nx; ++x) left.push_back(y * P.nx + x);
+    c->nleft = (int)left.size();
+    if ((e = cudaMalloc(&c->left, left.size() * sizeof(int))) != cudaSuccess) return fail(e, "leftover list");
+    cudaMemcpy(c->left, left.data(), left.size() * sizeof(int), cudaMemcpyHostToDevice);
   }
   cudaEventCreate(&c->e0);
   cudaEventCreate(&c->e1);
@@ -981,6 +1010,7 @@ extern "C" void dgb_destroy(dgb_ctx* c) {
       if (g) cudaGraphExecDestroy(g);
   for (double* b : {c->A, c->B, c->C, c->DU, c->X, c->ref}) if (b) cudaFree(b);
   if (c->nbr) cudaFree(c->nbr);
+  if (c->left) cudaFree(c->left);
   if (c->perm) cudaFree(c->perm);
   if (c->iperm) cudaFree(c->iperm);
   for (void* q : {(void*)c->ind_params, (void*)c->ind_w, (void*)c->ind_vec, (void*)c->ind_modes, (void*)c->ind_score,
@@ -1220,7 +1250,7 @@ extern "C" int dgb_indicator_scores(dgb_ctx* c, const double* U, float* score, i
 extern "C" int dgb_set_form(dgb_ctx* c, int form) {
   if (!c) return set_error(DGB_ERR_ARG, "null argument");
   if (form != DGB_FORM_FP64 && form != DGB_FORM_MIXED) return set_error(DGB_ERR_ARG, "unknown form");
-  if (form == DGB_FORM_MIXED && !(c->tiled && c->flux != DGB_FLUX_HLL && c->nmass == 0 && !c->gamcons))
+  if (form == DGB_FORM_MIXED && !(c->tiled_full && c->flux != DGB_FLUX_HLL && c->nmass == 0 && !c->gamcons))
     return set_error(DGB_ERR_UNSUPPORTED,
                      "the mixed form needs a structured 2D grid with nx a multiple of 32 and ny of 4 (p = 3: 2), "
                      "Rusanov or Roe");
