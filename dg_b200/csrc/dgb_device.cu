@@ -310,15 +310,16 @@ int tiles_then_strips(dgb_ctx* c, const StageArgs& a) {
 
 template <int MODE>
 int residual_dispatch(dgb_ctx* c, const StageArgs& a) {
-  if (c->tiled_full && c->form == DGB_FORM_MIXED) {
+  if (c->tiled && c->form == DGB_FORM_MIXED) {
+    // mixed full tiles; the strips outside them (if any) in the plain FP64 form
     const int key = c->p * 10 + c->flux;
     switch (key) {
-      case 10: launch_tile2d_mixed<1, 0, MODE>(c, a); return 0;
-      case 12: launch_tile2d_mixed<1, 2, MODE>(c, a); return 0;
-      case 20: launch_tile2d_mixed<2, 0, MODE>(c, a); return 0;
-      case 22: launch_tile2d_mixed<2, 2, MODE>(c, a); return 0;
-      case 30: launch_tile2d_mixed<3, 0, MODE>(c, a); return 0;
-      case 32: launch_tile2d_mixed<3, 2, MODE>(c, a); return 0;
+      case 10: launch_tile2d_mixed<1, 0, MODE>(c, a); if (c->nleft) launch_res2d<1, 0, MODE>(c, a, c->left, c->nleft); return 0;
+      case 12: launch_tile2d_mixed<1, 2, MODE>(c, a); if (c->nleft) launch_res2d<1, 2, MODE>(c, a, c->left, c->nleft); return 0;
+      case 20: launch_tile2d_mixed<2, 0, MODE>(c, a); if (c->nleft) launch_res2d<2, 0, MODE>(c, a, c->left, c->nleft); return 0;
+      case 22: launch_tile2d_mixed<2, 2, MODE>(c, a); if (c->nleft) launch_res2d<2, 2, MODE>(c, a, c->left, c->nleft); return 0;
+      case 30: launch_tile2d_mixed<3, 0, MODE>(c, a); if (c->nleft) launch_res2d<3, 0, MODE>(c, a, c->left, c->nleft); return 0;
+      case 32: launch_tile2d_mixed<3, 2, MODE>(c, a); if (c->nleft) launch_res2d<3, 2, MODE>(c, a, c->left, c->nleft); return 0;
       default: return set_error(DGB_ERR_UNSUPPORTED, "mixed form: p = 1..3 with Rusanov or Roe");
     }
   }
@@ -1250,7 +1251,7 @@ extern "C" int dgb_indicator_scores(dgb_ctx* c, const double* U, float* score, i
 extern "C" int dgb_set_form(dgb_ctx* c, int form) {
   if (!c) return set_error(DGB_ERR_ARG, "null argument");
   if (form != DGB_FORM_FP64 && form != DGB_FORM_MIXED) return set_error(DGB_ERR_ARG, "unknown form");
-  if (form == DGB_FORM_MIXED && !(c->tiled_full && c->flux != DGB_FLUX_HLL && c->nmass == 0 && !c->gamcons))
+  if (form == DGB_FORM_MIXED && !(c->tiled && c->flux != DGB_FLUX_HLL && c->nmass == 0 && !c->gamcons))
     return set_error(DGB_ERR_UNSUPPORTED,
                      "the mixed form needs a structured 2D grid with nx a multiple of 32 and ny of 4 (p = 3: 2), "
                      "Rusanov or Roe");
