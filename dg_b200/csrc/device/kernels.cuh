@@ -152,9 +152,9 @@ __global__ void __launch_bounds__(NT) residual2d_kernel(const Consts cin, const 
       dax += dPx[g * NS + t] * al;
       day += dPy[g * NS + t] * al;
     }
-    const double rho = ug[0], u = ug[1] / rho, v = ug[2] / rho, Et = ug[3];
-    const double gamma = 1 + 1.0 / ug[4];
-    const double p = (gamma - 1) * (Et - 0.5 * rho * (u * u + v * v));
+    // physics.cu:248-257 with correctly rounded reciprocals in place of its divisions
+    const double rho = ug[0], ir = __drcp_rn(rho), u = ug[1] * ir, v = ug[2] * ir, Et = ug[3];
+    const double p = __drcp_rn(ug[4]) * (Et - 0.5 * rho * (u * u + v * v));
     const double W = c.wq[g / NG1] * c.wq[g % NG1];
     const double cx = W * (c.ixx * c.J), cy = W * (c.iyy * c.J);
     G[(0 * NG + g) * TE + el] = cx * (rho * u);
@@ -214,8 +214,7 @@ __global__ void __launch_bounds__(NT) residual2d_kernel(const Consts cin, const 
 #pragma unroll
     for (int f = 0; f < NF; ++f) { L[f] = swapLR ? un[f] : uo[f]; R[f] = swapLR ? uo[f] : un[f]; }
     double F[NF], nc;
-    phys::riemann2d<FLUX>(L[0], R[0], L[1] / L[0], R[1] / R[0], L[2] / L[0], R[2] / R[0], L[3], R[3], L[4], R[4], nx,
-                          ny, F, nc);
+    phys::riemann2d_rcp<FLUX>(L, R, nx, ny, F, nc);  // the tiled kernel's flux (reciprocals for divisions)
     const double jw = (xface ? c.JFx : c.JFy) * c.wf[g];
 #pragma unroll
     for (int f = 0; f < NF; ++f) {
