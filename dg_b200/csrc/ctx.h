@@ -32,7 +32,8 @@ struct dgb_ctx {
   int slab_scheme = 0, slab_next = -1;
   bool slab_cfl = false;
   bool tiled = false;     // structured row-major grid with at least one full tile: tiled residual kernel
-  bool tiled_full = false;  // ... and extents that are tile multiples (no leftover strips)
+  bool tile_tma = false;  // ... with tensor maps for its tile loads (row pitch nx * 8 a multiple of 16)
+  bool tiled_full = false;  // ... with TMA and extents that are tile multiples (no leftover strips)
   int* left = nullptr;    // the elements outside the full tiles (generic residual kernel), nleft of them
   int nleft = 0;
   int form = DGB_FORM_FP64;  // arithmetic of the residual: plain FP64 or mixed FP32/FP64

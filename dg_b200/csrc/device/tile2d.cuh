@@ -110,7 +110,9 @@ constexpr bool kSfLift = DGB_SF_LIFT != 0;
 // rho*Y_k (u, v) (physics.cu:293-298) and the interface fluxes of phys::riemann2d_rcp.
 // GC: the GAMCONS model (fifth field rho/(gamma-1), conservative flux rho u/(gamma-1), no source;
 // physics.cu:253-281), with NY = 0.
-template <int P, int FLUX, int MODE, int TW, int TH, int UNROLL, int NY = 0, bool GC = false>
+// TMA = false: the tile and the stage base come in by plain coalesced loads (grids whose row pitch
+// nx * 8 bytes is not a multiple of 16, which a tensor map cannot describe); same arithmetic.
+template <int P, int FLUX, int MODE, int TW, int TH, int UNROLL, int NY = 0, bool GC = false, bool TMA = true>
 __device__ __forceinline__ void tile2d_body(const TileArgs& a, const CUtensorMap* mapU, const CUtensorMap* mapB,
                                             int tx0, int ty0, unsigned char* smraw, uint32_t& phase) {
   static_assert(!(GC && NY > 0), "GAMCONS with mass fractions is not built");
@@ -145,8 +147,14 @@ __device__ __forceinline__ void tile2d_body(const TileArgs& a, const CUtensorMap
   __syncthreads();
   // a TMA copy must land on a 128-byte shared boundary and start on a 16-byte global column;
   // otherwise record the fault and skip the copy (the wait below then reports it)
-  const bool tma_ok = (smem_u32(Us) & 127u) == 0 && (smem_u32(Fs) & 127u) == 0 && ((tx0 * 8) & 15) == 0;
-  if (tid == 0) {
+  const bool tma_ok = TMA && (smem_u32(Us) & 127u) == 0 && (smem_u32(Fs) & 127u) == 0 && ((tx0 * 8) & 15) == 0;
+  if constexpr (!TMA) {
+    for (int k = tid; k < NF * NS * NT; k += NT) {  // [plane][row][column], as the tensor map lands it
+      const int q = k / NT, el = k % NT;
+      Us[k] = __ldg(a.U + (size_t)q * ld + (size_t)(ty0 + el / TW) * nx + tx0 + el % TW);
+    }
+  }
+  if (TMA && tid == 0) {
     if (tma_ok) {
       mbar_arrive_expect_tx(bar, Dm::tile_bytes);
       tma_load_3d(Us, mapU, tx0, ty0, 0, bar);
@@ -173,8 +181,8 @@ __device__ __forceinline__ void tile2d_body(const TileArgs& a, const CUtensorMap
     (side == 0 ? HD : HU)[r] = v;
   }
   if (tid == 0) {
-    bool ok = tma_ok && mbar_wait(bar, phase & 1);
-    if (tma_ok && !ok) {
+    bool ok = !TMA || (tma_ok && mbar_wait(bar, phase & 1));
+    if (TMA && tma_ok && !ok) {
       atomicOr(a.errflag, (unsigned)FLAG_TIMEOUT);
       mbar_wait(bar, phase & 1);
     }
@@ -299,9 +307,17 @@ __device__ __forceinline__ void tile2d_body(const TileArgs& a, const CUtensorMap
     // the face buffer is free once every thread has read its face fluxes
     fence_proxy_async_smem();
     __syncthreads();
-    if (tid == 0 && need) {
-      mbar_arrive_expect_tx(bar, Dm::tile_bytes);
-      tma_load_3d(Ub, mapB, tx0, ty0, 0, bar);
+    if constexpr (TMA) {
+      if (tid == 0 && need) {
+        mbar_arrive_expect_tx(bar, Dm::tile_bytes);
+        tma_load_3d(Ub, mapB, tx0, ty0, 0, bar);
+      }
+    } else if (need) {
+      const double* base = MODE == MODE_SSP ? a.Ubase : a.Uacc;
+      for (int k = tid; k < NF * NS * NT; k += NT) {
+        const int q = k / NT, el = k % NT;
+        Ub[k] = __ldg(base + (size_t)q * ld + (size_t)(ty0 + el / TW) * nx + tx0 + el % TW);
+      }
     }
   }
 
@@ -396,7 +412,7 @@ __device__ __forceinline__ void tile2d_body(const TileArgs& a, const CUtensorMap
     return;
   }
   if (need) {
-    if (tid == 0) {
+    if (TMA && tid == 0) {
       bool ok = mbar_wait(bar, phase & 1);
       if (!ok) {
         atomicOr(a.errflag, (unsigned)FLAG_TIMEOUT);
@@ -404,7 +420,7 @@ __device__ __forceinline__ void tile2d_body(const TileArgs& a, const CUtensorMap
       }
       *s_ok = ok ? 1 : 0;
     }
-    ++phase;
+    if (TMA) ++phase;
     __syncthreads();
     if (!*s_ok) return;
   }
@@ -444,7 +460,7 @@ __device__ __forceinline__ void tile2d_body(const TileArgs& a, const CUtensorMap
   }
 }
 
-template <int P, int FLUX, int MODE, int TW, int TH, int NY = 0, bool GC = false>
+template <int P, int FLUX, int MODE, int TW, int TH, int NY = 0, bool GC = false, bool TMA = true>
 __global__ void __launch_bounds__(TW * TH, 2)
     residual2d_tile_kernel(const TileArgs a, const __grid_constant__ CUtensorMap mapU,
                            const __grid_constant__ CUtensorMap mapB) {
@@ -455,7 +471,7 @@ __global__ void __launch_bounds__(TW * TH, 2)
     fence_mbar_init();
   }
   uint32_t phase = 0;
-  tile2d_body<P, FLUX, MODE, TW, TH, vol_unroll<P>(), NY, GC>(a, &mapU, &mapB, blockIdx.x * TW, blockIdx.y * TH,
+  tile2d_body<P, FLUX, MODE, TW, TH, vol_unroll<P>(), NY, GC, TMA>(a, &mapU, &mapB, blockIdx.x * TW, blockIdx.y * TH,
                                                              smraw, phase);
 }
 

@@ -194,12 +194,12 @@ const CUtensorMap& map_of(dgb_ctx* c, const double* p) {
   return c->mapA;
 }
 
-template <int P, int FLUX, int MODE, int NY = 0, bool GC = false>
+template <int P, int FLUX, int MODE, int NY = 0, bool GC = false, bool TMA = true>
 void launch_tile2d(dgb_ctx* c, const StageArgs& s) {
   constexpr int TH = tile_h_for(P);
   using Dm = TileDims<P, TILE_W, TH, NY>;
   constexpr size_t smem = Dm::smem_bytes;
-  auto k = residual2d_tile_kernel<P, FLUX, MODE, TILE_W, TH, NY, GC>;
+  auto k = residual2d_tile_kernel<P, FLUX, MODE, TILE_W, TH, NY, GC, TMA>;
   static bool attr = false;
   if (!attr) { cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem); attr = true; }
   TileArgs a;
@@ -215,8 +215,10 @@ void launch_tile2d(dgb_ctx* c, const StageArgs& s) {
   a.JFx = c->cs.JFx;
   a.JFy = c->cs.JFy;
   a.nx = c->nx; a.ny = c->ny; a.ld = c->ld;
-  const CUtensorMap& mu = map_of(c, s.U);
-  const CUtensorMap& mb = MODE == MODE_SSP ? map_of(c, s.Ubase) : MODE == MODE_RK4 && s.Uacc ? map_of(c, s.Uacc) : mu;
+  // (without TMA the maps are not read: the tile loads are plain)
+  const CUtensorMap& mu = TMA ? map_of(c, s.U) : c->mapA;
+  const CUtensorMap& mb = !TMA ? c->mapA
+                          : MODE == MODE_SSP ? map_of(c, s.Ubase) : MODE == MODE_RK4 && s.Uacc ? map_of(c, s.Uacc) : mu;
   dim3 grid(c->nx / TILE_W, c->ny / TH);
   ProfScope ps(c, KC_RESIDUAL);
   k<<<grid, TILE_W * TH, smem, c->st>>>(a, mu, mb);
@@ -303,14 +305,15 @@ int residual_ny(dgb_ctx* c, const StageArgs& a) {
 // the stage input's neighbours from global memory
 template <int P, int FLUX, int MODE>
 int tiles_then_strips(dgb_ctx* c, const StageArgs& a) {
-  launch_tile2d<P, FLUX, MODE>(c, a);
+  if (c->tile_tma) launch_tile2d<P, FLUX, MODE>(c, a);
+  else launch_tile2d<P, FLUX, MODE, 0, false, false>(c, a);
   if (c->nleft) launch_res2d<P, FLUX, MODE>(c, a, c->left, c->nleft);
   return 0;
 }
 
 template <int MODE>
 int residual_dispatch(dgb_ctx* c, const StageArgs& a) {
-  if (c->tiled && c->form == DGB_FORM_MIXED) {
+  if (c->tile_tma && c->form == DGB_FORM_MIXED) {
     // mixed full tiles; the strips outside them (if any) in the plain FP64 form
     const int key = c->p * 10 + c->flux;
     switch (key) {
@@ -886,8 +889,12 @@ extern "C" int dgb_create(const dgb_problem* prob, int device, dgb_ctx** out) {
   c->rowmajor = P.D == 2 && is_row_major_grid(P) && std::getenv("DGB_NO_TILE") == nullptr;
   // tiled residual over the full tiles (the tensor map's row stride nx * 8 bytes must be a multiple
   // of 16: nx even); the strips left over on other extents go to the generic kernel
-  c->tiled = c->rowmajor && P.p <= 3 && P.nx % 2 == 0 && P.nx >= TILE_W && P.ny >= tile_h_for(P.p);
-  c->tiled_full = c->tiled && P.nx % TILE_W == 0 && P.ny % tile_h_for(P.p) == 0;
+  // tiled residual over the full tiles; the strips left over on other extents go to the generic
+  // kernel.  Tile loads by TMA where the tensor map's row pitch nx * 8 bytes is a multiple of 16
+  // (nx even), by plain loads otherwise
+  c->tiled = c->rowmajor && P.p <= 3 && P.nx >= TILE_W && P.ny >= tile_h_for(P.p);
+  c->tile_tma = c->tiled && P.nx % 2 == 0;
+  c->tiled_full = c->tile_tma && P.nx % TILE_W == 0 && P.ny % tile_h_for(P.p) == 0;
   // opt-in: measured slower than the two tiled passes on 512 x 256, p = 2 (64 vs 55 us per stage)
   c->fused_lim = c->rowmajor && (P.limiter == DGB_LIM_HRL || P.limiter == DGB_LIM_M2L) &&
                  std::getenv("DGB_FUSED_LIMITER") != nullptr && P.N_Y == 0;
@@ -976,13 +983,13 @@ extern "C" int dgb_create(const dgb_problem* prob, int device, dgb_ctx** out) {
   if ((e = cudaMalloc(&c->scal, sizeof(DevScalars))) != cudaSuccess) return fail(e, "scalars");
   cudaMemset(c->scal, 0, sizeof(DevScalars));
   if ((e = cudaMallocHost(&c->h_scal, sizeof(DevScalars))) != cudaSuccess) return fail(e, "pinned scalars");
-  if (c->tiled) {
+  if (c->tile_tma) {
     // row starts must be 16-byte aligned for TMA: nx is even and ld a multiple of 64
     const int th = tile_h_for(P.p);
     if (!(encode_state_map(c, c->A, &c->mapA, TILE_W, th) && encode_state_map(c, c->B, &c->mapB, TILE_W, th) &&
           encode_state_map(c, c->C, &c->mapC, TILE_W, th))) {
       if (P.N_Y > 0 || P.gamcons) return fail(cudaErrorInvalidValue, "tensor maps for the tiled residual");
-      c->tiled = c->tiled_full = false;
+      c->tile_tma = c->tiled_full = false;  // plain tile loads
     }
   }
   if (c->tiled && !c->tiled_full) {
@@ -1251,7 +1258,7 @@ extern "C" int dgb_indicator_scores(dgb_ctx* c, const double* U, float* score, i
 extern "C" int dgb_set_form(dgb_ctx* c, int form) {
   if (!c) return set_error(DGB_ERR_ARG, "null argument");
   if (form != DGB_FORM_FP64 && form != DGB_FORM_MIXED) return set_error(DGB_ERR_ARG, "unknown form");
-  if (form == DGB_FORM_MIXED && !(c->tiled && c->flux != DGB_FLUX_HLL && c->nmass == 0 && !c->gamcons))
+  if (form == DGB_FORM_MIXED && !(c->tile_tma && c->flux != DGB_FLUX_HLL && c->nmass == 0 && !c->gamcons))
     return set_error(DGB_ERR_UNSUPPORTED,
                      "the mixed form needs a structured 2D grid with nx a multiple of 32 and ny of 4 (p = 3: 2), "
                      "Rusanov or Roe");

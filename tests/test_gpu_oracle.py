@@ -26,11 +26,12 @@ CASES = [
     ("2d_p2_roe_hrl_tiled_box", 2, 2, 64, 32, ("reflective",) * 4, "roe", "hrl", "quadrants"),
     ("2d_p2_rus_m2l_tiled_walls", 2, 2, 96, 20, WALLS, "rusanov", "m2l", "shock_bubble"),
     ("2d_p1_rus_m2l_tiled", 2, 1, 64, 8, ("transmissive",) * 4, "rusanov", "m2l", "quadrants"),
-    # extents that are not tile multiples: full tiles by the tiled kernel, the right and top strips
-    # by the generic one (nx even), or all of it generic (nx odd)
+    # extents that are not tile multiples: full tiles by the tiled kernel (TMA tile loads for an even
+    # nx, plain loads for an odd one), the right and top strips by the generic kernel
     ("2d_p2_rus_m2l_strips_walls", 2, 2, 100, 46, WALLS, "rusanov", "m2l", "shock_bubble"),
     ("2d_p3_roe_hrl_strips", 2, 3, 70, 21, ("transmissive",) * 4, "roe", "hrl", "quadrants"),
     ("2d_p2_roe_m2l_odd_nx_periodic", 2, 2, 65, 20, ("periodic",) * 4, "roe", "m2l", "quadrants"),
+    ("2d_p3_rus_hrl_odd_nx_walls", 2, 3, 67, 9, WALLS, "rusanov", "hrl", "shock_bubble"),
     # p=3 with hrl between walls goes unstable at CFL 0.3 in the oracle as well; run it at 0.15
     ("1d_p3_hll_hrl_walls", 1, 3, 301, 1, ("reflective",) * 2, "hll", "hrl", "tube_noise", 0.15),
     ("1d_p1_rus_m2l_periodic", 1, 1, 257, 1, ("periodic",) * 2, "rusanov", "m2l", "tube_noise"),
