@@ -37,6 +37,7 @@ struct dgb_ctx {
   int* left = nullptr;    // the elements outside the full tiles (generic residual kernel), nleft of them
   int nleft = 0;
   int form = DGB_FORM_FP64;  // arithmetic of the residual: plain FP64 or mixed FP32/FP64
+  long long wait_polls = 1ll << 22;  // poll budget of the residual kernels' first wait per tile copy
   bool rowmajor = false;  // structured row-major grid: tiled limiter passes
   bool fused_lim = false; // row-major grid, hrl / m2l: both limiter passes in one kernel (opt-in)
   CUtensorMap mapA, mapB, mapC;  // TMA descriptors of the state buffers (tiled kernel)

@@ -34,6 +34,9 @@ struct Tab2 {
   double B1[NG1][N1];   // l_i(x_g) on the p+2 volume Gauss points (1D factor)
   double D1[NG1][N1];   // l_i'(x_g)
   double W1[NG1];       // 1D volume weights
+  // the 1D inverse mass matrix folded into the lift factors: Bt[g][i] = sum_j M1i[i][j] B1[g][j],
+  // Dt[g][i] = sum_j M1i[i][j] D1[g][j], Bft[g][i] = sum_j M1i[i][j] Bf[g][j]
+  double Bt[NG1][N1], Dt[NG1][N1], Bft[N1][N1];
 };
 
 static __constant__ Tab2<1> c_tab2_p1;
@@ -52,6 +55,7 @@ struct TileArgs {
   const int* __restrict__ nbr;
   const DevScalars* __restrict__ scal;
   unsigned int* errflag;  // receives FLAG_TIMEOUT when a bounded wait runs out
+  long long polls = kDefaultPolls;  // budget of the first wait on each tile copy (then drained)
   double a, b, dt_override;
   double invJ;           // 1 / J
   double cx, cy;         // J * 2/hx, J * 2/hy  (volume flux metric)
@@ -102,6 +106,92 @@ constexpr int vol_unroll() { return DGB_VOL_UNROLL > 0 ? DGB_VOL_UNROLL : (P == 
 #define DGB_SF_LIFT 1
 #endif
 constexpr bool kSfLift = DGB_SF_LIFT != 0;
+
+// Face fluxes of a tile, each face once: (TW+1)*TH x-faces and TW*(TH+1) y-faces, one work item
+// per face quadrature point spread over `nthr` threads, Riemann flux in the canonical orientation
+// (left/bottom state first, +x/+y normal).  Record k of Fs holds the NF fluxes and the ncterm;
+// boundary faces seen from the right/top element store -F so that every consumer forms (+F + nc)
+// on its left/bottom face and (-F + nc) on its right/top face.
+template <int P, int FLUX, int TW, int TH, int NY, bool GC>
+__device__ __forceinline__ void tile_face_fluxes(const double* Us, const double* HL, const double* HR,
+                                                 const double* HD, const double* HU, const int* codes, double* Fs,
+                                                 int tid, int nthr) {
+  using Dm = TileDims<P, TW, TH, NY>;
+  constexpr int N1 = Dm::N1, NS = Dm::NS, NF = Dm::NF, NT = Dm::NT, NXF = Dm::NXF, NYF = Dm::NYF;
+  constexpr int FS = NF + 1;
+  for (int k = tid; k < NXF + NYF; k += nthr) {
+    double L[NF], R[NF];
+    double nxv, nyv, sgn = 1.0;
+    double vl[NF][N1], vr[NF][N1];
+    int code = 0;
+    bool first_edge;
+    int mom;
+    int g;
+    if (k < NXF) {
+      // x-face fx (0..TW) of row fy; left element (fx-1, fy), right element (fx, fy)
+      g = k % N1;
+      const int fy = (k / N1) % TH, fx = k / (N1 * TH);
+      if (fx == 0) code = codes[fy];
+      if (fx == TW) code = codes[TH + fy];
+#pragma unroll
+      for (int f = 0; f < NF; ++f)
+#pragma unroll
+        for (int j = 0; j < N1; ++j) {
+          vl[f][j] = fx > 0 ? Us[(f * NS + P + N1 * j) * NT + fy * TW + fx - 1] : HL[(fy * NF + f) * N1 + j];
+          vr[f][j] = fx < TW ? Us[(f * NS + N1 * j) * NT + fy * TW + fx] : HR[(fy * NF + f) * N1 + j];
+        }
+      nxv = 1.0;
+      nyv = 0.0;
+      first_edge = fx == 0;
+      mom = 1;
+    } else {
+      const int kk = k - NXF;
+      g = kk % N1;
+      const int fx = (kk / N1) % TW, fy = kk / (N1 * TW);
+      if (fy == 0) code = codes[2 * TH + fx];
+      if (fy == TH) code = codes[2 * TH + TW + fx];
+#pragma unroll
+      for (int f = 0; f < NF; ++f)
+#pragma unroll
+        for (int j = 0; j < N1; ++j) {
+          vl[f][j] = fy > 0 ? Us[(f * NS + j + N1 * P) * NT + (fy - 1) * TW + fx] : HD[(fx * NF + f) * N1 + j];
+          vr[f][j] = fy < TH ? Us[(f * NS + j) * NT + fy * TW + fx] : HU[(fx * NF + f) * N1 + j];
+        }
+      nxv = 0.0;
+      nyv = 1.0;
+      first_edge = fy == 0;
+      mom = 2;
+    }
+    if (code < 0) {
+      // domain boundary: the inside element is L with its outward normal, the mirror state is R
+      // (reflective walls mirror the wall-normal momentum, code/src/bc/boundaries.cu:20-67)
+#pragma unroll
+      for (int f = 0; f < NF; ++f)
+#pragma unroll
+        for (int j = 0; j < N1; ++j) {
+          const double own = first_edge ? vr[f][j] : vl[f][j];
+          vl[f][j] = own;
+          vr[f][j] = (code == -3 && f == mom) ? -own : own;
+        }
+      if (first_edge) { nxv = -nxv; nyv = -nyv; sgn = -1.0; }
+    }
+#pragma unroll
+    for (int f = 0; f < NF; ++f) {
+      double sl = 0, sr = 0;
+#pragma unroll
+      for (int j = 0; j < N1; ++j) { sl += DGB_TAB2(P, Bf[g][j]) * vl[f][j]; sr += DGB_TAB2(P, Bf[g][j]) * vr[f][j]; }
+      L[f] = sl;
+      R[f] = sr;
+    }
+    double F[NF], nc;
+    phys::riemann2d_rcp<FLUX, NY, GC>(L, R, nxv, nyv, F, nc);
+    // boundary faces seen from the right/top element store -F so that every consumer forms
+    // (+F + nc) on its left/bottom face and (-F + nc) on its right/top face
+#pragma unroll
+    for (int f = 0; f < NF; ++f) Fs[k * FS + f] = sgn * F[f];
+    Fs[k * FS + NF] = nc;
+  }
+}
 
 // The work of one tile (origin tx0, ty0).  The caller has initialised the mbarrier at the start of
 // shared memory; `phase` counts its completed phases (a persistent caller runs many tiles on one
@@ -181,7 +271,7 @@ __device__ __forceinline__ void tile2d_body(const TileArgs& a, const CUtensorMap
     (side == 0 ? HD : HU)[r] = v;
   }
   if (tid == 0) {
-    bool ok = !TMA || (tma_ok && mbar_wait(bar, phase & 1));
+    bool ok = !TMA || (tma_ok && mbar_wait(bar, phase & 1, a.polls));
     if (TMA && tma_ok && !ok) {
       atomicOr(a.errflag, (unsigned)FLAG_TIMEOUT);
       mbar_wait(bar, phase & 1);
@@ -193,78 +283,7 @@ __device__ __forceinline__ void tile2d_body(const TileArgs& a, const CUtensorMap
   if (!*s_ok) return;
 
   // ---------------- phase 1: face fluxes, each face of the tile once ----------------
-  for (int k = tid; k < NXF + NYF; k += NT) {
-    double L[NF], R[NF];
-    double nxv, nyv, sgn = 1.0;
-    double vl[NF][N1], vr[NF][N1];
-    int code = 0;
-    bool first_edge;
-    int mom;
-    int g;
-    if (k < NXF) {
-      // x-face fx (0..TW) of row fy; left element (fx-1, fy), right element (fx, fy)
-      g = k % N1;
-      const int fy = (k / N1) % TH, fx = k / (N1 * TH);
-      if (fx == 0) code = codes[fy];
-      if (fx == TW) code = codes[TH + fy];
-#pragma unroll
-      for (int f = 0; f < NF; ++f)
-#pragma unroll
-        for (int j = 0; j < N1; ++j) {
-          vl[f][j] = fx > 0 ? Us[(f * NS + P + N1 * j) * NT + fy * TW + fx - 1] : HL[(fy * NF + f) * N1 + j];
-          vr[f][j] = fx < TW ? Us[(f * NS + N1 * j) * NT + fy * TW + fx] : HR[(fy * NF + f) * N1 + j];
-        }
-      nxv = 1.0;
-      nyv = 0.0;
-      first_edge = fx == 0;
-      mom = 1;
-    } else {
-      const int kk = k - NXF;
-      g = kk % N1;
-      const int fx = (kk / N1) % TW, fy = kk / (N1 * TW);
-      if (fy == 0) code = codes[2 * TH + fx];
-      if (fy == TH) code = codes[2 * TH + TW + fx];
-#pragma unroll
-      for (int f = 0; f < NF; ++f)
-#pragma unroll
-        for (int j = 0; j < N1; ++j) {
-          vl[f][j] = fy > 0 ? Us[(f * NS + j + N1 * P) * NT + (fy - 1) * TW + fx] : HD[(fx * NF + f) * N1 + j];
-          vr[f][j] = fy < TH ? Us[(f * NS + j) * NT + fy * TW + fx] : HU[(fx * NF + f) * N1 + j];
-        }
-      nxv = 0.0;
-      nyv = 1.0;
-      first_edge = fy == 0;
-      mom = 2;
-    }
-    if (code < 0) {
-      // domain boundary: the inside element is L with its outward normal, the mirror state is R
-      // (reflective walls mirror the wall-normal momentum, code/src/bc/boundaries.cu:20-67)
-#pragma unroll
-      for (int f = 0; f < NF; ++f)
-#pragma unroll
-        for (int j = 0; j < N1; ++j) {
-          const double own = first_edge ? vr[f][j] : vl[f][j];
-          vl[f][j] = own;
-          vr[f][j] = (code == -3 && f == mom) ? -own : own;
-        }
-      if (first_edge) { nxv = -nxv; nyv = -nyv; sgn = -1.0; }
-    }
-#pragma unroll
-    for (int f = 0; f < NF; ++f) {
-      double sl = 0, sr = 0;
-#pragma unroll
-      for (int j = 0; j < N1; ++j) { sl += DGB_TAB2(P, Bf[g][j]) * vl[f][j]; sr += DGB_TAB2(P, Bf[g][j]) * vr[f][j]; }
-      L[f] = sl;
-      R[f] = sr;
-    }
-    double F[NF], nc;
-    phys::riemann2d_rcp<FLUX, NY, GC>(L, R, nxv, nyv, F, nc);
-    // boundary faces seen from the right/top element store -F so that every consumer forms
-    // (+F + nc) on its left/bottom face and (-F + nc) on its right/top face
-#pragma unroll
-    for (int f = 0; f < NF; ++f) Fs[k * FS + f] = sgn * F[f];
-    Fs[k * FS + NF] = nc;
-  }
+  tile_face_fluxes<P, FLUX, TW, TH, NY, GC>(Us, HL, HR, HD, HU, codes, Fs, tid, NT);
   __syncthreads();
 
   // ---------------- phase 2: volume terms and assembly, one thread per element ----------------
@@ -413,7 +432,7 @@ __device__ __forceinline__ void tile2d_body(const TileArgs& a, const CUtensorMap
   }
   if (need) {
     if (TMA && tid == 0) {
-      bool ok = mbar_wait(bar, phase & 1);
+      bool ok = mbar_wait(bar, phase & 1, a.polls);
       if (!ok) {
         atomicOr(a.errflag, (unsigned)FLAG_TIMEOUT);
         mbar_wait(bar, phase & 1);

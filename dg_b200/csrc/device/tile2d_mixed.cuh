@@ -124,7 +124,7 @@ __global__ void __launch_bounds__(TW * TH, 3)
     (side == 0 ? HD : HU)[r] = v;
   }
   if (tid == 0) {
-    bool ok = tma_ok && mbar_wait(bar, 0);
+    bool ok = tma_ok && mbar_wait(bar, 0, a.polls);
     if (tma_ok && !ok) {
       atomicOr(a.errflag, (unsigned)FLAG_TIMEOUT);
       mbar_wait(bar, 0);

@@ -45,8 +45,13 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
   return ok != 0;
 }
 
-// Bounded wait for phase `parity` of `bar`; false when the budget ran out.
-__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, long long max_polls = (1ll << 22)) {
+// Default poll budget of a bounded wait (about 4 M polls: far beyond any copy's latency).
+constexpr long long kDefaultPolls = 1ll << 22;
+
+// Bounded wait for phase `parity` of `bar`; false when the budget ran out.  A caller whose first
+// wait gave up waits again with the default budget before it leaves, so that no copy still lands
+// in the shared memory of a finished CTA.
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, long long max_polls = kDefaultPolls) {
   for (long long k = 0; k < max_polls; ++k)
     if (mbar_try_wait(bar, parity)) return true;
   return false;

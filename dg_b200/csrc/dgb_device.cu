@@ -205,6 +205,7 @@ void launch_tile2d(dgb_ctx* c, const StageArgs& s) {
   TileArgs a;
   a.U = s.U; a.Ubase = s.Ubase; a.out = s.out; a.Uacc = s.Uacc; a.nbr = s.nbr; a.scal = s.scal;
   a.errflag = &c->scal->flags;
+  a.polls = c->wait_polls;
   a.a = s.a; a.b = s.b; a.dt_override = s.dt_override;
   a.J = c->cs.J;
   a.invJ = 1.0 / c->cs.J;
@@ -234,6 +235,7 @@ void launch_tile2d_mixed(dgb_ctx* c, const StageArgs& s) {
   TileArgs a;
   a.U = s.U; a.Ubase = s.Ubase; a.out = s.out; a.Uacc = s.Uacc; a.nbr = s.nbr; a.scal = s.scal;
   a.errflag = &c->scal->flags;
+  a.polls = c->wait_polls;
   a.a = s.a; a.b = s.b; a.dt_override = s.dt_override;
   a.J = c->cs.J;
   a.invJ = 1.0 / c->cs.J;
@@ -887,8 +889,6 @@ extern "C" int dgb_create(const dgb_problem* prob, int device, dgb_ctx** out) {
   c->hx = P.hx;
   c->hy = P.hy;
   c->rowmajor = P.D == 2 && is_row_major_grid(P) && std::getenv("DGB_NO_TILE") == nullptr;
-  // tiled residual over the full tiles (the tensor map's row stride nx * 8 bytes must be a multiple
-  // of 16: nx even); the strips left over on other extents go to the generic kernel
   // tiled residual over the full tiles; the strips left over on other extents go to the generic
   // kernel.  Tile loads by TMA where the tensor map's row pitch nx * 8 bytes is a multiple of 16
   // (nx even), by plain loads otherwise
@@ -983,6 +983,11 @@ extern "C" int dgb_create(const dgb_problem* prob, int device, dgb_ctx** out) {
   if ((e = cudaMalloc(&c->scal, sizeof(DevScalars))) != cudaSuccess) return fail(e, "scalars");
   cudaMemset(c->scal, 0, sizeof(DevScalars));
   if ((e = cudaMallocHost(&c->h_scal, sizeof(DevScalars))) != cudaSuccess) return fail(e, "pinned scalars");
+  // the tensor maps are kernel arguments of every tiled launch, also of the plain-load variant
+  // that never reads them: zeroed, not left undefined, when no map is encoded
+  std::memset(&c->mapA, 0, sizeof(CUtensorMap));
+  std::memset(&c->mapB, 0, sizeof(CUtensorMap));
+  std::memset(&c->mapC, 0, sizeof(CUtensorMap));
   if (c->tile_tma) {
     // row starts must be 16-byte aligned for TMA: nx is even and ld a multiple of 64
     const int th = tile_h_for(P.p);
@@ -1260,8 +1265,8 @@ extern "C" int dgb_set_form(dgb_ctx* c, int form) {
   if (form != DGB_FORM_FP64 && form != DGB_FORM_MIXED) return set_error(DGB_ERR_ARG, "unknown form");
   if (form == DGB_FORM_MIXED && !(c->tile_tma && c->flux != DGB_FLUX_HLL && c->nmass == 0 && !c->gamcons))
     return set_error(DGB_ERR_UNSUPPORTED,
-                     "the mixed form needs a structured 2D grid with nx a multiple of 32 and ny of 4 (p = 3: 2), "
-                     "Rusanov or Roe");
+                     "the mixed form needs a structured row-major 2D grid with even nx >= 32 and ny >= 4 "
+                     "(p = 3: 2), Rusanov or Roe, no mass fractions, GAMNCON");
   if (form != c->form) {
     DGB_CUDA(cudaSetDevice(c->device));
     DGB_CUDA(cudaStreamSynchronize(c->st));
@@ -1269,6 +1274,20 @@ extern "C" int dgb_set_form(dgb_ctx* c, int form) {
       for (auto& g : row)
         if (g) { cudaGraphExecDestroy(g); g = nullptr; }
     c->form = form;
+  }
+  return DGB_OK;
+}
+
+extern "C" int dgb_set_wait_limit(dgb_ctx* c, long long polls) {
+  if (!c) return set_error(DGB_ERR_ARG, "null argument");
+  if (polls < 0) return set_error(DGB_ERR_ARG, "negative poll budget");
+  if (polls != c->wait_polls) {
+    DGB_CUDA(cudaSetDevice(c->device));
+    DGB_CUDA(cudaStreamSynchronize(c->st));
+    for (auto& row : c->graphs)  // the budget is a kernel argument of the captured launches
+      for (auto& g : row)
+        if (g) { cudaGraphExecDestroy(g); g = nullptr; }
+    c->wait_polls = polls;
   }
   return DGB_OK;
 }

@@ -136,16 +136,36 @@ void launch(const View& v, cudaStream_t st) {
   }
 }
 
-bool row_major(const Problem& P) {
-  if (P.D != 2 || P.nx <= 0 || P.ny <= 0 || (long)P.nx * P.ny != P.N_E) return false;
-  for (int e = 0; e < P.N_E; ++e) {
-    const int ix = e % P.nx, iy = e / P.nx;
-    if (ix > 0 && P.nbr[(size_t)0 * P.N_E + e] != e - 1) return false;
-    if (ix < P.nx - 1 && P.nbr[(size_t)1 * P.N_E + e] != e + 1) return false;
-    if (iy > 0 && P.nbr[(size_t)2 * P.N_E + e] != e - P.nx) return false;
-    if (iy < P.ny - 1 && P.nbr[(size_t)3 * P.N_E + e] != e + P.nx) return false;
+// The neighbour table nbr[k*ld + e] of a structured grid (a 1D chain or a row-major nx x ny grid)
+// from the rule of each side (a boundary code < 0, or kSideWrap: the element on the opposite
+// side); columns beyond N_E hold the "frozen" code -4.  Filled on the device, so a call on a
+// structured problem copies nothing from the host.
+struct SideRules {
+  int rule[4];
+};
+
+__global__ void structured_nbr_kernel(int* nbr, int ld, int ne, int nx, int ny, int nsides, SideRules r) {
+  const int e = blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= ld) return;
+  const int ix = e % nx, iy = e / nx;
+  for (int k = 0; k < nsides; ++k) {
+    int v = -4;
+    if (e < ne) {
+      const bool edge = k == 0 ? ix == 0 : k == 1 ? ix == nx - 1 : k == 2 ? iy == 0 : iy == ny - 1;
+      const int inner = k == 0 ? e - 1 : k == 1 ? e + 1 : k == 2 ? e - nx : e + nx;
+      const int wrap = k == 0 ? e + nx - 1 : k == 1 ? e - (nx - 1) : k == 2 ? e + (ny - 1) * nx : e - (ny - 1) * nx;
+      v = !edge ? inner : r.rule[k] == Problem::kSideWrap ? wrap : r.rule[k];
+    }
+    nbr[(size_t)k * ld + e] = v;
   }
-  return true;
+}
+
+struct NodePerm {
+  int t[MAXNS];
+};
+
+__global__ void store_perm_kernel(int* dst, int n, NodePerm p) {
+  if ((int)threadIdx.x < n) dst[threadIdx.x] = p.t[threadIdx.x];
 }
 
 }  // namespace
@@ -180,19 +200,32 @@ extern "C" int dgb_limit_noalloc(const dgb_problem* prob, const double* U_in_dev
   unsigned char* base = static_cast<unsigned char*>(scratch);
   View v;
   v.D = P.D; v.p = P.p; v.nf = P.N_F; v.ns = P.N_s; v.ne = P.N_E; v.ld = ld; v.nx = P.nx; v.ny = P.ny;
-  v.rowmajor = row_major(P);
+  v.rowmajor = P.D == 2 && P.structured;
   v.nbr = reinterpret_cast<const int*>(base);
   v.perm = reinterpret_cast<const int*>(base + perm_off);
   v.Uint = reinterpret_cast<double*>(base + uint_off);
   v.X = reinterpret_cast<double*>(base + x_off);
-  // neighbour table (padding columns beyond N_E hold the "frozen" code) and node permutation
-  std::vector<int> nb((size_t)P.N_N * ld, -4);
-  for (int k = 0; k < P.N_N; ++k)
-    for (int el = 0; el < P.N_E; ++el) nb[(size_t)k * ld + el] = P.nbr[(size_t)k * P.N_E + el];
-  if ((e = cudaMemcpyAsync(base, nb.data(), nbr_bytes, cudaMemcpyHostToDevice, st)) != cudaSuccess ||
-      (e = cudaMemcpyAsync(base + perm_off, P.tensor_perm.data(), P.N_s * sizeof(int), cudaMemcpyHostToDevice, st)) !=
-          cudaSuccess)
-    return set_error(DGB_ERR_CUDA, std::string("neighbour upload: ") + cudaGetErrorString(e));
+  // the neighbour table: built on the device for a structured grid whose sides each follow one
+  // rule (found when the problem was set up); otherwise copied from the host (a pageable copy:
+  // CUDA stages it before returning, after synchronising the stream)
+  const int nsides = P.D == 1 ? 2 : 4;
+  bool uniform = P.structured;
+  for (int k = 0; k < nsides; ++k) uniform = uniform && P.side_rule[k] != Problem::kSideMixed;
+  if (uniform) {
+    SideRules r;
+    for (int k = 0; k < 4; ++k) r.rule[k] = P.side_rule[k];
+    structured_nbr_kernel<<<(ld + 255) / 256, 256, 0, st>>>(reinterpret_cast<int*>(base), ld, P.N_E, P.nx, P.ny,
+                                                             nsides, r);
+  } else {
+    std::vector<int> nb((size_t)P.N_N * ld, -4);
+    for (int k = 0; k < P.N_N; ++k)
+      for (int el = 0; el < P.N_E; ++el) nb[(size_t)k * ld + el] = P.nbr[(size_t)k * P.N_E + el];
+    if ((e = cudaMemcpyAsync(base, nb.data(), nbr_bytes, cudaMemcpyHostToDevice, st)) != cudaSuccess)
+      return set_error(DGB_ERR_CUDA, std::string("neighbour upload: ") + cudaGetErrorString(e));
+  }
+  NodePerm np;
+  for (int t = 0; t < MAXNS; ++t) np.t[t] = t < P.N_s ? P.tensor_perm[t] : 0;
+  store_perm_kernel<<<1, 32, 0, st>>>(reinterpret_cast<int*>(base + perm_off), P.N_s, np);
   const int grid = (int)std::min<size_t>(((size_t)P.N_E * P.N_F * P.N_s + 255) / 256, 148 * 32);
   ref_to_internal_kernel<<<grid, 256, 0, st>>>(U_in_dev, v.Uint, v.perm, P.N_E, P.N_F, P.N_s, ld);
   const int key = P.p * 10 + P.limiter;
@@ -207,8 +240,7 @@ extern "C" int dgb_limit_noalloc(const dgb_problem* prob, const double* U_in_dev
   }
   // the 1D limiter writes its result to the x-pass buffer, the 2D passes back into Uint
   internal_to_ref_kernel<<<grid, 256, 0, st>>>(P.D == 1 ? v.X : v.Uint, U_out_dev, v.perm, P.N_E, P.N_F, P.N_s, ld);
-  // the neighbour table above came from pageable memory that must outlive the copy
-  if ((e = cudaStreamSynchronize(st)) != cudaSuccess)
+  if ((e = cudaGetLastError()) != cudaSuccess)
     return set_error(DGB_ERR_CUDA, std::string("dgb_limit_noalloc: ") + cudaGetErrorString(e));
   return DGB_OK;
 }

@@ -100,6 +100,13 @@ struct Problem {
   std::vector<int> tensor_perm;       // tensor node t -> Gmsh node index
   std::vector<int> nbr;               // [face k][e], k = L,R(,D,U); boundary codes < 0
   double hx = 0.0, hy = 0.0;          // uniform element sizes
+  // Structured element order: 1D elements in a chain (neighbours e -+ 1), or a row-major nx x ny
+  // 2D grid (e -+ 1, e -+ nx); and, per side (L, R, D, U), the one rule its boundary elements share:
+  // a boundary code (< 0), kSideWrap (periodic: the element on the opposite side) or kSideMixed.
+  // Found once when the problem is set up.
+  static constexpr int kSideWrap = 1, kSideMixed = 2;
+  bool structured = false;
+  int side_rule[4] = {kSideMixed, kSideMixed, kSideMixed, kSideMixed};
 };
 
 // deck.cc
@@ -118,6 +125,7 @@ double lagrange1d(const std::vector<double>& nodes, int i, double x);
 double dlagrange1d(const std::vector<double>& nodes, int i, double x);
 bool invert(std::vector<double>& A, int n);  // column-major in-place inverse (partial pivoting LU)
 // setup.cc
+void classify_grid(Problem& P);  // fills Problem::structured and side_rule (setup.cc)
 Status build_problem(Mesh&& mesh, int dim, int order, const std::string& elem_kind, int flux, int limiter,
                      double cfl, const std::vector<double>& thresholds, const std::vector<double>& out_times,
                      double final_time, Problem& P, int n_mass = 0, bool gamcons = false);

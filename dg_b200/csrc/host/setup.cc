@@ -536,8 +536,43 @@ Status build_problem(Mesh&& mesh, int dim, int p, const std::string& kind, int f
       nxg += 1;
       if (nxg > 0 && NE % nxg == 0) { P.nx = nxg; P.ny = NE / nxg; }
     }
+    classify_grid(P);
   }
   return Status();
+}
+
+// Structured order and per-side boundary rules of the device neighbour table P.nbr (see host.h).
+void classify_grid(Problem& P) {
+  const int NE = P.N_E, nx = P.nx, ny = P.ny, nsides = P.D == 1 ? 2 : 4;
+  P.structured = false;
+  for (int k = 0; k < 4; ++k) P.side_rule[k] = Problem::kSideMixed;
+  if (nx <= 0 || ny <= 0 || (long)nx * ny != NE) return;
+  auto nb = [&](int k, int e) { return P.nbr[(size_t)k * NE + e]; };
+  for (int e = 0; e < NE; ++e) {
+    const int ix = e % nx, iy = e / nx;
+    if (ix > 0 && nb(0, e) != e - 1) return;
+    if (ix < nx - 1 && nb(1, e) != e + 1) return;
+    if (P.D == 2 && iy > 0 && nb(2, e) != e - nx) return;
+    if (P.D == 2 && iy < ny - 1 && nb(3, e) != e + nx) return;
+  }
+  P.structured = true;
+  for (int k = 0; k < nsides; ++k) {
+    // the boundary elements of side k, the element a wrap would reach, and their rule
+    const int n = k < 2 ? ny : nx;
+    int rule = 0;
+    for (int j = 0; j < n; ++j) {
+      int e, wrap;
+      if (k == 0) { e = j * nx; wrap = e + nx - 1; }
+      else if (k == 1) { e = j * nx + nx - 1; wrap = j * nx; }
+      else if (k == 2) { e = j; wrap = (ny - 1) * nx + j; }
+      else { e = (ny - 1) * nx + j; wrap = j; }
+      const int v = nb(k, e);
+      const int r = v < 0 ? v : (v == wrap ? Problem::kSideWrap : Problem::kSideMixed);
+      if (r == Problem::kSideMixed || (j > 0 && r != rule)) { rule = Problem::kSideMixed; break; }
+      rule = r;
+    }
+    P.side_rule[k] = rule;
+  }
 }
 
 // ---------------------------------------------------------------------------------------

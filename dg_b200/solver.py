@@ -178,6 +178,12 @@ class DGSolver:
         and fluxes on FP64 anchors, FP64 pressure recovery and stage update)."""
         F.check(F.lib().dgb_set_form(self._h, F.FORM[form]))
 
+    def set_wait_limit(self, polls: int = 1 << 22) -> None:
+        """Poll budget of the residual kernels' first wait on each tile copy (0: give up at once,
+        which makes the next step fail with DGB_ERR_TIMEOUT; the default restores the normal
+        budget)."""
+        F.check(F.lib().dgb_set_wait_limit(self._h, int(polls)))
+
     def sensors(self, U) -> np.ndarray:
         """Troubled-cell flags of U (SENSOR::sensing): 0 or the number of the sensor that fired."""
         flags = np.zeros(self.problem.info.n_elem, np.int32)

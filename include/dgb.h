@@ -199,6 +199,12 @@ int dgb_sensors(dgb_ctx* c, const double* U_host, int* flags_host);
 /* Selects the arithmetic of the residual kernels (enum dgb_form) for later calls; no counterpart
  * in the reference, which is FP64 only. */
 int dgb_set_form(dgb_ctx* c, int form);
+/* Poll budget of the first wait of the residual kernels on each tile copy (default 4194304 polls;
+ * the copy is drained with the default budget before the kernel returns).  A budget that runs out
+ * makes the step return DGB_ERR_TIMEOUT and leaves the context usable; a budget of 0 makes every
+ * such wait give up at once, which tests of the timeout path use.  No counterpart in the
+ * reference, whose kernels have no bounded waits. */
+int dgb_set_wait_limit(dgb_ctx* c, long long polls);
 /* CFL step of the context's current (device-resident) state, as dgb_dt_from_cfl computes it. */
 int dgb_cfl_dt(dgb_ctx* c, double* dt);
 /* Dt = CFL_scaled / max_nodes(|u|+a) (RK::DtFromCFL, rk.cc:250-272). */
@@ -336,9 +342,12 @@ int dgb_batch_last_timing(dgb_batch* b, double* ms, long long* launches);
  * fixed device-memory budget claimed at start-up, or a time loop that must not trigger
  * cudaMalloc (and the device synchronisation it implies) -- and therefore cannot call
  * dgb_create.  Applies the problem's limiter (hrl or m2l) to the state U_in_dev and writes the
- * result to U_out_dev (both in the caller's device memory, reference layout, may alias), on the
- * CUDA stream `stream` (0 = default stream) of the current device, and returns once it is done.
- * Temporaries live in one library-owned device array of 128 MiB, which every GPU that loads
+ * result to U_out_dev (both in the caller's device memory, reference layout, may alias).  The
+ * work is queued on the CUDA stream `stream` (0 = default stream) of the current device and the
+ * call returns without waiting for it: the result is there once the stream has reached it.  On a
+ * structured grid (a 1D chain or a row-major 2D grid, each side with one boundary rule) the call
+ * copies nothing from the host; on any other element order it copies the neighbour table from
+ * host memory every time, and that copy first waits for the stream.  Temporaries live in one library-owned device array of 128 MiB, which every GPU that loads
  * this library holds until the process exits; a problem that needs more (2D: above about 166k
  * elements at p=2, 94k at p=3) is rejected with DGB_ERR_ARG.  The first call on a device looks
  * up that array's device address and uploads the limiter tables; make it before any stream

@@ -20,7 +20,9 @@ Out-of-tree additions (none of them touch reference arithmetic):
   * ``--wrap`` of RK::RK_integration so the harness can drive single operators;
   * main() renamed to dgref_main.
 
-Usage: python oracle/build_ref.py [--ref /root/reference/code/src] [--jobs 8] [variant ...]
+Usage: python oracle/build_ref.py [--ref <reference checkout>/code/src] [--jobs 8] [variant ...]
+(defaults: $DGB_REFERENCE_SRC or /root/reference/code/src; OpenBLAS from $DGB_REF_BLAS or found in
+site-packages)
 """
 from __future__ import annotations
 
@@ -34,9 +36,24 @@ from pathlib import Path
 
 HERE = Path(__file__).resolve().parent
 OUT = HERE / "_ref"
-DEFAULT_REF = Path("/root/reference/code/src")
-BLAS_DIR = Path("/opt/prime-rl/.venv/lib/python3.12/site-packages/opencv_python_headless.libs")
-BLAS_LIB = "libopenblasp-r0-59ffcd50.3.15.so"
+# the read-only reference checkout; DGB_REFERENCE_SRC overrides it
+DEFAULT_REF = Path(os.environ.get("DGB_REFERENCE_SRC", "/root/reference/code/src"))
+
+
+def find_blas() -> Path:
+    """An LP64 OpenBLAS with plain F77 names (dgemm_, dgetrf_, ...): $DGB_REF_BLAS if set, else
+    the copy bundled with an installed opencv-python-headless wheel (site-packages/
+    opencv_python_headless.libs/libopenblas*.so; its libgfortran sits beside it)."""
+    env = os.environ.get("DGB_REF_BLAS")
+    if env:
+        return Path(env)
+    import site
+    import sysconfig
+    roots = [Path(p) for p in site.getsitepackages() + [sysconfig.get_paths()["purelib"]]]
+    for r in roots:
+        for cand in sorted((r / "opencv_python_headless.libs").glob("libopenblas*.so*")):
+            return cand
+    raise FileNotFoundError("no LP64 OpenBLAS found: set DGB_REF_BLAS to a libopenblas*.so with F77 names")
 
 VARIANTS = {
     "1d_roe": dict(dims="ONED", nf=4, d=1, flux="ROE"),
@@ -119,9 +136,10 @@ def build_variant(name: str, ref: Path, pool: cf.Executor) -> Path:
             raise RuntimeError(f"harness compile failed:\n{r.stderr[-3000:]}")
     exe = OUT / f"dgref_{name}"
     objs = sorted(str(p) for p in objdir.glob("*.o"))
+    blas = find_blas()
     link = (["g++", "-o", str(exe)] + objs +
             [f"-Wl,--wrap=_Z10blasIdamaxiPdi", f"-Wl,--wrap={RK_SYM}",
-             f"-L{BLAS_DIR}", f"-l:{BLAS_LIB}", "-Wl,--disable-new-dtags", f"-Wl,-rpath,{BLAS_DIR}", "-lm"])
+             f"-L{blas.parent}", f"-l:{blas.name}", "-Wl,--disable-new-dtags", f"-Wl,-rpath,{blas.parent}", "-lm"])
     r = subprocess.run(link, capture_output=True, text=True)
     if r.returncode != 0:
         raise RuntimeError(f"link failed for {name}:\n{r.stderr[-3000:]}")

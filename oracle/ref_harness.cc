@@ -200,6 +200,7 @@ __wrap__ZN2RK14RK_integrationEdiiiiiiiPdS0_R8LimitingbR9DG_SOLVERR12COMMUNICATOR
     auto t0 = std::chrono::steady_clock::now();
     for (int s = 0; s < a.nsteps; ++s) {
       const double Dt = a.dt > 0 ? a.dt : rk->DtFromCFL(N_s, N_E, CFL, U.data(), upa.data());
+      fprintf(stdout, "DGREF_DT %d %.17g\n", s, Dt);
       blasCopy(N_F * N_s * N_E, U.data(), 1, Us.data(), 1);
       for (int k = 0; k < 4; ++k) {
         blasCopy(N_F * N_s * N_E, Us.data(), 1, Ustar.data(), 1);
@@ -224,6 +225,7 @@ __wrap__ZN2RK14RK_integrationEdiiiiiiiPdS0_R8LimitingbR9DG_SOLVERR12COMMUNICATOR
     std::vector<double> upa((size_t)N_s * N_E);
     for (int s = 0; s < a.nsteps; ++s) {
       const double Dt = a.dt > 0 ? a.dt : rk->DtFromCFL(N_s, N_E, CFL, U.data(), upa.data());
+      fprintf(stdout, "DGREF_DT %d %.17g\n", s, Dt);
       Un = U;
       // stage 1: U1 = Un + dt L(Un)
       dg->dg_solver(U.data(), f.data());

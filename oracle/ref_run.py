@@ -65,9 +65,9 @@ class RefCase:
             self.workdir = Path(self._tmp.name)
         self.workdir = Path(self.workdir)
         self.workdir.mkdir(parents=True, exist_ok=True)
-        from dg_b200.solver import write_msh  # the mesh file is an input to both codes
-        write_msh(self.workdir / "mesh.msh", self.dim, self.order, self.nx, self.ny, self.x0, self.x1,
-                  self.y0, self.y1, self.bc)
+        from oracle.workload import structured_msh  # the mesh file is an input to both codes
+        structured_msh(self.workdir / "mesh.msh", self.dim, self.order, self.nx, self.ny, self.x0, self.x1,
+                       self.y0, self.y1, self.bc)
         self.write_deck()
 
     def write_deck(self, cfl: float | None = None, output_times=None) -> Path:

@@ -285,6 +285,41 @@ def make_cons_fixture() -> dict:
     return out
 
 
+# the 2D shock-bubble workloads run by the reference itself for 100 SSP-RK3 steps with the CFL
+# step (CFL 0.3), [0, 2] x [0, 1], reflective bottom / top, transmissive left / right: the benchmark
+# workload (512 x 256, p = 2, Rusanov, m2l) and the p = 3 Roe form at 256 x 128.  Stored: the
+# reference's step sizes, the cell means of density and energy at the end, and the nodal density
+# of a band of element rows through the bubble (the full state is 47 / 38 MB).
+FULL = [
+    dict(name="run_d2_bubble_p2_rus_m2l_512x256", order=2, nx=512, ny=256, flux="rusanov", limiter="m2l",
+         cfl=0.3, seed=7, steps=100, band=(120, 136)),
+    dict(name="run_d2_bubble_p3_roe_m2l_256x128", order=3, nx=256, ny=128, flux="roe", limiter="m2l",
+         cfl=0.3, seed=7, steps=100, band=(56, 72)),
+]
+WALLS = ("reflective", "transmissive", "reflective", "transmissive")
+
+
+def make_full_run(c: dict) -> dict:
+    from oracle.workload import shock_bubble
+    ref = RefCase(2, c["order"], c["nx"], c["ny"], 0.0, 2.0, 0.0, 1.0, WALLS, c["flux"], c["limiter"], cfl=c["cfl"])
+    ref.write_deck()
+    U0 = ref.limit(shock_bubble(c["order"], c["nx"], c["ny"], seed=c["seed"]))
+    U, log = ref.run("rk3", U0, dt=0.0, nsteps=c["steps"], timeout=7200)
+    dts = [float(l.split()[2]) for l in log.splitlines() if l.startswith("DGREF_DT")]
+    if len(dts) != c["steps"] or not np.all(np.isfinite(U)):
+        raise RuntimeError(f"{c['name']}: reference run incomplete")
+    prob = dgb.Problem.structured(2, c["order"], c["nx"], c["ny"], 0.0, 2.0, 0.0, 1.0, WALLS, flux=c["flux"],
+                                  limiter=c["limiter"], cfl=c["cfl"])
+    i = prob.info
+    w = prob.array("phi_w").reshape(i.n_s, i.n_g).sum(axis=1) / 4.0
+    V = U.reshape(i.n_elem, i.n_fields, i.n_s)
+    r0, r1 = c["band"]
+    return {"dt": np.array(dts), "rho_mean": V[:, 0, :] @ w, "E_mean": V[:, 3, :] @ w,
+            "rho_band": V[r0 * c["nx"]:r1 * c["nx"], 0, :].copy(),
+            "wall_s": np.array([float(log.split("DGREF_WALL_S")[1].split()[0])]),
+            "meta": np.array(json.dumps({**c, "bc": list(WALLS), "dom": [0, 2, 0, 1], "t_final": float(sum(dts))}))}
+
+
 def main(argv=None) -> int:
     only = set((argv if argv is not None else sys.argv[1:]))
     if ERRCASE["name"] in only:
@@ -293,6 +328,10 @@ def main(argv=None) -> int:
     if CONSCASE["name"] in only:
         np.savez_compressed(OUT / f"{CONSCASE['name']}.npz", **make_cons_fixture())
         print(f"wrote {CONSCASE['name']}.npz")
+    for c in FULL:
+        if c["name"] in only:
+            np.savez_compressed(OUT / f"{c['name']}.npz", **make_full_run(c))
+            print(f"wrote {c['name']}.npz")
     if only:  # regenerate the named fixtures only
         for k, c in enumerate(CASES):
             if c["name"] in only:

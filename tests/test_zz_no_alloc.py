@@ -4,7 +4,9 @@ dgb_limit_noalloc serves callers that own their device buffers and cannot alloca
 themselves, so they cannot create a context with dgb_create.  It keeps its temporaries in a fixed
 library-owned device array instead.  Here it must reproduce dgb_limit (the context path) on two
 calls in a row -- the second call reuses the array the first one left behind -- within the parity
-tolerance of the other GPU tests (1e-12 relative), and reject a problem larger than its array.
+tolerance of the other GPU tests (1e-12 relative), take no device memory while it runs, and reject
+a problem larger than its array.  The cases cover the tiled limiter passes (row-major grids, odd
+nx included), the generic passes (a grid whose elements are stored in a shuffled order) and 1D.
 This file is collected last so a failure here comes after every other test has run.
 """
 import ctypes as C
@@ -16,6 +18,8 @@ from conftest import rel_err
 
 pytestmark = pytest.mark.gpu
 
+WALLS = ("reflective", "transmissive", "reflective", "transmissive")
+
 
 def _noalloc(prob, U_in, U_out, stream=0):
     from dg_b200 import _ffi
@@ -23,17 +27,44 @@ def _noalloc(prob, U_in, U_out, stream=0):
                                         C.c_void_p(stream))
 
 
-@pytest.mark.parametrize("dim,order,nx,ny,limiter,bc", [
-    (2, 2, 64, 32, "m2l", ("reflective", "transmissive", "reflective", "transmissive")),
-    (2, 1, 48, 20, "hrl", ("periodic",) * 4),
-    (1, 2, 300, 1, "m2l", ("transmissive",) * 2),
-])
-def test_noalloc_limiter_matches_context_limiter(dim, order, nx, ny, limiter, bc):
+def shuffled_problem(tmp_path, order, nx, ny, limiter):
+    """A 2D grid read from a Gmsh file whose quadrilaterals are listed in a seeded random order, so
+    that the element order is not row-major (the generic limiter passes run)."""
+    import dg_b200 as dgb
+    from oracle.workload import structured_msh
+    structured_msh(tmp_path / "grid.msh", 2, order, nx, ny, 0.0, 2.0, 0.0, 1.0, WALLS)
+    lines = (tmp_path / "grid.msh").read_text().splitlines()
+    a, b = lines.index("$Elements") + 2 + 2 * nx + 2 * ny, lines.index("$EndElements")
+    quads = lines[a:b]
+    order_idx = np.random.default_rng(3).permutation(len(quads))
+    lines[a:b] = [quads[k] for k in order_idx]
+    (tmp_path / "mesh.msh").write_text("\n".join(lines) + "\n")
+    (tmp_path / "deck.inp").write_text("\n".join([
+        "#Code options", "#time integration", "rk4", "#output time array", "0.0 0.001", "#final time", "0.001",
+        "#Courant-Friedrichs-Lewy condition", "0.3", "#order", str(order), "#mesh file", "mesh.msh", "qua",
+        "#limiter", limiter, "#initial condition", "sodcirc"]) + "\n")
+    return dgb.Problem.from_deck(tmp_path / "deck.inp")
+
+
+CASES = [
+    (2, 2, 64, 32, "m2l", WALLS, False),
+    (2, 1, 48, 20, "hrl", ("periodic",) * 4, False),
+    (2, 2, 65, 20, "m2l", WALLS, False),          # odd nx
+    (2, 2, 24, 12, "m2l", WALLS, True),           # shuffled element order: not row-major
+    (1, 2, 300, 1, "m2l", ("transmissive",) * 2, False),
+]
+
+
+@pytest.mark.parametrize("dim,order,nx,ny,limiter,bc,shuffled", CASES)
+def test_noalloc_limiter_matches_context_limiter(tmp_path, dim, order, nx, ny, limiter, bc, shuffled):
     import torch
     import dg_b200 as dgb
     from dg_b200 import _ffi
-    prob = dgb.Problem.structured(dim, order, nx, ny, 0.0, 2.0 if dim == 2 else 1.0, 0.0, 1.0, bc,
-                                  flux="rusanov", limiter=limiter, cfl=0.3)
+    if shuffled:
+        prob = shuffled_problem(tmp_path, order, nx, ny, limiter)
+    else:
+        prob = dgb.Problem.structured(dim, order, nx, ny, 0.0, 2.0 if dim == 2 else 1.0, 0.0, 1.0, bc,
+                                      flux="rusanov", limiter=limiter, cfl=0.3)
     ic = "shock_bubble" if dim == 2 else "tube_noise"
     solver = dgb.DGSolver(prob)
     for call in range(2):
@@ -53,6 +84,34 @@ def test_noalloc_limiter_matches_context_limiter(dim, order, nx, ny, limiter, bc
     torch.cuda.synchronize()
     assert rel_err(U_dev.cpu().numpy(), expect) < 1e-12
     solver.close()
+
+
+def test_noalloc_limiter_takes_no_device_memory():
+    """Free device memory (cudaMemGetInfo) is the same before and after two calls, once the first
+    call on the device has looked up the library's array; torch's allocator is untouched.  The
+    device is shared with other processes, so the comparison is repeated a few times and one
+    undisturbed repetition must show no change."""
+    import torch
+    import dg_b200 as dgb
+    from dg_b200 import _ffi
+    prob = dgb.Problem.structured(2, 2, 64, 32, 0.0, 2.0, 0.0, 1.0, WALLS, flux="rusanov", limiter="m2l", cfl=0.3)
+    U_dev = torch.from_numpy(prob.init_state("shock_bubble", seed=3)).cuda()
+    out = torch.empty_like(U_dev)
+    assert _noalloc(prob, U_dev, out) == _ffi.OK  # device set-up of the first call
+    torch.cuda.synchronize()
+    alloc0, reserved0 = torch.cuda.memory_allocated(), torch.cuda.memory_reserved()
+    same = False
+    for _ in range(5):
+        free0, _total = torch.cuda.mem_get_info()
+        for _ in range(2):
+            assert _noalloc(prob, U_dev, out) == _ffi.OK
+        torch.cuda.synchronize()
+        free1, _total = torch.cuda.mem_get_info()
+        if free1 == free0:
+            same = True
+            break
+    assert same, "free device memory changed across dgb_limit_noalloc calls"
+    assert (torch.cuda.memory_allocated(), torch.cuda.memory_reserved()) == (alloc0, reserved0)
 
 
 def test_noalloc_limiter_rejects_problems_larger_than_its_scratch():
