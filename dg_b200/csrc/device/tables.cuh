@@ -51,19 +51,6 @@ static Tab2<P> make_tab2(const Consts& c) {
   invert(M, N1);
   for (int i = 0; i < N1; ++i)
     for (int j = 0; j < N1; ++j) T.M1i[i][j] = M[i + (size_t)j * N1];
-  for (int i = 0; i < N1; ++i) {
-    for (int g = 0; g < NG1; ++g) {
-      double b = 0, d = 0;
-      for (int j = 0; j < N1; ++j) { b += T.M1i[i][j] * T.B1[g][j]; d += T.M1i[i][j] * T.D1[g][j]; }
-      T.Bt[g][i] = b;
-      T.Dt[g][i] = d;
-    }
-    for (int g = 0; g < N1; ++g) {
-      double b = 0;
-      for (int j = 0; j < N1; ++j) b += T.M1i[i][j] * T.Bf[g][j];
-      T.Bft[g][i] = b;
-    }
-  }
   return T;
 }
 

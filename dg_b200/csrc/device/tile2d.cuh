@@ -34,9 +34,6 @@ struct Tab2 {
   double B1[NG1][N1];   // l_i(x_g) on the p+2 volume Gauss points (1D factor)
   double D1[NG1][N1];   // l_i'(x_g)
   double W1[NG1];       // 1D volume weights
-  // the 1D inverse mass matrix folded into the lift factors: Bt[g][i] = sum_j M1i[i][j] B1[g][j],
-  // Dt[g][i] = sum_j M1i[i][j] D1[g][j], Bft[g][i] = sum_j M1i[i][j] Bf[g][j]
-  double Bt[NG1][N1], Dt[NG1][N1], Bft[N1][N1];
 };
 
 static __constant__ Tab2<1> c_tab2_p1;
