@@ -545,11 +545,11 @@ def mass_fraction(dgb, dev, base_ms, steps=20, warmup=3):
 
 def slab_local(dgb, dev, steps=10, warmup=3):
     """The benchmark workload as 2 and 4 y-slabs (2 ghost rows a side), every slab a context in
-    this process on one GPU, ghost rows refreshed before every stage by device copies with the
-    slabs' streams synchronised around each exchange, the CFL wave speed max-reduced over the
-    slabs.  Wall time per step (host synchronisation is part of this transport), against the
-    whole grid's device time per step, and the max distance of the owned rows from the whole grid
-    after the same steps."""
+    this process on one GPU, ghost rows refreshed before every stage by device copies ordered by
+    events between the slabs' streams, the CFL wave speed max-reduced over the slabs on the device.
+    Wall time per step (the per-step status check synchronises the host), against the whole grid's
+    device time per step, and the max distance of the owned rows from the whole grid after the same
+    steps."""
     import time
     import torch
     from dg_b200 import slab as S
@@ -582,6 +582,86 @@ def slab_local(dgb, dev, steps=10, warmup=3):
         out[f"slabs_{ns}"] = {"rows": [r1 - r0 for r0, r1 in dec.ranges], "ms_per_step_wall": wall,
                               "max_abs_diff_vs_whole": float(np.abs(got - ref).max())}
     return out
+
+
+def free_port() -> int:
+    import socket
+    with socket.socket(socket.AF_INET, socket.SOCK_STREAM) as s:
+        s.bind(("127.0.0.1", 0))
+        return s.getsockname()[1]
+
+
+def run_slab(args, dgb, ws, rank, dev):
+    """--slab: one grid over all ranks.  The shock-bubble grid is 512 x (256 * ranks) elements on
+    [0, 2] x [0, ranks] (weak scaling: every rank owns the element count of the 512 x 256 workload),
+    split into one y-slab per rank with 2 ghost rows a side (dg_b200.slab.DistTransport): the ghost
+    rows cross between neighbour ranks by NCCL send/receive on the context's stream before every
+    stage, the CFL wave speed is MAX-all-reduced on the device, and the step's status once per step.
+    One rank runs the same code in a single-rank group.  Device time per step: CUDA events on the
+    slab's stream from the step's first to its last launch, summed over the timed steps, max over
+    ranks."""
+    import torch
+    import torch.distributed as dist
+    from dg_b200 import slab as S
+    if not dist.is_initialized():
+        dist.init_process_group("nccl", init_method=f"tcp://127.0.0.1:{free_port()}", rank=0, world_size=1,
+                                timeout=__import__("datetime").timedelta(seconds=120))
+    x0, x1, y0, y1 = DOMAIN
+    nyg = NY * ws
+    dec = S.Decomposition(ORDER, NX, nyg, ws, x0, x1, y0, y1 * ws, BC, flux="rusanov", limiter="m2l", cfl=CFL)
+    gprob = dec.global_problem()
+    g = dgb.DGSolver(gprob, device=dev)  # the initial limiting of the whole grid (rk.cc:108-114)
+    U0 = g.limit(gprob.init_state("shock_bubble", seed=SEED))
+    g.close()
+    run = S.SlabRun(dec, [rank], S.DistTransport(), device=dev)
+    (slab,) = run.slabs
+    run.set_global_state(U0)
+    dof = gprob.info.n_elem * gprob.info.n_s * gprob.info.n_fields
+    run.advance(max(args.warmup, 3), 0.0, scheme=dgb.SSPRK3)
+    torch.cuda.synchronize(dev)
+    dist.barrier()
+    dev_ms, launches = 0.0, 0
+    with Clocks(dev) as clk:
+        for _ in range(args.steps):
+            run.advance(1, 0.0, scheme=dgb.SSPRK3)
+            ms, n = slab.solver.last_timing()
+            dev_ms += ms
+            launches += n
+        torch.cuda.synchronize(dev)
+    dist.barrier()
+    clocks = clk.summary()
+    t_s = max_over_ranks(dev_ms / 1e3, ws, f"cuda:{dev}")
+    value = dof * STAGES_PER_STEP * args.steps / t_s
+    # end to end: every step the rank's slab from host memory, one step, its owned rows back
+    e2e_steps = max(args.e2e_steps, 1)
+    n_slab = slab.problem.state_size
+    n_owned = slab.owned().size
+    t0 = time.perf_counter()
+    for _ in range(e2e_steps):
+        run.set_global_state(U0)
+        run.advance(1, 0.0, scheme=dgb.SSPRK3)
+        slab.owned()
+    e2e_s = max_over_ranks(time.perf_counter() - t0, ws, f"cuda:{dev}")
+    run.close()
+    if rank == 0:
+        line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": 1e3 * t_s / args.steps, "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+                "config": config({"workload": f"2D shock-bubble {NX}x{nyg} quads on [0,2]x[0,{ws}] as {ws} y-slabs "
+                                              f"(2 ghost rows a side), p=2, Rusanov, m2l, SSP-RK3, CFL 0.3",
+                                  "n_elem": gprob.info.n_elem, "dof": dof,
+                                  "parallelism": f"slab{ws}: one y-slab per rank, ghost rows by NCCL send/recv "
+                                                 f"before every stage, wave speed MAX all-reduce per step",
+                                  "l2": "not flushed (state per rank 48 MB, streamed 3x per step)"}),
+                "e2e": {"value": dof * STAGES_PER_STEP * e2e_steps / e2e_s, "unit": UNIT,
+                        "h2d_bytes_per_step": ws * n_slab * 8, "d2h_bytes_per_step": ws * n_owned * 8,
+                        "steps": e2e_steps},
+                "clocks": clocks, "gpu_launches": launches,
+                "slab_rows": [r1 - r0 for r0, r1 in dec.ranges]}
+        print(json.dumps(line))
+    dist.barrier()
+    dist.destroy_process_group()
+    return 0
 
 
 def gamma_models(dgb, dev, steps=20, warmup=3):
@@ -753,6 +833,8 @@ def main(argv=None) -> int:
     ap.add_argument("--p3-only", action="store_true", help="print only the 2048x1024 p=3 FP64 / mixed comparison")
     ap.add_argument("--slab-only", action="store_true",
                     help="print only the one-GPU slab-mode line (512x256 as 2 and 4 slabs)")
+    ap.add_argument("--slab", action="store_true",
+                    help="one grid over all ranks as y-slabs with NCCL halo exchange (weak scaling)")
     ap.add_argument("--models-only", action="store_true",
                     help="print only the mass-fraction and gamma-model lines (512x256, p=2)")
     args = ap.parse_args(argv)
@@ -769,6 +851,8 @@ def main(argv=None) -> int:
         dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=120))
     torch.cuda.set_device(local)
     dev = local
+    if args.slab:
+        return run_slab(args, dgb, ws, rank, dev)
 
     if args.profile_case:
         return profile_case(dgb, dev, args.profile_case)

@@ -161,46 +161,74 @@ class Slab:
             __cuda_array_interface__ = {"shape": (1,), "typestr": "<i8", "data": (ptr, False), "version": 2}
         return torch.as_tensor(_Word(), device=self.device)
 
+    def torch_stream(self):
+        """The context's CUDA stream as a torch stream object."""
+        import torch
+        if getattr(self, "_ts", None) is None:
+            self._ts = torch.cuda.ExternalStream(self.solver.stream(), device=self.device)
+        return self._ts
+
     def stream(self):
         import torch
-        return torch.cuda.stream(torch.cuda.ExternalStream(self.solver.stream(), device=self.device))
+        return torch.cuda.stream(self.torch_stream())
+
+    def record(self):
+        """An event recorded on the context's stream now."""
+        import torch
+        ev = torch.cuda.Event()
+        ev.record(self.torch_stream())
+        return ev
+
+    def wait(self, ev) -> None:
+        """Later work on the context's stream waits for `ev` (no host synchronisation)."""
+        self.torch_stream().wait_event(ev)
 
     def synchronize(self) -> None:
-        import torch
-        torch.cuda.ExternalStream(self.solver.stream(), device=self.device).synchronize()
+        self.torch_stream().synchronize()
 
 
 class LocalTransport:
-    """Every slab in this process (one device): rows move by device-to-device copies, with the
-    slabs' streams synchronised around each exchange."""
+    """Every slab in this process (one device): rows move by device-to-device copies ordered by
+    CUDA events between the slabs' streams -- a slab unpacks after its neighbours have packed, and
+    packs again only after its neighbours have unpacked -- with no host synchronisation."""
 
     def exchange(self, run: "SlabRun") -> None:
+        packed = {}
         for s in run.slabs:
-            s.synchronize()
             for side, g in ((0, s.lo), (1, s.hi)):
                 if g:
                     s.pack(side)
-        for s in run.slabs:
-            s.synchronize()
+            packed[s.index] = s.record()
         by_index = {s.index: s for s in run.slabs}
+        unpacked = {}
         for s in run.slabs:
             below, above = neighbours(s.index, run.dec.nslabs, run.dec.periodic)
+            for nb in {below, above} - {None}:
+                s.wait(packed[nb])
             if below is not None:
                 s.unpack(0, by_index[below].send[1])  # the owned top rows of the slab below
             if above is not None:
                 s.unpack(1, by_index[above].send[0])
-        for s in run.slabs:
-            s.synchronize()
+            unpacked[s.index] = s.record()
+        for s in run.slabs:  # send buffers are rewritten by the next pack
+            below, above = neighbours(s.index, run.dec.nslabs, run.dec.periodic)
+            for nb in {below, above} - {None}:
+                s.wait(unpacked[nb])
 
     def reduce_umax(self, run: "SlabRun") -> None:
-        for s in run.slabs:
-            s.synchronize()
-        words = [s.umax() for s in run.slabs]
-        m = max(int(w.item()) for w in words)
-        for w in words:
-            w.fill_(m)
+        """MAX of the slabs' wave-speed words on the device, written back to every word."""
         import torch
-        torch.cuda.synchronize(run.slabs[0].device)
+        first = run.slabs[0]
+        for s in run.slabs[1:]:
+            first.wait(s.record())
+        with first.stream():
+            words = [s.umax() for s in run.slabs]
+            m = torch.stack(words).max(dim=0).values
+            for w in words:
+                w.copy_(m)
+        done = first.record()
+        for s in run.slabs[1:]:
+            s.wait(done)
 
     def reduce_status(self, run: "SlabRun", code: int) -> int:
         return code
