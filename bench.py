@@ -64,6 +64,10 @@ CFL = 0.3
 SEED = 7
 STAGES_PER_STEP = 3
 BYTES_PER_DOF_STAGE = (16.0 + 24.0 + 24.0) / 3.0  # SSP-RK3 Shu-Osher, fully fused stages
+# the learned indicator scores every IND_EVERY-th step: a discontinuity moves at most CFL/(2p+1) =
+# 0.06 of an element per step here, so the band (flagged cells and their face neighbours) of one
+# scoring covers it for half of the 16 steps it could
+IND_EVERY = 8
 
 
 def config(extra=None):
@@ -282,7 +286,7 @@ def compare_forms(dgb, U0_coarse, dev, steps, warmup, flush, acc_steps=200):
         s = dgb.DGSolver(prob, device=dev)
         s.set_form(form)
         if learned:
-            L.set_indicator(s, params, 0.2)
+            L.set_indicator(s, params, 0.2, every=IND_EVERY)
         s.set_state(U0_coarse)
         ms, n = time_steps(dgb, s, steps, warmup, flush)
         dof = prob.info.n_elem * prob.info.n_s * prob.info.n_fields
@@ -339,8 +343,8 @@ def compare_forms(dgb, U0_coarse, dev, steps, warmup, flush, acc_steps=200):
                 for f in range(i.n_fields)]
     out["protocol"] = (f"{steps} timed SSP-RK3 steps each (L2 flushed); accuracy: {acc_steps} steps of dt = 0.8 x "
                        f"the initial CFL step, truth = plain FP64 on 1024x512 with dt/2, cell-averaged onto "
-                       f"512x256; learned threshold 0.2, network {meta.get('samples')} samples, held-out recall "
-                       f"{meta.get('held_out', {}).get('0.2', {}).get('recall')}")
+                       f"512x256; learned threshold 0.2, scored every {IND_EVERY} steps, network {meta.get('samples')} "
+                       f"samples, held-out recall {meta.get('held_out', {}).get('0.2', {}).get('recall')}")
     return out
 
 
@@ -477,8 +481,8 @@ def learned_deploy(dgb, dev, timed=20, warmup=3, steps=DEPLOY_STEPS):
     """The learned indicator on its deployment problem: a seeded four-quadrant Riemann problem on
     1024 x 1024 quads, p = 2, Rusanov, m2l, SSP-RK3, CFL 0.3 (states as in the training set, a
     problem outside it).  Plain FP64 with the full limiter, mixed with the full limiter and mixed
-    with the indicator-gated limiter (threshold 0.2, band of face neighbours, scored once per
-    step): device time per step, and after `steps` fixed steps the L1 density distance of each
+    with the indicator-gated limiter (threshold 0.2, band of face neighbours, scored every
+    IND_EVERY steps): device time per step, and after `steps` fixed steps the L1 density distance of each
     run from the plain FP64 full-limiter run (the judge) and the flagged / band fractions."""
     from dg_b200 import learned as L
     params, _ = L.load()
@@ -496,7 +500,7 @@ def learned_deploy(dgb, dev, timed=20, warmup=3, steps=DEPLOY_STEPS):
             U0 = s.limit(prob.init_state("quadrants", seed=DEPLOY_SEED))
             dt = 0.8 * s.dt_from_cfl(U0)
         if learned:
-            L.set_indicator(s, params, 0.2)
+            L.set_indicator(s, params, 0.2, every=IND_EVERY)
         s.set_state(U0)
         s.advance(warmup, 0.0, scheme=dgb.SSPRK3)
         s.advance(timed, 0.0, scheme=dgb.SSPRK3)
@@ -749,17 +753,28 @@ def mixed_p3(dgb, dev, steps=P3_STEPS, timed=10):
     return out
 
 
-PROFILE_CASES = ("p2step", "p2mixed", "p3fp64", "p3mixed", "batch", "indicator")
+PROFILE_CASES = ("p2step", "p2mixed", "p2learned", "p3fp64", "p3mixed", "batch", "indicator")
 
 
 def profile_case(dgb, dev, name):
     """A small run of one kernel family for an ncu capture (inputs larger than L2, a few launches,
     no timing): p2step -- 3 SSP-RK3 steps of the benchmark workload's problem at 1024 x 512 (p=2,
-    Rusanov, m2l, FP64; 189 MB per state array); p2mixed -- the same in the mixed form; p3fp64 / p3mixed -- 2 SSP-RK3 steps of the 1024 x 512 p=3 Roe shock-bubble in the
+    Rusanov, m2l, FP64; 189 MB per state array); p2mixed -- the same in the mixed form; p2learned --
+    9 steps of the 512 x 256 workload in the mixed form with the learned-indicator-gated limiter
+    (scored every IND_EVERY steps); p3fp64 / p3mixed -- 2 SSP-RK3 steps of the 1024 x 512 p=3 Roe shock-bubble in the
     FP64 / mixed form; batch -- 2 batched steps of 8 2D quadrant problems (256^2, p=2) and 8 1D
     Riemann problems (5000 elements, p=2); indicator -- 3 scorings of the 1024 x 512 p=2
     shock-bubble (after 10 steps) by the trained network."""
-    if name in ("p2step", "p2mixed"):
+    if name == "p2learned":
+        from dg_b200 import learned as L
+        prob, U0 = build_problem()
+        s = dgb.DGSolver(prob, device=dev)
+        s.set_form("mixed")
+        L.set_indicator(s, L.load()[0], 0.2, every=IND_EVERY)
+        s.set_state(s.limit(U0))
+        s.advance(9, 0.0, scheme=dgb.SSPRK3)
+        s.close()
+    elif name in ("p2step", "p2mixed"):
         prob, U0 = build_problem(1024, 512)
         s = dgb.DGSolver(prob, device=dev)
         s.set_form("fp64" if name == "p2step" else "mixed")
@@ -799,7 +814,7 @@ def profile_case(dgb, dev, name):
         s.set_state(s.limit(U0))
         s.advance(10, 0.0, scheme=dgb.SSPRK3)
         U = s.get_state()
-        L.set_indicator(s, L.load()[0], 0.2)
+        L.set_indicator(s, L.load()[0], 0.2, every=IND_EVERY)
         for _ in range(3):
             L.scores(s, U)
         s.close()
@@ -887,7 +902,7 @@ def main(argv=None) -> int:
     U0 = solver.limit(U0)  # the reference limits the initial condition when CFL > 0 (rk.cc:108-114)
     if args.learned:
         from dg_b200 import learned as L
-        L.set_indicator(solver, L.load()[0], 0.2)
+        L.set_indicator(solver, L.load()[0], 0.2, every=IND_EVERY)
     solver.set_state(U0)
     dof = prob.info.n_elem * prob.info.n_s * prob.info.n_fields
 
@@ -985,7 +1000,7 @@ def main(argv=None) -> int:
 
     form_cfg = {"form": ("plain FP64" if args.form == "fp64" else
                          "mixed: FP32 contractions/Rusanov flux on FP64 anchors, FP64 pressure, state and update")
-                + (" + learned indicator (threshold 0.2)" if args.learned else "")}
+                + (f" + learned indicator (threshold 0.2, scored every {IND_EVERY} steps)" if args.learned else "")}
     if rank == 0:
         line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": dev_ms / args.steps, "higher_is_better": True,

@@ -32,7 +32,7 @@ EXPORTS = [
     "dgb_batch_autotune", "dgb_batch_set_tuning", "dgb_batch_advance", "dgb_problem_error_norms", "dgb_batch_case_stats",
     "dgb_batch_last_timing", "dgb_slab_ghost_rows", "dgb_step_begin", "dgb_step_wavespeed_word", "dgb_step_stage",
     "dgb_step_end", "dgb_halo_count", "dgb_halo_pack", "dgb_halo_unpack", "dgb_stream", "dgb_set_cfl_scale",
-    "dgb_set_wait_limit",
+    "dgb_set_wait_limit", "dgb_set_indicator_interval",
 ]
 
 
@@ -100,6 +100,7 @@ def lib() -> C.CDLL:
         "dgb_sensors": [vp, dp, C.POINTER(C.c_int)],
         "dgb_set_form": [vp, ip],
         "dgb_set_wait_limit": [vp, C.c_longlong],
+        "dgb_set_indicator_interval": [vp, ip],
         "dgb_cfl_dt": [vp, dp],
         "dgb_indicator_features": [vp, vp],
         "dgb_indicator_labels": [vp, vp],

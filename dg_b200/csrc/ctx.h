@@ -70,8 +70,18 @@ struct dgb_ctx {
   double last_ms = 0.0;
   long long last_launches = 0;
   long long launches_per_step = 0;
-  cudaGraphExec_t graphs[2][2] = {{nullptr, nullptr}, {nullptr, nullptr}};
-  long long graph_launches[2][2] = {{0, 0}, {0, 0}};
+  // captured steps per [scheme: SSP-RK3, RK4][CFL step][the step scores the learned indicator]
+  cudaGraphExec_t graphs[2][2][2] = {};
+  long long graph_launches[2][2][2] = {};
+  int ind_every = 1;       // steps between scorings of the learned indicator (1: every step)
+  long long ind_step = 0;  // steps taken since the last dgb_set_state / dgb_set_indicator
+  // destroys the captured steps (their kernel arguments or launch sequence changed)
+  void drop_graphs() {
+    for (auto& a : graphs)
+      for (auto& b : a)
+        for (auto& g : b)
+          if (g) { cudaGraphExecDestroy(g); g = nullptr; }
+  }
   // profiling (per kernel class)
   bool prof = false;
   std::vector<std::pair<int, std::pair<cudaEvent_t, cudaEvent_t>>> pev;

@@ -47,6 +47,61 @@ struct GateSparse {
   const double* alt = nullptr;
 };
 
+// The m2 limiter of one slice of one element for the sensor-gated limiters (M2Ilimiting,
+// limiting.cc:661-690, m2i1D limiting_kernels.cu:431-722): pressure recomputed from this pass's
+// input state, rho, alpha, p and the momenta limited (the wall-normal momentum of this pass left
+// as it is at a wall), total energy rebuilt from the limited p, alpha and kinetic energy.
+// c, l, r: the element's and its neighbours' nodal values [field][node] (l, r read only when
+// phys == 0).
+template <int D, int P, int PASS>
+__device__ __forceinline__ void m2i_slice(int phys, const double (&c)[D + 3][P + 1], const double (&l)[D + 3][P + 1],
+                                          const double (&r)[D + 3][P + 1], double (&res)[D + 3][P + 1]) {
+  constexpr int N1 = P + 1, IE = D + 1, IA = D + 2;
+  constexpr int UN = (D == 2 && PASS == 1) ? 2 : 1;  // wall-normal momentum of this pass
+  // nodal pressure of the three cells (pressure, limiting_kernels.cu:1870-1897)
+  double pc[N1], pl[N1], pr[N1];
+  auto press = [&](const double (*v)[N1], double* p) {
+#pragma unroll
+    for (int k = 0; k < N1; ++k) {
+      const double kin = v[1][k] * v[1][k] + (D == 2 ? v[2][k] * v[2][k] : 0.0);
+      p[k] = (v[IE][k] - 0.5 * kin * __drcp_rn(v[0][k])) * __drcp_rn(v[IA][k]);  // reciprocals for divisions
+    }
+  };
+  press(c, pc);
+  if (phys == 0) {
+    press(l, pl);
+    press(r, pr);
+  }
+  double mr[N1], ma[N1], mp[N1];
+  limit_slice<P>(phys, l[0], c[0], r[0], mr);
+  limit_slice<P>(phys, l[IA], c[IA], r[IA], ma);
+  limit_slice<P>(phys, pl, pc, pr, mp);
+  to_lag<P>(mr, res[0]);
+  to_lag<P>(ma, res[IA]);
+#pragma unroll
+  for (int f = 1; f <= D; ++f) {
+    if (phys == 3 && f == UN) {
+#pragma unroll
+      for (int k = 0; k < N1; ++k) res[f][k] = c[f][k];
+    } else {
+      double mm[N1];
+      limit_slice<P>(phys, l[f], c[f], r[f], mm);
+      to_lag<P>(mm, res[f]);
+    }
+  }
+  // total energy from the limited pressure, 1/(gamma-1) and kinetic energy
+  double K[N1], Km[N1], Em[N1], El[N1];
+#pragma unroll
+  for (int k = 0; k < N1; ++k) {
+    const double kin = res[1][k] * res[1][k] + (D == 2 ? res[2][k] * res[2][k] : 0.0);
+    K[k] = 0.5 * kin * __drcp_rn(res[0][k]);
+  }
+  to_mono<P>(K, Km);
+  to_mono<P>(c[IE], Em);
+  reconstruct_energy<P>(mp, ma, Km, Em, El);
+  to_lag<P>(El, res[IE]);
+}
+
 // One pass of hri / pri (METHOD 1) or m2i (METHOD 2).  PASS 0: x slices (row iy = blockIdx.y,
 // neighbours left/right); PASS 1: y slices (column ix = blockIdx.y, neighbours bottom/top); 1D: the
 // element is the slice.  IN_PRIM converts loaded values to primitive variables, OUT_CONS converts
@@ -123,50 +178,88 @@ __global__ void __launch_bounds__(128) lim_gated_kernel(const LimArgs la, const 
       to_lag<P>(lim, res[f]);
     }
   } else {
-    // nodal pressure of the three cells (pressure, limiting_kernels.cu:1870-1897)
-    double pc[N1], pl[N1], pr[N1];
-    auto press = [&](double (*v)[N1], double* p) {
-#pragma unroll
-      for (int k = 0; k < N1; ++k) {
-        const double kin = v[1][k] * v[1][k] + (D == 2 ? v[2][k] * v[2][k] : 0.0);
-        p[k] = (v[IE][k] - 0.5 * kin * __drcp_rn(v[0][k])) * __drcp_rn(v[IA][k]);  // reciprocals for divisions
-      }
-    };
-    press(c, pc);
-    if (phys == 0) {
-      press(l, pl);
-      press(r, pr);
-    }
-    double mr[N1], ma[N1], mp[N1];
-    limit_slice<P>(phys, l[0], c[0], r[0], mr);
-    limit_slice<P>(phys, l[IA], c[IA], r[IA], ma);
-    limit_slice<P>(phys, pl, pc, pr, mp);
-    to_lag<P>(mr, res[0]);
-    to_lag<P>(ma, res[IA]);
-#pragma unroll
-    for (int f = 1; f <= D; ++f) {
-      if (phys == 3 && f == UN) {
-#pragma unroll
-        for (int k = 0; k < N1; ++k) res[f][k] = c[f][k];
-      } else {
-        double mm[N1];
-        limit_slice<P>(phys, l[f], c[f], r[f], mm);
-        to_lag<P>(mm, res[f]);
-      }
-    }
-    // total energy from the limited pressure, 1/(gamma-1) and kinetic energy
-    double K[N1], Km[N1], Em[N1], El[N1];
-#pragma unroll
-    for (int k = 0; k < N1; ++k) {
-      const double kin = res[1][k] * res[1][k] + (D == 2 ? res[2][k] * res[2][k] : 0.0);
-      K[k] = 0.5 * kin * __drcp_rn(res[0][k]);
-    }
-    to_mono<P>(K, Km);
-    to_mono<P>(c[IE], Em);
-    reconstruct_energy<P>(mp, ma, Km, Em, El);
-    to_lag<P>(El, res[IE]);
+    m2i_slice<D, P, PASS>(phys, c, l, r, res);
   }
   store(res);
+}
+
+// Tiled form of the learned indicator's gated m2 limiter on a structured row-major grid (same
+// arithmetic as the sparse lim_gated_kernel<2, P, 2, PASS, false, false, true>): a CTA covers the
+// tile of the dense tiled limiter pass -- PASS 0: 30 elements of one element row (threads: element
+// slot with the left / right neighbour slots, x slice), PASS 1: 32 x 4 elements (threads: x slot,
+// row slot with the bottom / top neighbour rows) for node column blockIdx.z.  Every slot's slice is
+// loaded once, coalesced, and shared through shared memory; only the band elements (flag[e] != 0)
+// are limited and written, and a CTA whose tile holds no band element leaves after one block vote.
+// PASS 0 reads the raw state U and writes the band's x-limited slices to X; PASS 1 reads X for band
+// elements and U for the others and writes the band's result into U.
+template <int P, int PASS>
+__global__ void __launch_bounds__(PASS == 0 ? 32 * (P + 1) : 32 * 6)
+    lim_gated_tile_kernel(const LimArgs la, int nx, int ny, double* __restrict__ U, double* __restrict__ X,
+                          const int* __restrict__ nbr, const unsigned char* __restrict__ flag,
+                          const DevScalars* __restrict__ scal) {
+  constexpr int N1 = P + 1, NS = N1 * N1, NF = 5, TWI = 30, THI = 4;
+  constexpr int SLOTS = PASS == 0 ? N1 : 6;                  // thread rows: x slices, or row slots
+  __shared__ double V[NF][N1][SLOTS][32];                    // [field][node][thread row][slot]
+  if (scal && scal->flags) return;
+  const int ld = la.ld, tx = threadIdx.x, ty = threadIdx.y;
+  int e = -1;
+  bool interior;
+  int sl;  // the slice this thread's values belong to: x slice (PASS 0) or node column (PASS 1)
+  if (PASS == 0) {
+    const int x0 = blockIdx.x * TWI, ey = blockIdx.y, ex = x0 - 1 + tx;
+    sl = ty;
+    interior = tx >= 1 && tx <= TWI && ex < nx;
+    if (interior) e = ey * nx + ex;
+    else if (tx == 0) e = __ldg(nbr + (size_t)0 * ld + ey * nx + x0);
+    else if (ex - 1 < nx && ex - 1 >= 0) e = __ldg(nbr + (size_t)1 * ld + ey * nx + ex - 1);
+  } else {
+    const int x0 = blockIdx.x * 32, y0 = blockIdx.y * THI, x = x0 + tx, yy = y0 - 1 + ty;
+    sl = blockIdx.z;
+    interior = ty >= 1 && ty <= THI && yy < ny && x < nx;
+    if (x < nx) {
+      if (interior) e = yy * nx + x;
+      else if (ty == 0) e = __ldg(nbr + (size_t)2 * ld + y0 * nx + x);
+      else if (yy - 1 < ny && yy - 1 >= 0) e = __ldg(nbr + (size_t)3 * ld + (yy - 1) * nx + x);
+    }
+  }
+  const bool mine = interior && __ldg(flag + e) != 0;
+  if (!__syncthreads_or(mine)) return;  // no band element in this tile
+  auto node = [&](int k) { return PASS == 0 ? k + N1 * sl : sl + N1 * k; };
+  if (e >= 0) {
+    const double* src = (PASS == 1 && __ldg(flag + e)) ? X : U;
+#pragma unroll
+    for (int f = 0; f < NF; ++f)
+#pragma unroll
+      for (int k = 0; k < N1; ++k) V[f][k][ty][tx] = src[(size_t)(f * NS + node(k)) * ld + e];
+  }
+  __syncthreads();
+  if (!mine) return;
+  const int o = PASS == 0 ? 0 : 2;
+  const int phys = boundary_code(__ldg(nbr + (size_t)o * ld + e), __ldg(nbr + (size_t)(o + 1) * ld + e));
+  double c[NF][N1], l[NF][N1], r[NF][N1], res[NF][N1];
+  const int lx = PASS == 0 ? tx - 1 : tx, ly = PASS == 0 ? ty : ty - 1;
+  const int rx = PASS == 0 ? tx + 1 : tx, ry = PASS == 0 ? ty : ty + 1;
+#pragma unroll
+  for (int f = 0; f < NF; ++f)
+#pragma unroll
+    for (int k = 0; k < N1; ++k) {
+      c[f][k] = V[f][k][ty][tx];
+      l[f][k] = V[f][k][ly][lx];
+      r[f][k] = V[f][k][ry][rx];
+    }
+  double* out = PASS == 0 ? X : U;
+  if (phys == 4) {  // "leave data unchanged"
+#pragma unroll
+    for (int f = 0; f < NF; ++f)
+#pragma unroll
+      for (int k = 0; k < N1; ++k) out[(size_t)(f * NS + node(k)) * ld + e] = c[f][k];
+    return;
+  }
+  m2i_slice<2, P, PASS>(phys, c, l, r, res);
+#pragma unroll
+  for (int f = 0; f < NF; ++f)
+#pragma unroll
+    for (int k = 0; k < N1; ++k) out[(size_t)(f * NS + node(k)) * ld + e] = res[f][k];
 }
 
 // p0i: flagged elements to their cell average sum_t w_t U_t (w from phi_w / |reference element|)

@@ -528,15 +528,25 @@ void launch_indicator(dgb_ctx* c, const double* U) {
   cudaMemsetAsync(c->ind_blist + c->ld, 0, sizeof(int), c->st);
   indicator_band_kernel<<<(c->ne + 255) / 256, 256, 0, c->st>>>(c->ne, c->ld, 4, c->nbr, c->ind_flag, c->ind_band,
                                                                 c->ind_blist, c->ind_blist + c->ld, c->scal);
-  c->counter += 3;
+  c->counter += 2;  // three kernels (the scope counted one)
 }
 
 // learned-indicator-gated m2 limiter (m2i arithmetic on the band only), in place; score = false
-// reuses the band of the last scoring (the time steppers score once per step)
+// reuses the band of the last scoring (the time steppers score every ind_every steps).  Structured
+// row-major grids: the tiled passes, which skip tiles without band elements; otherwise the passes
+// over the band's element list.
 void launch_learned_limiter(dgb_ctx* c, double* U, bool score) {
   if (score) launch_indicator(c, U);
   ProfScope ps(c, KC_LIMITER);
   const LimArgs la{c->ld, c->ne};
+  if (c->rowmajor) {
+    dim3 gx((c->nx + 29) / 30, c->ny), bx(32, 3);
+    lim_gated_tile_kernel<2, 0><<<gx, bx, 0, c->st>>>(la, c->nx, c->ny, U, c->X, c->nbr, c->ind_band, c->scal);
+    dim3 gy((c->nx + 31) / 32, (c->ny + 3) / 4, 3), by(32, 6);
+    lim_gated_tile_kernel<2, 1><<<gy, by, 0, c->st>>>(la, c->nx, c->ny, U, c->X, c->nbr, c->ind_band, c->scal);
+    c->counter += 1;
+    return;
+  }
   GateSparse sp;
   sp.list = c->ind_blist;
   sp.count = c->ind_blist + c->ld;
@@ -766,11 +776,12 @@ int step1d_rk4(dgb_ctx* c, bool cfl) {
   return 0;
 }
 
-// One SSP-RK3 step on c->A; limiter after every stage.
-int step_ssprk3(dgb_ctx* c, bool cfl) {
+// One SSP-RK3 step on c->A; limiter after every stage.  score: the learned indicator (if set)
+// scores the step's initial state (else the band of its last scoring is reused).
+int step_ssprk3(dgb_ctx* c, bool cfl, bool score = true) {
   if (lim1d_direct(c)) return step1d_ssprk3(c, cfl);
   launch_dt(c, c->A, cfl);
-  if (c->ind_on) launch_indicator(c, c->A);  // the learned indicator's band, once per step
+  if (c->ind_on && score) launch_indicator(c, c->A);  // the learned indicator's band
   for (int s = 0; s < 3; ++s)
     if (int rc = ssp_stage(c, s)) return rc;
   return 0;
@@ -798,11 +809,11 @@ int rk4_stage(dgb_ctx* c, int k) {
   return limit_dispatch(c, c->C, false);
 }
 
-// One classical RK4 step.
-int step_rk4(dgb_ctx* c, bool cfl) {
+// One classical RK4 step (score: as step_ssprk3).
+int step_rk4(dgb_ctx* c, bool cfl, bool score = true) {
   if (lim1d_direct(c)) return step1d_rk4(c, cfl);
   launch_dt(c, c->A, cfl);
-  if (c->ind_on) launch_indicator(c, c->A);  // the learned indicator's band, once per step
+  if (c->ind_on && score) launch_indicator(c, c->A);  // the learned indicator's band
   cudaMemcpyAsync(c->B, c->A, c->nstate * sizeof(double), cudaMemcpyDeviceToDevice, c->st);
   for (int k = 0; k < 4; ++k)
     if (int rc = rk4_stage(c, k)) return rc;
@@ -1018,9 +1029,7 @@ extern "C" void dgb_destroy(dgb_ctx* c) {
   if (!c) return;
   cudaSetDevice(c->device);
   if (c->st) cudaStreamSynchronize(c->st);
-  for (auto& row : c->graphs)
-    for (auto& g : row)
-      if (g) cudaGraphExecDestroy(g);
+  c->drop_graphs();
   for (double* b : {c->A, c->B, c->C, c->DU, c->X, c->ref}) if (b) cudaFree(b);
   if (c->nbr) cudaFree(c->nbr);
   if (c->left) cudaFree(c->left);
@@ -1045,6 +1054,7 @@ extern "C" int dgb_set_state(dgb_ctx* c, const double* U) {
   DGB_CUDA(cudaSetDevice(c->device));
   if (int rc = upload(c, U, c->A)) return rc;
   DGB_CUDA(cudaStreamSynchronize(c->st));
+  c->ind_step = 0;  // a new state: the learned indicator scores the next step
   return DGB_OK;
 }
 
@@ -1059,6 +1069,7 @@ extern "C" int dgb_set_state_device(dgb_ctx* c, const double* U_dev) {
   DGB_CUDA(cudaSetDevice(c->device));
   if (int rc = to_internal(c, U_dev, c->A)) return rc;
   DGB_CUDA(cudaStreamSynchronize(c->st));
+  c->ind_step = 0;
   return DGB_OK;
 }
 
@@ -1196,13 +1207,20 @@ extern "C" int dgb_mlp_adam(float* params, const float* grad, float* m, float* v
   return DGB_OK;
 }
 
+extern "C" int dgb_set_indicator_interval(dgb_ctx* c, int steps) {
+  if (!c) return set_error(DGB_ERR_ARG, "null argument");
+  if (steps < 1) return set_error(DGB_ERR_ARG, "the scoring interval is at least one step");
+  c->ind_every = steps;
+  c->ind_step = 0;
+  return DGB_OK;
+}
+
 extern "C" int dgb_set_indicator(dgb_ctx* c, const float* params, float threshold) {
   if (!c) return set_error(DGB_ERR_ARG, "null argument");
   DGB_CUDA(cudaSetDevice(c->device));
   DGB_CUDA(cudaStreamSynchronize(c->st));
-  for (auto& row : c->graphs)
-    for (auto& g : row)
-      if (g) { cudaGraphExecDestroy(g); g = nullptr; }
+  c->drop_graphs();
+  c->ind_step = 0;
   if (!params) {
     c->ind_on = false;
     return DGB_OK;
@@ -1270,9 +1288,7 @@ extern "C" int dgb_set_form(dgb_ctx* c, int form) {
   if (form != c->form) {
     DGB_CUDA(cudaSetDevice(c->device));
     DGB_CUDA(cudaStreamSynchronize(c->st));
-    for (auto& row : c->graphs)
-      for (auto& g : row)
-        if (g) { cudaGraphExecDestroy(g); g = nullptr; }
+    c->drop_graphs();
     c->form = form;
   }
   return DGB_OK;
@@ -1284,9 +1300,7 @@ extern "C" int dgb_set_wait_limit(dgb_ctx* c, long long polls) {
   if (polls != c->wait_polls) {
     DGB_CUDA(cudaSetDevice(c->device));
     DGB_CUDA(cudaStreamSynchronize(c->st));
-    for (auto& row : c->graphs)  // the budget is a kernel argument of the captured launches
-      for (auto& g : row)
-        if (g) { cudaGraphExecDestroy(g); g = nullptr; }
+    c->drop_graphs();  // the budget is a kernel argument of the captured launches
     c->wait_polls = polls;
   }
   return DGB_OK;
@@ -1342,34 +1356,46 @@ extern "C" int dgb_advance(dgb_ctx* c, int scheme, int nsteps, double dt, double
   if (int rc = reset_scalars(c, cfl ? 0.0 : dt)) return rc;
   const int si = scheme == DGB_RK4 ? 1 : 0, mi = cfl ? 1 : 0;
   c->counter = 0;
+  // the learned indicator scores every ind_every-th step (counted from the last state set)
+  auto scores = [c]() { return !c->ind_on || c->ind_every <= 1 || c->ind_step % c->ind_every == 0; };
   if (c->prof) {
     // eager launches with per-kernel-class events
     DGB_CUDA(cudaEventRecord(c->e0, c->st));
     for (int s = 0; s < nsteps; ++s) {
-      int rc = scheme == DGB_RK4 ? step_rk4(c, cfl) : step_ssprk3(c, cfl);
+      const bool sc = scores();
+      int rc = scheme == DGB_RK4 ? step_rk4(c, cfl, sc) : step_ssprk3(c, cfl, sc);
       if (rc) return rc;
+      ++c->ind_step;
     }
     DGB_CUDA(cudaEventRecord(c->e1, c->st));
     DGB_CUDA(cudaGetLastError());
     c->last_launches = c->counter;
     if (int rc = prof_collect(c)) return rc;
   } else {
-    if (!c->graphs[si][mi] && nsteps > 0) {
+    for (int k = 0; k < 2 && nsteps > 0; ++k) {  // the scoring and the non-scoring step, as needed
+      const bool sc = k == 0;
+      if (c->graphs[si][mi][k] || (!sc && (!c->ind_on || c->ind_every <= 1))) continue;
       cudaGraph_t g;
       DGB_CUDA(cudaStreamBeginCapture(c->st, cudaStreamCaptureModeThreadLocal));
       c->counter = 0;
-      int rc = scheme == DGB_RK4 ? step_rk4(c, cfl) : step_ssprk3(c, cfl);
+      int rc = scheme == DGB_RK4 ? step_rk4(c, cfl, sc) : step_ssprk3(c, cfl, sc);
       cudaError_t ec = cudaStreamEndCapture(c->st, &g);
       if (rc) { if (ec == cudaSuccess) cudaGraphDestroy(g); return rc; }
       DGB_CUDA(ec);
-      DGB_CUDA(cudaGraphInstantiate(&c->graphs[si][mi], g, 0));
+      DGB_CUDA(cudaGraphInstantiate(&c->graphs[si][mi][k], g, 0));
       cudaGraphDestroy(g);
-      c->graph_launches[si][mi] = c->counter;
+      c->graph_launches[si][mi][k] = c->counter;
     }
     DGB_CUDA(cudaEventRecord(c->e0, c->st));
-    for (int s = 0; s < nsteps; ++s) DGB_CUDA(cudaGraphLaunch(c->graphs[si][mi], c->st));
+    long long launches = 0;
+    for (int s = 0; s < nsteps; ++s) {
+      const int k = scores() ? 0 : 1;
+      DGB_CUDA(cudaGraphLaunch(c->graphs[si][mi][k], c->st));
+      launches += c->graph_launches[si][mi][k];
+      ++c->ind_step;
+    }
     DGB_CUDA(cudaEventRecord(c->e1, c->st));
-    c->last_launches = c->graph_launches[si][mi] * nsteps;
+    c->last_launches = launches;
   }
   if (int rc = read_scalars(c)) return rc;
   float ms = 0;
@@ -1413,9 +1439,7 @@ extern "C" int dgb_set_cfl_scale(dgb_ctx* c, double cfl_scaled) {
   if (!c) return set_error(DGB_ERR_ARG, "null context");
   if (!std::isfinite(cfl_scaled)) return set_error(DGB_ERR_ARG, "CFL scale must be finite");
   c->cs.cfl_scaled = cfl_scaled;
-  for (auto& row : c->graphs)  // captured steps hold the old value
-    for (auto& g : row)
-      if (g) { cudaGraphExecDestroy(g); g = nullptr; }
+  c->drop_graphs();  // captured steps hold the old value
   return DGB_OK;
 }
 

@@ -168,9 +168,12 @@ def load(path=DEFAULT_WEIGHTS) -> tuple[np.ndarray, dict]:
     return d["params"].astype(np.float32), json.loads(str(d["meta"]))
 
 
-def set_indicator(solver: DGSolver, params: np.ndarray, threshold: float = 0.2) -> None:
+def set_indicator(solver: DGSolver, params: np.ndarray, threshold: float = 0.2, every: int = 1) -> None:
+    """Gate the solver's m2l limiter with the network `params`: elements scoring above `threshold`
+    and their face neighbours are limited; the time stepper scores every `every`-th step."""
     p = np.ascontiguousarray(params, np.float32)
     F.check(F.lib().dgb_set_indicator(solver._h, p.ctypes.data_as(C.c_void_p), C.c_float(threshold)))
+    F.check(F.lib().dgb_set_indicator_interval(solver._h, int(every)))
 
 
 def clear_indicator(solver: DGSolver) -> None:

@@ -292,6 +292,12 @@ int dgb_mlp_adam(float* params_dev, const float* grad_dev, float* m_dev, float* 
  * state (a discontinuity moves well under one element per step at CFL < 1), and on the given
  * state by dgb_limit.  params_host = NULL switches back to the full limiter. */
 int dgb_set_indicator(dgb_ctx* c, const float* params_host, float threshold);
+/* Steps between scorings of the learned indicator in dgb_advance (default 1: every step); the
+ * steps in between reuse the band (flagged elements and their face neighbours) of the last
+ * scoring.  A discontinuity moves at most CFL / (2p + 1) of an element per step, so the band keeps
+ * covering it for up to (2p + 1) / CFL steps (16 at p = 2, CFL 0.3).  Setting a state restarts the
+ * count (the next step scores).  No counterpart in the reference. */
+int dgb_set_indicator_interval(dgb_ctx* c, int steps);
 /* Scores [N_E] of U (reference layout, host) with the indicator set, and the flagged count. */
 int dgb_indicator_scores(dgb_ctx* c, const double* U_host, float* score_host, int* n_flagged);
 

@@ -144,3 +144,36 @@ def test_trained_indicator_gain():
     finally:
         for s in (full, learned, plain):
             s.close()
+
+
+def test_scoring_interval_keeps_the_full_limiter_result():
+    """Scoring every 8th step (the band of the last scoring covers the discontinuities for up to
+    (2p+1)/CFL = 16 steps): still within 1e-4 relative L1 density of the full limiter after 100
+    steps on the shock-bubble, and the steps in between launch the three scoring kernels less."""
+    import dg_b200 as dgb
+    from dg_b200 import learned as L
+    params, _ = L.load()
+    walls = ("reflective", "transmissive", "reflective", "transmissive")
+    prob = dgb.Problem.structured(2, 2, 128, 64, 0.0, 2.0, 0.0, 1.0, walls, flux="rusanov", limiter="m2l", cfl=0.3)
+    full, learned = dgb.DGSolver(prob), dgb.DGSolver(prob)
+    try:
+        U0 = full.limit(prob.init_state("shock_bubble", seed=7))
+        dt = 0.8 * full.dt_from_cfl(U0)
+        L.set_indicator(learned, params, 0.2, every=8)
+        learned.set_state(U0)
+        learned.advance(1, dt)
+        n_score = learned.last_timing()[1]
+        learned.advance(1, dt)
+        n_reuse = learned.last_timing()[1]
+        assert n_reuse == n_score - 3
+        out = {}
+        for name, s in (("full", full), ("learned", learned)):
+            s.set_state(U0)
+            s.advance(100, dt)
+            out[name] = s.get_state()
+        i = prob.info
+        rho = {k: v.reshape(i.n_elem, i.n_fields, i.n_s)[:, 0] for k, v in out.items()}
+        assert float(np.abs(rho["learned"] - rho["full"]).sum() / np.abs(rho["full"]).sum()) < 1e-4
+    finally:
+        full.close()
+        learned.close()
