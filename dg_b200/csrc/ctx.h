@@ -48,7 +48,9 @@ struct dgb_ctx {
   int *nbr = nullptr, *perm = nullptr;
   // sensor-gated limiters (hri, m2i, pri, p0i): sensor work arrays and flags
   bool gated = false, has_sensors = false;
+  int sm_count = 148;           // multiprocessors of the device
   bool ind_on = false;          // learned indicator gates the limiter (dgb_set_indicator)
+  bool ind_tc = true;           // scoring GEMMs on tcgen05 (else the mma.sync kernel)
   float ind_threshold = 0.2f;
   float* ind_params = nullptr;  // FP32 parameters (MLP_NPARAM)
   __nv_bfloat16* ind_w = nullptr;  // W1 [64][IND_KPAD] then W2 [64][64], BF16

@@ -292,6 +292,7 @@ struct IndicatorArgs {
   int* list;                     // flagged elements
   int* count;
   const DevScalars* scal;
+  unsigned int* errflag;         // receives FLAG_TIMEOUT when a bounded wait runs out
 };
 
 // the input compression in FP32 with the hardware base-2 logarithm

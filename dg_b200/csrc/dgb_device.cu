@@ -22,6 +22,7 @@
 #include "device/limiter_gated.cuh"
 #include "device/tile2d_mixed.cuh"
 #include "device/learned.cuh"
+#include "device/learned_tc.cuh"
 #include "device/tables.cuh"
 #include "device/sensor.h"
 #include "host/host.h"
@@ -517,14 +518,26 @@ void launch_indicator(dgb_ctx* c, const double* U) {
   a.n_elem = c->ne; a.ld = c->ld; a.threshold = c->ind_threshold; a.nbr = c->nbr; a.modes = c->ind_modes;
   a.w1 = c->ind_w; a.w2 = c->ind_w + MLP_H * IND_KPAD; a.vec = c->ind_vec;
   a.score = c->ind_score; a.flag = c->ind_flag; a.list = c->ind_list; a.count = c->ind_list + c->ld; a.scal = c->scal;
-  const int ntiles = (c->ne + 15) / 16;
-  const int grid = std::min((ntiles + IND_WARPS - 1) / IND_WARPS, 148 * 2);  // persistent: 2 CTAs per SM
-  static bool attr = false;
-  if (!attr) {
-    cudaFuncSetAttribute(indicator_infer_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)IND_SMEM_BYTES);
-    attr = true;
+  a.errflag = &c->scal->flags;
+  if (c->ind_tc) {
+    // tcgen05 GEMMs on 128-element tiles, persistent: one CTA per SM
+    static bool attr_tc = false;
+    if (!attr_tc) {
+      cudaFuncSetAttribute(indicator_infer_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)TCI_SMEM_BYTES);
+      attr_tc = true;
+    }
+    const int ntiles = (c->ne + TCI_M - 1) / TCI_M;
+    indicator_infer_tc_kernel<<<std::min(ntiles, c->sm_count), TCI_THREADS, TCI_SMEM_BYTES, c->st>>>(a);
+  } else {
+    const int ntiles = (c->ne + 15) / 16;
+    const int grid = std::min((ntiles + IND_WARPS - 1) / IND_WARPS, c->sm_count * 2);  // persistent: 2 CTAs per SM
+    static bool attr = false;
+    if (!attr) {
+      cudaFuncSetAttribute(indicator_infer_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)IND_SMEM_BYTES);
+      attr = true;
+    }
+    indicator_infer_kernel<<<grid, 32 * IND_WARPS, IND_SMEM_BYTES, c->st>>>(a);
   }
-  indicator_infer_kernel<<<grid, 32 * IND_WARPS, IND_SMEM_BYTES, c->st>>>(a);
   cudaMemsetAsync(c->ind_blist + c->ld, 0, sizeof(int), c->st);
   indicator_band_kernel<<<(c->ne + 255) / 256, 256, 0, c->st>>>(c->ne, c->ld, 4, c->nbr, c->ind_flag, c->ind_band,
                                                                 c->ind_blist, c->ind_blist + c->ld, c->scal);
@@ -890,6 +903,12 @@ extern "C" int dgb_create(const dgb_problem* prob, int device, dgb_ctx** out) {
   DGB_CUDA(cudaSetDevice(device));
   auto* c = new dgb_ctx();
   c->device = device;
+  c->sm_count = prop.multiProcessorCount;
+  {
+    // learned-indicator scoring: tcgen05 GEMMs (DGB_INDICATOR_KERNEL=mma: the mma.sync form)
+    const char* ik = std::getenv("DGB_INDICATOR_KERNEL");
+    c->ind_tc = !(ik && std::string(ik) == "mma");
+  }
   c->D = P.D; c->p = P.p; c->nf = P.N_F; c->ns = P.N_s; c->ne = P.N_E;
   c->ld = (P.N_E + 63) / 64 * 64;
   c->flux = P.flux; c->limiter = P.limiter;

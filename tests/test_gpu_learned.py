@@ -177,3 +177,29 @@ def test_scoring_interval_keeps_the_full_limiter_result():
     finally:
         full.close()
         learned.close()
+
+
+def test_tcgen05_scores_match_the_mma_sync_kernel():
+    """The scoring GEMMs on the 5th-generation tensor cores (tcgen05.mma, accumulators in tensor
+    memory) against the warp-level mma.sync kernel: the same BF16 inputs and weights with FP32
+    accumulation in another order, so the scores agree to rounding and the flags almost
+    everywhere."""
+    import os
+    from dg_b200 import learned as L
+    params, _ = L.load()
+    out = {}
+    for kind in ("mma", "tc"):
+        os.environ["DGB_INDICATOR_KERNEL"] = kind
+        try:
+            prob, s = quadrant_state(nx=60, ny=50, seed=13, steps=4)  # 3000 elements: a ragged last tile
+        finally:
+            del os.environ["DGB_INDICATOR_KERNEL"]
+        try:
+            L.set_indicator(s, params, 0.2)
+            out[kind] = L.scores(s, s.get_state())
+        finally:
+            s.close()
+    (sa, ca), (sb, cb) = out["mma"], out["tc"]
+    assert np.abs(sa - sb).max() < 2e-3
+    assert np.mean((sa > 0.2) == (sb > 0.2)) > 0.999
+    assert abs(ca - cb) <= max(2, 0.001 * sa.size)
