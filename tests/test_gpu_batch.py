@@ -168,3 +168,38 @@ def test_batch_rejects_unsupported_cases():
         dgb.DGBatch([s2, s2])
     s.close()
     s2.close()
+
+
+def test_batched_golden_cases_match_the_reference():
+    """Reference golden cases advanced together in batches (1D and tiled 2D classes, p = 1-3,
+    Rusanov / Roe / HLL, m2l / hrl): after the fixture's SSP-RK3 steps with each case's own CFL
+    step, every case equals the reference's run (the harness's Shu-Osher steps over the reference
+    operators, fixture key rk3c) within the parity tests' 1e-10."""
+    import json
+    from pathlib import Path
+    import dg_b200 as dgb
+    from conftest import problem_for, rel_err
+    gold = Path(__file__).resolve().parent / "golden"
+    names = ["d1_p2_roe_m2l", "d1_p1_rus_hrl_wall", "d1_p3_hll_m2l_periodic", "t2_p2_rus_m2l_walls",
+             "t2_p1_roe_hrl_periodic", "t2_p2_roe_m2l_box"]
+    fixtures, solvers = [], []
+    for n in names:
+        d = dict(np.load(gold / f"{n}.npz"))
+        meta = json.loads(str(d.pop("meta")))
+        s = dgb.DGSolver(problem_for(meta))
+        s.set_state(d["U0"])
+        fixtures.append((meta, d))
+        solvers.append(s)
+    try:
+        for nsteps in sorted({m["nsteps"] for m, _ in fixtures}):  # one batch per step count
+            group = [(f, s) for f, s in zip(fixtures, solvers) if f[0]["nsteps"] == nsteps]
+            b = dgb.DGBatch([s for _, s in group])
+            try:
+                b.advance(nsteps, 0.0)
+            finally:
+                b.close()
+            for (meta, d), s in group:
+                assert rel_err(s.get_state(), d["rk3c"]) < 1e-10, meta["name"]
+    finally:
+        for s in solvers:
+            s.close()
