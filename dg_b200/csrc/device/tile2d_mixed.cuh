@@ -61,6 +61,15 @@ __device__ __forceinline__ void rusanov2d_mixed(const double* L, const double* R
   nc = -0.25f * (vnL + vnR) * dal;
 }
 
+// Paired FP32 arithmetic (sm_100 FFMA2 / FMUL2: two independent, correctly rounded FP32 operations
+// per instruction).  The mixed kernel keeps fields (0, 1) and (2, 3) of its contractions in float2
+// pairs (field 4 alone) and multiplies each pair by a broadcast basis coefficient.
+__device__ __forceinline__ float2 bcast2(float v) { return make_float2(v, v); }
+__device__ __forceinline__ float2 fma2(float2 a, float2 b, float2 c) { return __ffma2_rn(a, b, c); }
+__device__ __forceinline__ float2 dev2(double u0, double u1, double a0, double a1) {
+  return make_float2((float)(u0 - a0), (float)(u1 - a1));
+}
+
 template <int P, int FLUX, int MODE, int TW, int TH>
 __global__ void __launch_bounds__(TW * TH, 3)
     residual2d_tile_mixed_kernel(const TileArgs a, const __grid_constant__ CUtensorMap mapU) {
@@ -185,18 +194,16 @@ __global__ void __launch_bounds__(TW * TH, 3)
         }
       if (first_edge) { nxv = -nxv; nyv = -nyv; sgn = -1.0f; }
     }
-    // traces: anchor (face node 0) + FP32 contraction of the deviations
+    // traces: anchor (face node 0) + FP32 contraction of the deviations, left and right paired
     double L[NF], R[NF];
 #pragma unroll
     for (int f = 0; f < NF; ++f) {
-      float sl = 0.f, sr = 0.f;
+      float2 s = make_float2(0.f, 0.f);
 #pragma unroll
-      for (int j = 1; j < N1; ++j) {
-        sl += DGB_TAB2F(P, Bf[g][j]) * (float)(vl[f][j] - vl[f][0]);
-        sr += DGB_TAB2F(P, Bf[g][j]) * (float)(vr[f][j] - vr[f][0]);
-      }
-      L[f] = vl[f][0] + (double)sl;
-      R[f] = vr[f][0] + (double)sr;
+      for (int j = 1; j < N1; ++j)
+        s = fma2(bcast2(DGB_TAB2F(P, Bf[g][j])), dev2(vl[f][j], vr[f][j], vl[f][0], vr[f][0]), s);
+      L[f] = vl[f][0] + (double)s.x;
+      R[f] = vr[f][0] + (double)s.y;
     }
     float F[NF], nc;
     if (FLUX == phys::FLUX_ROE) {
@@ -215,14 +222,14 @@ __global__ void __launch_bounds__(TW * TH, 3)
   __syncthreads();
 
   // ---------------- phase 2: volume terms and assembly, one thread per element ----------------
+  // accumulators: fields (0, 1) and (2, 3) as float2 pairs, field 4 alone
   const int tx = tid % TW, ty = tid / TW;
   const int e = (ty0 + ty) * nx + tx0 + tx;
   constexpr int NG1 = Tab2<P>::NG1;
-  float r[NF][NS];
+  float2 r01[NS], r23[NS];
+  float r4[NS];
 #pragma unroll
-  for (int f = 0; f < NF; ++f)
-#pragma unroll
-    for (int t = 0; t < NS; ++t) r[f][t] = 0.f;
+  for (int t = 0; t < NS; ++t) { r01[t] = r23[t] = make_float2(0.f, 0.f); r4[t] = 0.f; }
 #pragma unroll
   for (int kf = 0; kf < 4; ++kf) {
     int base;
@@ -235,15 +242,15 @@ __global__ void __launch_bounds__(TW * TH, 3)
     for (int g = 0; g < N1; ++g) {
       const float* fp = Fs + (base + g) * 6;
       const float w = jw * DGB_TAB2F(P, wf[g]);
-      float c[NF];
-#pragma unroll
-      for (int f = 0; f < NF; ++f) c[f] = (s * fp[f] + (f == 4 ? fp[5] : 0.f)) * w;
+      const float2 c01 = make_float2(s * fp[0] * w, s * fp[1] * w), c23 = make_float2(s * fp[2] * w, s * fp[3] * w);
+      const float c4 = (s * fp[4] + fp[5]) * w;
 #pragma unroll
       for (int j = 0; j < N1; ++j) {
         const int t = kf == 0 ? N1 * j : kf == 1 ? P + N1 * j : kf == 2 ? j : j + N1 * P;
         const float b = DGB_TAB2F(P, Bf[g][j]);
-#pragma unroll
-        for (int f = 0; f < NF; ++f) r[f][t] += b * c[f];
+        r01[t] = fma2(bcast2(b), c01, r01[t]);
+        r23[t] = fma2(bcast2(b), c23, r23[t]);
+        r4[t] = fmaf(b, c4, r4[t]);
       }
     }
   }
@@ -256,126 +263,143 @@ __global__ void __launch_bounds__(TW * TH, 3)
   const float cx = (float)a.cx, cy = (float)a.cy, cJ = (float)a.J, sx = (float)a.sx, sy = (float)a.sy;
 #pragma unroll 1  // rolled quadrature-column loop (instruction cache), as in the FP64 kernel
   for (int gx = 0; gx < NG1; ++gx) {
-    float Tc[NF][N1], dT[N1];
+    float2 T01[N1], T23[N1];
+    float T4[N1], dT[N1];
 #pragma unroll
     for (int iy = 0; iy < N1; ++iy) {
+      float2 s01 = make_float2(0.f, 0.f), s23 = make_float2(0.f, 0.f);
+      float s4 = 0.f, sd = 0.f;
 #pragma unroll
-      for (int f = 0; f < NF; ++f) {
-        float sacc = 0.f;
-#pragma unroll
-        for (int ix = 0; ix < N1; ++ix)
-          sacc += DGB_TAB2F(P, B1[gx][ix]) * (float)(us[(f * NS + ix + N1 * iy) * NT] - anc[f]);
-        Tc[f][iy] = sacc;
+      for (int ix = 0; ix < N1; ++ix) {
+        const int t = ix + N1 * iy;
+        const float2 b = bcast2(DGB_TAB2F(P, B1[gx][ix]));
+        s01 = fma2(b, dev2(us[(0 * NS + t) * NT], us[(1 * NS + t) * NT], anc[0], anc[1]), s01);
+        s23 = fma2(b, dev2(us[(2 * NS + t) * NT], us[(3 * NS + t) * NT], anc[2], anc[3]), s23);
+        const float d4 = (float)(us[(4 * NS + t) * NT] - anc[4]);
+        s4 = fmaf(b.x, d4, s4);
+        sd = fmaf(DGB_TAB2F(P, D1[gx][ix]), d4, sd);
       }
-      float sd = 0.f;
-#pragma unroll
-      for (int ix = 0; ix < N1; ++ix)
-        sd += DGB_TAB2F(P, D1[gx][ix]) * (float)(us[(4 * NS + ix + N1 * iy) * NT] - anc[4]);
+      T01[iy] = s01;
+      T23[iy] = s23;
+      T4[iy] = s4;
       dT[iy] = sd;
     }
-    float Ax[4][N1], Ay[4][N1], As[N1];
+    float2 Ax01[N1], Ax23[N1], Ay01[N1], Ay23[N1];
+    float As[N1];
 #pragma unroll
     for (int iy = 0; iy < N1; ++iy) {
       As[iy] = 0.f;
-#pragma unroll
-      for (int f = 0; f < 4; ++f) Ax[f][iy] = Ay[f][iy] = 0.f;
+      Ax01[iy] = Ax23[iy] = Ay01[iy] = Ay23[iy] = make_float2(0.f, 0.f);
     }
 #pragma unroll
     for (int gy = 0; gy < NG1; ++gy) {
       const int g = gx * NG1 + gy;
-      double ug[NF];
-      float dax = 0.f, day = 0.f;
-#pragma unroll
-      for (int f = 0; f < NF; ++f) {
-        float sacc = 0.f;
-#pragma unroll
-        for (int iy = 0; iy < N1; ++iy) sacc += DGB_TAB2F(P, B1[gy][iy]) * Tc[f][iy];
-        ug[f] = anc[f] + (double)sacc;
-      }
+      float2 u01 = make_float2(0.f, 0.f), u23 = make_float2(0.f, 0.f);
+      float u4 = 0.f;
+      float2 dd = make_float2(0.f, 0.f);  // (d alpha / dx, d alpha / dy) on the reference element
 #pragma unroll
       for (int iy = 0; iy < N1; ++iy) {
-        dax += DGB_TAB2F(P, B1[gy][iy]) * dT[iy];
-        day += DGB_TAB2F(P, D1[gy][iy]) * Tc[4][iy];
+        const float b = DGB_TAB2F(P, B1[gy][iy]);
+        u01 = fma2(bcast2(b), T01[iy], u01);
+        u23 = fma2(bcast2(b), T23[iy], u23);
+        u4 = fmaf(b, T4[iy], u4);
+        dd = fma2(make_float2(b, DGB_TAB2F(P, D1[gy][iy])), make_float2(dT[iy], T4[iy]), dd);
       }
+      double ug[NF] = {anc[0] + (double)u01.x, anc[1] + (double)u01.y, anc[2] + (double)u23.x,
+                       anc[3] + (double)u23.y, anc[4] + (double)u4};
+      const float dax = dd.x, day = dd.y;
       const double irho = __drcp_rn(ug[0]);
       const double pd = __drcp_rn(ug[4]) * (ug[3] - 0.5 * (ug[1] * ug[1] + ug[2] * ug[2]) * irho);
       const float uu = (float)(ug[1] * irho), vv = (float)(ug[2] * irho), Et = (float)ug[3], p = (float)pd;
       const float wq = DGB_TAB2F(P, W[g]);
       const float wx = wq * cx, wy = wq * cy;
       const float mx = (float)ug[1] * wx, my = (float)ug[2] * wy;
-      const float gxv[4] = {mx, mx * uu + wx * p, mx * vv, wx * ((Et + p) * uu)};
-      const float gyv[4] = {my, my * uu, my * vv + wy * p, wy * ((Et + p) * vv)};
+      const float2 gx01 = make_float2(mx, mx * uu + wx * p), gx23 = make_float2(mx * vv, wx * ((Et + p) * uu));
+      const float2 gy01 = make_float2(my, my * uu), gy23 = make_float2(my * vv + wy * p, wy * ((Et + p) * vv));
       const float gs = (wq * cJ) * (-uu * dax * sx - vv * day * sy);
-      if constexpr (kSfLift) {
 #pragma unroll
-        for (int iy = 0; iy < N1; ++iy) {
-          const float b = DGB_TAB2F(P, B1[gy][iy]), d = DGB_TAB2F(P, D1[gy][iy]);
-#pragma unroll
-          for (int f = 0; f < 4; ++f) { Ax[f][iy] += b * gxv[f]; Ay[f][iy] += d * gyv[f]; }
-          As[iy] += b * gs;
-        }
-      } else {
-#pragma unroll
-        for (int t = 0; t < NS; ++t) {
-#pragma unroll
-          for (int f = 0; f < 4; ++f) r[f][t] += DGB_TAB2F(P, dPx[g][t]) * gxv[f] + DGB_TAB2F(P, dPy[g][t]) * gyv[f];
-          r[4][t] += DGB_TAB2F(P, Phi[g][t]) * gs;
-        }
+      for (int iy = 0; iy < N1; ++iy) {
+        const float2 b = bcast2(DGB_TAB2F(P, B1[gy][iy])), d = bcast2(DGB_TAB2F(P, D1[gy][iy]));
+        Ax01[iy] = fma2(b, gx01, Ax01[iy]);
+        Ax23[iy] = fma2(b, gx23, Ax23[iy]);
+        Ay01[iy] = fma2(d, gy01, Ay01[iy]);
+        Ay23[iy] = fma2(d, gy23, Ay23[iy]);
+        As[iy] = fmaf(b.x, gs, As[iy]);
       }
     }
-    if constexpr (kSfLift) {
+    // dPx = l'_ix(x_gx) l_iy(x_gy), dPy = l_ix(x_gx) l'_iy(x_gy), Phi = l_ix(x_gx) l_iy(x_gy)
 #pragma unroll
-      for (int iy = 0; iy < N1; ++iy)
+    for (int iy = 0; iy < N1; ++iy)
 #pragma unroll
-        for (int ix = 0; ix < N1; ++ix) {
-          const float dx = DGB_TAB2F(P, D1[gx][ix]), bx = DGB_TAB2F(P, B1[gx][ix]);
-          const int t = ix + N1 * iy;
-#pragma unroll
-          for (int f = 0; f < 4; ++f) r[f][t] += dx * Ax[f][iy] + bx * Ay[f][iy];
-          r[4][t] += bx * As[iy];
-        }
-    }
+      for (int ix = 0; ix < N1; ++ix) {
+        const float2 dx = bcast2(DGB_TAB2F(P, D1[gx][ix])), bx = bcast2(DGB_TAB2F(P, B1[gx][ix]));
+        const int t = ix + N1 * iy;
+        r01[t] = fma2(bx, Ay01[iy], fma2(dx, Ax01[iy], r01[t]));
+        r23[t] = fma2(bx, Ay23[iy], fma2(dx, Ax23[iy], r23[t]));
+        r4[t] = fmaf(bx.x, As[iy], r4[t]);
+      }
   }
   if (MODE == MODE_RESIDUAL) {
 #pragma unroll
-    for (int f = 0; f < NF; ++f)
-#pragma unroll
-      for (int t = 0; t < NS; ++t) a.out[(size_t)(f * NS + t) * ld + e] = (double)r[f][t];
+    for (int t = 0; t < NS; ++t) {
+      a.out[(size_t)(0 * NS + t) * ld + e] = (double)r01[t].x;
+      a.out[(size_t)(1 * NS + t) * ld + e] = (double)r01[t].y;
+      a.out[(size_t)(2 * NS + t) * ld + e] = (double)r23[t].x;
+      a.out[(size_t)(3 * NS + t) * ld + e] = (double)r23[t].y;
+      a.out[(size_t)(4 * NS + t) * ld + e] = (double)r4[t];
+    }
     return;
   }
   const double dt = a.dt_override > 0 ? a.dt_override : a.scal->dt;
   const float sc = (float)(dt * a.invJ);
+  // DU = dt/J (M1^-1 (x) M1^-1) R, first along x then along y, on the pairs and on field 4
+  float2 m01[NS], m23[NS];
+  float m4[NS];
 #pragma unroll
-  for (int f = 0; f < NF; ++f) {
-    float tmp[NS];
+  for (int iy = 0; iy < N1; ++iy)
 #pragma unroll
-    for (int iy = 0; iy < N1; ++iy)
+    for (int ix = 0; ix < N1; ++ix) {
+      float2 s01 = make_float2(0.f, 0.f), s23 = make_float2(0.f, 0.f);
+      float s4 = 0.f;
 #pragma unroll
-      for (int ix = 0; ix < N1; ++ix) {
-        float s = 0.f;
-#pragma unroll
-        for (int q = 0; q < N1; ++q) s += DGB_TAB2F(P, M1i[ix][q]) * r[f][q + N1 * iy];
-        tmp[ix + N1 * iy] = s;
+      for (int q = 0; q < N1; ++q) {
+        const float m = DGB_TAB2F(P, M1i[ix][q]);
+        s01 = fma2(bcast2(m), r01[q + N1 * iy], s01);
+        s23 = fma2(bcast2(m), r23[q + N1 * iy], s23);
+        s4 = fmaf(m, r4[q + N1 * iy], s4);
       }
+      m01[ix + N1 * iy] = s01;
+      m23[ix + N1 * iy] = s23;
+      m4[ix + N1 * iy] = s4;
+    }
 #pragma unroll
-    for (int iy = 0; iy < N1; ++iy)
+  for (int iy = 0; iy < N1; ++iy)
 #pragma unroll
-      for (int ix = 0; ix < N1; ++ix) {
-        float s = 0.f;
+    for (int ix = 0; ix < N1; ++ix) {
+      float2 s01 = make_float2(0.f, 0.f), s23 = make_float2(0.f, 0.f);
+      float s4 = 0.f;
 #pragma unroll
-        for (int q = 0; q < N1; ++q) s += DGB_TAB2F(P, M1i[iy][q]) * tmp[ix + N1 * q];
-        const double du = (double)(sc * s);
-        const int t = ix + N1 * iy;
+      for (int q = 0; q < N1; ++q) {
+        const float m = DGB_TAB2F(P, M1i[iy][q]);
+        s01 = fma2(bcast2(m), m01[ix + N1 * q], s01);
+        s23 = fma2(bcast2(m), m23[ix + N1 * q], s23);
+        s4 = fmaf(m, m4[ix + N1 * q], s4);
+      }
+      const int t = ix + N1 * iy;
+      const double du[NF] = {(double)(sc * s01.x), (double)(sc * s01.y), (double)(sc * s23.x), (double)(sc * s23.y),
+                             (double)(sc * s4)};
+#pragma unroll
+      for (int f = 0; f < NF; ++f) {
         const size_t gi = (size_t)(f * NS + t) * ld + e;
         if (MODE == MODE_SSP) {
           const double base = a.a != 0.0 ? a.a * __ldg(a.Ubase + gi) : 0.0;
-          a.out[gi] = base + a.b * (us[(f * NS + t) * NT] + du);
+          a.out[gi] = base + a.b * (us[(f * NS + t) * NT] + du[f]);
         } else {
-          a.out[gi] = du;
-          if (a.Uacc) a.Uacc[gi] = a.Uacc[gi] + a.b * du;
+          a.out[gi] = du[f];
+          if (a.Uacc) a.Uacc[gi] = a.Uacc[gi] + a.b * du[f];
         }
       }
-  }
+    }
 }
 
 }  // namespace dgb
