@@ -5,12 +5,15 @@ The network (225 -> 64 -> 64 -> 1, GELU, sigmoid) predicts, from an element's an
 neighbours' normalised modes, whether the problem's m2 limiter would change that element.  Labels
 come from the full limiter run on seeded four-quadrant Riemann problems (per quadrant rho, p in
 U[0.1, 2], u, v in U[-1, 1], gamma in {1.4, 1.67}), p = 2, Rusanov flux, snapshots taken along
-SSP-RK3 runs so that the discontinuities are the ones the solver produces.  Features, labels,
+SSP-RK3 runs so that the discontinuities are the ones the solver produces: an element is labelled
+when the limiter changes one of its non-constant modes by more than 1e-8 of the field scale and
+its own modes rise above the inputs' rounding floor (5e-5 of the field scale; below it the mixed
+form's FP32 rounding and real structure look alike, so inputs are soft-thresholded there).  Features, labels,
 forward pass, backward pass and Adam updates are the CUDA kernels behind include/dgb.h
 (dgb_indicator_features / _labels, dgb_mlp_forward / _backward / _adam); torch only provides device
 buffers.  The solver uses the trained network through dgb_set_indicator (BF16 tensor-core scoring).
 
-    python -m dg_b200.learned train --out dg_b200/data/indicator_p2.npz
+    python -m dg_b200.learned train --out dg_b200/data/indicator_p2.npz   # 4096 problems at 256^2
 """
 from __future__ import annotations
 
@@ -69,26 +72,35 @@ def quadrant_problem(nx: int, ny: int, seed: int):
     return prob, prob.init_state("quadrants", seed=seed)
 
 
-def generate_dataset(seeds, nx: int = 64, ny: int = 64, snapshots=(1, 8, 24)):
+def generate_dataset(seeds, nx: int = 64, ny: int = 64, snapshots=(1, 8, 24), keep_quiet: float = 1.0,
+                     store_dtype=None, seed: int = 0):
     """Samples of every element at the given step counts of each seeded problem (the state is
-    limited first, as the reference limits its initial condition)."""
+    limited first, as the reference limits its initial condition).  Elements whose inputs are all
+    zero -- the whole stencil below the rounding floor, so never labelled -- are kept with
+    probability `keep_quiet`; `store_dtype` (torch.bfloat16, the scoring kernels' input type) halves
+    the inputs' footprint."""
     import torch
+    gen = torch.Generator(device="cuda")
+    gen.manual_seed(seed)
+    prob, _ = quadrant_problem(nx, ny, 0)  # one mesh for every seed
+    s = DGSolver(prob)
     Xs, ys = [], []
-    for sd in seeds:
-        prob, U0 = quadrant_problem(nx, ny, sd)
-        s = DGSolver(prob)
-        try:
-            s.set_state(s.limit(U0))
+    try:
+        for sd in seeds:
+            s.set_state(s.limit(prob.init_state("quadrants", seed=sd)))
             done = 0
             for k in snapshots:
                 if k > done:
                     s.advance(k - done, 0.0)
                     done = k
                 X, y = snapshot_samples(s)
-                Xs.append(X)
+                if keep_quiet < 1.0:
+                    keep = X.ne(0).any(dim=1) | (torch.rand(X.shape[0], device="cuda", generator=gen) < keep_quiet)
+                    X, y = X[keep], y[keep]
+                Xs.append(X.to(store_dtype) if store_dtype is not None else X)
                 ys.append(y)
-        finally:
-            s.close()
+    finally:
+        s.close()
     return torch.cat(Xs), torch.cat(ys)
 
 
@@ -140,7 +152,7 @@ def train(X, y, steps: int = 3000, batch: int = 8192, lr: float = 2e-3, seed: in
     for it in range(steps):
         idx = torch.randint(0, X.shape[0], (batch,), device="cuda", generator=gen)
         lr_t = lr * (0.5 * (1 + np.cos(np.pi * it / steps)))  # cosine decay
-        tr.step(X.index_select(0, idx).contiguous(), y.index_select(0, idx).contiguous(), lr_t, pos_weight)
+        tr.step(X.index_select(0, idx).float().contiguous(), y.index_select(0, idx).contiguous(), lr_t, pos_weight)
         if (it + 1) % log_every == 0 or it == 0:
             hist.append((it + 1, float(tr.loss.item())))
     return tr.params(), {"pos_weight": pos_weight, "loss": hist}
@@ -149,7 +161,7 @@ def train(X, y, steps: int = 3000, batch: int = 8192, lr: float = 2e-3, seed: in
 def evaluate(params: np.ndarray, X, y, threshold: float = 0.2) -> dict:
     """Recall / precision / flagged fraction of the FP32 network at `threshold`."""
     tr = Trainer(params, batch=1)
-    p = tr.predict(X)
+    p = tr.predict(X.float().contiguous())
     f = p > threshold
     yy = y > 0.5
     tp = float((f & yy).sum().item())
@@ -190,29 +202,36 @@ def scores(solver: DGSolver, U) -> tuple[np.ndarray, int]:
 
 
 def main(argv=None) -> int:
+    import torch
     ap = argparse.ArgumentParser()
     sub = ap.add_subparsers(dest="cmd", required=True)
     t = sub.add_parser("train")
     t.add_argument("--out", default=str(DEFAULT_WEIGHTS))
-    t.add_argument("--problems", type=int, default=96)
-    t.add_argument("--held-out", type=int, default=16)
-    t.add_argument("--n", type=int, default=64, help="elements per direction of each training problem")
-    t.add_argument("--steps", type=int, default=3000)
-    t.add_argument("--batch", type=int, default=8192)
+    t.add_argument("--problems", type=int, default=4096)
+    t.add_argument("--held-out", type=int, default=64)
+    t.add_argument("--n", type=int, default=256, help="elements per direction of each training problem")
+    t.add_argument("--snapshots", default="1,8,32,100", help="SSP-RK3 step counts at which samples are taken")
+    t.add_argument("--keep-quiet", type=float, default=1.0 / 32,
+                   help="fraction of the all-zero-input (never labelled) training samples kept")
+    t.add_argument("--steps", type=int, default=12000)
+    t.add_argument("--batch", type=int, default=16384)
     t.add_argument("--lr", type=float, default=2e-3)
     a = ap.parse_args(argv)
+    snaps = tuple(int(v) for v in a.snapshots.split(","))
     t0 = time.time()
-    X, y = generate_dataset(range(a.problems), a.n, a.n)
-    Xv, yv = generate_dataset(range(10000, 10000 + a.held_out), a.n, a.n)
+    X, y = generate_dataset(range(a.problems), a.n, a.n, snaps, a.keep_quiet, torch.bfloat16)
+    Xv, yv = generate_dataset(range(10000, 10000 + a.held_out), a.n, a.n, snaps, 1.0, torch.bfloat16)
     t1 = time.time()
     params, hist = train(X, y, a.steps, a.batch, a.lr)
     t2 = time.time()
     ev = {f"{th}": evaluate(params, Xv, yv, th) for th in (0.2, 0.5)}
-    meta = {"problems": a.problems, "n": a.n, "samples": int(X.shape[0]), "label_fraction": float(y.mean().item()),
+    meta = {"problems": a.problems, "n": a.n, "snapshots": list(snaps), "keep_quiet": a.keep_quiet,
+            "samples": int(X.shape[0]), "label_fraction": float(y.mean().item()),
             "steps": a.steps, "batch": a.batch, "lr": a.lr, "history": hist, "held_out": ev,
             "dataset_s": round(t1 - t0, 2), "train_s": round(t2 - t1, 2),
-            "recipe": "four-quadrant problems 0..problems-1 on n x n p=2 meshes, snapshots after 1, 8, 24 "
-                      "SSP-RK3 steps; held-out seeds 10000.."}
+            "recipe": f"four-quadrant problems 0..{a.problems - 1} on {a.n} x {a.n} p=2 meshes, samples after "
+                      f"{a.snapshots} SSP-RK3 steps (all-zero-input samples kept at {a.keep_quiet:g}, inputs "
+                      f"stored as BF16); held-out seeds 10000..{10000 + a.held_out - 1}, every element"}
     save(a.out, params, meta)
     print(json.dumps({k: v for k, v in meta.items() if k != "history"}))
     return 0

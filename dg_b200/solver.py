@@ -24,6 +24,7 @@ class Problem:
 
     def __init__(self, handle: C.c_void_p):
         self._h = handle
+        self._destroy = F.lib().dgb_problem_destroy  # bound now: module globals are gone at interpreter exit
         info = F.Info()
         F.check(F.lib().dgb_problem_info(self._h, C.byref(info)))
         self.info = info
@@ -57,7 +58,7 @@ class Problem:
     def __del__(self):
         h = getattr(self, "_h", None)
         if h:
-            F.lib().dgb_problem_destroy(h)
+            self._destroy(h)
             self._h = None
 
     @property
@@ -122,13 +123,14 @@ class DGSolver:
 
     def __init__(self, problem: Problem, device: int = 0):
         self.problem = problem
+        self._destroy = F.lib().dgb_destroy
         self._h = C.c_void_p()
         F.check(F.lib().dgb_create(problem._h, int(device), C.byref(self._h)))
         self.n = problem.state_size
 
     def close(self):
         if getattr(self, "_h", None):
-            F.lib().dgb_destroy(self._h)
+            self._destroy(self._h)
             self._h = None
 
     def __del__(self):
@@ -274,13 +276,14 @@ class DGBatch:
 
     def __init__(self, solvers: Sequence["DGSolver"]):
         self.solvers = list(solvers)
+        self._destroy = F.lib().dgb_batch_destroy
         arr = (C.c_void_p * len(self.solvers))(*[s._h for s in self.solvers])
         self._h = C.c_void_p()
         F.check(F.lib().dgb_batch_create(arr, len(self.solvers), C.byref(self._h)))
 
     def close(self):
         if getattr(self, "_h", None):
-            F.lib().dgb_batch_destroy(self._h)
+            self._destroy(self._h)
             self._h = None
 
     def __del__(self):

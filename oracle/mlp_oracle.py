@@ -91,12 +91,14 @@ def scales(a):
     return s + 1e-300
 
 
-FEAT_S0 = 1e-7
+FEAT_FLOOR = 5e-5  # rounding floor of the normalised inputs
+FEAT_S0 = 1e-5
 
 
 def compress(x):
-    """The fixed signed-log compression of the inputs: sign(x) log(1 + |x| / 1e-7) / log(1 + 1e7)."""
-    return np.sign(x) * np.log1p(np.abs(x) / FEAT_S0) / np.log1p(1.0 / FEAT_S0)
+    """The fixed input compression: soft threshold at the rounding floor, then a signed log,
+    sign(x) log(1 + max(|x| - 5e-5, 0) / 1e-5) / log(1 + 1e5)."""
+    return np.sign(x) * np.log1p(np.maximum(np.abs(x) - FEAT_FLOOR, 0.0) / FEAT_S0) / np.log1p(1.0 / FEAT_S0)
 
 
 def features(S: O.Setup, U, perm):
@@ -114,10 +116,14 @@ def features(S: O.Setup, U, perm):
 
 
 def labels(S: O.Setup, U, perm, tol=1e-8):
+    """1 where the full limiter changes a non-constant mode by more than tol of the field scale, in
+    an element whose own non-constant modes rise above the rounding floor of the inputs."""
     a = modes(U, S.N_E, perm)
     b = modes(O.limit(S, U), S.N_E, perm)
     s = scales(a)
-    return (np.abs(b - a)[:, :, 1:] > tol * s[:, :, None]).any(axis=(1, 2)).astype(np.float64)
+    changed = (np.abs(b - a)[:, :, 1:] > tol * s[:, :, None]).any(axis=(1, 2))
+    above = (np.abs(a)[:, :, 1:] > FEAT_FLOOR * s[:, :, None]).any(axis=(1, 2))
+    return (changed & above).astype(np.float64)
 
 
 def band(S: O.Setup, flags):

@@ -52,3 +52,25 @@ def test_band_adds_face_neighbours():
     b = M.band(S, f)
     exp = {3 * 8 + 4, 3 * 8 + 3, 3 * 8 + 5, 2 * 8 + 4, 4 * 8 + 4, 0, 1, 8, 7}  # corner: right, up, periodic left
     assert set(np.nonzero(b)[0].tolist()) == exp
+
+
+def test_rounding_floor_hides_fp32_level_noise():
+    """Inputs below the rounding floor (5e-5 of the field scale) are zero and carry no label: a
+    uniform state with 5e-7 relative noise on every node (the mixed form's FP32 flux arithmetic
+    leaves up to ~7e-7 on the nodes, up to ~2e-5 on the modes) looks like the clean state, while a
+    1e-3 perturbation stays visible."""
+    import dg_b200 as dgb
+    from oracle import dg_oracle as O
+    prob = dgb.Problem.structured(2, 2, 6, 4, flux="rusanov", limiter="m2l", cfl=0.3)
+    U = prob.init_state("quadrants", params=(10.0, 10.0), seed=1)
+    S = O.Setup.from_problem(prob)
+    perm = prob.array("tensor_perm")
+    rng = np.random.default_rng(5)
+    noisy = U * (1.0 + 5e-7 * rng.uniform(-1.0, 1.0, U.shape))
+    assert np.all(M.features(S, noisy, perm) == 0.0)
+    assert np.all(M.labels(S, noisy, perm) == 0)
+    bumped = U * (1.0 + 1e-3 * rng.uniform(-1.0, 1.0, U.shape))
+    assert np.abs(M.features(S, bumped, perm)).max() > 0.3
+    x = np.array([-1.0, -1e-3, -5e-5, 0.0, 2e-5, 5e-5, 6e-5, 1e-3, 1.0])
+    c = M.compress(x)
+    assert np.all(np.diff(c) > -1e-300) and np.all(c[2:6] == 0.0) and c[6] > 0 and abs(c[-1] - 1.0) < 1e-4
