@@ -50,6 +50,7 @@ struct dgb_ctx {
   bool gated = false, has_sensors = false;
   int sm_count = 148;           // multiprocessors of the device
   bool ind_on = false;          // learned indicator gates the limiter (dgb_set_indicator)
+  bool tile_dmma = false;       // p = 2 FP64 stages: the DMMA residual (else the scalar tiled kernel)
   bool ind_tc = true;           // scoring GEMMs on tcgen05 (else the mma.sync kernel)
   float ind_threshold = 0.2f;
   float* ind_params = nullptr;  // FP32 parameters (MLP_NPARAM)

@@ -190,24 +190,16 @@ __device__ __forceinline__ void tile_face_fluxes(const double* Us, const double*
   }
 }
 
-// The work of one tile (origin tx0, ty0).  The caller has initialised the mbarrier at the start of
-// shared memory; `phase` counts its completed phases (a persistent caller runs many tiles on one
-// barrier).  Every early return is taken by the whole CTA, after its last barrier.
-// NY passive mass fractions rho*Y_k follow the five gamma-model fields: conservative volume flux
-// rho*Y_k (u, v) (physics.cu:293-298) and the interface fluxes of phys::riemann2d_rcp.
-// GC: the GAMCONS model (fifth field rho/(gamma-1), conservative flux rho u/(gamma-1), no source;
-// physics.cu:253-281), with NY = 0.
-// TMA = false: the tile and the stage base come in by plain coalesced loads (grids whose row pitch
-// nx * 8 bytes is not a multiple of 16, which a tensor map cannot describe); same arithmetic.
-template <int P, int FLUX, int MODE, int TW, int TH, int UNROLL, int NY = 0, bool GC = false, bool TMA = true>
-__device__ __forceinline__ void tile2d_body(const TileArgs& a, const CUtensorMap* mapU, const CUtensorMap* mapB,
-                                            int tx0, int ty0, unsigned char* smraw, uint32_t& phase) {
-  static_assert(!(GC && NY > 0), "GAMCONS with mass fractions is not built");
+// Phase 0 of a tile (origin tx0, ty0): boundary codes of the tile edges, the tile's nodal state
+// (TMA copy, or plain coalesced loads when TMA = false) and the four neighbour face-node strips into
+// shared memory, by `nthr` threads.  Returns whether the tile copy arrived (CTA-uniform); a copy that
+// could not start or whose bounded wait ran out sets FLAG_TIMEOUT.  `phase` counts the mbarrier's
+// completed phases.
+template <int P, int TW, int TH, int NY, bool TMA>
+__device__ __forceinline__ bool tile_stage_in(const TileArgs& a, const CUtensorMap* mapU, int tx0, int ty0,
+                                              unsigned char* smraw, uint32_t& phase, int tid, int nthr) {
   using Dm = TileDims<P, TW, TH, NY>;
-  constexpr int N1 = Dm::N1, NS = Dm::NS, NF = Dm::NF, NT = Dm::NT, NXF = Dm::NXF, NYF = Dm::NYF;
-  constexpr int FS = NF + 1;             // face record: NF fluxes, ncterm
-  constexpr int NFL = 4 + NY + (GC ? 1 : 0);  // fields with a volume flux (rho, rho u, rho v, E, alpha | rho Y_k)
-  auto fld = [](int k) { return (GC || k < 4) ? k : k + 1; };
+  constexpr int N1 = Dm::N1, NS = Dm::NS, NF = Dm::NF, NT = Dm::NT;
   uint64_t* bar = reinterpret_cast<uint64_t*>(smraw);
   int* s_ok = reinterpret_cast<int*>(smraw + 8);
   int* codes = reinterpret_cast<int*>(smraw + Dm::head_bytes);  // [L: TH][R: TH][D: TW][U: TW]
@@ -216,14 +208,9 @@ __device__ __forceinline__ void tile2d_body(const TileArgs& a, const CUtensorMap
   double* HR = HL + TH * NF * N1;          // [TH][NF][N1]
   double* HD = HR + TH * NF * N1;          // [TW][NF][N1]  bottom neighbours' top-face nodes
   double* HU = HD + TW * NF * N1;          // [TW][NF][N1]
-  double* Fs = reinterpret_cast<double*>(smraw + Dm::off_face);  // [NXF + NYF][6] F[5], nc
-
-  const int tid = threadIdx.x;
+  double* Fs = reinterpret_cast<double*>(smraw + Dm::off_face);
   const int ld = a.ld, nx = a.nx;
-  constexpr bool kPrefetch = MODE != MODE_RESIDUAL;
-
-  // ---------------- phase 0: stage the tile (TMA) and the neighbour strips ----------------
-  for (int k = tid; k < Dm::NCODE; k += NT) {
+  for (int k = tid; k < Dm::NCODE; k += nthr) {
     int face, eo;
     if (k < TH) { face = 0; eo = (ty0 + k) * nx + tx0; }
     else if (k < 2 * TH) { face = 1; eo = (ty0 + k - TH) * nx + tx0 + TW - 1; }
@@ -236,7 +223,7 @@ __device__ __forceinline__ void tile2d_body(const TileArgs& a, const CUtensorMap
   // otherwise record the fault and skip the copy (the wait below then reports it)
   const bool tma_ok = TMA && (smem_u32(Us) & 127u) == 0 && (smem_u32(Fs) & 127u) == 0 && ((tx0 * 8) & 15) == 0;
   if constexpr (!TMA) {
-    for (int k = tid; k < NF * NS * NT; k += NT) {  // [plane][row][column], as the tensor map lands it
+    for (int k = tid; k < NF * NS * NT; k += nthr) {  // [plane][row][column], as the tensor map lands it
       const int q = k / NT, el = k % NT;
       Us[k] = __ldg(a.U + (size_t)q * ld + (size_t)(ty0 + el / TW) * nx + tx0 + el % TW);
     }
@@ -249,7 +236,7 @@ __device__ __forceinline__ void tile2d_body(const TileArgs& a, const CUtensorMap
       atomicOr(a.errflag, (unsigned)FLAG_TIMEOUT);
     }
   }
-  for (int k = tid; k < 2 * TH * NF * N1; k += NT) {
+  for (int k = tid; k < 2 * TH * NF * N1; k += nthr) {
     const int side = k / (TH * NF * N1);
     const int r = k % (TH * NF * N1);
     const int ty = r / (NF * N1), f = (r / N1) % NF, j = r % N1;
@@ -258,7 +245,7 @@ __device__ __forceinline__ void tile2d_body(const TileArgs& a, const CUtensorMap
     if (nb >= 0) v = __ldg(a.U + (size_t)(f * NS + (side == 0 ? P + N1 * j : N1 * j)) * ld + nb);
     (side == 0 ? HL : HR)[r] = v;
   }
-  for (int k = tid; k < 2 * TW * NF * N1; k += NT) {
+  for (int k = tid; k < 2 * TW * NF * N1; k += nthr) {
     const int side = k / (TW * NF * N1);
     const int r = k % (TW * NF * N1);
     const int tx = r / (NF * N1), f = (r / N1) % NF, j = r % N1;
@@ -277,7 +264,64 @@ __device__ __forceinline__ void tile2d_body(const TileArgs& a, const CUtensorMap
   }
   if (tma_ok) ++phase;
   __syncthreads();
-  if (!*s_ok) return;
+  return *s_ok != 0;
+}
+
+// Weighted volume terms at one quadrature point of quadrature weight Wg: gxv / gyv the x / y fluxes
+// of the NFL fields with a conservative flux (times Wg and the metric factors cx, cy), gs the
+// non-conservative source of alpha = 1/(gamma-1) (times Wg J), from the point values ug and the
+// reference derivatives (dax, day) of alpha (evaluate_sf, code/src/physics/physics.cu:248-301).
+template <int NF, int NFL, int NY, bool GC>
+__device__ __forceinline__ void point_terms(const double (&ug)[NF], double dax, double day, double Wg,
+                                            const TileArgs& a, double (&gxv)[NFL], double (&gyv)[NFL], double& gs) {
+  const double rho = ug[0], irho = __drcp_rn(rho);
+  const double uu = ug[1] * irho, vv = ug[2] * irho, Et = ug[3];
+  const double gm1 = GC ? rho * __drcp_rn(ug[4]) : __drcp_rn(ug[4]);  // gamma - 1
+  const double p = gm1 * (Et - 0.5 * rho * (uu * uu + vv * vv));
+  const double wx = Wg * a.cx, wy = Wg * a.cy;
+  const double mx = ug[1] * wx, my = ug[2] * wy;
+  gxv[0] = mx; gxv[1] = mx * uu + wx * p; gxv[2] = mx * vv; gxv[3] = wx * ((Et + p) * uu);
+  gyv[0] = my; gyv[1] = my * uu; gyv[2] = my * vv + wy * p; gyv[3] = wy * ((Et + p) * vv);
+#pragma unroll
+  for (int k = 0; k < NY; ++k) { gxv[4 + k] = wx * (ug[5 + k] * uu); gyv[4 + k] = wy * (ug[5 + k] * vv); }
+  if constexpr (GC) { gxv[4] = wx * (ug[4] * uu); gyv[4] = wy * (ug[4] * vv); }
+  gs = (Wg * a.J) * (-uu * dax * a.sx - vv * day * a.sy);
+}
+
+// The work of one tile (origin tx0, ty0).  The caller has initialised the mbarrier at the start of
+// shared memory; `phase` counts its completed phases (a persistent caller runs many tiles on one
+// barrier).  Every early return is taken by the whole CTA, after its last barrier.
+// NY passive mass fractions rho*Y_k follow the five gamma-model fields: conservative volume flux
+// rho*Y_k (u, v) (physics.cu:293-298) and the interface fluxes of phys::riemann2d_rcp.
+// GC: the GAMCONS model (fifth field rho/(gamma-1), conservative flux rho u/(gamma-1), no source;
+// physics.cu:253-281), with NY = 0.
+// TMA = false: the tile and the stage base come in by plain coalesced loads (grids whose row pitch
+// nx * 8 bytes is not a multiple of 16, which a tensor map cannot describe); same arithmetic.
+template <int P, int FLUX, int MODE, int TW, int TH, int UNROLL, int NY = 0, bool GC = false, bool TMA = true>
+__device__ __forceinline__ void tile2d_body(const TileArgs& a, const CUtensorMap* mapU, const CUtensorMap* mapB,
+                                            int tx0, int ty0, unsigned char* smraw, uint32_t& phase) {
+  static_assert(!(GC && NY > 0), "GAMCONS with mass fractions is not built");
+  using Dm = TileDims<P, TW, TH, NY>;
+  constexpr int N1 = Dm::N1, NS = Dm::NS, NF = Dm::NF, NT = Dm::NT, NXF = Dm::NXF;
+  constexpr int FS = NF + 1;             // face record: NF fluxes, ncterm
+  constexpr int NFL = 4 + NY + (GC ? 1 : 0);  // fields with a volume flux (rho, rho u, rho v, E, alpha | rho Y_k)
+  auto fld = [](int k) { return (GC || k < 4) ? k : k + 1; };
+  uint64_t* bar = reinterpret_cast<uint64_t*>(smraw);
+  int* s_ok = reinterpret_cast<int*>(smraw + 8);
+  int* codes = reinterpret_cast<int*>(smraw + Dm::head_bytes);  // [L: TH][R: TH][D: TW][U: TW]
+  double* Us = reinterpret_cast<double*>(smraw + Dm::off_tile);  // [NF*NS][NT]
+  double* HL = reinterpret_cast<double*>(smraw + Dm::off_halo);  // [TH][NF][N1] left neighbours' right-face nodes
+  double* HR = HL + TH * NF * N1;          // [TH][NF][N1]
+  double* HD = HR + TH * NF * N1;          // [TW][NF][N1]  bottom neighbours' top-face nodes
+  double* HU = HD + TW * NF * N1;          // [TW][NF][N1]
+  double* Fs = reinterpret_cast<double*>(smraw + Dm::off_face);  // [NXF + NYF][6] F[5], nc
+
+  const int tid = threadIdx.x;
+  const int ld = a.ld, nx = a.nx;
+  constexpr bool kPrefetch = MODE != MODE_RESIDUAL;
+
+  // ---------------- phase 0: stage the tile (TMA) and the neighbour strips ----------------
+  if (!tile_stage_in<P, TW, TH, NY, TMA>(a, mapU, tx0, ty0, smraw, phase, tid, NT)) return;
 
   // ---------------- phase 1: face fluxes, each face of the tile once ----------------
   tile_face_fluxes<P, FLUX, TW, TH, NY, GC>(Us, HL, HR, HD, HU, codes, Fs, tid, NT);
@@ -377,18 +421,8 @@ __device__ __forceinline__ void tile2d_body(const TileArgs& a, const CUtensorMap
       }
 #pragma unroll
       for (int iy = 0; iy < N1; ++iy) { dax += DGB_TAB2(P, B1[gy][iy]) * dT[iy]; day += DGB_TAB2(P, D1[gy][iy]) * Tc[4][iy]; }
-      const double rho = ug[0], irho = __drcp_rn(rho);
-      const double uu = ug[1] * irho, vv = ug[2] * irho, Et = ug[3];
-      const double gm1 = GC ? rho * __drcp_rn(ug[4]) : __drcp_rn(ug[4]);  // gamma - 1
-      const double p = gm1 * (Et - 0.5 * rho * (uu * uu + vv * vv));
-      const double wx = DGB_TAB2(P, W[g]) * a.cx, wy = DGB_TAB2(P, W[g]) * a.cy;
-      const double mx = ug[1] * wx, my = ug[2] * wy;
-      double gxv[NFL] = {mx, mx * uu + wx * p, mx * vv, wx * ((Et + p) * uu)};
-      double gyv[NFL] = {my, my * uu, my * vv + wy * p, wy * ((Et + p) * vv)};
-#pragma unroll
-      for (int k = 0; k < NY; ++k) { gxv[4 + k] = wx * (ug[5 + k] * uu); gyv[4 + k] = wy * (ug[5 + k] * vv); }
-      if constexpr (GC) { gxv[4] = wx * (ug[4] * uu); gyv[4] = wy * (ug[4] * vv); }
-      const double gs = (DGB_TAB2(P, W[g]) * a.J) * (-uu * dax * a.sx - vv * day * a.sy);
+      double gxv[NFL], gyv[NFL], gs;
+      point_terms<NF, NFL, NY, GC>(ug, dax, day, DGB_TAB2(P, W[g]), a, gxv, gyv, gs);
       if constexpr (kSfLift) {
 #pragma unroll
         for (int iy = 0; iy < N1; ++iy) {

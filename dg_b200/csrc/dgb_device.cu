@@ -18,6 +18,7 @@
 #include "../../include/dgb.h"
 #include "device/kernels.cuh"
 #include "device/tile2d.cuh"
+#include "device/tile2d_dmma.cuh"
 #include "device/limiter2d_tile.cuh"
 #include "device/limiter_gated.cuh"
 #include "device/tile2d_mixed.cuh"
@@ -195,14 +196,8 @@ const CUtensorMap& map_of(dgb_ctx* c, const double* p) {
   return c->mapA;
 }
 
-template <int P, int FLUX, int MODE, int NY = 0, bool GC = false, bool TMA = true>
-void launch_tile2d(dgb_ctx* c, const StageArgs& s) {
-  constexpr int TH = tile_h_for(P);
-  using Dm = TileDims<P, TILE_W, TH, NY>;
-  constexpr size_t smem = Dm::smem_bytes;
-  auto k = residual2d_tile_kernel<P, FLUX, MODE, TILE_W, TH, NY, GC, TMA>;
-  static bool attr = false;
-  if (!attr) { cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem); attr = true; }
+// kernel arguments of the tiled residuals for one stage
+TileArgs tile_args(dgb_ctx* c, const StageArgs& s) {
   TileArgs a;
   a.U = s.U; a.Ubase = s.Ubase; a.out = s.out; a.Uacc = s.Uacc; a.nbr = s.nbr; a.scal = s.scal;
   a.errflag = &c->scal->flags;
@@ -217,6 +212,18 @@ void launch_tile2d(dgb_ctx* c, const StageArgs& s) {
   a.JFx = c->cs.JFx;
   a.JFy = c->cs.JFy;
   a.nx = c->nx; a.ny = c->ny; a.ld = c->ld;
+  return a;
+}
+
+template <int P, int FLUX, int MODE, int NY = 0, bool GC = false, bool TMA = true>
+void launch_tile2d(dgb_ctx* c, const StageArgs& s) {
+  constexpr int TH = tile_h_for(P);
+  using Dm = TileDims<P, TILE_W, TH, NY>;
+  constexpr size_t smem = Dm::smem_bytes;
+  auto k = residual2d_tile_kernel<P, FLUX, MODE, TILE_W, TH, NY, GC, TMA>;
+  static bool attr = false;
+  if (!attr) { cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem); attr = true; }
+  const TileArgs a = tile_args(c, s);
   // (without TMA the maps are not read: the tile loads are plain)
   const CUtensorMap& mu = TMA ? map_of(c, s.U) : c->mapA;
   const CUtensorMap& mb = !TMA ? c->mapA
@@ -233,23 +240,23 @@ void launch_tile2d_mixed(dgb_ctx* c, const StageArgs& s) {
   auto k = residual2d_tile_mixed_kernel<P, FLUX, MODE, TILE_W, TH>;
   static bool attr = false;
   if (!attr) { cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem); attr = true; }
-  TileArgs a;
-  a.U = s.U; a.Ubase = s.Ubase; a.out = s.out; a.Uacc = s.Uacc; a.nbr = s.nbr; a.scal = s.scal;
-  a.errflag = &c->scal->flags;
-  a.polls = c->wait_polls;
-  a.a = s.a; a.b = s.b; a.dt_override = s.dt_override;
-  a.J = c->cs.J;
-  a.invJ = 1.0 / c->cs.J;
-  a.cx = c->cs.J * c->cs.ixx;
-  a.cy = c->cs.J * c->cs.iyy;
-  a.sx = c->cs.ixx;
-  a.sy = c->cs.iyy;
-  a.JFx = c->cs.JFx;
-  a.JFy = c->cs.JFy;
-  a.nx = c->nx; a.ny = c->ny; a.ld = c->ld;
+  const TileArgs a = tile_args(c, s);
   dim3 grid(c->nx / TILE_W, c->ny / TH);
   ProfScope ps(c, KC_RESIDUAL);
   k<<<grid, TILE_W * TH, smem, c->st>>>(a, map_of(c, s.U));
+}
+
+// p = 2 FP64 stage on the FP64 tensor cores (tile2d_dmma.cuh): same tiles and tensor map
+template <int FLUX, int MODE>
+void launch_tile2d_dmma(dgb_ctx* c, const StageArgs& s) {
+  constexpr size_t smem = DmmaDims::smem_bytes;
+  auto k = residual2d_tile_dmma_kernel<FLUX, MODE>;
+  static bool attr = false;
+  if (!attr) { cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem); attr = true; }
+  const TileArgs a = tile_args(c, s);
+  dim3 grid(c->nx / DMMA_TW, c->ny / DMMA_TH);
+  ProfScope ps(c, KC_RESIDUAL);
+  k<<<grid, DMMA_THREADS, smem, c->st>>>(a, map_of(c, s.U));
 }
 
 }  // namespace
@@ -308,6 +315,13 @@ int residual_ny(dgb_ctx* c, const StageArgs& a) {
 // the stage input's neighbours from global memory
 template <int P, int FLUX, int MODE>
 int tiles_then_strips(dgb_ctx* c, const StageArgs& a) {
+  if constexpr (P == 2 && MODE != MODE_RESIDUAL) {
+    if (c->tile_tma && c->tile_dmma) {
+      launch_tile2d_dmma<FLUX, MODE>(c, a);
+      if (c->nleft) launch_res2d<P, FLUX, MODE>(c, a, c->left, c->nleft);
+      return 0;
+    }
+  }
   if (c->tile_tma) launch_tile2d<P, FLUX, MODE>(c, a);
   else launch_tile2d<P, FLUX, MODE, 0, false, false>(c, a);
   if (c->nleft) launch_res2d<P, FLUX, MODE>(c, a, c->left, c->nleft);
@@ -908,6 +922,11 @@ extern "C" int dgb_create(const dgb_problem* prob, int device, dgb_ctx** out) {
     // learned-indicator scoring: tcgen05 GEMMs (DGB_INDICATOR_KERNEL=mma: the mma.sync form)
     const char* ik = std::getenv("DGB_INDICATOR_KERNEL");
     c->ind_tc = !(ik && std::string(ik) == "mma");
+    // p = 2 FP64 tiled stages: the one-thread-per-element kernel; DGB_TILE_KERNEL=dmma selects the
+    // form with the basis contractions on the FP64 tensor cores (measured slower on B200, whose
+    // FP64 tensor rate equals its FP64 vector rate)
+    const char* tk = std::getenv("DGB_TILE_KERNEL");
+    c->tile_dmma = tk && std::string(tk) == "dmma";
   }
   c->D = P.D; c->p = P.p; c->nf = P.N_F; c->ns = P.N_s; c->ne = P.N_E;
   c->ld = (P.N_E + 63) / 64 * 64;
