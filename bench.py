@@ -265,6 +265,17 @@ def time_steps(dgb, solver, steps, warmup, flush):
     return dev_ms, launches
 
 
+def kernel_breakdown(dgb, solver, steps=2 * IND_EVERY):
+    """Device time per step of each kernel class (residual, limiter, learned-indicator scoring, CFL
+    step) from a separate profiled pass of `steps` CFL steps: eager launches, each class bracketed by
+    CUDA events (adds launch gaps; the timed figures are graph replays)."""
+    solver.set_profiling(True)
+    solver.advance(steps, 0.0, scheme=dgb.SSPRK3)
+    out = {k: solver.kernel_timing(k)[0] / steps for k in ("residual", "limiter", "indicator", "dt")}
+    solver.set_profiling(False)
+    return out
+
+
 def cell_means(prob, U, field=0):
     """Cell averages of one field: sum_i w_i U_i with w_i = sum_g phi_w[g, i] / |reference element|."""
     i = prob.info
@@ -291,7 +302,7 @@ def compare_forms(dgb, U0_coarse, dev, steps, warmup, flush, acc_steps=200):
         ms, n = time_steps(dgb, s, steps, warmup, flush)
         dof = prob.info.n_elem * prob.info.n_s * prob.info.n_fields
         out[name] = {"value": dof * STAGES_PER_STEP * steps / (ms / 1e3), "ms_per_step": ms / steps,
-                     "gpu_launches_per_step": n / steps}
+                     "gpu_launches_per_step": n / steps, "kernel_ms_per_step": kernel_breakdown(dgb, s)}
         solvers[name] = s
     base = out["fp64"]["value"]
     for k in out:
@@ -506,7 +517,7 @@ def learned_deploy(dgb, dev, timed=20, warmup=3, steps=DEPLOY_STEPS):
         s.advance(timed, 0.0, scheme=dgb.SSPRK3)
         ms, n = s.last_timing()
         out[name] = {"value": dof * STAGES_PER_STEP * timed / (ms / 1e3), "ms_per_step": ms / timed,
-                     "gpu_launches_per_step": n / timed}
+                     "gpu_launches_per_step": n / timed, "kernel_ms_per_step": kernel_breakdown(dgb, s)}
         s.set_state(U0)
         s.advance(steps, dt, scheme=dgb.SSPRK3)
         finals[name] = s.get_state()
@@ -939,6 +950,7 @@ def main(argv=None) -> int:
     res_ms, res_n = solver.kernel_timing("residual")
     lim_ms, lim_n = solver.kernel_timing("limiter")
     dt_ms, dt_n = solver.kernel_timing("dt")
+    ind_ms, _ = solver.kernel_timing("indicator")
     solver.set_profiling(False)
     res_avg_s = res_ms / 1e3 / max(res_n, 1)
     achieved_gbs = BYTES_PER_DOF_STAGE * dof / res_avg_s / 1e9
@@ -1024,6 +1036,7 @@ def main(argv=None) -> int:
                              "peak_source": "MEASURED_PEAKS.json hbm_gbs (measured copy)"},
                 "kernel_ms_per_step": {"residual": res_ms / args.steps, "limiter": lim_ms / args.steps,
                                        "dt": dt_ms / args.steps,
+                                       **({"indicator": ind_ms / args.steps} if args.learned else {}),
                                        "source": "separate profiled pass: eager launches, each kernel class "
                                                  "bracketed by CUDA events (adds launch gaps; the headline "
                                                  "ms_per_step is the captured graph's replay)"},

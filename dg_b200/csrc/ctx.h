@@ -15,7 +15,7 @@
 #include "device/sensor.h"
 
 namespace dgb {
-enum { KC_RESIDUAL = 0, KC_LIMITER = 1, KC_DT = 2, KC_OTHER = 3, KC_N = 4 };
+enum { KC_RESIDUAL = 0, KC_LIMITER = 1, KC_DT = 2, KC_INDICATOR = 3, KC_OTHER = 4, KC_N = 5 };
 }
 
 struct dgb_ctx {
@@ -62,6 +62,8 @@ struct dgb_ctx {
   int* ind_list = nullptr;      // [N_E] + count
   unsigned char* ind_band = nullptr;  // flagged elements and their neighbours
   int* ind_blist = nullptr;     // [N_E] + count: the band as a list
+  int* ind_tiles = nullptr;     // row-major grids: the gated passes' tiles with band elements,
+  int ind_n0 = 0, ind_n1 = 0;   //   [n0] x-pass tiles, [n1] y-pass tiles, then the two counts
   dgb::SensorLaunch sl;
   int* iperm = nullptr;
   double* smean = nullptr;
@@ -90,8 +92,8 @@ struct dgb_ctx {
   std::vector<std::pair<int, std::pair<cudaEvent_t, cudaEvent_t>>> pev;
   std::vector<cudaEvent_t> ev_pool;
   size_t ev_used = 0;
-  double kc_ms[dgb::KC_N] = {0, 0, 0, 0};
-  long long kc_n[dgb::KC_N] = {0, 0, 0, 0};
+  double kc_ms[dgb::KC_N] = {0, 0, 0, 0, 0};
+  long long kc_n[dgb::KC_N] = {0, 0, 0, 0, 0};
   long long counter = 0;  // launches issued since the last reset
 };
 

@@ -187,34 +187,35 @@ __global__ void __launch_bounds__(128) lim_gated_kernel(const LimArgs la, const 
 // arithmetic as the sparse lim_gated_kernel<2, P, 2, PASS, false, false, true>): a CTA covers the
 // tile of the dense tiled limiter pass -- PASS 0: 30 elements of one element row (threads: element
 // slot with the left / right neighbour slots, x slice), PASS 1: 32 x 4 elements (threads: x slot,
-// row slot with the bottom / top neighbour rows) for node column blockIdx.z.  Every slot's slice is
+// row slot with the bottom / top neighbour rows) for one node column `sl`.  Every slot's slice is
 // loaded once, coalesced, and shared through shared memory; only the band elements (flag[e] != 0)
-// are limited and written, and a CTA whose tile holds no band element leaves after one block vote.
+// are limited and written, and a tile without band elements is left after one block vote.
 // PASS 0 reads the raw state U and writes the band's x-limited slices to X; PASS 1 reads X for band
-// elements and U for the others and writes the band's result into U.
+// elements and U for the others and writes the band's result into U.  Every thread of the CTA runs
+// both of the tile's barriers (the vote and the shared-slice barrier), so a CTA can run the tiles of
+// a list one after another on the same shared memory.
+constexpr int GATED_TW0 = 30, GATED_TW1 = 32, GATED_TH1 = 4;  // x-pass tile width, y-pass tile
+
 template <int P, int PASS>
-__global__ void __launch_bounds__(PASS == 0 ? 32 * (P + 1) : 32 * 6)
-    lim_gated_tile_kernel(const LimArgs la, int nx, int ny, double* __restrict__ U, double* __restrict__ X,
-                          const int* __restrict__ nbr, const unsigned char* __restrict__ flag,
-                          const DevScalars* __restrict__ scal) {
-  constexpr int N1 = P + 1, NS = N1 * N1, NF = 5, TWI = 30, THI = 4;
-  constexpr int SLOTS = PASS == 0 ? N1 : 6;                  // thread rows: x slices, or row slots
-  __shared__ double V[NF][N1][SLOTS][32];                    // [field][node][thread row][slot]
-  if (scal && scal->flags) return;
+__device__ __forceinline__ void lim_gated_tile(const LimArgs& la, int nx, int ny, double* __restrict__ U,
+                                               double* __restrict__ X, const int* __restrict__ nbr,
+                                               const unsigned char* __restrict__ flag, int bxi, int byi, int slc,
+                                               double (&V)[5][P + 1][PASS == 0 ? P + 1 : 6][32]) {
+  constexpr int N1 = P + 1, NS = N1 * N1, NF = 5, TWI = GATED_TW0, THI = GATED_TH1;
   const int ld = la.ld, tx = threadIdx.x, ty = threadIdx.y;
   int e = -1;
   bool interior;
   int sl;  // the slice this thread's values belong to: x slice (PASS 0) or node column (PASS 1)
   if (PASS == 0) {
-    const int x0 = blockIdx.x * TWI, ey = blockIdx.y, ex = x0 - 1 + tx;
+    const int x0 = bxi * TWI, ey = byi, ex = x0 - 1 + tx;
     sl = ty;
     interior = tx >= 1 && tx <= TWI && ex < nx;
     if (interior) e = ey * nx + ex;
     else if (tx == 0) e = __ldg(nbr + (size_t)0 * ld + ey * nx + x0);
     else if (ex - 1 < nx && ex - 1 >= 0) e = __ldg(nbr + (size_t)1 * ld + ey * nx + ex - 1);
   } else {
-    const int x0 = blockIdx.x * 32, y0 = blockIdx.y * THI, x = x0 + tx, yy = y0 - 1 + ty;
-    sl = blockIdx.z;
+    const int x0 = bxi * GATED_TW1, y0 = byi * THI, x = x0 + tx, yy = y0 - 1 + ty;
+    sl = slc;
     interior = ty >= 1 && ty <= THI && yy < ny && x < nx;
     if (x < nx) {
       if (interior) e = yy * nx + x;
@@ -260,6 +261,54 @@ __global__ void __launch_bounds__(PASS == 0 ? 32 * (P + 1) : 32 * 6)
   for (int f = 0; f < NF; ++f)
 #pragma unroll
     for (int k = 0; k < N1; ++k) out[(size_t)(f * NS + node(k)) * ld + e] = res[f][k];
+}
+
+// The gated pass over a list of its tiles that hold band elements (built with the band,
+// gated_tile_list_kernel), by persistent CTAs: CTA b takes list entries b, b + gridDim.x, ... (tile
+// index = tile row * tiles per row + tile column); for PASS 1 blockIdx.z is the node column.  Tiles
+// without band elements are not visited at all.
+template <int P, int PASS>
+__global__ void __launch_bounds__(PASS == 0 ? 32 * (P + 1) : 32 * 6)
+    lim_gated_tile_list_kernel(const LimArgs la, int nx, int ny, double* __restrict__ U, double* __restrict__ X,
+                               const int* __restrict__ nbr, const unsigned char* __restrict__ flag,
+                               const int* __restrict__ tiles, const int* __restrict__ count,
+                               const DevScalars* __restrict__ scal) {
+  __shared__ double V[5][P + 1][PASS == 0 ? P + 1 : 6][32];
+  if (scal && scal->flags) return;
+  const int ntx = PASS == 0 ? (nx + GATED_TW0 - 1) / GATED_TW0 : (nx + GATED_TW1 - 1) / GATED_TW1;
+  const int n = *count;
+  for (int i = blockIdx.x; i < n; i += gridDim.x) {
+    const int t = tiles[i];
+    lim_gated_tile<P, PASS>(la, nx, ny, U, X, nbr, flag, t % ntx, t / ntx, blockIdx.z, V);
+  }
+}
+
+// the tiles of both gated passes that hold band elements, as two lists (order immaterial): thread
+// t < n0 checks x-pass tile t (30 elements of one row), thread n0 + t checks y-pass tile t (32 x 4)
+static __global__ void __launch_bounds__(256) gated_tile_list_kernel(int nx, int ny, const unsigned char* __restrict__ band,
+                                                              int* __restrict__ list0, int* __restrict__ count0,
+                                                              int* __restrict__ list1, int* __restrict__ count1,
+                                                              const DevScalars* __restrict__ scal) {
+  if (scal && scal->flags) return;
+  const int ntx0 = (nx + GATED_TW0 - 1) / GATED_TW0, n0 = ntx0 * ny;
+  const int ntx1 = (nx + GATED_TW1 - 1) / GATED_TW1, n1 = ntx1 * ((ny + GATED_TH1 - 1) / GATED_TH1);
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  bool any = false;
+  int* list = list0;
+  int* count = count0;
+  int t = k;
+  if (k < n0) {
+    const int x0 = (k % ntx0) * GATED_TW0, y = k / ntx0;
+    for (int x = x0; x < min(x0 + GATED_TW0, nx) && !any; ++x) any = band[(size_t)y * nx + x] != 0;
+  } else if (k < n0 + n1) {
+    t = k - n0;
+    list = list1;
+    count = count1;
+    const int x0 = (t % ntx1) * GATED_TW1, y0 = (t / ntx1) * GATED_TH1;
+    for (int y = y0; y < min(y0 + GATED_TH1, ny) && !any; ++y)
+      for (int x = x0; x < min(x0 + GATED_TW1, nx) && !any; ++x) any = band[(size_t)y * nx + x] != 0;
+  }
+  if (any) list[atomicAdd(count, 1)] = t;
 }
 
 // p0i: flagged elements to their cell average sum_t w_t U_t (w from phi_w / |reference element|)

@@ -525,7 +525,7 @@ int limit_to(dgb_ctx* c, const double* in, double* out) {
 // learned indicator: scores and flags of U (modes, then the BF16 tensor-core MLP), then the band
 // (flagged elements and their face neighbours) that the sparse limiter works on
 void launch_indicator(dgb_ctx* c, const double* U) {
-  ProfScope ps(c, KC_LIMITER);
+  ProfScope ps(c, KC_INDICATOR);
   indicator_modes_kernel<2><<<(c->ne + 127) / 128, 128, 0, c->st>>>(U, c->ld, c->ne, c->ind_modes);
   cudaMemsetAsync(c->ind_list + c->ld, 0, sizeof(int), c->st);
   IndicatorArgs a;
@@ -556,6 +556,16 @@ void launch_indicator(dgb_ctx* c, const double* U) {
   indicator_band_kernel<<<(c->ne + 255) / 256, 256, 0, c->st>>>(c->ne, c->ld, 4, c->nbr, c->ind_flag, c->ind_band,
                                                                 c->ind_blist, c->ind_blist + c->ld, c->scal);
   c->counter += 2;  // three kernels (the scope counted one)
+  if (c->ind_tiles) {
+    // the gated passes' tiles that hold band elements
+    int* l0 = c->ind_tiles;
+    int* l1 = l0 + c->ind_n0;
+    int* cnt = l1 + c->ind_n1;
+    cudaMemsetAsync(cnt, 0, 2 * sizeof(int), c->st);
+    gated_tile_list_kernel<<<(c->ind_n0 + c->ind_n1 + 255) / 256, 256, 0, c->st>>>(c->nx, c->ny, c->ind_band, l0, cnt,
+                                                                                   l1, cnt + 1, c->scal);
+    c->counter += 1;
+  }
 }
 
 // learned-indicator-gated m2 limiter (m2i arithmetic on the band only), in place; score = false
@@ -567,10 +577,17 @@ void launch_learned_limiter(dgb_ctx* c, double* U, bool score) {
   ProfScope ps(c, KC_LIMITER);
   const LimArgs la{c->ld, c->ne};
   if (c->rowmajor) {
-    dim3 gx((c->nx + 29) / 30, c->ny), bx(32, 3);
-    lim_gated_tile_kernel<2, 0><<<gx, bx, 0, c->st>>>(la, c->nx, c->ny, U, c->X, c->nbr, c->ind_band, c->scal);
-    dim3 gy((c->nx + 31) / 32, (c->ny + 3) / 4, 3), by(32, 6);
-    lim_gated_tile_kernel<2, 1><<<gy, by, 0, c->st>>>(la, c->nx, c->ny, U, c->X, c->nbr, c->ind_band, c->scal);
+    // persistent CTAs over the lists of tiles with band elements (built with the band): the tiles
+    // without any are not launched at all
+    const int* l0 = c->ind_tiles;
+    const int* l1 = l0 + c->ind_n0;
+    const int* cnt = l1 + c->ind_n1;
+    dim3 gx(std::min(c->ind_n0, c->sm_count * 16)), bx(32, 3);
+    lim_gated_tile_list_kernel<2, 0><<<gx, bx, 0, c->st>>>(la, c->nx, c->ny, U, c->X, c->nbr, c->ind_band, l0, cnt,
+                                                           c->scal);
+    dim3 gy(std::min(c->ind_n1, c->sm_count * 4), 1, 3), by(32, 6);
+    lim_gated_tile_list_kernel<2, 1><<<gy, by, 0, c->st>>>(la, c->nx, c->ny, U, c->X, c->nbr, c->ind_band, l1,
+                                                           cnt + 1, c->scal);
     c->counter += 1;
     return;
   }
@@ -1074,7 +1091,8 @@ extern "C" void dgb_destroy(dgb_ctx* c) {
   if (c->perm) cudaFree(c->perm);
   if (c->iperm) cudaFree(c->iperm);
   for (void* q : {(void*)c->ind_params, (void*)c->ind_w, (void*)c->ind_vec, (void*)c->ind_modes, (void*)c->ind_score,
-                  (void*)c->ind_flag, (void*)c->ind_list, (void*)c->ind_band, (void*)c->ind_blist})
+                  (void*)c->ind_flag, (void*)c->ind_list, (void*)c->ind_band, (void*)c->ind_blist,
+                  (void*)c->ind_tiles})
     if (q) cudaFree(q);
   if (c->smean) cudaFree(c->smean);
   if (c->sint) cudaFree(c->sint);
@@ -1278,6 +1296,12 @@ extern "C" int dgb_set_indicator(dgb_ctx* c, const float* params, float threshol
         (e = cudaMalloc(&c->ind_band, (size_t)c->ld)) != cudaSuccess ||
         (e = cudaMalloc(&c->ind_blist, ((size_t)c->ld + 1) * sizeof(int))) != cudaSuccess)
       return set_error(DGB_ERR_CUDA, std::string("indicator buffers: ") + cudaGetErrorString(e));
+    if (c->rowmajor) {
+      c->ind_n0 = (c->nx + GATED_TW0 - 1) / GATED_TW0 * c->ny;
+      c->ind_n1 = (c->nx + GATED_TW1 - 1) / GATED_TW1 * ((c->ny + GATED_TH1 - 1) / GATED_TH1);
+      if ((e = cudaMalloc(&c->ind_tiles, ((size_t)c->ind_n0 + c->ind_n1 + 2) * sizeof(int))) != cudaSuccess)
+        return set_error(DGB_ERR_CUDA, std::string("indicator buffers: ") + cudaGetErrorString(e));
+    }
   }
   std::vector<__nv_bfloat16> w((size_t)MLP_H * IND_KPAD + MLP_H * MLP_H, __float2bfloat16(0.f));
   for (int j = 0; j < MLP_H; ++j)
@@ -1619,7 +1643,8 @@ extern "C" int dgb_set_profiling(dgb_ctx* c, int on) {
 extern "C" int dgb_kernel_timing(dgb_ctx* c, const char* name, double* ms, long long* launches) {
   if (!c || !name) return set_error(DGB_ERR_ARG, "null argument");
   const std::string n = name;
-  int k = n == "residual" ? KC_RESIDUAL : n == "limiter" ? KC_LIMITER : n == "dt" ? KC_DT : n == "other" ? KC_OTHER : -1;
+  int k = n == "residual" ? KC_RESIDUAL : n == "limiter" ? KC_LIMITER : n == "dt" ? KC_DT
+          : n == "indicator" ? KC_INDICATOR : n == "other" ? KC_OTHER : -1;
   if (k < 0) return set_error(DGB_ERR_ARG, "unknown kernel class " + n);
   if (ms) *ms = c->kc_ms[k];
   if (launches) *launches = c->kc_n[k];

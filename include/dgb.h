@@ -259,7 +259,8 @@ int dgb_conservation(dgb_ctx* c, double* totals /* N_F */);
  * and the number of kernel launches it issued. */
 int dgb_last_timing(dgb_ctx* c, double* ms, long long* launches);
 /* Per-kernel device time of the last dgb_advance when profiling is on:
- * names "residual", "limiter", "dt"; ms and launches of that kernel class. */
+ * names "residual", "limiter", "dt", "indicator" (the learned indicator's scoring kernels);
+ * ms and launches of that kernel class. */
 int dgb_set_profiling(dgb_ctx* c, int on);
 int dgb_kernel_timing(dgb_ctx* c, const char* name, double* ms, long long* launches);
 
@@ -267,8 +268,10 @@ int dgb_kernel_timing(dgb_ctx* c, const char* name, double* ms, long long* launc
  * Learned troubled-cell indicator (no counterpart in the reference)
  * ------------------------------------------------------------------------------------
  * A 225 -> 64 -> 64 -> 1 MLP (GELU, sigmoid) reads each element's and its four neighbours'
- * normalised scaled-Taylor modes (2D, p = 2; each input compressed by sign(x) log(1 + |x| / 1e-7) / log(1 + 1e7))
- * and predicts whether the problem's limiter would change the element.  Parameters: one FP32 array of dgb_mlp_param_count() values laid out as
+ * normalised scaled-Taylor modes (2D, p = 2; each input x soft-thresholded at the rounding floor
+ * 5e-5 and compressed, sign(x) log(1 + max(|x| - 5e-5, 0) / 1e-5) / log(1 + 1e5)) and predicts
+ * whether the problem's limiter would change the element (labels: a non-constant mode changed by
+ * more than 1e-8 of the field scale, in an element whose own modes rise above the floor).  Parameters: one FP32 array of dgb_mlp_param_count() values laid out as
  * W1[64][225], b1[64], W2[64][64], b2[64], w3[64], b3.  Pointers marked _dev are device memory. */
 int dgb_mlp_param_count(void);
 /* Features [N_E][225] (FP32, row-major) of the context's current state. */

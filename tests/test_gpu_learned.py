@@ -149,7 +149,8 @@ def test_trained_indicator_gain():
 def test_scoring_interval_keeps_the_full_limiter_result():
     """Scoring every 8th step (the band of the last scoring covers the discontinuities for up to
     (2p+1)/CFL = 16 steps): still within 1e-4 relative L1 density of the full limiter after 100
-    steps on the shock-bubble, and the steps in between launch the three scoring kernels less."""
+    steps on the shock-bubble, and the steps in between launch the four scoring kernels less
+    (modes, scores, band, and the lists of the gated passes' tiles with band elements)."""
     import dg_b200 as dgb
     from dg_b200 import learned as L
     params, _ = L.load()
@@ -165,7 +166,7 @@ def test_scoring_interval_keeps_the_full_limiter_result():
         n_score = learned.last_timing()[1]
         learned.advance(1, dt)
         n_reuse = learned.last_timing()[1]
-        assert n_reuse == n_score - 3
+        assert n_reuse == n_score - 4
         out = {}
         for name, s in (("full", full), ("learned", learned)):
             s.set_state(U0)
