@@ -764,7 +764,7 @@ def mixed_p3(dgb, dev, steps=P3_STEPS, timed=10):
     return out
 
 
-PROFILE_CASES = ("p2step", "p2mixed", "p2learned", "p3fp64", "p3mixed", "batch", "indicator")
+PROFILE_CASES = ("p2step", "p2mixed", "p2learned", "deploylearned", "p3fp64", "p3mixed", "batch", "indicator")
 
 
 def profile_case(dgb, dev, name):
@@ -772,13 +772,19 @@ def profile_case(dgb, dev, name):
     no timing): p2step -- 3 SSP-RK3 steps of the benchmark workload's problem at 1024 x 512 (p=2,
     Rusanov, m2l, FP64; 189 MB per state array); p2mixed -- the same in the mixed form; p2learned --
     9 steps of the 512 x 256 workload in the mixed form with the learned-indicator-gated limiter
-    (scored every IND_EVERY steps); p3fp64 / p3mixed -- 2 SSP-RK3 steps of the 1024 x 512 p=3 Roe shock-bubble in the
+    (scored every IND_EVERY steps); deploylearned -- the same 9 steps on the learned indicator's 1024^2
+    four-quadrant deployment problem; p3fp64 / p3mixed -- 2 SSP-RK3 steps of the 1024 x 512 p=3 Roe shock-bubble in the
     FP64 / mixed form; batch -- 2 batched steps of 8 2D quadrant problems (256^2, p=2) and 8 1D
     Riemann problems (5000 elements, p=2); indicator -- 3 scorings of the 1024 x 512 p=2
     shock-bubble (after 10 steps) by the trained network."""
-    if name == "p2learned":
+    if name in ("p2learned", "deploylearned"):
         from dg_b200 import learned as L
-        prob, U0 = build_problem()
+        if name == "p2learned":
+            prob, U0 = build_problem()
+        else:
+            prob = dgb.Problem.structured(2, 2, DEPLOY_N, DEPLOY_N, 0.0, 1.0, 0.0, 1.0, bc=("transmissive",) * 4,
+                                          flux="rusanov", limiter="m2l", cfl=CFL)
+            U0 = prob.init_state("quadrants", seed=DEPLOY_SEED)
         s = dgb.DGSolver(prob, device=dev)
         s.set_form("mixed")
         L.set_indicator(s, L.load()[0], 0.2, every=IND_EVERY)
