@@ -403,3 +403,393 @@ __global__ void __launch_bounds__(TW * TH, 3)
 }
 
 }  // namespace dgb
+
+namespace dgb {
+
+// ---------------------------------------------------------------------------------------------
+// Compressed-tile variant of the mixed kernel.  The shared tile holds, per element, the FP64
+// anchors (node-0 values of the five fields) and the FP32 deviations of the other nodes from them
+// -- 200 instead of 360 bytes per element at p = 2 -- written by each thread for its own element
+// from plain coalesced loads.  Collocation then reads its FP32 operands straight from shared memory
+// (no FP64 subtraction and conversion per quadrature column), the CTA fits in ~55 KB at p = 2 (four
+// CTAs per SM instead of three), and the stage update re-reads the FP64 stage input through L2.
+// The face traces are formed from the same anchors and deviations: the FP64 value of the face's
+// first node plus an FP32 contraction of the other nodes' deviations from it, as in the TMA-tile
+// kernel.
+template <int P, int TW, int TH>
+struct TileDimsMixedCT {
+  static constexpr int N1 = P + 1, NS = N1 * N1, NF = 5, NT = TW * TH;
+  static constexpr int NXF = (TW + 1) * TH * N1, NYF = TW * (TH + 1) * N1, NCODE = 2 * TH + 2 * TW;
+  static constexpr size_t head_bytes = 128;
+  static constexpr size_t code_bytes = (NCODE * 4 + 127) / 128 * 128;
+  static constexpr size_t off_anc = head_bytes + code_bytes;              // double [NF][NT]
+  static constexpr size_t off_d01 = off_anc + (size_t)NF * NT * 8;        // float2 [NS-1][NT]: fields 0, 1
+  static constexpr size_t off_d23 = off_d01 + (size_t)(NS - 1) * NT * 8;  // float2 [NS-1][NT]: fields 2, 3
+  static constexpr size_t off_d4 = off_d23 + (size_t)(NS - 1) * NT * 8;   // float  [NS-1][NT]: field 4
+  static constexpr size_t off_halo = off_d4 + ((size_t)(NS - 1) * NT * 4 + 15) / 16 * 16;
+  static constexpr size_t halo_doubles = (size_t)2 * TH * NF * N1 + (size_t)2 * TW * NF * N1;
+  static constexpr size_t off_face = off_halo + halo_doubles * 8;
+  static constexpr size_t smem_bytes = off_face + (size_t)6 * (NXF + NYF) * sizeof(float);
+};
+
+// FP32 deviation of node t of field f from the field's anchor, element i of the tile (t = 0: zero)
+template <int NT>
+__device__ __forceinline__ float ct_dev(const float2* d01, const float2* d23, const float* d4, int f, int t, int i) {
+  if (t == 0) return 0.f;
+  const int r = (t - 1) * NT + i;
+  return f == 0 ? d01[r].x : f == 1 ? d01[r].y : f == 2 ? d23[r].x : f == 3 ? d23[r].y : d4[r];
+}
+
+template <int P, int FLUX, int MODE, int TW, int TH, int MINB>
+__global__ void __launch_bounds__(TW * TH, MINB)
+    residual2d_tile_mixed_ct_kernel(const TileArgs a) {
+  using Dm = TileDimsMixedCT<P, TW, TH>;
+  constexpr int N1 = Dm::N1, NS = Dm::NS, NF = 5, NT = Dm::NT, NXF = Dm::NXF, NYF = Dm::NYF;
+  extern __shared__ __align__(128) unsigned char smraw[];
+  int* codes = reinterpret_cast<int*>(smraw + Dm::head_bytes);
+  double* Anc = reinterpret_cast<double*>(smraw + Dm::off_anc);
+  float2* D01 = reinterpret_cast<float2*>(smraw + Dm::off_d01);
+  float2* D23 = reinterpret_cast<float2*>(smraw + Dm::off_d23);
+  float* D4 = reinterpret_cast<float*>(smraw + Dm::off_d4);
+  double* HL = reinterpret_cast<double*>(smraw + Dm::off_halo);
+  double* HR = HL + TH * NF * N1;
+  double* HD = HR + TH * NF * N1;
+  double* HU = HD + TW * NF * N1;
+  float* Fs = reinterpret_cast<float*>(smraw + Dm::off_face);  // [NXF + NYF][6]
+
+  if (a.scal && a.scal->flags) return;
+  const int tid = threadIdx.x;
+  const int tx0 = blockIdx.x * TW, ty0 = blockIdx.y * TH;
+  const int ld = a.ld, nx = a.nx;
+  const int tx = tid % TW, ty = tid / TW;
+  const int e = (ty0 + ty) * nx + tx0 + tx;
+
+  // ---------------- phase 0: own element compressed, neighbour strips by plain loads ----------------
+  for (int k = tid; k < Dm::NCODE; k += NT) {
+    int face, eo;
+    if (k < TH) { face = 0; eo = (ty0 + k) * nx + tx0; }
+    else if (k < 2 * TH) { face = 1; eo = (ty0 + k - TH) * nx + tx0 + TW - 1; }
+    else if (k < 2 * TH + TW) { face = 2; eo = ty0 * nx + tx0 + (k - 2 * TH); }
+    else { face = 3; eo = (ty0 + TH - 1) * nx + tx0 + (k - 2 * TH - TW); }
+    codes[k] = __ldg(a.nbr + (size_t)face * ld + eo);
+  }
+  {
+    const double* ue = a.U + e;
+#pragma unroll
+    for (int pr = 0; pr < 2; ++pr) {
+      double u0[NS], u1[NS];
+#pragma unroll
+      for (int t = 0; t < NS; ++t) {
+        u0[t] = __ldg(ue + (size_t)((2 * pr) * NS + t) * ld);
+        u1[t] = __ldg(ue + (size_t)((2 * pr + 1) * NS + t) * ld);
+      }
+      Anc[(2 * pr) * NT + tid] = u0[0];
+      Anc[(2 * pr + 1) * NT + tid] = u1[0];
+      float2* Dp = pr == 0 ? D01 : D23;
+#pragma unroll
+      for (int t = 1; t < NS; ++t) Dp[(t - 1) * NT + tid] = dev2(u0[t], u1[t], u0[0], u1[0]);
+    }
+    double u4[NS];
+#pragma unroll
+    for (int t = 0; t < NS; ++t) u4[t] = __ldg(ue + (size_t)(4 * NS + t) * ld);
+    Anc[4 * NT + tid] = u4[0];
+#pragma unroll
+    for (int t = 1; t < NS; ++t) D4[(t - 1) * NT + tid] = (float)(u4[t] - u4[0]);
+  }
+  __syncthreads();  // codes
+  for (int k = tid; k < 2 * TH * NF * N1; k += NT) {
+    const int side = k / (TH * NF * N1);
+    const int r = k % (TH * NF * N1);
+    const int ry = r / (NF * N1), f = (r / N1) % NF, j = r % N1;
+    const int nb = codes[side * TH + ry];
+    double v = 0.0;
+    if (nb >= 0) v = __ldg(a.U + (size_t)(f * NS + (side == 0 ? P + N1 * j : N1 * j)) * ld + nb);
+    (side == 0 ? HL : HR)[r] = v;
+  }
+  for (int k = tid; k < 2 * TW * NF * N1; k += NT) {
+    const int side = k / (TW * NF * N1);
+    const int r = k % (TW * NF * N1);
+    const int rx = r / (NF * N1), f = (r / N1) % NF, j = r % N1;
+    const int nb = codes[2 * TH + side * TW + rx];
+    double v = 0.0;
+    if (nb >= 0) v = __ldg(a.U + (size_t)(f * NS + (side == 0 ? j + N1 * P : j)) * ld + nb);
+    (side == 0 ? HD : HU)[r] = v;
+  }
+  __syncthreads();
+
+  // ---------------- phase 1: face fluxes, each face of the tile once ----------------
+  for (int k = tid; k < NXF + NYF; k += NT) {
+    // each side: FP64 value of face node 0 and FP32 deviations of face nodes 1..P from it
+    double bl[NF], br[NF];
+    float dl[NF][N1], dr[NF][N1];
+    float nxv, nyv, sgn = 1.0f;
+    int code = 0, mom, g;
+    bool first_edge;
+    // in-tile element i, face nodes t_j = t0 + j * st
+    auto side_tile = [&](int i, int t0, int st, double* b, float (*d)[N1]) {
+#pragma unroll
+      for (int f = 0; f < NF; ++f) {
+        const float d0 = ct_dev<NT>(D01, D23, D4, f, t0, i);
+        b[f] = Anc[f * NT + i] + (double)d0;
+#pragma unroll
+        for (int j = 1; j < N1; ++j) d[f][j] = ct_dev<NT>(D01, D23, D4, f, t0 + j * st, i) - d0;
+      }
+    };
+    auto side_halo = [&](const double* H, double* b, float (*d)[N1]) {
+#pragma unroll
+      for (int f = 0; f < NF; ++f) {
+        b[f] = H[f * N1];
+#pragma unroll
+        for (int j = 1; j < N1; ++j) d[f][j] = (float)(H[f * N1 + j] - H[f * N1]);
+      }
+    };
+    if (k < NXF) {
+      g = k % N1;
+      const int fy = (k / N1) % TH, fx = k / (N1 * TH);
+      if (fx == 0) code = codes[fy];
+      if (fx == TW) code = codes[TH + fy];
+      if (fx > 0) side_tile(fy * TW + fx - 1, P, N1, bl, dl);
+      else side_halo(HL + fy * NF * N1, bl, dl);
+      if (fx < TW) side_tile(fy * TW + fx, 0, N1, br, dr);
+      else side_halo(HR + fy * NF * N1, br, dr);
+      nxv = 1.0f;
+      nyv = 0.0f;
+      first_edge = fx == 0;
+      mom = 1;
+    } else {
+      const int kk = k - NXF;
+      g = kk % N1;
+      const int fx = (kk / N1) % TW, fy = kk / (N1 * TW);
+      if (fy == 0) code = codes[2 * TH + fx];
+      if (fy == TH) code = codes[2 * TH + TW + fx];
+      if (fy > 0) side_tile((fy - 1) * TW + fx, N1 * P, 1, bl, dl);
+      else side_halo(HD + fx * NF * N1, bl, dl);
+      if (fy < TH) side_tile(fy * TW + fx, 0, 1, br, dr);
+      else side_halo(HU + fx * NF * N1, br, dr);
+      nxv = 0.0f;
+      nyv = 1.0f;
+      first_edge = fy == 0;
+      mom = 2;
+    }
+    if (code < 0) {
+      // domain boundary: the inside element's state on both sides, the wall-normal momentum
+      // mirrored on reflective walls
+#pragma unroll
+      for (int f = 0; f < NF; ++f) {
+        const double ob = first_edge ? br[f] : bl[f];
+        const float sg = (code == -3 && f == mom) ? -1.f : 1.f;
+        bl[f] = ob;
+        br[f] = sg * ob;
+#pragma unroll
+        for (int j = 1; j < N1; ++j) {
+          const float od = first_edge ? dr[f][j] : dl[f][j];
+          dl[f][j] = od;
+          dr[f][j] = sg * od;
+        }
+      }
+      if (first_edge) { nxv = -nxv; nyv = -nyv; sgn = -1.0f; }
+    }
+    double L[NF], R[NF];
+#pragma unroll
+    for (int f = 0; f < NF; ++f) {
+      float2 s = make_float2(0.f, 0.f);
+#pragma unroll
+      for (int j = 1; j < N1; ++j) s = fma2(bcast2(DGB_TAB2F(P, Bf[g][j])), make_float2(dl[f][j], dr[f][j]), s);
+      L[f] = bl[f] + (double)s.x;
+      R[f] = br[f] + (double)s.y;
+    }
+    float F[NF], nc;
+    if (FLUX == phys::FLUX_ROE) {
+      double Fd[NF], ncd;
+      phys::riemann2d_rcp<FLUX>(L, R, (double)nxv, (double)nyv, Fd, ncd);
+#pragma unroll
+      for (int f = 0; f < NF; ++f) F[f] = (float)Fd[f];
+      nc = (float)ncd;
+    } else {
+      rusanov2d_mixed(L, R, nxv, nyv, F, nc);
+    }
+#pragma unroll
+    for (int f = 0; f < NF; ++f) Fs[k * 6 + f] = sgn * F[f];
+    Fs[k * 6 + 5] = nc;
+  }
+  __syncthreads();
+
+  // ---------------- phase 2: volume terms and assembly, one thread per element ----------------
+  constexpr int NG1 = Tab2<P>::NG1;
+  float2 r01[NS], r23[NS];
+  float r4[NS];
+#pragma unroll
+  for (int t = 0; t < NS; ++t) { r01[t] = r23[t] = make_float2(0.f, 0.f); r4[t] = 0.f; }
+#pragma unroll
+  for (int kf = 0; kf < 4; ++kf) {
+    int base;
+    float s, jw;
+    if (kf == 0) { base = (tx * TH + ty) * N1; s = 1.f; jw = (float)a.JFx; }
+    else if (kf == 1) { base = ((tx + 1) * TH + ty) * N1; s = -1.f; jw = (float)a.JFx; }
+    else if (kf == 2) { base = NXF + (ty * TW + tx) * N1; s = 1.f; jw = (float)a.JFy; }
+    else { base = NXF + ((ty + 1) * TW + tx) * N1; s = -1.f; jw = (float)a.JFy; }
+#pragma unroll
+    for (int g = 0; g < N1; ++g) {
+      const float* fp = Fs + (base + g) * 6;
+      const float w = jw * DGB_TAB2F(P, wf[g]);
+      const float2 c01 = make_float2(s * fp[0] * w, s * fp[1] * w), c23 = make_float2(s * fp[2] * w, s * fp[3] * w);
+      const float c4 = (s * fp[4] + fp[5]) * w;
+#pragma unroll
+      for (int j = 0; j < N1; ++j) {
+        const int t = kf == 0 ? N1 * j : kf == 1 ? P + N1 * j : kf == 2 ? j : j + N1 * P;
+        const float b = DGB_TAB2F(P, Bf[g][j]);
+        r01[t] = fma2(bcast2(b), c01, r01[t]);
+        r23[t] = fma2(bcast2(b), c23, r23[t]);
+        r4[t] = fmaf(b, c4, r4[t]);
+      }
+    }
+  }
+
+  double anc[NF];
+#pragma unroll
+  for (int f = 0; f < NF; ++f) anc[f] = Anc[f * NT + tid];
+  const float2* d01 = D01 + tid;
+  const float2* d23 = D23 + tid;
+  const float* d4 = D4 + tid;
+  const float cx = (float)a.cx, cy = (float)a.cy, cJ = (float)a.J, sx = (float)a.sx, sy = (float)a.sy;
+#pragma unroll 1
+  for (int gx = 0; gx < NG1; ++gx) {
+    float2 T01[N1], T23[N1];
+    float T4[N1], dT[N1];
+#pragma unroll
+    for (int iy = 0; iy < N1; ++iy) {
+      float2 s01 = make_float2(0.f, 0.f), s23 = make_float2(0.f, 0.f);
+      float s4 = 0.f, sd = 0.f;
+#pragma unroll
+      for (int ix = 0; ix < N1; ++ix) {
+        const int t = ix + N1 * iy;
+        if (t == 0) continue;  // the anchor's deviation is zero
+        const float2 b = bcast2(DGB_TAB2F(P, B1[gx][ix]));
+        s01 = fma2(b, d01[(t - 1) * NT], s01);
+        s23 = fma2(b, d23[(t - 1) * NT], s23);
+        const float v4 = d4[(t - 1) * NT];
+        s4 = fmaf(b.x, v4, s4);
+        sd = fmaf(DGB_TAB2F(P, D1[gx][ix]), v4, sd);
+      }
+      T01[iy] = s01;
+      T23[iy] = s23;
+      T4[iy] = s4;
+      dT[iy] = sd;
+    }
+    float2 Ax01[N1], Ax23[N1], Ay01[N1], Ay23[N1];
+    float As[N1];
+#pragma unroll
+    for (int iy = 0; iy < N1; ++iy) {
+      As[iy] = 0.f;
+      Ax01[iy] = Ax23[iy] = Ay01[iy] = Ay23[iy] = make_float2(0.f, 0.f);
+    }
+#pragma unroll
+    for (int gy = 0; gy < NG1; ++gy) {
+      const int g = gx * NG1 + gy;
+      float2 u01 = make_float2(0.f, 0.f), u23 = make_float2(0.f, 0.f);
+      float u4 = 0.f;
+      float2 dd = make_float2(0.f, 0.f);  // (d alpha / dx, d alpha / dy) on the reference element
+#pragma unroll
+      for (int iy = 0; iy < N1; ++iy) {
+        const float b = DGB_TAB2F(P, B1[gy][iy]);
+        u01 = fma2(bcast2(b), T01[iy], u01);
+        u23 = fma2(bcast2(b), T23[iy], u23);
+        u4 = fmaf(b, T4[iy], u4);
+        dd = fma2(make_float2(b, DGB_TAB2F(P, D1[gy][iy])), make_float2(dT[iy], T4[iy]), dd);
+      }
+      double ug[NF] = {anc[0] + (double)u01.x, anc[1] + (double)u01.y, anc[2] + (double)u23.x,
+                       anc[3] + (double)u23.y, anc[4] + (double)u4};
+      const float dax = dd.x, day = dd.y;
+      const double irho = __drcp_rn(ug[0]);
+      const double pd = __drcp_rn(ug[4]) * (ug[3] - 0.5 * (ug[1] * ug[1] + ug[2] * ug[2]) * irho);
+      const float uu = (float)(ug[1] * irho), vv = (float)(ug[2] * irho), Et = (float)ug[3], p = (float)pd;
+      const float wq = DGB_TAB2F(P, W[g]);
+      const float wx = wq * cx, wy = wq * cy;
+      const float mx = (float)ug[1] * wx, my = (float)ug[2] * wy;
+      const float2 gx01 = make_float2(mx, mx * uu + wx * p), gx23 = make_float2(mx * vv, wx * ((Et + p) * uu));
+      const float2 gy01 = make_float2(my, my * uu), gy23 = make_float2(my * vv + wy * p, wy * ((Et + p) * vv));
+      const float gs = (wq * cJ) * (-uu * dax * sx - vv * day * sy);
+#pragma unroll
+      for (int iy = 0; iy < N1; ++iy) {
+        const float2 b = bcast2(DGB_TAB2F(P, B1[gy][iy])), d = bcast2(DGB_TAB2F(P, D1[gy][iy]));
+        Ax01[iy] = fma2(b, gx01, Ax01[iy]);
+        Ax23[iy] = fma2(b, gx23, Ax23[iy]);
+        Ay01[iy] = fma2(d, gy01, Ay01[iy]);
+        Ay23[iy] = fma2(d, gy23, Ay23[iy]);
+        As[iy] = fmaf(b.x, gs, As[iy]);
+      }
+    }
+#pragma unroll
+    for (int iy = 0; iy < N1; ++iy)
+#pragma unroll
+      for (int ix = 0; ix < N1; ++ix) {
+        const float2 dx = bcast2(DGB_TAB2F(P, D1[gx][ix])), bx = bcast2(DGB_TAB2F(P, B1[gx][ix]));
+        const int t = ix + N1 * iy;
+        r01[t] = fma2(bx, Ay01[iy], fma2(dx, Ax01[iy], r01[t]));
+        r23[t] = fma2(bx, Ay23[iy], fma2(dx, Ax23[iy], r23[t]));
+        r4[t] = fmaf(bx.x, As[iy], r4[t]);
+      }
+  }
+  if (MODE == MODE_RESIDUAL) {
+#pragma unroll
+    for (int t = 0; t < NS; ++t) {
+      a.out[(size_t)(0 * NS + t) * ld + e] = (double)r01[t].x;
+      a.out[(size_t)(1 * NS + t) * ld + e] = (double)r01[t].y;
+      a.out[(size_t)(2 * NS + t) * ld + e] = (double)r23[t].x;
+      a.out[(size_t)(3 * NS + t) * ld + e] = (double)r23[t].y;
+      a.out[(size_t)(4 * NS + t) * ld + e] = (double)r4[t];
+    }
+    return;
+  }
+  const double dt = a.dt_override > 0 ? a.dt_override : a.scal->dt;
+  const float sc = (float)(dt * a.invJ);
+  float2 m01[NS], m23[NS];
+  float m4[NS];
+#pragma unroll
+  for (int iy = 0; iy < N1; ++iy)
+#pragma unroll
+    for (int ix = 0; ix < N1; ++ix) {
+      float2 s01 = make_float2(0.f, 0.f), s23 = make_float2(0.f, 0.f);
+      float s4 = 0.f;
+#pragma unroll
+      for (int q = 0; q < N1; ++q) {
+        const float m = DGB_TAB2F(P, M1i[ix][q]);
+        s01 = fma2(bcast2(m), r01[q + N1 * iy], s01);
+        s23 = fma2(bcast2(m), r23[q + N1 * iy], s23);
+        s4 = fmaf(m, r4[q + N1 * iy], s4);
+      }
+      m01[ix + N1 * iy] = s01;
+      m23[ix + N1 * iy] = s23;
+      m4[ix + N1 * iy] = s4;
+    }
+#pragma unroll
+  for (int iy = 0; iy < N1; ++iy)
+#pragma unroll
+    for (int ix = 0; ix < N1; ++ix) {
+      float2 s01 = make_float2(0.f, 0.f), s23 = make_float2(0.f, 0.f);
+      float s4 = 0.f;
+#pragma unroll
+      for (int q = 0; q < N1; ++q) {
+        const float m = DGB_TAB2F(P, M1i[iy][q]);
+        s01 = fma2(bcast2(m), m01[ix + N1 * q], s01);
+        s23 = fma2(bcast2(m), m23[ix + N1 * q], s23);
+        s4 = fmaf(m, m4[ix + N1 * q], s4);
+      }
+      const int t = ix + N1 * iy;
+      const double du[NF] = {(double)(sc * s01.x), (double)(sc * s01.y), (double)(sc * s23.x), (double)(sc * s23.y),
+                             (double)(sc * s4)};
+#pragma unroll
+      for (int f = 0; f < NF; ++f) {
+        const size_t gi = (size_t)(f * NS + t) * ld + e;
+        if (MODE == MODE_SSP) {
+          const double base = a.a != 0.0 ? a.a * __ldg(a.Ubase + gi) : 0.0;
+          a.out[gi] = base + a.b * (__ldg(a.U + gi) + du[f]);
+        } else {
+          a.out[gi] = du[f];
+          if (a.Uacc) a.Uacc[gi] = a.Uacc[gi] + a.b * du[f];
+        }
+      }
+    }
+}
+
+}  // namespace dgb

@@ -236,6 +236,22 @@ void launch_tile2d(dgb_ctx* c, const StageArgs& s) {
 template <int P, int FLUX, int MODE>
 void launch_tile2d_mixed(dgb_ctx* c, const StageArgs& s) {
   constexpr int TH = tile_h_for(P);
+  if (c->mixed_ct) {
+    constexpr size_t smem = TileDimsMixedCT<P, TILE_W, TH>::smem_bytes;
+    auto k3 = residual2d_tile_mixed_ct_kernel<P, FLUX, MODE, TILE_W, TH, 3>;
+    auto k4 = residual2d_tile_mixed_ct_kernel<P, FLUX, MODE, TILE_W, TH, 4>;
+    static bool attr = false;
+    if (!attr) {
+      cudaFuncSetAttribute(k3, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+      cudaFuncSetAttribute(k4, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+      attr = true;
+    }
+    const TileArgs a = tile_args(c, s);
+    dim3 grid(c->nx / TILE_W, c->ny / TH);
+    ProfScope ps(c, KC_RESIDUAL);
+    (c->mixed_minb == 3 ? k3 : k4)<<<grid, TILE_W * TH, smem, c->st>>>(a);
+    return;
+  }
   constexpr size_t smem = TileDimsMixed<P, TILE_W, TH>::smem_bytes;
   auto k = residual2d_tile_mixed_kernel<P, FLUX, MODE, TILE_W, TH>;
   static bool attr = false;
@@ -944,6 +960,12 @@ extern "C" int dgb_create(const dgb_problem* prob, int device, dgb_ctx** out) {
     // FP64 tensor rate equals its FP64 vector rate)
     const char* tk = std::getenv("DGB_TILE_KERNEL");
     c->tile_dmma = tk && std::string(tk) == "dmma";
+    // mixed-form tiles: DGB_MIXED_TILE=ct selects the compressed shared tile (FP64 anchors + FP32
+    // deviations, plain loads), otherwise the TMA-loaded FP64 tile
+    const char* mk = std::getenv("DGB_MIXED_TILE");
+    c->mixed_ct = mk && std::string(mk) == "ct";
+    const char* mb = std::getenv("DGB_MIXED_CT_MINB");
+    c->mixed_minb = mb && std::string(mb) == "3" ? 3 : 4;
   }
   c->D = P.D; c->p = P.p; c->nf = P.N_F; c->ns = P.N_s; c->ne = P.N_E;
   c->ld = (P.N_E + 63) / 64 * 64;

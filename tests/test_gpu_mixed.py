@@ -125,3 +125,32 @@ def test_mixed_form_on_a_grid_with_strips():
     finally:
         ref.close()
         mix.close()
+
+
+@pytest.mark.parametrize("flux,order", [("rusanov", 2), ("roe", 2), ("roe", 3)])
+def test_compressed_tile_kernel_close_to_tma_tile_kernel(flux, order, monkeypatch):
+    """The mixed kernel whose shared tile holds FP64 anchors and FP32 deviations
+    (DGB_MIXED_TILE=ct) against the mixed kernel that keeps the TMA-loaded FP64 tile
+    (DGB_MIXED_TILE=tma): the volume terms read the same FP32 deviations; only the FP64 base of a
+    face trace differs, by the FP32 rounding of one deviation.  Residual and 10 SSP-RK3 steps, per
+    field."""
+    import dg_b200 as dgb
+    prob = dgb.Problem.structured(2, order, 64, 32, 0.0, 2.0, 0.0, 1.0, WALLS, flux=flux, limiter="m2l", cfl=0.3)
+    U0, out = None, {}
+    for mode in ("tma", "ct"):
+        monkeypatch.setenv("DGB_MIXED_TILE", mode)  # read when the context is created
+        s = dgb.DGSolver(prob)
+        try:
+            if U0 is None:
+                U0 = s.limit(perturbed_state(prob, "shock_bubble", 5))
+            s.set_form("mixed")
+            f = s.dg_solver(U0)
+            s.set_state(U0)
+            s.advance(10, 0.0, scheme=dgb.SSPRK3)
+            out[mode] = (f, s.get_state())
+        finally:
+            s.close()
+    err_f = per_field(out["ct"][0], out["tma"][0], prob.info)
+    err_u = per_field(out["ct"][1], out["tma"][1], prob.info, norm="l1")
+    print(f"compressed vs TMA tile ({flux}, p={order}): residual {err_f}, 10 steps L1 {err_u}")
+    assert max(err_f) < 1e-6 and max(err_u) < 1e-7
