@@ -580,9 +580,9 @@ def slab_local(dgb, dev, steps=10, warmup=3):
     ref = whole.get_state()
     whole.close()
     out["whole_ms_per_step"] = ms / steps
-    for ns in (2, 4):
+    for ns, captured in ((2, True), (4, True), (2, False)):
         dec = S.Decomposition(ORDER, NX, NY, ns, x0, x1, y0, y1, BC, flux="rusanov", limiter="m2l", cfl=CFL)
-        run = S.SlabRun(dec, range(ns), S.LocalTransport(), device=dev)
+        run = S.SlabRun(dec, range(ns), S.LocalTransport(captured=captured), device=dev)
         try:
             run.set_global_state(U0)
             run.advance(warmup, 0.0, scheme=dgb.SSPRK3)
@@ -594,8 +594,11 @@ def slab_local(dgb, dev, steps=10, warmup=3):
             got = run.global_state()
         finally:
             run.close()
-        out[f"slabs_{ns}"] = {"rows": [r1 - r0 for r0, r1 in dec.ranges], "ms_per_step_wall": wall,
-                              "max_abs_diff_vs_whole": float(np.abs(got - ref).max())}
+        out[f"slabs_{ns}" + ("" if captured else "_eager")] = {
+            "rows": [r1 - r0 for r0, r1 in dec.ranges], "ms_per_step_wall": wall,
+            "step": "one captured graph per step (dgb_slabs_advance_local)" if captured
+            else "phase-level step driven from Python, eager launches",
+            "max_abs_diff_vs_whole": float(np.abs(got - ref).max())}
     return out
 
 

@@ -32,7 +32,7 @@ EXPORTS = [
     "dgb_batch_autotune", "dgb_batch_set_tuning", "dgb_batch_advance", "dgb_problem_error_norms", "dgb_batch_case_stats",
     "dgb_batch_last_timing", "dgb_slab_ghost_rows", "dgb_step_begin", "dgb_step_wavespeed_word", "dgb_step_stage",
     "dgb_step_end", "dgb_halo_count", "dgb_halo_pack", "dgb_halo_unpack", "dgb_stream", "dgb_set_cfl_scale",
-    "dgb_set_wait_limit", "dgb_set_indicator_interval",
+    "dgb_set_wait_limit", "dgb_set_indicator_interval", "dgb_slabs_advance_local",
 ]
 
 
@@ -135,6 +135,7 @@ def lib() -> C.CDLL:
         "dgb_halo_unpack": [vp, ip, vp],
         "dgb_stream": [vp, C.POINTER(vp)],
         "dgb_set_cfl_scale": [vp, C.c_double],
+        "dgb_slabs_advance_local": [C.POINTER(vp), ip, ip, ip, ip, C.c_double, dp],
     }
     for name, args in sig.items():
         f = getattr(L, name)

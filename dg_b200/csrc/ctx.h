@@ -51,7 +51,6 @@ struct dgb_ctx {
   int sm_count = 148;           // multiprocessors of the device
   bool ind_on = false;          // learned indicator gates the limiter (dgb_set_indicator)
   bool mixed_ct = false;        // mixed form: the compressed-tile kernel (else the TMA-tile kernel)
-  int mixed_minb = 4;           // ... its CTAs per SM in the launch bounds (3 or 4)
   bool tile_dmma = false;       // p = 2 FP64 stages: the DMMA residual (else the scalar tiled kernel)
   bool ind_tc = true;           // scoring GEMMs on tcgen05 (else the mma.sync kernel)
   float ind_threshold = 0.2f;
@@ -83,7 +82,10 @@ struct dgb_ctx {
   int ind_every = 1;       // steps between scorings of the learned indicator (1: every step)
   long long ind_step = 0;  // steps taken since the last dgb_set_state / dgb_set_indicator
   // destroys the captured steps (their kernel arguments or launch sequence changed)
+  unsigned graph_gen = 0;   // counts drop_graphs calls (captured slab steps compare it)
+  double* halo_send[2] = {nullptr, nullptr};  // slab mode, local exchange: packed owned rows per side
   void drop_graphs() {
+    ++graph_gen;
     for (auto& a : graphs)
       for (auto& b : a)
         for (auto& g : b)

@@ -409,10 +409,10 @@ namespace dgb {
 // ---------------------------------------------------------------------------------------------
 // Compressed-tile variant of the mixed kernel.  The shared tile holds, per element, the FP64
 // anchors (node-0 values of the five fields) and the FP32 deviations of the other nodes from them
-// -- 200 instead of 360 bytes per element at p = 2 -- written by each thread for its own element
-// from plain coalesced loads.  Collocation then reads its FP32 operands straight from shared memory
-// (no FP64 subtraction and conversion per quadrature column), the CTA fits in ~55 KB at p = 2 (four
-// CTAs per SM instead of three), and the stage update re-reads the FP64 stage input through L2.
+// -- 200 instead of 360 bytes per element at p = 2, 344 instead of 640 at p = 3 -- written by each
+// thread for its own element from plain coalesced loads.  Collocation then reads its FP32 operands
+// straight from shared memory (no FP64 subtraction and conversion per quadrature column), the CTA
+// needs less shared memory, and the stage update re-reads the FP64 stage input through L2.
 // The face traces are formed from the same anchors and deviations: the FP64 value of the face's
 // first node plus an FP32 contraction of the other nodes' deviations from it, as in the TMA-tile
 // kernel.
@@ -440,8 +440,15 @@ __device__ __forceinline__ float ct_dev(const float2* d01, const float2* d23, co
   return f == 0 ? d01[r].x : f == 1 ? d01[r].y : f == 2 ? d23[r].x : f == 3 ? d23[r].y : d4[r];
 }
 
-template <int P, int FLUX, int MODE, int TW, int TH, int MINB>
-__global__ void __launch_bounds__(TW * TH, MINB)
+// p = 3 (32 x 2 tiles, 64 threads): 48 KB of shared memory instead of 66 KB, four CTAs per SM
+// instead of three, measured 11.3 -> 10.3 ms per step at 2048 x 1024.  p = 2: four 128-thread CTAs
+// would cap the kernel at 128 registers (260 bytes of spills; measured slower), three run no faster
+// than the TMA-tile kernel, which stays the default there.
+template <int P>
+constexpr int mixed_ct_min_blocks() { return P == 3 ? 4 : 3; }
+
+template <int P, int FLUX, int MODE, int TW, int TH>
+__global__ void __launch_bounds__(TW * TH, mixed_ct_min_blocks<P>())
     residual2d_tile_mixed_ct_kernel(const TileArgs a) {
   using Dm = TileDimsMixedCT<P, TW, TH>;
   constexpr int N1 = Dm::N1, NS = Dm::NS, NF = 5, NT = Dm::NT, NXF = Dm::NXF, NYF = Dm::NYF;

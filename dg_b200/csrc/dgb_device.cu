@@ -11,6 +11,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
+#include <algorithm>
 #include <cstring>
 #include <string>
 #include <vector>
@@ -238,18 +239,13 @@ void launch_tile2d_mixed(dgb_ctx* c, const StageArgs& s) {
   constexpr int TH = tile_h_for(P);
   if (c->mixed_ct) {
     constexpr size_t smem = TileDimsMixedCT<P, TILE_W, TH>::smem_bytes;
-    auto k3 = residual2d_tile_mixed_ct_kernel<P, FLUX, MODE, TILE_W, TH, 3>;
-    auto k4 = residual2d_tile_mixed_ct_kernel<P, FLUX, MODE, TILE_W, TH, 4>;
+    auto k = residual2d_tile_mixed_ct_kernel<P, FLUX, MODE, TILE_W, TH>;
     static bool attr = false;
-    if (!attr) {
-      cudaFuncSetAttribute(k3, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-      cudaFuncSetAttribute(k4, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-      attr = true;
-    }
+    if (!attr) { cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem); attr = true; }
     const TileArgs a = tile_args(c, s);
     dim3 grid(c->nx / TILE_W, c->ny / TH);
     ProfScope ps(c, KC_RESIDUAL);
-    (c->mixed_minb == 3 ? k3 : k4)<<<grid, TILE_W * TH, smem, c->st>>>(a);
+    k<<<grid, TILE_W * TH, smem, c->st>>>(a);
     return;
   }
   constexpr size_t smem = TileDimsMixed<P, TILE_W, TH>::smem_bytes;
@@ -960,12 +956,11 @@ extern "C" int dgb_create(const dgb_problem* prob, int device, dgb_ctx** out) {
     // FP64 tensor rate equals its FP64 vector rate)
     const char* tk = std::getenv("DGB_TILE_KERNEL");
     c->tile_dmma = tk && std::string(tk) == "dmma";
-    // mixed-form tiles: DGB_MIXED_TILE=ct selects the compressed shared tile (FP64 anchors + FP32
-    // deviations, plain loads), otherwise the TMA-loaded FP64 tile
+    // mixed-form tiles: the compressed shared tile (FP64 anchors + FP32 deviations, plain loads)
+    // at p = 3, the TMA-loaded FP64 tile at p = 1, 2 (the faster of the two at each order);
+    // DGB_MIXED_TILE=ct / tma selects one for every order
     const char* mk = std::getenv("DGB_MIXED_TILE");
-    c->mixed_ct = mk && std::string(mk) == "ct";
-    const char* mb = std::getenv("DGB_MIXED_CT_MINB");
-    c->mixed_minb = mb && std::string(mb) == "3" ? 3 : 4;
+    c->mixed_ct = mk ? std::string(mk) == "ct" : P.p == 3;
   }
   c->D = P.D; c->p = P.p; c->nf = P.N_F; c->ns = P.N_s; c->ne = P.N_E;
   c->ld = (P.N_E + 63) / 64 * 64;
@@ -1102,11 +1097,17 @@ extern "C" int dgb_create(const dgb_problem* prob, int device, dgb_ctx** out) {
   return DGB_OK;
 }
 
+namespace dgb {
+void drop_slab_graphs(dgb_ctx* c);
+}
+
 extern "C" void dgb_destroy(dgb_ctx* c) {
   if (!c) return;
   cudaSetDevice(c->device);
   if (c->st) cudaStreamSynchronize(c->st);
   c->drop_graphs();
+  dgb::drop_slab_graphs(c);
+  for (double* b : c->halo_send) if (b) cudaFree(b);
   for (double* b : {c->A, c->B, c->C, c->DU, c->X, c->ref}) if (b) cudaFree(b);
   if (c->nbr) cudaFree(c->nbr);
   if (c->left) cudaFree(c->left);
@@ -1634,6 +1635,230 @@ extern "C" int dgb_halo_unpack(dgb_ctx* c, int side, const double* src_dev) {
   if (side != 0 && side != 1) return set_error(DGB_ERR_ARG, "side is 0 (bottom) or 1 (top)");
   double* src = const_cast<double*>(src_dev);
   return side == 0 ? halo_copy(c, 0, c->halo_lo, src, false) : halo_copy(c, c->ny - c->halo_hi, c->halo_hi, src, false);
+}
+
+// ------------------------------------------------------------------------------------------
+// Slab mode in one process: every slab context of the grid on this device, advanced together by one
+// CUDA graph per step.  The graph holds every slab's CFL reduction, the MAX of their wave speeds,
+// and per stage the halo exchange (each slab packs the owned rows next to its ghost sides into its
+// own send buffer, each slab then copies its neighbours' send buffers into its ghost rows) and the
+// stage itself.  Ordering is by graph edges only: a slab unpacks after its neighbours packed, and
+// packs again after its neighbours unpacked.  Captured once per (slabs, scheme, CFL / fixed step),
+// dropped when any slab's own captured steps are.
+namespace {
+constexpr int kMaxLocalSlabs = 16;
+struct SlabGraph {
+  std::vector<dgb_ctx*> ctx;
+  std::vector<unsigned> gen;
+  int scheme = 0;
+  bool cfl = false, periodic = false;
+  cudaGraphExec_t exec = nullptr;
+  long long launches = 0;
+};
+std::vector<SlabGraph> g_slab_graphs;
+
+struct UmaxWords {
+  unsigned long long* w[kMaxLocalSlabs];
+  int n;
+};
+// MAX of the slabs' wave-speed words (bits of non-negative doubles order as integers), written back
+// to every word
+__global__ void umax_all_kernel(UmaxWords p) {
+  unsigned long long m = 0;
+  for (int i = 0; i < p.n; ++i) m = max(m, *p.w[i]);
+  for (int i = 0; i < p.n; ++i) *p.w[i] = m;
+}
+
+int slab_below(int i, int n, bool periodic) { return i > 0 ? i - 1 : (periodic && n > 1 ? n - 1 : -1); }
+int slab_above(int i, int n, bool periodic) { return i < n - 1 ? i + 1 : (periodic && n > 1 ? 0 : -1); }
+
+// one step of all slabs into a graph, captured from the first slab's stream
+int capture_slab_step(dgb_ctx* const* s, int n, bool periodic, int scheme, bool cfl, cudaGraphExec_t* exec,
+                      long long* launches) {
+  cudaStream_t s0 = s[0]->st;
+  std::vector<cudaEvent_t> ev(3 * n + 1, nullptr);
+  for (auto& e : ev) DGB_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+  cudaEvent_t fork = ev[3 * n];
+  auto destroy_events = [&]() { for (auto e : ev) cudaEventDestroy(e); };
+  DGB_CUDA(cudaStreamBeginCapture(s0, cudaStreamCaptureModeThreadLocal));
+  const int rc = [&]() -> int {
+    auto fork_all = [&]() -> int {
+      DGB_CUDA(cudaEventRecord(fork, s0));
+      for (int i = 1; i < n; ++i) DGB_CUDA(cudaStreamWaitEvent(s[i]->st, fork, 0));
+      return DGB_OK;
+    };
+    auto join_all = [&]() -> int {
+      for (int i = 1; i < n; ++i) {
+        DGB_CUDA(cudaEventRecord(ev[i], s[i]->st));
+        DGB_CUDA(cudaStreamWaitEvent(s0, ev[i], 0));
+      }
+      return DGB_OK;
+    };
+    auto after = [&](int i, cudaEvent_t* set, int nb) -> int {  // stream of slab i waits for set[nb]
+      if (nb >= 0 && nb != i) DGB_CUDA(cudaStreamWaitEvent(s[i]->st, set[nb], 0));
+      return DGB_OK;
+    };
+    if (int r = fork_all()) return r;
+    for (int i = 0; i < n; ++i) {
+      dgb_ctx* c = s[i];
+      c->counter = 0;
+      c->slab_scheme = scheme;
+      c->slab_next = 0;
+      c->slab_cur = c->A;
+      c->slab_cfl = cfl;
+      if (cfl) launch_wavespeed(c, c->A);  // owned rows only
+    }
+    if (cfl && n > 1) {
+      if (int r = join_all()) return r;
+      UmaxWords w{};
+      w.n = n;
+      for (int i = 0; i < n; ++i) w.w[i] = &s[i]->scal->umax;
+      umax_all_kernel<<<1, 1, 0, s0>>>(w);
+      ++s[0]->counter;
+      DGB_CUDA(cudaGetLastError());
+      if (int r = fork_all()) return r;
+    }
+    cudaEvent_t* packed = ev.data();
+    cudaEvent_t* unpacked = ev.data() + n;
+    for (int k = 0; k < nstages(scheme); ++k) {
+      for (int i = 0; i < n; ++i) {
+        dgb_ctx* c = s[i];
+        if (int r = halo_copy(c, c->halo_lo, c->halo_lo, c->halo_send[0], true)) return r;
+        if (int r = halo_copy(c, c->ny - 2 * c->halo_hi, c->halo_hi, c->halo_send[1], true)) return r;
+        DGB_CUDA(cudaEventRecord(packed[i], c->st));
+      }
+      for (int i = 0; i < n; ++i) {
+        dgb_ctx* c = s[i];
+        const int b = slab_below(i, n, periodic), a = slab_above(i, n, periodic);
+        if (int r = after(i, packed, b)) return r;
+        if (int r = after(i, packed, a)) return r;
+        if (b >= 0)
+          if (int r = halo_copy(c, 0, c->halo_lo, s[b]->halo_send[1], false)) return r;
+        if (a >= 0)
+          if (int r = halo_copy(c, c->ny - c->halo_hi, c->halo_hi, s[a]->halo_send[0], false)) return r;
+        DGB_CUDA(cudaEventRecord(unpacked[i], c->st));
+      }
+      for (int i = 0; i < n; ++i) {  // the neighbours have read this slab's send buffers
+        if (int r = after(i, unpacked, slab_below(i, n, periodic))) return r;
+        if (int r = after(i, unpacked, slab_above(i, n, periodic))) return r;
+      }
+      for (int i = 0; i < n; ++i)
+        if (int r = dgb_step_stage(s[i], k)) return r;
+    }
+    return join_all();
+  }();
+  cudaGraph_t g = nullptr;
+  const cudaError_t ec = cudaStreamEndCapture(s0, &g);
+  long long nl = 0;
+  for (int i = 0; i < n; ++i) {
+    nl += s[i]->counter;
+    s[i]->slab_next = -1;
+    s[i]->slab_cur = nullptr;
+  }
+  destroy_events();
+  if (rc || ec != cudaSuccess) {
+    if (g) cudaGraphDestroy(g);
+    if (rc) return rc;
+    return set_error(DGB_ERR_CUDA, std::string("slab step capture: ") + cudaGetErrorString(ec));
+  }
+  const cudaError_t ei = cudaGraphInstantiate(exec, g, 0);
+  cudaGraphDestroy(g);
+  if (ei != cudaSuccess) return set_error(DGB_ERR_CUDA, std::string("slab step graph: ") + cudaGetErrorString(ei));
+  *launches = nl;
+  return DGB_OK;
+}
+}  // namespace
+
+void dgb::drop_slab_graphs(dgb_ctx* c) {
+  for (size_t i = 0; i < g_slab_graphs.size();) {
+    SlabGraph& g = g_slab_graphs[i];
+    if (std::find(g.ctx.begin(), g.ctx.end(), c) != g.ctx.end()) {
+      if (g.exec) cudaGraphExecDestroy(g.exec);
+      g_slab_graphs.erase(g_slab_graphs.begin() + i);
+    } else {
+      ++i;
+    }
+  }
+}
+
+extern "C" int dgb_slabs_advance_local(dgb_ctx* const* slabs, int n, int periodic, int scheme, int nsteps, double dt,
+                                       double* time) {
+  if (!slabs || n < 1 || n > kMaxLocalSlabs) return set_error(DGB_ERR_ARG, "1 to 16 slab contexts");
+  if (scheme != DGB_SSPRK3 && scheme != DGB_RK4) return set_error(DGB_ERR_ARG, "scheme must be 3 or 4");
+  if (nsteps < 0) return set_error(DGB_ERR_ARG, "nsteps < 0");
+  const bool cfl = !(dt > 0), per = periodic != 0;
+  for (int i = 0; i < n; ++i) {
+    dgb_ctx* c = slabs[i];
+    if (!c) return set_error(DGB_ERR_ARG, "null slab context");
+    if (c->device != slabs[0]->device) return set_error(DGB_ERR_ARG, "the slabs of a local run share one device");
+    if (c->nx != slabs[0]->nx || c->nf != slabs[0]->nf || c->ns != slabs[0]->ns)
+      return set_error(DGB_ERR_ARG, "the slabs of one grid have the same nx, fields and nodes");
+    for (int j = 0; j < i; ++j)
+      if (slabs[j] == c) return set_error(DGB_ERR_ARG, "a slab context appears twice");
+    if (c->ind_on) return set_error(DGB_ERR_UNSUPPORTED, "slab mode does not take the learned indicator");
+    if (c->slab_next >= 0) return set_error(DGB_ERR_ARG, "a phase-level step is open on a slab");
+    if (c->prof) return set_error(DGB_ERR_UNSUPPORTED, "profiling times eager launches: use the phase-level step");
+    if (cfl && !(c->cs.cfl_scaled > 0)) return set_error(DGB_ERR_ARG, "no fixed dt and no positive CFL");
+    const int b = slab_below(i, n, per), a = slab_above(i, n, per);
+    if ((b < 0) != (c->halo_lo == 0) || (a < 0) != (c->halo_hi == 0) || (b >= 0 && slabs[b]->halo_hi != c->halo_lo) ||
+        (a >= 0 && slabs[a]->halo_lo != c->halo_hi))
+      return set_error(DGB_ERR_ARG, "ghost rows do not match the slab order (dgb_slab_ghost_rows)");
+  }
+  DGB_CUDA(cudaSetDevice(slabs[0]->device));
+  for (int i = 0; i < n; ++i)
+    for (int side = 0; side < 2; ++side) {
+      dgb_ctx* c = slabs[i];
+      const int g = side == 0 ? c->halo_lo : c->halo_hi;
+      if (g && !c->halo_send[side])
+        DGB_CUDA(cudaMalloc(&c->halo_send[side], (size_t)g * c->nx * c->nf * c->ns * sizeof(double)));
+    }
+  SlabGraph* sg = nullptr;
+  for (auto& g : g_slab_graphs) {
+    if (g.scheme != scheme || g.cfl != cfl || g.periodic != per || (int)g.ctx.size() != n) continue;
+    bool same = true;
+    for (int i = 0; i < n && same; ++i) same = g.ctx[i] == slabs[i] && g.gen[i] == slabs[i]->graph_gen;
+    if (same) { sg = &g; break; }
+  }
+  if (!sg && nsteps > 0) {
+    for (int i = 0; i < n; ++i) drop_slab_graphs(slabs[i]);  // stale captures of these slabs
+    SlabGraph g;
+    g.ctx.assign(slabs, slabs + n);
+    for (int i = 0; i < n; ++i) g.gen.push_back(slabs[i]->graph_gen);
+    g.scheme = scheme;
+    g.cfl = cfl;
+    g.periodic = per;
+    if (int rc = capture_slab_step(slabs, n, per, scheme, cfl, &g.exec, &g.launches)) return rc;
+    g_slab_graphs.push_back(g);
+    sg = &g_slab_graphs.back();
+  }
+  dgb_ctx* c0 = slabs[0];
+  // every slab's scalars reset once (flags clear, time 0, the fixed step), then the steps replayed
+  // on the first slab's stream; the other streams wait for it before their next work
+  for (int i = 0; i < n; ++i) {
+    if (int rc = reset_scalars(slabs[i], cfl ? 0.0 : dt)) return rc;
+    if (i) {
+      DGB_CUDA(cudaEventRecord(slabs[i]->e0, slabs[i]->st));
+      DGB_CUDA(cudaStreamWaitEvent(c0->st, slabs[i]->e0, 0));
+    }
+  }
+  DGB_CUDA(cudaEventRecord(c0->e0, c0->st));
+  for (int s = 0; s < nsteps; ++s) DGB_CUDA(cudaGraphLaunch(sg->exec, c0->st));
+  DGB_CUDA(cudaEventRecord(c0->e1, c0->st));
+  for (int i = 1; i < n; ++i) DGB_CUDA(cudaStreamWaitEvent(slabs[i]->st, c0->e1, 0));
+  unsigned flags = 0;
+  for (int i = 0; i < n; ++i) {
+    if (int rc = read_scalars(slabs[i])) return rc;
+    flags |= slabs[i]->h_scal->flags;
+  }
+  float ms = 0;
+  cudaEventElapsedTime(&ms, c0->e0, c0->e1);
+  c0->last_ms = ms;
+  c0->last_launches = sg ? sg->launches * nsteps : 0;
+  if (time) *time += c0->h_scal->time;
+  if (flags & FLAG_TIMEOUT) return set_error(DGB_ERR_TIMEOUT, "a bounded device wait expired");
+  if (flags & FLAG_NONFINITE) return set_error(DGB_ERR_NONFINITE, "time step is NaN");
+  if (flags & FLAG_DT_SMALL) return set_error(DGB_ERR_DT_SMALL, "next time step is too small (< 1e-14)");
+  return DGB_OK;
 }
 
 extern "C" int dgb_stream(dgb_ctx* c, void** stream) {

@@ -190,7 +190,25 @@ class Slab:
 class LocalTransport:
     """Every slab in this process (one device): rows move by device-to-device copies ordered by
     CUDA events between the slabs' streams -- a slab unpacks after its neighbours have packed, and
-    packs again only after its neighbours have unpacked -- with no host synchronisation."""
+    packs again only after its neighbours have unpacked -- with no host synchronisation.
+
+    captured=True (default): SlabRun.advance hands the whole sequence to the library
+    (dgb_slabs_advance_local), which captures one step of every slab, exchanges included, into one
+    CUDA graph and replays it; captured=False drives the phase-level step from here, eagerly."""
+
+    def __init__(self, captured: bool = True):
+        self.captured = captured
+
+    def advance(self, run: "SlabRun", nsteps: int, dt: float, scheme: int) -> float:
+        """nsteps steps of every slab through the library's captured local step; the time advanced."""
+        import ctypes as C
+        n = len(run.slabs)
+        order = sorted(run.slabs, key=lambda s: s.index)
+        handles = (C.c_void_p * n)(*[s.solver._h.value for s in order])
+        t = C.c_double(0.0)
+        F.check(F.lib().dgb_slabs_advance_local(handles, n, int(run.dec.periodic), int(scheme), int(nsteps),
+                                                float(dt), C.byref(t)))
+        return t.value
 
     def exchange(self, run: "SlabRun") -> None:
         packed = {}
@@ -354,6 +372,8 @@ class SlabRun:
     def advance(self, nsteps: int, dt: float = 0.0, scheme: int = F.SSPRK3) -> float:
         """nsteps steps of the whole grid (dt <= 0: the CFL step of the whole grid); returns the
         time advanced.  Raises DGBError on every rank when any slab's step failed."""
+        if getattr(self.transport, "captured", False) and len(self.slabs) == self.dec.nslabs:
+            return self.transport.advance(self, nsteps, dt, scheme)
         nst = 4 if scheme == F.RK4 else 3
         t = 0.0
         for _ in range(nsteps):

@@ -251,6 +251,15 @@ int dgb_halo_count(dgb_ctx* c, int side, size_t* n);
 int dgb_halo_pack(dgb_ctx* c, int side, double* dst_dev);
 int dgb_halo_unpack(dgb_ctx* c, int side, const double* src_dev);
 int dgb_stream(dgb_ctx* c, void** stream);  /* the context's cudaStream_t */
+/* Every slab of one grid in this process on one device (slabs[0] the bottom slab, in order;
+ * periodic != 0: the bottom and top slabs are neighbours), advanced nsteps steps together: the
+ * phase-level sequence above with the ghost rows copied device to device between the slabs, one
+ * CUDA graph per step (captured on the first call for these slabs, scheme and step kind) replayed
+ * on slabs[0]'s stream.  Same arithmetic as the phase-level step; *time += the time advanced,
+ * dgb_last_timing(slabs[0]) gives the device time.  No reference counterpart: the reference
+ * exchanges ghosts through MPI (communicator_cpu.cc:14-59). */
+int dgb_slabs_advance_local(dgb_ctx* const* slabs, int n, int periodic, int scheme, int nsteps, double dt,
+                            double* time);
 
 /* Conserved totals sum_e sum_g U_g J w_g per field (DG_SOLVER::conservation, dg_solver.h:367). */
 int dgb_conservation(dgb_ctx* c, double* totals /* N_F */);

@@ -65,8 +65,32 @@ def test_slabs_reproduce_the_whole_grid(case):
 
 
 class NoExchange(S.LocalTransport):
+    def __init__(self):
+        super().__init__(captured=False)  # the phase-level step driven from here, without exchanges
+
     def exchange(self, run):
         pass
+
+
+@pytest.mark.parametrize("case", CASES[:2], ids=[c[0] for c in CASES[:2]])
+def test_captured_local_step_equals_the_eager_phase_level_step(case):
+    """dgb_slabs_advance_local (one graph per step of every slab) against the same slabs driven
+    phase by phase from Python: the same arithmetic, bit for bit, and the same time."""
+    dec, prob, U0, whole = setup(case)
+    whole.close()
+    scheme, dt, steps = case[9], case[10], case[11]
+    out = {}
+    for captured in (False, True):
+        run = S.SlabRun(dec, range(dec.nslabs), S.LocalTransport(captured=captured))
+        try:
+            run.set_global_state(U0)
+            t = run.advance(steps, dt, scheme=scheme)
+            t += run.advance(1, dt, scheme=scheme)  # a second call replays the captured step
+            out[captured] = (t, run.global_state())
+        finally:
+            run.close()
+    assert out[True][0] == out[False][0]
+    assert np.array_equal(out[True][1], out[False][1])
 
 
 def test_without_the_exchange_the_slabs_drift():
