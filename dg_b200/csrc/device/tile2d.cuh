@@ -73,9 +73,15 @@ struct TileDims {
   static constexpr size_t tile_doubles = (size_t)NF * NS * NT;
   static constexpr uint32_t tile_bytes = (uint32_t)(tile_doubles * 8);
   static constexpr size_t halo_doubles = (size_t)2 * TH * NF * N1 + (size_t)2 * TW * NF * N1;
-  static constexpr size_t face_doubles = (size_t)(NF + 1) * (NXF + NYF);  // NF fluxes + ncterm per point
-  // the face buffer is reused for the prefetched stage base, so it is at least one tile
-  static constexpr size_t fbuf_doubles = face_doubles > tile_doubles ? face_doubles : tile_doubles;
+  // p = 3: the x-faces and then the y-faces pass through one face buffer, and the stage base is read
+  // from global memory in the epilogue instead of being prefetched into it -- 70 instead of 93 KB
+  // per 64-thread CTA, three CTAs per SM instead of two
+  static constexpr bool split_faces = P == 3;
+  static constexpr int NFREC = split_faces ? (NXF > NYF ? NXF : NYF) : NXF + NYF;  // face records held
+  static constexpr size_t face_doubles = (size_t)(NF + 1) * NFREC;  // NF fluxes + ncterm per point
+  // otherwise the face buffer is reused for the prefetched stage base, so it is at least one tile
+  static constexpr size_t fbuf_doubles =
+      split_faces || face_doubles > tile_doubles ? face_doubles : tile_doubles;
   // byte offsets; every region a TMA copy lands in starts on a 128-byte boundary
   static constexpr size_t off_tile = head_bytes + code_bytes;
   static constexpr size_t off_halo = off_tile + (tile_doubles * 8 + 127) / 128 * 128;
@@ -109,14 +115,15 @@ constexpr bool kSfLift = DGB_SF_LIFT != 0;
 // (left/bottom state first, +x/+y normal).  Record k of Fs holds the NF fluxes and the ncterm;
 // boundary faces seen from the right/top element store -F so that every consumer forms (+F + nc)
 // on its left/bottom face and (-F + nc) on its right/top face.
+// Work items k0 <= k < k1 (x-faces first, then y-faces); item k goes to record k - rec0.
 template <int P, int FLUX, int TW, int TH, int NY, bool GC>
 __device__ __forceinline__ void tile_face_fluxes(const double* Us, const double* HL, const double* HR,
                                                  const double* HD, const double* HU, const int* codes, double* Fs,
-                                                 int tid, int nthr) {
+                                                 int tid, int nthr, int k0, int k1, int rec0) {
   using Dm = TileDims<P, TW, TH, NY>;
-  constexpr int N1 = Dm::N1, NS = Dm::NS, NF = Dm::NF, NT = Dm::NT, NXF = Dm::NXF, NYF = Dm::NYF;
+  constexpr int N1 = Dm::N1, NS = Dm::NS, NF = Dm::NF, NT = Dm::NT, NXF = Dm::NXF;
   constexpr int FS = NF + 1;
-  for (int k = tid; k < NXF + NYF; k += nthr) {
+  for (int k = k0 + tid; k < k1; k += nthr) {
     double L[NF], R[NF];
     double nxv, nyv, sgn = 1.0;
     double vl[NF][N1], vr[NF][N1];
@@ -185,8 +192,8 @@ __device__ __forceinline__ void tile_face_fluxes(const double* Us, const double*
     // boundary faces seen from the right/top element store -F so that every consumer forms
     // (+F + nc) on its left/bottom face and (-F + nc) on its right/top face
 #pragma unroll
-    for (int f = 0; f < NF; ++f) Fs[k * FS + f] = sgn * F[f];
-    Fs[k * FS + NF] = nc;
+    for (int f = 0; f < NF; ++f) Fs[(k - rec0) * FS + f] = sgn * F[f];
+    Fs[(k - rec0) * FS + NF] = nc;
   }
 }
 
@@ -318,13 +325,15 @@ __device__ __forceinline__ void tile2d_body(const TileArgs& a, const CUtensorMap
 
   const int tid = threadIdx.x;
   const int ld = a.ld, nx = a.nx;
-  constexpr bool kPrefetch = MODE != MODE_RESIDUAL;
+  constexpr bool kSplit = Dm::split_faces;
+  constexpr bool kPrefetch = MODE != MODE_RESIDUAL && !kSplit;
+  constexpr int NYF = Dm::NYF;
 
   // ---------------- phase 0: stage the tile (TMA) and the neighbour strips ----------------
   if (!tile_stage_in<P, TW, TH, NY, TMA>(a, mapU, tx0, ty0, smraw, phase, tid, NT)) return;
 
   // ---------------- phase 1: face fluxes, each face of the tile once ----------------
-  tile_face_fluxes<P, FLUX, TW, TH, NY, GC>(Us, HL, HR, HD, HU, codes, Fs, tid, NT);
+  tile_face_fluxes<P, FLUX, TW, TH, NY, GC>(Us, HL, HR, HD, HU, codes, Fs, tid, NT, 0, kSplit ? NXF : NXF + NYF, 0);
   __syncthreads();
 
   // ---------------- phase 2: volume terms and assembly, one thread per element ----------------
@@ -336,15 +345,22 @@ __device__ __forceinline__ void tile2d_body(const TileArgs& a, const CUtensorMap
   for (int f = 0; f < NF; ++f)
 #pragma unroll
     for (int t = 0; t < NS; ++t) r[f][t] = 0.0;
-  // face contributions of the four faces (L: +F+nc, R: -F+nc, D: +F+nc, U: -F+nc)
+  // face contributions of the four faces (L: +F+nc, R: -F+nc, D: +F+nc, U: -F+nc); split faces:
+  // the x-faces' records, then (after the y-faces replaced them) the y-faces'
 #pragma unroll
   for (int kf = 0; kf < 4; ++kf) {
+    if (kSplit && kf == 2) {
+      __syncthreads();  // every thread has read its x-face records
+      tile_face_fluxes<P, FLUX, TW, TH, NY, GC>(Us, HL, HR, HD, HU, codes, Fs, tid, NT, NXF, NXF + NYF, NXF);
+      __syncthreads();
+    }
+    const int yrec = kSplit ? 0 : NXF;  // first y-face record in the buffer
     int base;
     double s, jw;
     if (kf == 0) { base = (tx * TH + ty) * N1; s = 1.0; jw = a.JFx; }
     else if (kf == 1) { base = ((tx + 1) * TH + ty) * N1; s = -1.0; jw = a.JFx; }
-    else if (kf == 2) { base = NXF + (ty * TW + tx) * N1; s = 1.0; jw = a.JFy; }
-    else { base = NXF + ((ty + 1) * TW + tx) * N1; s = -1.0; jw = a.JFy; }
+    else if (kf == 2) { base = yrec + (ty * TW + tx) * N1; s = 1.0; jw = a.JFy; }
+    else { base = yrec + ((ty + 1) * TW + tx) * N1; s = -1.0; jw = a.JFy; }
 #pragma unroll
     for (int g = 0; g < N1; ++g) {
       const double* fp = Fs + (base + g) * FS;
@@ -362,7 +378,7 @@ __device__ __forceinline__ void tile2d_body(const TileArgs& a, const CUtensorMap
     }
   }
   double* Ub = Fs;  // prefetched stage base (SSP) / accumulator (RK4), [NF*NS][NT]
-  const bool need = (MODE == MODE_SSP && a.a != 0.0) || (MODE == MODE_RK4 && a.Uacc != nullptr);
+  const bool need = kPrefetch && ((MODE == MODE_SSP && a.a != 0.0) || (MODE == MODE_RK4 && a.Uacc != nullptr));
   if (kPrefetch) {
     // the face buffer is free once every thread has read its face fluxes
     fence_proxy_async_smem();
@@ -500,11 +516,12 @@ __device__ __forceinline__ void tile2d_body(const TileArgs& a, const CUtensorMap
         const int t = ix + N1 * iy;
         const size_t gi = (size_t)(f * NS + t) * ld + e;
         if (MODE == MODE_SSP) {
-          const double base = a.a != 0.0 ? a.a * Ub[(f * NS + t) * NT + tid] : 0.0;
+          const double ub = kPrefetch ? Ub[(f * NS + t) * NT + tid] : (a.a != 0.0 ? __ldg(a.Ubase + gi) : 0.0);
+          const double base = a.a != 0.0 ? a.a * ub : 0.0;
           a.out[gi] = base + a.b * (us[(f * NS + t) * NT] + du);
         } else {
           a.out[gi] = du;
-          if (a.Uacc) a.Uacc[gi] = Ub[(f * NS + t) * NT + tid] + a.b * du;
+          if (a.Uacc) a.Uacc[gi] = (kPrefetch ? Ub[(f * NS + t) * NT + tid] : a.Uacc[gi]) + a.b * du;
         }
       }
   }

@@ -89,7 +89,7 @@ __global__ void __launch_bounds__(DMMA_THREADS, 2)
   double* HU = HD + TW * NF * N1;
   double* Fs = reinterpret_cast<double*>(smraw + Dm::off_face);
   const int* codes = reinterpret_cast<const int*>(smraw + Dm::head_bytes);
-  tile_face_fluxes<P, FLUX, TW, TH, 0, false>(Us, HL, HR, HD, HU, codes, Fs, tid, DMMA_THREADS);
+  tile_face_fluxes<P, FLUX, TW, TH, 0, false>(Us, HL, HR, HD, HU, codes, Fs, tid, DMMA_THREADS, 0, Dm::NXF + Dm::NYF, 0);
   __syncthreads();
 
   const int lane = tid & 31, warp = tid >> 5;
