@@ -1042,7 +1042,8 @@ def main(argv=None) -> int:
                              "avg_launch_ms": res_avg_s * 1e3,
                              "avg_launch_ms_source": "CUDA events around each residual launch in a separate profiled "
                                                      "pass of the same number of steps (eager launches)",
-                             "peak_source": "MEASURED_PEAKS.json hbm_gbs (measured copy)"},
+                             "peak_source": "MEASURED_PEAKS.json hbm_gbs (measured copy)" if "hbm_gbs" in peaks
+                             else "fallback 6650 GB/s (an earlier copy measurement on this pool; MEASURED_PEAKS.json absent)"},
                 "kernel_ms_per_step": {"residual": res_ms / args.steps, "limiter": lim_ms / args.steps,
                                        "dt": dt_ms / args.steps,
                                        **({"indicator": ind_ms / args.steps} if args.learned else {}),
