@@ -1512,6 +1512,7 @@ extern "C" int dgb_slab_ghost_rows(dgb_ctx* c, int lo, int hi) {
                                           "which no ghost depth reproduces; use none, hrl, m2l or prl");
   c->halo_lo = lo;
   c->halo_hi = hi;
+  c->drop_graphs();  // captured steps (own and multi-slab) hold the old rows
   return DGB_OK;
 }
 
