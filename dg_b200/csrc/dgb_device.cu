@@ -13,6 +13,7 @@
 #include <cstdlib>
 #include <algorithm>
 #include <cstring>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -1657,6 +1658,7 @@ struct SlabGraph {
   long long launches = 0;
 };
 std::vector<SlabGraph> g_slab_graphs;
+std::mutex g_slab_mutex;  // guards g_slab_graphs (calls on different slab sets may come from several threads)
 
 struct UmaxWords {
   unsigned long long* w[kMaxLocalSlabs];
@@ -1770,16 +1772,26 @@ int capture_slab_step(dgb_ctx* const* s, int n, bool periodic, int scheme, bool 
 }
 }  // namespace
 
-void dgb::drop_slab_graphs(dgb_ctx* c) {
+namespace {
+// (g_slab_mutex held) every captured slab step that involves c
+void drop_slab_graphs_locked(dgb_ctx* c) {
   for (size_t i = 0; i < g_slab_graphs.size();) {
     SlabGraph& g = g_slab_graphs[i];
     if (std::find(g.ctx.begin(), g.ctx.end(), c) != g.ctx.end()) {
+      // replays run on the first slab's stream and use every slab's buffers: let them finish
+      cudaStreamSynchronize(g.ctx[0]->st);
       if (g.exec) cudaGraphExecDestroy(g.exec);
       g_slab_graphs.erase(g_slab_graphs.begin() + i);
     } else {
       ++i;
     }
   }
+}
+}  // namespace
+
+void dgb::drop_slab_graphs(dgb_ctx* c) {
+  std::lock_guard<std::mutex> lock(g_slab_mutex);
+  drop_slab_graphs_locked(c);
 }
 
 extern "C" int dgb_slabs_advance_local(dgb_ctx* const* slabs, int n, int periodic, int scheme, int nsteps, double dt,
@@ -1813,6 +1825,14 @@ extern "C" int dgb_slabs_advance_local(dgb_ctx* const* slabs, int n, int periodi
       if (g && !c->halo_send[side])
         DGB_CUDA(cudaMalloc(&c->halo_send[side], (size_t)g * c->nx * c->nf * c->ns * sizeof(double)));
     }
+  std::lock_guard<std::mutex> lock(g_slab_mutex);
+  for (int i = 0; i < n; ++i) {  // captures that hold a slab whose own captured steps were dropped since
+    bool stale = false;
+    for (const auto& g : g_slab_graphs)
+      for (size_t j = 0; j < g.ctx.size(); ++j)
+        if (g.ctx[j] == slabs[i] && g.gen[j] != slabs[i]->graph_gen) stale = true;
+    if (stale) drop_slab_graphs_locked(slabs[i]);
+  }
   SlabGraph* sg = nullptr;
   for (auto& g : g_slab_graphs) {
     if (g.scheme != scheme || g.cfl != cfl || g.periodic != per || (int)g.ctx.size() != n) continue;
@@ -1821,7 +1841,6 @@ extern "C" int dgb_slabs_advance_local(dgb_ctx* const* slabs, int n, int periodi
     if (same) { sg = &g; break; }
   }
   if (!sg && nsteps > 0) {
-    for (int i = 0; i < n; ++i) drop_slab_graphs(slabs[i]);  // stale captures of these slabs
     SlabGraph g;
     g.ctx.assign(slabs, slabs + n);
     for (int i = 0; i < n; ++i) g.gen.push_back(slabs[i]->graph_gen);
