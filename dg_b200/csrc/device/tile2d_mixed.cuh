@@ -72,7 +72,8 @@ __device__ __forceinline__ float2 dev2(double u0, double u1, double a0, double a
 
 template <int P, int FLUX, int MODE, int TW, int TH>
 __global__ void __launch_bounds__(TW * TH, 3)
-    residual2d_tile_mixed_kernel(const TileArgs a, const __grid_constant__ CUtensorMap mapU) {
+    residual2d_tile_mixed_kernel(const TileArgs a, const __grid_constant__ CUtensorMap mapU,
+                                 const __grid_constant__ CUtensorMap mapB) {
   using Dm = TileDims<P, TW, TH>;
   constexpr int N1 = Dm::N1, NS = Dm::NS, NF = 5, NT = Dm::NT, NXF = Dm::NXF, NYF = Dm::NYF;
   extern __shared__ __align__(128) unsigned char smraw[];
@@ -110,6 +111,9 @@ __global__ void __launch_bounds__(TW * TH, 3)
     if (tma_ok) {
       mbar_arrive_expect_tx(bar, Dm::tile_bytes);
       tma_load_3d(Us, &mapU, tx0, ty0, 0, bar);
+      // the stage base (SSP) / accumulator (RK4) the epilogue reads, on its way to L2 meanwhile
+      if ((MODE == MODE_SSP && a.a != 0.0) || (MODE == MODE_RK4 && a.Uacc))
+        tma_prefetch_3d(&mapB, tx0, ty0, 0);
     } else {
       atomicOr(a.errflag, (unsigned)FLAG_TIMEOUT);
     }
@@ -502,6 +506,17 @@ __global__ void __launch_bounds__(TW * TH, mixed_ct_min_blocks<P>())
     Anc[4 * NT + tid] = u4[0];
 #pragma unroll
     for (int t = 1; t < NS; ++t) D4[(t - 1) * NT + tid] = (float)(u4[t] - u4[0]);
+  }
+  // the stage base (SSP) / accumulator (RK4) the epilogue reads, on its way to L2 meanwhile: the
+  // tile's rows of every (field, node) plane, 128-byte lines spread over the threads
+  const double* pb = MODE == MODE_SSP && a.a != 0.0 ? a.Ubase : MODE == MODE_RK4 ? a.Uacc : nullptr;
+  if (pb) {
+    constexpr int LPR = TW * 8 / 128;  // lines per tile row of one plane
+    for (int k = tid; k < NF * NS * TH * LPR; k += NT) {
+      const int q = k / (TH * LPR), r = (k / LPR) % TH, l = k % LPR;
+      const double* p = pb + (size_t)q * ld + (size_t)(ty0 + r) * nx + tx0 + l * 16;
+      asm volatile("prefetch.global.L2 [%0];" ::"l"(p));
+    }
   }
   __syncthreads();  // codes
   for (int k = tid; k < 2 * TH * NF * N1; k += NT) {

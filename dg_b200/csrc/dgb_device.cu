@@ -254,9 +254,11 @@ void launch_tile2d_mixed(dgb_ctx* c, const StageArgs& s) {
   static bool attr = false;
   if (!attr) { cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem); attr = true; }
   const TileArgs a = tile_args(c, s);
+  const CUtensorMap& mb = MODE == MODE_SSP ? map_of(c, s.Ubase)
+                          : MODE == MODE_RK4 && s.Uacc ? map_of(c, s.Uacc) : map_of(c, s.U);
   dim3 grid(c->nx / TILE_W, c->ny / TH);
   ProfScope ps(c, KC_RESIDUAL);
-  k<<<grid, TILE_W * TH, smem, c->st>>>(a, map_of(c, s.U));
+  k<<<grid, TILE_W * TH, smem, c->st>>>(a, map_of(c, s.U), mb);
 }
 
 // p = 2 FP64 stage on the FP64 tensor cores (tile2d_dmma.cuh): same tiles and tensor map
