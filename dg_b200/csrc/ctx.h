@@ -39,6 +39,7 @@ struct dgb_ctx {
   int form = DGB_FORM_FP64;  // arithmetic of the residual: plain FP64 or mixed FP32/FP64
   long long wait_polls = 1ll << 22;  // poll budget of the residual kernels' first wait per tile copy
   bool rowmajor = false;  // structured row-major grid: tiled limiter passes
+  bool chain1d = false;   // 1D elements in chain order: fused residual + limiter stages
   bool fused_lim = false; // row-major grid, hrl / m2l: both limiter passes in one kernel (opt-in)
   CUtensorMap mapA, mapB, mapC;  // TMA descriptors of the state buffers (tiled kernel)
   double hx = 0, hy = 0;

@@ -269,11 +269,12 @@ __global__ void __launch_bounds__(NT) residual2d_kernel(const Consts cin, const 
 // element e (< c.n_elem) with the problem constants c (in shared memory) and dt; NY passive mass
 // fractions follow the four gamma-model fields
 // GC: the GAMCONS model (fields rho, rho u, E, rho/(gamma-1)): conservative alpha flux, no source
-template <int P, int FLUX, int MODE, int NY = 0, bool GC = false>
-__device__ __forceinline__ void res1d_body(const Consts& c, const StageArgs& a, int e, double dt) {
+// The residual r = S + F + Q of element e (its nodal state in u, read from a.U)
+template <int P, int FLUX, int NY = 0, bool GC = false>
+__device__ __forceinline__ void res1d_residual(const Consts& c, const StageArgs& a, int e, double (&u)[4 + NY][P + 1],
+                                               double (&r)[4 + NY][P + 1]) {
   constexpr int N1 = P + 1, NG = P + 1, NF = 4 + NY;
   const int ld = c.ld;
-  double u[NF][N1], r[NF][N1];
 #pragma unroll
   for (int f = 0; f < NF; ++f)
 #pragma unroll
@@ -332,6 +333,14 @@ __device__ __forceinline__ void res1d_body(const Consts& c, const StageArgs& a, 
 #pragma unroll
     for (int f = 0; f < NF; ++f) r[f][to] += sgn * F[f] + (f == 3 ? nc : 0.0);
   }
+}
+
+template <int P, int FLUX, int MODE, int NY = 0, bool GC = false>
+__device__ __forceinline__ void res1d_body(const Consts& c, const StageArgs& a, int e, double dt) {
+  constexpr int N1 = P + 1, NF = 4 + NY;
+  const int ld = c.ld;
+  double u[NF][N1], r[NF][N1];
+  res1d_residual<P, FLUX, NY, GC>(c, a, e, u, r);
   if constexpr (MODE == MODE_RESIDUAL) {
 #pragma unroll
     for (int f = 0; f < NF; ++f)
@@ -591,33 +600,19 @@ __global__ void __launch_bounds__(128) lim2d_ypass_kernel(const LimArgs la, cons
   }
 }
 
-// 1D HR / m2 limiter, one thread per element (reads U, writes Uout).  Mass fractions are limited
-// like the density (HR: every field; m2: the MACRO block of M2limiting, limiting.cc:186-193).
+// The limited nodal values o of one element from its slices v[0] (left neighbour), v[1] (itself),
+// v[2] (right neighbour; the neighbours' slices are read only when phys == 0).
 template <int P, int METHOD, int NY = 0>
-__device__ __forceinline__ void lim1d_body(int ld, int e, const double* __restrict__ U, const int* __restrict__ nbr,
-                                           double* __restrict__ Uout) {
+__device__ __forceinline__ void lim1d_limit(int phys, const double (&v)[3][4 + NY][P + 1],
+                                            double (&o)[4 + NY][P + 1]) {
   constexpr int N1 = P + 1, NF = 4 + NY;
-  const int nL = __ldg(nbr + e), nR = __ldg(nbr + (size_t)ld + e);
-  const int phys = boundary_code(nL, nR);
-  double v[3][NF][N1];
-#pragma unroll
-  for (int s = 0; s < 3; ++s) {
-    const int el = s == 0 ? nL : s == 1 ? e : nR;
-    if (s != 1 && phys != 0) continue;
-#pragma unroll
-    for (int f = 0; f < NF; ++f)
-#pragma unroll
-      for (int i = 0; i < N1; ++i) v[s][f][i] = __ldg(U + (size_t)(f * N1 + i) * ld + el);
-  }
   if constexpr (METHOD == 1) {
 #pragma unroll
     for (int f = 0; f < NF; ++f) {
-      double lim[N1], out[N1];
+      double lim[N1];
       const int ph = (phys == 3 && f == 1) ? 5 : phys;
       limit_slice<P>(ph, v[0][f], v[1][f], v[2][f], lim);
-      to_lag<P>(lim, out);
-#pragma unroll
-      for (int i = 0; i < N1; ++i) Uout[(size_t)(f * N1 + i) * ld + e] = out[i];
+      to_lag<P>(lim, o[f]);
     }
   } else {
     double pr[3][N1];
@@ -636,32 +631,49 @@ __device__ __forceinline__ void lim1d_body(int ld, int e, const double* __restri
     limit_slice<P>(phys, v[0][1], v[1][1], v[2][1], lu);
     limit_slice<P>(phys, v[0][3], v[1][3], v[2][3], la_);
     limit_slice<P>(phys, pr[0], pr[1], pr[2], lp);
-    double r_[N1], u_[N1], a_[N1], K[N1], Km[N1], Em[N1], El[N1], E_[N1];
-    to_lag<P>(lr, r_);
-    to_lag<P>(lu, u_);
-    to_lag<P>(la_, a_);
+    double K[N1], Km[N1], Em[N1], El[N1];
+    to_lag<P>(lr, o[0]);
+    to_lag<P>(lu, o[1]);
+    to_lag<P>(la_, o[3]);
 #pragma unroll
-    for (int i = 0; i < N1; ++i) K[i] = 0.5 * u_[i] * u_[i] * __drcp_rn(r_[i]);  // kinetic_energy1D
+    for (int i = 0; i < N1; ++i) K[i] = 0.5 * o[1][i] * o[1][i] * __drcp_rn(o[0][i]);  // kinetic_energy1D
     to_mono<P>(K, Km);
     to_mono<P>(v[1][2], Em);
     reconstruct_energy<P>(lp, la_, Km, Em, El);
-    to_lag<P>(El, E_);
-#pragma unroll
-    for (int i = 0; i < N1; ++i) {
-      Uout[(size_t)(0 * N1 + i) * ld + e] = r_[i];
-      Uout[(size_t)(1 * N1 + i) * ld + e] = u_[i];
-      Uout[(size_t)(2 * N1 + i) * ld + e] = E_[i];
-      Uout[(size_t)(3 * N1 + i) * ld + e] = a_[i];
-    }
+    to_lag<P>(El, o[2]);
 #pragma unroll
     for (int k = 4; k < NF; ++k) {
-      double ly[N1], y_[N1];
+      double ly[N1];
       limit_slice<P>(phys, v[0][k], v[1][k], v[2][k], ly);
-      to_lag<P>(ly, y_);
-#pragma unroll
-      for (int i = 0; i < N1; ++i) Uout[(size_t)(k * N1 + i) * ld + e] = y_[i];
+      to_lag<P>(ly, o[k]);
     }
   }
+}
+
+// 1D HR / m2 limiter, one thread per element (reads U, writes Uout).  Mass fractions are limited
+// like the density (HR: every field; m2: the MACRO block of M2limiting, limiting.cc:186-193).
+template <int P, int METHOD, int NY = 0>
+__device__ __forceinline__ void lim1d_body(int ld, int e, const double* __restrict__ U, const int* __restrict__ nbr,
+                                           double* __restrict__ Uout) {
+  constexpr int N1 = P + 1, NF = 4 + NY;
+  const int nL = __ldg(nbr + e), nR = __ldg(nbr + (size_t)ld + e);
+  const int phys = boundary_code(nL, nR);
+  double v[3][NF][N1];
+#pragma unroll
+  for (int s = 0; s < 3; ++s) {
+    const int el = s == 0 ? nL : s == 1 ? e : nR;
+    if (s != 1 && phys != 0) continue;
+#pragma unroll
+    for (int f = 0; f < NF; ++f)
+#pragma unroll
+      for (int i = 0; i < N1; ++i) v[s][f][i] = __ldg(U + (size_t)(f * N1 + i) * ld + el);
+  }
+  double o[NF][N1];
+  lim1d_limit<P, METHOD, NY>(phys, v, o);
+#pragma unroll
+  for (int f = 0; f < NF; ++f)
+#pragma unroll
+    for (int i = 0; i < N1; ++i) Uout[(size_t)(f * N1 + i) * ld + e] = o[f][i];
 }
 
 template <int P, int METHOD, int NY = 0>
@@ -672,6 +684,81 @@ __global__ void __launch_bounds__(128) lim1d_kernel(const LimArgs la, const doub
   const int e = blockIdx.x * blockDim.x + threadIdx.x;
   if (e >= la.n_elem) return;
   lim1d_body<P, METHOD, NY>(la.ld, e, U, nbr, Uout);
+}
+
+// One stage of a 1D problem whose elements form a chain (the neighbours of element e are e - 1 and
+// e + 1; at the ends a boundary code or, periodic, the other end): residual, stage update and the
+// hrl / m2l limiter in one launch.  A CTA advances a block of RL1D_B elements plus the element on
+// either side of it (recomputed here, not written), keeps the limiter's input in shared memory
+// and limits the block from there, so the unlimited stage output never goes to global memory.
+//   MODE_SSP  limiter input a Ubase + b (U + du)
+//   MODE_RK4  accumulator acc_out = acc_in + b du (two buffers: a neighbouring block reads acc_in);
+//             limiter input the next stage input Us + beta_next du, or (last stage) acc_out
+// lim_out must be none of the buffers the stage reads (U, Ubase, Us, acc_in).
+constexpr int RL1D_B = 64;
+template <int P, int FLUX, int MODE, int METHOD>
+__global__ void __launch_bounds__(96) res_lim1d_chain_kernel(const Consts cin, const StageArgs a,
+                                                             const double* __restrict__ acc_in,
+                                                             double* __restrict__ acc_out, int last,
+                                                             double* __restrict__ lim_out) {
+  constexpr int N1 = P + 1, NF = 4, B = RL1D_B;
+  __shared__ Consts c;
+  __shared__ double V[NF * N1][B + 2];  // limiter input of slot s: element e0 + s - 1
+  copy_consts(c, cin);
+  if (a.scal && a.scal->flags) return;
+  __syncthreads();
+  const int ld = c.ld;
+  const int e0 = blockIdx.x * B, nb = min(B, c.n_elem - e0);
+  const int s = threadIdx.x;
+  if (s < nb + 2) {
+    const bool own = s >= 1 && s <= nb;
+    const int e = own ? e0 + s - 1 : s == 0 ? __ldg(a.nbr + e0) : __ldg(a.nbr + (size_t)ld + e0 + nb - 1);
+    if (e >= 0) {
+      const double dt = a.dt_override > 0 ? a.dt_override : a.scal->dt;
+      double u[NF][N1], r[NF][N1];
+      res1d_residual<P, FLUX>(c, a, e, u, r);
+#pragma unroll
+      for (int f = 0; f < NF; ++f)
+#pragma unroll
+        for (int t = 0; t < N1; ++t) {
+          double sm = 0.0;
+#pragma unroll
+          for (int tt = 0; tt < N1; ++tt) sm += c.Minv[t][tt] * r[f][tt];
+          const double du = dt * sm;
+          const size_t gi = (size_t)(f * N1 + t) * ld + e;
+          double w;
+          if constexpr (MODE == MODE_SSP) {
+            const double base = a.a != 0.0 ? a.a * __ldg(a.Ubase + gi) : 0.0;
+            w = base + a.b * (u[f][t] + du);
+          } else {
+            const double acc = __ldg(acc_in + gi) + a.b * du;
+            if (own) acc_out[gi] = acc;
+            w = last ? acc : __ldg(a.Us + gi) + a.beta_next * du;  // rk.cc:164-170
+          }
+          V[f * N1 + t][s] = w;
+        }
+    }
+  }
+  __syncthreads();
+  if (s >= 1 && s <= nb) {
+    const int e = e0 + s - 1;
+    const int phys = boundary_code(__ldg(a.nbr + e), __ldg(a.nbr + (size_t)ld + e));
+    double v[3][NF][N1];
+#pragma unroll
+    for (int sl = 0; sl < 3; ++sl) {
+      if (sl != 1 && phys != 0) continue;
+#pragma unroll
+      for (int f = 0; f < NF; ++f)
+#pragma unroll
+        for (int i = 0; i < N1; ++i) v[sl][f][i] = V[f * N1 + i][s - 1 + sl];
+    }
+    double o[NF][N1];
+    lim1d_limit<P, METHOD>(phys, v, o);
+#pragma unroll
+    for (int f = 0; f < NF; ++f)
+#pragma unroll
+      for (int i = 0; i < N1; ++i) lim_out[(size_t)(f * N1 + i) * ld + e] = o[f][i];
+  }
 }
 
 // ------------------------------------------------------------------------------------------

@@ -123,6 +123,18 @@ Consts make_consts(const Problem& P, int ld) {
 }
 
 // structured row-major grid test: interior neighbours are e-1, e+1, e-nx, e+nx
+// the neighbours of element e are e - 1 and e + 1 (at the ends: a boundary code, or the other end)
+bool is_chain_1d(const Problem& P) {
+  if (P.D != 1 || P.N_E < 2) return false;
+  const int ne = P.N_E;
+  for (int e = 0; e < ne; ++e) {
+    const int L = P.nbr[e], R = P.nbr[(size_t)ne + e];
+    if (e > 0 ? L != e - 1 : !(L < 0 || L == ne - 1)) return false;
+    if (e < ne - 1 ? R != e + 1 : !(R < 0 || R == 0)) return false;
+  }
+  return true;
+}
+
 bool is_row_major_grid(const Problem& P) {
   if (P.D != 2 || P.nx <= 0 || P.ny <= 0 || (long)P.nx * P.ny != P.N_E) return false;
   const int nx = P.nx, ne = P.N_E;
@@ -792,8 +804,80 @@ bool lim1d_direct(const dgb_ctx* c) {
   return c->D == 1 && !c->gated && !c->ind_on && (c->limiter == DGB_LIM_HRL || c->limiter == DGB_LIM_M2L);
 }
 
+// 1D chains with hrl / m2l: residual, stage update and limiter of a stage in one launch
+// (res_lim1d_chain_kernel); the stage inputs and accumulators alternate between buffers so that
+// no launch writes what a neighbouring block still reads
+template <int P, int FLUX, int METHOD>
+void launch_res_lim1d(dgb_ctx* c, const StageArgs& a, int mode, const double* acc_in, double* acc_out, int last,
+                      double* lim_out) {
+  const int grid = (c->ne + RL1D_B - 1) / RL1D_B;
+  ProfScope ps(c, KC_RESIDUAL);
+  if (mode == MODE_SSP)
+    res_lim1d_chain_kernel<P, FLUX, MODE_SSP, METHOD><<<grid, 96, 0, c->st>>>(c->cs, a, acc_in, acc_out, last, lim_out);
+  else
+    res_lim1d_chain_kernel<P, FLUX, MODE_RK4, METHOD><<<grid, 96, 0, c->st>>>(c->cs, a, acc_in, acc_out, last, lim_out);
+}
+
+int res_lim1d(dgb_ctx* c, const StageArgs& a, int mode, const double* acc_in, double* acc_out, int last,
+              double* lim_out) {
+#define RL(P, F, M)                                                   \
+  case P * 100 + F * 10 + M:                                          \
+    launch_res_lim1d<P, F, M>(c, a, mode, acc_in, acc_out, last, lim_out); \
+    return 0;
+  switch (c->p * 100 + c->flux * 10 + c->limiter) {
+    RL(1, 0, 1) RL(1, 0, 2) RL(1, 1, 1) RL(1, 1, 2) RL(1, 2, 1) RL(1, 2, 2)
+    RL(2, 0, 1) RL(2, 0, 2) RL(2, 1, 1) RL(2, 1, 2) RL(2, 2, 1) RL(2, 2, 2)
+    RL(3, 0, 1) RL(3, 0, 2) RL(3, 1, 1) RL(3, 1, 2) RL(3, 2, 1) RL(3, 2, 2)
+    default: return set_error(DGB_ERR_UNSUPPORTED, "no fused 1D stage for this (p, flux, limiter)");
+  }
+#undef RL
+}
+
+bool fused1d(const dgb_ctx* c) { return c->chain1d && c->nmass == 0 && !c->gamcons; }
+
+// SSP-RK3, fused 1D stages: inputs A, X, B; limited into X, B, C; C copied to A
+int step1d_ssprk3_fused(dgb_ctx* c, bool cfl) {
+  launch_dt(c, c->A, cfl);
+  const double coef[3][2] = {{0.0, 1.0}, {0.75, 0.25}, {1.0 / 3.0, 2.0 / 3.0}};
+  const double* in[3] = {c->A, c->X, c->B};
+  double* lim[3] = {c->X, c->B, c->C};
+  for (int s = 0; s < 3; ++s) {
+    StageArgs a = stage_args(c);
+    a.U = in[s];
+    a.Ubase = c->A;
+    a.a = coef[s][0];
+    a.b = coef[s][1];
+    if (int rc = res_lim1d(c, a, MODE_SSP, nullptr, nullptr, 0, lim[s])) return rc;
+  }
+  DGB_CUDA(cudaMemcpyAsync(c->A, c->C, c->nstate * sizeof(double), cudaMemcpyDeviceToDevice, c->st));
+  return 0;
+}
+
+// RK4, fused 1D stages: Us = A; stage inputs A, B, C, B; accumulator X (from the CFL reduction) ->
+// DU -> X -> DU; limited into B, C, B and, from the last accumulator, A
+int step1d_rk4_fused(dgb_ctx* c, bool cfl) {
+  launch_dt(c, c->A, cfl, cfl ? c->X : nullptr);
+  if (!cfl) DGB_CUDA(cudaMemcpyAsync(c->X, c->A, c->nstate * sizeof(double), cudaMemcpyDeviceToDevice, c->st));
+  const double beta[4] = {0.0, 0.5, 0.5, 1.0};
+  const double gam[4] = {1.0 / 6.0, 2.0 / 6.0, 2.0 / 6.0, 1.0 / 6.0};
+  const double* in[4] = {c->A, c->B, c->C, c->B};
+  double* lim[4] = {c->B, c->C, c->B, c->A};
+  const double* ain[4] = {c->X, c->DU, c->X, c->DU};
+  double* aout[4] = {c->DU, c->X, c->DU, c->X};
+  for (int k = 0; k < 4; ++k) {
+    StageArgs a = stage_args(c);
+    a.U = in[k];
+    a.Us = c->A;
+    a.b = gam[k];
+    a.beta_next = k < 3 ? beta[k + 1] : 0.0;
+    if (int rc = res_lim1d(c, a, MODE_RK4, ain[k], aout[k], k == 3, lim[k])) return rc;
+  }
+  return 0;
+}
+
 // SSP-RK3, 1D: stage inputs A, X, B; unlimited outputs B, C, X; limited into X, B, A
 int step1d_ssprk3(dgb_ctx* c, bool cfl) {
+  if (fused1d(c)) return step1d_ssprk3_fused(c, cfl);
   launch_dt(c, c->A, cfl);
   const double coef[3][2] = {{0.0, 1.0}, {0.75, 0.25}, {1.0 / 3.0, 2.0 / 3.0}};
   const double* in[3] = {c->A, c->X, c->B};
@@ -816,6 +900,7 @@ int step1d_ssprk3(dgb_ctx* c, bool cfl) {
 // stage k's residual also forms the next input C = Us + beta DU, limited into B; the last stage's
 // accumulator is limited into A
 int step1d_rk4(dgb_ctx* c, bool cfl) {
+  if (fused1d(c)) return step1d_rk4_fused(c, cfl);
   launch_dt(c, c->A, cfl, cfl ? c->X : nullptr);
   if (!cfl) cudaMemcpyAsync(c->X, c->A, c->nstate * sizeof(double), cudaMemcpyDeviceToDevice, c->st);
   const double beta[4] = {0.0, 0.5, 0.5, 1.0};
@@ -975,6 +1060,11 @@ extern "C" int dgb_create(const dgb_problem* prob, int device, dgb_ctx** out) {
   c->hx = P.hx;
   c->hy = P.hy;
   c->rowmajor = P.D == 2 && is_row_major_grid(P) && std::getenv("DGB_NO_TILE") == nullptr;
+  // 1D elements in chain order: fused residual + limiter stages (DGB_1D_FUSED=0: separate kernels)
+  {
+    const char* f1 = std::getenv("DGB_1D_FUSED");
+    c->chain1d = P.D == 1 && is_chain_1d(P) && !(f1 && std::string(f1) == "0");
+  }
   // tiled residual over the full tiles; the strips left over on other extents go to the generic
   // kernel.  Tile loads by TMA where the tensor map's row pitch nx * 8 bytes is a multiple of 16
   // (nx even), by plain loads otherwise

@@ -41,3 +41,46 @@ def test_tube_rk4_cfl_run_matches_reference():
           f"max |dU| / max |U| after 2000: {full:.3e}")
     assert e100 <= 1e-10
     assert e2000 <= 1e-8
+
+
+CASES_1D = [
+    # order, flux, limiter, scheme, dt (0: CFL step), nsteps, elements, boundaries
+    (2, "roe", "m2l", "rk4", 0.0, 40, 1000, ("transmissive",) * 2),
+    (2, "roe", "m2l", "ssprk3", 0.0, 40, 1000, ("transmissive",) * 2),
+    (1, "rusanov", "hrl", "rk4", 1e-4, 30, 777, ("reflective",) * 2),
+    (3, "hll", "m2l", "ssprk3", 0.0, 25, 5000, ("reflective", "transmissive")),
+    (3, "roe", "hrl", "rk4", 0.0, 25, 130, ("periodic",) * 2),
+]
+
+
+@pytest.mark.parametrize("case", CASES_1D, ids=[f"p{c[0]}_{c[1]}_{c[2]}_{c[3]}_{c[6]}" for c in CASES_1D])
+def test_fused_1d_stages_equal_the_separate_kernels(case, monkeypatch):
+    """1D elements in chain order: residual, stage update and limiter of a stage in one launch
+    (each block of elements recomputes its two outside neighbours and limits from shared memory)
+    against the separate residual and limiter kernels (DGB_1D_FUSED=0), over two calls in a row:
+    the same states to rounding (the compiler may contract products into multiply-adds
+    differently in the two kernels) and the same time."""
+    import dg_b200 as dgb
+    order, flux, lim, scheme, dt, n, ne, bc = case
+    sch = dgb.RK4 if scheme == "rk4" else dgb.SSPRK3
+    prob = dgb.Problem.structured(1, order, ne, 1, 0.0, 1.0, bc=bc, flux=flux, limiter=lim, cfl=0.4)
+    d = np.load(GOLDEN / "run_d1_tube_p2_roe_m2l_1000.npz")
+    base = d["U0"].reshape(1000, 4, 3)
+    idx = (np.arange(ne) * 1000) // ne  # the shock tube's cell means resampled onto this grid
+    U0 = np.repeat(base[idx].mean(axis=2)[:, :, None], order + 1, axis=2).reshape(-1)
+    out = {}
+    for mode in ("0", "1"):
+        monkeypatch.setenv("DGB_1D_FUSED", mode)  # read when the context is created
+        s = dgb.DGSolver(prob)
+        try:
+            s.set_state(s.limit(U0))
+            t = s.advance(n, dt, scheme=sch)
+            t += s.advance(n // 2, dt, scheme=sch)
+            out[mode] = (t, s.get_state(), s.last_timing())
+        finally:
+            s.close()
+    (ts, Us, (ms_s, l_s)), (tf, Uf, (ms_f, l_f)) = out["0"], out["1"]
+    print(f"1D {case}: {n // 2} steps separate {ms_s:.3f} ms ({l_s} launches), fused {ms_f:.3f} ms ({l_f})")
+    assert np.isfinite(Uf).all()
+    assert abs(tf - ts) <= 1e-13 * ts
+    assert np.abs(Uf - Us).max() <= 1e-13 * np.abs(Us).max(), np.abs(Uf - Us).max()
