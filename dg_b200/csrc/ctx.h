@@ -105,6 +105,30 @@ struct dgb_ctx {
 
 namespace dgb {
 int set_error(int code, const std::string& msg);
+
+// an event of the context's profiling pool (reused from one profiled call to the next)
+inline cudaEvent_t pool_event(dgb_ctx* c) {
+  if (c->ev_used == c->ev_pool.size()) {
+    cudaEvent_t e;
+    cudaEventCreate(&e);
+    c->ev_pool.push_back(e);
+  }
+  return c->ev_pool[c->ev_used++];
+}
+
+// one kernel launch of kernel class kc: counted, and bracketed by events when profiling is on
+struct ProfScope {
+  dgb_ctx* c;
+  int kc;
+  cudaEvent_t a = nullptr, b = nullptr;
+  ProfScope(dgb_ctx* ctx, int k) : c(ctx), kc(k) {
+    c->counter++;
+    if (c->prof) { a = pool_event(c); b = pool_event(c); cudaEventRecord(a, c->st); }
+  }
+  ~ProfScope() {
+    if (c->prof) { cudaEventRecord(b, c->st); c->pev.push_back({kc, {a, b}}); }
+  }
+};
 // TMA descriptor of one of the context's state buffers with a tw x th element box
 bool encode_state_map(dgb_ctx* c, double* ptr, CUtensorMap* map, int tw, int th);
 }

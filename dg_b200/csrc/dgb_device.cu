@@ -28,6 +28,13 @@
 #include "device/learned_tc.cuh"
 #include "device/tables.cuh"
 #include "device/sensor.h"
+
+namespace dgb {
+// 1D with 4 to 10 mass fractions (dgb_device_ny.cu)
+int residual1d_many_y(dgb_ctx* c, const StageArgs& a, int mode);
+int limit1d_many_y(dgb_ctx* c, const double* in, double* out);
+int upload_many_y_tables(const Consts& cs, int p);
+}  // namespace dgb
 #include "host/host.h"
 #include "ctx.h"
 
@@ -155,27 +162,6 @@ bool is_row_major_grid(const Problem& P) {
 
 namespace {
 
-cudaEvent_t pool_event(dgb_ctx* c) {
-  if (c->ev_used == c->ev_pool.size()) {
-    cudaEvent_t e;
-    cudaEventCreate(&e);
-    c->ev_pool.push_back(e);
-  }
-  return c->ev_pool[c->ev_used++];
-}
-
-struct ProfScope {
-  dgb_ctx* c;
-  int kc;
-  cudaEvent_t a = nullptr, b = nullptr;
-  ProfScope(dgb_ctx* ctx, int k) : c(ctx), kc(k) {
-    c->counter++;
-    if (c->prof) { a = pool_event(c); b = pool_event(c); cudaEventRecord(a, c->st); }
-  }
-  ~ProfScope() {
-    if (c->prof) { cudaEventRecord(b, c->st); c->pev.push_back({kc, {a, b}}); }
-  }
-};
 
 // generic 2D residual over every element, or over the listed ones (elist, n)
 template <int P, int FLUX, int MODE>
@@ -394,7 +380,9 @@ int residual_dispatch(dgb_ctx* c, const StageArgs& a) {
       case 1: return residual_ny<MODE, 1>(c, a);
       case 2: return residual_ny<MODE, 2>(c, a);
       case 3: return residual_ny<MODE, 3>(c, a);
-      default: return set_error(DGB_ERR_UNSUPPORTED, "at most three mass fractions on the device path");
+      default:
+        if (c->D == 1) return residual1d_many_y(c, a, MODE);
+        return set_error(DGB_ERR_UNSUPPORTED, "at most three mass fractions on the 2D device path");
     }
   }
   if (c->tiled) {
@@ -682,7 +670,13 @@ int limit_dispatch(dgb_ctx* c, double* U, bool rescore = true) {
     case 1: return limit_ny<1>(c, U, key);
     case 2: return limit_ny<2>(c, U, key);
     case 3: return limit_ny<3>(c, U, key);
-    default: return set_error(DGB_ERR_UNSUPPORTED, "at most three mass fractions on the device path");
+    default:
+      if (c->D == 1) {
+        if (int rc = limit1d_many_y(c, U, c->X)) return rc;
+        DGB_CUDA(cudaMemcpyAsync(U, c->X, c->nstate * sizeof(double), cudaMemcpyDeviceToDevice, c->st));
+        return 0;
+      }
+      return set_error(DGB_ERR_UNSUPPORTED, "at most three mass fractions on the 2D device path");
   }
 #define L2(P, M) case P * 10 + M: launch_lim2d<P, M>(c, U); return 0;
 #define L1(P, M) case P * 10 + M: launch_lim1d<P, M>(c, U); return 0;
@@ -794,7 +788,7 @@ int limit1d_to(dgb_ctx* c, const double* in, double* out) {
     case 1: return limit1d_to_ny<1>(c, in, out);
     case 2: return limit1d_to_ny<2>(c, in, out);
     case 3: return limit1d_to_ny<3>(c, in, out);
-    default: return set_error(DGB_ERR_UNSUPPORTED, "at most three mass fractions on the device path");
+    default: return limit1d_many_y(c, in, out);
   }
 }
 
@@ -1090,7 +1084,13 @@ extern "C" int dgb_create(const dgb_problem* prob, int device, dgb_ctx** out) {
     if (why) { delete c; return set_error(DGB_ERR_UNSUPPORTED, why); }
     c->fused_lim = false;
   }
-  if (P.N_Y > 3) { delete c; return set_error(DGB_ERR_UNSUPPORTED, "at most three mass fractions on the device path"); }
+  if (P.N_Y > (P.D == 1 ? 10 : 3)) {
+    delete c;
+    return set_error(DGB_ERR_UNSUPPORTED, "mass fractions on the device path: up to 10 in 1D, up to 3 in 2D");
+  }
+  if (P.D == 1 && P.N_Y > 3) {
+    if (int rc = upload_many_y_tables(c->cs, P.p)) { delete c; return rc; }
+  }
   if (P.N_Y > 0 && P.D == 2 && !c->tiled_full) {
     delete c;
     return set_error(DGB_ERR_UNSUPPORTED, "mass fractions in 2D need a structured row-major grid with nx a multiple "

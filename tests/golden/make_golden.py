@@ -124,6 +124,11 @@ CASES = [
          flux="roe", limiter="none", ic="quadrants", cfl=0.1, dt=5e-4, nsteps=4, gamma_model="gamcons"),
     dict(name="g2_p3_roe_hrl", dim=2, order=3, nx=32, ny=4, dom=(0, 2, 0, 1), bc=("transmissive",) * 4,
          flux="roe", limiter="hrl", ic="shock_bubble", cfl=0.3, dt=2.5e-4, nsteps=4, gamma_model="gamcons"),
+    # five and ten mass fractions in 1D (MASS=5, MASS=10)
+    dict(name="m10_d1_p2_roe_m2l", dim=1, order=2, nx=24, ny=1, dom=(0, 1, 0, 1), bc=("transmissive",) * 2,
+         flux="roe", limiter="m2l", ic="tube_noise", cfl=0.4, dt=4e-4, nsteps=5, n_mass=10),
+    dict(name="m5_d1_p3_rus_hrl_wall", dim=1, order=3, nx=20, ny=1, dom=(0, 1, 0, 1), bc=("reflective",) * 2,
+         flux="rusanov", limiter="hrl", ic="riemann", cfl=0.2, dt=2e-4, nsteps=5, n_mass=5),
 ]
 
 
