@@ -52,6 +52,7 @@ struct dgb_ctx {
   int sm_count = 148;           // multiprocessors of the device
   bool ind_on = false;          // learned indicator gates the limiter (dgb_set_indicator)
   bool mixed_ct = false;        // mixed form: the compressed-tile kernel (else the TMA-tile kernel)
+  bool pdl = true;              // programmatic dependent launches (kernels that wait in pdl_wait)
   bool tile_dmma = false;       // p = 2 FP64 stages: the DMMA residual (else the scalar tiled kernel)
   bool ind_tc = true;           // scoring GEMMs on tcgen05 (else the mma.sync kernel)
   float ind_threshold = 0.2f;

@@ -51,6 +51,14 @@ struct DevScalars {
 
 enum { FLAG_NONFINITE = 1u, FLAG_DT_SMALL = 2u };
 
+// Programmatic dependent launch (a kernel launched with programmatic stream serialization may be
+// scheduled before its predecessor in the stream has finished): pdl_wait blocks until the
+// predecessor grid has completed and its memory is visible (at once when the launch was not
+// programmatic), so it comes before a kernel's first access to global data; pdl_trigger lets the
+// next kernel's CTAs be scheduled as this one's finish.
+__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+__device__ __forceinline__ void pdl_trigger() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
+
 __device__ __forceinline__ int signum_d(double v) { return v > 0 ? 1 : (v < 0 ? -1 : 0); }
 
 // minmod of two arguments (limiting_kernels.cu:1470-1486)

@@ -793,6 +793,7 @@ template <int DIM, int NS, bool GC = false>
 __global__ void __launch_bounds__(256) wavespeed_kernel(const double* __restrict__ U, int n_elem, int ld,
                                                         DevScalars* __restrict__ scal,
                                                         double* __restrict__ copy_to, int nf, double finish) {
+  pdl_wait();
   if (scal->flags) return;
   double m = 0.0;
   bool bad = false;

@@ -136,8 +136,10 @@ __global__ void __launch_bounds__(32 * (P + 1)) lim2d_xpass_tile_kernel(const Li
                                                                       const int* __restrict__ nbr,
                                                                       double* __restrict__ X,
                                                                       const DevScalars* __restrict__ scal) {
+  pdl_wait();
   if (scal && scal->flags) return;
   lim2d_xpass_body<P, METHOD, NY>(la, nx, U, nbr, X, blockIdx.x * 30, blockIdx.y);
+  pdl_trigger();
 }
 
 // y pass over the 32 x 4 element block at (x0, y0) for the node column ix; the CTA returns from
@@ -244,8 +246,10 @@ __global__ void __launch_bounds__(32 * 6) lim2d_ypass_tile_kernel(const LimArgs 
                                                                   const int* __restrict__ nbr,
                                                                   double* __restrict__ Uout,
                                                                   const DevScalars* __restrict__ scal) {
+  pdl_wait();
   if (scal && scal->flags) return;
   lim2d_ypass_body<P, METHOD, NY>(la, nx, ny, X, nbr, Uout, blockIdx.x * 32, blockIdx.y * 4, blockIdx.z);
+  pdl_trigger();
 }
 
 }  // namespace dgb

@@ -532,6 +532,7 @@ __global__ void __launch_bounds__(TW * TH, 2)
     residual2d_tile_kernel(const TileArgs a, const __grid_constant__ CUtensorMap mapU,
                            const __grid_constant__ CUtensorMap mapB) {
   extern __shared__ __align__(128) unsigned char smraw[];
+  pdl_wait();
   if (a.scal && a.scal->flags) return;
   if (threadIdx.x == 0) {
     mbar_init(reinterpret_cast<uint64_t*>(smraw), 1);
@@ -540,6 +541,7 @@ __global__ void __launch_bounds__(TW * TH, 2)
   uint32_t phase = 0;
   tile2d_body<P, FLUX, MODE, TW, TH, vol_unroll<P>(), NY, GC, TMA>(a, &mapU, &mapB, blockIdx.x * TW, blockIdx.y * TH,
                                                              smraw, phase);
+  pdl_trigger();
 }
 
 }  // namespace dgb

@@ -87,6 +87,7 @@ __global__ void __launch_bounds__(TW * TH, 3)
   double* HU = HD + TW * NF * N1;
   float* Fs = reinterpret_cast<float*>(smraw + Dm::off_face);  // [NXF + NYF][6]
 
+  pdl_wait();
   if (a.scal && a.scal->flags) return;
   const int tid = threadIdx.x;
   const int tx0 = blockIdx.x * TW, ty0 = blockIdx.y * TH;
@@ -343,6 +344,7 @@ __global__ void __launch_bounds__(TW * TH, 3)
         r4[t] = fmaf(bx.x, As[iy], r4[t]);
       }
   }
+  pdl_trigger();
   if (MODE == MODE_RESIDUAL) {
 #pragma unroll
     for (int t = 0; t < NS; ++t) {
@@ -468,6 +470,7 @@ __global__ void __launch_bounds__(TW * TH, mixed_ct_min_blocks<P>())
   double* HU = HD + TW * NF * N1;
   float* Fs = reinterpret_cast<float*>(smraw + Dm::off_face);  // [NXF + NYF][6]
 
+  pdl_wait();
   if (a.scal && a.scal->flags) return;
   const int tid = threadIdx.x;
   const int tx0 = blockIdx.x * TW, ty0 = blockIdx.y * TH;
@@ -752,6 +755,7 @@ __global__ void __launch_bounds__(TW * TH, mixed_ct_min_blocks<P>())
         r4[t] = fmaf(bx.x, As[iy], r4[t]);
       }
   }
+  pdl_trigger();
   if (MODE == MODE_RESIDUAL) {
 #pragma unroll
     for (int t = 0; t < NS; ++t) {

@@ -15,6 +15,7 @@
 #include <cstring>
 #include <mutex>
 #include <string>
+#include <utility>
 #include <vector>
 
 #include "../../include/dgb.h"
@@ -178,6 +179,24 @@ void launch_res2d(dgb_ctx* c, const StageArgs& a, const int* elist = nullptr, in
   k<<<grid, RES2D_NT, smem, c->st>>>(c->cs, s);
 }
 
+// A launch on the context's stream, programmatic (the kernel may be scheduled while its predecessor
+// finishes; it waits in pdl_wait) when the context allows it.  Only kernels that call pdl_wait
+// before touching global data are launched this way.
+template <typename... KArgs, typename... Args>
+void launch_pdl(dgb_ctx* c, void (*k)(KArgs...), dim3 grid, dim3 block, size_t smem, Args&&... args) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = grid;
+  cfg.blockDim = block;
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = c->st;
+  cudaLaunchAttribute at[1];
+  at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  at[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = at;
+  cfg.numAttrs = c->pdl ? 1 : 0;
+  cudaLaunchKernelEx(&cfg, k, std::forward<Args>(args)...);
+}
+
 template <int P, int FLUX, int MODE, int NY = 0, bool GC = false>
 void launch_res1d(dgb_ctx* c, const StageArgs& a) {
   const int grid = (c->ne + 127) / 128;
@@ -230,7 +249,7 @@ void launch_tile2d(dgb_ctx* c, const StageArgs& s) {
                           : MODE == MODE_SSP ? map_of(c, s.Ubase) : MODE == MODE_RK4 && s.Uacc ? map_of(c, s.Uacc) : mu;
   dim3 grid(c->nx / TILE_W, c->ny / TH);
   ProfScope ps(c, KC_RESIDUAL);
-  k<<<grid, TILE_W * TH, smem, c->st>>>(a, mu, mb);
+  launch_pdl(c, k, grid, dim3(TILE_W * TH), smem, a, mu, mb);
 }
 
 template <int P, int FLUX, int MODE>
@@ -244,7 +263,7 @@ void launch_tile2d_mixed(dgb_ctx* c, const StageArgs& s) {
     const TileArgs a = tile_args(c, s);
     dim3 grid(c->nx / TILE_W, c->ny / TH);
     ProfScope ps(c, KC_RESIDUAL);
-    k<<<grid, TILE_W * TH, smem, c->st>>>(a);
+    launch_pdl(c, k, grid, dim3(TILE_W * TH), smem, a);
     return;
   }
   constexpr size_t smem = TileDimsMixed<P, TILE_W, TH>::smem_bytes;
@@ -256,7 +275,7 @@ void launch_tile2d_mixed(dgb_ctx* c, const StageArgs& s) {
                           : MODE == MODE_RK4 && s.Uacc ? map_of(c, s.Uacc) : map_of(c, s.U);
   dim3 grid(c->nx / TILE_W, c->ny / TH);
   ProfScope ps(c, KC_RESIDUAL);
-  k<<<grid, TILE_W * TH, smem, c->st>>>(a, map_of(c, s.U), mb);
+  launch_pdl(c, k, grid, dim3(TILE_W * TH), smem, a, map_of(c, s.U), mb);
 }
 
 // p = 2 FP64 stage on the FP64 tensor cores (tile2d_dmma.cuh): same tiles and tensor map
@@ -442,9 +461,11 @@ void launch_lim2d(dgb_ctx* c, double* U) {
   const LimArgs la{c->ld, c->ne};
   if (c->rowmajor) {
     dim3 gx((c->nx + 29) / 30, c->ny), bx(32, P + 1);
-    lim2d_xpass_tile_kernel<P, METHOD, NY><<<gx, bx, 0, c->st>>>(la, c->nx, U, c->nbr, c->X, c->scal);
+    launch_pdl(c, lim2d_xpass_tile_kernel<P, METHOD, NY>, gx, bx, 0, la, c->nx, (const double*)U,
+               (const int*)c->nbr, c->X, (const DevScalars*)c->scal);
     dim3 gy((c->nx + 31) / 32, (c->ny + 3) / 4, P + 1), by(32, 6);
-    lim2d_ypass_tile_kernel<P, METHOD, NY><<<gy, by, 0, c->st>>>(la, c->nx, c->ny, c->X, c->nbr, U, c->scal);
+    launch_pdl(c, lim2d_ypass_tile_kernel<P, METHOD, NY>, gy, by, 0, la, c->nx, c->ny, (const double*)c->X,
+               (const int*)c->nbr, U, (const DevScalars*)c->scal);
   } else if (NY == 0) {
     dim3 grid((c->ne + 127) / 128, P + 1);
     lim2d_xpass_kernel<P, METHOD><<<grid, 128, 0, c->st>>>(la, U, c->nbr, c->X, c->scal);
@@ -700,22 +721,22 @@ void launch_wavespeed(dgb_ctx* c, const double* Uall, double* copy_to = nullptr,
   {
     if (c->gamcons) {
       switch (c->D * 100 + c->ns) {
-        case 102: wavespeed_kernel<1, 2, true><<<grid, 256, 0, c->st>>>(U, n, c->ld, c->scal, copy_to, c->nf, finish); break;
-        case 103: wavespeed_kernel<1, 3, true><<<grid, 256, 0, c->st>>>(U, n, c->ld, c->scal, copy_to, c->nf, finish); break;
-        case 104: wavespeed_kernel<1, 4, true><<<grid, 256, 0, c->st>>>(U, n, c->ld, c->scal, copy_to, c->nf, finish); break;
-        case 204: wavespeed_kernel<2, 4, true><<<grid, 256, 0, c->st>>>(U, n, c->ld, c->scal, copy_to, c->nf, finish); break;
-        case 209: wavespeed_kernel<2, 9, true><<<grid, 256, 0, c->st>>>(U, n, c->ld, c->scal, copy_to, c->nf, finish); break;
-        case 216: wavespeed_kernel<2, 16, true><<<grid, 256, 0, c->st>>>(U, n, c->ld, c->scal, copy_to, c->nf, finish); break;
+        case 102: launch_pdl(c, wavespeed_kernel<1, 2, true>, dim3(grid), dim3(256), 0, U, n, c->ld, c->scal, copy_to, c->nf, finish); break;
+        case 103: launch_pdl(c, wavespeed_kernel<1, 3, true>, dim3(grid), dim3(256), 0, U, n, c->ld, c->scal, copy_to, c->nf, finish); break;
+        case 104: launch_pdl(c, wavespeed_kernel<1, 4, true>, dim3(grid), dim3(256), 0, U, n, c->ld, c->scal, copy_to, c->nf, finish); break;
+        case 204: launch_pdl(c, wavespeed_kernel<2, 4, true>, dim3(grid), dim3(256), 0, U, n, c->ld, c->scal, copy_to, c->nf, finish); break;
+        case 209: launch_pdl(c, wavespeed_kernel<2, 9, true>, dim3(grid), dim3(256), 0, U, n, c->ld, c->scal, copy_to, c->nf, finish); break;
+        case 216: launch_pdl(c, wavespeed_kernel<2, 16, true>, dim3(grid), dim3(256), 0, U, n, c->ld, c->scal, copy_to, c->nf, finish); break;
         default: break;
       }
     } else
     switch (c->D * 100 + c->ns) {
-      case 102: wavespeed_kernel<1, 2><<<grid, 256, 0, c->st>>>(U, n, c->ld, c->scal, copy_to, c->nf, finish); break;
-      case 103: wavespeed_kernel<1, 3><<<grid, 256, 0, c->st>>>(U, n, c->ld, c->scal, copy_to, c->nf, finish); break;
-      case 104: wavespeed_kernel<1, 4><<<grid, 256, 0, c->st>>>(U, n, c->ld, c->scal, copy_to, c->nf, finish); break;
-      case 204: wavespeed_kernel<2, 4><<<grid, 256, 0, c->st>>>(U, n, c->ld, c->scal, copy_to, c->nf, finish); break;
-      case 209: wavespeed_kernel<2, 9><<<grid, 256, 0, c->st>>>(U, n, c->ld, c->scal, copy_to, c->nf, finish); break;
-      case 216: wavespeed_kernel<2, 16><<<grid, 256, 0, c->st>>>(U, n, c->ld, c->scal, copy_to, c->nf, finish); break;
+      case 102: launch_pdl(c, wavespeed_kernel<1, 2>, dim3(grid), dim3(256), 0, U, n, c->ld, c->scal, copy_to, c->nf, finish); break;
+      case 103: launch_pdl(c, wavespeed_kernel<1, 3>, dim3(grid), dim3(256), 0, U, n, c->ld, c->scal, copy_to, c->nf, finish); break;
+      case 104: launch_pdl(c, wavespeed_kernel<1, 4>, dim3(grid), dim3(256), 0, U, n, c->ld, c->scal, copy_to, c->nf, finish); break;
+      case 204: launch_pdl(c, wavespeed_kernel<2, 4>, dim3(grid), dim3(256), 0, U, n, c->ld, c->scal, copy_to, c->nf, finish); break;
+      case 209: launch_pdl(c, wavespeed_kernel<2, 9>, dim3(grid), dim3(256), 0, U, n, c->ld, c->scal, copy_to, c->nf, finish); break;
+      case 216: launch_pdl(c, wavespeed_kernel<2, 16>, dim3(grid), dim3(256), 0, U, n, c->ld, c->scal, copy_to, c->nf, finish); break;
       default: break;
     }
   }
@@ -1041,6 +1062,9 @@ extern "C" int dgb_create(const dgb_problem* prob, int device, dgb_ctx** out) {
     // mixed-form tiles: the compressed shared tile (FP64 anchors + FP32 deviations, plain loads)
     // at p = 3, the TMA-loaded FP64 tile at p = 1, 2 (the faster of the two at each order);
     // DGB_MIXED_TILE=ct / tma selects one for every order
+    // programmatic dependent launches of the 2D step's kernels unless DGB_PDL=0
+    const char* pk = std::getenv("DGB_PDL");
+    c->pdl = !(pk && std::string(pk) == "0");
     const char* mk = std::getenv("DGB_MIXED_TILE");
     c->mixed_ct = mk ? std::string(mk) == "ct" : P.p == 3;
   }
