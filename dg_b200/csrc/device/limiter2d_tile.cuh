@@ -15,6 +15,19 @@
 
 namespace dgb {
 
+// Dynamic shared memory of the tiled limiter passes: 0 while their per-quantity arrays fit the
+// static limit (up to three mass fractions), else the arrays' size
+template <int P, int NY>
+constexpr size_t lim2d_xpass_smem_bytes() {
+  const size_t b = sizeof(double) * (5 + NY) * (P + 1) * (P + 1) * 32;
+  return b <= 48 * 1024 ? 0 : b;
+}
+template <int P, int NY>
+constexpr size_t lim2d_ypass_smem_bytes() {
+  const size_t b = sizeof(double) * (5 + NY) * (P + 1) * 6 * 32;
+  return b <= 48 * 1024 ? 0 : b;
+}
+
 // x pass over one block of the row ey starting at element column x0 (a multiple of 30); the CTA
 // returns from here together, after its last barrier
 // NY mass fractions: limited like the density (m2: the MACRO blocks of M2limiting,
@@ -24,7 +37,16 @@ __device__ __forceinline__ void lim2d_xpass_body(const LimArgs la, int nx, const
                                                  const int* __restrict__ nbr, double* __restrict__ X, int x0,
                                                  int ey) {
   constexpr int N1 = P + 1, NS = N1 * N1, NQ = 5 + NY, NF = 5 + NY, TWI = 30;
-  __shared__ double A[NQ][N1][N1][32];  // [quantity][slice][coefficient][slot]
+  // [quantity][slice][coefficient][slot]: static shared memory, or dynamic (lim2d_xpass_smem_bytes)
+  // when the quantities would not fit the static limit (many mass fractions)
+  double(*A)[N1][N1][32];
+  if constexpr (lim2d_xpass_smem_bytes<P, NY>() == 0) {
+    __shared__ double As[NQ][N1][N1][32];
+    A = As;
+  } else {
+    extern __shared__ __align__(16) double lsm[];
+    A = reinterpret_cast<double(*)[N1][N1][32]>(lsm);
+  }
   const int ld = la.ld;
   const int tx = threadIdx.x, sl = threadIdx.y;
   const int ex = x0 - 1 + tx;
@@ -151,7 +173,15 @@ __device__ __forceinline__ void lim2d_ypass_body(const LimArgs la, int nx, int n
   constexpr int N1 = P + 1, NS = N1 * N1, NQ = 5 + NY, THI = 4;
   // row of quantity k in X: HR -> field k; m2 -> [rho, rhou, rhov, alpha, p, E, rho Y_k]
   auto xrow = [](int k) { return (METHOD == 2 && k >= 5) ? k + 1 : k; };
-  __shared__ double B[NQ][N1][THI + 2][32];  // [quantity][coefficient][row slot][x slot]
+  // [quantity][coefficient][row slot][x slot]: static or (many mass fractions) dynamic
+  double(*B)[N1][THI + 2][32];
+  if constexpr (lim2d_ypass_smem_bytes<P, NY>() == 0) {
+    __shared__ double Bs[NQ][N1][THI + 2][32];
+    B = Bs;
+  } else {
+    extern __shared__ __align__(16) double lsm[];
+    B = reinterpret_cast<double(*)[N1][THI + 2][32]>(lsm);
+  }
   const int ld = la.ld;
   const int tx = threadIdx.x, ty = threadIdx.y;
   const int x = x0 + tx;

@@ -73,10 +73,11 @@ struct TileDims {
   static constexpr size_t tile_doubles = (size_t)NF * NS * NT;
   static constexpr uint32_t tile_bytes = (uint32_t)(tile_doubles * 8);
   static constexpr size_t halo_doubles = (size_t)2 * TH * NF * N1 + (size_t)2 * TW * NF * N1;
-  // p = 3: the x-faces and then the y-faces pass through one face buffer, and the stage base is read
-  // from global memory in the epilogue instead of being prefetched into it -- 70 instead of 93 KB
-  // per 64-thread CTA, three CTAs per SM instead of two
-  static constexpr bool split_faces = P == 3;
+  // p = 3, or more than three mass fractions: the x-faces and then the y-faces pass through one
+  // face buffer, and the stage base is read from global memory in the epilogue instead of being
+  // prefetched into it (p = 3: 70 instead of 93 KB per 64-thread CTA, three CTAs per SM instead of
+  // two; ten mass fractions at p = 2: 131 KB, within one CTA's limit)
+  static constexpr bool split_faces = P == 3 || NY > 3;
   static constexpr int NFREC = split_faces ? (NXF > NYF ? NXF : NYF) : NXF + NYF;  // face records held
   static constexpr size_t face_doubles = (size_t)(NF + 1) * NFREC;  // NF fluxes + ncterm per point
   // otherwise the face buffer is reused for the prefetched stage base, so it is at least one tile

@@ -29,12 +29,15 @@
 #include "device/learned_tc.cuh"
 #include "device/tables.cuh"
 #include "device/sensor.h"
+#include "launch.h"
 
 namespace dgb {
-// 1D with 4 to 10 mass fractions (dgb_device_ny.cu)
+// 4 to 10 mass fractions (dgb_device_ny.cu)
 int residual1d_many_y(dgb_ctx* c, const StageArgs& a, int mode);
 int limit1d_many_y(dgb_ctx* c, const double* in, double* out);
-int upload_many_y_tables(const Consts& cs, int p);
+int residual2d_many_y(dgb_ctx* c, const StageArgs& a, int mode);
+int limit2d_many_y(dgb_ctx* c, double* U);
+int upload_many_y_tables(const Consts& cs, int D, int p);
 }  // namespace dgb
 #include "host/host.h"
 #include "ctx.h"
@@ -179,77 +182,11 @@ void launch_res2d(dgb_ctx* c, const StageArgs& a, const int* elist = nullptr, in
   k<<<grid, RES2D_NT, smem, c->st>>>(c->cs, s);
 }
 
-// A launch on the context's stream, programmatic (the kernel may be scheduled while its predecessor
-// finishes; it waits in pdl_wait) when the context allows it.  Only kernels that call pdl_wait
-// before touching global data are launched this way.
-template <typename... KArgs, typename... Args>
-void launch_pdl(dgb_ctx* c, void (*k)(KArgs...), dim3 grid, dim3 block, size_t smem, Args&&... args) {
-  cudaLaunchConfig_t cfg = {};
-  cfg.gridDim = grid;
-  cfg.blockDim = block;
-  cfg.dynamicSmemBytes = smem;
-  cfg.stream = c->st;
-  cudaLaunchAttribute at[1];
-  at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
-  at[0].val.programmaticStreamSerializationAllowed = 1;
-  cfg.attrs = at;
-  cfg.numAttrs = c->pdl ? 1 : 0;
-  cudaLaunchKernelEx(&cfg, k, std::forward<Args>(args)...);
-}
-
 template <int P, int FLUX, int MODE, int NY = 0, bool GC = false>
 void launch_res1d(dgb_ctx* c, const StageArgs& a) {
   const int grid = (c->ne + 127) / 128;
   ProfScope ps(c, KC_RESIDUAL);
   residual1d_kernel<P, FLUX, MODE, NY, GC><<<grid, 128, 0, c->st>>>(c->cs, a);
-}
-
-constexpr int TILE_W = 32, TILE_H = 4;
-// p = 3 tiles are two element rows high: the per-element register state (80 nodal values per
-// field set) and the shared tile then leave room for two (FP64) or three (mixed) CTAs per SM
-constexpr int tile_h_for(int p) { return p == 3 ? 2 : TILE_H; }
-
-const CUtensorMap& map_of(dgb_ctx* c, const double* p) {
-  if (p == c->B) return c->mapB;
-  if (p == c->C) return c->mapC;
-  return c->mapA;
-}
-
-// kernel arguments of the tiled residuals for one stage
-TileArgs tile_args(dgb_ctx* c, const StageArgs& s) {
-  TileArgs a;
-  a.U = s.U; a.Ubase = s.Ubase; a.out = s.out; a.Uacc = s.Uacc; a.nbr = s.nbr; a.scal = s.scal;
-  a.errflag = &c->scal->flags;
-  a.polls = c->wait_polls;
-  a.a = s.a; a.b = s.b; a.dt_override = s.dt_override;
-  a.J = c->cs.J;
-  a.invJ = 1.0 / c->cs.J;
-  a.cx = c->cs.J * c->cs.ixx;
-  a.cy = c->cs.J * c->cs.iyy;
-  a.sx = c->cs.ixx;
-  a.sy = c->cs.iyy;
-  a.JFx = c->cs.JFx;
-  a.JFy = c->cs.JFy;
-  a.nx = c->nx; a.ny = c->ny; a.ld = c->ld;
-  return a;
-}
-
-template <int P, int FLUX, int MODE, int NY = 0, bool GC = false, bool TMA = true>
-void launch_tile2d(dgb_ctx* c, const StageArgs& s) {
-  constexpr int TH = tile_h_for(P);
-  using Dm = TileDims<P, TILE_W, TH, NY>;
-  constexpr size_t smem = Dm::smem_bytes;
-  auto k = residual2d_tile_kernel<P, FLUX, MODE, TILE_W, TH, NY, GC, TMA>;
-  static bool attr = false;
-  if (!attr) { cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem); attr = true; }
-  const TileArgs a = tile_args(c, s);
-  // (without TMA the maps are not read: the tile loads are plain)
-  const CUtensorMap& mu = TMA ? map_of(c, s.U) : c->mapA;
-  const CUtensorMap& mb = !TMA ? c->mapA
-                          : MODE == MODE_SSP ? map_of(c, s.Ubase) : MODE == MODE_RK4 && s.Uacc ? map_of(c, s.Uacc) : mu;
-  dim3 grid(c->nx / TILE_W, c->ny / TH);
-  ProfScope ps(c, KC_RESIDUAL);
-  launch_pdl(c, k, grid, dim3(TILE_W * TH), smem, a, mu, mb);
 }
 
 template <int P, int FLUX, int MODE>
@@ -399,9 +336,7 @@ int residual_dispatch(dgb_ctx* c, const StageArgs& a) {
       case 1: return residual_ny<MODE, 1>(c, a);
       case 2: return residual_ny<MODE, 2>(c, a);
       case 3: return residual_ny<MODE, 3>(c, a);
-      default:
-        if (c->D == 1) return residual1d_many_y(c, a, MODE);
-        return set_error(DGB_ERR_UNSUPPORTED, "at most three mass fractions on the 2D device path");
+      default: return c->D == 1 ? residual1d_many_y(c, a, MODE) : residual2d_many_y(c, a, MODE);
     }
   }
   if (c->tiled) {
@@ -697,7 +632,7 @@ int limit_dispatch(dgb_ctx* c, double* U, bool rescore = true) {
         DGB_CUDA(cudaMemcpyAsync(U, c->X, c->nstate * sizeof(double), cudaMemcpyDeviceToDevice, c->st));
         return 0;
       }
-      return set_error(DGB_ERR_UNSUPPORTED, "at most three mass fractions on the 2D device path");
+      return limit2d_many_y(c, U);
   }
 #define L2(P, M) case P * 10 + M: launch_lim2d<P, M>(c, U); return 0;
 #define L1(P, M) case P * 10 + M: launch_lim1d<P, M>(c, U); return 0;
@@ -1086,9 +1021,9 @@ extern "C" int dgb_create(const dgb_problem* prob, int device, dgb_ctx** out) {
   // tiled residual over the full tiles; the strips left over on other extents go to the generic
   // kernel.  Tile loads by TMA where the tensor map's row pitch nx * 8 bytes is a multiple of 16
   // (nx even), by plain loads otherwise
-  c->tiled = c->rowmajor && P.p <= 3 && P.nx >= TILE_W && P.ny >= tile_h_for(P.p);
+  c->tiled = c->rowmajor && P.p <= 3 && P.nx >= TILE_W && P.ny >= tile_h_for(P.p, P.N_Y);
   c->tile_tma = c->tiled && P.nx % 2 == 0;
-  c->tiled_full = c->tile_tma && P.nx % TILE_W == 0 && P.ny % tile_h_for(P.p) == 0;
+  c->tiled_full = c->tile_tma && P.nx % TILE_W == 0 && P.ny % tile_h_for(P.p, P.N_Y) == 0;
   // opt-in: measured slower than the two tiled passes on 512 x 256, p = 2 (64 vs 55 us per stage)
   c->fused_lim = c->rowmajor && (P.limiter == DGB_LIM_HRL || P.limiter == DGB_LIM_M2L) &&
                  std::getenv("DGB_FUSED_LIMITER") != nullptr && P.N_Y == 0;
@@ -1108,17 +1043,14 @@ extern "C" int dgb_create(const dgb_problem* prob, int device, dgb_ctx** out) {
     if (why) { delete c; return set_error(DGB_ERR_UNSUPPORTED, why); }
     c->fused_lim = false;
   }
-  if (P.N_Y > (P.D == 1 ? 10 : 3)) {
-    delete c;
-    return set_error(DGB_ERR_UNSUPPORTED, "mass fractions on the device path: up to 10 in 1D, up to 3 in 2D");
-  }
-  if (P.D == 1 && P.N_Y > 3) {
-    if (int rc = upload_many_y_tables(c->cs, P.p)) { delete c; return rc; }
+  if (P.N_Y > 10) { delete c; return set_error(DGB_ERR_UNSUPPORTED, "at most ten mass fractions"); }
+  if (P.N_Y > 3) {
+    if (int rc = upload_many_y_tables(c->cs, P.D, P.p)) { delete c; return rc; }
   }
   if (P.N_Y > 0 && P.D == 2 && !c->tiled_full) {
     delete c;
     return set_error(DGB_ERR_UNSUPPORTED, "mass fractions in 2D need a structured row-major grid with nx a multiple "
-                                          "of 32 and ny of 4 (p = 3: 2)");
+                                          "of 32 and ny of 4 (p = 3 or more than three mass fractions: 2)");
   }
   if (P.N_Y > 0 && P.limiter != DGB_LIM_NONE && P.limiter != DGB_LIM_HRL && P.limiter != DGB_LIM_M2L) {
     delete c;
@@ -1190,7 +1122,7 @@ extern "C" int dgb_create(const dgb_problem* prob, int device, dgb_ctx** out) {
   std::memset(&c->mapC, 0, sizeof(CUtensorMap));
   if (c->tile_tma) {
     // row starts must be 16-byte aligned for TMA: nx is even and ld a multiple of 64
-    const int th = tile_h_for(P.p);
+    const int th = tile_h_for(P.p, P.N_Y);
     if (!(encode_state_map(c, c->A, &c->mapA, TILE_W, th) && encode_state_map(c, c->B, &c->mapB, TILE_W, th) &&
           encode_state_map(c, c->C, &c->mapC, TILE_W, th))) {
       if (P.N_Y > 0 || P.gamcons) return fail(cudaErrorInvalidValue, "tensor maps for the tiled residual");
@@ -1199,7 +1131,7 @@ extern "C" int dgb_create(const dgb_problem* prob, int device, dgb_ctx** out) {
   }
   if (c->tiled && !c->tiled_full) {
     // the right strip (rows of the full tiles) and the top strip (all columns), in element order
-    const int th = tile_h_for(P.p), nxt = P.nx / TILE_W * TILE_W, nyt = P.ny / th * th;
+    const int th = tile_h_for(P.p, P.N_Y), nxt = P.nx / TILE_W * TILE_W, nyt = P.ny / th * th;
     std::vector<int> left;
     for (int y = 0; y < P.ny; ++y)
       for (int x = (y < nyt ? nxt : 0); x < P.nx; ++x) left.push_back(y * P.nx + x);

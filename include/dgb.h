@@ -104,8 +104,7 @@ typedef struct {
   double thresholds[3];/* sensor thresholds (sensor.h:35-45); n_thresholds of them are set */
   int n_thresholds;
   int n_mass;          /* passive mass fractions rho*Y_k appended to the state (MASS of the
-                        * reference Makefile, 0..10; N_F = 4 (1D) / 5 (2D) + n_mass; the device
-                        * path takes 0..10 in 1D, 0..3 in 2D) */
+                        * reference Makefile, 0..10; N_F = 4 (1D) / 5 (2D) + n_mass) */
   int gamma_model;     /* enum dgb_gamma_model */
 } dgb_options;
 

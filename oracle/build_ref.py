@@ -72,9 +72,11 @@ VARIANTS = {
     "1d_hll_y3": dict(dims="ONED", nf=7, d=1, flux="HLL", ny=3),
     "2d_rus_y2": dict(dims="TWOD", nf=7, d=2, flux="RUS", ny=2),
     "2d_roe_y3": dict(dims="TWOD", nf=8, d=2, flux="ROE", ny=3),
-    # five and ten (MASS=5, MASS=10; the reference's maximum), 1D
+    # five and ten (MASS=5, MASS=10; the reference's maximum)
     "1d_rus_y5": dict(dims="ONED", nf=9, d=1, flux="RUS", ny=5),
     "1d_roe_y10": dict(dims="ONED", nf=14, d=1, flux="ROE", ny=10),
+    "2d_roe_y5": dict(dims="TWOD", nf=10, d=2, flux="ROE", ny=5),
+    "2d_rus_y10": dict(dims="TWOD", nf=15, d=2, flux="RUS", ny=10),
     # the ERROR diagnostic compiled in (ERRR=ERROR in code/Makefile): error.dat after the run
     "1d_rus_err": dict(dims="ONED", nf=4, d=1, flux="RUS", err=True),
     # the conservative gamma model (GAMM=GAMCONS in code/Makefile): rho/(gamma-1) as the field

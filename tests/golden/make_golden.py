@@ -129,6 +129,12 @@ CASES = [
          flux="roe", limiter="m2l", ic="tube_noise", cfl=0.4, dt=4e-4, nsteps=5, n_mass=10),
     dict(name="m5_d1_p3_rus_hrl_wall", dim=1, order=3, nx=20, ny=1, dom=(0, 1, 0, 1), bc=("reflective",) * 2,
          flux="rusanov", limiter="hrl", ic="riemann", cfl=0.2, dt=2e-4, nsteps=5, n_mass=5),
+    # ten and five in 2D (tile-aligned: the device path takes mass fractions on full tiles)
+    dict(name="m10_d2_p2_rus_m2l_walls", dim=2, order=2, nx=32, ny=4, dom=(0, 2, 0, 1),
+         bc=("reflective", "transmissive", "reflective", "transmissive"), flux="rusanov", limiter="m2l",
+         ic="shock_bubble", cfl=0.3, dt=5e-4, nsteps=4, n_mass=10),
+    dict(name="m5_d2_p3_roe_hrl_periodic", dim=2, order=3, nx=32, ny=4, dom=(0, 1, 0, 1), bc=("periodic",) * 4,
+         flux="roe", limiter="hrl", ic="quadrants", cfl=0.3, dt=2.5e-4, nsteps=4, n_mass=5),
 ]
 
 

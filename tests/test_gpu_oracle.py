@@ -1,7 +1,7 @@
 """CUDA path (through the C ABI) against the numpy oracle at sizes and seeds the golden fixtures
 do not cover: ragged grids (extents not multiples of the 32 x 4 element tile), tile-aligned grids
 (tiled kernels), p = 1..3, all fluxes, both limiters, walls / periodic / transmissive
-boundaries, one to three passive mass fractions, the GAMCONS gamma model, the 1D shock-tube workload (1000 elements, p=2, Roe, m2l,
+boundaries, one to ten passive mass fractions, the GAMCONS gamma model, the 1D shock-tube workload (1000 elements, p=2, Roe, m2l,
 RK4) and the 2D shock-bubble workload at its full size (512 x 256 elements, p=2, Rusanov, m2l,
 SSP-RK3).
 
@@ -47,6 +47,13 @@ CASES = [
     ("2d_p3_rus_hrl_tiled_periodic_y2", 2, 3, 32, 8, ("periodic",) * 4, "rusanov", "hrl", "quadrants", 0.3, 2),
     ("1d_p2_rus_m2l_y2", 1, 2, 201, 1, ("transmissive",) * 2, "rusanov", "m2l", "tube_noise", 0.3, 2),
     ("1d_p1_roe_hrl_periodic_y3", 1, 1, 150, 1, ("periodic",) * 2, "roe", "hrl", "riemann", 0.3, 3),
+    # four to ten (2D on 32 x 2 tiles, the faces through one buffer, the limiter passes' arrays in
+    # dynamic shared memory)
+    ("2d_p2_rus_m2l_tiled_walls_y10", 2, 2, 64, 10, WALLS, "rusanov", "m2l", "shock_bubble", 0.3, 10),
+    ("2d_p1_roe_hrl_tiled_periodic_y7", 2, 1, 64, 6, ("periodic",) * 4, "roe", "hrl", "quadrants", 0.3, 7),
+    ("2d_p3_roe_m2l_tiled_box_y4", 2, 3, 32, 6, ("reflective",) * 4, "roe", "m2l", "quadrants", 0.3, 4),
+    ("1d_p2_hll_m2l_y8", 1, 2, 180, 1, ("transmissive",) * 2, "hll", "m2l", "tube_noise", 0.3, 8),
+    ("1d_p3_roe_hrl_walls_y6", 1, 3, 90, 1, ("reflective",) * 2, "roe", "hrl", "riemann", 0.15, 6),
     # the GAMCONS gamma model (last entry); limiters hrl and none (the reference's M2limiting stops
     # for this model)
     ("2d_p2_rus_hrl_tiled_walls_gc", 2, 2, 64, 16, WALLS, "rusanov", "hrl", "shock_bubble", 0.3, 0, "gamcons"),
@@ -182,7 +189,8 @@ def test_mass_fraction_configurations_outside_the_device_path_are_rejected():
         with pytest.raises(dgb.DGBError) as e:
             dgb.DGSolver(prob)
         assert e.value.code == 4
-    prob = dgb.Problem.structured(2, 2, 32, 8, flux="rusanov", limiter="m2l", cfl=0.3, n_mass=4)
+    # four or more mass fractions run on 32 x 2 tiles: an odd number of element rows is refused
+    prob = dgb.Problem.structured(2, 2, 32, 7, flux="rusanov", limiter="m2l", cfl=0.3, n_mass=4)
     with pytest.raises(dgb.DGBError) as e:
         dgb.DGSolver(prob)
     assert e.value.code == 4
