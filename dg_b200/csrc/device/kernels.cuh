@@ -56,11 +56,19 @@ struct Dims2 {
   static constexpr int NG = NG1 * NG1;
   static constexpr int NF = 5;
 };
+// NY mass fractions / the GAMCONS model: NF fields, NFL of them with a conservative volume flux,
+// NGV volume slots per quadrature point (x and y flux of each, and the alpha source under GAMNCON)
+template <int P, int NY, bool GC>
+struct Dims2V : Dims2<P> {
+  static constexpr int NF = 5 + NY;
+  static constexpr int NFL = 4 + NY + (GC ? 1 : 0);
+  static constexpr int NGV = 2 * NFL + (GC ? 0 : 1);
+};
 
-template <int P, int TE>
+template <int P, int TE, int NY = 0, bool GC = false>
 constexpr size_t residual2d_smem_doubles() {
-  using Dm = Dims2<P>;
-  constexpr size_t g1 = (size_t)9 * Dm::NG * TE;
+  using Dm = Dims2V<P, NY, GC>;
+  constexpr size_t g1 = (size_t)Dm::NGV * Dm::NG * TE;
   constexpr size_t g2 = (size_t)Dm::NF * 4 * Dm::N1 * TE;
   return (size_t)Dm::NF * Dm::NS * TE * 2 + (size_t)4 * Dm::NF * Dm::N1 * TE + (g1 > g2 ? g1 : g2) +
          (size_t)3 * Dm::NG * Dm::NS;
@@ -79,11 +87,12 @@ __device__ __forceinline__ int across_node(int k, int j) {
   return k == 0 ? P + N1 * j : k == 1 ? N1 * j : k == 2 ? j + N1 * P : j;
 }
 
-template <int P, int FLUX, int MODE, int TE, int NT>
+template <int P, int FLUX, int MODE, int TE, int NT, int NY = 0, bool GC = false>
 __global__ void __launch_bounds__(NT) residual2d_kernel(const Consts cin, const StageArgs a) {
-  using Dm = Dims2<P>;
-  constexpr int N1 = Dm::N1, NG1 = Dm::NG1, NS = Dm::NS, NG = Dm::NG, NF = Dm::NF;
-  constexpr int GSZ = (9 * NG * TE > NF * 4 * N1 * TE) ? 9 * NG * TE : NF * 4 * N1 * TE;
+  static_assert(!(GC && NY > 0), "GAMCONS with mass fractions is not built");
+  using Dm = Dims2V<P, NY, GC>;
+  constexpr int N1 = Dm::N1, NG1 = Dm::NG1, NS = Dm::NS, NG = Dm::NG, NF = Dm::NF, NFL = Dm::NFL, NGV = Dm::NGV;
+  constexpr int GSZ = (NGV * NG * TE > NF * 4 * N1 * TE) ? NGV * NG * TE : NF * 4 * N1 * TE;
   __shared__ Consts c;
   extern __shared__ double sm[];
   double* Us = sm;                        // [NF][NS][TE]
@@ -142,7 +151,9 @@ __global__ void __launch_bounds__(NT) residual2d_kernel(const Consts cin, const 
   for (int i = tid; i < NG * TE; i += NT) {
     const int el = i % TE, g = i / TE;
     if (elem(el) < 0) continue;
-    double ug[NF] = {0, 0, 0, 0, 0}, dax = 0, day = 0;
+    double ug[NF], dax = 0, day = 0;
+#pragma unroll
+    for (int f = 0; f < NF; ++f) ug[f] = 0.0;
 #pragma unroll
     for (int t = 0; t < NS; ++t) {
       const double ph = Phi[g * NS + t];
@@ -151,6 +162,31 @@ __global__ void __launch_bounds__(NT) residual2d_kernel(const Consts cin, const 
       const double al = Us[(4 * NS + t) * TE + el];
       dax += dPx[g * NS + t] * al;
       day += dPy[g * NS + t] * al;
+    }
+    if constexpr (NY > 0 || GC) {
+      // the volume terms of the tiled kernel's point_terms: the conservative fluxes of the NFL
+      // fields (mass fractions rho Y_k u, physics.cu:293-298; GAMCONS alpha flux rho u/(gamma-1),
+      // physics.cu:253-281) and, under GAMNCON, the alpha source
+      const double rho = ug[0], irho = __drcp_rn(rho);
+      const double uu = ug[1] * irho, vv = ug[2] * irho, Et = ug[3];
+      const double gm1 = GC ? rho * __drcp_rn(ug[4]) : __drcp_rn(ug[4]);
+      const double p = gm1 * (Et - 0.5 * rho * (uu * uu + vv * vv));
+      const double W = c.wq[g / NG1] * c.wq[g % NG1];
+      const double wx = W * (c.J * c.ixx), wy = W * (c.J * c.iyy);
+      const double mx = ug[1] * wx, my = ug[2] * wy;
+      double gxv[NFL], gyv[NFL];
+      gxv[0] = mx; gxv[1] = mx * uu + wx * p; gxv[2] = mx * vv; gxv[3] = wx * ((Et + p) * uu);
+      gyv[0] = my; gyv[1] = my * uu; gyv[2] = my * vv + wy * p; gyv[3] = wy * ((Et + p) * vv);
+#pragma unroll
+      for (int k = 0; k < NY; ++k) { gxv[4 + k] = wx * (ug[5 + k] * uu); gyv[4 + k] = wy * (ug[5 + k] * vv); }
+      if constexpr (GC) { gxv[4] = wx * (ug[4] * uu); gyv[4] = wy * (ug[4] * vv); }
+#pragma unroll
+      for (int q = 0; q < NFL; ++q) {
+        G[(q * NG + g) * TE + el] = gxv[q];
+        G[((NFL + q) * NG + g) * TE + el] = gyv[q];
+      }
+      if constexpr (!GC) G[(2 * NFL * NG + g) * TE + el] = (W * c.J) * (-uu * dax * c.ixx - vv * day * c.iyy);
+      continue;
     }
     // physics.cu:248-257 with correctly rounded reciprocals in place of its divisions
     const double rho = ug[0], ir = __drcp_rn(rho), u = ug[1] * ir, v = ug[2] * ir, Et = ug[3];
@@ -174,6 +210,20 @@ __global__ void __launch_bounds__(NT) residual2d_kernel(const Consts cin, const 
   for (int i = tid; i < NF * NS * TE; i += NT) {
     const int el = i % TE, ft = i / TE, f = ft / NS, t = ft % NS;
     double r = 0.0;
+    if constexpr (NY > 0 || GC) {
+      // flux slot of field f: rho, rho u, rho v, E; alpha (GAMCONS) or rho Y_k after them
+      const int q = f < 4 ? f : GC ? 4 : f - 1;
+      if (f == 4 && !GC) {
+#pragma unroll 4
+        for (int g = 0; g < NG; ++g) r += Phi[g * NS + t] * G[(2 * NFL * NG + g) * TE + el];
+      } else {
+#pragma unroll 4
+        for (int g = 0; g < NG; ++g)
+          r += dPx[g * NS + t] * G[(q * NG + g) * TE + el] + dPy[g * NS + t] * G[((NFL + q) * NG + g) * TE + el];
+      }
+      Rs[i] = r;
+      continue;
+    }
     if (f < 4) {
 #pragma unroll 4
       for (int g = 0; g < NG; ++g)
@@ -214,7 +264,7 @@ __global__ void __launch_bounds__(NT) residual2d_kernel(const Consts cin, const 
 #pragma unroll
     for (int f = 0; f < NF; ++f) { L[f] = swapLR ? un[f] : uo[f]; R[f] = swapLR ? uo[f] : un[f]; }
     double F[NF], nc;
-    phys::riemann2d_rcp<FLUX>(L, R, nx, ny, F, nc);  // the tiled kernel's flux (reciprocals for divisions)
+    phys::riemann2d_rcp<FLUX, NY, GC>(L, R, nx, ny, F, nc);  // the tiled kernel's flux (reciprocals for divisions)
     const double jw = (xface ? c.JFx : c.JFy) * c.wf[g];
 #pragma unroll
     for (int f = 0; f < NF; ++f) {

@@ -58,8 +58,6 @@ using namespace dgb;
 
 namespace {
 
-constexpr int RES2D_TE = 16;
-constexpr int RES2D_NT = 256;
 
 double fact(int n) { double f = 1; for (int i = 2; i <= n; ++i) f *= i; return f; }
 
@@ -167,20 +165,6 @@ bool is_row_major_grid(const Problem& P) {
 namespace {
 
 
-// generic 2D residual over every element, or over the listed ones (elist, n)
-template <int P, int FLUX, int MODE>
-void launch_res2d(dgb_ctx* c, const StageArgs& a, const int* elist = nullptr, int n = 0) {
-  constexpr size_t smem = residual2d_smem_doubles<P, RES2D_TE>() * sizeof(double);
-  auto k = residual2d_kernel<P, FLUX, MODE, RES2D_TE, RES2D_NT>;
-  static bool attr = false;
-  if (!attr) { cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem); attr = true; }
-  StageArgs s = a;
-  s.elist = elist;
-  s.nlist = n;
-  const int grid = ((elist ? n : c->ne) + RES2D_TE - 1) / RES2D_TE;
-  ProfScope ps(c, KC_RESIDUAL);
-  k<<<grid, RES2D_NT, smem, c->st>>>(c->cs, s);
-}
 
 template <int P, int FLUX, int MODE, int NY = 0, bool GC = false>
 void launch_res1d(dgb_ctx* c, const StageArgs& a) {
@@ -257,16 +241,17 @@ namespace {
 // NY passive mass fractions (1D or tiled 2D, FP64 form; checked at create)
 template <int MODE, int NY>
 int residual_ny(dgb_ctx* c, const StageArgs& a) {
-  if (c->tiled_full) {
+  if (c->tile_tma) {  // full tiles, then the strips outside them (if any) with the generic kernel
+#define T2Y(P, F)                                                               \
+  case P * 10 + F:                                                              \
+    launch_tile2d<P, F, MODE, NY>(c, a);                                        \
+    if (c->nleft) launch_res2d<P, F, MODE, NY>(c, a, c->left, c->nleft);        \
+    return 0;
     switch (c->p * 10 + c->flux) {
-      case 10: launch_tile2d<1, 0, MODE, NY>(c, a); return 0;
-      case 12: launch_tile2d<1, 2, MODE, NY>(c, a); return 0;
-      case 20: launch_tile2d<2, 0, MODE, NY>(c, a); return 0;
-      case 22: launch_tile2d<2, 2, MODE, NY>(c, a); return 0;
-      case 30: launch_tile2d<3, 0, MODE, NY>(c, a); return 0;
-      case 32: launch_tile2d<3, 2, MODE, NY>(c, a); return 0;
+      T2Y(1, 0) T2Y(1, 2) T2Y(2, 0) T2Y(2, 2) T2Y(3, 0) T2Y(3, 2)
       default: return set_error(DGB_ERR_UNSUPPORTED, "no residual kernel for this (p, flux) with mass fractions");
     }
+#undef T2Y
   }
   if (c->D == 1) {
 #define R1Y(P, F) case P * 10 + F: launch_res1d<P, F, MODE, NY>(c, a); return 0;
@@ -313,16 +298,17 @@ int residual_dispatch(dgb_ctx* c, const StageArgs& a) {
     }
   }
   if (c->gamcons) {  // GAMCONS: tiled 2D or 1D, FP64 form, no mass fractions (checked at create)
-    if (c->D == 2) {
+    if (c->D == 2) {  // full tiles, then the strips outside them (if any) with the generic kernel
+#define T2G(P, F)                                                               \
+  case P * 10 + F:                                                              \
+    launch_tile2d<P, F, MODE, 0, true>(c, a);                                   \
+    if (c->nleft) launch_res2d<P, F, MODE, 0, true>(c, a, c->left, c->nleft);   \
+    return 0;
       switch (c->p * 10 + c->flux) {
-        case 10: launch_tile2d<1, 0, MODE, 0, true>(c, a); return 0;
-        case 12: launch_tile2d<1, 2, MODE, 0, true>(c, a); return 0;
-        case 20: launch_tile2d<2, 0, MODE, 0, true>(c, a); return 0;
-        case 22: launch_tile2d<2, 2, MODE, 0, true>(c, a); return 0;
-        case 30: launch_tile2d<3, 0, MODE, 0, true>(c, a); return 0;
-        case 32: launch_tile2d<3, 2, MODE, 0, true>(c, a); return 0;
+        T2G(1, 0) T2G(1, 2) T2G(2, 0) T2G(2, 2) T2G(3, 0) T2G(3, 2)
         default: return set_error(DGB_ERR_UNSUPPORTED, "no GAMCONS residual kernel for this (p, flux)");
       }
+#undef T2G
     }
 #define R1G(P, F) case P * 10 + F: launch_res1d<P, F, MODE, 0, true>(c, a); return 0;
     switch (c->p * 10 + c->flux) {
@@ -1032,8 +1018,9 @@ extern "C" int dgb_create(const dgb_problem* prob, int device, dgb_ctx** out) {
   if (P.gamcons) {
     const char* why = nullptr;
     if (P.N_Y != 0) why = "GAMCONS with mass fractions is not on the device path";
-    else if (P.D == 2 && !c->tiled_full)
-      why = "GAMCONS in 2D needs a structured row-major grid with nx a multiple of 32 and ny of 4 (p = 3: 2)";
+    else if (P.D == 2 && !c->tile_tma)
+      why = "GAMCONS in 2D needs a structured row-major grid with an even nx of at least 32 and at least one "
+            "tile's height of rows (4; p = 3: 2)";
     else if (P.limiter == DGB_LIM_M2L)  // M2limiting stops there too (limiting.cc:193-194, 410-411)
       why = "M2L is only implemented for gamncon";
     else if (P.limiter != DGB_LIM_NONE && P.limiter != DGB_LIM_HRL)
@@ -1047,10 +1034,11 @@ extern "C" int dgb_create(const dgb_problem* prob, int device, dgb_ctx** out) {
   if (P.N_Y > 3) {
     if (int rc = upload_many_y_tables(c->cs, P.D, P.p)) { delete c; return rc; }
   }
-  if (P.N_Y > 0 && P.D == 2 && !c->tiled_full) {
+  if (P.N_Y > 0 && P.D == 2 && !c->tile_tma) {
     delete c;
-    return set_error(DGB_ERR_UNSUPPORTED, "mass fractions in 2D need a structured row-major grid with nx a multiple "
-                                          "of 32 and ny of 4 (p = 3 or more than three mass fractions: 2)");
+    return set_error(DGB_ERR_UNSUPPORTED, "mass fractions in 2D need a structured row-major grid with an even nx of "
+                                          "at least 32 and at least one tile's height of rows (4; p = 3 or more "
+                                          "than three mass fractions: 2)");
   }
   if (P.N_Y > 0 && P.limiter != DGB_LIM_NONE && P.limiter != DGB_LIM_HRL && P.limiter != DGB_LIM_M2L) {
     delete c;

@@ -52,10 +52,15 @@ int limit_ny(dgb_ctx* c, const double* in, double* out) {
 #undef L1
 }
 
-// 2D: full tiles of a structured grid (checked when the context is created)
+// 2D: full tiles of a structured grid (TMA tile loads: checked when the context is created), then the
+// strips outside them (if any) with the generic kernel
 template <int MODE, int NY>
 int residual2d_ny(dgb_ctx* c, const StageArgs& a) {
-#define R2(P, F) case P * 10 + F: launch_tile2d<P, F, MODE, NY>(c, a); return 0;
+#define R2(P, F)                                                               \
+  case P * 10 + F:                                                             \
+    launch_tile2d<P, F, MODE, NY>(c, a);                                       \
+    if (c->nleft) launch_res2d<P, F, MODE, NY>(c, a, c->left, c->nleft);       \
+    return 0;
   switch (c->p * 10 + c->flux) {
     R2(1, 0) R2(1, 2) R2(2, 0) R2(2, 2) R2(3, 0) R2(3, 2)
     default: return set_error(DGB_ERR_UNSUPPORTED, "no residual kernel for this (p, flux) with mass fractions");

@@ -79,4 +79,22 @@ void launch_tile2d(dgb_ctx* c, const StageArgs& s) {
   launch_pdl(c, k, grid, dim3(TILE_W * TH), smem, a, mu, mb);
 }
 
+constexpr int RES2D_TE = 16;
+constexpr int RES2D_NT = 256;
+
+// generic 2D residual over every element, or over the listed ones (elist, n)
+template <int P, int FLUX, int MODE, int NY = 0, bool GC = false>
+void launch_res2d(dgb_ctx* c, const StageArgs& a, const int* elist = nullptr, int n = 0) {
+  constexpr size_t smem = residual2d_smem_doubles<P, RES2D_TE, NY, GC>() * sizeof(double);
+  auto k = residual2d_kernel<P, FLUX, MODE, RES2D_TE, RES2D_NT, NY, GC>;
+  static bool attr = false;
+  if (!attr) { cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem); attr = true; }
+  StageArgs s = a;
+  s.elist = elist;
+  s.nlist = n;
+  const int grid = ((elist ? n : c->ne) + RES2D_TE - 1) / RES2D_TE;
+  ProfScope ps(c, KC_RESIDUAL);
+  k<<<grid, RES2D_NT, smem, c->st>>>(c->cs, s);
+}
+
 }  // namespace dgb

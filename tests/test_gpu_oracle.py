@@ -54,11 +54,16 @@ CASES = [
     ("2d_p3_roe_m2l_tiled_box_y4", 2, 3, 32, 6, ("reflective",) * 4, "roe", "m2l", "quadrants", 0.3, 4),
     ("1d_p2_hll_m2l_y8", 1, 2, 180, 1, ("transmissive",) * 2, "hll", "m2l", "tube_noise", 0.3, 8),
     ("1d_p3_roe_hrl_walls_y6", 1, 3, 90, 1, ("reflective",) * 2, "roe", "hrl", "riemann", 0.15, 6),
+    # extents that are not tile multiples: full tiles, then the strips with the generic kernel
+    ("2d_p2_rus_m2l_strips_walls_y2", 2, 2, 100, 46, WALLS, "rusanov", "m2l", "shock_bubble", 0.3, 2),
+    ("2d_p3_roe_hrl_strips_y5", 2, 3, 70, 21, ("transmissive",) * 4, "roe", "hrl", "quadrants", 0.3, 5),
+    ("2d_p1_rus_m2l_strips_periodic_y1", 2, 1, 50, 10, ("periodic",) * 4, "rusanov", "m2l", "quadrants", 0.3, 1),
     # the GAMCONS gamma model (last entry); limiters hrl and none (the reference's M2limiting stops
     # for this model)
     ("2d_p2_rus_hrl_tiled_walls_gc", 2, 2, 64, 16, WALLS, "rusanov", "hrl", "shock_bubble", 0.3, 0, "gamcons"),
     ("2d_p1_roe_hrl_tiled_periodic_gc", 2, 1, 64, 8, ("periodic",) * 4, "roe", "hrl", "quadrants", 0.3, 0, "gamcons"),
     ("2d_p3_roe_none_tiled_box_gc", 2, 3, 32, 6, ("reflective",) * 4, "roe", "none", "quadrants", 0.1, 0, "gamcons"),
+    ("2d_p2_roe_hrl_strips_walls_gc", 2, 2, 100, 46, WALLS, "roe", "hrl", "shock_bubble", 0.3, 0, "gamcons"),
     ("1d_p2_roe_hrl_gc", 1, 2, 211, 1, ("transmissive",) * 2, "roe", "hrl", "tube_noise", 0.3, 0, "gamcons"),
     ("1d_p1_hll_hrl_periodic_gc", 1, 1, 150, 1, ("periodic",) * 2, "hll", "hrl", "riemann", 0.3, 0, "gamcons"),
     ("1d_p3_rus_none_walls_gc", 1, 3, 77, 1, ("reflective",) * 2, "rusanov", "none", "tube_noise", 0.05, 0, "gamcons"),
@@ -179,7 +184,7 @@ def test_shock_bubble_mass_fraction_100_steps_l1():
 
 def test_mass_fraction_configurations_outside_the_device_path_are_rejected():
     import dg_b200 as dgb
-    bad = [dict(dim=2, order=2, nx=40, ny=8, limiter="m2l"),       # 2D grid not tile-aligned
+    bad = [dict(dim=2, order=2, nx=41, ny=8, limiter="m2l"),       # odd nx: no TMA tiles
            dict(dim=1, order=2, nx=50, ny=1, limiter="m2i", thresholds=(0.05,)),  # sensor-gated limiter
            dict(dim=1, order=2, nx=50, ny=1, limiter="prl")]
     for kw in bad:
@@ -189,8 +194,8 @@ def test_mass_fraction_configurations_outside_the_device_path_are_rejected():
         with pytest.raises(dgb.DGBError) as e:
             dgb.DGSolver(prob)
         assert e.value.code == 4
-    # four or more mass fractions run on 32 x 2 tiles: an odd number of element rows is refused
-    prob = dgb.Problem.structured(2, 2, 32, 7, flux="rusanov", limiter="m2l", cfl=0.3, n_mass=4)
+    # four or more mass fractions run on 32 x 2 tiles: a grid of one element row has none
+    prob = dgb.Problem.structured(2, 2, 32, 1, flux="rusanov", limiter="m2l", cfl=0.3, n_mass=4)
     with pytest.raises(dgb.DGBError) as e:
         dgb.DGSolver(prob)
     assert e.value.code == 4
@@ -254,11 +259,11 @@ def test_gamcons_rusanov_2d_breaks_down_like_the_reference():
 
 def test_gamcons_configurations_outside_the_device_path_are_rejected():
     """M2L stops with GAMCONS (as in the reference), and the device path has no GAMCONS variant of
-    the sensors, of mass fractions, of the mixed form or of untiled 2D grids."""
+    the sensors, of mass fractions, of the mixed form or of 2D grids without TMA tiles."""
     import dg_b200 as dgb
     bad = [dict(dim=2, order=2, nx=32, ny=8, limiter="m2l"),
            dict(dim=1, order=2, nx=50, ny=1, limiter="m2l"),
-           dict(dim=2, order=2, nx=40, ny=8, limiter="hrl"),               # 2D grid not tile-aligned
+           dict(dim=2, order=2, nx=41, ny=8, limiter="hrl"),               # odd nx: no TMA tiles
            dict(dim=1, order=2, nx=50, ny=1, limiter="hri", thresholds=(0.05,)),
            dict(dim=1, order=2, nx=50, ny=1, limiter="prl"),
            dict(dim=1, order=2, nx=50, ny=1, limiter="hrl", n_mass=1)]
