@@ -632,35 +632,29 @@ int limit_dispatch(dgb_ctx* c, double* U, bool rescore = true) {
   return set_error(DGB_ERR_UNSUPPORTED, "limiter not available on the device path");
 }
 
+template <int DIM, int NS, bool GC>
+void launch_ws(dgb_ctx* c, const double* U, int n, double* copy_to, double finish) {
+  // one thread per (element, group of ws_nodes<NS>() nodes): grid.y runs over the node groups
+  const dim3 grid(std::max(1, std::min(65535, (n + 255) / 256)), NS / ws_nodes<NS>());
+  launch_pdl(c, wavespeed_kernel<DIM, NS, GC>, grid, dim3(256), 0, U, n, c->ld, c->scal, copy_to, c->nf, finish);
+}
+
 // the wave-speed reduction into scal->umax over the elements the context owns (all of them, or
 // in slab mode the rows between the ghost rows)
 // finish > 0: the reduction's last CTA also forms the step dt with that CFL scale
 void launch_wavespeed(dgb_ctx* c, const double* Uall, double* copy_to = nullptr, double finish = 0.0) {
   const int e0 = c->halo_lo * c->nx, n = c->ne - (c->halo_lo + c->halo_hi) * c->nx;
   const double* U = Uall + e0;  // element offset inside every (field, node) plane of stride ld
-  const int grid = std::max(1, std::min(4 * 148, (n + 255) / 256));
-  {
-    if (c->gamcons) {
-      switch (c->D * 100 + c->ns) {
-        case 102: launch_pdl(c, wavespeed_kernel<1, 2, true>, dim3(grid), dim3(256), 0, U, n, c->ld, c->scal, copy_to, c->nf, finish); break;
-        case 103: launch_pdl(c, wavespeed_kernel<1, 3, true>, dim3(grid), dim3(256), 0, U, n, c->ld, c->scal, copy_to, c->nf, finish); break;
-        case 104: launch_pdl(c, wavespeed_kernel<1, 4, true>, dim3(grid), dim3(256), 0, U, n, c->ld, c->scal, copy_to, c->nf, finish); break;
-        case 204: launch_pdl(c, wavespeed_kernel<2, 4, true>, dim3(grid), dim3(256), 0, U, n, c->ld, c->scal, copy_to, c->nf, finish); break;
-        case 209: launch_pdl(c, wavespeed_kernel<2, 9, true>, dim3(grid), dim3(256), 0, U, n, c->ld, c->scal, copy_to, c->nf, finish); break;
-        case 216: launch_pdl(c, wavespeed_kernel<2, 16, true>, dim3(grid), dim3(256), 0, U, n, c->ld, c->scal, copy_to, c->nf, finish); break;
-        default: break;
-      }
-    } else
-    switch (c->D * 100 + c->ns) {
-      case 102: launch_pdl(c, wavespeed_kernel<1, 2>, dim3(grid), dim3(256), 0, U, n, c->ld, c->scal, copy_to, c->nf, finish); break;
-      case 103: launch_pdl(c, wavespeed_kernel<1, 3>, dim3(grid), dim3(256), 0, U, n, c->ld, c->scal, copy_to, c->nf, finish); break;
-      case 104: launch_pdl(c, wavespeed_kernel<1, 4>, dim3(grid), dim3(256), 0, U, n, c->ld, c->scal, copy_to, c->nf, finish); break;
-      case 204: launch_pdl(c, wavespeed_kernel<2, 4>, dim3(grid), dim3(256), 0, U, n, c->ld, c->scal, copy_to, c->nf, finish); break;
-      case 209: launch_pdl(c, wavespeed_kernel<2, 9>, dim3(grid), dim3(256), 0, U, n, c->ld, c->scal, copy_to, c->nf, finish); break;
-      case 216: launch_pdl(c, wavespeed_kernel<2, 16>, dim3(grid), dim3(256), 0, U, n, c->ld, c->scal, copy_to, c->nf, finish); break;
-      default: break;
-    }
+#define WS(D, NS)                                                                              \
+  case D * 100 + NS:                                                                           \
+    if (c->gamcons) launch_ws<D, NS, true>(c, U, n, copy_to, finish);                          \
+    else launch_ws<D, NS, false>(c, U, n, copy_to, finish);                                    \
+    break;
+  switch (c->D * 100 + c->ns) {
+    WS(1, 2) WS(1, 3) WS(1, 4) WS(2, 4) WS(2, 9) WS(2, 16)
+    default: break;
   }
+#undef WS
 }
 
 void launch_dt(dgb_ctx* c, const double* U, bool cfl, double* copy_to = nullptr) {
