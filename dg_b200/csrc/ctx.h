@@ -5,6 +5,8 @@
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
 
+#include <mutex>
+#include <set>
 #include <string>
 #include <utility>
 #include <vector>
@@ -15,6 +17,25 @@
 #include "device/sensor.h"
 
 namespace dgb {
+// Dynamic shared memory above 48 KB is opted into per kernel, and cudaFuncSetAttribute acts on the
+// current device only: done once per (kernel, device), under a lock
+inline cudaError_t allow_dynamic_smem(const void* kernel, size_t bytes) {
+  static std::mutex mu;
+  static std::set<std::pair<const void*, int>> done;
+  int dev = 0;
+  cudaError_t err = cudaGetDevice(&dev);
+  if (err != cudaSuccess) return err;
+  std::lock_guard<std::mutex> lock(mu);
+  if (done.count({kernel, dev})) return cudaSuccess;
+  err = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+  if (err == cudaSuccess) done.insert({kernel, dev});
+  return err;
+}
+template <typename K>
+inline cudaError_t allow_dynamic_smem(K* kernel, size_t bytes) {
+  return allow_dynamic_smem(reinterpret_cast<const void*>(kernel), bytes);
+}
+
 enum { KC_RESIDUAL = 0, KC_LIMITER = 1, KC_DT = 2, KC_INDICATOR = 3, KC_OTHER = 4, KC_N = 5 };
 }
 

@@ -835,47 +835,46 @@ __device__ __forceinline__ void finish_dt(DevScalars* scal, double cfl_scaled) {
   v->time = v->time + dt;
 }
 
-// Nodes one thread of the wave-speed reduction covers: the loads of their fields are issued
-// together, and the grid's y dimension runs over the NS / G groups of nodes, so a launch has
-// enough independent loads in flight to stream the state
-template <int NS>
-constexpr int ws_nodes() { return NS % 3 == 0 ? 3 : NS % 4 == 0 ? 4 : NS; }
-
 // copy_to (1D RK4, or null): the nf fields of every element read are also written there (the
 // step's accumulator starts as the state).  finish > 0: the last CTA to add its maximum forms the
 // step from it (that CFL scale), so no separate finish launch is needed; 0 leaves umax for a caller
-// that reduces it further (slab mode).  Grid: (element blocks of 256, NS / ws_nodes<NS>()).
+// that reduces it further (slab mode).
+// Grid: (element blocks, NS): a CTA reads one node of its elements -- five loads per element, few
+// registers, full occupancy -- and strides over the elements two at a time, so that both
+// elements' loads are in flight together.
 template <int DIM, int NS, bool GC = false>
 __global__ void __launch_bounds__(256) wavespeed_kernel(const double* __restrict__ U, int n_elem, int ld,
                                                         DevScalars* __restrict__ scal,
                                                         double* __restrict__ copy_to, int nf, double finish) {
-  constexpr int G = ws_nodes<NS>(), NV = DIM == 1 ? 4 : 5;  // nodes per thread, fields read
-  static_assert(NS % G == 0, "node groups must tile the element");
+  constexpr int NV = DIM == 1 ? 4 : 5;  // fields the wave speed reads
   pdl_wait();
   if (scal->flags) return;
   double m = 0.0;
   bool bad = false;
-  const int t0 = blockIdx.y * G;
-  for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < n_elem; e += gridDim.x * blockDim.x) {
-    double v[G][NV];
+  const int t = blockIdx.y, stride = gridDim.x * blockDim.x;
+  for (int e0 = blockIdx.x * blockDim.x + threadIdx.x; e0 < n_elem; e0 += 2 * stride) {
+    double v[2][NV];
 #pragma unroll
-    for (int g = 0; g < G; ++g)
+    for (int r = 0; r < 2; ++r) {
+      const int e = e0 + r * stride;
+      if (e < n_elem)
 #pragma unroll
-      for (int f = 0; f < NV; ++f) v[g][f] = __ldg(U + (size_t)(f * NS + t0 + g) * ld + e);
+        for (int f = 0; f < NV; ++f) v[r][f] = __ldg(U + (size_t)(f * NS + t) * ld + e);
+    }
 #pragma unroll
-    for (int g = 0; g < G; ++g) {
+    for (int r = 0; r < 2; ++r) {
+      const int e = e0 + r * stride;
+      if (e >= n_elem) continue;
       double w;
       if constexpr (DIM == 1)
-        w = phys::wave_speed1d<GC>(v[g][0], v[g][1], v[g][2], v[g][3]);
+        w = phys::wave_speed1d<GC>(v[r][0], v[r][1], v[r][2], v[r][3]);
       else
-        w = phys::wave_speed2d<GC>(v[g][0], v[g][1], v[g][2], v[g][3], v[g][4]);
+        w = phys::wave_speed2d<GC>(v[r][0], v[r][1], v[r][2], v[r][3], v[r][4]);
       if (!(w == w)) bad = true;
       else m = fmax(m, fabs(w));
+      if (copy_to)
+        for (int f = 0; f < nf; ++f) copy_to[(size_t)(f * NS + t) * ld + e] = __ldg(U + (size_t)(f * NS + t) * ld + e);
     }
-    if (copy_to)
-      for (int g = 0; g < G; ++g)
-        for (int f = 0; f < nf; ++f)
-          copy_to[(size_t)(f * NS + t0 + g) * ld + e] = __ldg(U + (size_t)(f * NS + t0 + g) * ld + e);
   }
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));

@@ -167,11 +167,7 @@ template <int P, int FLUX, int TW, int TH, int UNROLL>
 int launch_tile2d_batch(dgb_batch* b, const Class& k, int stage, cudaStream_t st) {
   auto kern = batch_tile2d_kernel<P, FLUX, TW, TH, UNROLL>;
   constexpr size_t smem = batch_tile2d_smem_bytes<P, TW, TH>();
-  static bool attr = false;
-  if (!attr) {
-    DGB_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    attr = true;
-  }
+  DGB_CUDA(allow_dynamic_smem(kern, smem));
   const int grid = persistent_grid(b, kern, TW * TH, smem, k.n_res, k.ctas_per_sm);
   kern<<<grid, TW * TH, smem, st>>>(b->d_cases, b->d_maps, k.d_res, k.n_res, stage);
   return 0;

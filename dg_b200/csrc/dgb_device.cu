@@ -179,8 +179,7 @@ void launch_tile2d_mixed(dgb_ctx* c, const StageArgs& s) {
   if (c->mixed_ct) {
     constexpr size_t smem = TileDimsMixedCT<P, TILE_W, TH>::smem_bytes;
     auto k = residual2d_tile_mixed_ct_kernel<P, FLUX, MODE, TILE_W, TH>;
-    static bool attr = false;
-    if (!attr) { cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem); attr = true; }
+    allow_dynamic_smem(k, smem);
     const TileArgs a = tile_args(c, s);
     dim3 grid(c->nx / TILE_W, c->ny / TH);
     ProfScope ps(c, KC_RESIDUAL);
@@ -189,8 +188,7 @@ void launch_tile2d_mixed(dgb_ctx* c, const StageArgs& s) {
   }
   constexpr size_t smem = TileDimsMixed<P, TILE_W, TH>::smem_bytes;
   auto k = residual2d_tile_mixed_kernel<P, FLUX, MODE, TILE_W, TH>;
-  static bool attr = false;
-  if (!attr) { cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem); attr = true; }
+  allow_dynamic_smem(k, smem);
   const TileArgs a = tile_args(c, s);
   const CUtensorMap& mb = MODE == MODE_SSP ? map_of(c, s.Ubase)
                           : MODE == MODE_RK4 && s.Uacc ? map_of(c, s.Uacc) : map_of(c, s.U);
@@ -204,8 +202,7 @@ template <int FLUX, int MODE>
 void launch_tile2d_dmma(dgb_ctx* c, const StageArgs& s) {
   constexpr size_t smem = DmmaDims::smem_bytes;
   auto k = residual2d_tile_dmma_kernel<FLUX, MODE>;
-  static bool attr = false;
-  if (!attr) { cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem); attr = true; }
+  allow_dynamic_smem(k, smem);
   const TileArgs a = tile_args(c, s);
   dim3 grid(c->nx / DMMA_TW, c->ny / DMMA_TH);
   ProfScope ps(c, KC_RESIDUAL);
@@ -365,8 +362,7 @@ void launch_lim2d_fused(dgb_ctx* c, const double* in, double* out) {
   const LimArgs la{c->ld, c->ne};
   constexpr size_t smem = lim2d_fused_smem_bytes<P, METHOD>();
   auto k = lim2d_fused_tile_kernel<P, METHOD, LIM_STRIP_H>;
-  static bool attr = false;
-  if (!attr) { cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem); attr = true; }
+  allow_dynamic_smem(k, smem);
   dim3 grid((c->nx + 29) / 30, (c->ny + LIM_STRIP_H - 1) / LIM_STRIP_H), block(32, P + 1);
   k<<<grid, block, smem, c->st>>>(la, c->nx, c->ny, in, c->nbr, out, c->scal);
 }
@@ -492,21 +488,13 @@ void launch_indicator(dgb_ctx* c, const double* U) {
   a.errflag = &c->scal->flags;
   if (c->ind_tc) {
     // tcgen05 GEMMs on 128-element tiles, persistent: one CTA per SM
-    static bool attr_tc = false;
-    if (!attr_tc) {
-      cudaFuncSetAttribute(indicator_infer_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)TCI_SMEM_BYTES);
-      attr_tc = true;
-    }
+    allow_dynamic_smem(indicator_infer_tc_kernel, TCI_SMEM_BYTES);
     const int ntiles = (c->ne + TCI_M - 1) / TCI_M;
     indicator_infer_tc_kernel<<<std::min(ntiles, c->sm_count), TCI_THREADS, TCI_SMEM_BYTES, c->st>>>(a);
   } else {
     const int ntiles = (c->ne + 15) / 16;
     const int grid = std::min((ntiles + IND_WARPS - 1) / IND_WARPS, c->sm_count * 2);  // persistent: 2 CTAs per SM
-    static bool attr = false;
-    if (!attr) {
-      cudaFuncSetAttribute(indicator_infer_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)IND_SMEM_BYTES);
-      attr = true;
-    }
+    allow_dynamic_smem(indicator_infer_kernel, IND_SMEM_BYTES);
     indicator_infer_kernel<<<grid, 32 * IND_WARPS, IND_SMEM_BYTES, c->st>>>(a);
   }
   cudaMemsetAsync(c->ind_blist + c->ld, 0, sizeof(int), c->st);
@@ -634,8 +622,9 @@ int limit_dispatch(dgb_ctx* c, double* U, bool rescore = true) {
 
 template <int DIM, int NS, bool GC>
 void launch_ws(dgb_ctx* c, const double* U, int n, double* copy_to, double finish) {
-  // one thread per (element, group of ws_nodes<NS>() nodes): grid.y runs over the node groups
-  const dim3 grid(std::max(1, std::min(65535, (n + 255) / 256)), NS / ws_nodes<NS>());
+  // grid.y over the nodes; about eight 256-thread CTAs per SM in all, each striding over elements
+  const int gx = std::max(1, std::min((n + 255) / 256, c->sm_count * 8 / NS));
+  const dim3 grid(gx, NS);
   launch_pdl(c, wavespeed_kernel<DIM, NS, GC>, grid, dim3(256), 0, U, n, c->ld, c->scal, copy_to, c->nf, finish);
 }
 
@@ -1276,8 +1265,7 @@ extern "C" int dgb_mlp_forward(const float* params, const float* X, int n, float
   if (n == 0) return DGB_OK;
   cudaStream_t st = static_cast<cudaStream_t>(stream);
   const size_t smem = MLP_NPARAM * sizeof(float);
-  static bool attr = false;
-  if (!attr) { cudaFuncSetAttribute(mlp_forward_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem); attr = true; }
+  allow_dynamic_smem(mlp_forward_kernel, smem);
   mlp_forward_kernel<<<(n + 127) / 128, 128, smem, st>>>(params, X, n, cache, prob);
   DGB_CUDA(cudaGetLastError());
   return DGB_OK;

@@ -75,12 +75,8 @@ void launch_lim2d_ny(dgb_ctx* c, double* U) {
   auto kx = lim2d_xpass_tile_kernel<P, METHOD, NY>;
   auto ky = lim2d_ypass_tile_kernel<P, METHOD, NY>;
   constexpr size_t sx = lim2d_xpass_smem_bytes<P, NY>(), sy = lim2d_ypass_smem_bytes<P, NY>();
-  static bool attr = false;
-  if (!attr) {
-    if (sx) cudaFuncSetAttribute(kx, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sx);
-    if (sy) cudaFuncSetAttribute(ky, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sy);
-    attr = true;
-  }
+  if (sx) allow_dynamic_smem(kx, sx);
+  if (sy) allow_dynamic_smem(ky, sy);
   const dim3 gx((c->nx + 29) / 30, c->ny), bx(32, P + 1);
   launch_pdl(c, kx, gx, bx, sx, la, c->nx, (const double*)U, (const int*)c->nbr, c->X, (const DevScalars*)c->scal);
   const dim3 gy((c->nx + 31) / 32, (c->ny + 3) / 4, P + 1), by(32, 6);

@@ -67,8 +67,7 @@ void launch_tile2d(dgb_ctx* c, const StageArgs& s) {
   using Dm = TileDims<P, TILE_W, TH, NY>;
   constexpr size_t smem = Dm::smem_bytes;
   auto k = residual2d_tile_kernel<P, FLUX, MODE, TILE_W, TH, NY, GC, TMA>;
-  static bool attr = false;
-  if (!attr) { cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem); attr = true; }
+  allow_dynamic_smem(k, smem);
   const TileArgs a = tile_args(c, s);
   // (without TMA the maps are not read: the tile loads are plain)
   const CUtensorMap& mu = TMA ? map_of(c, s.U) : c->mapA;
@@ -87,8 +86,7 @@ template <int P, int FLUX, int MODE, int NY = 0, bool GC = false>
 void launch_res2d(dgb_ctx* c, const StageArgs& a, const int* elist = nullptr, int n = 0) {
   constexpr size_t smem = residual2d_smem_doubles<P, RES2D_TE, NY, GC>() * sizeof(double);
   auto k = residual2d_kernel<P, FLUX, MODE, RES2D_TE, RES2D_NT, NY, GC>;
-  static bool attr = false;
-  if (!attr) { cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem); attr = true; }
+  allow_dynamic_smem(k, smem);
   StageArgs s = a;
   s.elist = elist;
   s.nlist = n;
