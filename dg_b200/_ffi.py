@@ -32,7 +32,7 @@ EXPORTS = [
     "dgb_batch_autotune", "dgb_batch_set_tuning", "dgb_batch_advance", "dgb_problem_error_norms", "dgb_batch_case_stats",
     "dgb_batch_last_timing", "dgb_slab_ghost_rows", "dgb_step_begin", "dgb_step_wavespeed_word", "dgb_step_stage",
     "dgb_step_end", "dgb_halo_count", "dgb_halo_pack", "dgb_halo_unpack", "dgb_stream", "dgb_set_cfl_scale",
-    "dgb_set_wait_limit", "dgb_set_indicator_interval", "dgb_slabs_advance_local",
+    "dgb_set_wait_limit", "dgb_set_indicator_interval", "dgb_slabs_advance_local", "dgb_advance_host",
 ]
 
 
@@ -111,6 +111,7 @@ def lib() -> C.CDLL:
         "dgb_indicator_scores": [vp, dp, C.POINTER(C.c_float), C.POINTER(C.c_int)],
         "dgb_dt_from_cfl": [vp, dp, dp],
         "dgb_advance": [vp, ip, ip, C.c_double, dp],
+        "dgb_advance_host": [vp, dp, ip, ip, C.c_double, dp],
         "dgb_last_dt": [vp, dp],
         "dgb_conservation": [vp, dp],
         "dgb_last_timing": [vp, dp, C.POINTER(C.c_longlong)],

@@ -36,6 +36,9 @@ inline cudaError_t allow_dynamic_smem(K* kernel, size_t bytes) {
   return allow_dynamic_smem(reinterpret_cast<const void*>(kernel), bytes);
 }
 
+// element chunks of the host-resident time loop's copies (dgb_advance_host)
+constexpr int kHostChunks = 16;
+
 enum { KC_RESIDUAL = 0, KC_LIMITER = 1, KC_DT = 2, KC_INDICATOR = 3, KC_OTHER = 4, KC_N = 5 };
 }
 
@@ -107,6 +110,9 @@ struct dgb_ctx {
   // destroys the captured steps (their kernel arguments or launch sequence changed)
   unsigned graph_gen = 0;   // counts drop_graphs calls (captured slab steps compare it)
   double* halo_send[2] = {nullptr, nullptr};  // slab mode, local exchange: packed owned rows per side
+  // dgb_advance_host: upload / download streams, per-chunk events, the step's end
+  cudaStream_t hl_st[2] = {nullptr, nullptr};
+  cudaEvent_t hl_up[dgb::kHostChunks] = {}, hl_down[dgb::kHostChunks] = {}, hl_done = nullptr;
   void drop_graphs() {
     ++graph_gen;
     for (auto& a : graphs)

@@ -1142,6 +1142,10 @@ extern "C" void dgb_destroy(dgb_ctx* c) {
   if (c->scal) cudaFree(c->scal);
   if (c->h_scal) cudaFreeHost(c->h_scal);
   for (auto ev : c->ev_pool) cudaEventDestroy(ev);
+  for (auto ev : c->hl_up) if (ev) cudaEventDestroy(ev);
+  for (auto ev : c->hl_down) if (ev) cudaEventDestroy(ev);
+  if (c->hl_done) cudaEventDestroy(c->hl_done);
+  for (auto st : c->hl_st) if (st) cudaStreamDestroy(st);
   if (c->e0) cudaEventDestroy(c->e0);
   if (c->e1) cudaEventDestroy(c->e1);
   if (c->st) cudaStreamDestroy(c->st);
@@ -1450,6 +1454,42 @@ extern "C" int dgb_dt_from_cfl(dgb_ctx* c, const double* U, double* dt) {
   return DGB_OK;
 }
 
+namespace {
+// captures the steps dgb_advance replays for (scheme, CFL or fixed step): the step that scores the
+// learned indicator and, when scoring is every few steps, the one that does not
+int ensure_step_graphs(dgb_ctx* c, int scheme, bool cfl) {
+  const int si = scheme == DGB_RK4 ? 1 : 0, mi = cfl ? 1 : 0;
+  for (int k = 0; k < 2; ++k) {
+    const bool sc = k == 0;
+    if (c->graphs[si][mi][k] || (!sc && (!c->ind_on || c->ind_every <= 1))) continue;
+    cudaGraph_t g;
+    DGB_CUDA(cudaStreamBeginCapture(c->st, cudaStreamCaptureModeThreadLocal));
+    c->counter = 0;
+    int rc = scheme == DGB_RK4 ? step_rk4(c, cfl, sc) : step_ssprk3(c, cfl, sc);
+    cudaError_t ec = cudaStreamEndCapture(c->st, &g);
+    if (rc) { if (ec == cudaSuccess) cudaGraphDestroy(g); return rc; }
+    DGB_CUDA(ec);
+    DGB_CUDA(cudaGraphInstantiate(&c->graphs[si][mi][k], g, 0));
+    cudaGraphDestroy(g);
+    c->graph_launches[si][mi][k] = c->counter;
+  }
+  return DGB_OK;
+}
+
+// the step's status from the device scalars (read after the step's last kernel)
+int step_status(dgb_ctx* c, double* time) {
+  if (int rc = read_scalars(c)) return rc;
+  float ms = 0;
+  cudaEventElapsedTime(&ms, c->e0, c->e1);
+  c->last_ms = ms;
+  if (time) *time += c->h_scal->time;
+  if (c->h_scal->flags & FLAG_TIMEOUT) return set_error(DGB_ERR_TIMEOUT, "a bounded device wait expired");
+  if (c->h_scal->flags & FLAG_NONFINITE) return set_error(DGB_ERR_NONFINITE, "time step is NaN");
+  if (c->h_scal->flags & FLAG_DT_SMALL) return set_error(DGB_ERR_DT_SMALL, "next time step is too small (< 1e-14)");
+  return DGB_OK;
+}
+}  // namespace
+
 extern "C" int dgb_advance(dgb_ctx* c, int scheme, int nsteps, double dt, double* time) {
   if (!c) return set_error(DGB_ERR_ARG, "null context");
   if (scheme != DGB_SSPRK3 && scheme != DGB_RK4) return set_error(DGB_ERR_ARG, "scheme must be 3 or 4");
@@ -1476,20 +1516,8 @@ extern "C" int dgb_advance(dgb_ctx* c, int scheme, int nsteps, double dt, double
     c->last_launches = c->counter;
     if (int rc = prof_collect(c)) return rc;
   } else {
-    for (int k = 0; k < 2 && nsteps > 0; ++k) {  // the scoring and the non-scoring step, as needed
-      const bool sc = k == 0;
-      if (c->graphs[si][mi][k] || (!sc && (!c->ind_on || c->ind_every <= 1))) continue;
-      cudaGraph_t g;
-      DGB_CUDA(cudaStreamBeginCapture(c->st, cudaStreamCaptureModeThreadLocal));
-      c->counter = 0;
-      int rc = scheme == DGB_RK4 ? step_rk4(c, cfl, sc) : step_ssprk3(c, cfl, sc);
-      cudaError_t ec = cudaStreamEndCapture(c->st, &g);
-      if (rc) { if (ec == cudaSuccess) cudaGraphDestroy(g); return rc; }
-      DGB_CUDA(ec);
-      DGB_CUDA(cudaGraphInstantiate(&c->graphs[si][mi][k], g, 0));
-      cudaGraphDestroy(g);
-      c->graph_launches[si][mi][k] = c->counter;
-    }
+    if (nsteps > 0)
+      if (int rc = ensure_step_graphs(c, scheme, cfl)) return rc;
     DGB_CUDA(cudaEventRecord(c->e0, c->st));
     long long launches = 0;
     for (int s = 0; s < nsteps; ++s) {
@@ -1501,15 +1529,70 @@ extern "C" int dgb_advance(dgb_ctx* c, int scheme, int nsteps, double dt, double
     DGB_CUDA(cudaEventRecord(c->e1, c->st));
     c->last_launches = launches;
   }
-  if (int rc = read_scalars(c)) return rc;
-  float ms = 0;
-  cudaEventElapsedTime(&ms, c->e0, c->e1);
-  c->last_ms = ms;
-  if (time) *time += c->h_scal->time;
-  if (c->h_scal->flags & FLAG_TIMEOUT) return set_error(DGB_ERR_TIMEOUT, "a bounded device wait expired");
-  if (c->h_scal->flags & FLAG_NONFINITE) return set_error(DGB_ERR_NONFINITE, "time step is NaN");
-  if (c->h_scal->flags & FLAG_DT_SMALL) return set_error(DGB_ERR_DT_SMALL, "next time step is too small (< 1e-14)");
-  return DGB_OK;
+  return step_status(c, time);
+}
+
+// The time loop with the state of record in host memory.  Every step uploads the state from U
+// (reference layout), advances it one step with the captured step and downloads the result into
+// U.  The copies go in element chunks on two copy streams: the upload of chunk j for step k+1
+// waits only for the download of chunk j from step k, so the two directions of the host link
+// overlap; the conversion of each uploaded chunk to the internal layout runs as it lands.
+extern "C" int dgb_advance_host(dgb_ctx* c, double* U, int scheme, int nsteps, double dt, double* time) {
+  if (!c || !U) return set_error(DGB_ERR_ARG, "null argument");
+  if (scheme != DGB_SSPRK3 && scheme != DGB_RK4) return set_error(DGB_ERR_ARG, "scheme must be 3 or 4");
+  if (nsteps < 0) return set_error(DGB_ERR_ARG, "nsteps < 0");
+  if (!(dt > 0) && !(c->cs.cfl_scaled > 0)) return set_error(DGB_ERR_ARG, "no fixed dt and no positive CFL");
+  if (c->prof) return set_error(DGB_ERR_UNSUPPORTED, "profiling times eager launches: use dgb_advance");
+  DGB_CUDA(cudaSetDevice(c->device));
+  const bool cfl = !(dt > 0);
+  const int si = scheme == DGB_RK4 ? 1 : 0, mi = cfl ? 1 : 0;
+  if (!c->hl_st[0]) {
+    for (auto& st : c->hl_st) DGB_CUDA(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+    for (auto& e : c->hl_up) DGB_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    for (auto& e : c->hl_down) DGB_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    DGB_CUDA(cudaEventCreateWithFlags(&c->hl_done, cudaEventDisableTiming));
+  }
+  if (nsteps > 0)
+    if (int rc = ensure_step_graphs(c, scheme, cfl)) return rc;
+  if (int rc = reset_scalars(c, cfl ? 0.0 : dt)) return rc;
+  c->ind_step = 0;  // the state comes from the host: the learned indicator scores the first step
+  const size_t per = (size_t)c->nf * c->ns;  // values per element in the reference layout
+  const int nch = std::min(kHostChunks, c->ne);
+  auto first = [&](int j) { return (int)((long long)c->ne * j / nch); };
+  cudaStream_t up = c->hl_st[0], down = c->hl_st[1];
+  DGB_CUDA(cudaEventRecord(c->e0, c->st));
+  DGB_CUDA(cudaStreamWaitEvent(up, c->e0, 0));  // the copies follow the work queued before the call
+  DGB_CUDA(cudaStreamWaitEvent(down, c->e0, 0));
+  long long launches = 0;
+  for (int s = 0; s < nsteps; ++s) {
+    for (int j = 0; j < nch; ++j) {
+      const int e0 = first(j), n = first(j + 1) - e0;
+      if (s > 0) DGB_CUDA(cudaStreamWaitEvent(up, c->hl_down[j], 0));  // the last step's result is in U
+      DGB_CUDA(cudaMemcpyAsync(c->ref + e0 * per, U + e0 * per, n * per * sizeof(double), cudaMemcpyHostToDevice, up));
+      DGB_CUDA(cudaEventRecord(c->hl_up[j], up));
+      DGB_CUDA(cudaStreamWaitEvent(c->st, c->hl_up[j], 0));
+      const int grid = (int)std::min<size_t>((n * per + 255) / 256, 148 * 32);
+      ref_to_internal_kernel<<<grid, 256, 0, c->st>>>(c->ref + e0 * per, c->A + e0, c->perm, n, c->nf, c->ns, c->ld);
+      DGB_CUDA(cudaGetLastError());
+    }
+    const int k = !c->ind_on || c->ind_every <= 1 || c->ind_step % c->ind_every == 0 ? 0 : 1;
+    DGB_CUDA(cudaGraphLaunch(c->graphs[si][mi][k], c->st));
+    launches += c->graph_launches[si][mi][k] + nch + 1;
+    ++c->ind_step;
+    if (int rc = to_ref(c, c->A, c->ref)) return rc;
+    DGB_CUDA(cudaEventRecord(c->hl_done, c->st));
+    DGB_CUDA(cudaStreamWaitEvent(down, c->hl_done, 0));
+    for (int j = 0; j < nch; ++j) {
+      const int e0 = first(j), n = first(j + 1) - e0;
+      DGB_CUDA(cudaMemcpyAsync(U + e0 * per, c->ref + e0 * per, n * per * sizeof(double), cudaMemcpyDeviceToHost, down));
+      DGB_CUDA(cudaEventRecord(c->hl_down[j], down));
+    }
+  }
+  DGB_CUDA(cudaEventRecord(c->hl_done, down));  // the context's stream waits for the last download
+  DGB_CUDA(cudaStreamWaitEvent(c->st, c->hl_done, 0));
+  DGB_CUDA(cudaEventRecord(c->e1, c->st));
+  c->last_launches = launches;
+  return step_status(c, time);
 }
 
 // ------------------------------------------------------------------------------------------

@@ -203,6 +203,16 @@ class DGSolver:
         F.check(F.lib().dgb_advance(self._h, int(scheme), int(nsteps), float(dt), C.byref(t)))
         return t.value
 
+    def advance_host(self, U: np.ndarray, nsteps: int, dt: float = 0.0, scheme: int = F.SSPRK3) -> float:
+        """Advances nsteps steps with the state of record in the host array U (reference layout,
+        contiguous float64, updated in place): every step uploads U, advances one step and
+        downloads the result into U (dgb_advance_host).  Returns the time advanced."""
+        if U.dtype != np.float64 or U.size != self.n or not U.flags.c_contiguous or not U.flags.writeable:
+            raise ValueError(f"U must be a writable contiguous float64 array of {self.n} values")
+        t = C.c_double(0.0)
+        F.check(F.lib().dgb_advance_host(self._h, F.dptr(U), int(scheme), int(nsteps), float(dt), C.byref(t)))
+        return t.value
+
     def last_timing(self) -> tuple[float, int]:
         ms = C.c_double()
         n = C.c_longlong()

@@ -216,6 +216,15 @@ int dgb_dt_from_cfl(dgb_ctx* c, const double* U_host, double* dt);
  * *time is advanced by the steps taken.  Status DGB_ERR_NONFINITE / DGB_ERR_DT_SMALL when the
  * CFL step is NaN / < 1e-14 (checked after the run; the state then holds the failing step). */
 int dgb_advance(dgb_ctx* c, int scheme, int nsteps, double dt, double* time);
+/* The same time loop with the state of record in host memory (reference layout): every step
+ * uploads the state from U_host, advances it one step and downloads the result into U_host, so
+ * that U_host holds each step's result as it completes.  The copies go in element chunks on two
+ * copy streams, a chunk's upload for the next step waiting only for its own download, so the host
+ * link's two directions overlap.  U_host should be pinned (cudaHostAlloc / cudaHostRegister) for
+ * the copies to run asynchronously.  The learned indicator scores the first step of the call.
+ * Status and *time as dgb_advance; returns after the last download.  No counterpart in the
+ * reference, whose state lives in host memory between its per-stage device launches. */
+int dgb_advance_host(dgb_ctx* c, double* U_host, int scheme, int nsteps, double dt, double* time);
 
 /* Last step size used by dgb_advance (host copy). */
 int dgb_last_dt(dgb_ctx* c, double* dt);
