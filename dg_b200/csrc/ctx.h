@@ -36,8 +36,8 @@ inline cudaError_t allow_dynamic_smem(K* kernel, size_t bytes) {
   return allow_dynamic_smem(reinterpret_cast<const void*>(kernel), bytes);
 }
 
-// element chunks of the host-resident time loop's copies (dgb_advance_host)
-constexpr int kHostChunks = 16;
+// element chunks of the host-resident time loop's copies (dgb_advance_host): at most, by default
+constexpr int kHostChunks = 16, kHostChunksDefault = 8;
 
 enum { KC_RESIDUAL = 0, KC_LIMITER = 1, KC_DT = 2, KC_INDICATOR = 3, KC_OTHER = 4, KC_N = 5 };
 }
@@ -111,6 +111,7 @@ struct dgb_ctx {
   unsigned graph_gen = 0;   // counts drop_graphs calls (captured slab steps compare it)
   double* halo_send[2] = {nullptr, nullptr};  // slab mode, local exchange: packed owned rows per side
   // dgb_advance_host: upload / download streams, per-chunk events, the step's end
+  int host_chunks = dgb::kHostChunksDefault;
   cudaStream_t hl_st[2] = {nullptr, nullptr};
   cudaEvent_t hl_up[dgb::kHostChunks] = {}, hl_down[dgb::kHostChunks] = {}, hl_done = nullptr;
   void drop_graphs() {

@@ -963,14 +963,17 @@ extern "C" int dgb_create(const dgb_problem* prob, int device, dgb_ctx** out) {
     // FP64 tensor rate equals its FP64 vector rate)
     const char* tk = std::getenv("DGB_TILE_KERNEL");
     c->tile_dmma = tk && std::string(tk) == "dmma";
-    // mixed-form tiles: the compressed shared tile (FP64 anchors + FP32 deviations, plain loads)
-    // at p = 3, the TMA-loaded FP64 tile at p = 1, 2 (the faster of the two at each order);
-    // DGB_MIXED_TILE=ct / tma selects one for every order
     // programmatic dependent launches of the 2D step's kernels unless DGB_PDL=0
     const char* pk = std::getenv("DGB_PDL");
     c->pdl = !(pk && std::string(pk) == "0");
+    // mixed-form tiles: the compressed shared tile (FP64 anchors + FP32 deviations, plain loads)
+    // at p = 3, the TMA-loaded FP64 tile at p = 1, 2 (the faster of the two at each order);
+    // DGB_MIXED_TILE=ct / tma selects one for every order
     const char* mk = std::getenv("DGB_MIXED_TILE");
     c->mixed_ct = mk ? std::string(mk) == "ct" : P.p == 3;
+    // element chunks of dgb_advance_host's copies (DGB_HOST_CHUNKS, 1 .. kHostChunks)
+    const char* hk = std::getenv("DGB_HOST_CHUNKS");
+    c->host_chunks = hk ? std::max(1, std::min(kHostChunks, std::atoi(hk))) : kHostChunksDefault;
   }
   c->D = P.D; c->p = P.p; c->nf = P.N_F; c->ns = P.N_s; c->ne = P.N_E;
   c->ld = (P.N_E + 63) / 64 * 64;
@@ -1557,7 +1560,7 @@ extern "C" int dgb_advance_host(dgb_ctx* c, double* U, int scheme, int nsteps, d
   if (int rc = reset_scalars(c, cfl ? 0.0 : dt)) return rc;
   c->ind_step = 0;  // the state comes from the host: the learned indicator scores the first step
   const size_t per = (size_t)c->nf * c->ns;  // values per element in the reference layout
-  const int nch = std::min(kHostChunks, c->ne);
+  const int nch = std::min(c->host_chunks, c->ne);
   auto first = [&](int j) { return (int)((long long)c->ne * j / nch); };
   cudaStream_t up = c->hl_st[0], down = c->hl_st[1];
   DGB_CUDA(cudaEventRecord(c->e0, c->st));
