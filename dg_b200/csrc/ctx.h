@@ -37,7 +37,7 @@ inline cudaError_t allow_dynamic_smem(K* kernel, size_t bytes) {
 }
 
 // element chunks of the host-resident time loop's copies (dgb_advance_host): at most, by default
-constexpr int kHostChunks = 16, kHostChunksDefault = 8;
+constexpr int kHostChunks = 16, kHostChunksDefault = 16;
 
 enum { KC_RESIDUAL = 0, KC_LIMITER = 1, KC_DT = 2, KC_INDICATOR = 3, KC_OTHER = 4, KC_N = 5 };
 }
