@@ -110,10 +110,12 @@ struct dgb_ctx {
   // destroys the captured steps (their kernel arguments or launch sequence changed)
   unsigned graph_gen = 0;   // counts drop_graphs calls (captured slab steps compare it)
   double* halo_send[2] = {nullptr, nullptr};  // slab mode, local exchange: packed owned rows per side
-  // dgb_advance_host: upload / download streams, per-chunk events, the step's end
+  // dgb_advance_host: upload / download streams, per-chunk events (uploaded, downloaded, converted
+  // for the download), the end of the last download
   int host_chunks = dgb::kHostChunksDefault;
   cudaStream_t hl_st[2] = {nullptr, nullptr};
-  cudaEvent_t hl_up[dgb::kHostChunks] = {}, hl_down[dgb::kHostChunks] = {}, hl_done = nullptr;
+  cudaEvent_t hl_up[dgb::kHostChunks] = {}, hl_down[dgb::kHostChunks] = {}, hl_conv[dgb::kHostChunks] = {};
+  cudaEvent_t hl_done = nullptr;
   void drop_graphs() {
     ++graph_gen;
     for (auto& a : graphs)

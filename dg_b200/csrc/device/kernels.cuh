@@ -925,6 +925,51 @@ static __global__ void internal_to_ref_kernel(const double* __restrict__ Uint, d
     Uref[((size_t)e * nf + f) * ns + perm[t]] = Uint[(size_t)(f * ns + t) * ld + e];
   }
 }
+// The same conversions through a shared-memory tile of CONV_EB elements, so that both layouts are
+// read and written in contiguous runs: the element-major reference block (CONV_EB * nf * ns
+// values in a row) on one side, CONV_EB consecutive elements of every (field, node) plane on the
+// other.  Grid-stride over the element blocks; dynamic shared memory CONV_EB * (nf * ns + 1) doubles.
+constexpr int CONV_EB = 16;
+inline size_t convert_smem_bytes(int nf, int ns) { return sizeof(double) * CONV_EB * (nf * ns + 1); }
+template <bool TO_INTERNAL>
+__global__ void __launch_bounds__(256) convert_layout_kernel(const double* __restrict__ src, double* __restrict__ dst,
+                                                             const int* __restrict__ perm, int n_elem, int nf, int ns,
+                                                             int ld) {
+  extern __shared__ double cs_tile[];  // [element][reference-layout value], pitch nv + 1
+  const int nv = nf * ns, pitch = nv + 1, nblocks = (n_elem + CONV_EB - 1) / CONV_EB;
+  for (int b = blockIdx.x; b < nblocks; b += gridDim.x) {
+    const int e0 = b * CONV_EB, ne = min(CONV_EB, n_elem - e0);
+    if (TO_INTERNAL) {
+      const double* s = src + (size_t)e0 * nv;
+      for (int j = threadIdx.x; j < ne * nv; j += blockDim.x) {
+        const int el = j / nv;
+        cs_tile[el * pitch + (j - el * nv)] = s[j];
+      }
+      __syncthreads();
+      for (int j = threadIdx.x; j < nv * CONV_EB; j += blockDim.x) {
+        const int q = j / CONV_EB, el = j - q * CONV_EB;  // q = f * ns + t (internal plane)
+        if (el >= ne) continue;
+        const int f = q / ns, t = q - f * ns;
+        dst[(size_t)q * ld + e0 + el] = cs_tile[el * pitch + f * ns + __ldg(perm + t)];
+      }
+    } else {
+      for (int j = threadIdx.x; j < nv * CONV_EB; j += blockDim.x) {
+        const int q = j / CONV_EB, el = j - q * CONV_EB;
+        if (el >= ne) continue;
+        const int f = q / ns, t = q - f * ns;
+        cs_tile[el * pitch + f * ns + __ldg(perm + t)] = src[(size_t)q * ld + e0 + el];
+      }
+      __syncthreads();
+      double* d = dst + (size_t)e0 * nv;
+      for (int j = threadIdx.x; j < ne * nv; j += blockDim.x) {
+        const int el = j / nv;
+        d[j] = cs_tile[el * pitch + (j - el * nv)];
+      }
+    }
+    __syncthreads();  // the tile is rewritten by the next block
+  }
+}
+
 // y = x + beta*d over n values (Ustar = Us + beta DU, rk.cc:167-168)
 static __global__ void axpy_kernel(const double* __restrict__ x, const double* __restrict__ d, double beta,
                             double* __restrict__ y, size_t n, const DevScalars* __restrict__ scal) {

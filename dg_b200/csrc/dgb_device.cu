@@ -883,17 +883,22 @@ int step_rk4(dgb_ctx* c, bool cfl, bool score = true) {
   return 0;
 }
 
-int to_internal(dgb_ctx* c, const double* Uref_dev, double* Uint) {
-  const int grid = (int)std::min<size_t>(((size_t)c->ne * c->nf * c->ns + 255) / 256, 148 * 32);
-  ref_to_internal_kernel<<<grid, 256, 0, c->st>>>(Uref_dev, Uint, c->perm, c->ne, c->nf, c->ns, c->ld);
+// layout conversions of elements [e0, e0 + n) (reference <-> internal) on the context's stream
+int convert_range(dgb_ctx* c, bool to_int, const double* src, double* dst, int e0, int n) {
+  const size_t per = (size_t)c->nf * c->ns, smem = convert_smem_bytes(c->nf, c->ns);
+  const int grid = std::max(1, std::min((n + CONV_EB - 1) / CONV_EB, c->sm_count * 16));
+  if (to_int)
+    convert_layout_kernel<true><<<grid, 256, smem, c->st>>>(src + e0 * per, dst + e0, c->perm, n, c->nf, c->ns, c->ld);
+  else
+    convert_layout_kernel<false><<<grid, 256, smem, c->st>>>(src + e0, dst + e0 * per, c->perm, n, c->nf, c->ns, c->ld);
   DGB_CUDA(cudaGetLastError());
   return 0;
 }
+int to_internal(dgb_ctx* c, const double* Uref_dev, double* Uint) {
+  return convert_range(c, true, Uref_dev, Uint, 0, c->ne);
+}
 int to_ref(dgb_ctx* c, const double* Uint, double* Uref_dev) {
-  const int grid = (int)std::min<size_t>(((size_t)c->ne * c->nf * c->ns + 255) / 256, 148 * 32);
-  internal_to_ref_kernel<<<grid, 256, 0, c->st>>>(Uint, Uref_dev, c->perm, c->ne, c->nf, c->ns, c->ld);
-  DGB_CUDA(cudaGetLastError());
-  return 0;
+  return convert_range(c, false, Uint, Uref_dev, 0, c->ne);
 }
 size_t ref_bytes(dgb_ctx* c) { return (size_t)c->ne * c->nf * c->ns * sizeof(double); }
 
@@ -1147,6 +1152,7 @@ extern "C" void dgb_destroy(dgb_ctx* c) {
   for (auto ev : c->ev_pool) cudaEventDestroy(ev);
   for (auto ev : c->hl_up) if (ev) cudaEventDestroy(ev);
   for (auto ev : c->hl_down) if (ev) cudaEventDestroy(ev);
+  for (auto ev : c->hl_conv) if (ev) cudaEventDestroy(ev);
   if (c->hl_done) cudaEventDestroy(c->hl_done);
   for (auto st : c->hl_st) if (st) cudaStreamDestroy(st);
   if (c->e0) cudaEventDestroy(c->e0);
@@ -1553,6 +1559,7 @@ extern "C" int dgb_advance_host(dgb_ctx* c, double* U, int scheme, int nsteps, d
     for (auto& st : c->hl_st) DGB_CUDA(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
     for (auto& e : c->hl_up) DGB_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
     for (auto& e : c->hl_down) DGB_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    for (auto& e : c->hl_conv) DGB_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
     DGB_CUDA(cudaEventCreateWithFlags(&c->hl_done, cudaEventDisableTiming));
   }
   if (nsteps > 0)
@@ -1574,19 +1581,17 @@ extern "C" int dgb_advance_host(dgb_ctx* c, double* U, int scheme, int nsteps, d
       DGB_CUDA(cudaMemcpyAsync(c->ref + e0 * per, U + e0 * per, n * per * sizeof(double), cudaMemcpyHostToDevice, up));
       DGB_CUDA(cudaEventRecord(c->hl_up[j], up));
       DGB_CUDA(cudaStreamWaitEvent(c->st, c->hl_up[j], 0));
-      const int grid = (int)std::min<size_t>((n * per + 255) / 256, 148 * 32);
-      ref_to_internal_kernel<<<grid, 256, 0, c->st>>>(c->ref + e0 * per, c->A + e0, c->perm, n, c->nf, c->ns, c->ld);
-      DGB_CUDA(cudaGetLastError());
+      if (int rc = convert_range(c, true, c->ref, c->A, e0, n)) return rc;
     }
     const int k = !c->ind_on || c->ind_every <= 1 || c->ind_step % c->ind_every == 0 ? 0 : 1;
     DGB_CUDA(cudaGraphLaunch(c->graphs[si][mi][k], c->st));
-    launches += c->graph_launches[si][mi][k] + nch + 1;
+    launches += c->graph_launches[si][mi][k] + 2 * nch;
     ++c->ind_step;
-    if (int rc = to_ref(c, c->A, c->ref)) return rc;
-    DGB_CUDA(cudaEventRecord(c->hl_done, c->st));
-    DGB_CUDA(cudaStreamWaitEvent(down, c->hl_done, 0));
-    for (int j = 0; j < nch; ++j) {
+    for (int j = 0; j < nch; ++j) {  // each chunk's download starts once it is converted
       const int e0 = first(j), n = first(j + 1) - e0;
+      if (int rc = convert_range(c, false, c->A, c->ref, e0, n)) return rc;
+      DGB_CUDA(cudaEventRecord(c->hl_conv[j], c->st));
+      DGB_CUDA(cudaStreamWaitEvent(down, c->hl_conv[j], 0));
       DGB_CUDA(cudaMemcpyAsync(U + e0 * per, c->ref + e0 * per, n * per * sizeof(double), cudaMemcpyDeviceToHost, down));
       DGB_CUDA(cudaEventRecord(c->hl_down[j], down));
     }
