@@ -222,7 +222,8 @@ int dgb_advance(dgb_ctx* c, int scheme, int nsteps, double dt, double* time);
  * copy streams, a chunk's upload for the next step waiting only for its own download, so the host
  * link's two directions overlap.  U_host should be pinned (cudaHostAlloc / cudaHostRegister) for
  * the copies to run asynchronously.  The learned indicator scores the first step of the call.
- * Status and *time as dgb_advance; returns after the last download.  No counterpart in the
+ * Status and *time as dgb_advance; returns after the last download.  Refused (DGB_ERR_UNSUPPORTED)
+ * while per-kernel profiling is on (dgb_set_profiling), which times eager launches.  No counterpart in the
  * reference, whose state lives in host memory between its per-stage device launches. */
 int dgb_advance_host(dgb_ctx* c, double* U_host, int scheme, int nsteps, double dt, double* time);
 
