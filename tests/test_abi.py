@@ -2,6 +2,7 @@
 import re
 from pathlib import Path
 
+import numpy as np
 import pytest
 
 ROOT = Path(__file__).resolve().parents[1]
@@ -36,6 +37,19 @@ def test_device_calls_fail_loudly_without_gpu():
     with pytest.raises(dgb.DGBError) as e:
         dgb.DGSolver(p)
     assert e.value.code == 9  # DGB_ERR_NO_DEVICE
+
+
+def test_time_loops_refuse_a_null_context_before_any_device_call():
+    """dgb_advance, dgb_advance_host and the state transfers check their arguments first, so a
+    null context or array is DGB_ERR_ARG with or without a GPU."""
+    from dg_b200 import _ffi as F
+    L = F.lib()
+    U = np.zeros(4)
+    assert L.dgb_advance(None, F.SSPRK3, 1, 0.0, None) == F.ERR_ARG
+    assert L.dgb_advance_host(None, F.dptr(U), F.SSPRK3, 1, 0.0, None) == F.ERR_ARG
+    assert L.dgb_set_state(None, F.dptr(U)) == F.ERR_ARG
+    assert L.dgb_get_state(None, F.dptr(U)) == F.ERR_ARG
+    assert b"null" in L.dgb_last_error()
 
 
 def test_error_codes_for_bad_input(tmp_path):
